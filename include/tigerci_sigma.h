@@ -1,0 +1,122 @@
+/*
+ * tigerci_sigma.h - C ABI of the B200 sigma-vector build for TigerCI's
+ * multireference singles-and-doubles CI (MRSDCI).
+ *
+ * All integers are int64_t (TigerCI is compiled with -fdefault-integer-8,
+ * tiger_ci/CMakeLists.txt:39), all reals are double.  Every entry point that
+ * returns int returns 0 on success and a non-zero TCI_ERR_* code otherwise; it
+ * never aborts the process.  The message of the last failure on the calling
+ * thread is available from tci_last_error().  Contexts are owned by the
+ * library and are not thread-safe: use one context per stream / request.
+ */
+#ifndef TIGERCI_SIGMA_H
+#define TIGERCI_SIGMA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCI_OK 0
+#define TCI_ERR_ARG 1      /* bad argument (null pointer, size mismatch)          */
+#define TCI_ERR_CUDA 2     /* CUDA runtime failure or no usable device            */
+#define TCI_ERR_INPUT 3    /* input deck / operator inconsistent or unsupported   */
+#define TCI_ERR_INTERNAL 4 /* internal consistency check failed                   */
+#define TCI_ERR_MEMORY 5   /* device or host allocation failed / over budget      */
+#define TCI_ERR_TIMEOUT 6  /* a bounded device wait gave up                       */
+
+typedef struct tci_space tci_space;
+typedef struct tci_plan tci_plan;
+typedef struct tci_ctx tci_ctx;
+
+/* Input keywords that define the CSF space (tc/InputReader.cpp:36-196):
+ * NUMBER OF ORBITALS / FROZEN / INACTIVE / ACTIVE ORBITALS, NUMBER OF
+ * ELECTRONS, SPIN MULTIPLICITY, NUMBER OF REFERENCES, REFERENCE OCCUPATIONS.
+ * Optional local pair domains (allowed virtuals per internal path, the data of
+ * tiger_fortran/allowed_virtuals_mod.f90) are given in CSR form over the N-1
+ * and N-2 paths in lexical order, external indices 0-based and sorted; a path
+ * whose list is the single entry -1 is removed.  NULL pointers mean non-local. */
+typedef struct tci_deck {
+  int64_t num_orbitals;
+  int64_t num_frozen;
+  int64_t num_inactive;
+  int64_t num_active;
+  int64_t num_elec;
+  int64_t spin_mult;
+  int64_t num_ref;
+  const int64_t* ref_occ; /* num_ref x (num_inactive + num_active), row major */
+  const int64_t* nm1_domain_ptr;
+  const int64_t* nm1_domain_idx;
+  const int64_t* nm2_domain_ptr;
+  const int64_t* nm2_domain_idx;
+} tci_deck;
+
+/* Molecular-orbital Hamiltonian.  h is num_orbitals x num_orbitals (symmetric,
+ * row major).  chol holds the Cholesky vectors in the layout of TigerCI's
+ * cholesky_data%cho_vectors(numcho, npair) (tiger_fortran/cholesky_structs.f90:35-39):
+ * element (J, pq) at chol[pq * nchol + J] with pq = p(p+1)/2 + q, p >= q,
+ * 0-based orbitals, so that (pq|rs) = sum_J L^J_pq L^J_rs. */
+typedef struct tci_operator {
+  const double* h;
+  const double* chol;
+  int64_t nchol;
+  double core_energy;
+} tci_operator;
+
+/* Thread-local message of the last failure (empty string if none). */
+int tci_last_error(char* buf, int64_t len);
+
+/* ---- CSF space (host only; no GPU needed) --------------------------------
+ * Replaces graph_driver (tiger_fortran/graph_mod.f90:48-99): distinct-row
+ * table, tree search and CI-vector index vectors. */
+int tci_space_create(const tci_deck* deck, tci_space** out);
+/* out[0..11]: total_csfs, num_valence, num_nm1, num_nm2, total_configurations,
+ * removed, open_shells, paths(N), paths(N-1), paths(N-2), num_vertices, n_domains */
+int tci_space_counts(const tci_space* sp, int64_t* out, int64_t len);
+/* Index vector of kind 0 (valence, internal_index_vector0), 1 (N-1, vector1),
+ * 2 (N-2 "ab", vector2) or 3 (N-2 "aa", vector3): 1-based CSF offsets as in the
+ * reference, kill_number (-1000000) for removed paths.  len = number of paths. */
+int tci_space_index_vector(const tci_space* sp, int64_t kind, int64_t* out, int64_t len);
+/* Occupation (num_internal entries) and info[0..5] = lex, singles, kept, nsf,
+ * nsf_aa, n_virtuals of path lex (1-based) of kind 0/1/2. */
+int tci_space_path(const tci_space* sp, int64_t kind, int64_t lex, int64_t* occ, int64_t* info);
+/* Number of "For s singles there are f spinfunctions and c configurations"
+ * entries of block kind (0 valence, 1 N-1, 2 N-2), written as (s, f, c) triples. */
+int tci_space_block_counts(const tci_space* sp, int64_t kind, int64_t* out, int64_t max_triples, int64_t* n_triples);
+void tci_space_destroy(tci_space* sp);
+
+/* ---- Sigma plan (host only) ------------------------------------------------
+ * Replaces the iteration-1 loop enumeration ("dry run") of the sigma build:
+ * every coupling coefficient and task table, built once. */
+int tci_plan_create(const tci_deck* deck, const tci_operator* op, tci_plan** out);
+/* Writes the plan as a flat binary file (layout: tigerci_b200/plan_io.py). */
+int tci_plan_export(const tci_plan* plan, const char* path);
+/* out[0..7]: total_csfs, n_dense, n_singlet, n_triplet, flops_allext,
+ * flops_total, bytes_allext, n_steps */
+int tci_plan_stats(const tci_plan* plan, double* out, int64_t len);
+void tci_plan_destroy(tci_plan* plan);
+
+/* ---- Device sigma build ------------------------------------------------------
+ * Replaces htimesc(civec, sigmavec, data) (tiger_fortran/htimesc.f90:46-147).
+ * tci_sigma_init uploads the operator, builds the integral banks and the plan on
+ * `device`.  tci_sigma accumulates sigma += H c exactly like htimesc (the caller
+ * zeroes sigma, tiger_fortran/davidson.f90:126); c and sigma are host arrays of
+ * length total_csfs.  tci_sigma_device does the same on device arrays on the
+ * given cudaStream_t (NULL = the context's stream). */
+int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out);
+int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n);
+int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n, void* stream);
+/* Diagonal H_ii (tiger_fortran/diag_element_mod_2.f90:83) for the
+ * preconditioner, host array of length total_csfs. */
+int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n);
+/* out[0..7]: total_csfs, device bytes held, init seconds, last sigma ms,
+ * flops per sigma, all-external flops, all-external bytes, sigma builds */
+int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len);
+void tci_destroy(tci_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TIGERCI_SIGMA_H */

@@ -1,0 +1,199 @@
+"""Python host API over the C ABI, mirroring TigerCI's own interfaces.
+
+* ``Deck`` holds the input keywords that define the CSF space
+  (tc/InputReader.cpp:36-196; REFERENCE OCCUPATIONS as strings).
+* ``CsfSpace`` replaces ``graph_driver`` (tiger_fortran/graph_mod.f90:48-99).
+* ``Plan`` exposes the host-built sigma plan (replaces the iteration-1 dry run).
+* ``SigmaBuilder.htimesc(civec, sigmavec)`` accumulates sigma += H c exactly
+  like ``htimesc`` (tiger_fortran/htimesc.f90:46); the caller zeroes sigma.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import TciDeck, TciOperator, check, lib, ptr
+
+KILL_NUMBER = -1000000
+
+
+@dataclass
+class Deck:
+    num_orbitals: int
+    num_inactive: int
+    num_active: int
+    num_elec: int
+    spin_mult: int
+    refs: Sequence[str]
+    num_frozen: int = 0
+    nm1_domains: Optional[Sequence[Sequence[int]]] = None
+    nm2_domains: Optional[Sequence[Sequence[int]]] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def num_internal(self):
+        return self.num_inactive + self.num_active
+
+    @property
+    def num_external(self):
+        return self.num_orbitals - self.num_internal
+
+    def c_struct(self) -> TciDeck:
+        nint = self.num_internal
+        occ = np.array([[int(ch) for ch in str(r)[:nint]] for r in self.refs], dtype=np.int64)
+        if occ.shape[1] != nint:
+            raise ValueError("reference occupation strings must cover the internal orbitals")
+        self._keep = [occ]
+        d = TciDeck(self.num_orbitals, self.num_frozen, self.num_inactive, self.num_active, self.num_elec,
+                    self.spin_mult, len(self.refs), ptr(occ), None, None, None, None)
+        for name, doms in (("nm1", self.nm1_domains), ("nm2", self.nm2_domains)):
+            if doms is None:
+                continue
+            p = np.zeros(len(doms) + 1, dtype=np.int64)
+            for i, dm in enumerate(doms):
+                p[i + 1] = p[i] + len(dm)
+            idx = np.concatenate([np.asarray(dm, dtype=np.int64) for dm in doms]) if len(doms) else np.zeros(0, np.int64)
+            idx = np.ascontiguousarray(idx, dtype=np.int64)
+            self._keep += [p, idx]
+            setattr(d, f"{name}_domain_ptr", ptr(p))
+            setattr(d, f"{name}_domain_idx", ptr(idx))
+        return d
+
+
+class CsfSpace:
+    """Distinct-row table, tree search and CI-vector index vectors."""
+
+    def __init__(self, deck: Deck):
+        self.deck = deck
+        self._d = deck.c_struct()
+        h = C.c_void_p()
+        check(lib().tci_space_create(C.byref(self._d), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().tci_space_destroy(self._h)
+            self._h = None
+
+    def counts(self) -> dict:
+        out = np.zeros(12, dtype=np.int64)
+        check(lib().tci_space_counts(self._h, ptr(out), 12))
+        keys = ["total_csfs", "num_valence", "num_nm1", "num_nm2", "total_configurations", "removed",
+                "open_shells", "paths_v", "paths_nm1", "paths_nm2", "num_vertices", "n_domains"]
+        return dict(zip(keys, (int(x) for x in out)))
+
+    def index_vector(self, kind: int) -> np.ndarray:
+        c = self.counts()
+        n = [c["paths_v"], c["paths_nm1"], c["paths_nm2"], c["paths_nm2"]][kind]
+        out = np.zeros(n, dtype=np.int64)
+        check(lib().tci_space_index_vector(self._h, kind, ptr(out), n))
+        return out
+
+    def path(self, kind: int, lex: int):
+        occ = np.zeros(self.deck.num_internal, dtype=np.int64)
+        info = np.zeros(6, dtype=np.int64)
+        check(lib().tci_space_path(self._h, kind, lex, ptr(occ), ptr(info)))
+        return occ, dict(zip(["lex", "singles", "kept", "nsf", "nsf_aa", "n_virt"], (int(x) for x in info)))
+
+    def block_counts(self, kind: int) -> dict:
+        out = np.zeros(3 * 64, dtype=np.int64)
+        nt = C.c_int64()
+        check(lib().tci_space_block_counts(self._h, kind, ptr(out), 64, C.byref(nt)))
+        return {int(out[3 * t]): (int(out[3 * t + 1]), int(out[3 * t + 2])) for t in range(nt.value)}
+
+
+class Operator:
+    """MO Hamiltonian: h (n_orb x n_orb) and Cholesky vectors in TigerCI's
+    cho_vectors(numcho, npair) layout, i.e. chol[pair, J] with
+    pair = p(p+1)/2 + q for p >= q (0-based)."""
+
+    def __init__(self, h: np.ndarray, chol: np.ndarray, core_energy: float = 0.0):
+        self.h = np.ascontiguousarray(h, dtype=np.float64)
+        self.chol = np.ascontiguousarray(chol, dtype=np.float64)
+        n = self.h.shape[0]
+        if self.h.shape != (n, n) or self.chol.ndim != 2 or self.chol.shape[0] != n * (n + 1) // 2:
+            raise ValueError("h must be n x n and chol n(n+1)/2 x nchol")
+        self.core_energy = float(core_energy)
+
+    @property
+    def nchol(self):
+        return self.chol.shape[1]
+
+    def c_struct(self) -> TciOperator:
+        return TciOperator(ptr(self.h), ptr(self.chol), self.nchol, self.core_energy)
+
+
+class Plan:
+    """Host-built sigma plan (no GPU)."""
+
+    def __init__(self, deck: Deck, op: Operator):
+        self._d = deck.c_struct()
+        self._o = op.c_struct()
+        self._op = op
+        h = C.c_void_p()
+        check(lib().tci_plan_create(C.byref(self._d), C.byref(self._o), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().tci_plan_destroy(self._h)
+            self._h = None
+
+    def export(self, path: str):
+        check(lib().tci_plan_export(self._h, path.encode()))
+
+    def stats(self) -> dict:
+        out = np.zeros(8, dtype=np.float64)
+        check(lib().tci_plan_stats(self._h, ptr(out), 8))
+        keys = ["total_csfs", "n_dense", "n_singlet", "n_triplet", "flops_allext", "flops_total", "bytes_allext",
+                "n_steps"]
+        return dict(zip(keys, out.tolist()))
+
+
+class SigmaBuilder:
+    """Device-resident sigma = H c on one GPU (the htimesc slot)."""
+
+    def __init__(self, deck: Deck, op: Operator, device: int = 0):
+        self._d = deck.c_struct()
+        self._o = op.c_struct()
+        self._op = op
+        h = C.c_void_p()
+        check(lib().tci_sigma_init(C.byref(self._d), C.byref(self._o), device, C.byref(h)))
+        self._h = h
+        self.n = int(self.stats()["total_csfs"])
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tci_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def htimesc(self, civec: np.ndarray, sigmavec: np.ndarray):
+        """sigmavec += H civec (host float64 arrays of length total_csfs)."""
+        if civec.dtype != np.float64 or sigmavec.dtype != np.float64:
+            raise TypeError("float64 arrays required")
+        if not (civec.flags.c_contiguous and sigmavec.flags.c_contiguous):
+            raise ValueError("contiguous arrays required")
+        check(lib().tci_sigma(self._h, ptr(civec), ptr(sigmavec), civec.size))
+
+    def sigma(self, civec: np.ndarray) -> np.ndarray:
+        s = np.zeros_like(civec, dtype=np.float64)
+        self.htimesc(np.ascontiguousarray(civec, dtype=np.float64), s)
+        return s
+
+    def htimesc_device(self, c_ptr: int, s_ptr: int, n: int, stream: int = 0):
+        """Device pointers (e.g. torch tensors' data_ptr()) on `stream`."""
+        check(lib().tci_sigma_device(self._h, C.c_void_p(c_ptr), C.c_void_p(s_ptr), n, C.c_void_p(stream or None)))
+
+    def stats(self) -> dict:
+        out = np.zeros(8, dtype=np.float64)
+        check(lib().tci_ctx_stats(self._h, ptr(out), 8))
+        keys = ["total_csfs", "device_bytes", "init_seconds", "last_sigma_ms", "flops_per_sigma",
+                "flops_allext", "bytes_allext", "sigma_count"]
+        return dict(zip(keys, out.tolist()))

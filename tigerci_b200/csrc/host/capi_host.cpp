@@ -1,0 +1,281 @@
+// Host-only part of the C ABI (include/tigerci_sigma.h): error reporting, CSF
+// space queries and plan construction / export.  No CUDA dependency.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../../include/tigerci_sigma.h"
+#include "capi_internal.h"
+#include "plan.h"
+
+namespace tci {
+thread_local std::string g_last_error;
+void set_error(const std::string& m) { g_last_error = m; }
+}  // namespace tci
+
+using namespace tci;
+
+struct tci_space {
+  CsfSpace sp;
+};
+struct tci_plan {
+  CsfSpace sp;
+  Plan plan;
+};
+
+namespace tci {
+
+int guard_status(const std::exception_ptr& ep) {
+  try {
+    std::rethrow_exception(ep);
+  } catch (const Error& e) {
+    set_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return TCI_ERR_MEMORY;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return TCI_ERR_INTERNAL;
+  } catch (...) {
+    set_error("unknown failure");
+    return TCI_ERR_INTERNAL;
+  }
+}
+
+void deck_from_c(const tci_deck* d, Deck& out, DomainSpec& dom) {
+  if (!d) throw Error(TCI_ERR_ARG, "deck is null");
+  out.num_orbitals = d->num_orbitals;
+  out.num_frozen = d->num_frozen;
+  out.num_inactive = d->num_inactive;
+  out.num_active = d->num_active;
+  out.num_elec = d->num_elec;
+  out.spin_mult = d->spin_mult;
+  out.num_ref = d->num_ref;
+  const i64 nint = out.num_internal();
+  if (out.num_orbitals <= 0 || nint <= 0 || out.num_ref <= 0 || out.num_frozen < 0 ||
+      out.num_frozen > out.num_inactive || nint >= out.num_orbitals)
+    throw Error(TCI_ERR_INPUT, "inconsistent orbital counts in deck");
+  if (!d->ref_occ) throw Error(TCI_ERR_ARG, "reference occupations are null");
+  out.refs.resize(out.num_ref * nint);
+  for (i64 i = 0; i < out.num_ref * nint; ++i) {
+    const i64 v = d->ref_occ[i];
+    if (v < 0 || v > 2) throw Error(TCI_ERR_INPUT, "reference occupation outside 0..2");
+    out.refs[i] = (int)v;
+  }
+  auto csr = [&](const int64_t* ptr, const int64_t* idx, std::vector<std::vector<int>>& dst) {
+    dst.clear();
+    if (!ptr) return;
+    if (!idx) throw Error(TCI_ERR_ARG, "domain index array is null");
+    return;  // filled once the path counts are known (see expand_domains)
+  };
+  csr(d->nm1_domain_ptr, d->nm1_domain_idx, dom.nm1);
+  csr(d->nm2_domain_ptr, d->nm2_domain_idx, dom.nm2);
+}
+
+void build_space_from_c(const tci_deck* d, CsfSpace& sp) {
+  Deck deck;
+  DomainSpec dom;
+  deck_from_c(d, deck, dom);
+  if (d->nm1_domain_ptr || d->nm2_domain_ptr) {
+    // path counts are needed to read the CSR arrays: build once non-locally
+    CsfSpace probe;
+    build_csf_space(deck, DomainSpec(), probe);
+    auto rd = [&](const int64_t* ptr, const int64_t* idx, size_t np, std::vector<std::vector<int>>& dst) {
+      if (!ptr) return;
+      dst.resize(np);
+      for (size_t p = 0; p < np; ++p) {
+        if (ptr[p + 1] < ptr[p]) throw Error(TCI_ERR_INPUT, "domain CSR pointers decrease");
+        for (int64_t t = ptr[p]; t < ptr[p + 1]; ++t) dst[p].push_back((int)idx[t]);
+      }
+    };
+    rd(d->nm1_domain_ptr, d->nm1_domain_idx, probe.paths[1].size(), dom.nm1);
+    rd(d->nm2_domain_ptr, d->nm2_domain_idx, probe.paths[2].size(), dom.nm2);
+  }
+  build_csf_space(deck, dom, sp);
+}
+
+void operator_from_c(const tci_operator* op, const CsfSpace& sp, Operator& out) {
+  if (!op || !op->h || !op->chol) throw Error(TCI_ERR_ARG, "operator or its arrays are null");
+  if (op->nchol <= 0) throw Error(TCI_ERR_INPUT, "nchol must be positive");
+  (void)sp;
+  out.h = op->h;
+  out.chol = op->chol;
+  out.nchol = op->nchol;
+  out.core_energy = op->core_energy;
+}
+
+}  // namespace tci
+
+extern "C" {
+
+int tci_last_error(char* buf, int64_t len) {
+  if (!buf || len <= 0) return TCI_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+  return TCI_OK;
+}
+
+int tci_space_create(const tci_deck* deck, tci_space** out) {
+  if (!out) return TCI_ERR_ARG;
+  *out = nullptr;
+  try {
+    auto* s = new tci_space();
+    try {
+      build_space_from_c(deck, s->sp);
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+int tci_space_counts(const tci_space* s, int64_t* out, int64_t len) {
+  if (!s || !out || len < 12) return TCI_ERR_ARG;
+  const CsfSpace& sp = s->sp;
+  out[0] = sp.total_csfs;
+  out[1] = sp.num_valence;
+  out[2] = sp.num_nm1;
+  out[3] = sp.num_nm2;
+  out[4] = sp.total_configurations;
+  out[5] = sp.removed;
+  out[6] = sp.open_shells;
+  out[7] = (int64_t)sp.paths[0].size();
+  out[8] = (int64_t)sp.paths[1].size();
+  out[9] = (int64_t)sp.paths[2].size();
+  out[10] = sp.num_vert;
+  out[11] = (int64_t)sp.domains.size();
+  return TCI_OK;
+}
+
+int tci_space_index_vector(const tci_space* s, int64_t kind, int64_t* out, int64_t len) {
+  if (!s || !out || kind < 0 || kind > 3) return TCI_ERR_ARG;
+  const auto& P = s->sp.paths[kind == 3 ? 2 : kind];
+  if (len != (int64_t)P.size()) {
+    set_error("index vector length mismatch");
+    return TCI_ERR_ARG;
+  }
+  for (size_t p = 0; p < P.size(); ++p) {
+    const Head& h = P[p];
+    i64 v = (kind == 3) ? h.off_aa : h.off;
+    out[p] = v >= 0 ? v + 1 : kKillNumber;
+  }
+  return TCI_OK;
+}
+
+int tci_space_path(const tci_space* s, int64_t kind, int64_t lex, int64_t* occ, int64_t* info) {
+  if (!s || kind < 0 || kind > 2 || !occ || !info) return TCI_ERR_ARG;
+  const auto& P = s->sp.paths[kind];
+  if (lex < 1 || lex > (int64_t)P.size()) return TCI_ERR_ARG;
+  const Head& h = P[lex - 1];
+  for (i64 j = 0; j < s->sp.n_int; ++j) occ[j] = h.occ.empty() ? -1 : h.occ[j];
+  info[0] = h.lex;
+  info[1] = h.singles;
+  info[2] = h.kept ? 1 : 0;
+  info[3] = h.nsf;
+  info[4] = h.nsf_aa;
+  info[5] = h.domain < 0 ? (kind == 0 ? 0 : 0) : (int64_t)s->sp.domains[h.domain].size();
+  return TCI_OK;
+}
+
+int tci_space_block_counts(const tci_space* s, int64_t kind, int64_t* out, int64_t max_triples, int64_t* n_triples) {
+  if (!s || kind < 0 || kind > 2 || !n_triples) return TCI_ERR_ARG;
+  const auto& m = s->sp.cfg_count[kind];
+  *n_triples = (int64_t)m.size();
+  int64_t t = 0;
+  for (auto& kv : m) {
+    if (t >= max_triples || !out) break;
+    out[3 * t + 0] = kv.first;
+    // the reference prints fsn before its final zeroing; recompute it here
+    SpinTables tb;
+    build_spin_tables((int)s->sp.open_shells, (int)s->sp.deck.spin_mult, tb);
+    out[3 * t + 1] = kv.first <= s->sp.open_shells ? tb.fsn_all[kv.first] : 0;
+    out[3 * t + 2] = kv.second;
+    ++t;
+  }
+  return TCI_OK;
+}
+
+void tci_space_destroy(tci_space* s) { delete s; }
+
+int tci_plan_create(const tci_deck* deck, const tci_operator* op, tci_plan** out) {
+  if (!out) return TCI_ERR_ARG;
+  *out = nullptr;
+  try {
+    auto* p = new tci_plan();
+    try {
+      build_space_from_c(deck, p->sp);
+      Operator o;
+      operator_from_c(op, p->sp, o);
+      build_plan(p->sp, o, p->plan);
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *out = p;
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+int tci_plan_export(const tci_plan* p, const char* path) {
+  if (!p || !path) return TCI_ERR_ARG;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    set_error(std::string("cannot open ") + path);
+    return TCI_ERR_ARG;
+  }
+  const Plan& P = p->plan;
+  auto wi = [&](int64_t v) { std::fwrite(&v, 8, 1, f); };
+  auto wd = [&](double v) { std::fwrite(&v, 8, 1, f); };
+  std::fwrite("TCIPLAN1", 1, 8, f);
+  const std::vector<Step>* lists[2] = {&P.init_steps, &P.sigma_steps};
+  wi(P.nint); wi(P.n); wi(P.nchol); wi(P.total_csfs); wi(P.npair_all); wi(P.nD);
+  wi((int64_t)P.dheads.size()); wi(NUM_BUFS); wi((int64_t)P.init_steps.size()); wi((int64_t)P.sigma_steps.size());
+  wi((int64_t)P.h_vv.size()); wi((int64_t)P.wv.size()); wi(P.np); wi(P.nm);
+  for (int b = 0; b < NUM_BUFS; ++b) wi(P.buf_size[b]);
+  for (auto& d : P.dheads) { wi(d.off_ab); wi(d.off_aa); wi(d.nsf_ab); wi(d.nsf_aa); wi(d.nsing); wi(d.nD); wi(d.dk0); }
+  for (double v : P.dk_sign) wd(v);
+  for (double v : P.h_vv) wd(v);
+  for (double v : P.wv) wd(v);
+  for (auto* L : lists)
+    for (const Step& s : *L) {
+      wi(s.kind);
+      char name[64] = {0};
+      std::snprintf(name, sizeof(name), "%s", s.name.c_str());
+      std::fwrite(name, 1, 64, f);
+      wi((int64_t)s.gp.size()); wi((int64_t)s.gs.size()); wi((int64_t)s.at.size());
+      wi((int64_t)s.as.size()); wi((int64_t)s.dt.size()); wi((int64_t)s.ds.size());
+      wi(s.buf); wi(s.off); wi(s.len);
+      for (auto& g : s.gp) { wi(g.c); wi(g.offC); wi(g.ldc); wi(g.M); wi(g.N); wd(g.beta); wi(g.seg_begin); wi(g.seg_end); }
+      for (auto& g : s.gs) { wi(g.a); wi(g.b); wi(g.offA); wi(g.lda); wi(g.offB); wi(g.ldb); wi(g.K); wi(g.tA); wi(g.tB); wd(g.alpha); }
+      for (auto& t : s.at) { wi(t.dst); wi(t.off); wi(t.len); wi(t.src_begin); wi(t.src_end); }
+      for (auto& t : s.as) { wi(t.src); wi(t.off); wd(t.coef); wi(t.sbuf); wi(t.sidx); }
+      for (auto& t : s.dt) { wi(t.dst); wi(t.off); wi(t.src_begin); wi(t.src_end); }
+      for (auto& t : s.ds) { wi(t.a); wi(t.b); wi(t.aoff); wi(t.boff); wi(t.len); wd(t.coef); }
+    }
+  std::fclose(f);
+  return TCI_OK;
+}
+
+int tci_plan_stats(const tci_plan* p, double* out, int64_t len) {
+  if (!p || !out || len < 8) return TCI_ERR_ARG;
+  const Plan& P = p->plan;
+  out[0] = (double)P.total_csfs;
+  out[1] = (double)P.nD;
+  out[2] = (double)P.n_sing;
+  out[3] = (double)P.n_trip;
+  out[4] = P.flops_allext;
+  out[5] = P.flops_total;
+  out[6] = P.bytes_allext;
+  out[7] = (double)P.sigma_steps.size();
+  return TCI_OK;
+}
+
+void tci_plan_destroy(tci_plan* p) { delete p; }
+
+}  // extern "C"

@@ -1,0 +1,1071 @@
+// Builds the sigma plan (plan.h) for a non-local MRSDCI space.
+//
+// Term classes (external electrons N-2 = "D", N-1 = "S", valence = "V"), with
+// the reference routines they replace:
+//   DD all-external (ab|cd) ........ three_and_four_seg_mod_1.f90:318-632, 3240-3627
+//   DD two-external (ij|ab),(ia|jb)  three_and_four_seg_mod_2.f90:1000-1408, 7137-8005
+//                                    two_seg_mod_3.f90:274-406, 2177-2795 (same head)
+//   DS three-external (ia|bc) ...... three_and_four_seg_mod_1.f90:636-1756, 2867-3140
+//   DS one-external (ij|ka), h_ia .. two_seg_mod_3.f90:617, 2797; mod_1.f90:1757-2216
+//   DV two-external (ia|jb) ........ three_and_four_seg_mod_2.f90:7346-7408, 8007-8165
+//   SS two-external ................ three_and_four_seg_mod_2.f90:7792-7956; two_seg_mod_3.f90
+//   SV one-external ................ two_seg_mod_3.f90:617-883
+//   zero-external / same config .... two_seg_mod_3.f90:884-1065; mod_2.f90:305-6233; diagtimesc.f90
+// Coupling coefficients come from the CSF expansion of coupling.cpp applied to
+// model configurations in which the external orbitals are replaced by three
+// representative orbitals e0 < e1 < e2 placed after the internal ones (the
+// coupling depends only on the relative order of the open shells).  Each
+// coefficient is normalised against the dense-matrix form the device applies
+// (UNPACK -> products -> PACK), so one canonical external pattern fixes it.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <unordered_map>
+
+#include "coupling.h"
+
+namespace tci {
+
+namespace {
+
+const double kSqrt2 = std::sqrt(2.0);
+constexpr double kTiny = 1e-14;
+
+struct VecHash {
+  size_t operator()(const std::vector<int8_t>& v) const {
+    size_t h = 1469598103934665603ull;
+    for (int8_t x : v) h = (h ^ (uint8_t)x) * 1099511628211ull;
+    return h;
+  }
+};
+
+inline int parity_below(Det d, int x) {
+  Det m = d & ((((Det)1) << x) - 1);
+  return (__builtin_popcountll((uint64_t)m) + __builtin_popcountll((uint64_t)(m >> 64))) & 1;
+}
+
+struct Ints {
+  i64 norb = 0, nint = 0, n = 0, N = 0;
+  const double* h = nullptr;
+  const double* L = nullptr;
+  std::vector<double> I4;  // (ij|kl), internal
+  std::vector<double> I3;  // (iq|jk): [i][j][k][q]
+  static i64 pair(i64 p, i64 q) { return p >= q ? p * (p + 1) / 2 + q : q * (q + 1) / 2 + p; }
+  double eri(i64 p, i64 q, i64 r, i64 s) const {
+    const double* a = L + pair(p, q) * N;
+    const double* b = L + pair(r, s) * N;
+    double acc = 0;
+    for (i64 J = 0; J < N; ++J) acc += a[J] * b[J];
+    return acc;
+  }
+  double h1(i64 p, i64 q) const { return h[p * norb + q]; }
+  double i4(i64 i, i64 j, i64 k, i64 l) const { return I4[((i * nint + j) * nint + k) * nint + l]; }
+  const double* i3(i64 i, i64 j, i64 k) const { return I3.data() + ((i * nint + j) * nint + k) * n; }
+  void build() {
+    const i64 ni = nint;
+    I4.assign(ni * ni * ni * ni, 0.0);
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (i64 i = 0; i < ni; ++i)
+      for (i64 j = 0; j < ni; ++j)
+        for (i64 k = 0; k < ni; ++k)
+          for (i64 l = 0; l < ni; ++l) I4[((i * ni + j) * ni + k) * ni + l] = eri(i, j, k, l);
+    I3.assign(ni * ni * ni * n, 0.0);
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (i64 i = 0; i < ni; ++i)
+      for (i64 q = 0; q < n; ++q)
+        for (i64 j = 0; j < ni; ++j)
+          for (i64 k = 0; k < ni; ++k) I3[((i * ni + j) * ni + k) * n + q] = eri(i, ni + q, j, k);
+  }
+};
+
+// Bump allocator over one scratch buffer.
+struct Scratch {
+  i64 top = 0;
+  i64 alloc(i64 len) {
+    i64 o = top;
+    top += (len + 31) / 32 * 32;
+    return o;
+  }
+};
+
+struct Builder {
+  const CsfSpace& sp;
+  const Operator& op;
+  Plan& P;
+  SpinTables tables;
+  std::unique_ptr<CouplingEngine> eng;
+  Ints I;
+  i64 nint = 0, n = 0, n2 = 0, nab = 0, N = 0;
+  int e0 = 0, e1 = 0, e2 = 0;
+  std::unordered_map<std::vector<int8_t>, i64, VecHash> idx[3];
+  std::vector<i64> dk0, nDh;  // per N-2 path
+  i64 nF = 0;                 // matrices used in BUF_F
+  Scratch T;                  // BUF_T0 regions used per sigma build
+  i64 init_scratch = 0;       // BUF_T0 doubles used during init
+  i64 offJ = 0, offK = 0, offH = 0;
+
+  Builder(const CsfSpace& s, const Operator& o, Plan& p) : sp(s), op(o), P(p) {}
+
+  i64 Jof(i64 i, i64 j) const { return offJ + (i * nint + j) * n2; }
+  i64 Kof(i64 p, i64 q) const { return offK + (p * nint + q) * n2; }
+
+  std::vector<int8_t> ext(const Head& h, int x, int y) const {
+    std::vector<int8_t> o(h.occ.begin(), h.occ.end());
+    o.resize(nint + 3, 0);
+    if (x >= 0) o[x] += 1;
+    if (y >= 0) o[y] += 1;
+    return o;
+  }
+  Config cfgV(const Head& h) const { return Config{ext(h, -1, -1)}; }
+  Config cfgS(const Head& h, int x) const { return Config{ext(h, x, -1)}; }
+  Config cfgD(const Head& h, int x, int y) const { return Config{ext(h, x, y)}; }
+  const Head* find(int kind, const std::vector<int8_t>& occ) const {
+    auto it = idx[kind].find(occ);
+    if (it == idx[kind].end()) return nullptr;
+    const Head& h = sp.paths[kind][it->second];
+    return h.kept ? &h : nullptr;
+  }
+  std::vector<double> M(const Config& L, const Config& R, const Op& o) {
+    std::vector<double> m;
+    eng->matrix(L, R, o, m);
+    return m;
+  }
+  double sgn(const Head& h, i64 k) const { return P.dk_sign[dk0[h.lex - 1] + k]; }
+  i64 dk(const Head& h, i64 k) const { return dk0[h.lex - 1] + k; }
+  i64 nD(const Head& h) const { return nDh[h.lex - 1]; }
+  static bool has(const Head& h) { return h.kept && h.nsf > 0 && h.off >= 0; }
+
+  void run();
+  void setup_heads();
+  void init_steps();
+  void allext();
+  void dd_x();
+  void ds();
+  void dv();
+  void ss();
+  void sv();
+  void internal_blocks();
+  Step& step(std::vector<Step>& v, int kind, const char* name) {
+    v.push_back(Step());
+    v.back().kind = kind;
+    v.back().name = name;
+    return v.back();
+  }
+  void zero_step(std::vector<Step>& v, int buf, i64 off, i64 len, const char* name) {
+    Step& s = step(v, STEP_ZERO, name);
+    s.buf = buf;
+    s.off = off;
+    s.len = len;
+  }
+};
+
+void Builder::setup_heads() {
+  for (int k = 0; k < 3; ++k)
+    for (size_t p = 0; p < sp.paths[k].size(); ++p)
+      if (sp.paths[k][p].kept) idx[k][sp.paths[k][p].occ] = (i64)p;
+  const auto& D = sp.paths[2];
+  dk0.assign(D.size(), -1);
+  nDh.assign(D.size(), 0);
+  for (size_t p = 0; p < D.size(); ++p) {
+    const Head& h = D[p];
+    if (!h.kept) continue;
+    i64 nab_f = h.off >= 0 ? h.nsf : 0, naa_f = h.off_aa >= 0 ? h.nsf_aa : 0;
+    i64 nd = std::max(nab_f, naa_f);
+    if (nd == 0) continue;
+    dk0[p] = P.nD;
+    nDh[p] = nd;
+    DHeadInfo di{h.off >= 0 ? h.off : -1, h.off_aa, nab_f, naa_f, naa_f > 0 ? (i64)sp.fsn[h.singles] : 0, nd, P.nD};
+    P.dheads.push_back(di);
+    for (i64 k = 0; k < nd; ++k) P.dk_sign.push_back(k < di.nsing ? 1.0 : -1.0);
+    P.nD += nd;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Zero-external terms: all-internal Hamiltonian between configurations of one
+// kind with spectator externals, by Slater rules on the CSF determinants.
+void Builder::internal_blocks() {
+  Step& st = step(P.sigma_steps, STEP_AXPY, "zero-external");
+  struct Pat {
+    int kind, x, y, block;  // block: 0 valence, 1 N-1 row, 2 N-2 aa, 3 N-2 ab
+  };
+  const Pat pats[4] = {{0, -1, -1, 0}, {1, e0, -1, 1}, {2, e0, e0, 2}, {2, e0, e1, 3}};
+  const int ni = (int)nint;
+  for (const Pat& pt : pats) {
+    const auto& heads = sp.paths[pt.kind];
+    auto nsf_of = [&](const Head& h) -> i64 {
+      if (pt.block == 2) return h.off_aa >= 0 ? h.nsf_aa : 0;
+      if (pt.block == 3) return h.off >= 0 ? h.nsf : 0;
+      return h.off >= 0 ? h.nsf : 0;
+    };
+    auto off_of = [&](const Head& h) -> i64 { return pt.block == 2 ? h.off_aa : h.off; };
+    const i64 len = pt.block == 0 ? 1 : pt.block == 3 ? nab : n;
+    if (len == 0) continue;
+    auto cfg = [&](const Head& h) {
+      return pt.kind == 0 ? cfgV(h) : pt.kind == 1 ? cfgS(h, pt.x) : cfgD(h, pt.x, pt.y);
+    };
+    std::map<std::pair<i64, i64>, std::vector<double>> blocks;
+    for (size_t hs = 0; hs < heads.size(); ++hs) {
+      const Head& S = heads[hs];
+      if (!S.kept || nsf_of(S) == 0) continue;
+      const CsfExpansion& eS = eng->expand(cfg(S));
+      if (eS.nsf != nsf_of(S)) throw Error(4, "spin-function count mismatch in zero-external block");
+      for (size_t r = 0; r < eS.dets.size(); ++r) {
+        const double* thS = eS.basis->coeff.data() + r * eS.nsf;
+        const Det d0 = eS.dets[r];
+        int occ[128], vir[128], no = 0, nv = 0;
+        for (int x = 0; x < 2 * ni; ++x) {
+          if ((d0 >> x) & 1) occ[no++] = x;
+          else vir[nv++] = x;
+        }
+        auto emit = [&](Det d, double val) {
+          if (val == 0.0) return;
+          std::vector<int8_t> o(ni);
+          for (int p = 0; p < ni; ++p) o[p] = (int8_t)(((d >> (2 * p)) & 1) + ((d >> (2 * p + 1)) & 1));
+          const Head* Tg = find(pt.kind, o);
+          if (!Tg || nsf_of(*Tg) == 0) return;
+          const CsfExpansion& eT = eng->expand(cfg(*Tg));
+          auto it = eT.index.find(d);
+          if (it == eT.index.end()) return;
+          const double* thT = eT.basis->coeff.data() + (size_t)it->second * eT.nsf;
+          auto& blk = blocks[{Tg->lex - 1, (i64)hs}];
+          if (blk.empty()) blk.assign((size_t)eT.nsf * eS.nsf, 0.0);
+          const double f = val * eT.sign * eS.sign;
+          for (int a = 0; a < eT.nsf; ++a) {
+            if (thT[a] == 0.0) continue;
+            for (int b = 0; b < eS.nsf; ++b) blk[(size_t)a * eS.nsf + b] += f * thT[a] * thS[b];
+          }
+        };
+        auto orb = [](int x) { return x >> 1; };
+        auto spn = [](int x) { return x & 1; };
+        {  // diagonal
+          double e = 0;
+          for (int a = 0; a < no; ++a) {
+            const int p = orb(occ[a]);
+            e += I.h1(p, p);
+            for (int b = 0; b < no; ++b) {
+              const int q = orb(occ[b]);
+              e += 0.5 * I.i4(p, p, q, q);
+              if (spn(occ[a]) == spn(occ[b])) e -= 0.5 * I.i4(p, q, q, p);
+            }
+          }
+          emit(d0, e);
+        }
+        for (int a = 0; a < no; ++a)  // singles xa -> xb
+          for (int b = 0; b < nv; ++b) {
+            const int xa = occ[a], xb = vir[b];
+            if (spn(xa) != spn(xb)) continue;
+            const int p = orb(xb), q = orb(xa);
+            double v = I.h1(p, q);
+            for (int c = 0; c < no; ++c) {
+              if (c == a) continue;
+              const int r = orb(occ[c]);
+              v += I.i4(p, q, r, r);
+              if (spn(occ[c]) == spn(xa)) v -= I.i4(p, r, r, q);
+            }
+            Det d = d0;
+            double ph = parity_below(d, xa) ? -1.0 : 1.0;
+            d &= ~(((Det)1) << xa);
+            if (parity_below(d, xb)) ph = -ph;
+            d |= ((Det)1) << xb;
+            emit(d, ph * v);
+          }
+        for (int a = 0; a < no; ++a)  // doubles (xa,xb) -> (xc,xd)
+          for (int b = a + 1; b < no; ++b)
+            for (int c = 0; c < nv; ++c)
+              for (int dd = c + 1; dd < nv; ++dd) {
+                const int xa = occ[a], xb = occ[b], xc = vir[c], xd = vir[dd];
+                if (spn(xa) + spn(xb) != spn(xc) + spn(xd)) continue;
+                double v = 0;
+                if (spn(xc) == spn(xa) && spn(xd) == spn(xb)) v += I.i4(orb(xc), orb(xa), orb(xd), orb(xb));
+                if (spn(xc) == spn(xb) && spn(xd) == spn(xa)) v -= I.i4(orb(xc), orb(xb), orb(xd), orb(xa));
+                if (v == 0.0) continue;
+                Det d = d0;  // a+_c a+_d a_b a_a
+                double ph = 1.0;
+                if (parity_below(d, xa)) ph = -ph;
+                d &= ~(((Det)1) << xa);
+                if (parity_below(d, xb)) ph = -ph;
+                d &= ~(((Det)1) << xb);
+                if (parity_below(d, xd)) ph = -ph;
+                d |= ((Det)1) << xd;
+                if (parity_below(d, xc)) ph = -ph;
+                d |= ((Det)1) << xc;
+                emit(d, ph * v);
+              }
+      }
+    }
+    std::map<i64, std::vector<std::pair<i64, const std::vector<double>*>>> bytgt;
+    for (auto& kv : blocks) bytgt[kv.first.first].push_back({kv.first.second, &kv.second});
+    for (auto& tv : bytgt) {
+      const Head& Tg = heads[tv.first];
+      const i64 nsfT = nsf_of(Tg);
+      for (i64 a = 0; a < nsfT; ++a) {
+        AxpyTarget tg{BUF_S, off_of(Tg) + a * len, len, (i64)st.as.size(), 0};
+        for (auto& sv : tv.second) {
+          const Head& S = heads[sv.first];
+          const i64 nsfS = nsf_of(S);
+          for (i64 b = 0; b < nsfS; ++b) {
+            const double v = (*sv.second)[(size_t)a * nsfS + b];
+            if (std::fabs(v) < kTiny) continue;
+            st.as.push_back(AxpySource{BUF_C, off_of(S) + b * len, v, -1, 0});
+            P.flops_total += 2.0 * len;
+          }
+        }
+        tg.src_end = (i64)st.as.size();
+        if (tg.src_end > tg.src_begin) st.at.push_back(tg);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One-electron-in-the-external-space operators X acting on one external
+// electron: R[T,kt] += a * X * D[S,ks].  Returns a (nD(T) x nD(S)).
+// op(x,z) creates external x and annihilates external z.
+template <class MakeOp>
+std::vector<double> alpha_dd(Builder& B, const Head& Tg, const Head& S, MakeOp make_op) {
+  const i64 nT = B.nD(Tg), nS = B.nD(S);
+  std::vector<double> a((size_t)nT * nS, 0.0);
+  const bool Tab = Tg.off >= 0, Sab = S.off >= 0, Taa = Tg.off_aa >= 0, Saa = S.off_aa >= 0;
+  if (Tab && Sab) {  // target (e0,e1) <- source (e2,e1): predicted p_s
+    auto m = B.M(B.cfgD(Tg, B.e0, B.e1), B.cfgD(S, B.e2, B.e1), make_op(B.e0, B.e2));
+    for (i64 kt = 0; kt < Tg.nsf; ++kt)
+      for (i64 ks = 0; ks < S.nsf; ++ks) a[kt * nS + ks] = m[kt * S.nsf + ks] * B.sgn(S, ks);
+  } else if (Tab && Saa) {  // target (e0,e2) <- source (e2,e2): predicted sqrt2
+    auto m = B.M(B.cfgD(Tg, B.e0, B.e2), B.cfgD(S, B.e2, B.e2), make_op(B.e0, B.e2));
+    for (i64 kt = 0; kt < Tg.nsf; ++kt)
+      for (i64 ks = 0; ks < S.nsf_aa; ++ks) a[kt * nS + ks] = m[kt * S.nsf_aa + ks] / kSqrt2;
+  } else if (Taa && Sab) {  // target (e0,e0) <- source (e2,e0): predicted sqrt2*p_s
+    auto m = B.M(B.cfgD(Tg, B.e0, B.e0), B.cfgD(S, B.e2, B.e0), make_op(B.e0, B.e2));
+    for (i64 kt = 0; kt < Tg.nsf_aa; ++kt)
+      for (i64 ks = 0; ks < S.nsf; ++ks) a[kt * nS + ks] = m[kt * S.nsf + ks] / (kSqrt2 * B.sgn(S, ks));
+  } else if (Taa && Saa) {  // target (e0,e0) <- source (e0,e0), x = z: predicted 2
+    auto m = B.M(B.cfgD(Tg, B.e0, B.e0), B.cfgD(S, B.e0, B.e0), make_op(B.e0, B.e0));
+    for (i64 kt = 0; kt < Tg.nsf_aa; ++kt)
+      for (i64 ks = 0; ks < S.nsf_aa; ++ks) a[kt * nS + ks] = m[kt * S.nsf_aa + ks] / 2.0;
+  }
+  return a;
+}
+
+void Builder::dd_x() {
+  Step& fcomb = step(P.init_steps, STEP_AXPY, "dd same-head operators");
+  struct Term {
+    i64 src_dk;
+    int xbuf;
+    i64 xoff;
+    double a;
+  };
+  std::vector<std::vector<Term>> terms(P.nD);
+  auto opJ = [](i64 i, i64 j) { return [=](int x, int z) { return Op{x, z, (int)i, (int)j}; }; };
+  auto opK = [](i64 i, i64 j) { return [=](int x, int z) { return Op{x, (int)j, (int)i, z}; }; };
+  auto opH = []() { return [](int x, int z) { return Op{x, z, -1, -1}; }; };
+  for (size_t hs = 0; hs < sp.paths[2].size(); ++hs) {
+    const Head& S = sp.paths[2][hs];
+    if (!S.kept || nD(S) == 0) continue;
+    const i64 nS = nD(S);
+    {  // same head: F = a_h h + sum_i a_J J_ii + a_K K_ii
+      std::vector<std::vector<std::pair<i64, double>>> comb((size_t)nS * nS);
+      auto add = [&](const std::vector<double>& a, i64 xoff) {
+        for (size_t t = 0; t < a.size(); ++t)
+          if (std::fabs(a[t]) > kTiny) comb[t].push_back({xoff, a[t]});
+      };
+      add(alpha_dd(*this, S, S, opH()), offH);
+      for (i64 i = 0; i < nint; ++i) {
+        if (S.occ[i] == 0) continue;
+        add(alpha_dd(*this, S, S, opJ(i, i)), Jof(i, i));
+        add(alpha_dd(*this, S, S, opK(i, i)), Kof(i, i));
+      }
+      for (i64 kt = 0; kt < nS; ++kt)
+        for (i64 ks = 0; ks < nS; ++ks) {
+          auto& c = comb[kt * nS + ks];
+          if (c.empty()) continue;
+          AxpyTarget tg{BUF_F, nF * n2, n2, (i64)fcomb.as.size(), 0};
+          for (auto& pr : c) fcomb.as.push_back(AxpySource{BUF_JK, pr.first, pr.second, -1, 0});
+          tg.src_end = (i64)fcomb.as.size();
+          fcomb.at.push_back(tg);
+          terms[dk(S, kt)].push_back(Term{dk(S, ks), BUF_F, nF * n2, 1.0});
+          ++nF;
+        }
+    }
+    for (i64 j = 0; j < nint; ++j) {  // other heads: internal j -> i
+      if (S.occ[j] == 0) continue;
+      for (i64 i = 0; i < nint; ++i) {
+        if (i == j || S.occ[i] == 2) continue;
+        std::vector<int8_t> o(S.occ.begin(), S.occ.end());
+        o[j] -= 1;
+        o[i] += 1;
+        const Head* Tg = find(2, o);
+        if (!Tg || nD(*Tg) == 0) continue;
+        auto aJ = alpha_dd(*this, *Tg, S, opJ(i, j));
+        auto aK = alpha_dd(*this, *Tg, S, opK(i, j));
+        const i64 nT = nD(*Tg);
+        for (i64 kt = 0; kt < nT; ++kt)
+          for (i64 ks = 0; ks < nS; ++ks) {
+            const double vj = aJ[kt * nS + ks], vk = aK[kt * nS + ks];
+            if (std::fabs(vj) > kTiny) terms[dk(*Tg, kt)].push_back(Term{dk(S, ks), BUF_JK, Jof(i, j), vj});
+            if (std::fabs(vk) > kTiny) terms[dk(*Tg, kt)].push_back(Term{dk(S, ks), BUF_JK, Kof(j, i), vk});
+          }
+      }
+    }
+  }
+  Step& st = step(P.sigma_steps, STEP_GEMM, "dd two-external");
+  for (i64 d = 0; d < P.nD; ++d) {
+    if (terms[d].empty()) continue;
+    GemmProblem gp{BUF_R, d * n2, n, n, n, 1.0, (i64)st.gs.size(), 0};
+    for (auto& t : terms[d]) st.gs.push_back(GemmSeg{t.xbuf, BUF_D, t.xoff, n, t.src_dk * n2, n, n, 0, 0, t.a});
+    gp.seg_end = (i64)st.gs.size();
+    st.gp.push_back(gp);
+    P.flops_total += 2.0 * n * n * n * (double)terms[d].size();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// DS: three-external (iq|bs) and one-external (iq|jk), h_iq.
+void Builder::ds() {
+  // ---- three-external: sigma_mu[b] += a * sum_{q,s} (iq|bs) D[q][s]
+  struct T3 {
+    i64 mu_row;  // CI offset of row (mu, k')
+    i64 i, dkk;
+    double a;
+  };
+  std::vector<T3> t3;
+  // ---- one-external vectors: w(q) = sum a_op (iq|jk) (+ a h_iq), one per (mu k', dk)
+  struct T1 {
+    i64 mu_row, dkk;
+    std::vector<double> w;
+  };
+  std::map<std::pair<i64, i64>, size_t> t1_index;
+  std::vector<T1> t1;
+  auto w_of = [&](i64 mu_row, i64 dkk) -> std::vector<double>& {
+    auto key = std::make_pair(mu_row, dkk);
+    auto it = t1_index.find(key);
+    if (it != t1_index.end()) return t1[it->second].w;
+    t1_index[key] = t1.size();
+    t1.push_back(T1{mu_row, dkk, std::vector<double>(n, 0.0)});
+    return t1.back().w;
+  };
+  for (size_t hs = 0; hs < sp.paths[2].size(); ++hs) {
+    const Head& S = sp.paths[2][hs];
+    if (!S.kept || nD(S) == 0) continue;
+    const i64 nS = nD(S);
+    const bool Sab = S.off >= 0;
+    // three-external: mu = S + e_i
+    for (i64 i = 0; i < nint; ++i) {
+      if (S.occ[i] == 2) continue;
+      std::vector<int8_t> o(S.occ.begin(), S.occ.end());
+      o[i] += 1;
+      const Head* Mu = find(1, o);
+      if (!Mu || Mu->nsf == 0) continue;
+      std::vector<double> a((size_t)Mu->nsf * nS, 0.0);
+      if (Sab) {  // source (e1,e0), target (e2), op e_{i e0, e2 e1}: predicted 1
+        auto m = M(cfgS(*Mu, e2), cfgD(S, e1, e0), Op{(int)i, e0, e2, e1});
+        for (i64 kt = 0; kt < Mu->nsf; ++kt)
+          for (i64 ks = 0; ks < S.nsf; ++ks) a[kt * nS + ks] = m[kt * S.nsf + ks];
+      } else {  // source (e0,e0), target (e2), op e_{i e0, e2 e0}: predicted sqrt2
+        auto m = M(cfgS(*Mu, e2), cfgD(S, e0, e0), Op{(int)i, e0, e2, e0});
+        for (i64 kt = 0; kt < Mu->nsf; ++kt)
+          for (i64 ks = 0; ks < S.nsf_aa; ++ks) a[kt * nS + ks] = m[kt * S.nsf_aa + ks] / kSqrt2;
+      }
+      for (i64 kt = 0; kt < Mu->nsf; ++kt)
+        for (i64 ks = 0; ks < nS; ++ks)
+          if (std::fabs(a[kt * nS + ks]) > kTiny) t3.push_back(T3{Mu->off + kt * n, i, dk(S, ks), a[kt * nS + ks]});
+    }
+    // one-external: ops e_{iq,jk} (a+_i a+_j a_k a_q) and E_iq
+    auto add_op = [&](const Head* Mu, int i, int j, int k, bool one_el) {
+      const i64 nT = Mu->nsf;
+      std::vector<double> a((size_t)nT * nS, 0.0);
+      if (Sab) {  // source (e1,e0) -> target (e0), annihilate q = e1: predicted p_s
+        Op o = one_el ? Op{i, e1, -1, -1} : Op{i, e1, j, k};
+        auto m = M(cfgS(*Mu, e0), cfgD(S, e1, e0), o);
+        for (i64 kt = 0; kt < nT; ++kt)
+          for (i64 ks = 0; ks < S.nsf; ++ks) a[kt * nS + ks] = m[kt * S.nsf + ks] * sgn(S, ks);
+      } else {  // source (e0,e0) -> target (e0): predicted sqrt2
+        Op o = one_el ? Op{i, e0, -1, -1} : Op{i, e0, j, k};
+        auto m = M(cfgS(*Mu, e0), cfgD(S, e0, e0), o);
+        for (i64 kt = 0; kt < nT; ++kt)
+          for (i64 ks = 0; ks < S.nsf_aa; ++ks) a[kt * nS + ks] = m[kt * S.nsf_aa + ks] / kSqrt2;
+      }
+      for (i64 kt = 0; kt < nT; ++kt)
+        for (i64 ks = 0; ks < nS; ++ks) {
+          const double v = a[kt * nS + ks];
+          if (std::fabs(v) <= kTiny) continue;
+          auto& w = w_of(Mu->off + kt * n, dk(S, ks));
+          if (one_el) {
+            for (i64 q = 0; q < n; ++q) w[q] += v * I.h1(i, nint + q);
+          } else {
+            const double* iq = I.i3(i, j, k);
+            for (i64 q = 0; q < n; ++q) w[q] += v * iq[q];
+          }
+        }
+    };
+    for (i64 i = 0; i < nint; ++i) {  // E_iq
+      if (S.occ[i] == 2) continue;
+      std::vector<int8_t> o(S.occ.begin(), S.occ.end());
+      o[i] += 1;
+      const Head* Mu = find(1, o);
+      if (Mu && Mu->nsf > 0) add_op(Mu, (int)i, -1, -1, true);
+    }
+    for (i64 k = 0; k < nint; ++k) {
+      if (S.occ[k] == 0) continue;
+      for (i64 j = 0; j < nint; ++j) {
+        std::vector<int8_t> o1(S.occ.begin(), S.occ.end());
+        o1[k] -= 1;
+        if (o1[j] == 2) continue;
+        o1[j] += 1;
+        for (i64 i = 0; i < nint; ++i) {
+          if (o1[i] == 2) continue;
+          std::vector<int8_t> o2 = o1;
+          o2[i] += 1;
+          const Head* Mu = find(1, o2);
+          if (Mu && Mu->nsf > 0) add_op(Mu, (int)i, (int)j, (int)k, false);
+        }
+      }
+    }
+  }
+
+  // ---- device steps for the three-external term
+  if (!t3.empty()) {
+    const i64 Y = T.alloc(nint * P.nD * n);  // Y[i][dk][b] = sum_{q,s} D[dk][q][s] V_i[q][b][s]
+    Step& g = step(P.sigma_steps, STEP_GEMM, "three-external forward");
+    std::vector<char> used(nint, 0);
+    for (auto& t : t3) used[t.i] = 1;
+    for (i64 i = 0; i < nint; ++i) {
+      if (!used[i]) continue;
+      GemmProblem gp{BUF_T0, Y + i * P.nD * n, n, P.nD, n, 0.0, (i64)g.gs.size(), 0};
+      for (i64 q = 0; q < n; ++q)  // D[:, q, :] (nD x n, ld n^2) * V_i[q]^T (n x n)
+        g.gs.push_back(GemmSeg{BUF_D, BUF_V, q * n, n2, (i * n + q) * n2, n, n, 0, 1, 1.0});
+      gp.seg_end = (i64)g.gs.size();
+      g.gp.push_back(gp);
+      P.flops_total += 2.0 * P.nD * n * n2;
+    }
+    Step& sc = step(P.sigma_steps, STEP_AXPY, "three-external scatter");
+    std::map<i64, std::vector<const T3*>> by_mu;
+    for (auto& t : t3) by_mu[t.mu_row].push_back(&t);
+    for (auto& kv : by_mu) {
+      AxpyTarget tg{BUF_S, kv.first, n, (i64)sc.as.size(), 0};
+      for (auto* t : kv.second) sc.as.push_back(AxpySource{BUF_T0, Y + (t->i * P.nD + t->dkk) * n, t->a, -1, 0});
+      tg.src_end = (i64)sc.as.size();
+      sc.at.push_back(tg);
+    }
+    // reverse: U[i][dk] = sum a c_mu ; R[dk][q][:] += sum_i U[i][dk] V_i[q]
+    const i64 U = T.alloc(nint * P.nD * n);
+    zero_step(P.sigma_steps, BUF_T0, U, nint * P.nD * n, "three-external reverse zero");
+    Step& ga = step(P.sigma_steps, STEP_AXPY, "three-external reverse gather");
+    std::map<std::pair<i64, i64>, std::vector<const T3*>> by_idk;
+    for (auto& t : t3) by_idk[{t.i, t.dkk}].push_back(&t);
+    for (auto& kv : by_idk) {
+      AxpyTarget tg{BUF_T0, U + (kv.first.first * P.nD + kv.first.second) * n, n, (i64)ga.as.size(), 0};
+      for (auto* t : kv.second) ga.as.push_back(AxpySource{BUF_C, t->mu_row, t->a, -1, 0});
+      tg.src_end = (i64)ga.as.size();
+      ga.at.push_back(tg);
+    }
+    Step& gr = step(P.sigma_steps, STEP_GEMM, "three-external reverse");
+    for (i64 q = 0; q < n; ++q) {
+      GemmProblem gp{BUF_R, q * n, n2, P.nD, n, 1.0, (i64)gr.gs.size(), 0};
+      for (i64 i = 0; i < nint; ++i)
+        if (used[i]) gr.gs.push_back(GemmSeg{BUF_T0, BUF_V, U + i * P.nD * n, n, (i * n + q) * n2, n, n, 0, 0, 1.0});
+      gp.seg_end = (i64)gr.gs.size();
+      if (gp.seg_end > gp.seg_begin) gr.gp.push_back(gp);
+    }
+    for (i64 i = 0; i < nint; ++i)
+      if (used[i]) P.flops_total += 2.0 * P.nD * n * n2;
+  }
+
+  // ---- device steps for the one-external term (vectors ordered by dk)
+  if (!t1.empty()) {
+    std::vector<size_t> order(t1.size());
+    for (size_t t = 0; t < t1.size(); ++t) order[t] = t;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return t1[x].dkk < t1[y].dkk; });
+    const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
+    for (size_t r = 0; r < order.size(); ++r) P.wv.insert(P.wv.end(), t1[order[r]].w.begin(), t1[order[r]].w.end());
+    const i64 m = (i64)order.size();
+    const i64 Z = T.alloc(m * n), Cg = T.alloc(m * n);
+    Step& g = step(P.sigma_steps, STEP_GEMM, "one-external forward");
+    Step& ga = step(P.sigma_steps, STEP_AXPY, "one-external reverse gather");
+    Step& gr = step(P.sigma_steps, STEP_GEMM, "one-external reverse");
+    Step& sc = step(P.sigma_steps, STEP_AXPY, "one-external scatter");
+    size_t r = 0;
+    while (r < order.size()) {
+      size_t e = r;
+      const i64 d = t1[order[r]].dkk;
+      while (e < order.size() && t1[order[e]].dkk == d) ++e;
+      const i64 cnt = (i64)(e - r);
+      // Z[r:e] = W[r:e] (cnt x n) * D[d] (n x n)
+      GemmProblem gp{BUF_T0, Z + (i64)r * n, n, cnt, n, 0.0, (i64)g.gs.size(), 0};
+      g.gs.push_back(GemmSeg{BUF_WV, BUF_D, (wbase + (i64)r) * n, n, d * n2, n, n, 0, 0, 1.0});
+      gp.seg_end = (i64)g.gs.size();
+      g.gp.push_back(gp);
+      // R[d] += W[r:e]^T (n x cnt) * Cg[r:e] (cnt x n)
+      GemmProblem gq{BUF_R, d * n2, n, n, n, 1.0, (i64)gr.gs.size(), 0};
+      gr.gs.push_back(GemmSeg{BUF_WV, BUF_T0, (wbase + (i64)r) * n, n, Cg + (i64)r * n, n, cnt, 1, 0, 1.0});
+      gq.seg_end = (i64)gr.gs.size();
+      gr.gp.push_back(gq);
+      P.flops_total += 4.0 * cnt * n * n;
+      r = e;
+    }
+    for (size_t t = 0; t < order.size(); ++t) {
+      AxpyTarget tg{BUF_T0, Cg + (i64)t * n, n, (i64)ga.as.size(), 0};
+      ga.as.push_back(AxpySource{BUF_C, t1[order[t]].mu_row, 1.0, -1, 0});
+      tg.src_end = (i64)ga.as.size();
+      ga.at.push_back(tg);
+    }
+    std::map<i64, std::vector<i64>> by_mu;
+    for (size_t t = 0; t < order.size(); ++t) by_mu[t1[order[t]].mu_row].push_back((i64)t);
+    for (auto& kv : by_mu) {
+      AxpyTarget tg{BUF_S, kv.first, n, (i64)sc.as.size(), 0};
+      for (i64 t : kv.second) sc.as.push_back(AxpySource{BUF_T0, Z + t * n, 1.0, -1, 0});
+      tg.src_end = (i64)sc.as.size();
+      sc.at.push_back(tg);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// DV: sigma_v += a <K^{ij}, D>; R += a c_v K^{ij}.  ops e_{iq,js}, i <= j.
+void Builder::dv() {
+  struct TV {
+    i64 v_csf, pq, dkk;
+    double a;
+  };
+  std::vector<TV> tv;
+  for (size_t hs = 0; hs < sp.paths[2].size(); ++hs) {
+    const Head& S = sp.paths[2][hs];
+    if (!S.kept || nD(S) == 0) continue;
+    const i64 nS = nD(S);
+    for (i64 i = 0; i < nint; ++i)
+      for (i64 j = i; j < nint; ++j) {
+        std::vector<int8_t> o(S.occ.begin(), S.occ.end());
+        o[i] += 1;
+        o[j] += 1;
+        if (o[i] > 2 || o[j] > 2) continue;
+        const Head* V = find(0, o);
+        if (!V || V->nsf == 0) continue;
+        std::vector<double> a((size_t)V->nsf * nS, 0.0);
+        if (S.off >= 0) {  // source (e1,e0): unit (i e0|j e1)
+          auto m = M(cfgV(*V), cfgD(S, e1, e0), Op{(int)i, e0, (int)j, e1});
+          const double div = (i == j) ? 2.0 : 1.0;
+          for (i64 kt = 0; kt < V->nsf; ++kt)
+            for (i64 ks = 0; ks < S.nsf; ++ks) a[kt * nS + ks] = m[kt * S.nsf + ks] / div;
+        } else {  // source (e0,e0)
+          auto m = M(cfgV(*V), cfgD(S, e0, e0), Op{(int)i, e0, (int)j, e0});
+          const double f = (i == j) ? 0.5 / kSqrt2 : 1.0 / kSqrt2;
+          for (i64 kt = 0; kt < V->nsf; ++kt)
+            for (i64 ks = 0; ks < S.nsf_aa; ++ks) a[kt * nS + ks] = m[kt * S.nsf_aa + ks] * f;
+        }
+        for (i64 kt = 0; kt < V->nsf; ++kt)
+          for (i64 ks = 0; ks < nS; ++ks)
+            if (std::fabs(a[kt * nS + ks]) > kTiny) tv.push_back(TV{V->off + kt, i * nint + j, dk(S, ks), a[kt * nS + ks]});
+      }
+  }
+  if (tv.empty()) return;
+  const i64 nk = nint * nint;
+  const i64 F2 = T.alloc(nk * P.nD), G2 = T.alloc(nk * P.nD);
+  Step& g = step(P.sigma_steps, STEP_GEMM, "dv forward");
+  {  // F2 (nk x nD) = Kbank (nk x n^2) * D^T
+    GemmProblem gp{BUF_T0, F2, P.nD, nk, P.nD, 0.0, (i64)g.gs.size(), 0};
+    g.gs.push_back(GemmSeg{BUF_JK, BUF_D, offK, n2, 0, n2, n2, 0, 1, 1.0});
+    gp.seg_end = (i64)g.gs.size();
+    g.gp.push_back(gp);
+    P.flops_total += 2.0 * nk * P.nD * n2;
+  }
+  Step& sc = step(P.sigma_steps, STEP_AXPY, "dv scatter");
+  std::map<i64, std::vector<const TV*>> by_v;
+  for (auto& t : tv) by_v[t.v_csf].push_back(&t);
+  for (auto& kv : by_v) {
+    AxpyTarget tg{BUF_S, kv.first, 1, (i64)sc.as.size(), 0};
+    for (auto* t : kv.second) sc.as.push_back(AxpySource{BUF_T0, F2 + t->pq * P.nD + t->dkk, t->a, -1, 0});
+    tg.src_end = (i64)sc.as.size();
+    sc.at.push_back(tg);
+  }
+  zero_step(P.sigma_steps, BUF_T0, G2, nk * P.nD, "dv reverse zero");
+  Step& ga = step(P.sigma_steps, STEP_AXPY, "dv reverse gather");
+  std::map<std::pair<i64, i64>, std::vector<const TV*>> by_g;
+  for (auto& t : tv) by_g[{t.pq, t.dkk}].push_back(&t);
+  for (auto& kv : by_g) {
+    AxpyTarget tg{BUF_T0, G2 + kv.first.first * P.nD + kv.first.second, 1, (i64)ga.as.size(), 0};
+    for (auto* t : kv.second) ga.as.push_back(AxpySource{BUF_C, t->v_csf, t->a, -1, 0});
+    tg.src_end = (i64)ga.as.size();
+    ga.at.push_back(tg);
+  }
+  Step& gr = step(P.sigma_steps, STEP_GEMM, "dv reverse");
+  {  // R (nD x n^2) += G2^T (nD x nk) * Kbank (nk x n^2)
+    GemmProblem gp{BUF_R, 0, n2, P.nD, n2, 1.0, (i64)gr.gs.size(), 0};
+    gr.gs.push_back(GemmSeg{BUF_T0, BUF_JK, G2, P.nD, offK, n2, nk, 1, 0, 1.0});
+    gp.seg_end = (i64)gr.gs.size();
+    gr.gp.push_back(gp);
+    P.flops_total += 2.0 * nk * P.nD * n2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SS: sigma_mu'[k'] += a X c_mu[k] with X in {J_ij, K_ji, combined same-head}.
+void Builder::ss() {
+  Step& fcomb = step(P.init_steps, STEP_AXPY, "ss same-head operators");
+  struct TS {
+    i64 tgt_row, src_row;
+    int xbuf;
+    i64 xoff;
+    double a;
+  };
+  std::vector<TS> ts;
+  for (size_t hs = 0; hs < sp.paths[1].size(); ++hs) {
+    const Head& S = sp.paths[1][hs];
+    if (!has(S)) continue;
+    const i64 nS = S.nsf;
+    auto al = [&](const Head& Tg, Op o) {
+      return M(cfgS(Tg, e0), cfgS(S, e1), o);  // predicted 1
+    };
+    {  // same head
+      std::vector<std::vector<std::pair<i64, double>>> comb((size_t)nS * nS);
+      auto add = [&](const std::vector<double>& a, i64 xoff) {
+        for (size_t t = 0; t < a.size(); ++t)
+          if (std::fabs(a[t]) > kTiny) comb[t].push_back({xoff, a[t]});
+      };
+      add(al(S, Op{e0, e1, -1, -1}), offH);
+      for (i64 i = 0; i < nint; ++i) {
+        if (S.occ[i] == 0) continue;
+        add(al(S, Op{e0, e1, (int)i, (int)i}), Jof(i, i));
+        add(al(S, Op{e0, (int)i, (int)i, e1}), Kof(i, i));
+      }
+      for (i64 kt = 0; kt < nS; ++kt)
+        for (i64 ks = 0; ks < nS; ++ks) {
+          auto& c = comb[kt * nS + ks];
+          if (c.empty()) continue;
+          AxpyTarget tg{BUF_F, nF * n2, n2, (i64)fcomb.as.size(), 0};
+          for (auto& pr : c) fcomb.as.push_back(AxpySource{BUF_JK, pr.first, pr.second, -1, 0});
+          tg.src_end = (i64)fcomb.as.size();
+          fcomb.at.push_back(tg);
+          ts.push_back(TS{S.off + kt * n, S.off + ks * n, BUF_F, nF * n2, 1.0});
+          ++nF;
+        }
+    }
+    for (i64 j = 0; j < nint; ++j) {
+      if (S.occ[j] == 0) continue;
+      for (i64 i = 0; i < nint; ++i) {
+        if (i == j || S.occ[i] == 2) continue;
+        std::vector<int8_t> o(S.occ.begin(), S.occ.end());
+        o[j] -= 1;
+        o[i] += 1;
+        const Head* Tg = find(1, o);
+        if (!Tg || !has(*Tg)) continue;
+        auto aJ = al(*Tg, Op{e0, e1, (int)i, (int)j});
+        auto aK = al(*Tg, Op{e0, (int)j, (int)i, e1});
+        for (i64 kt = 0; kt < Tg->nsf; ++kt)
+          for (i64 ks = 0; ks < nS; ++ks) {
+            const double vj = aJ[kt * nS + ks], vk = aK[kt * nS + ks];
+            if (std::fabs(vj) > kTiny) ts.push_back(TS{Tg->off + kt * n, S.off + ks * n, BUF_JK, Jof(i, j), vj});
+            if (std::fabs(vk) > kTiny) ts.push_back(TS{Tg->off + kt * n, S.off + ks * n, BUF_JK, Kof(j, i), vk});
+          }
+      }
+    }
+  }
+  if (ts.empty()) return;
+  // group by operator: Y[rows] = Cg[rows] * X^T
+  std::vector<size_t> order(ts.size());
+  for (size_t t = 0; t < ts.size(); ++t) order[t] = t;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+    return std::make_pair(ts[x].xbuf, ts[x].xoff) < std::make_pair(ts[y].xbuf, ts[y].xoff);
+  });
+  const i64 m = (i64)ts.size();
+  const i64 Cg = T.alloc(m * n), Yr = T.alloc(m * n);
+  Step& ga = step(P.sigma_steps, STEP_AXPY, "ss gather");
+  Step& g = step(P.sigma_steps, STEP_GEMM, "ss two-external");
+  Step& sc = step(P.sigma_steps, STEP_AXPY, "ss scatter");
+  for (i64 r = 0; r < m; ++r) {
+    AxpyTarget tg{BUF_T0, Cg + r * n, n, (i64)ga.as.size(), 0};
+    ga.as.push_back(AxpySource{BUF_C, ts[order[r]].src_row, 1.0, -1, 0});
+    tg.src_end = (i64)ga.as.size();
+    ga.at.push_back(tg);
+  }
+  i64 r = 0;
+  while (r < m) {
+    i64 e = r;
+    const auto key = std::make_pair(ts[order[r]].xbuf, ts[order[r]].xoff);
+    while (e < m && std::make_pair(ts[order[e]].xbuf, ts[order[e]].xoff) == key) ++e;
+    GemmProblem gp{BUF_T0, Yr + r * n, n, e - r, n, 0.0, (i64)g.gs.size(), 0};
+    g.gs.push_back(GemmSeg{BUF_T0, key.first, Cg + r * n, n, key.second, n, n, 0, 1, 1.0});
+    gp.seg_end = (i64)g.gs.size();
+    g.gp.push_back(gp);
+    P.flops_total += 2.0 * (e - r) * n * n;
+    r = e;
+  }
+  std::map<i64, std::vector<i64>> by_t;
+  for (i64 q = 0; q < m; ++q) by_t[ts[order[q]].tgt_row].push_back(q);
+  for (auto& kv : by_t) {
+    AxpyTarget tg{BUF_S, kv.first, n, (i64)sc.as.size(), 0};
+    for (i64 q : kv.second) sc.as.push_back(AxpySource{BUF_T0, Yr + q * n, ts[order[q]].a, -1, 0});
+    tg.src_end = (i64)sc.as.size();
+    sc.at.push_back(tg);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SV: sigma_mu[k'] += c_v[k] w ; sigma_v[k] += <w, c_mu[k']>.
+// ops e_{xi,jk} = a+_x a+_j a_k a_i with (xi|jk), and E_xi with h_xi.
+void Builder::sv() {
+  std::map<std::pair<i64, i64>, std::vector<double>> wmap;  // (mu row, v csf) -> w
+  for (size_t hv = 0; hv < sp.paths[0].size(); ++hv) {
+    const Head& V = sp.paths[0][hv];
+    if (!has(V)) continue;
+    auto add = [&](const Head* Mu, Op o, const double* vec, double hval_scale, i64 hi) {
+      auto m = M(cfgS(*Mu, e0), cfgV(V), o);  // predicted 1
+      for (i64 kt = 0; kt < Mu->nsf; ++kt)
+        for (i64 ks = 0; ks < V.nsf; ++ks) {
+          const double a = m[kt * V.nsf + ks];
+          if (std::fabs(a) <= kTiny) continue;
+          auto& w = wmap[{Mu->off + kt * n, V.off + ks}];
+          if (w.empty()) w.assign(n, 0.0);
+          if (vec) {
+            for (i64 x = 0; x < n; ++x) w[x] += a * vec[x];
+          } else {
+            for (i64 x = 0; x < n; ++x) w[x] += a * hval_scale * I.h1(nint + x, hi);
+          }
+        }
+    };
+    for (i64 i = 0; i < nint; ++i) {
+      if (V.occ[i] == 0) continue;
+      std::vector<int8_t> o1(V.occ.begin(), V.occ.end());
+      o1[i] -= 1;
+      if (const Head* Mu = find(1, o1); Mu && has(*Mu)) add(Mu, Op{e0, (int)i, -1, -1}, nullptr, 1.0, i);
+      for (i64 k = 0; k < nint; ++k) {
+        if (o1[k] == 0) continue;
+        std::vector<int8_t> o2 = o1;
+        o2[k] -= 1;
+        for (i64 j = 0; j < nint; ++j) {
+          if (o2[j] == 2) continue;
+          std::vector<int8_t> o3 = o2;
+          o3[j] += 1;
+          const Head* Mu = find(1, o3);
+          if (!Mu || !has(*Mu)) continue;
+          // (xi|jk) = (ix|jk) = I3[i][j][k][x]
+          add(Mu, Op{e0, (int)i, (int)j, (int)k}, I.i3(i, j, k), 0.0, 0);
+        }
+      }
+    }
+  }
+  if (wmap.empty()) return;
+  const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
+  std::vector<std::pair<std::pair<i64, i64>, i64>> rows;
+  for (auto& kv : wmap) {
+    rows.push_back({kv.first, wbase + (i64)rows.size()});
+    P.wv.insert(P.wv.end(), kv.second.begin(), kv.second.end());
+  }
+  Step& fw = step(P.sigma_steps, STEP_AXPY, "sv forward");
+  std::map<i64, std::vector<size_t>> by_mu;
+  for (size_t t = 0; t < rows.size(); ++t) by_mu[rows[t].first.first].push_back(t);
+  for (auto& kv : by_mu) {
+    AxpyTarget tg{BUF_S, kv.first, n, (i64)fw.as.size(), 0};
+    for (size_t t : kv.second) fw.as.push_back(AxpySource{BUF_WV, rows[t].second * n, 1.0, BUF_C, rows[t].first.second});
+    tg.src_end = (i64)fw.as.size();
+    fw.at.push_back(tg);
+  }
+  Step& rv = step(P.sigma_steps, STEP_DOT, "sv reverse");
+  std::map<i64, std::vector<size_t>> by_v;
+  for (size_t t = 0; t < rows.size(); ++t) by_v[rows[t].first.second].push_back(t);
+  for (auto& kv : by_v) {
+    DotTarget tg{BUF_S, kv.first, (i64)rv.ds.size(), 0};
+    for (size_t t : kv.second) rv.ds.push_back(DotSource{BUF_WV, BUF_C, rows[t].second * n, rows[t].first.first, n, 1.0});
+    tg.src_end = (i64)rv.ds.size();
+    rv.dt.push_back(tg);
+  }
+  P.flops_total += 4.0 * n * rows.size();
+}
+
+// ---------------------------------------------------------------------------
+// All-external term in packed integral form:
+//   singlet: [s_aa; s_ab] += W+ [c_aa; c_ab]    triplet: s_ab += W- c_ab
+// W+ rows/cols: n diagonal pairs then the n(n-1)/2 pairs a>b in the
+// reference's order idx = a(a-1)/2 + b (scepmaker_mod.f90:60-90).
+void Builder::allext() {
+  const i64 np = n + nab, nm = nab;
+  P.np = np;
+  P.nm = nm;
+  std::vector<std::pair<const DHeadInfo*, i64>> sing, trip;
+  for (auto& d : P.dheads)
+    for (i64 k = 0; k < d.nD; ++k) (k < d.nsing ? sing : trip).push_back({&d, k});
+  P.n_sing = (i64)sing.size();
+  P.n_trip = (i64)trip.size();
+  const i64 Us = T.alloc(std::max<i64>(1, P.n_sing) * np), Ys = T.alloc(std::max<i64>(1, P.n_sing) * np);
+  const i64 Ut = T.alloc(std::max<i64>(1, P.n_trip) * nm), Yt = T.alloc(std::max<i64>(1, P.n_trip) * nm);
+  zero_step(P.sigma_steps, BUF_T0, Us, P.n_sing * np, "all-external gather zero");
+  zero_step(P.sigma_steps, BUF_T0, Ut, P.n_trip * nm, "all-external gather zero");
+  Step& ga = step(P.sigma_steps, STEP_AXPY, "all-external gather");
+  auto gather = [&](i64 dst, i64 len, i64 src) {
+    AxpyTarget tg{BUF_T0, dst, len, (i64)ga.as.size(), 0};
+    ga.as.push_back(AxpySource{BUF_C, src, 1.0, -1, 0});
+    tg.src_end = (i64)ga.as.size();
+    ga.at.push_back(tg);
+  };
+  for (i64 r = 0; r < P.n_sing; ++r) {
+    const DHeadInfo& d = *sing[r].first;
+    const i64 k = sing[r].second;
+    if (k < d.nsf_aa) gather(Us + r * np, n, d.off_aa + k * n);
+    if (k < d.nsf_ab && nab > 0) gather(Us + r * np + n, nab, d.off_ab + k * nab);
+  }
+  for (i64 r = 0; r < P.n_trip; ++r) {
+    const DHeadInfo& d = *trip[r].first;
+    const i64 k = trip[r].second;
+    if (nab > 0) gather(Ut + r * nm, nab, d.off_ab + k * nab);
+  }
+  Step& g = step(P.sigma_steps, STEP_GEMM, "all-external");
+  const i64 offWm = np * np;
+  if (P.n_sing > 0) {
+    GemmProblem gp{BUF_T0, Ys, np, P.n_sing, np, 0.0, (i64)g.gs.size(), 0};
+    g.gs.push_back(GemmSeg{BUF_T0, BUF_W, Us, np, 0, np, np, 0, 0, 1.0});
+    gp.seg_end = (i64)g.gs.size();
+    g.gp.push_back(gp);
+  }
+  if (P.n_trip > 0 && nm > 0) {
+    GemmProblem gp{BUF_T0, Yt, nm, P.n_trip, nm, 0.0, (i64)g.gs.size(), 0};
+    g.gs.push_back(GemmSeg{BUF_T0, BUF_W, Ut, nm, offWm, nm, nm, 0, 0, 1.0});
+    gp.seg_end = (i64)g.gs.size();
+    g.gp.push_back(gp);
+  }
+  P.flops_allext = 2.0 * (double)np * np * P.n_sing + 2.0 * (double)nm * nm * P.n_trip;
+  P.bytes_allext = 8.0 * ((double)np * np + (P.n_trip > 0 ? (double)nm * nm : 0.0)) +
+                   16.0 * ((double)P.n_sing * np + (double)P.n_trip * nm);
+  P.flops_total += P.flops_allext;
+  Step& sc = step(P.sigma_steps, STEP_AXPY, "all-external scatter");
+  auto scatter = [&](i64 dst, i64 len, i64 src) {
+    AxpyTarget tg{BUF_S, dst, len, (i64)sc.as.size(), 0};
+    sc.as.push_back(AxpySource{BUF_T0, src, 1.0, -1, 0});
+    tg.src_end = (i64)sc.as.size();
+    sc.at.push_back(tg);
+  };
+  for (i64 r = 0; r < P.n_sing; ++r) {
+    const DHeadInfo& d = *sing[r].first;
+    const i64 k = sing[r].second;
+    if (k < d.nsf_aa) scatter(d.off_aa + k * n, n, Ys + r * np);
+    if (k < d.nsf_ab && nab > 0) scatter(d.off_ab + k * nab, nab, Ys + r * np + n);
+  }
+  for (i64 r = 0; r < P.n_trip; ++r) {
+    const DHeadInfo& d = *trip[r].first;
+    if (nab > 0) scatter(d.off_ab + trip[r].second * nab, nab, Yt + r * nm);
+  }
+  P.buf_size[BUF_W] = np * np + nm * nm;
+  P.buf_size[BUF_X] = (n * (n + 1) / 2) * (n * (n + 1) / 2);
+}
+
+// ---------------------------------------------------------------------------
+void Builder::init_steps() {
+  // gather L rows into dense blocks
+  Step& ga = step(P.init_steps, STEP_AXPY, "gather cholesky rows");
+  auto g1 = [&](int dst, i64 doff, i64 len, i64 pair) {
+    AxpyTarget tg{dst, doff, len, (i64)ga.as.size(), 0};
+    ga.as.push_back(AxpySource{BUF_L, pair * N, 1.0, -1, 0});
+    tg.src_end = (i64)ga.as.size();
+    ga.at.push_back(tg);
+  };
+  for (i64 i = 0; i < nint; ++i)
+    for (i64 q = 0; q < n; ++q) g1(BUF_LE, (i * n + q) * N, N, Ints::pair(i, nint + q));
+  for (i64 a = 0; a < n; ++a)
+    for (i64 b = 0; b < n; ++b) g1(BUF_LV, (a * n + b) * N, N, Ints::pair(nint + a, nint + b));
+  for (i64 i = 0; i < nint; ++i)
+    for (i64 j = 0; j < nint; ++j) g1(BUF_LI, (i * nint + j) * N, N, Ints::pair(i, j));
+  // packed external pairs (a>=b): rows a(a+1)/2 + b, contiguous in L for each a
+  const i64 npk = n * (n + 1) / 2;
+  Scratch Ti;
+  const i64 Lpk_off = Ti.alloc(npk * N);
+  for (i64 a = 0; a < n; ++a) g1(BUF_T0, Lpk_off + (a * (a + 1) / 2) * N, (a + 1) * N, Ints::pair(nint + a, nint));
+  init_scratch = Ti.top;
+  Step& gb = step(P.init_steps, STEP_GEMM, "integral banks");
+  {  // J[(ij)][(ab)] = LI (nint^2 x N) * LV^T
+    GemmProblem gp{BUF_JK, offJ, n2, nint * nint, n2, 0.0, (i64)gb.gs.size(), 0};
+    gb.gs.push_back(GemmSeg{BUF_LI, BUF_LV, 0, N, 0, N, N, 0, 1, 1.0});
+    gp.seg_end = (i64)gb.gs.size();
+    gb.gp.push_back(gp);
+  }
+  for (i64 p = 0; p < nint; ++p)
+    for (i64 q = 0; q < nint; ++q) {  // K[p][q] = LE[p] * LE[q]^T
+      GemmProblem gp{BUF_JK, Kof(p, q), n, n, n, 0.0, (i64)gb.gs.size(), 0};
+      gb.gs.push_back(GemmSeg{BUF_LE, BUF_LE, p * n * N, N, q * n * N, N, N, 0, 1, 1.0});
+      gp.seg_end = (i64)gb.gs.size();
+      gb.gp.push_back(gp);
+    }
+  for (i64 i = 0; i < nint; ++i) {  // V_i[q][(b,s)] = LE[i] (n x N) * LV^T (N x n^2)
+    GemmProblem gp{BUF_V, i * n * n2, n2, n, n2, 0.0, (i64)gb.gs.size(), 0};
+    gb.gs.push_back(GemmSeg{BUF_LE, BUF_LV, i * n * N, N, 0, N, N, 0, 1, 1.0});
+    gp.seg_end = (i64)gb.gs.size();
+    gb.gp.push_back(gp);
+  }
+  {  // X = Lpk Lpk^T
+    GemmProblem gp{BUF_X, 0, npk, npk, npk, 0.0, (i64)gb.gs.size(), 0};
+    gb.gs.push_back(GemmSeg{BUF_T0, BUF_T0, Lpk_off, N, Lpk_off, N, N, 0, 1, 1.0});
+    gp.seg_end = (i64)gb.gs.size();
+    gb.gp.push_back(gp);
+  }
+  step(P.init_steps, STEP_WBUILD, "all-external operators");
+}
+
+void Builder::run() {
+  const Deck& d = sp.deck;
+  nint = sp.n_int;
+  n = sp.n_ext;
+  n2 = n * n;
+  nab = n * (n - 1) / 2;
+  N = op.nchol;
+  for (const auto& dm : sp.domains)
+    if ((i64)dm.size() != n) throw Error(3, "local pair domains are not supported by the dense-operator plan");
+  if (nint + 3 > 64) throw Error(3, "at most 61 internal orbitals are supported");
+  P.nint = nint;
+  P.n = n;
+  P.nchol = N;
+  P.total_csfs = sp.total_csfs;
+  P.npair_all = d.num_orbitals * (d.num_orbitals + 1) / 2;
+  P.buf_size.assign(NUM_BUFS, 0);
+  build_spin_tables((int)sp.open_shells, (int)d.spin_mult, tables);
+  eng = std::make_unique<CouplingEngine>(tables);
+  e0 = (int)nint;
+  e1 = (int)nint + 1;
+  e2 = (int)nint + 2;
+  I.norb = d.num_orbitals;
+  I.nint = nint;
+  I.n = n;
+  I.N = N;
+  I.h = op.h;
+  I.L = op.chol;
+  I.build();
+  offJ = 0;
+  offK = nint * nint * n2;
+  offH = 2 * nint * nint * n2;
+  setup_heads();
+  init_steps();
+  zero_step(P.sigma_steps, BUF_R, 0, P.nD * n2, "zero accumulators");
+  step(P.sigma_steps, STEP_UNPACK, "unpack");
+  allext();
+  dd_x();
+  ds();
+  dv();
+  ss();
+  sv();
+  internal_blocks();
+  step(P.sigma_steps, STEP_PACK, "pack");
+  P.h_vv.assign(n2, 0.0);
+  for (i64 a = 0; a < n; ++a)
+    for (i64 b = 0; b < n; ++b) P.h_vv[a * n + b] = I.h1(nint + a, nint + b);
+  P.buf_size[BUF_C] = sp.total_csfs;
+  P.buf_size[BUF_S] = sp.total_csfs;
+  P.buf_size[BUF_D] = std::max<i64>(1, P.nD * n2);
+  P.buf_size[BUF_R] = std::max<i64>(1, P.nD * n2);
+  P.buf_size[BUF_T0] = std::max<i64>(T.top, init_scratch);
+  P.buf_size[BUF_JK] = (2 * nint * nint + 1) * n2;
+  P.buf_size[BUF_V] = nint * n * n2;
+  P.buf_size[BUF_F] = std::max<i64>(1, nF * n2);
+  P.buf_size[BUF_WV] = std::max<i64>(1, (i64)P.wv.size());
+  P.buf_size[BUF_L] = P.npair_all * N;
+  P.buf_size[BUF_LE] = nint * n * N;
+  P.buf_size[BUF_LV] = n2 * N;
+  P.buf_size[BUF_LI] = nint * nint * N;
+}
+
+}  // namespace
+
+void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan) {
+  plan = Plan();
+  Builder b(sp, op, plan);
+  b.run();
+}
+
+}  // namespace tci

@@ -1,0 +1,129 @@
+// The sigma plan: the complete sigma = H c of the MRSDCI space written as a
+// short program over a handful of device buffers.  The host builds it once
+// (this replaces the reference's iteration-1 "dry run" that enumerates loop
+// records, e.g. three_and_four_seg_mod_1.f90:412-438, 695-776 and
+// three_and_four_seg_mod_2.f90:1095-1195) and the device replays it on every
+// sigma build.
+//
+// Step kinds:
+//   GEMM   C(M x N) = beta*C + sum_seg alpha_seg * op(A_seg) op(B_seg)   (row major)
+//   AXPY   dst[off:off+len] += sum_src coef * scale * src[soff:soff+len]
+//   DOT    dst[off] += sum_src coef * <a[aoff:aoff+len], b[boff:boff+len]>
+//   UNPACK CI vector -> dense external pair matrices of the N-2 heads (SCEP)
+//   PACK   dense accumulators -> sigma (unSCEP), tiger_fortran/scepmaker_mod.f90
+//   ZERO   buffer range
+// Every target range is written by exactly one table entry per launch and the
+// sources of an entry are summed in table order, so a sigma build is
+// deterministic (same result alone or interleaved with other requests).
+#pragma once
+#include "tci_host.h"
+
+namespace tci {
+
+enum BufId : int {
+  BUF_C = 0,   // input CI vector
+  BUF_S,       // output sigma vector (accumulated)
+  BUF_D,       // dense N-2 pair matrices, nD x n x n
+  BUF_R,       // dense N-2 accumulators, nD x n x n
+  BUF_T0,      // scratch
+  BUF_T1,
+  BUF_T2,
+  BUF_T3,
+  BUF_JK,      // (ij|ab) and (ia|jb) banks + h_ab: (2*nint^2 + 1) x n x n
+  BUF_V,       // three-external banks, nint x n x n^2: V_i[b][q][s] = (iq|bs)
+  BUF_W,       // all-external operators W+ (np x np) then W- (nm x nm)
+  BUF_F,       // same-head combined one-external-electron operators, n x n each
+  BUF_WV,      // precomputed vectors (one-external couplings), n each
+  BUF_L,       // Cholesky vectors as given, npair_all x nchol
+  BUF_LE,      // gathered L: internal-external rows, nint x n x nchol
+  BUF_LV,      // gathered L: external-external rows, n*n x nchol
+  BUF_LI,      // gathered L: internal-internal rows, nint*nint x nchol
+  BUF_X,       // packed external (ab|cd), np x np (init only)
+  NUM_BUFS
+};
+
+enum StepKind : int { STEP_GEMM = 0, STEP_AXPY, STEP_DOT, STEP_UNPACK, STEP_PACK, STEP_ZERO, STEP_WBUILD };
+
+struct GemmProblem {
+  int c;
+  i64 offC, ldc, M, N;
+  double beta;
+  i64 seg_begin, seg_end;
+};
+struct GemmSeg {
+  int a, b;
+  i64 offA, lda, offB, ldb, K;
+  int tA, tB;
+  double alpha;
+};
+struct AxpyTarget {
+  int dst;
+  i64 off, len;
+  i64 src_begin, src_end;
+};
+struct AxpySource {
+  int src;
+  i64 off;
+  double coef;
+  int sbuf;    // -1: no data-dependent scale
+  i64 sidx;
+};
+struct DotTarget {
+  int dst;
+  i64 off;
+  i64 src_begin, src_end;
+};
+struct DotSource {
+  int a, b;
+  i64 aoff, boff, len;
+  double coef;
+};
+
+struct Step {
+  int kind = 0;
+  std::string name;
+  std::vector<GemmProblem> gp;
+  std::vector<GemmSeg> gs;
+  std::vector<AxpyTarget> at;
+  std::vector<AxpySource> as;
+  std::vector<DotTarget> dt;
+  std::vector<DotSource> ds;
+  int buf = 0;          // ZERO
+  i64 off = 0, len = 0; // ZERO
+};
+
+// One N-2 head as seen by UNPACK/PACK.
+struct DHeadInfo {
+  i64 off_ab, off_aa;  // CI-vector offsets (-1 if absent)
+  i64 nsf_ab, nsf_aa;  // spin functions of each block
+  i64 nsing;           // singlet-coupled functions (first nsing of the ab block)
+  i64 nD;              // dense matrices of this head = max(nsf_ab, nsf_aa)
+  i64 dk0;             // first dense matrix index
+};
+
+struct Plan {
+  i64 nint = 0, n = 0, nchol = 0, total_csfs = 0, npair_all = 0;
+  i64 nD = 0;                    // dense N-2 matrices
+  std::vector<DHeadInfo> dheads;
+  std::vector<double> dk_sign;   // +1 singlet-coupled, -1 triplet-coupled per dense matrix
+  std::vector<i64> buf_size;     // doubles per buffer
+  std::vector<double> h_vv;      // external one-electron block (n x n), uploaded into BUF_JK tail
+  std::vector<double> wv;        // BUF_WV contents
+  std::vector<Step> init_steps;  // run once after upload of L
+  std::vector<Step> sigma_steps; // run per sigma build
+  // algorithmic work per sigma build, for roofline reporting
+  double flops_allext = 0, flops_total = 0, bytes_allext = 0;
+  i64 np = 0, nm = 0;            // packed pair dimensions of W+ / W-
+  i64 n_sing = 0, n_trip = 0;    // dense matrices per coupling type
+};
+
+struct Operator {
+  const double* h = nullptr;     // n_orb x n_orb, row major, symmetric
+  const double* chol = nullptr;  // [pair][J], pair = p(p+1)/2 + q, p >= q (0-based)
+  i64 nchol = 0;
+  double core_energy = 0.0;
+};
+
+void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan);
+
+}  // namespace tci

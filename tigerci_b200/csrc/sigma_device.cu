@@ -1,0 +1,593 @@
+// Device executor of the sigma plan (host/plan.h) and the device half of the C
+// ABI.  FP64 throughout.  Kernels:
+//   gemm_grouped_f64  C = beta*C + sum_seg alpha*op(A)op(B), one CTA per 64x64
+//                     tile of every problem, segments summed in table order
+//   axpy_segments     one warp per target range, sources summed in table order
+//   dot_segments      one warp per target scalar
+//   unpack_pairs / pack_pairs   SCEP <-> dense external pair matrices
+//                     (tiger_fortran/scepmaker_mod.f90:121-257, 633-800)
+//   build_allext      W+ / W- from the packed external (ab|cd) block
+// The plan is replayed in a fixed launch order on one stream, so every sigma
+// build is bitwise reproducible.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/tigerci_sigma.h"
+#include "host/capi_internal.h"
+#include "host/plan.h"
+
+using namespace tci;
+
+#define TCI_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t _e = (call);                                                                 \
+    if (_e != cudaSuccess)                                                                   \
+      throw Error(TCI_ERR_CUDA, std::string(#call) + " failed: " + cudaGetErrorString(_e)); \
+  } while (0)
+
+namespace {
+
+// ----------------------------------------------------------------------------
+// device-side table layouts (plain structs, 8-byte fields)
+struct DGemmProblem {
+  double* C;
+  long long ldc, M, N, tiles_n, tile_begin;
+  double beta;
+  long long seg_begin, seg_end;
+};
+struct DGemmSeg {
+  const double* A;
+  const double* B;
+  long long lda, ldb, K;
+  int tA, tB;
+  double alpha;
+};
+struct DAxpyTarget {
+  double* dst;
+  long long len, src_begin, src_end;
+};
+struct DAxpySource {
+  const double* src;
+  const double* scale;  // nullptr: 1
+  double coef;
+};
+struct DDotTarget {
+  double* dst;
+  long long src_begin, src_end;
+};
+struct DDotSource {
+  const double* a;
+  const double* b;
+  long long len;
+  double coef;
+};
+struct DHead {
+  long long off_ab, off_aa, nsf_ab, nsf_aa, nsing, nD, dk0;
+};
+
+constexpr int GT = 64;   // tile edge
+constexpr int GK = 16;   // k step
+constexpr int GTH = 256; // threads (16 x 16, 4 x 4 outputs each)
+
+__global__ void __launch_bounds__(GTH) gemm_grouped_f64(const DGemmProblem* __restrict__ probs, int nprob,
+                                                        const DGemmSeg* __restrict__ segs) {
+  __shared__ double As[GK][GT + 1];
+  __shared__ double Bs[GK][GT + 1];
+  // locate problem of this tile
+  const long long tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const DGemmProblem P = probs[lo];
+  const long long t = tile - P.tile_begin;
+  const long long m0 = (t / P.tiles_n) * GT, n0 = (t % P.tiles_n) * GT;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (long long s = P.seg_begin; s < P.seg_end; ++s) {
+    const DGemmSeg S = segs[s];
+    double acs[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acs[i][j] = 0.0;
+    for (long long k0 = 0; k0 < S.K; k0 += GK) {
+      // load A tile (GT rows x GK cols) into As[k][m]
+      for (int e = threadIdx.x; e < GT * GK; e += GTH) {
+        int mm, kk;
+        if (S.tA) { mm = e % GT; kk = e / GT; }   // A stored K x M: contiguous in m
+        else { kk = e % GK; mm = e / GK; }        // A stored M x K: contiguous in k
+        const long long gm = m0 + mm, gk = k0 + kk;
+        double v = 0.0;
+        if (gm < P.M && gk < S.K) v = S.tA ? S.A[gk * S.lda + gm] : S.A[gm * S.lda + gk];
+        As[kk][mm] = v;
+      }
+      for (int e = threadIdx.x; e < GT * GK; e += GTH) {
+        int nn, kk;
+        if (S.tB) { kk = e % GK; nn = e / GK; }   // B stored N x K
+        else { nn = e % GT; kk = e / GT; }        // B stored K x N
+        const long long gn = n0 + nn, gk = k0 + kk;
+        double v = 0.0;
+        if (gn < P.N && gk < S.K) v = S.tB ? S.B[gn * S.ldb + gk] : S.B[gk * S.ldb + gn];
+        Bs[kk][nn] = v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < GK; ++kk) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acs[i][j] = fma(a[i], b[j], acs[i][j]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = fma(S.alpha, acs[i][j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long gm = m0 + ty + 16 * i;
+    if (gm >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const long long gn = n0 + tx + 16 * j;
+      if (gn >= P.N) continue;
+      double* c = P.C + gm * P.ldc + gn;
+      *c = (P.beta == 0.0) ? acc[i][j] : fma(P.beta, *c, acc[i][j]);
+    }
+  }
+}
+
+__global__ void axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg, const DAxpySource* __restrict__ src) {
+  const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= ntg) return;
+  const DAxpyTarget T = tg[w];
+  for (long long i = lane; i < T.len; i += 32) {
+    double acc = 0.0;
+    for (long long s = T.src_begin; s < T.src_end; ++s) {
+      const DAxpySource S = src[s];
+      const double c = S.scale ? S.coef * (*S.scale) : S.coef;
+      acc = fma(c, S.src[i], acc);
+    }
+    T.dst[i] += acc;
+  }
+}
+
+__global__ void dot_segments(const DDotTarget* __restrict__ tg, long long ntg, const DDotSource* __restrict__ src) {
+  const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= ntg) return;
+  const DDotTarget T = tg[w];
+  double total = 0.0;
+  for (long long s = T.src_begin; s < T.src_end; ++s) {
+    const DDotSource S = src[s];
+    double acc = 0.0;
+    for (long long i = lane; i < S.len; i += 32) acc = fma(S.a[i], S.b[i], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    total = fma(S.coef, acc, total);
+  }
+  if (lane == 0) *T.dst += total;
+}
+
+// D[dk](j,i) = c_ab[k][i(i-1)/2+j], D(i,j) = p * same (i > j); D(a,a) = sqrt2 c_aa[k][a]
+__global__ void unpack_pairs(const DHead* __restrict__ heads, const int* __restrict__ dk_head, long long nD, long long n,
+                             const double* __restrict__ c, double* __restrict__ D) {
+  const long long dk = blockIdx.y;
+  if (dk >= nD) return;
+  const DHead H = heads[dk_head[dk]];
+  const long long k = dk - H.dk0;
+  const double p = (k < H.nsing) ? 1.0 : -1.0;
+  const long long nab = n * (n - 1) / 2;
+  double* Dk = D + dk * n * n;
+  const bool ab = k < H.nsf_ab, aa = k < H.nsf_aa;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / n, s = e % n;
+    double v = 0.0;
+    if (r == s) {
+      if (aa) v = 1.4142135623730951 * c[H.off_aa + k * n + r];
+    } else if (ab) {
+      const long long i = r > s ? r : s, j = r > s ? s : r;
+      const double x = c[H.off_ab + k * nab + i * (i - 1) / 2 + j];
+      v = (r < s) ? x : p * x;
+    }
+    Dk[e] = v;
+  }
+}
+
+// sigma_ab[k][i(i-1)/2+j] += R(j,i) + p R(i,j); sigma_aa[k][a] += sqrt2 R(a,a)
+__global__ void pack_pairs(const DHead* __restrict__ heads, const int* __restrict__ dk_head, long long nD, long long n,
+                           const double* __restrict__ R, double* __restrict__ sigma) {
+  const long long dk = blockIdx.y;
+  if (dk >= nD) return;
+  const DHead H = heads[dk_head[dk]];
+  const long long k = dk - H.dk0;
+  const double p = (k < H.nsing) ? 1.0 : -1.0;
+  const long long nab = n * (n - 1) / 2;
+  const double* Rk = R + dk * n * n;
+  if (k < H.nsf_ab) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nab; e += (long long)gridDim.x * blockDim.x) {
+      // invert e = i(i-1)/2 + j, i > j >= 0
+      long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
+      while (i * (i - 1) / 2 > e) --i;
+      while ((i + 1) * i / 2 <= e) ++i;
+      const long long j = e - i * (i - 1) / 2;
+      sigma[H.off_ab + k * nab + e] += Rk[j * n + i] + p * Rk[i * n + j];
+    }
+  }
+  if (k < H.nsf_aa) {
+    for (long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x; a < n; a += (long long)gridDim.x * blockDim.x)
+      sigma[H.off_aa + k * n + a] += 1.4142135623730951 * Rk[a * n + a];
+  }
+}
+
+__device__ __forceinline__ long long pk(long long a, long long b) {
+  return a >= b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a;
+}
+
+// W+ (np x np, rows [aa (n); ab a>b]) and W- (nm x nm) from X[(ab)][(cd)] = (ab|cd)
+__global__ void build_allext(const double* __restrict__ X, long long n, double* __restrict__ W) {
+  const long long nab = n * (n - 1) / 2, np = n + nab, nm = nab, npk = n * (n + 1) / 2;
+  const long long total = np * np + nm * nm;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    long long r, c;
+    bool plus;
+    if (e < np * np) { r = e / np; c = e % np; plus = true; }
+    else { r = (e - np * np) / nm; c = (e - np * np) % nm; plus = false; }
+    auto unpair = [&](long long x, long long& a, long long& b) {
+      long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)x)) * 0.5);
+      while (i * (i - 1) / 2 > x) --i;
+      while ((i + 1) * i / 2 <= x) ++i;
+      a = i;
+      b = x - i * (i - 1) / 2;
+    };
+    double v;
+    if (plus) {
+      const bool rd = r < n, cd = c < n;
+      long long a, cc, b, d;
+      if (rd) { a = r; cc = r; } else unpair(r - n, a, cc);
+      if (cd) { b = c; d = c; } else unpair(c - n, b, d);
+      if (rd && cd) v = X[pk(a, b) * npk + pk(a, b)];
+      else if (rd) v = 1.4142135623730951 * X[pk(a, b) * npk + pk(a, d)];
+      else if (cd) v = 1.4142135623730951 * X[pk(a, b) * npk + pk(cc, b)];
+      else v = X[pk(a, b) * npk + pk(cc, d)] + X[pk(a, d) * npk + pk(cc, b)];
+    } else {
+      long long a, cc, b, d;
+      unpair(r, a, cc);
+      unpair(c, b, d);
+      v = X[pk(a, b) * npk + pk(cc, d)] - X[pk(a, d) * npk + pk(cc, b)];
+    }
+    W[e] = v;
+  }
+}
+
+// ----------------------------------------------------------------------------
+struct DevStep {
+  int kind = 0;
+  std::string name;
+  // GEMM
+  DGemmProblem* probs = nullptr;
+  DGemmSeg* segs = nullptr;
+  int nprob = 0;
+  long long ntiles = 0;
+  // AXPY / DOT
+  DAxpyTarget* at = nullptr;
+  DAxpySource* as = nullptr;
+  DDotTarget* dt = nullptr;
+  DDotSource* ds = nullptr;
+  long long ntg = 0;
+  // ZERO
+  double* zptr = nullptr;
+  long long zlen = 0;
+};
+
+template <class T>
+T* upload(const std::vector<T>& v, std::vector<void*>& owned) {
+  if (v.empty()) return nullptr;
+  T* d = nullptr;
+  TCI_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+  owned.push_back(d);
+  TCI_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return d;
+}
+
+}  // namespace
+
+struct tci_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  CsfSpace sp;
+  Plan plan;
+  double* buf[NUM_BUFS] = {};
+  std::vector<void*> owned;  // table allocations
+  std::vector<DevStep> init, sigma;
+  DHead* dheads = nullptr;
+  int* dk_head = nullptr;
+  double* h_c = nullptr;  // device staging for host-buffer calls
+  double* h_s = nullptr;
+  double bytes_held = 0;
+  double init_seconds = 0;
+  double last_sigma_ms = 0;
+  long long sigma_count = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  ~tci_ctx() {
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (int b = 0; b < NUM_BUFS; ++b)
+      if (buf[b]) cudaFree(buf[b]);
+    for (void* p : owned) cudaFree(p);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  double* ptr(int b, i64 off) {
+    if (b < 0 || b >= NUM_BUFS || !buf[b]) throw Error(TCI_ERR_INTERNAL, "plan references an unallocated buffer");
+    if (off < 0 || off > plan.buf_size[b]) throw Error(TCI_ERR_INTERNAL, "plan offset outside its buffer");
+    return buf[b] + off;
+  }
+
+  DevStep lower(const Step& s) {
+    DevStep d;
+    d.kind = s.kind;
+    d.name = s.name;
+    if (s.kind == STEP_GEMM) {
+      std::vector<DGemmProblem> pr;
+      std::vector<DGemmSeg> sg;
+      long long tiles = 0;
+      for (auto& g : s.gp) {
+        const i64 tm = (g.M + GT - 1) / GT, tn = (g.N + GT - 1) / GT;
+        if (g.M <= 0 || g.N <= 0) continue;
+        check_range(g.c, g.offC, (g.M - 1) * g.ldc + g.N);
+        pr.push_back(DGemmProblem{ptr(g.c, g.offC), g.ldc, g.M, g.N, tn, tiles, g.beta, g.seg_begin, g.seg_end});
+        tiles += tm * tn;
+      }
+      for (auto& g : s.gs) {
+        // operand extents: A is M x K (or K x M), B is K x N (or N x K); checked loosely by offsets
+        sg.push_back(DGemmSeg{ptr(g.a, g.offA), ptr(g.b, g.offB), g.lda, g.ldb, g.K, g.tA, g.tB, g.alpha});
+      }
+      d.probs = upload(pr, owned);
+      d.segs = upload(sg, owned);
+      d.nprob = (int)pr.size();
+      d.ntiles = tiles;
+    } else if (s.kind == STEP_AXPY) {
+      std::vector<DAxpyTarget> t;
+      std::vector<DAxpySource> so;
+      for (auto& x : s.at) {
+        check_range(x.dst, x.off, x.len);
+        t.push_back(DAxpyTarget{ptr(x.dst, x.off), x.len, x.src_begin, x.src_end});
+      }
+      for (auto& x : s.as) {
+        // source length equals its target's length; the offset is checked against the buffer
+        so.push_back(DAxpySource{ptr(x.src, x.off), x.sbuf >= 0 ? ptr(x.sbuf, x.sidx) : nullptr, x.coef});
+      }
+      for (auto& x : s.at)
+        for (i64 q = x.src_begin; q < x.src_end; ++q) check_range(s.as[q].src, s.as[q].off, x.len);
+      d.at = upload(t, owned);
+      d.as = upload(so, owned);
+      d.ntg = (long long)t.size();
+    } else if (s.kind == STEP_DOT) {
+      std::vector<DDotTarget> t;
+      std::vector<DDotSource> so;
+      for (auto& x : s.dt) t.push_back(DDotTarget{ptr(x.dst, x.off), x.src_begin, x.src_end});
+      for (auto& x : s.ds) {
+        check_range(x.a, x.aoff, x.len);
+        check_range(x.b, x.boff, x.len);
+        so.push_back(DDotSource{ptr(x.a, x.aoff), ptr(x.b, x.boff), x.len, x.coef});
+      }
+      d.dt = upload(t, owned);
+      d.ds = upload(so, owned);
+      d.ntg = (long long)t.size();
+    } else if (s.kind == STEP_ZERO) {
+      check_range(s.buf, s.off, s.len);
+      d.zptr = ptr(s.buf, s.off);
+      d.zlen = s.len;
+    }
+    return d;
+  }
+
+  void check_range(int b, i64 off, i64 len) const {
+    if (b < 0 || b >= NUM_BUFS || off < 0 || len < 0 || off + len > plan.buf_size[b])
+      throw Error(TCI_ERR_INTERNAL, "plan range outside its buffer");
+  }
+
+  void run(const DevStep& s) {
+    switch (s.kind) {
+      case STEP_GEMM:
+        if (s.ntiles > 0) gemm_grouped_f64<<<(unsigned)s.ntiles, GTH, 0, stream>>>(s.probs, s.nprob, s.segs);
+        break;
+      case STEP_AXPY:
+        if (s.ntg > 0) axpy_segments<<<(unsigned)((s.ntg + 7) / 8), 256, 0, stream>>>(s.at, s.ntg, s.as);
+        break;
+      case STEP_DOT:
+        if (s.ntg > 0) dot_segments<<<(unsigned)((s.ntg + 7) / 8), 256, 0, stream>>>(s.dt, s.ntg, s.ds);
+        break;
+      case STEP_ZERO:
+        if (s.zlen > 0) TCI_CUDA(cudaMemsetAsync(s.zptr, 0, s.zlen * sizeof(double), stream));
+        break;
+      case STEP_UNPACK:
+        if (plan.nD > 0) {
+          dim3 g((unsigned)std::min<long long>(64, (plan.n * plan.n + 255) / 256), (unsigned)plan.nD);
+          unpack_pairs<<<g, 256, 0, stream>>>(dheads, dk_head, plan.nD, plan.n, buf[BUF_C], buf[BUF_D]);
+        }
+        break;
+      case STEP_PACK:
+        if (plan.nD > 0) {
+          dim3 g((unsigned)std::min<long long>(64, (plan.n * plan.n / 2 + 255) / 256 + 1), (unsigned)plan.nD);
+          pack_pairs<<<g, 256, 0, stream>>>(dheads, dk_head, plan.nD, plan.n, buf[BUF_R], buf[BUF_S]);
+        }
+        break;
+      case STEP_WBUILD:
+        build_allext<<<148 * 16, 256, 0, stream>>>(buf[BUF_X], plan.n, buf[BUF_W]);
+        break;
+    }
+    TCI_CUDA(cudaGetLastError());
+  }
+};
+
+extern "C" {
+
+int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out) {
+  if (!out) return TCI_ERR_ARG;
+  *out = nullptr;
+  try {
+    auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<tci_ctx> ctx(new tci_ctx());
+    int ndev = 0;
+    TCI_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) throw Error(TCI_ERR_CUDA, "requested device is not available");
+    ctx->device = (int)device;
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    TCI_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    TCI_CUDA(cudaEventCreate(&ctx->ev0));
+    TCI_CUDA(cudaEventCreate(&ctx->ev1));
+    build_space_from_c(deck, ctx->sp);
+    Operator o;
+    operator_from_c(op, ctx->sp, o);
+    build_plan(ctx->sp, o, ctx->plan);
+    Plan& P = ctx->plan;
+    for (int b = 0; b < NUM_BUFS; ++b) {
+      if (P.buf_size[b] <= 0) continue;
+      cudaError_t e = cudaMalloc(&ctx->buf[b], P.buf_size[b] * sizeof(double));
+      if (e != cudaSuccess) throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+      ctx->bytes_held += (double)P.buf_size[b] * sizeof(double);
+    }
+    TCI_CUDA(cudaMemcpy(ctx->buf[BUF_L], o.chol, P.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice));
+    TCI_CUDA(cudaMemcpy(ctx->buf[BUF_JK] + 2 * P.nint * P.nint * P.n * P.n, P.h_vv.data(), P.h_vv.size() * sizeof(double),
+                        cudaMemcpyHostToDevice));
+    if (!P.wv.empty())
+      TCI_CUDA(cudaMemcpy(ctx->buf[BUF_WV], P.wv.data(), P.wv.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<DHead> dh;
+    std::vector<int> dkh;
+    for (size_t h = 0; h < P.dheads.size(); ++h) {
+      const auto& d = P.dheads[h];
+      dh.push_back(DHead{d.off_ab, d.off_aa, d.nsf_ab, d.nsf_aa, d.nsing, d.nD, d.dk0});
+      for (i64 k = 0; k < d.nD; ++k) dkh.push_back((int)h);
+    }
+    ctx->dheads = upload(dh, ctx->owned);
+    ctx->dk_head = upload(dkh, ctx->owned);
+    for (auto& s : P.init_steps) ctx->init.push_back(ctx->lower(s));
+    for (auto& s : P.sigma_steps) ctx->sigma.push_back(ctx->lower(s));
+    for (auto& s : ctx->init) ctx->run(s);
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+    // init-only buffers
+    for (int b : {BUF_X, BUF_L, BUF_LE, BUF_LI}) {
+      if (ctx->buf[b]) {
+        TCI_CUDA(cudaFree(ctx->buf[b]));
+        ctx->bytes_held -= (double)P.buf_size[b] * sizeof(double);
+        ctx->buf[b] = nullptr;
+      }
+    }
+    ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = ctx.release();
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n, void* stream) {
+  if (!ctx || !d_c || !d_sigma) return TCI_ERR_ARG;
+  try {
+    if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t user = stream ? (cudaStream_t)stream : ctx->stream;
+    if (user != ctx->stream) {
+      TCI_CUDA(cudaEventRecord(ctx->ev0, user));
+      TCI_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev0, 0));
+    }
+    // the plan addresses BUF_C / BUF_S: copy in and accumulate out
+    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
+    TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (auto& s : ctx->sigma) ctx->run(s);
+    TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    // sigma += S
+    DAxpyTarget t{d_sigma, n, 0, 1};
+    DAxpySource so{ctx->buf[BUF_S], nullptr, 1.0};
+    // small one-off tables live in the staging allocation
+    if (!ctx->h_c) {
+      TCI_CUDA(cudaMalloc(&ctx->h_c, 64));
+      ctx->owned.push_back(ctx->h_c);
+    }
+    TCI_CUDA(cudaMemcpyAsync(ctx->h_c, &t, sizeof(t), cudaMemcpyHostToDevice, ctx->stream));
+    TCI_CUDA(cudaMemcpyAsync(((char*)ctx->h_c) + 32, &so, sizeof(so), cudaMemcpyHostToDevice, ctx->stream));
+    axpy_segments<<<1, 256, 0, ctx->stream>>>((DAxpyTarget*)ctx->h_c, 1, (DAxpySource*)(((char*)ctx->h_c) + 32));
+    TCI_CUDA(cudaGetLastError());
+    if (user != ctx->stream) {
+      TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+      TCI_CUDA(cudaStreamWaitEvent(user, ctx->ev1, 0));
+    }
+    ctx->sigma_count++;
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n) {
+  if (!ctx || !c || !sigma) return TCI_ERR_ARG;
+  try {
+    if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], c, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
+    TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (auto& s : ctx->sigma) ctx->run(s);
+    TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    std::vector<double> tmp(n);
+    TCI_CUDA(cudaMemcpyAsync(tmp.data(), ctx->buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+    float ms = 0;
+    TCI_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_sigma_ms = ms;
+    for (int64_t i = 0; i < n; ++i) sigma[i] += tmp[i];
+    ctx->sigma_count++;
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n) {
+  if (!ctx || !hdiag) return TCI_ERR_ARG;
+  set_error("tci_diag is not available in this build");
+  return TCI_ERR_INPUT;
+}
+
+int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
+  if (!ctx || !out || len < 8) return TCI_ERR_ARG;
+  out[0] = (double)ctx->plan.total_csfs;
+  out[1] = ctx->bytes_held;
+  out[2] = ctx->init_seconds;
+  out[3] = ctx->last_sigma_ms;
+  out[4] = ctx->plan.flops_total;
+  out[5] = ctx->plan.flops_allext;
+  out[6] = ctx->plan.bytes_allext;
+  out[7] = (double)ctx->sigma_count;
+  return TCI_OK;
+}
+
+void tci_destroy(tci_ctx* ctx) { delete ctx; }
+
+}  // extern "C"
