@@ -1,0 +1,66 @@
+"""The host-built sigma plan (coupling coefficients, task tables, dense
+pair-matrix algebra) replayed by a numpy interpreter equals sigma = H c of
+the dense oracle in the reference's CSF basis, for every term class."""
+import numpy as np
+import pytest
+
+import tigerci_b200 as T
+from cases import SMALL_CASES, case_id, oracle_deck, product_deck
+from oracle import dense
+from plan_exec import PlanInterpreter
+from tigerci_b200.synthetic import random_civec, synthetic_operator
+
+
+def _setup(c, tmp_path, nchol=10, seed=11):
+    h, L = synthetic_operator(c["no"], nchol, seed=seed, scale=0.3, diag_range=(-3, 1), offdiag_sigma=0.1)
+    plan = T.Plan(product_deck(c), T.Operator(h, L))
+    p = str(tmp_path / "plan.bin")
+    plan.export(p)
+    return h, L, PlanInterpreter(p, h, L), dense.DenseSigma(oracle_deck(c))
+
+
+@pytest.mark.parametrize("c", SMALL_CASES, ids=case_id)
+def test_plan_sigma_equals_dense_oracle(c, tmp_path):
+    h, L, pi, od = _setup(c, tmp_path)
+    for seed in (1, 2):
+        x = random_civec(od.ncsf, seed)
+        ref = od.sigma(h, L, x)
+        got = pi.sigma(x)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("c", SMALL_CASES[:3], ids=case_id)
+def test_plan_block_classes(c, tmp_path):
+    """Each source block (valence / N-1 / N-2) into each target block."""
+    h, L, pi, od = _setup(c, tmp_path, seed=3)
+    sp = od.space
+    nv, n1 = sp.num_valence, sp.num_nm1
+    blocks = [slice(0, nv), slice(nv, nv + n1), slice(nv + n1, od.ncsf)]
+    for sb in blocks:
+        x = np.zeros(od.ncsf)
+        x[sb] = random_civec(od.ncsf, 4)[sb]
+        ref = od.sigma(h, L, x)
+        got = pi.sigma(x)
+        assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def test_one_electron_only_operator(tmp_path):
+    """Zero Cholesky vectors isolate the one-electron couplings of every class."""
+    c = SMALL_CASES[2]
+    h, L = synthetic_operator(c["no"], 4, seed=2, scale=0.3, diag_range=(-3, 1), offdiag_sigma=0.2)
+    L[:] = 0.0
+    plan = T.Plan(product_deck(c), T.Operator(h, L))
+    p = str(tmp_path / "p.bin")
+    plan.export(p)
+    pi = PlanInterpreter(p, h, L)
+    od = dense.DenseSigma(oracle_deck(c))
+    x = random_civec(od.ncsf, 9)
+    ref = od.sigma(h, L, x)
+    assert np.abs(pi.sigma(x) - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_plan_is_deterministic(tmp_path):
+    c = SMALL_CASES[5]
+    h, L, pi, od = _setup(c, tmp_path)
+    x = random_civec(od.ncsf, 3)
+    assert np.array_equal(pi.sigma(x), pi.sigma(x))

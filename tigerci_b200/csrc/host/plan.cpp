@@ -147,6 +147,13 @@ struct Builder {
   void ss();
   void sv();
   void internal_blocks();
+  static Step mkstep(int kind, const char* name) {
+    Step s;
+    s.kind = kind;
+    s.name = name;
+    return s;
+  }
+  // Returned references are invalidated by the next push onto the same list.
   Step& step(std::vector<Step>& v, int kind, const char* name) {
     v.push_back(Step());
     v.back().kind = kind;
@@ -582,10 +589,11 @@ void Builder::ds() {
     for (size_t r = 0; r < order.size(); ++r) P.wv.insert(P.wv.end(), t1[order[r]].w.begin(), t1[order[r]].w.end());
     const i64 m = (i64)order.size();
     const i64 Z = T.alloc(m * n), Cg = T.alloc(m * n);
-    Step& g = step(P.sigma_steps, STEP_GEMM, "one-external forward");
-    Step& ga = step(P.sigma_steps, STEP_AXPY, "one-external reverse gather");
-    Step& gr = step(P.sigma_steps, STEP_GEMM, "one-external reverse");
-    Step& sc = step(P.sigma_steps, STEP_AXPY, "one-external scatter");
+    zero_step(P.sigma_steps, BUF_T0, Cg, m * n, "one-external gather zero");
+    Step g = mkstep(STEP_GEMM, "one-external forward");
+    Step ga = mkstep(STEP_AXPY, "one-external reverse gather");
+    Step gr = mkstep(STEP_GEMM, "one-external reverse");
+    Step sc = mkstep(STEP_AXPY, "one-external scatter");
     size_t r = 0;
     while (r < order.size()) {
       size_t e = r;
@@ -619,6 +627,10 @@ void Builder::ds() {
       tg.src_end = (i64)sc.as.size();
       sc.at.push_back(tg);
     }
+    P.sigma_steps.push_back(std::move(g));
+    P.sigma_steps.push_back(std::move(ga));
+    P.sigma_steps.push_back(std::move(gr));
+    P.sigma_steps.push_back(std::move(sc));
   }
 }
 
@@ -770,9 +782,10 @@ void Builder::ss() {
   });
   const i64 m = (i64)ts.size();
   const i64 Cg = T.alloc(m * n), Yr = T.alloc(m * n);
-  Step& ga = step(P.sigma_steps, STEP_AXPY, "ss gather");
-  Step& g = step(P.sigma_steps, STEP_GEMM, "ss two-external");
-  Step& sc = step(P.sigma_steps, STEP_AXPY, "ss scatter");
+  zero_step(P.sigma_steps, BUF_T0, Cg, m * n, "ss gather zero");
+  Step ga = mkstep(STEP_AXPY, "ss gather");
+  Step g = mkstep(STEP_GEMM, "ss two-external");
+  Step sc = mkstep(STEP_AXPY, "ss scatter");
   for (i64 r = 0; r < m; ++r) {
     AxpyTarget tg{BUF_T0, Cg + r * n, n, (i64)ga.as.size(), 0};
     ga.as.push_back(AxpySource{BUF_C, ts[order[r]].src_row, 1.0, -1, 0});
@@ -799,6 +812,9 @@ void Builder::ss() {
     tg.src_end = (i64)sc.as.size();
     sc.at.push_back(tg);
   }
+  P.sigma_steps.push_back(std::move(ga));
+  P.sigma_steps.push_back(std::move(g));
+  P.sigma_steps.push_back(std::move(sc));
 }
 
 // ---------------------------------------------------------------------------
