@@ -110,9 +110,17 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
 /* Diagonal H_ii (tiger_fortran/diag_element_mod_2.f90:83) for the
  * preconditioner, host array of length total_csfs. */
 int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n);
-/* out[0..7]: total_csfs, device bytes held, init seconds, last sigma ms,
- * flops per sigma, all-external flops, all-external bytes, sigma builds */
+/* out[0..8]: total_csfs, device bytes held, init seconds, last sigma ms,
+ * flops per sigma, all-external flops, all-external bytes, sigma builds,
+ * kernel launches per sigma build (out[8] written when len >= 9) */
 int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len);
+/* Per-step CUDA-event timing of the sigma plan (off by default).  When on,
+ * every sigma build records an event pair around each plan step on the
+ * context's stream; tci_step_times returns the accumulated milliseconds per
+ * step and the number of profiled builds since tci_profile was called. */
+int tci_profile(tci_ctx* ctx, int64_t on);
+int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps, int64_t* nbuilds);
+int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len);
 void tci_destroy(tci_ctx* ctx);
 
 #ifdef __cplusplus

@@ -46,7 +46,8 @@ def lib():
         L.oracle_hdet_matvec.argtypes = [C.c_int64, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p]
         L.oracle_allext_sigma.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
-                                          C.c_void_p, C.c_void_p]
+                                          C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
+        L.oracle_set_dgemm.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -171,8 +172,28 @@ class DenseSigma:
         return H
 
 
-def allext_sigma(space, nint, n, chol, c, nthreads=None):
-    """Reference integral-form all-external sigma (detci.c oracle_allext_sigma)."""
+def use_blas():
+    """Route the oracle's (ab|cd) slab through scipy's bundled OpenBLAS dgemm
+    (the reference calls dgemm there).  Returns True when found."""
+    import glob
+
+    import scipy
+
+    libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs", "libscipy_openblas*.so"))
+    for p in libs:
+        try:
+            ob = C.CDLL(p)
+            fn = getattr(ob, "scipy_dgemm_")
+        except (OSError, AttributeError):
+            continue
+        lib().oracle_set_dgemm(C.cast(fn, C.c_void_p))
+        return True
+    return False
+
+
+def allext_sigma(space, nint, n, chol, c, nthreads=None, a_range=None):
+    """Reference integral-form all-external sigma (detci.c oracle_allext_sigma);
+    a_range=(a0, a1) restricts the outer external index (a sample)."""
     heads = []
     for h in space.paths[2]:
         off_ab = -1 if h["off"] is None else h["off"]
@@ -189,6 +210,7 @@ def allext_sigma(space, nint, n, chol, c, nthreads=None):
     s = np.zeros_like(c)
     if nthreads:
         os.environ["OMP_NUM_THREADS"] = str(nthreads)
+    a0, a1 = a_range if a_range else (0, n)
     lib().oracle_allext_sigma(nint, n, chol.shape[1], chol.ctypes.data, len(heads), heads.ctypes.data,
-                              c.ctypes.data, s.ctypes.data)
+                              c.ctypes.data, s.ctypes.data, a0, a1)
     return s

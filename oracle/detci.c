@@ -112,8 +112,15 @@ void oracle_hdet_matvec(int64_t ndet, const uint64_t* dets, int n, const double*
  * Loops over a (OpenMP, like mod_1:442-465) and c <= a, forms the slab
  * V[b][d] = (ab|cd) for all b, d, and applies it to every head.
  */
+typedef void (*dgemm_fn)(const char*, const char*, const int*, const int*, const int*, const double*,
+                         const double*, const int*, const double*, const int*, const double*, double*, const int*);
+static dgemm_fn g_dgemm = 0;
+/* Optional BLAS dgemm (Fortran ABI), e.g. scipy's bundled OpenBLAS, used for
+ * the (ab|cd) slab like the reference's dgemm at mod_1:556. */
+void oracle_set_dgemm(void* fn) { g_dgemm = (dgemm_fn)fn; }
+
 void oracle_allext_sigma(int64_t nint, int64_t n, int64_t nchol, const double* chol, int64_t nh,
-                         const int64_t* heads, const double* c, double* sigma) {
+                         const int64_t* heads, const double* c, double* sigma, int64_t a_begin, int64_t a_end) {
   const double s2 = sqrt(2.0);
   const int64_t nab = n * (n - 1) / 2;
 #define PAIR(p, q) ((p) >= (q) ? (p) * ((p) + 1) / 2 + (q) : (q) * ((q) + 1) / 2 + (p))
@@ -124,19 +131,26 @@ void oracle_allext_sigma(int64_t nint, int64_t n, int64_t nchol, const double* c
     double* V = (double*)malloc(sizeof(double) * n * n);
     double* Vx = (double*)malloc(sizeof(double) * n * n);
 #pragma omp for schedule(dynamic, 1)
-    for (int64_t a = 0; a < n; ++a) {
+    for (int64_t a = a_begin; a < a_end; ++a) {
       for (int64_t b = 0; b < n; ++b) memcpy(Lab + b * nchol, chol + PAIR(nint + a, nint + b) * nchol, sizeof(double) * nchol);
       for (int64_t cc = 0; cc <= a; ++cc) {
         for (int64_t d = 0; d < n; ++d) memcpy(Lcd + d * nchol, chol + PAIR(nint + cc, nint + d) * nchol, sizeof(double) * nchol);
         /* V[b][d] = (ab|cd) = sum_J Lab[b][J] Lcd[d][J]  (the dgemm of mod_1:556) */
-        for (int64_t b = 0; b < n; ++b)
-          for (int64_t d = 0; d < n; ++d) {
-            const double* x = Lab + b * nchol;
-            const double* y = Lcd + d * nchol;
-            double acc = 0.0;
-            for (int64_t J = 0; J < nchol; ++J) acc += x[J] * y[J];
-            V[b * n + d] = acc;
-          }
+        if (g_dgemm) {
+          /* column-major view: V^T(d,b) = Lcd^T(d,J) Lab(J,b) */
+          const int nn = (int)n, kk = (int)nchol;
+          const double one = 1.0, zero = 0.0;
+          g_dgemm("T", "N", &nn, &nn, &kk, &one, Lcd, &kk, Lab, &kk, &zero, V, &nn);
+        } else {
+          for (int64_t b = 0; b < n; ++b)
+            for (int64_t d = 0; d < n; ++d) {
+              const double* x = Lab + b * nchol;
+              const double* y = Lcd + d * nchol;
+              double acc = 0.0;
+              for (int64_t J = 0; J < nchol; ++J) acc += x[J] * y[J];
+              V[b * n + d] = acc;
+            }
+        }
         /* exchange slab (ad|cb) = V'[d][b] needs (ad|cb): for fixed a,c it is V transposed */
         for (int64_t b = 0; b < n; ++b)
           for (int64_t d = 0; d < n; ++d) Vx[b * n + d] = V[d * n + b];

@@ -35,6 +35,9 @@ EXPORTS = [
     "tci_sigma_device",
     "tci_diag",
     "tci_ctx_stats",
+    "tci_profile",
+    "tci_step_times",
+    "tci_step_name",
     "tci_destroy",
 ]
 
@@ -95,6 +98,9 @@ def lib():
         L.tci_sigma_device.argtypes = [P, P, P, i64, P]
         L.tci_diag.argtypes = [P, P, i64]
         L.tci_ctx_stats.argtypes = [P, P, i64]
+        L.tci_profile.argtypes = [P, i64]
+        L.tci_step_times.argtypes = [P, P, i64, P, P]
+        L.tci_step_name.argtypes = [P, i64, C.c_char_p, i64]
         L.tci_destroy.argtypes = [P]
         L.tci_destroy.restype = None
         _lib = L

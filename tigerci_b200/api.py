@@ -191,9 +191,26 @@ class SigmaBuilder:
         """Device pointers (e.g. torch tensors' data_ptr()) on `stream`."""
         check(lib().tci_sigma_device(self._h, C.c_void_p(c_ptr), C.c_void_p(s_ptr), n, C.c_void_p(stream or None)))
 
+    def profile(self, on: bool = True):
+        """Per-step CUDA-event timing of subsequent sigma builds."""
+        check(lib().tci_profile(self._h, 1 if on else 0))
+
+    def step_times(self) -> list:
+        """[(step name, accumulated ms)] and the number of profiled builds."""
+        ns, nb = C.c_int64(), C.c_int64()
+        check(lib().tci_step_times(self._h, None, 0, C.byref(ns), C.byref(nb)))
+        ms = np.zeros(ns.value)
+        check(lib().tci_step_times(self._h, ptr(ms), ns.value, C.byref(ns), C.byref(nb)))
+        names = []
+        buf = C.create_string_buffer(128)
+        for i in range(ns.value):
+            check(lib().tci_step_name(self._h, i, buf, 128))
+            names.append(buf.value.decode())
+        return list(zip(names, ms.tolist())), nb.value
+
     def stats(self) -> dict:
-        out = np.zeros(8, dtype=np.float64)
-        check(lib().tci_ctx_stats(self._h, ptr(out), 8))
+        out = np.zeros(9, dtype=np.float64)
+        check(lib().tci_ctx_stats(self._h, ptr(out), 9))
         keys = ["total_csfs", "device_bytes", "init_seconds", "last_sigma_ms", "flops_per_sigma",
-                "flops_allext", "bytes_allext", "sigma_count"]
+                "flops_allext", "bytes_allext", "sigma_count", "launches_per_sigma"]
         return dict(zip(keys, out.tolist()))

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -240,6 +241,11 @@ __global__ void pack_pairs(const DHead* __restrict__ heads, const int* __restric
   }
 }
 
+__global__ void accumulate_f64(double* __restrict__ dst, const double* __restrict__ src, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] += src[i];
+}
+
 __device__ __forceinline__ long long pk(long long a, long long b) {
   return a >= b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a;
 }
@@ -322,15 +328,18 @@ struct tci_ctx {
   std::vector<DevStep> init, sigma;
   DHead* dheads = nullptr;
   int* dk_head = nullptr;
-  double* h_c = nullptr;  // device staging for host-buffer calls
-  double* h_s = nullptr;
   double bytes_held = 0;
   double init_seconds = 0;
   double last_sigma_ms = 0;
   long long sigma_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool profiling = false;
+  std::vector<cudaEvent_t> step_ev;     // 2 per sigma step
+  std::vector<double> step_ms;          // accumulated per sigma step
+  long long profiled_builds = 0;
 
   ~tci_ctx() {
+    for (auto e : step_ev) cudaEventDestroy(e);
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     for (int b = 0; b < NUM_BUFS; ++b)
@@ -362,9 +371,19 @@ struct tci_ctx {
         pr.push_back(DGemmProblem{ptr(g.c, g.offC), g.ldc, g.M, g.N, tn, tiles, g.beta, g.seg_begin, g.seg_end});
         tiles += tm * tn;
       }
-      for (auto& g : s.gs) {
-        // operand extents: A is M x K (or K x M), B is K x N (or N x K); checked loosely by offsets
-        sg.push_back(DGemmSeg{ptr(g.a, g.offA), ptr(g.b, g.offB), g.lda, g.ldb, g.K, g.tA, g.tB, g.alpha});
+      for (auto& g : s.gs) sg.push_back(DGemmSeg{ptr(g.a, g.offA), ptr(g.b, g.offB), g.lda, g.ldb, g.K, g.tA, g.tB, g.alpha});
+      // full operand extents: A is M x K (K x M if transposed), B is K x N (N x K)
+      for (auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        for (i64 q = g.seg_begin; q < g.seg_end; ++q) {
+          const GemmSeg& x = s.gs[q];
+          if (x.K <= 0) throw Error(TCI_ERR_INTERNAL, "GEMM segment with empty K");
+          const i64 ra = x.tA ? x.K : g.M, ca = x.tA ? g.M : x.K;
+          const i64 rb = x.tB ? g.N : x.K, cb = x.tB ? x.K : g.N;
+          if (ca > x.lda || cb > x.ldb) throw Error(TCI_ERR_INTERNAL, "GEMM leading dimension too small");
+          check_range(x.a, x.offA, (ra - 1) * x.lda + ca);
+          check_range(x.b, x.offB, (rb - 1) * x.ldb + cb);
+        }
       }
       d.probs = upload(pr, owned);
       d.segs = upload(sg, owned);
@@ -406,6 +425,28 @@ struct tci_ctx {
     return d;
   }
 
+  void run_sigma_steps() {
+    if (profiling && step_ev.size() != 2 * sigma.size()) {
+      step_ev.resize(2 * sigma.size());
+      for (auto& e : step_ev) TCI_CUDA(cudaEventCreate(&e));
+      step_ms.assign(sigma.size(), 0.0);
+    }
+    for (size_t i = 0; i < sigma.size(); ++i) {
+      if (profiling) TCI_CUDA(cudaEventRecord(step_ev[2 * i], stream));
+      run(sigma[i]);
+      if (profiling) TCI_CUDA(cudaEventRecord(step_ev[2 * i + 1], stream));
+    }
+    if (profiling) {
+      TCI_CUDA(cudaStreamSynchronize(stream));
+      for (size_t i = 0; i < sigma.size(); ++i) {
+        float ms = 0;
+        TCI_CUDA(cudaEventElapsedTime(&ms, step_ev[2 * i], step_ev[2 * i + 1]));
+        step_ms[i] += ms;
+      }
+      profiled_builds++;
+    }
+  }
+
   void check_range(int b, i64 off, i64 len) const {
     if (b < 0 || b >= NUM_BUFS || off < 0 || len < 0 || off + len > plan.buf_size[b])
       throw Error(TCI_ERR_INTERNAL, "plan range outside its buffer");
@@ -426,6 +467,7 @@ struct tci_ctx {
         if (s.zlen > 0) TCI_CUDA(cudaMemsetAsync(s.zptr, 0, s.zlen * sizeof(double), stream));
         break;
       case STEP_UNPACK:
+        if (plan.nD > 65535) throw Error(TCI_ERR_INPUT, "too many dense pair matrices for one launch");
         if (plan.nD > 0) {
           dim3 g((unsigned)std::min<long long>(64, (plan.n * plan.n + 255) / 256), (unsigned)plan.nD);
           unpack_pairs<<<g, 256, 0, stream>>>(dheads, dk_head, plan.nD, plan.n, buf[BUF_C], buf[BUF_D]);
@@ -520,19 +562,10 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
     TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
     TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (auto& s : ctx->sigma) ctx->run(s);
+    ctx->run_sigma_steps();
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
-    // sigma += S
-    DAxpyTarget t{d_sigma, n, 0, 1};
-    DAxpySource so{ctx->buf[BUF_S], nullptr, 1.0};
-    // small one-off tables live in the staging allocation
-    if (!ctx->h_c) {
-      TCI_CUDA(cudaMalloc(&ctx->h_c, 64));
-      ctx->owned.push_back(ctx->h_c);
-    }
-    TCI_CUDA(cudaMemcpyAsync(ctx->h_c, &t, sizeof(t), cudaMemcpyHostToDevice, ctx->stream));
-    TCI_CUDA(cudaMemcpyAsync(((char*)ctx->h_c) + 32, &so, sizeof(so), cudaMemcpyHostToDevice, ctx->stream));
-    axpy_segments<<<1, 256, 0, ctx->stream>>>((DAxpyTarget*)ctx->h_c, 1, (DAxpySource*)(((char*)ctx->h_c) + 32));
+    // sigma += S (the caller's sigma accumulates, like htimesc)
+    accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(d_sigma, ctx->buf[BUF_S], n);
     TCI_CUDA(cudaGetLastError());
     if (user != ctx->stream) {
       TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -553,7 +586,7 @@ int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n) {
     TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], c, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
     TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (auto& s : ctx->sigma) ctx->run(s);
+    ctx->run_sigma_steps();
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     std::vector<double> tmp(n);
     TCI_CUDA(cudaMemcpyAsync(tmp.data(), ctx->buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -577,6 +610,14 @@ int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n) {
 
 int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   if (!ctx || !out || len < 8) return TCI_ERR_ARG;
+  if (len >= 9) {
+    double launches = 1.0;  // final accumulation into the caller's sigma
+    for (const auto& s : ctx->sigma)
+      if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
+          ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && ctx->plan.nD > 0))
+        launches += 1.0;
+    out[8] = launches;
+  }
   out[0] = (double)ctx->plan.total_csfs;
   out[1] = ctx->bytes_held;
   out[2] = ctx->init_seconds;
@@ -585,6 +626,28 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   out[5] = ctx->plan.flops_allext;
   out[6] = ctx->plan.bytes_allext;
   out[7] = (double)ctx->sigma_count;
+  return TCI_OK;
+}
+
+int tci_profile(tci_ctx* ctx, int64_t on) {
+  if (!ctx) return TCI_ERR_ARG;
+  ctx->profiling = on != 0;
+  ctx->step_ms.assign(ctx->sigma.size(), 0.0);
+  ctx->profiled_builds = 0;
+  return TCI_OK;
+}
+
+int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps, int64_t* nbuilds) {
+  if (!ctx || !nsteps) return TCI_ERR_ARG;
+  *nsteps = (int64_t)ctx->sigma.size();
+  if (nbuilds) *nbuilds = ctx->profiled_builds;
+  for (int64_t i = 0; ms && i < len && i < (int64_t)ctx->step_ms.size(); ++i) ms[i] = ctx->step_ms[i];
+  return TCI_OK;
+}
+
+int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len) {
+  if (!ctx || !buf || len <= 0 || i < 0 || i >= (int64_t)ctx->sigma.size()) return TCI_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", ctx->sigma[i].name.c_str());
   return TCI_OK;
 }
 
