@@ -110,6 +110,15 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
 /* Diagonal H_ii (tiger_fortran/diag_element_mod_2.f90:83) for the
  * preconditioner, host array of length total_csfs. */
 int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n);
+/* Device-resident Davidson-Liu solve for the nroots lowest roots (replaces
+ * davidson_liu, tiger_fortran/davidson.f90:47-239, with the expansion and
+ * sigma vectors kept in HBM instead of on disk).  Converges a root when the
+ * residual norm drops below tol_residual (RESIDUAL TOLERANCE) or the energy
+ * change below tol_energy (ENERGY TOLERANCE); maxit <= 0 means 50 * nroots.
+ * energies[nroots] receives the eigenvalues of H (without the core energy);
+ * vectors (nroots x total_csfs, may be NULL) the normalised eigenvectors. */
+int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                 double* energies, double* vectors, int64_t* iterations);
 /* out[0..8]: total_csfs, device bytes held, init seconds, last sigma ms,
  * flops per sigma, all-external flops, all-external bytes, sigma builds,
  * kernel launches per sigma build (out[8] written when len >= 9) */

@@ -151,6 +151,35 @@ class PlanInterpreter:
             self.run(st)
         return self.bufs[_bid("S")].copy()
 
+    def diagonal(self):
+        """H_ii assembled from the plan's diagonal entries (same formula as the device)."""
+        pf = self.pf
+        n = pf.n
+        out = np.zeros(pf.total_csfs)
+        F = self.bufs[_bid("F")]
+        W = self.bufs[_bid("W")]
+        npl, nm = pf.np, pf.nm
+        for d in pf.diag:
+            o, ln, t, b, fo = int(d["off"]), int(d["len"]), int(d["type"]), float(d["beta"]), int(d["foff"])
+
+            def fd(a):
+                return F[fo + a * (n + 1)] if fo >= 0 else 0.0
+
+            if t == 0:
+                out[o] = b
+            elif t == 1:
+                out[o:o + ln] = [b + fd(a) for a in range(n)]
+            elif t == 2:
+                out[o:o + ln] = [b + 2 * fd(a) + W[a * npl + a] for a in range(n)]
+            else:
+                e = 0
+                for i in range(1, n):
+                    for j in range(i):
+                        w = W[(n + e) * npl + (n + e)] if d["singlet"] else W[npl * npl + e * nm + e]
+                        out[o + e] = b + fd(i) + fd(j) + w
+                        e += 1
+        return out
+
     def trace(self, c):
         """Per-step sigma increments (for debugging)."""
         pf = self.pf

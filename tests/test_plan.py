@@ -64,3 +64,14 @@ def test_plan_is_deterministic(tmp_path):
     h, L, pi, od = _setup(c, tmp_path)
     x = random_civec(od.ncsf, 3)
     assert np.array_equal(pi.sigma(x), pi.sigma(x))
+
+
+@pytest.mark.parametrize("c", SMALL_CASES, ids=case_id)
+def test_plan_diagonal_equals_dense_diagonal(c, tmp_path):
+    """H_ii assembled from zero-external betas, same-head operator diagonals
+    and the W diagonals (replaces diag_element, diag_element_mod_2.f90:83)."""
+    h, L, pi, od = _setup(c, tmp_path)
+    if od.ncsf > 800:
+        pytest.skip("dense diagonal too large")
+    H = od.hamiltonian(h, L)
+    assert np.abs(pi.diagonal() - np.diag(H)).max() <= 1e-12 * np.abs(np.diag(H)).max()

@@ -191,6 +191,22 @@ class SigmaBuilder:
         """Device pointers (e.g. torch tensors' data_ptr()) on `stream`."""
         check(lib().tci_sigma_device(self._h, C.c_void_p(c_ptr), C.c_void_p(s_ptr), n, C.c_void_p(stream or None)))
 
+    def diag(self) -> np.ndarray:
+        """Diagonal H_ii (preconditioner input)."""
+        out = np.zeros(self.n)
+        check(lib().tci_diag(self._h, ptr(out), self.n))
+        return out
+
+    def davidson(self, nroots: int = 1, tol_residual: float = 1e-6, tol_energy: float = 1e-6, maxit: int = 0,
+                 want_vectors: bool = False):
+        """Device-resident Davidson-Liu (davidson_liu); returns (energies, vectors|None, iterations)."""
+        e = np.zeros(nroots)
+        v = np.zeros((nroots, self.n)) if want_vectors else None
+        it = C.c_int64()
+        check(lib().tci_davidson(self._h, nroots, tol_residual, tol_energy, maxit, ptr(e),
+                                 ptr(v) if v is not None else None, C.byref(it)))
+        return e, v, it.value
+
     def profile(self, on: bool = True):
         """Per-step CUDA-event timing of subsequent sigma builds."""
         check(lib().tci_profile(self._h, 1 if on else 0))

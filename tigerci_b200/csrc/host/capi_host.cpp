@@ -236,12 +236,13 @@ int tci_plan_export(const tci_plan* p, const char* path) {
   const std::vector<Step>* lists[2] = {&P.init_steps, &P.sigma_steps};
   wi(P.nint); wi(P.n); wi(P.nchol); wi(P.total_csfs); wi(P.npair_all); wi(P.nD);
   wi((int64_t)P.dheads.size()); wi(NUM_BUFS); wi((int64_t)P.init_steps.size()); wi((int64_t)P.sigma_steps.size());
-  wi((int64_t)P.h_vv.size()); wi((int64_t)P.wv.size()); wi(P.np); wi(P.nm);
+  wi((int64_t)P.h_vv.size()); wi((int64_t)P.wv.size()); wi(P.np); wi(P.nm); wi((int64_t)P.diag.size());
   for (int b = 0; b < NUM_BUFS; ++b) wi(P.buf_size[b]);
   for (auto& d : P.dheads) { wi(d.off_ab); wi(d.off_aa); wi(d.nsf_ab); wi(d.nsf_aa); wi(d.nsing); wi(d.nD); wi(d.dk0); }
   for (double v : P.dk_sign) wd(v);
   for (double v : P.h_vv) wd(v);
   for (double v : P.wv) wd(v);
+  for (auto& d : P.diag) { wi(d.off); wi(d.len); wi(d.type); wd(d.beta); wi(d.foff); wi(d.singlet); }
   for (auto* L : lists)
     for (const Step& s : *L) {
       wi(s.kind);

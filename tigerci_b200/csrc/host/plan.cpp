@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <memory>
+#include <tuple>
 #include <unordered_map>
 
 #include "coupling.h"
@@ -105,6 +106,10 @@ struct Builder {
   Scratch T;                  // BUF_T0 regions used per sigma build
   i64 init_scratch = 0;       // BUF_T0 doubles used during init
   i64 offJ = 0, offK = 0, offH = 0;
+  // zero-external diagonal beta per (block, path, k) and same-head operator offsets per (kind, path, k)
+  std::map<std::tuple<int, i64, i64>, double> beta_diag;
+  std::map<std::tuple<int, i64, i64>, i64> fdiag;
+  void build_diag();
 
   Builder(const CsfSpace& s, const Operator& o, Plan& p) : sp(s), op(o), P(p) {}
 
@@ -303,6 +308,11 @@ void Builder::internal_blocks() {
               }
       }
     }
+    for (auto& kv : blocks)
+      if (kv.first.first == kv.first.second) {
+        const i64 ns = nsf_of(heads[kv.first.first]);
+        for (i64 a = 0; a < ns; ++a) beta_diag[{pt.block, kv.first.first, a}] = kv.second[(size_t)a * ns + a];
+      }
     std::map<i64, std::vector<std::pair<i64, const std::vector<double>*>>> bytgt;
     for (auto& kv : blocks) bytgt[kv.first.first].push_back({kv.first.second, &kv.second});
     for (auto& tv : bytgt) {
@@ -393,6 +403,7 @@ void Builder::dd_x() {
           tg.src_end = (i64)fcomb.as.size();
           fcomb.at.push_back(tg);
           terms[dk(S, kt)].push_back(Term{dk(S, ks), BUF_F, nF * n2, 1.0});
+          if (kt == ks) fdiag[{2, (i64)hs, kt}] = nF * n2;
           ++nF;
         }
     }
@@ -750,6 +761,7 @@ void Builder::ss() {
           tg.src_end = (i64)fcomb.as.size();
           fcomb.at.push_back(tg);
           ts.push_back(TS{S.off + kt * n, S.off + ks * n, BUF_F, nF * n2, 1.0});
+          if (kt == ks) fdiag[{1, (i64)hs, kt}] = nF * n2;
           ++nF;
         }
     }
@@ -965,6 +977,38 @@ void Builder::allext() {
 }
 
 // ---------------------------------------------------------------------------
+void Builder::build_diag() {
+  auto beta = [&](int block, i64 p, i64 k) {
+    auto it = beta_diag.find({block, p, k});
+    return it == beta_diag.end() ? 0.0 : it->second;
+  };
+  auto foff = [&](int kind, i64 p, i64 k) -> i64 {
+    auto it = fdiag.find({kind, p, k});
+    return it == fdiag.end() ? -1 : it->second;
+  };
+  for (size_t p = 0; p < sp.paths[0].size(); ++p) {
+    const Head& h = sp.paths[0][p];
+    if (!has(h)) continue;
+    for (i64 k = 0; k < h.nsf; ++k) P.diag.push_back(DiagEntry{h.off + k, 1, 0, beta(0, (i64)p, k), -1, 1});
+  }
+  for (size_t p = 0; p < sp.paths[1].size(); ++p) {
+    const Head& h = sp.paths[1][p];
+    if (!has(h)) continue;
+    for (i64 k = 0; k < h.nsf; ++k) P.diag.push_back(DiagEntry{h.off + k * n, n, 1, beta(1, (i64)p, k), foff(1, (i64)p, k), 1});
+  }
+  for (size_t p = 0; p < sp.paths[2].size(); ++p) {
+    const Head& h = sp.paths[2][p];
+    if (!h.kept || nDh[p] == 0) continue;
+    if (h.off_aa >= 0)
+      for (i64 k = 0; k < h.nsf_aa; ++k)
+        P.diag.push_back(DiagEntry{h.off_aa + k * n, n, 2, beta(2, (i64)p, k), foff(2, (i64)p, k), 1});
+    if (h.off >= 0 && nab > 0)
+      for (i64 k = 0; k < h.nsf; ++k)
+        P.diag.push_back(DiagEntry{h.off + k * nab, nab, 3, beta(3, (i64)p, k), foff(2, (i64)p, k),
+                                   P.dk_sign[dk0[p] + k] > 0 ? 1 : 0});
+  }
+}
+
 void Builder::init_steps() {
   // gather L rows into dense blocks
   Step& ga = step(P.init_steps, STEP_AXPY, "gather cholesky rows");
@@ -1058,6 +1102,7 @@ void Builder::run() {
   sv();
   internal_blocks();
   step(P.sigma_steps, STEP_PACK, "pack");
+  build_diag();
   P.h_vv.assign(n2, 0.0);
   for (i64 a = 0; a < n; ++a)
     for (i64 b = 0; b < n; ++b) P.h_vv[a * n + b] = I.h1(nint + a, nint + b);

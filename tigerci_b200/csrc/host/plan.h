@@ -101,6 +101,21 @@ struct DHeadInfo {
   i64 dk0;             // first dense matrix index
 };
 
+// One contiguous run of CSFs whose diagonal H_ii is assembled on the device:
+//   type 0 valence:   beta
+//   type 1 N-1 row:   beta + F(a,a)
+//   type 2 N-2 aa:    beta + 2 F(a,a) + W+(a,a)
+//   type 3 N-2 ab:    beta + F(i,i) + F(j,j) + W+-((ij),(ij))
+// beta is the zero-external diagonal, F the same-head operator (BUF_F offset
+// foff, -1 if none) and W the all-external operator.
+struct DiagEntry {
+  i64 off, len;
+  i64 type;
+  double beta;
+  i64 foff;
+  i64 singlet;
+};
+
 struct Plan {
   i64 nint = 0, n = 0, nchol = 0, total_csfs = 0, npair_all = 0;
   i64 nD = 0;                    // dense N-2 matrices
@@ -111,6 +126,7 @@ struct Plan {
   std::vector<double> wv;        // BUF_WV contents
   std::vector<Step> init_steps;  // run once after upload of L
   std::vector<Step> sigma_steps; // run per sigma build
+  std::vector<DiagEntry> diag;   // diagonal H_ii assembly
   // algorithmic work per sigma build, for roofline reporting
   double flops_allext = 0, flops_total = 0, bytes_allext = 0;
   i64 np = 0, nm = 0;            // packed pair dimensions of W+ / W-

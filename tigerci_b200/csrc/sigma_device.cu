@@ -11,6 +11,7 @@
 // build is bitwise reproducible.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cmath>
@@ -286,6 +287,109 @@ __global__ void build_allext(const double* __restrict__ X, long long n, double* 
   }
 }
 
+
+// ----------------------------------------------------------------------------
+// diagonal H_ii from the plan's diagonal entries (plan.h DiagEntry)
+struct DDiag {
+  long long off, len, type;
+  double beta;
+  long long foff, singlet;
+};
+
+__global__ void build_diag_kernel(const DDiag* __restrict__ ent, long long nent, long long n, long long np, long long nm,
+                                  const double* __restrict__ F, const double* __restrict__ W, double* __restrict__ hd) {
+  const long long e = blockIdx.x;
+  if (e >= nent) return;
+  const DDiag D = ent[e];
+  for (long long t = threadIdx.x; t < D.len; t += blockDim.x) {
+    double v = D.beta;
+    if (D.type == 1) {
+      if (D.foff >= 0) v += F[D.foff + t * (n + 1)];
+    } else if (D.type == 2) {
+      if (D.foff >= 0) v += 2.0 * F[D.foff + t * (n + 1)];
+      v += W[t * np + t];
+    } else if (D.type == 3) {
+      long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)t)) * 0.5);
+      while (i * (i - 1) / 2 > t) --i;
+      while ((i + 1) * i / 2 <= t) ++i;
+      const long long j = t - i * (i - 1) / 2;
+      if (D.foff >= 0) v += F[D.foff + i * (n + 1)] + F[D.foff + j * (n + 1)];
+      v += D.singlet ? W[(n + t) * np + (n + t)] : W[np * np + t * nm + t];
+    }
+    hd[D.off + t] = v;
+  }
+}
+
+// Davidson vector kernels (FP64, deterministic two-pass reductions)
+constexpr int RB = 256;     // threads per reduction block
+constexpr int RBLK = 592;   // reduction blocks (4 x 148 SMs)
+
+// partial[k * RBLK + b] = sum over block b's chunk of A[k][i] * x[i]
+__global__ void __launch_bounds__(RB) multi_dot_partial(const double* __restrict__ A, long long lda, int m,
+                                                        const double* __restrict__ x, long long n,
+                                                        double* __restrict__ partial) {
+  __shared__ double red[RB / 32];
+  const long long chunk = (n + gridDim.x - 1) / gridDim.x;
+  const long long i0 = (long long)blockIdx.x * chunk, i1 = min(n, i0 + chunk);
+  for (int k = 0; k < m; ++k) {
+    const double* a = A + (long long)k * lda;
+    double acc = 0.0;
+    for (long long i = i0 + threadIdx.x; i < i1; i += RB) acc = fma(a[i], x[i], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < RB / 32; ++w) t += red[w];
+      partial[(long long)k * gridDim.x + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void multi_dot_final(const double* __restrict__ partial, int m, int nblk, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  double t = 0.0;
+  for (int b = 0; b < nblk; ++b) t += partial[(long long)k * nblk + b];
+  out[k] = t;
+}
+
+// out[i] = beta*out[i] + sum_k ca[k] A[k][i] + sum_k cb[k] B[k][i]
+__global__ void lincomb_kernel(double* __restrict__ out, double beta, const double* __restrict__ A,
+                               const double* __restrict__ ca, const double* __restrict__ B,
+                               const double* __restrict__ cb, int m, long long lda, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double v = (beta == 0.0) ? 0.0 : beta * out[i];
+    for (int k = 0; k < m; ++k) {
+      if (A) v = fma(ca[k], A[(long long)k * lda + i], v);
+      if (B) v = fma(cb[k], B[(long long)k * lda + i], v);
+    }
+    out[i] = v;
+  }
+}
+
+// r_i <- -r_i / (hd_i - E), 0 where hd_i == E (davidson.f90:609-631)
+__global__ void precondition_kernel(double* __restrict__ r, const double* __restrict__ hd, double E, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double p = hd[i] - E;
+    r[i] = (p == 0.0) ? 0.0 : -r[i] / p;
+  }
+}
+
+// r <- (r - ov*c) then scaled by 1/|r| (or zeroed) in a second pass
+__global__ void axpy_scale_kernel(double* __restrict__ r, const double* __restrict__ c, const double* __restrict__ ov,
+                                  long long n) {
+  const double a = *ov;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    r[i] = fma(-a, c[i], r[i]);
+}
+__global__ void normalize_kernel(double* __restrict__ r, const double* __restrict__ nrm2, long long n) {
+  const double nr = sqrt(*nrm2);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    r[i] = (fabs(nr) < 1e-14) ? 0.0 : r[i] / nr;
+}
 // ----------------------------------------------------------------------------
 struct DevStep {
   int kind = 0;
@@ -334,6 +438,9 @@ struct tci_ctx {
   long long sigma_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool profiling = false;
+  double* hd = nullptr;          // diagonal H_ii (device), built on first use
+  double* dots = nullptr;        // reduction scratch: partial sums and results
+  double* coefs = nullptr;       // small device coefficient arrays
   std::vector<cudaEvent_t> step_ev;     // 2 per sigma step
   std::vector<double> step_ms;          // accumulated per sigma step
   long long profiled_builds = 0;
@@ -425,6 +532,55 @@ struct tci_ctx {
     return d;
   }
 
+
+  void ensure_diag() {
+    if (hd) return;
+    const i64 n = plan.total_csfs;
+    TCI_CUDA(cudaMalloc(&hd, n * sizeof(double)));
+    owned.push_back(hd);
+    TCI_CUDA(cudaMemsetAsync(hd, 0, n * sizeof(double), stream));
+    std::vector<DDiag> e;
+    for (auto& d : plan.diag) e.push_back(DDiag{d.off, d.len, d.type, d.beta, d.foff, d.singlet});
+    for (auto& d : plan.diag) check_range(BUF_S, d.off, d.len);
+    DDiag* de = upload(e, owned);
+    if (!e.empty())
+      build_diag_kernel<<<(unsigned)e.size(), 256, 0, stream>>>(de, (long long)e.size(), plan.n, plan.np, plan.nm,
+                                                                buf[BUF_F], buf[BUF_W], hd);
+    TCI_CUDA(cudaGetLastError());
+    TCI_CUDA(cudaStreamSynchronize(stream));
+  }
+
+  void ensure_scratch(int mmax) {
+    if (dots) return;
+    TCI_CUDA(cudaMalloc(&dots, ((size_t)mmax * (RBLK + 1) + 16) * sizeof(double)));
+    owned.push_back(dots);
+    TCI_CUDA(cudaMalloc(&coefs, (size_t)4 * mmax * sizeof(double)));
+    owned.push_back(coefs);
+  }
+
+  // out[0..m) = A[k] . x  (host result), deterministic
+  void multi_dot(const double* A, i64 lda, int m, const double* x, i64 n, double* host_out) {
+    multi_dot_partial<<<RBLK, RB, 0, stream>>>(A, lda, m, x, n, dots);
+    multi_dot_final<<<(m + 127) / 128, 128, 0, stream>>>(dots, m, RBLK, dots + (size_t)m * RBLK);
+    TCI_CUDA(cudaGetLastError());
+    TCI_CUDA(cudaMemcpyAsync(host_out, dots + (size_t)m * RBLK, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    TCI_CUDA(cudaStreamSynchronize(stream));
+  }
+  // device-resident single dot into dots[off]
+  void dot_dev(const double* a, const double* x, i64 n, double* dev_out) {
+    multi_dot_partial<<<RBLK, RB, 0, stream>>>(a, 0, 1, x, n, dots);
+    multi_dot_final<<<1, 32, 0, stream>>>(dots, 1, RBLK, dev_out);
+    TCI_CUDA(cudaGetLastError());
+  }
+
+  void sigma_of(const double* d_c, double* d_s) {
+    const i64 n = plan.total_csfs;
+    TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
+    run_sigma_steps();
+    TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    sigma_count++;
+  }
   void run_sigma_steps() {
     if (profiling && step_ev.size() != 2 * sigma.size()) {
       step_ev.resize(2 * sigma.size());
@@ -512,8 +668,11 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
       if (P.buf_size[b] <= 0) continue;
       cudaError_t e = cudaMalloc(&ctx->buf[b], P.buf_size[b] * sizeof(double));
       if (e != cudaSuccess) throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+      // plan steps accumulate into their targets: every buffer starts at zero
+      TCI_CUDA(cudaMemsetAsync(ctx->buf[b], 0, P.buf_size[b] * sizeof(double), ctx->stream));
       ctx->bytes_held += (double)P.buf_size[b] * sizeof(double);
     }
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     TCI_CUDA(cudaMemcpy(ctx->buf[BUF_L], o.chol, P.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice));
     TCI_CUDA(cudaMemcpy(ctx->buf[BUF_JK] + 2 * P.nint * P.nint * P.n * P.n, P.h_vv.data(), P.h_vv.size() * sizeof(double),
                         cudaMemcpyHostToDevice));
@@ -604,8 +763,247 @@ int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n) {
 
 int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n) {
   if (!ctx || !hdiag) return TCI_ERR_ARG;
-  set_error("tci_diag is not available in this build");
-  return TCI_ERR_INPUT;
+  try {
+    if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    ctx->ensure_diag();
+    TCI_CUDA(cudaMemcpy(hdiag, ctx->hd, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+}  // extern "C"
+
+namespace {
+
+// Cyclic Jacobi eigensolver for the small symmetric subspace matrix (the role of
+// dsyev in dsyev_wrapper, tiger_fortran/math_utils.f90:417-479).  A is m x m row
+// major; on exit w holds ascending eigenvalues and V (m x m, columns) the vectors.
+void jacobi_eigh(std::vector<double> A, int m, std::vector<double>& w, std::vector<double>& V) {
+  V.assign((size_t)m * m, 0.0);
+  for (int i = 0; i < m; ++i) V[(size_t)i * m + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) {
+        const double a = A[(size_t)i * m + j] * A[(size_t)i * m + j];
+        tot += a;
+        if (i != j) off += a;
+      }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < m - 1; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = A[(size_t)p * m + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double app = A[(size_t)p * m + p], aqq = A[(size_t)q * m + q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < m; ++k) {
+          const double akp = A[(size_t)k * m + p], akq = A[(size_t)k * m + q];
+          A[(size_t)k * m + p] = c * akp - s * akq;
+          A[(size_t)k * m + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < m; ++k) {
+          const double apk = A[(size_t)p * m + k], aqk = A[(size_t)q * m + k];
+          A[(size_t)p * m + k] = c * apk - s * aqk;
+          A[(size_t)q * m + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < m; ++k) {
+          const double vkp = V[(size_t)k * m + p], vkq = V[(size_t)k * m + q];
+          V[(size_t)k * m + p] = c * vkp - s * vkq;
+          V[(size_t)k * m + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<int> ord(m);
+  for (int i = 0; i < m; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int a, int b) { return A[(size_t)a * m + a] < A[(size_t)b * m + b]; });
+  w.resize(m);
+  std::vector<double> V2((size_t)m * m);
+  for (int j = 0; j < m; ++j) {
+    w[j] = A[(size_t)ord[j] * m + ord[j]];
+    // fix the sign so that the largest component is positive (deterministic output)
+    int big = 0;
+    for (int k = 1; k < m; ++k)
+      if (std::fabs(V[(size_t)k * m + ord[j]]) > std::fabs(V[(size_t)big * m + ord[j]])) big = k;
+    const double sg = V[(size_t)big * m + ord[j]] < 0 ? -1.0 : 1.0;
+    for (int k = 0; k < m; ++k) V2[(size_t)k * m + j] = sg * V[(size_t)k * m + ord[j]];
+  }
+  V.swap(V2);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Block Davidson-Liu with HBM-resident expansion and sigma vectors, restating
+// davidson_liu (tiger_fortran/davidson.f90:47-239): per unconverged root one
+// sigma build and subspace expansion; subspace eigensolve; wavefunction,
+// residual, convergence test (is_converged :564-602), diagonal preconditioner
+// (:609-631) and modified Gram-Schmidt with renormalisation after every
+// projection (:702-723).  The initial guess is the unit vectors of the lowest
+// diagonal elements (init_from_diag, initial_davidson_guess.f90:99-137).  When
+// the subspace reaches its capacity it collapses onto the current Ritz vectors.
+int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                 double* energies, double* vectors, int64_t* iterations) {
+  if (!ctx || !energies || nroots <= 0) return TCI_ERR_ARG;
+  try {
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    const i64 n = ctx->plan.total_csfs;
+    if (nroots > n) throw Error(TCI_ERR_ARG, "more roots than CSFs");
+    if (maxit <= 0) maxit = 50 * nroots;
+    const int cap = (int)std::min<i64>(n, std::max<i64>(2 * nroots, (maxit + 1) * nroots));
+    ctx->ensure_diag();
+    ctx->ensure_scratch(cap + 4);
+    double *Cs = nullptr, *HCs = nullptr, *r = nullptr;
+    auto free_all = [&]() {
+      if (Cs) cudaFree(Cs);
+      if (HCs) cudaFree(HCs);
+      if (r) cudaFree(r);
+    };
+    try {
+      cudaError_t e1 = cudaMalloc(&Cs, (size_t)cap * n * sizeof(double));
+      cudaError_t e2 = cudaMalloc(&HCs, (size_t)cap * n * sizeof(double));
+      cudaError_t e3 = cudaMalloc(&r, (size_t)(n + 8) * sizeof(double));
+      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        throw Error(TCI_ERR_MEMORY, "device allocation of the Davidson subspace failed");
+      cudaStream_t st = ctx->stream;
+      const unsigned G = 148 * 8, TB = 256;
+      // initial guess: unit vectors at the lowest diagonal elements
+      std::vector<double> hd(n);
+      TCI_CUDA(cudaMemcpy(hd.data(), ctx->hd, n * sizeof(double), cudaMemcpyDeviceToHost));
+      std::vector<i64> idx(n);
+      for (i64 i = 0; i < n; ++i) idx[i] = i;
+      std::partial_sort(idx.begin(), idx.begin() + nroots, idx.end(),
+                        [&](i64 a, i64 b) { return hd[a] < hd[b] || (hd[a] == hd[b] && a < b); });
+      TCI_CUDA(cudaMemsetAsync(Cs, 0, (size_t)nroots * n * sizeof(double), st));
+      const double one = 1.0;
+      for (i64 k = 0; k < nroots; ++k)
+        TCI_CUDA(cudaMemcpyAsync(Cs + k * n + idx[k], &one, sizeof(double), cudaMemcpyHostToDevice, st));
+      TCI_CUDA(cudaStreamSynchronize(st));
+      int num_vec = (int)nroots;
+      std::vector<int> root2index(nroots);
+      for (int k = 0; k < nroots; ++k) root2index[k] = k;
+      std::vector<char> conv(nroots, 0), restarted(maxit + 2, 0);
+      std::vector<double> energy(nroots, 0.0), dE(nroots, 0.0), hsub((size_t)cap * cap, 0.0), w, V, col(cap);
+      i64 it = 0;
+      for (it = 1; it <= maxit; ++it) {
+        for (int q = 0; q < nroots; ++q) {
+          if (conv[q]) continue;
+          const int index = root2index[q];
+          ctx->sigma_of(Cs + (size_t)index * n, HCs + (size_t)index * n);
+          ctx->multi_dot(Cs, n, index + 1, HCs + (size_t)index * n, n, col.data());
+          for (int k = 0; k <= index; ++k) hsub[(size_t)k * cap + index] = hsub[(size_t)index * cap + k] = col[k];
+        }
+        std::vector<double> h((size_t)num_vec * num_vec);
+        for (int a = 0; a < num_vec; ++a)
+          for (int b = 0; b < num_vec; ++b) h[(size_t)a * num_vec + b] = hsub[(size_t)a * cap + b];
+        jacobi_eigh(h, num_vec, w, V);
+        for (int q = 0; q < nroots; ++q) {
+          dE[q] = std::fabs(w[q] - energy[q]);
+          energy[q] = w[q];
+        }
+        if (num_vec + nroots > cap) {
+          // collapse onto the current Ritz vectors (and their sigma vectors)
+          restarted[it] = 1;
+          std::vector<double> cvec((size_t)nroots * num_vec);
+          for (int q = 0; q < nroots; ++q)
+            for (int k = 0; k < num_vec; ++k) cvec[(size_t)q * num_vec + k] = V[(size_t)k * num_vec + q];
+          double *tmpC = nullptr, *tmpH = nullptr;
+          TCI_CUDA(cudaMalloc(&tmpC, (size_t)nroots * n * sizeof(double)));
+          TCI_CUDA(cudaMalloc(&tmpH, (size_t)nroots * n * sizeof(double)));
+          for (int q = 0; q < nroots; ++q) {
+            TCI_CUDA(cudaMemcpyAsync(ctx->coefs, cvec.data() + (size_t)q * num_vec, num_vec * sizeof(double),
+                                     cudaMemcpyHostToDevice, st));
+            lincomb_kernel<<<G, TB, 0, st>>>(tmpC + (size_t)q * n, 0.0, Cs, ctx->coefs, nullptr, nullptr, num_vec, n, n);
+            lincomb_kernel<<<G, TB, 0, st>>>(tmpH + (size_t)q * n, 0.0, HCs, ctx->coefs, nullptr, nullptr, num_vec, n, n);
+            TCI_CUDA(cudaStreamSynchronize(st));
+          }
+          TCI_CUDA(cudaMemcpyAsync(Cs, tmpC, (size_t)nroots * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          TCI_CUDA(cudaMemcpyAsync(HCs, tmpH, (size_t)nroots * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          TCI_CUDA(cudaStreamSynchronize(st));
+          cudaFree(tmpC);
+          cudaFree(tmpH);
+          std::fill(hsub.begin(), hsub.end(), 0.0);
+          for (int q = 0; q < nroots; ++q) hsub[(size_t)q * cap + q] = w[q];
+          num_vec = (int)nroots;
+          V.assign((size_t)num_vec * num_vec, 0.0);
+          for (int q = 0; q < nroots; ++q) V[(size_t)q * num_vec + q] = 1.0;
+        }
+        for (int q = 0; q < nroots; ++q) {
+          if (conv[q]) continue;
+          // residual r = sum_k a_k (Hc_k - E c_k)
+          std::vector<double> ca(num_vec), cb(num_vec);
+          for (int k = 0; k < num_vec; ++k) {
+            cb[k] = V[(size_t)k * num_vec + q];
+            ca[k] = -energy[q] * cb[k];
+          }
+          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, ca.data(), num_vec * sizeof(double), cudaMemcpyHostToDevice, st));
+          TCI_CUDA(cudaMemcpyAsync(ctx->coefs + cap, cb.data(), num_vec * sizeof(double), cudaMemcpyHostToDevice, st));
+          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, HCs, ctx->coefs + cap, num_vec, n, n);
+          TCI_CUDA(cudaGetLastError());
+          double nrm2 = 0.0;
+          ctx->multi_dot(r, 0, 1, r, n, &nrm2);
+          const double norm = std::sqrt(nrm2);
+          // is_converged: never right after a restart; residual norm, then energy change (i > 1), then maxit
+          bool halt = false;
+          if (!(restarted[it] || (it > 1 && restarted[it - 1]))) {
+            if (norm < tol_residual) halt = true;
+            else if (std::fabs(dE[q]) < tol_energy) halt = it > 1;
+            else if (it == maxit) halt = true;
+          }
+          if (halt) {
+            conv[q] = 1;
+            continue;
+          }
+          precondition_kernel<<<G, TB, 0, st>>>(r, ctx->hd, energy[q], n);
+          TCI_CUDA(cudaGetLastError());
+          double* dev_ov = ctx->dots + (size_t)(cap + 4) * RBLK;
+          for (int k = 0; k < num_vec; ++k) {
+            ctx->dot_dev(r, Cs + (size_t)k * n, n, dev_ov);
+            axpy_scale_kernel<<<G, TB, 0, st>>>(r, Cs + (size_t)k * n, dev_ov, n);
+            ctx->dot_dev(r, r, n, dev_ov + 1);
+            normalize_kernel<<<G, TB, 0, st>>>(r, dev_ov + 1, n);
+          }
+          TCI_CUDA(cudaGetLastError());
+          if (num_vec >= cap) throw Error(TCI_ERR_INTERNAL, "Davidson subspace capacity exceeded");
+          TCI_CUDA(cudaMemcpyAsync(Cs + (size_t)num_vec * n, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          root2index[q] = num_vec;
+          num_vec++;
+        }
+        TCI_CUDA(cudaStreamSynchronize(st));
+        bool all = true;
+        for (int q = 0; q < nroots; ++q) all = all && conv[q];
+        if (all) break;
+      }
+      for (int q = 0; q < nroots; ++q) energies[q] = energy[q];
+      if (iterations) *iterations = std::min<i64>(it, maxit);
+      if (vectors) {
+        for (int q = 0; q < nroots; ++q) {
+          std::vector<double> cb(num_vec);
+          for (int k = 0; k < num_vec; ++k) cb[k] = V[(size_t)k * num_vec + q];
+          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, cb.data(), num_vec * sizeof(double), cudaMemcpyHostToDevice, st));
+          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, nullptr, nullptr, num_vec, n, n);
+          double nrm2 = 0.0;
+          ctx->multi_dot(r, 0, 1, r, n, &nrm2);
+          std::vector<double> hv(n);
+          TCI_CUDA(cudaMemcpy(hv.data(), r, n * sizeof(double), cudaMemcpyDeviceToHost));
+          const double inv = 1.0 / std::sqrt(nrm2);
+          for (i64 i = 0; i < n; ++i) vectors[(size_t)q * n + i] = hv[i] * inv;
+        }
+      }
+    } catch (...) {
+      free_all();
+      throw;
+    }
+    free_all();
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
 }
 
 int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {

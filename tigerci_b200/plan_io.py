@@ -2,8 +2,9 @@
 
 Layout (all fields 8 bytes, little endian): magic "TCIPLAN1"; header
 (nint, n, nchol, total_csfs, npair_all, nD, n_dheads, NUM_BUFS, n_init,
-n_sigma, len h_vv, len wv, np, nm); buffer sizes; N-2 head records
-(off_ab, off_aa, nsf_ab, nsf_aa, nsing, nD, dk0); dk signs; h_vv; wv; then
+n_sigma, len h_vv, len wv, np, nm, n_diag); buffer sizes; N-2 head records
+(off_ab, off_aa, nsf_ab, nsf_aa, nsing, nD, dk0); dk signs; h_vv; wv; diagonal
+entries (off, len, type, beta, foff, singlet); then
 each step: kind, 64-byte name, counts (gp, gs, at, as, dt, ds), buf, off,
 len and the tables.
 """
@@ -22,6 +23,7 @@ AT = np.dtype([("dst", "<i8"), ("off", "<i8"), ("len", "<i8"), ("src_begin", "<i
 AS = np.dtype([("src", "<i8"), ("off", "<i8"), ("coef", "<f8"), ("sbuf", "<i8"), ("sidx", "<i8")])
 DT = np.dtype([("dst", "<i8"), ("off", "<i8"), ("src_begin", "<i8"), ("src_end", "<i8")])
 DS = np.dtype([("a", "<i8"), ("b", "<i8"), ("aoff", "<i8"), ("boff", "<i8"), ("len", "<i8"), ("coef", "<f8")])
+DG = np.dtype([("off", "<i8"), ("len", "<i8"), ("type", "<i8"), ("beta", "<f8"), ("foff", "<i8"), ("singlet", "<i8")])
 DH = np.dtype([("off_ab", "<i8"), ("off_aa", "<i8"), ("nsf_ab", "<i8"), ("nsf_aa", "<i8"), ("nsing", "<i8"),
                ("nD", "<i8"), ("dk0", "<i8")])
 
@@ -34,12 +36,13 @@ class PlanFile:
         self._b = raw
         self._p = 8
         (self.nint, self.n, self.nchol, self.total_csfs, self.npair_all, self.nD, ndh, nbuf, ninit, nsig, nh,
-         nwv, self.np, self.nm) = self._i(14)
+         nwv, self.np, self.nm, ndiag) = self._i(15)
         self.buf_size = self._i(nbuf)
         self.dheads = self._arr(DH, ndh)
         self.dk_sign = self._f(self.nD)
         self.h_vv = self._f(nh)
         self.wv = self._f(nwv)
+        self.diag = self._arr(DG, ndiag)
         self.init_steps = [self._step() for _ in range(ninit)]
         self.sigma_steps = [self._step() for _ in range(nsig)]
 
