@@ -932,18 +932,22 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
           num_vec = (int)nroots;
           V.assign((size_t)num_vec * num_vec, 0.0);
           for (int q = 0; q < nroots; ++q) V[(size_t)q * num_vec + q] = 1.0;
+          w.resize(num_vec);
         }
+        // the Ritz vectors live in the subspace of this iteration (subspace_size in
+        // davidson.f90:140); vectors appended below for earlier roots are not part of it
+        const int subspace_size = num_vec;
         for (int q = 0; q < nroots; ++q) {
           if (conv[q]) continue;
           // residual r = sum_k a_k (Hc_k - E c_k)
-          std::vector<double> ca(num_vec), cb(num_vec);
-          for (int k = 0; k < num_vec; ++k) {
-            cb[k] = V[(size_t)k * num_vec + q];
+          std::vector<double> ca(subspace_size), cb(subspace_size);
+          for (int k = 0; k < subspace_size; ++k) {
+            cb[k] = V[(size_t)k * subspace_size + q];
             ca[k] = -energy[q] * cb[k];
           }
-          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, ca.data(), num_vec * sizeof(double), cudaMemcpyHostToDevice, st));
-          TCI_CUDA(cudaMemcpyAsync(ctx->coefs + cap, cb.data(), num_vec * sizeof(double), cudaMemcpyHostToDevice, st));
-          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, HCs, ctx->coefs + cap, num_vec, n, n);
+          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, ca.data(), subspace_size * sizeof(double), cudaMemcpyHostToDevice, st));
+          TCI_CUDA(cudaMemcpyAsync(ctx->coefs + cap, cb.data(), subspace_size * sizeof(double), cudaMemcpyHostToDevice, st));
+          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, HCs, ctx->coefs + cap, subspace_size, n, n);
           TCI_CUDA(cudaGetLastError());
           double nrm2 = 0.0;
           ctx->multi_dot(r, 0, 1, r, n, &nrm2);
@@ -982,11 +986,12 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
       for (int q = 0; q < nroots; ++q) energies[q] = energy[q];
       if (iterations) *iterations = std::min<i64>(it, maxit);
       if (vectors) {
+        const int m = (int)w.size();  // dimension of the last subspace eigensolve
         for (int q = 0; q < nroots; ++q) {
-          std::vector<double> cb(num_vec);
-          for (int k = 0; k < num_vec; ++k) cb[k] = V[(size_t)k * num_vec + q];
-          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, cb.data(), num_vec * sizeof(double), cudaMemcpyHostToDevice, st));
-          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, nullptr, nullptr, num_vec, n, n);
+          std::vector<double> cb(m);
+          for (int k = 0; k < m; ++k) cb[k] = V[(size_t)k * m + q];
+          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, cb.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
+          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, nullptr, nullptr, m, n, n);
           double nrm2 = 0.0;
           ctx->multi_dot(r, 0, 1, r, n, &nrm2);
           std::vector<double> hv(n);
