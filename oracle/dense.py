@@ -186,6 +186,14 @@ def use_blas():
             fn = getattr(ob, "scipy_dgemm_")
         except (OSError, AttributeError):
             continue
+        # one BLAS thread per call: the oracle already runs one OpenMP thread per outer index
+        try:
+            ob.scipy_openblas_set_num_threads64_(1)
+        except AttributeError:
+            for name in ("openblas_set_num_threads", "scipy_openblas_set_num_threads"):
+                if hasattr(ob, name):
+                    getattr(ob, name)(1)
+                    break
         lib().oracle_set_dgemm(C.cast(fn, C.c_void_p))
         return True
     return False

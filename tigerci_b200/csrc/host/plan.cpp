@@ -543,21 +543,40 @@ void Builder::ds() {
     }
   }
 
-  // ---- device steps for the three-external term
+  // ---- device steps for the three-external term (V_i stored [b][(q,s)])
   if (!t3.empty()) {
-    const i64 Y = T.alloc(nint * P.nD * n);  // Y[i][dk][b] = sum_{q,s} D[dk][q][s] V_i[q][b][s]
-    Step& g = step(P.sigma_steps, STEP_GEMM, "three-external forward");
+    const i64 Y = T.alloc(nint * P.nD * n);  // Y[i][dk][b] = sum_{(q,s)} D[dk][(q,s)] V_i[b][(q,s)]
     std::vector<char> used(nint, 0);
     for (auto& t : t3) used[t.i] = 1;
-    for (i64 i = 0; i < nint; ++i) {
-      if (!used[i]) continue;
-      GemmProblem gp{BUF_T0, Y + i * P.nD * n, n, P.nD, n, 0.0, (i64)g.gs.size(), 0};
-      for (i64 q = 0; q < n; ++q)  // D[:, q, :] (nD x n, ld n^2) * V_i[q]^T (n x n)
-        g.gs.push_back(GemmSeg{BUF_D, BUF_V, q * n, n2, (i * n + q) * n2, n, n, 0, 1, 1.0});
-      gp.seg_end = (i64)g.gs.size();
-      g.gp.push_back(gp);
-      P.flops_total += 2.0 * P.nD * n * n2;
+    std::vector<std::pair<i64, i64>> outs;  // (offset into T0 of Y_i, i)
+    for (i64 i = 0; i < nint; ++i)
+      if (used[i]) outs.push_back({Y + i * P.nD * n, i});
+    // split-K over (q,s): the output is only nD x n, the contraction n^2 long
+    const i64 S = std::max<i64>(1, std::min<i64>(32, n2 / 2048));
+    const i64 kc = (n2 + S - 1) / S;
+    const i64 Pt = T.alloc(S * (i64)outs.size() * P.nD * n);
+    Step g = mkstep(STEP_GEMM, "three-external forward");
+    for (size_t o = 0; o < outs.size(); ++o)
+      for (i64 sidx = 0; sidx < S; ++sidx) {
+        const i64 k0 = sidx * kc, kl = std::min(kc, n2 - k0);
+        if (kl <= 0) continue;
+        GemmProblem gp{BUF_T0, Pt + ((i64)o * S + sidx) * P.nD * n, n, P.nD, n, 0.0, (i64)g.gs.size(), 0};
+        g.gs.push_back(GemmSeg{BUF_D, BUF_V, k0, n2, outs[o].second * n * n2 + k0, n2, kl, 0, 1, 1.0});
+        gp.seg_end = (i64)g.gs.size();
+        g.gp.push_back(gp);
+      }
+    P.sigma_steps.push_back(std::move(g));
+    Step red = mkstep(STEP_AXPY, "three-external split-k sum");
+    for (size_t o = 0; o < outs.size(); ++o) {
+      AxpyTarget tg{BUF_T0, outs[o].first, P.nD * n, (i64)red.as.size(), 0};
+      for (i64 sidx = 0; sidx < S; ++sidx)
+        if (sidx * kc < n2) red.as.push_back(AxpySource{BUF_T0, Pt + ((i64)o * S + sidx) * P.nD * n, 1.0, -1, 0});
+      tg.src_end = (i64)red.as.size();
+      red.at.push_back(tg);
     }
+    zero_step(P.sigma_steps, BUF_T0, Y, nint * P.nD * n, "three-external zero");
+    P.sigma_steps.push_back(std::move(red));
+    P.flops_total += 2.0 * P.nD * n * n2 * (double)outs.size();
     Step& sc = step(P.sigma_steps, STEP_AXPY, "three-external scatter");
     std::map<i64, std::vector<const T3*>> by_mu;
     for (auto& t : t3) by_mu[t.mu_row].push_back(&t);
@@ -567,7 +586,7 @@ void Builder::ds() {
       tg.src_end = (i64)sc.as.size();
       sc.at.push_back(tg);
     }
-    // reverse: U[i][dk] = sum a c_mu ; R[dk][q][:] += sum_i U[i][dk] V_i[q]
+    // reverse: U[i][dk][b] = sum a c_mu ; R[dk][(q,s)] += sum_i U[i][dk][b] V_i[b][(q,s)]
     const i64 U = T.alloc(nint * P.nD * n);
     zero_step(P.sigma_steps, BUF_T0, U, nint * P.nD * n, "three-external reverse zero");
     Step& ga = step(P.sigma_steps, STEP_AXPY, "three-external reverse gather");
@@ -580,13 +599,11 @@ void Builder::ds() {
       ga.at.push_back(tg);
     }
     Step& gr = step(P.sigma_steps, STEP_GEMM, "three-external reverse");
-    for (i64 q = 0; q < n; ++q) {
-      GemmProblem gp{BUF_R, q * n, n2, P.nD, n, 1.0, (i64)gr.gs.size(), 0};
-      for (i64 i = 0; i < nint; ++i)
-        if (used[i]) gr.gs.push_back(GemmSeg{BUF_T0, BUF_V, U + i * P.nD * n, n, (i * n + q) * n2, n, n, 0, 0, 1.0});
-      gp.seg_end = (i64)gr.gs.size();
-      if (gp.seg_end > gp.seg_begin) gr.gp.push_back(gp);
-    }
+    GemmProblem gp{BUF_R, 0, n2, P.nD, n2, 1.0, (i64)gr.gs.size(), 0};
+    for (i64 i = 0; i < nint; ++i)
+      if (used[i]) gr.gs.push_back(GemmSeg{BUF_T0, BUF_V, U + i * P.nD * n, n, i * n * n2, n2, n, 0, 0, 1.0});
+    gp.seg_end = (i64)gr.gs.size();
+    if (gp.seg_end > gp.seg_begin) gr.gp.push_back(gp);
     for (i64 i = 0; i < nint; ++i)
       if (used[i]) P.flops_total += 2.0 * P.nD * n * n2;
   }
@@ -685,12 +702,26 @@ void Builder::dv() {
   if (tv.empty()) return;
   const i64 nk = nint * nint;
   const i64 F2 = T.alloc(nk * P.nD), G2 = T.alloc(nk * P.nD);
-  Step& g = step(P.sigma_steps, STEP_GEMM, "dv forward");
-  {  // F2 (nk x nD) = Kbank (nk x n^2) * D^T
-    GemmProblem gp{BUF_T0, F2, P.nD, nk, P.nD, 0.0, (i64)g.gs.size(), 0};
-    g.gs.push_back(GemmSeg{BUF_JK, BUF_D, offK, n2, 0, n2, n2, 0, 1, 1.0});
-    gp.seg_end = (i64)g.gs.size();
-    g.gp.push_back(gp);
+  zero_step(P.sigma_steps, BUF_T0, F2, nk * P.nD, "dv forward zero");
+  {  // F2 (nk x nD) = Kbank (nk x n^2) * D^T, split over the n^2 contraction
+    const i64 S = std::max<i64>(1, std::min<i64>(64, n2 / 1024));
+    const i64 kc = (n2 + S - 1) / S;
+    const i64 Pt = T.alloc(S * nk * P.nD);
+    Step& g = step(P.sigma_steps, STEP_GEMM, "dv forward");
+    for (i64 sidx = 0; sidx < S; ++sidx) {
+      const i64 k0 = sidx * kc, kl = std::min(kc, n2 - k0);
+      if (kl <= 0) continue;
+      GemmProblem gp{BUF_T0, Pt + sidx * nk * P.nD, P.nD, nk, P.nD, 0.0, (i64)g.gs.size(), 0};
+      g.gs.push_back(GemmSeg{BUF_JK, BUF_D, offK + k0, n2, k0, n2, kl, 0, 1, 1.0});
+      gp.seg_end = (i64)g.gs.size();
+      g.gp.push_back(gp);
+    }
+    Step& red = step(P.sigma_steps, STEP_AXPY, "dv split-k sum");
+    AxpyTarget tg{BUF_T0, F2, nk * P.nD, 0, 0};
+    for (i64 sidx = 0; sidx < S; ++sidx)
+      if (sidx * kc < n2) red.as.push_back(AxpySource{BUF_T0, Pt + sidx * nk * P.nD, 1.0, -1, 0});
+    tg.src_end = (i64)red.as.size();
+    red.at.push_back(tg);
     P.flops_total += 2.0 * nk * P.nD * n2;
   }
   Step& sc = step(P.sigma_steps, STEP_AXPY, "dv scatter");
@@ -1044,12 +1075,13 @@ void Builder::init_steps() {
       gp.seg_end = (i64)gb.gs.size();
       gb.gp.push_back(gp);
     }
-  for (i64 i = 0; i < nint; ++i) {  // V_i[q][(b,s)] = LE[i] (n x N) * LV^T (N x n^2)
-    GemmProblem gp{BUF_V, i * n * n2, n2, n, n2, 0.0, (i64)gb.gs.size(), 0};
-    gb.gs.push_back(GemmSeg{BUF_LE, BUF_LV, i * n * N, N, 0, N, N, 0, 1, 1.0});
-    gp.seg_end = (i64)gb.gs.size();
-    gb.gp.push_back(gp);
-  }
+  for (i64 i = 0; i < nint; ++i)  // V_i[b][q][s] = (iq|bs) = LE[i] (n x N) * LV[b rows]^T (N x n)
+    for (i64 b = 0; b < n; ++b) {
+      GemmProblem gp{BUF_V, (i * n + b) * n2, n, n, n, 0.0, (i64)gb.gs.size(), 0};
+      gb.gs.push_back(GemmSeg{BUF_LE, BUF_LV, i * n * N, N, b * n * N, N, N, 0, 1, 1.0});
+      gp.seg_end = (i64)gb.gs.size();
+      gb.gp.push_back(gp);
+    }
   {  // X = Lpk Lpk^T
     GemmProblem gp{BUF_X, 0, npk, npk, npk, 0.0, (i64)gb.gs.size(), 0};
     gb.gs.push_back(GemmSeg{BUF_T0, BUF_T0, Lpk_off, N, Lpk_off, N, N, 0, 1, 1.0});

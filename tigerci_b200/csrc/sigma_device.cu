@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -50,7 +51,8 @@ struct DGemmSeg {
   double alpha;
 };
 struct DAxpyTarget {
-  double* dst;
+  double* dst;             // already offset by base
+  long long base;          // offset of this chunk inside the target range (applied to sources)
   long long len, src_begin, src_end;
 };
 struct DAxpySource {
@@ -158,17 +160,140 @@ __global__ void __launch_bounds__(GTH) gemm_grouped_f64(const DGemmProblem* __re
   }
 }
 
+
+// Register-blocked FP64 GEMM: CTA tile BM x BN, k-step 16, each of the 256
+// threads owns a TM x TN block of C; the next k-tile is prefetched into
+// registers while the current one is consumed from shared memory (double
+// buffered).  Same problem/segment tables and summation order per element as
+// gemm_grouped_f64: segments in table order, k ascending within a segment.
+template <int BM, int BN, int TM, int TN>
+__global__ void __launch_bounds__(256, 2) gemm_tiled_f64(const DGemmProblem* __restrict__ probs, int nprob,
+                                                      const DGemmSeg* __restrict__ segs) {
+  constexpr int BK = 8;
+  constexpr int NTX = BN / TN;  // threads along n
+  static_assert((BM / TM) * (BN / TN) == 256, "256 threads");
+  constexpr int LA = BM * BK / 256, LB = BN * BK / 256;  // elements loaded per thread
+  __shared__ double As[2][BK][BM + 2];
+  __shared__ double Bs[2][BK][BN + 2];
+  const long long tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const DGemmProblem P = probs[lo];
+  const long long t = tile - P.tile_begin;
+  const long long m0 = (t / P.tiles_n) * BM, n0 = (t % P.tiles_n) * BN;
+  const int tid = threadIdx.x, tx = tid % NTX, ty = tid / NTX;
+  double acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0;
+  for (long long sgi = P.seg_begin; sgi < P.seg_end; ++sgi) {
+    const DGemmSeg S = segs[sgi];
+    double ra[LA], rb[LB];
+    // the segment's alpha is folded into its B operand as it is loaded
+    auto load = [&](long long k0) {
+#pragma unroll
+      for (int u = 0; u < LA; ++u) {
+        const int e = tid + u * 256;
+        int mm, kk;
+        if (S.tA) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
+        const long long gm = m0 + mm, gk = k0 + kk;
+        ra[u] = (gm < P.M && gk < S.K) ? (S.tA ? S.A[gk * S.lda + gm] : S.A[gm * S.lda + gk]) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < LB; ++u) {
+        const int e = tid + u * 256;
+        int nn, kk;
+        if (S.tB) { kk = e % BK; nn = e / BK; } else { nn = e % BN; kk = e / BN; }
+        const long long gn = n0 + nn, gk = k0 + kk;
+        rb[u] = (gn < P.N && gk < S.K) ? S.alpha * (S.tB ? S.B[gn * S.ldb + gk] : S.B[gk * S.ldb + gn]) : 0.0;
+      }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+      for (int u = 0; u < LA; ++u) {
+        const int e = tid + u * 256;
+        int mm, kk;
+        if (S.tA) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
+        As[buf][kk][mm] = ra[u];
+      }
+#pragma unroll
+      for (int u = 0; u < LB; ++u) {
+        const int e = tid + u * 256;
+        int nn, kk;
+        if (S.tB) { kk = e % BK; nn = e / BK; } else { nn = e % BN; kk = e / BN; }
+        Bs[buf][kk][nn] = rb[u];
+      }
+    };
+    __syncthreads();  // previous segment finished reading the buffers
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (long long k0 = 0; k0 < S.K; k0 += BK) {
+      const bool more = k0 + BK < S.K;
+      if (more) load(k0 + BK);
+#pragma unroll
+      for (int kk = 0; kk < BK; ++kk) {
+        double a[TM], b[TN];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) a[i] = As[buf][kk][ty + (BM / TM) * i];
+#pragma unroll
+        for (int j = 0; j < TN; ++j) b[j] = Bs[buf][kk][tx + NTX * j];
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      }
+      if (more) store(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const long long gm = m0 + ty + (BM / TM) * i;
+    if (gm >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      const long long gn = n0 + tx + NTX * j;
+      if (gn >= P.N) continue;
+      double* c = P.C + gm * P.ldc + gn;
+      *c = (P.beta == 0.0) ? acc[i][j] : fma(P.beta, *c, acc[i][j]);
+    }
+  }
+}
+
 __global__ void axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg, const DAxpySource* __restrict__ src) {
   const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (w >= ntg) return;
   const DAxpyTarget T = tg[w];
+  if (T.len < 8 && T.src_end - T.src_begin > 8) {
+    // short target, many sources: lanes stride over the sources, fixed-order warp reduction
+    for (long long i = 0; i < T.len; ++i) {
+      double acc = 0.0;
+      for (long long s = T.src_begin + lane; s < T.src_end; s += 32) {
+        const DAxpySource S = src[s];
+        const double c = S.scale ? S.coef * (*S.scale) : S.coef;
+        acc = fma(c, S.src[T.base + i], acc);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) T.dst[i] += acc;
+    }
+    return;
+  }
   for (long long i = lane; i < T.len; i += 32) {
     double acc = 0.0;
     for (long long s = T.src_begin; s < T.src_end; ++s) {
       const DAxpySource S = src[s];
       const double c = S.scale ? S.coef * (*S.scale) : S.coef;
-      acc = fma(c, S.src[i], acc);
+      acc = fma(c, S.src[T.base + i], acc);
     }
     T.dst[i] += acc;
   }
@@ -399,6 +524,7 @@ struct DevStep {
   DGemmSeg* segs = nullptr;
   int nprob = 0;
   long long ntiles = 0;
+  int cfg = 0;  // 0: 64x128 tiles, 1: 128x64 tiles
   // AXPY / DOT
   DAxpyTarget* at = nullptr;
   DAxpySource* as = nullptr;
@@ -438,6 +564,9 @@ struct tci_ctx {
   long long sigma_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool profiling = false;
+  bool use_graph = true;                // replay the sigma steps as one CUDA graph
+  cudaGraph_t graph = nullptr, graph_prof = nullptr;
+  cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
   double* dots = nullptr;        // reduction scratch: partial sums and results
   double* coefs = nullptr;       // small device coefficient arrays
@@ -446,6 +575,10 @@ struct tci_ctx {
   long long profiled_builds = 0;
 
   ~tci_ctx() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (graph_exec_prof) cudaGraphExecDestroy(graph_exec_prof);
+    if (graph_prof) cudaGraphDestroy(graph_prof);
     for (auto e : step_ev) cudaEventDestroy(e);
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
@@ -471,8 +604,16 @@ struct tci_ctx {
       std::vector<DGemmProblem> pr;
       std::vector<DGemmSeg> sg;
       long long tiles = 0;
+      // tile shape: wide in n when the problems are short in m (e.g. few CI blocks times an operator)
+      double sm = 0, sn = 0;
       for (auto& g : s.gp) {
-        const i64 tm = (g.M + GT - 1) / GT, tn = (g.N + GT - 1) / GT;
+        sm += (double)g.M;
+        sn += (double)g.N;
+      }
+      d.cfg = (sm <= sn) ? 0 : 1;
+      const i64 BMh = d.cfg == 0 ? 64 : 128, BNh = d.cfg == 0 ? 128 : 64;
+      for (auto& g : s.gp) {
+        const i64 tm = (g.M + BMh - 1) / BMh, tn = (g.N + BNh - 1) / BNh;
         if (g.M <= 0 || g.N <= 0) continue;
         check_range(g.c, g.offC, (g.M - 1) * g.ldc + g.N);
         pr.push_back(DGemmProblem{ptr(g.c, g.offC), g.ldc, g.M, g.N, tn, tiles, g.beta, g.seg_begin, g.seg_end});
@@ -499,9 +640,11 @@ struct tci_ctx {
     } else if (s.kind == STEP_AXPY) {
       std::vector<DAxpyTarget> t;
       std::vector<DAxpySource> so;
+      constexpr i64 kChunk = 1024;  // elements per warp: long rows are spread over many warps
       for (auto& x : s.at) {
         check_range(x.dst, x.off, x.len);
-        t.push_back(DAxpyTarget{ptr(x.dst, x.off), x.len, x.src_begin, x.src_end});
+        for (i64 b = 0; b < x.len; b += kChunk)
+          t.push_back(DAxpyTarget{ptr(x.dst, x.off) + b, b, std::min(kChunk, x.len - b), x.src_begin, x.src_end});
       }
       for (auto& x : s.as) {
         // source length equals its target's length; the offset is checked against the buffer
@@ -581,16 +724,46 @@ struct tci_ctx {
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     sigma_count++;
   }
-  void run_sigma_steps() {
-    if (profiling && step_ev.size() != 2 * sigma.size()) {
+  void ensure_step_events() {
+    if (step_ev.size() != 2 * sigma.size()) {
       step_ev.resize(2 * sigma.size());
       for (auto& e : step_ev) TCI_CUDA(cudaEventCreate(&e));
       step_ms.assign(sigma.size(), 0.0);
     }
+  }
+
+  void record_steps(bool with_events) {
     for (size_t i = 0; i < sigma.size(); ++i) {
-      if (profiling) TCI_CUDA(cudaEventRecord(step_ev[2 * i], stream));
+      if (with_events) TCI_CUDA(cudaEventRecord(step_ev[2 * i], stream));
       run(sigma[i]);
-      if (profiling) TCI_CUDA(cudaEventRecord(step_ev[2 * i + 1], stream));
+      if (with_events) TCI_CUDA(cudaEventRecord(step_ev[2 * i + 1], stream));
+    }
+  }
+
+  // One sigma build.  With graphs on, the step sequence is captured once (a
+  // second capture carries an event-record node around every step for the
+  // profiler) and replayed with a single launch.
+  void run_sigma_steps() {
+    if (profiling) ensure_step_events();
+    if (use_graph) {
+      cudaGraph_t& g = profiling ? graph_prof : graph;
+      cudaGraphExec_t& ge = profiling ? graph_exec_prof : graph_exec;
+      if (!ge) {
+        TCI_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          record_steps(profiling);
+        } catch (...) {
+          cudaGraph_t tmp = nullptr;
+          cudaStreamEndCapture(stream, &tmp);
+          if (tmp) cudaGraphDestroy(tmp);
+          throw;
+        }
+        TCI_CUDA(cudaStreamEndCapture(stream, &g));
+        TCI_CUDA(cudaGraphInstantiate(&ge, g, 0));
+      }
+      TCI_CUDA(cudaGraphLaunch(ge, stream));
+    } else {
+      record_steps(profiling);
     }
     if (profiling) {
       TCI_CUDA(cudaStreamSynchronize(stream));
@@ -611,7 +784,10 @@ struct tci_ctx {
   void run(const DevStep& s) {
     switch (s.kind) {
       case STEP_GEMM:
-        if (s.ntiles > 0) gemm_grouped_f64<<<(unsigned)s.ntiles, GTH, 0, stream>>>(s.probs, s.nprob, s.segs);
+        if (s.ntiles > 0) {
+          if (s.cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
+          else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
+        }
         break;
       case STEP_AXPY:
         if (s.ntg > 0) axpy_segments<<<(unsigned)((s.ntg + 7) / 8), 256, 0, stream>>>(s.at, s.ntg, s.as);
@@ -699,6 +875,7 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
         ctx->buf[b] = nullptr;
       }
     }
+    if (const char* g = std::getenv("TCI_NO_GRAPH")) ctx->use_graph = (g[0] == '0');
     ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = ctx.release();
     return TCI_OK;
