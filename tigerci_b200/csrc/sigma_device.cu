@@ -732,11 +732,14 @@ struct tci_ctx {
     }
   }
 
-  void record_steps(bool with_events) {
+  void record_steps(bool with_events, bool capturing) {
+    // inside a stream capture an event record becomes a graph node only when
+    // it is marked external
+    const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     for (size_t i = 0; i < sigma.size(); ++i) {
-      if (with_events) TCI_CUDA(cudaEventRecord(step_ev[2 * i], stream));
+      if (with_events) TCI_CUDA(cudaEventRecordWithFlags(step_ev[2 * i], stream, fl));
       run(sigma[i]);
-      if (with_events) TCI_CUDA(cudaEventRecord(step_ev[2 * i + 1], stream));
+      if (with_events) TCI_CUDA(cudaEventRecordWithFlags(step_ev[2 * i + 1], stream, fl));
     }
   }
 
@@ -751,7 +754,7 @@ struct tci_ctx {
       if (!ge) {
         TCI_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         try {
-          record_steps(profiling);
+          record_steps(profiling, true);
         } catch (...) {
           cudaGraph_t tmp = nullptr;
           cudaStreamEndCapture(stream, &tmp);
@@ -763,7 +766,7 @@ struct tci_ctx {
       }
       TCI_CUDA(cudaGraphLaunch(ge, stream));
     } else {
-      record_steps(profiling);
+      record_steps(profiling, false);
     }
     if (profiling) {
       TCI_CUDA(cudaStreamSynchronize(stream));
