@@ -102,9 +102,18 @@ void tci_plan_destroy(tci_plan* plan);
  * tci_sigma_init uploads the operator, builds the integral banks and the plan on
  * `device`.  tci_sigma accumulates sigma += H c exactly like htimesc (the caller
  * zeroes sigma, tiger_fortran/davidson.f90:126); c and sigma are host arrays of
- * length total_csfs.  tci_sigma_device does the same on device arrays on the
- * given cudaStream_t (NULL = the context's stream). */
+ * length total_csfs.  tci_sigma_device does the same on device arrays, ordered
+ * after prior work on the given cudaStream_t and before later work on it
+ * (NULL = the legacy default stream). */
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out);
+/* As tci_sigma_init with options: options[0] = precision mode, 0 plain FP64
+ * (default), 1 the all-external term on tcgen05 tensor cores with FP32 W
+ * operators, 3xTF32 split products and FP64 promotion every 1024 k
+ * (TCI_PRECISION_TF32X3); every other term stays FP64. */
+#define TCI_PRECISION_FP64 0
+#define TCI_PRECISION_TF32X3 1
+int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
+                      int64_t n_options, tci_ctx** out);
 int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n);
 int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n, void* stream);
 /* Diagonal H_ii (tiger_fortran/diag_element_mod_2.f90:83) for the
@@ -127,6 +136,9 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len);
  * every sigma build records an event pair around each plan step on the
  * context's stream; tci_step_times returns the accumulated milliseconds per
  * step and the number of profiled builds since tci_profile was called. */
+/* Waits for the context's stream and reports a device-side failure recorded
+ * by a bounded wait (TCI_ERR_TIMEOUT), else 0. */
+int tci_check(tci_ctx* ctx);
 int tci_profile(tci_ctx* ctx, int64_t on);
 int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps, int64_t* nbuilds);
 int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len);

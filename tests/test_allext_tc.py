@@ -1,0 +1,52 @@
+"""Mixed-precision all-external product on tcgen05 (3xTF32 with FP64 block
+promotion) against the plain-FP64 sigma build."""
+import numpy as np
+import pytest
+
+import tigerci_b200 as T
+from cases import SMALL_CASES, case_id, product_deck
+from tigerci_b200.synthetic import random_civec, synthetic_operator
+
+pytestmark = pytest.mark.gpu
+
+# The mixed form only changes the all-external product: FP32 storage of W
+# (2^-24) and split TF32 products (~2^-22) bound its relative error.
+MIXED_RTOL = 2e-6
+
+
+def _pair(deck, h, L):
+    a = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="fp64")
+    b = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="tf32x3")
+    return a, b
+
+
+@pytest.mark.parametrize("c", [SMALL_CASES[2], SMALL_CASES[3], SMALL_CASES[8]], ids=case_id)
+def test_mixed_small_cases(c, need_gpu):
+    h, L = synthetic_operator(c["no"], 10, seed=11, scale=0.3, diag_range=(-3, 1), offdiag_sigma=0.1)
+    a, b = _pair(product_deck(c), h, L)
+    x = random_civec(a.n, 1)
+    sa, sb = a.sigma(x), b.sigma(x)
+    b.check()
+    assert np.abs(sa - sb).max() <= MIXED_RTOL * np.abs(sa).max()
+
+
+def test_mixed_medium_case_and_determinism(need_gpu):
+    # 60 externals: W+ is 1830 x 1830 (15 row tiles, partial last tile, 2 promotion blocks)
+    deck = T.Deck(16 + 60, 8, 8, 16, 1, ["2" * 8 + "0" * 8])
+    h, L = synthetic_operator(76, 200, seed=1234)
+    a, b = _pair(deck, h, L)
+    x = random_civec(a.n, 3)
+    sa, sb = a.sigma(x), b.sigma(x)
+    b.check()
+    assert np.abs(sa - sb).max() <= MIXED_RTOL * np.abs(sa).max()
+    assert np.array_equal(sb, b.sigma(x))
+
+
+def test_mixed_davidson_energy_within_one_microhartree(need_gpu):
+    deck = T.Deck(16 + 60, 8, 8, 16, 1, ["2" * 8 + "0" * 8])
+    h, L = synthetic_operator(76, 200, seed=1234)
+    a, b = _pair(deck, h, L)
+    ea, _, _ = a.davidson(2, 1e-6, 1e-10)
+    eb, _, _ = b.davidson(2, 1e-6, 1e-10)
+    b.check()
+    assert np.abs(ea - eb).max() < 1e-6

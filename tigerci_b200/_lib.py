@@ -31,6 +31,8 @@ EXPORTS = [
     "tci_plan_stats",
     "tci_plan_destroy",
     "tci_sigma_init",
+    "tci_sigma_init_ex",
+    "tci_check",
     "tci_sigma",
     "tci_sigma_device",
     "tci_diag",
@@ -95,6 +97,8 @@ def lib():
         L.tci_plan_destroy.argtypes = [P]
         L.tci_plan_destroy.restype = None
         L.tci_sigma_init.argtypes = [C.POINTER(TciDeck), C.POINTER(TciOperator), i64, C.POINTER(P)]
+        L.tci_sigma_init_ex.argtypes = [C.POINTER(TciDeck), C.POINTER(TciOperator), i64, P, i64, C.POINTER(P)]
+        L.tci_check.argtypes = [P]
         L.tci_sigma.argtypes = [P, P, P, i64]
         L.tci_sigma_device.argtypes = [P, P, P, i64, P]
         L.tci_diag.argtypes = [P, P, i64]

@@ -157,12 +157,16 @@ class Plan:
 class SigmaBuilder:
     """Device-resident sigma = H c on one GPU (the htimesc slot)."""
 
-    def __init__(self, deck: Deck, op: Operator, device: int = 0):
+    PRECISIONS = {"fp64": 0, "tf32x3": 1}
+
+    def __init__(self, deck: Deck, op: Operator, device: int = 0, precision: str = "fp64"):
         self._d = deck.c_struct()
         self._o = op.c_struct()
         self._op = op
+        self.precision = precision
         h = C.c_void_p()
-        check(lib().tci_sigma_init(C.byref(self._d), C.byref(self._o), device, C.byref(h)))
+        opts = np.array([self.PRECISIONS[precision]], dtype=np.int64)
+        check(lib().tci_sigma_init_ex(C.byref(self._d), C.byref(self._o), device, ptr(opts), 1, C.byref(h)))
         self._h = h
         self.n = int(self.stats()["total_csfs"])
 
@@ -186,6 +190,10 @@ class SigmaBuilder:
         s = np.zeros_like(civec, dtype=np.float64)
         self.htimesc(np.ascontiguousarray(civec, dtype=np.float64), s)
         return s
+
+    def check(self):
+        """Synchronise and raise if a bounded device wait gave up."""
+        check(lib().tci_check(self._h))
 
     def htimesc_device(self, c_ptr: int, s_ptr: int, n: int, stream: int = 0):
         """Device pointers (e.g. torch tensors' data_ptr()) on `stream`."""

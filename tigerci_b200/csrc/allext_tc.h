@@ -1,0 +1,26 @@
+// Host interface of the tcgen05 all-external product (allext_tc.cu).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+namespace tci_tc_host {
+
+struct AllextTc {
+  CUtensorMap wmap, uhi, ulo;  // W (np x np, fp32), U hi / lo (padded rows x np, fp32)
+  int64_t np = 0, m = 0;
+  double* y = nullptr;         // m x np FP64 output (overwritten)
+  int* status = nullptr;       // device status word (0 ok, else a bounded wait gave up)
+};
+
+int64_t padded_ld(int64_t np);   // fp32 row pitch (multiple of 32 elements)
+int64_t padded_rows(int64_t m);  // rows of the split U (multiple of 64)
+cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st);
+cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo, cudaStream_t st);
+bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
+             int* status, std::string& err);
+cudaError_t launch(const AllextTc& t, cudaStream_t st);
+
+}  // namespace tci_tc_host

@@ -948,6 +948,10 @@ void Builder::allext() {
   P.n_trip = (i64)trip.size();
   const i64 Us = T.alloc(std::max<i64>(1, P.n_sing) * np), Ys = T.alloc(std::max<i64>(1, P.n_sing) * np);
   const i64 Ut = T.alloc(std::max<i64>(1, P.n_trip) * nm), Yt = T.alloc(std::max<i64>(1, P.n_trip) * nm);
+  P.allext_us = Us;
+  P.allext_ys = Ys;
+  P.allext_ut = Ut;
+  P.allext_yt = Yt;
   zero_step(P.sigma_steps, BUF_T0, Us, P.n_sing * np, "all-external gather zero");
   zero_step(P.sigma_steps, BUF_T0, Ut, P.n_trip * nm, "all-external gather zero");
   Step& ga = step(P.sigma_steps, STEP_AXPY, "all-external gather");
@@ -968,20 +972,39 @@ void Builder::allext() {
     const i64 k = trip[r].second;
     if (nab > 0) gather(Ut + r * nm, nab, d.off_ab + k * nab);
   }
-  Step& g = step(P.sigma_steps, STEP_GEMM, "all-external");
+  // FP64 form: Y = U W with the contraction split in S slices (the product has
+  // few output tiles and a very long k); the slices are summed in order.
   const i64 offWm = np * np;
-  if (P.n_sing > 0) {
-    GemmProblem gp{BUF_T0, Ys, np, P.n_sing, np, 0.0, (i64)g.gs.size(), 0};
-    g.gs.push_back(GemmSeg{BUF_T0, BUF_W, Us, np, 0, np, np, 0, 0, 1.0});
-    gp.seg_end = (i64)g.gs.size();
-    g.gp.push_back(gp);
-  }
-  if (P.n_trip > 0 && nm > 0) {
-    GemmProblem gp{BUF_T0, Yt, nm, P.n_trip, nm, 0.0, (i64)g.gs.size(), 0};
-    g.gs.push_back(GemmSeg{BUF_T0, BUF_W, Ut, nm, offWm, nm, nm, 0, 0, 1.0});
-    gp.seg_end = (i64)g.gs.size();
-    g.gp.push_back(gp);
-  }
+  const i64 S = std::max<i64>(1, std::min<i64>(8, np / 2048));
+  const i64 Ps = T.alloc(S * std::max<i64>(1, P.n_sing) * np), Pt = T.alloc(S * std::max<i64>(1, P.n_trip) * nm);
+  Step& g = step(P.sigma_steps, STEP_GEMM, "all-external");
+  auto add_split = [&](i64 m, i64 dim, i64 U, i64 woff, i64 part) {
+    const i64 kc = (dim + S - 1) / S;
+    for (i64 sidx = 0; sidx < S; ++sidx) {
+      const i64 k0 = sidx * kc, kl = std::min(kc, dim - k0);
+      if (kl <= 0) continue;
+      GemmProblem gp{BUF_T0, part + sidx * m * dim, dim, m, dim, 0.0, (i64)g.gs.size(), 0};
+      g.gs.push_back(GemmSeg{BUF_T0, BUF_W, U + k0, dim, woff + k0 * dim, dim, kl, 0, 0, 1.0});
+      gp.seg_end = (i64)g.gs.size();
+      g.gp.push_back(gp);
+    }
+  };
+  if (P.n_sing > 0) add_split(P.n_sing, np, Us, 0, Ps);
+  if (P.n_trip > 0 && nm > 0) add_split(P.n_trip, nm, Ut, offWm, Pt);
+  Step red = mkstep(STEP_AXPY, "all-external split-k sum");
+  auto add_sum = [&](i64 m, i64 dim, i64 Y, i64 part) {
+    const i64 kc = (dim + S - 1) / S;
+    AxpyTarget tg{BUF_T0, Y, m * dim, (i64)red.as.size(), 0};
+    for (i64 sidx = 0; sidx < S; ++sidx)
+      if (sidx * kc < dim) red.as.push_back(AxpySource{BUF_T0, part + sidx * m * dim, 1.0, -1, 0});
+    tg.src_end = (i64)red.as.size();
+    red.at.push_back(tg);
+  };
+  zero_step(P.sigma_steps, BUF_T0, Ys, std::max<i64>(1, P.n_sing) * np, "all-external zero");
+  zero_step(P.sigma_steps, BUF_T0, Yt, std::max<i64>(1, P.n_trip) * nm, "all-external zero");
+  if (P.n_sing > 0) add_sum(P.n_sing, np, Ys, Ps);
+  if (P.n_trip > 0 && nm > 0) add_sum(P.n_trip, nm, Yt, Pt);
+  P.sigma_steps.push_back(std::move(red));
   P.flops_allext = 2.0 * (double)np * np * P.n_sing + 2.0 * (double)nm * nm * P.n_trip;
   P.bytes_allext = 8.0 * ((double)np * np + (P.n_trip > 0 ? (double)nm * nm : 0.0)) +
                    16.0 * ((double)P.n_sing * np + (double)P.n_trip * nm);

@@ -131,6 +131,7 @@ struct Plan {
   double flops_allext = 0, flops_total = 0, bytes_allext = 0;
   i64 np = 0, nm = 0;            // packed pair dimensions of W+ / W-
   i64 n_sing = 0, n_trip = 0;    // dense matrices per coupling type
+  i64 allext_us = -1, allext_ys = -1, allext_ut = -1, allext_yt = -1;  // BUF_T0 offsets of U+/Y+/U-/Y-
 };
 
 struct Operator {

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/tigerci_sigma.h"
+#include "allext_tc.h"
 #include "host/capi_internal.h"
 #include "host/plan.h"
 
@@ -565,6 +566,13 @@ struct tci_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool profiling = false;
   bool use_graph = true;                // replay the sigma steps as one CUDA graph
+  int64_t precision = 0;                // 0 plain FP64; 1 all-external on tcgen05 (3xTF32, FP64 promotion)
+  float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
+  float* w32m = nullptr;
+  float* uhi = nullptr;                 // split CI blocks for the tensor-core product
+  float* ulo = nullptr;
+  int* tc_status = nullptr;
+  tci_tc_host::AllextTc tc_sing, tc_trip;
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
   cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
@@ -779,14 +787,71 @@ struct tci_ctx {
     }
   }
 
+  void run_allext_tc() {
+    if (plan.n_sing > 0) {
+      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_us, plan.n_sing, plan.np, uhi, ulo, stream));
+      TCI_CUDA(tci_tc_host::launch(tc_sing, stream));
+    }
+    if (plan.n_trip > 0 && plan.nm > 0) {
+      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, uhi, ulo, stream));
+      TCI_CUDA(tci_tc_host::launch(tc_trip, stream));
+    }
+  }
+
+  // Moves W+/W- to FP32 for the tensor-core product and releases the FP64 copy.
+  void setup_precision() {
+    if (precision != 1) return;
+    ensure_diag();  // the diagonal reads the FP64 W
+    const i64 np = plan.np, nm = plan.nm;
+    auto alloc_f = [&](float** p, size_t n) {
+      if (cudaMalloc(p, n * sizeof(float)) != cudaSuccess) throw Error(TCI_ERR_MEMORY, "device allocation failed (fp32 operators)");
+      owned.push_back(*p);
+      bytes_held += (double)n * sizeof(float);
+    };
+    alloc_f(&w32p, (size_t)np * tci_tc_host::padded_ld(np));
+    if (nm > 0) alloc_f(&w32m, (size_t)nm * tci_tc_host::padded_ld(nm));
+    const i64 mrows = tci_tc_host::padded_rows(std::max<i64>(1, std::max(plan.n_sing, plan.n_trip)));
+    alloc_f(&uhi, (size_t)mrows * tci_tc_host::padded_ld(np));
+    alloc_f(&ulo, (size_t)mrows * tci_tc_host::padded_ld(np));
+    TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
+    owned.push_back(tc_status);
+    TCI_CUDA(cudaMemsetAsync(tc_status, 0, sizeof(int), stream));
+    TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
+    if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
+    TCI_CUDA(cudaStreamSynchronize(stream));
+    std::string err;
+    if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, uhi, ulo, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, err))
+      throw Error(TCI_ERR_CUDA, err);
+    if (plan.n_trip > 0 && nm > 0 &&
+        !tci_tc_host::prepare(tc_trip, w32m, nm, uhi, ulo, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, err))
+      throw Error(TCI_ERR_CUDA, err);
+    TCI_CUDA(cudaFree(buf[BUF_W]));
+    bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
+    buf[BUF_W] = nullptr;
+  }
+
+  // Status word of the bounded waits inside the tensor-core kernel.
+  void check_tc_status() {
+    if (!tc_status) return;
+    int st = 0;
+    TCI_CUDA(cudaMemcpy(&st, tc_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0) throw Error(TCI_ERR_TIMEOUT, "tensor-core all-external kernel: a bounded wait gave up (code " + std::to_string(st) + ")");
+  }
+
   void check_range(int b, i64 off, i64 len) const {
     if (b < 0 || b >= NUM_BUFS || off < 0 || len < 0 || off + len > plan.buf_size[b])
       throw Error(TCI_ERR_INTERNAL, "plan range outside its buffer");
   }
 
   void run(const DevStep& s) {
+    // the tensor-core form writes the all-external products directly
+    if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
     switch (s.kind) {
       case STEP_GEMM:
+        if (precision == 1 && s.name == "all-external") {
+          run_allext_tc();
+          break;
+        }
         if (s.ntiles > 0) {
           if (s.cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
           else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
@@ -824,7 +889,24 @@ struct tci_ctx {
 
 extern "C" {
 
+static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, tci_ctx** out);
+
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out) {
+  return init_impl(deck, op, device, 0, out);
+}
+
+int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
+                      int64_t n_options, tci_ctx** out) {
+  int64_t precision = 0;
+  if (options && n_options > 0) precision = options[0];
+  if (precision < 0 || precision > 1) {
+    set_error("unknown precision mode");
+    return TCI_ERR_ARG;
+  }
+  return init_impl(deck, op, device, precision, out);
+}
+
+static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, tci_ctx** out) {
   if (!out) return TCI_ERR_ARG;
   *out = nullptr;
   try {
@@ -879,6 +961,8 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
       }
     }
     if (const char* g = std::getenv("TCI_NO_GRAPH")) ctx->use_graph = (g[0] == '0');
+    ctx->precision = precision;
+    ctx->setup_precision();
     ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = ctx.release();
     return TCI_OK;
@@ -892,11 +976,10 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
   try {
     if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
     TCI_CUDA(cudaSetDevice(ctx->device));
-    cudaStream_t user = stream ? (cudaStream_t)stream : ctx->stream;
-    if (user != ctx->stream) {
-      TCI_CUDA(cudaEventRecord(ctx->ev0, user));
-      TCI_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev0, 0));
-    }
+    // NULL means the legacy default stream (what an unqualified caller and torch's default stream use)
+    cudaStream_t user = stream ? (cudaStream_t)stream : cudaStreamLegacy;
+    TCI_CUDA(cudaEventRecord(ctx->ev0, user));
+    TCI_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev0, 0));
     // the plan addresses BUF_C / BUF_S: copy in and accumulate out
     TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
@@ -906,10 +989,8 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
     // sigma += S (the caller's sigma accumulates, like htimesc)
     accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(d_sigma, ctx->buf[BUF_S], n);
     TCI_CUDA(cudaGetLastError());
-    if (user != ctx->stream) {
-      TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
-      TCI_CUDA(cudaStreamWaitEvent(user, ctx->ev1, 0));
-    }
+    TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    TCI_CUDA(cudaStreamWaitEvent(user, ctx->ev1, 0));
     ctx->sigma_count++;
     return TCI_OK;
   } catch (...) {
@@ -933,6 +1014,7 @@ int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n) {
     float ms = 0;
     TCI_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->last_sigma_ms = ms;
+    ctx->check_tc_status();
     for (int64_t i = 0; i < n; ++i) sigma[i] += tmp[i];
     ctx->sigma_count++;
     return TCI_OK;
@@ -1163,6 +1245,7 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
         for (int q = 0; q < nroots; ++q) all = all && conv[q];
         if (all) break;
       }
+      ctx->check_tc_status();
       for (int q = 0; q < nroots; ++q) energies[q] = energy[q];
       if (iterations) *iterations = std::min<i64>(it, maxit);
       if (vectors) {
@@ -1210,6 +1293,18 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   out[6] = ctx->plan.bytes_allext;
   out[7] = (double)ctx->sigma_count;
   return TCI_OK;
+}
+
+int tci_check(tci_ctx* ctx) {
+  if (!ctx) return TCI_ERR_ARG;
+  try {
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->check_tc_status();
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
 }
 
 int tci_profile(tci_ctx* ctx, int64_t on) {
