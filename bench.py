@@ -181,51 +181,66 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
     deck, op = deck_and_operator()
-    t0 = time.perf_counter()
-    sb = T.SigmaBuilder(deck, op, device=local)
-    init_s = time.perf_counter() - t0
-    n = sb.n
-    st = sb.stats()
-    rng = np.random.default_rng(7 + rank)
-    c_host = rng.standard_normal(n)
-    c_host /= np.linalg.norm(c_host)
-    c = torch.from_numpy(c_host).to(f"cuda:{local}")
-    s = torch.zeros_like(c)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-    stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
-        sb.htimesc_device(c.data_ptr(), s.data_ptr(), n, stream.cuda_stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    def timed_region(profile):
-        sb.profile(profile)
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        with ClockSampler(local) as clk:
-            torch.cuda.synchronize()
-            for i in range(args.steps):
-                flush.fill_(float(i))  # write 256 MB > L2 between timed builds
-                s.zero_()
-                evs[i][0].record(stream)
-                sb.htimesc_device(c.data_ptr(), s.data_ptr(), n, stream.cuda_stream)
-                evs[i][1].record(stream)
-            torch.cuda.synchronize()
-        prof = sb.step_times() if profile else None
-        sb.profile(False)
-        return sum(a.elapsed_time(b) for a, b in evs) / 1e3, clk, prof
+    hbm, bf16, peak_kind = measured_peaks()
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    # value: the sigma graph replayed without per-step events
-    t_total, clk, _ = timed_region(False)
-    # roofline: the same timed loop with event-record nodes around every plan step
-    t_prof, _, (steps_prof, nb) = timed_region(True)
-    if dist:
-        tt = torch.tensor([t_total], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_total = float(tt.item())
-    value = world * args.steps / t_total
-    # e2e through the C ABI with host buffers
-    pin_c = torch.from_numpy(c_host).pin_memory().numpy()
+    def measure(precision, n_steps):
+        """Warm-up, timed sigma builds (graph replay), then a profiled pass with
+        event nodes around every plan step (roofline of the all-external kernel)."""
+        t0 = time.perf_counter()
+        sb = T.SigmaBuilder(deck, op, device=local, precision=precision)
+        init_s = time.perf_counter() - t0
+        n = sb.n
+        rng = np.random.default_rng(7 + rank)
+        c_host = rng.standard_normal(n)
+        c_host /= np.linalg.norm(c_host)
+        c = torch.from_numpy(c_host).to(dev)
+        s = torch.zeros_like(c)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                sb.htimesc_device(c.data_ptr(), s.data_ptr(), n, stream.cuda_stream)
+        torch.cuda.synchronize()
+
+        def timed(profile):
+            sb.profile(profile)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n_steps)]
+            with ClockSampler(local) as clk, torch.cuda.stream(stream):
+                torch.cuda.synchronize()
+                for i in range(n_steps):
+                    flush.fill_(float(i))  # write 256 MB > L2 between timed builds
+                    s.zero_()
+                    evs[i][0].record(stream)
+                    sb.htimesc_device(c.data_ptr(), s.data_ptr(), n, stream.cuda_stream)
+                    evs[i][1].record(stream)
+                torch.cuda.synchronize()
+            prof = sb.step_times() if profile else None
+            sb.profile(False)
+            return sum(a.elapsed_time(b) for a, b in evs) / 1e3, clk, prof
+
+        if dist:
+            dist.barrier()
+        t_total, clk, _ = timed(False)
+        if dist:
+            tt = torch.tensor([t_total], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_total = float(tt.item())
+        t_prof, _, (steps_prof, nb) = timed(True)
+        sb.check()
+        sigma = s.cpu().numpy().copy()
+        st = sb.stats()
+        prof = {name: ms / max(nb, 1) for name, ms in steps_prof}
+        return dict(sb=sb, n=n, c_host=c_host, t_total=t_total, clk=clk, prof=prof, t_prof=t_prof, stats=st,
+                    init_s=init_s, sigma=sigma)
+
+    m64 = measure("fp64", args.steps)
+    sb = m64["sb"]
+    n = m64["n"]
+    value = world * args.steps / m64["t_total"]
+    # e2e through the C ABI with host buffers (H2D of c and D2H of sigma per step)
+    pin_c = torch.from_numpy(m64["c_host"]).pin_memory().numpy()
     sig = np.zeros(n)
     e2e_times = []
     for i in range(max(2, min(args.steps, 5))):
@@ -235,38 +250,67 @@ def main():
         sb.htimesc(pin_c, sig)
         e2e_times.append(time.perf_counter() - t)
     e2e = 1.0 / float(np.mean(e2e_times))
-    # roofline of the dominant step
-    hbm, bf16, peak_kind = measured_peaks()
-    prof = {name: ms / max(nb, 1) for name, ms in steps_prof}
-    dom = "all-external"  # the north-star kernel; step_ms lists every step
-    t_dom = prof[dom] / 1e3
-    if dom in prof:
-        roof = {"kernel": "gemm_grouped_f64 (all-external W+/W- product)", "bound": "hbm",
-                "achieved": st["bytes_allext"] / t_dom / 1e9, "peak": hbm, "unit": "GB/s",
-                "frac": st["bytes_allext"] / t_dom / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind}
-    else:
-        roof = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
-                "traffic": None, "peak_kind": peak_kind}
+    st = m64["stats"]
+    t_dom = m64["prof"]["all-external"] / 1e3 + m64["prof"].get("all-external split-k sum", 0.0) / 1e3
+    roof = {"kernel": "gemm_tiled_f64 split-k (all-external W+/W- product, FP64)", "bound": "hbm",
+            "achieved": st["bytes_allext"] / t_dom / 1e9, "peak": hbm, "unit": "GB/s",
+            "frac": st["bytes_allext"] / t_dom / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind}
+    # Davidson solves at the reference's default tolerances (RESIDUAL/ENERGY TOLERANCE 1e-6)
+    def solves(b, k):
+        ts, es, its = [], None, None
+        for _ in range(k):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            es, _, its = b.davidson(1, 1e-6, 1e-6)
+            ts.append(time.perf_counter() - t)
+        return 1.0 / float(np.mean(ts)), es, its
+
+    dav64 = solves(sb, 2)
+    sb.close()
+    mixed = {}
+    try:
+        mx = measure("tf32x3", args.steps)
+        sbx = mx["sb"]
+        stx = mx["stats"]
+        t_tc = mx["prof"]["all-external"] / 1e3
+        np_, nm_ = None, None
+        dav_x = solves(sbx, 2)
+        w32_bytes = stx["bytes_allext"] / 2.0  # FP32 W: half of the FP64 bytes (padding aside)
+        mixed = {"sigma_builds_per_s": world * args.steps / mx["t_total"],
+                 "ms_per_step": 1e3 * mx["t_total"] / args.steps,
+                 "sigma_rel_err_vs_fp64": float(np.abs(mx["sigma"] - m64["sigma"]).max() / np.abs(m64["sigma"]).max()),
+                 "roofline": {"kernel": "allext_tf32x3_kernel (tcgen05 kind::tf32, TMA, 3xTF32, FP64 promotion)",
+                              "bound": "hbm", "achieved": w32_bytes / t_tc / 1e9, "peak": hbm, "unit": "GB/s",
+                              "frac": w32_bytes / t_tc / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind},
+                 "davidson_solves_per_s": dav_x[0], "davidson_iterations": int(dav_x[2]),
+                 "energy": float(dav_x[1][0]), "step_ms": {k: round(v, 4) for k, v in sorted(mx["prof"].items(), key=lambda kv: -kv[1])[:8]},
+                 "init_s": mx["init_s"]}
+        sbx.close()
+    except Exception as exc:  # the FP64 line stands on its own
+        mixed = {"error": str(exc)[:300]}
     line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * m64["t_total"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded operator of the benchmark shape)",
             "config": {"workload": WORKLOAD, "total_csfs": n, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "flushed by a 256 MB write between timed builds; W operators (13.3 GB) exceed L2"},
-            "sigma_tflops": st["flops_per_sigma"] * args.steps * world / t_total / 1e12,
+            "sigma_tflops": st["flops_per_sigma"] * args.steps * world / m64["t_total"] / 1e12,
             "e2e": {"value": e2e, "unit": "builds/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
             "gpu_launches": int(st["launches_per_sigma"]) * args.steps,
             "roofline": roof,
-            "step_ms": {k: round(v, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1])},
-            "profiled_ms_per_step": 1e3 * t_prof / args.steps,
-            "init_s": init_s, "clocks": clk.summary()}
+            "davidson": {"fp64_solves_per_s": dav64[0], "fp64_iterations": int(dav64[2]), "fp64_energy": float(dav64[1][0]),
+                         "tf32x3_solves_per_s": mixed.get("davidson_solves_per_s"),
+                         "tf32x3_energy_minus_fp64": (mixed["energy"] - float(dav64[1][0])) if "energy" in mixed else None},
+            "mixed_tf32x3": mixed,
+            "step_ms": {k: round(v, 4) for k, v in sorted(m64["prof"].items(), key=lambda kv: -kv[1])},
+            "profiled_ms_per_step": 1e3 * m64["t_prof"] / args.steps,
+            "init_s": m64["init_s"], "clocks": m64["clk"].summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_sample()
         line["cpu_baseline"] = {"value": 1.0 / cb["t_sigma"], "unit": "builds/s", "cores": cb["cores"],
                                 "kind": "port", "sample": cb["sample"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sb.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

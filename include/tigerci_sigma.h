@@ -128,6 +128,13 @@ int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n);
  * vectors (nroots x total_csfs, may be NULL) the normalised eigenvectors. */
 int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
                  double* energies, double* vectors, int64_t* iterations);
+/* Batched projections for a caller-driven Davidson with device-resident vectors
+ * (expand_krylov_subspace / orthonormalize_vector, tiger_fortran/davidson.f90:478,
+ * 702): d_out[k] = sum_i d_A[k*lda + i] * d_x[i] for k < m, all device arrays,
+ * ordered on `stream` (NULL = legacy default stream).  Deterministic
+ * fixed-order reduction; scratch is owned by the context. */
+int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
+             void* stream);
 /* out[0..8]: total_csfs, device bytes held, init seconds, last sigma ms,
  * flops per sigma, all-external flops, all-external bytes, sigma builds,
  * kernel launches per sigma build (out[8] written when len >= 9) */

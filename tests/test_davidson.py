@@ -71,3 +71,26 @@ def test_contexts_do_not_share_state(need_gpu):
     assert np.array_equal(c2.sigma(x), ref)
     a.close()
     c2.close()
+
+
+@pytest.mark.gpu
+def test_projection_entry_point_matches_host_dots(need_gpu):
+    import torch
+
+    c = SMALL_CASES[8]
+    h, L = _op(c)
+    sb = T.SigmaBuilder(product_deck(c), T.Operator(h, L), device=0)
+    rng = np.random.default_rng(4)
+    n, m = 100003, 7
+    A = torch.from_numpy(rng.standard_normal((m, n))).cuda()
+    x = torch.from_numpy(rng.standard_normal(n)).cuda()
+    out = torch.zeros(m, dtype=torch.float64, device="cuda")
+    sb.dots(A.data_ptr(), n, m, x.data_ptr(), n, out.data_ptr())
+    torch.cuda.synchronize()
+    ref = A.cpu().numpy() @ x.cpu().numpy()
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max() + 1e-12
+    out2 = torch.zeros_like(out)
+    sb.dots(A.data_ptr(), n, m, x.data_ptr(), n, out2.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(out, out2)
+    sb.close()

@@ -191,6 +191,11 @@ class SigmaBuilder:
         self.htimesc(np.ascontiguousarray(civec, dtype=np.float64), s)
         return s
 
+    def dots(self, A_ptr: int, lda: int, m: int, x_ptr: int, n: int, out_ptr: int, stream: int = 0):
+        """out[k] = A[k] . x on device arrays (deterministic)."""
+        check(lib().tci_dots(self._h, C.c_void_p(A_ptr), lda, m, C.c_void_p(x_ptr), n, C.c_void_p(out_ptr),
+                             C.c_void_p(stream or None)))
+
     def check(self):
         """Synchronise and raise if a bounded device wait gave up."""
         check(lib().tci_check(self._h))

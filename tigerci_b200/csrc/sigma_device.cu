@@ -578,11 +578,14 @@ struct tci_ctx {
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
   double* dots = nullptr;        // reduction scratch: partial sums and results
   double* coefs = nullptr;       // small device coefficient arrays
+  double* dotbuf = nullptr;      // tci_dots reduction scratch
+  int64_t dotbuf_cap = 0;        // doubles
   std::vector<cudaEvent_t> step_ev;     // 2 per sigma step
   std::vector<double> step_ms;          // accumulated per sigma step
   long long profiled_builds = 0;
 
   ~tci_ctx() {
+    if (dotbuf) cudaFree(dotbuf);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (graph_exec_prof) cudaGraphExecDestroy(graph_exec_prof);
@@ -1293,6 +1296,41 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   out[6] = ctx->plan.bytes_allext;
   out[7] = (double)ctx->sigma_count;
   return TCI_OK;
+}
+
+// Batched deterministic projections out[k] = sum_i A[k*lda + i] x[i], k < m, on
+// device arrays (the dot products of expand_krylov_subspace and the MGS
+// overlaps, tiger_fortran/davidson.f90:478-494, 702-723, for a caller that
+// keeps its Davidson vectors in HBM).  Two-pass reduction in a fixed order:
+// the result does not depend on timing.  Scratch (m * 593 doubles) is owned by
+// the context and grows on demand.
+int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
+             void* stream) {
+  if (!ctx || !d_A || !d_x || !d_out || m <= 0 || n <= 0 || (m > 1 && lda < n)) return TCI_ERR_ARG;
+  try {
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t user = stream ? (cudaStream_t)stream : cudaStreamLegacy;
+    const int64_t need = m * (RBLK + 1);
+    if (need > ctx->dotbuf_cap) {
+      TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (ctx->dotbuf) TCI_CUDA(cudaFree(ctx->dotbuf));
+      ctx->dotbuf = nullptr;
+      ctx->dotbuf_cap = 0;
+      if (cudaMalloc(&ctx->dotbuf, need * sizeof(double)) != cudaSuccess)
+        throw Error(TCI_ERR_MEMORY, "device allocation of the projection scratch failed");
+      ctx->dotbuf_cap = need;
+    }
+    TCI_CUDA(cudaEventRecord(ctx->ev0, user));
+    TCI_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev0, 0));
+    multi_dot_partial<<<RBLK, RB, 0, ctx->stream>>>(d_A, lda, (int)m, d_x, n, ctx->dotbuf);
+    multi_dot_final<<<(unsigned)((m + 127) / 128), 128, 0, ctx->stream>>>(ctx->dotbuf, (int)m, RBLK, d_out);
+    TCI_CUDA(cudaGetLastError());
+    TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    TCI_CUDA(cudaStreamWaitEvent(user, ctx->ev1, 0));
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
 }
 
 int tci_check(tci_ctx* ctx) {
