@@ -159,14 +159,14 @@ class SigmaBuilder:
 
     PRECISIONS = {"fp64": 0, "tf32x3": 1}
 
-    def __init__(self, deck: Deck, op: Operator, device: int = 0, precision: str = "fp64"):
+    def __init__(self, deck: Deck, op: Operator, device: int = 0, precision: str = "fp64", promote_every: int = 128):
         self._d = deck.c_struct()
         self._o = op.c_struct()
         self._op = op
         self.precision = precision
         h = C.c_void_p()
-        opts = np.array([self.PRECISIONS[precision]], dtype=np.int64)
-        check(lib().tci_sigma_init_ex(C.byref(self._d), C.byref(self._o), device, ptr(opts), 1, C.byref(h)))
+        opts = np.array([self.PRECISIONS[precision], promote_every], dtype=np.int64)
+        check(lib().tci_sigma_init_ex(C.byref(self._d), C.byref(self._o), device, ptr(opts), 2, C.byref(h)))
         self._h = h
         self.n = int(self.stats()["total_csfs"])
 

@@ -30,8 +30,8 @@ constexpr int BM = 128;      // W rows per CTA tile (MMA M)
 constexpr int BN = 64;       // CI blocks per tile (MMA N)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
 constexpr int STAGES = 4;
-constexpr int KBLOCK = 1024; // k elements per FP64 promotion block
-constexpr int KB_PER_BLOCK = KBLOCK / BK;
+// The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
+// a launch parameter: the tensor core's FP32 accumulation error grows with it.
 constexpr int W_BYTES = BM * BK * 4;   // 16 KB
 constexpr int U_BYTES = BN * BK * 4;   // 8 KB
 constexpr int STAGE_BYTES = 2 * W_BYTES + 2 * U_BYTES;
@@ -112,7 +112,8 @@ enum : int { ST_OK = 0, ST_TIMEOUT_FULL = 1, ST_TIMEOUT_CONV = 2, ST_TIMEOUT_EMP
 __global__ void __launch_bounds__(NTHREADS, 1)
     allext_tf32x3_kernel(const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap uhi_map,
                          const __grid_constant__ CUtensorMap ulo_map, int np, int m, double* __restrict__ Y,
-                         long long ldy, int* __restrict__ status) {
+                         long long ldy, int* __restrict__ status, int kb_per_block) {
+  const int KB_PER_BLOCK = kb_per_block;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
@@ -366,7 +367,12 @@ cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo
 }
 
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
-             int* status, std::string& err) {
+             int* status, int64_t kblock, std::string& err) {
+  if (kblock < tci_tc::BK || kblock % tci_tc::BK) {
+    err = "promotion block must be a positive multiple of 32";
+    return false;
+  }
+  t.kblock = kblock;
   t.np = np;
   t.m = m;
   t.y = y;
@@ -392,7 +398,7 @@ cudaError_t launch(const AllextTc& t, cudaStream_t st) {
   const int smem = tci_tc::STAGES * tci_tc::STAGE_BYTES + 1024 + 256;
   dim3 grid((unsigned)((t.np + tci_tc::BM - 1) / tci_tc::BM), (unsigned)(padded_rows(t.m) / tci_tc::BN));
   tci_tc::allext_tf32x3_kernel<<<grid, tci_tc::NTHREADS, smem, st>>>(t.wmap, t.uhi, t.ulo, (int)t.np, (int)t.m, t.y,
-                                                                     t.np, t.status);
+                                                                     t.np, t.status, (int)(t.kblock / tci_tc::BK));
   return cudaGetLastError();
 }
 

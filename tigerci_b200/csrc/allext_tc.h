@@ -13,6 +13,7 @@ struct AllextTc {
   int64_t np = 0, m = 0;
   double* y = nullptr;         // m x np FP64 output (overwritten)
   int* status = nullptr;       // device status word (0 ok, else a bounded wait gave up)
+  int64_t kblock = 256;        // k elements per FP64 promotion block
 };
 
 int64_t padded_ld(int64_t np);   // fp32 row pitch (multiple of 32 elements)
@@ -20,7 +21,7 @@ int64_t padded_rows(int64_t m);  // rows of the split U (multiple of 64)
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st);
 cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo, cudaStream_t st);
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
-             int* status, std::string& err);
+             int* status, int64_t kblock, std::string& err);
 cudaError_t launch(const AllextTc& t, cudaStream_t st);
 
 }  // namespace tci_tc_host

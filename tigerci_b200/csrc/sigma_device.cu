@@ -567,6 +567,7 @@ struct tci_ctx {
   bool profiling = false;
   bool use_graph = true;                // replay the sigma steps as one CUDA graph
   int64_t precision = 0;                // 0 plain FP64; 1 all-external on tcgen05 (3xTF32, FP64 promotion)
+  int64_t tc_kblock = 128;              // k elements per FP64 promotion block of the tensor-core product
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* uhi = nullptr;                 // split CI blocks for the tensor-core product
@@ -823,10 +824,10 @@ struct tci_ctx {
     if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
     TCI_CUDA(cudaStreamSynchronize(stream));
     std::string err;
-    if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, uhi, ulo, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, err))
+    if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, uhi, ulo, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     if (plan.n_trip > 0 && nm > 0 &&
-        !tci_tc_host::prepare(tc_trip, w32m, nm, uhi, ulo, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, err))
+        !tci_tc_host::prepare(tc_trip, w32m, nm, uhi, ulo, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     TCI_CUDA(cudaFree(buf[BUF_W]));
     bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
@@ -892,24 +893,27 @@ struct tci_ctx {
 
 extern "C" {
 
-static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, tci_ctx** out);
+static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, int64_t kblock,
+                     tci_ctx** out);
 
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out) {
-  return init_impl(deck, op, device, 0, out);
+  return init_impl(deck, op, device, 0, 128, out);
 }
 
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
                       int64_t n_options, tci_ctx** out) {
-  int64_t precision = 0;
+  int64_t precision = 0, kblock = 128;
   if (options && n_options > 0) precision = options[0];
+  if (options && n_options > 1 && options[1] > 0) kblock = options[1];
   if (precision < 0 || precision > 1) {
     set_error("unknown precision mode");
     return TCI_ERR_ARG;
   }
-  return init_impl(deck, op, device, precision, out);
+  return init_impl(deck, op, device, precision, kblock, out);
 }
 
-static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, tci_ctx** out) {
+static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, int64_t kblock,
+                     tci_ctx** out) {
   if (!out) return TCI_ERR_ARG;
   *out = nullptr;
   try {
@@ -965,6 +969,7 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
     }
     if (const char* g = std::getenv("TCI_NO_GRAPH")) ctx->use_graph = (g[0] == '0');
     ctx->precision = precision;
+    ctx->tc_kblock = kblock;
     ctx->setup_precision();
     ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = ctx.release();
