@@ -108,7 +108,8 @@ void tci_plan_destroy(tci_plan* plan);
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out);
 /* As tci_sigma_init with options: options[0] = precision mode, 0 plain FP64
  * (default), 1 the all-external term on tcgen05 tensor cores with FP32 W
- * operators, 3xTF32 split products and FP64 promotion every 1024 k
+ * operators, 3xTF32 split products and FP64 promotion of the FP32 tensor-core
+ * sums every options[1] k elements (multiple of 32, default 128)
  * (TCI_PRECISION_TF32X3); every other term stays FP64. */
 #define TCI_PRECISION_FP64 0
 #define TCI_PRECISION_TF32X3 1
