@@ -136,6 +136,22 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
  * fixed-order reduction; scratch is owned by the context. */
 int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
              void* stream);
+/* tci_dots without device allocation, for callers that cannot call cudaMalloc
+ * when they need projections: a solver loop being recorded into a CUDA graph,
+ * a latency-bound service loop that must avoid cudaMalloc/cudaFree's implicit
+ * device synchronisation, or a program whose GPU memory is fully handed out
+ * by an admission budget or another allocator.  No counterpart in the
+ * reference (its projections run on the host, tiger_fortran/davidson.f90).
+ * Needs no context.  At most TCI_DOTS_NOALLOC_MAX_ROWS rows per call (larger m
+ * returns TCI_ERR_ARG).  The partial sums live in one fixed device array
+ * (TCI_DOTS_NOALLOC_MAX_ROWS x 592 doubles, 303 KB) that each GPU loading the
+ * library holds until exit.  Every call shares it and overwrites what it
+ * reads, so calls whose kernels overlap on a GPU race.  The first call on a
+ * device looks the array's address up (cudaGetSymbolAddress), so make it
+ * before any stream capture. */
+#define TCI_DOTS_NOALLOC_MAX_ROWS 64
+int tci_dots_noalloc(const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
+                     void* stream);
 /* out[0..8]: total_csfs, device bytes held, init seconds, last sigma ms,
  * flops per sigma, all-external flops, all-external bytes, sigma builds,
  * kernel launches per sigma build (out[8] written when len >= 9) */

@@ -38,6 +38,7 @@ EXPORTS = [
     "tci_diag",
     "tci_davidson",
     "tci_dots",
+    "tci_dots_noalloc",
     "tci_ctx_stats",
     "tci_profile",
     "tci_step_times",
@@ -105,6 +106,7 @@ def lib():
         L.tci_diag.argtypes = [P, P, i64]
         L.tci_davidson.argtypes = [P, i64, dbl, dbl, i64, P, P, P]
         L.tci_dots.argtypes = [P, P, i64, i64, P, i64, P, P]
+        L.tci_dots_noalloc.argtypes = [P, i64, i64, P, i64, P, P]
         L.tci_ctx_stats.argtypes = [P, P, i64]
         L.tci_profile.argtypes = [P, i64]
         L.tci_step_times.argtypes = [P, P, i64, P, P]
