@@ -25,6 +25,7 @@ extern "C" {
 #define TCI_ERR_INTERNAL 4 /* internal consistency check failed                   */
 #define TCI_ERR_MEMORY 5   /* device or host allocation failed / over budget      */
 #define TCI_ERR_TIMEOUT 6  /* a bounded device wait gave up                       */
+#define TCI_ERR_CANCELLED 7 /* the caller cancelled the solve                     */
 
 typedef struct tci_space tci_space;
 typedef struct tci_plan tci_plan;
@@ -93,7 +94,9 @@ int tci_plan_create(const tci_deck* deck, const tci_operator* op, tci_plan** out
 /* Writes the plan as a flat binary file (layout: tigerci_b200/plan_io.py). */
 int tci_plan_export(const tci_plan* plan, const char* path);
 /* out[0..7]: total_csfs, n_dense, n_singlet, n_triplet, flops_allext,
- * flops_total, bytes_allext, n_steps */
+ * flops_total, bytes_allext, n_steps; when len >= 10 also out[8] = peak
+ * device bytes of tci_sigma_init (FP64 form) and out[9] = device bytes held
+ * after it.  Host only: used to admit requests against a memory budget. */
 int tci_plan_stats(const tci_plan* plan, double* out, int64_t len);
 void tci_plan_destroy(tci_plan* plan);
 
@@ -129,6 +132,20 @@ int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n);
  * vectors (nroots x total_csfs, may be NULL) the normalised eigenvectors. */
 int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
                  double* energies, double* vectors, int64_t* iterations);
+/* tci_davidson with a subspace memory budget and cancellation.
+ * subspace_bytes plays the role of DAVIDSON HARD DRIVE SPACE
+ * (tiger_cpp/InputReader.cpp:76, 30 GB when 0): once the subspace holds more
+ * than 4 vectors per root and its c and H c vectors need that many bytes, it
+ * restarts from the current and previous Ritz vectors of each root
+ * (restart_davidson_subspace, tiger_fortran/davidson_restart.f90:26-139).
+ * cancel (may be NULL) is polled at every iteration; a non-zero value ends
+ * the solve with TCI_ERR_CANCELLED.  tci_davidson_bytes gives the device bytes
+ * such a solve allocates (host only), tci_davidson_capacity its vector count. */
+int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                    int64_t subspace_bytes, const int32_t* cancel, double* energies, double* vectors,
+                    int64_t* iterations);
+int64_t tci_davidson_capacity(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes);
+int64_t tci_davidson_bytes(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes);
 /* Batched projections for a caller-driven Davidson with device-resident vectors
  * (expand_krylov_subspace / orthonormalize_vector, tiger_fortran/davidson.f90:478,
  * 702): d_out[k] = sum_i d_A[k*lda + i] * d_x[i] for k < m, all device arrays,
@@ -152,9 +169,10 @@ int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const doub
 #define TCI_DOTS_NOALLOC_MAX_ROWS 64
 int tci_dots_noalloc(const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
                      void* stream);
-/* out[0..8]: total_csfs, device bytes held, init seconds, last sigma ms,
+/* out[0..9]: total_csfs, device bytes held, init seconds, last sigma ms,
  * flops per sigma, all-external flops, all-external bytes, sigma builds,
- * kernel launches per sigma build (out[8] written when len >= 9) */
+ * kernel launches per sigma build (out[8], when len >= 9), kernels launched
+ * by this context so far (out[9], when len >= 10) */
 int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len);
 /* Per-step CUDA-event timing of the sigma plan (off by default).  When on,
  * every sigma build records an event pair around each plan step on the

@@ -7,15 +7,23 @@ Davidson-Liu solver, tiger_fortran/davidson.f90:47-239, with
   build_wavefunction ....... :675-694
   orthonormalize_vector .... :702-723  (MGS, renormalised after every projection)
   init_from_diag ........... initial_davidson_guess.f90:99-137
+  need_to_restart_subspace / restart_davidson_subspace
+  ........................... davidson_restart.f90:26-139 (when disk_space is
+                              given: more than 4 vectors per root and
+                              2 * num_vec * n * 8 bytes >= disk_space)
 and numpy's symmetric eigensolver in place of dsyev.  Vectors are kept in
-memory instead of on disk.
+memory instead of on disk.  A restart keeps the current and the previous
+Ritz vector of every unconverged root (the current one of a converged root);
+the reference orthonormalises each root's pair on its own, which for one root
+is the same thing; for several roots this restatement orthonormalises the
+whole collapsed set, so that the basis stays orthonormal.
 """
 from __future__ import annotations
 
 import numpy as np
 
 
-def davidson_liu(sigma, hdiag, roots=1, tol_residual=1e-6, tol_energy=1e-6, maxit=None):
+def davidson_liu(sigma, hdiag, roots=1, tol_residual=1e-6, tol_energy=1e-6, maxit=None, disk_space=None):
     n = len(hdiag)
     maxit = maxit or 50 * roots
     order = np.lexsort((np.arange(n), hdiag))[:roots]
@@ -27,6 +35,8 @@ def davidson_liu(sigma, hdiag, roots=1, tol_residual=1e-6, tol_energy=1e-6, maxi
     energy = np.zeros(roots)
     root2index = list(range(roots))
     converged = [False] * roots
+    restarted = set()
+    V = None
     it = 0
     for it in range(1, maxit + 1):
         for q in range(roots):
@@ -45,16 +55,42 @@ def davidson_liu(sigma, hdiag, roots=1, tol_residual=1e-6, tol_energy=1e-6, maxi
             for k in range(m):
                 hsub[k, idx] = hsub[idx, k] = C[k] @ s
         num_vec = len(C)
+        prevV = V
         w, V = np.linalg.eigh(hsub[:num_vec, :num_vec])
         dE = np.abs(w[:roots] - energy)
         energy = w[:roots].copy()
+        if disk_space is not None and num_vec > 4 * roots and 16.0 * n * num_vec >= disk_space:
+            restarted.add(it)
+            B = [V[:, q].copy() for q in range(roots)]
+            if prevV is not None:
+                for q in range(roots):
+                    if not converged[q]:
+                        b = np.zeros(num_vec)
+                        b[:prevV.shape[0]] = prevV[:, q]
+                        B.append(b)
+            Q = []
+            for b in B:
+                for qv in Q:
+                    b = b - (qv @ b) * qv
+                nb = np.linalg.norm(b)
+                if nb >= 1e-8 and len(Q) < 2 * roots:
+                    Q.append(b / nb)
+            Q = np.array(Q).T  # num_vec x m
+            C = [sum(Q[k, j] * C[k] for k in range(num_vec)) for j in range(Q.shape[1])]
+            HC = [sum(Q[k, j] * HC[k] for k in range(num_vec)) for j in range(Q.shape[1])]
+            hsub = Q.T @ hsub[:num_vec, :num_vec] @ Q
+            hsub = 0.5 * (hsub + hsub.T)
+            num_vec = len(C)
+            w, V = np.linalg.eigh(hsub)
+            energy = w[:roots].copy()
         for q in range(roots):
             if converged[q]:
                 continue
             a = V[:, q]
             r = sum(a[k] * (HC[k] - energy[q] * C[k]) for k in range(num_vec))
             norm = np.sqrt(r @ r)
-            if norm < tol_residual or (abs(dE[q]) < tol_energy and it > 1) or it == maxit:
+            if it not in restarted and (it - 1) not in restarted and (
+                    norm < tol_residual or (abs(dE[q]) < tol_energy and it > 1) or it == maxit):
                 converged[q] = True
                 continue
             p = hdiag - energy[q]

@@ -18,7 +18,7 @@ def declared_symbols():
     for hdr in glob.glob(os.path.join(ROOT, "include", "*.h")):
         txt = open(hdr).read()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-        for m in re.finditer(r"^\s*(?:int|void|const char\s*\*)\s+(tci_\w+)\s*\(", txt, flags=re.M):
+        for m in re.finditer(r"^\s*(?:int|int64_t|void|const char\s*\*)\s+(tci_\w+)\s*\(", txt, flags=re.M):
             syms.add(m.group(1))
     return syms
 

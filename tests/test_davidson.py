@@ -94,3 +94,70 @@ def test_projection_entry_point_matches_host_dots(need_gpu):
     torch.cuda.synchronize()
     assert torch.equal(out, out2)
     sb.close()
+
+
+@pytest.mark.parametrize("roots", [1, 2])
+def test_oracle_restart_under_a_disk_budget_reaches_the_same_roots(roots):
+    """need_to_restart_subspace / restart_davidson_subspace (davidson_restart.f90:26-139):
+    with room for only a few vectors the solver collapses onto current + previous
+    Ritz vectors and still converges to the exact roots."""
+    c = SMALL_CASES[3]
+    h, L = _op(c)
+    od = dense.DenseSigma(oracle_deck(c))
+    H = od.hamiltonian(h, L)
+    n = H.shape[0]
+    exact = np.linalg.eigvalsh(H)[:roots]
+    budget = 16 * n * (4 * roots + 2)
+    e, v, it = odav.davidson_liu(lambda x: H @ x, np.diag(H).copy(), roots=roots, tol_residual=1e-9,
+                                 tol_energy=1e-13, disk_space=budget)
+    assert np.abs(e - exact).max() < 1e-9
+
+
+def test_subspace_capacity_follows_the_budget():
+    from tigerci_b200 import _lib
+
+    L = _lib.lib()
+    n = 1000
+    # default budget (30 GB) leaves the reference's maxit-bound subspace
+    assert L.tci_davidson_capacity(n, 1, 0, 0) == 51
+    assert L.tci_davidson_capacity(n, 2, 0, 0) == 2 * 101
+    # a budget for 12 vectors: restart at 12 (> 4 roots), room for the expansion after the test
+    assert L.tci_davidson_capacity(n, 2, 0, 16 * n * 12) == 11 + 2
+    # never below 4 vectors per root + 1 before a restart can fire
+    assert L.tci_davidson_capacity(n, 2, 0, 16) == 8 + 2
+    b = L.tci_davidson_bytes(n, 2, 0, 16 * n * 12)
+    assert b >= 8 * n * (2 * 13 + 1)
+
+
+@pytest.mark.gpu
+def test_device_restart_under_a_subspace_budget(need_gpu):
+    c = SMALL_CASES[3]
+    h, L = _op(c)
+    sb = T.SigmaBuilder(product_deck(c), T.Operator(h, L), device=0)
+    od = dense.DenseSigma(oracle_deck(c))
+    H = od.hamiltonian(h, L)
+    exact = np.linalg.eigvalsh(H)[:2]
+    n = sb.n
+    e_free, _, it_free = sb.davidson(2, 1e-9, 1e-13)
+    e_rs, _, it_rs = sb.davidson(2, 1e-9, 1e-13, subspace_bytes=16 * n * 10)
+    assert np.abs(e_free - exact).max() < 1e-8
+    assert np.abs(e_rs - exact).max() < 1e-8
+    assert it_rs > 5  # the capacity (11 vectors) forces restarts before convergence
+    sb.close()
+
+
+@pytest.mark.gpu
+def test_device_solve_can_be_cancelled(need_gpu):
+    c = SMALL_CASES[3]
+    h, L = _op(c)
+    sb = T.SigmaBuilder(product_deck(c), T.Operator(h, L), device=0)
+    flag = np.ones(1, dtype=np.int32)
+    from tigerci_b200 import _lib
+
+    with pytest.raises(_lib.TciError) as ei:
+        sb.davidson(1, 1e-9, 1e-13, cancel=flag)
+    assert ei.value.code == 7
+    flag[0] = 0
+    e, _, _ = sb.davidson(1, 1e-9, 1e-13, cancel=flag)  # the context stays usable
+    assert np.isfinite(e).all()
+    sb.close()

@@ -37,6 +37,9 @@ EXPORTS = [
     "tci_sigma_device",
     "tci_diag",
     "tci_davidson",
+    "tci_davidson_ex",
+    "tci_davidson_capacity",
+    "tci_davidson_bytes",
     "tci_dots",
     "tci_dots_noalloc",
     "tci_ctx_stats",
@@ -105,6 +108,11 @@ def lib():
         L.tci_sigma_device.argtypes = [P, P, P, i64, P]
         L.tci_diag.argtypes = [P, P, i64]
         L.tci_davidson.argtypes = [P, i64, dbl, dbl, i64, P, P, P]
+        L.tci_davidson_ex.argtypes = [P, i64, dbl, dbl, i64, i64, P, P, P, P]
+        L.tci_davidson_capacity.argtypes = [i64, i64, i64, i64]
+        L.tci_davidson_capacity.restype = i64
+        L.tci_davidson_bytes.argtypes = [i64, i64, i64, i64]
+        L.tci_davidson_bytes.restype = i64
         L.tci_dots.argtypes = [P, P, i64, i64, P, i64, P, P]
         L.tci_dots_noalloc.argtypes = [P, i64, i64, P, i64, P, P]
         L.tci_ctx_stats.argtypes = [P, P, i64]

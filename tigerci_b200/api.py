@@ -147,10 +147,10 @@ class Plan:
         check(lib().tci_plan_export(self._h, path.encode()))
 
     def stats(self) -> dict:
-        out = np.zeros(8, dtype=np.float64)
-        check(lib().tci_plan_stats(self._h, ptr(out), 8))
+        out = np.zeros(10, dtype=np.float64)
+        check(lib().tci_plan_stats(self._h, ptr(out), 10))
         keys = ["total_csfs", "n_dense", "n_singlet", "n_triplet", "flops_allext", "flops_total", "bytes_allext",
-                "n_steps"]
+                "n_steps", "device_bytes_peak", "device_bytes_resident"]
         return dict(zip(keys, out.tolist()))
 
 
@@ -211,13 +211,20 @@ class SigmaBuilder:
         return out
 
     def davidson(self, nroots: int = 1, tol_residual: float = 1e-6, tol_energy: float = 1e-6, maxit: int = 0,
-                 want_vectors: bool = False):
-        """Device-resident Davidson-Liu (davidson_liu); returns (energies, vectors|None, iterations)."""
+                 want_vectors: bool = False, subspace_bytes: int = 0, cancel=None):
+        """Device-resident Davidson-Liu (davidson_liu); returns (energies, vectors|None, iterations).
+
+        subspace_bytes bounds the c / H c subspace like DAVIDSON HARD DRIVE
+        SPACE (0: 30 GB); cancel is an optional numpy int32 array of one
+        element whose becoming non-zero ends the solve (TCI_ERR_CANCELLED)."""
         e = np.zeros(nroots)
         v = np.zeros((nroots, self.n)) if want_vectors else None
         it = C.c_int64()
-        check(lib().tci_davidson(self._h, nroots, tol_residual, tol_energy, maxit, ptr(e),
-                                 ptr(v) if v is not None else None, C.byref(it)))
+        if cancel is not None and (cancel.dtype != np.int32 or cancel.size < 1):
+            raise TypeError("cancel must be an int32 array")
+        check(lib().tci_davidson_ex(self._h, nroots, tol_residual, tol_energy, maxit, int(subspace_bytes),
+                                    ptr(cancel) if cancel is not None else None, ptr(e),
+                                    ptr(v) if v is not None else None, C.byref(it)))
         return e, v, it.value
 
     def profile(self, on: bool = True):
@@ -238,8 +245,8 @@ class SigmaBuilder:
         return list(zip(names, ms.tolist())), nb.value
 
     def stats(self) -> dict:
-        out = np.zeros(9, dtype=np.float64)
-        check(lib().tci_ctx_stats(self._h, ptr(out), 9))
+        out = np.zeros(10, dtype=np.float64)
+        check(lib().tci_ctx_stats(self._h, ptr(out), 10))
         keys = ["total_csfs", "device_bytes", "init_seconds", "last_sigma_ms", "flops_per_sigma",
-                "flops_allext", "bytes_allext", "sigma_count", "launches_per_sigma"]
+                "flops_allext", "bytes_allext", "sigma_count", "launches_per_sigma", "launches"]
         return dict(zip(keys, out.tolist()))

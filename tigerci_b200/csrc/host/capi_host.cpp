@@ -1,5 +1,6 @@
 // Host-only part of the C ABI (include/tigerci_sigma.h): error reporting, CSF
 // space queries and plan construction / export.  No CUDA dependency.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -266,6 +267,18 @@ int tci_plan_export(const tci_plan* p, const char* path) {
 int tci_plan_stats(const tci_plan* p, double* out, int64_t len) {
   if (!p || !out || len < 8) return TCI_ERR_ARG;
   const Plan& P = p->plan;
+  if (len >= 10) {
+    // device bytes: peak during set-up (every plan buffer) and resident after it
+    // (set-up-only buffers released); a Davidson subspace adds 2 * vectors * total_csfs * 8
+    double peak = 0, resident = 0;
+    for (int b = 0; b < NUM_BUFS; ++b) {
+      const double bytes = (double)std::max<i64>(0, P.buf_size[b]) * 8.0;
+      peak += bytes;
+      if (b != BUF_X && b != BUF_L && b != BUF_LE && b != BUF_LI) resident += bytes;
+    }
+    out[8] = peak;
+    out[9] = resident;
+  }
   out[0] = (double)P.total_csfs;
   out[1] = (double)P.nD;
   out[2] = (double)P.n_sing;

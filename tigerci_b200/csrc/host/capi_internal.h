@@ -11,4 +11,10 @@ void set_error(const std::string& m);
 int guard_status(const std::exception_ptr& ep);
 void build_space_from_c(const tci_deck* d, CsfSpace& sp);
 void operator_from_c(const tci_operator* op, const CsfSpace& sp, Operator& out);
+// Device half of tci_sigma_init: a context from a host-built space and plan
+// (chol: the host Cholesky vectors the plan was built for).
+int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
+                  tci_ctx** out);
+// Device bytes of such a context: peak during set-up and held afterwards.
+void ctx_device_bytes(const Plan& plan, int64_t precision, double* peak, double* resident);
 }  // namespace tci

@@ -449,6 +449,8 @@ __global__ void build_diag_kernel(const DDiag* __restrict__ ent, long long nent,
 // Davidson vector kernels (FP64, deterministic two-pass reductions)
 constexpr int RB = 256;     // threads per reduction block
 constexpr int RBLK = 592;   // reduction blocks (4 x 148 SMs)
+// default Davidson subspace budget: the reference's DAVIDSON HARD DRIVE SPACE default of 30 GB
+constexpr double kDefaultSubspaceBytes = 30e9;
 
 // partial[k * RBLK + b] = sum over block b's chunk of A[k][i] * x[i]
 __global__ void __launch_bounds__(RB) multi_dot_partial(const double* __restrict__ A, long long lda, int m,
@@ -584,6 +586,7 @@ struct tci_ctx {
   std::vector<cudaEvent_t> step_ev;     // 2 per sigma step
   std::vector<double> step_ms;          // accumulated per sigma step
   long long profiled_builds = 0;
+  long long launch_count = 0;    // kernels this context has launched (sigma builds, Davidson, projections)
 
   ~tci_ctx() {
     if (dotbuf) cudaFree(dotbuf);
@@ -717,6 +720,7 @@ struct tci_ctx {
   void multi_dot(const double* A, i64 lda, int m, const double* x, i64 n, double* host_out) {
     multi_dot_partial<<<RBLK, RB, 0, stream>>>(A, lda, m, x, n, dots);
     multi_dot_final<<<(m + 127) / 128, 128, 0, stream>>>(dots, m, RBLK, dots + (size_t)m * RBLK);
+    launch_count += 2;
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaMemcpyAsync(host_out, dots + (size_t)m * RBLK, m * sizeof(double), cudaMemcpyDeviceToHost, stream));
     TCI_CUDA(cudaStreamSynchronize(stream));
@@ -725,6 +729,7 @@ struct tci_ctx {
   void dot_dev(const double* a, const double* x, i64 n, double* dev_out) {
     multi_dot_partial<<<RBLK, RB, 0, stream>>>(a, 0, 1, x, n, dots);
     multi_dot_final<<<1, 32, 0, stream>>>(dots, 1, RBLK, dev_out);
+    launch_count += 2;
     TCI_CUDA(cudaGetLastError());
   }
 
@@ -736,6 +741,22 @@ struct tci_ctx {
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     sigma_count++;
   }
+  // kernels one sigma build launches (graph nodes included)
+  long long sigma_launches() const {
+    long long k = 0;
+    for (const auto& s : sigma) {
+      if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
+      if (precision == 1 && s.kind == STEP_GEMM && s.name == "all-external") {
+        k += (plan.n_sing > 0 ? 2 : 0) + (plan.n_trip > 0 && plan.nm > 0 ? 2 : 0);
+        continue;
+      }
+      if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
+          ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && plan.nD > 0))
+        k += 1;
+    }
+    return k;
+  }
+
   void ensure_step_events() {
     if (step_ev.size() != 2 * sigma.size()) {
       step_ev.resize(2 * sigma.size());
@@ -780,6 +801,7 @@ struct tci_ctx {
     } else {
       record_steps(profiling, false);
     }
+    launch_count += sigma_launches();
     if (profiling) {
       TCI_CUDA(cudaStreamSynchronize(stream));
       for (size_t i = 0; i < sigma.size(); ++i) {
@@ -918,6 +940,56 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
   *out = nullptr;
   try {
     auto t0 = std::chrono::steady_clock::now();
+    CsfSpace sp;
+    Plan plan;
+    build_space_from_c(deck, sp);
+    Operator o;
+    operator_from_c(op, sp, o);
+    build_plan(sp, o, plan);
+    const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out);
+    if (rc == TCI_OK) (*out)->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
+}  // extern "C"
+
+namespace tci {
+
+void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* resident) {
+  double all = 0, init_only = 0;
+  for (int b = 0; b < NUM_BUFS; ++b) {
+    const double bytes = (double)std::max<i64>(0, P.buf_size[b]) * 8.0;
+    all += bytes;
+    if (b == BUF_X || b == BUF_L || b == BUF_LE || b == BUF_LI) init_only += bytes;
+  }
+  // tables (steps, heads) are small next to the buffers; the diagonal is built on first use
+  const double diag = 8.0 * (double)P.total_csfs;
+  double pk = all, res = all - init_only + diag;
+  if (precision == 1) {
+    const i64 mrows = tci_tc_host::padded_rows(std::max<i64>(1, std::max(P.n_sing, P.n_trip)));
+    const double f32 = 4.0 * ((double)P.np * tci_tc_host::padded_ld(P.np) +
+                              (P.nm > 0 ? (double)P.nm * tci_tc_host::padded_ld(P.nm) : 0.0) +
+                              2.0 * (double)mrows * tci_tc_host::padded_ld(P.np));
+    pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
+    res += f32 - 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]);
+  }
+  *peak = std::max(pk, res);
+  *resident = res;
+}
+
+int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
+                  tci_ctx** out) {
+  if (!out || !chol) return TCI_ERR_ARG;
+  *out = nullptr;
+  if (precision < 0 || precision > 1) {
+    set_error("unknown precision mode");
+    return TCI_ERR_ARG;
+  }
+  try {
+    auto t0 = std::chrono::steady_clock::now();
     std::unique_ptr<tci_ctx> ctx(new tci_ctx());
     int ndev = 0;
     TCI_CUDA(cudaGetDeviceCount(&ndev));
@@ -927,25 +999,29 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
     TCI_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     TCI_CUDA(cudaEventCreate(&ctx->ev0));
     TCI_CUDA(cudaEventCreate(&ctx->ev1));
-    build_space_from_c(deck, ctx->sp);
-    Operator o;
-    operator_from_c(op, ctx->sp, o);
-    build_plan(ctx->sp, o, ctx->plan);
+    ctx->sp = std::move(sp);
+    ctx->plan = std::move(plan);
     Plan& P = ctx->plan;
     for (int b = 0; b < NUM_BUFS; ++b) {
       if (P.buf_size[b] <= 0) continue;
       cudaError_t e = cudaMalloc(&ctx->buf[b], P.buf_size[b] * sizeof(double));
-      if (e != cudaSuccess) throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+      }
       // plan steps accumulate into their targets: every buffer starts at zero
       TCI_CUDA(cudaMemsetAsync(ctx->buf[b], 0, P.buf_size[b] * sizeof(double), ctx->stream));
       ctx->bytes_held += (double)P.buf_size[b] * sizeof(double);
     }
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
-    TCI_CUDA(cudaMemcpy(ctx->buf[BUF_L], o.chol, P.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice));
-    TCI_CUDA(cudaMemcpy(ctx->buf[BUF_JK] + 2 * P.nint * P.nint * P.n * P.n, P.h_vv.data(), P.h_vv.size() * sizeof(double),
-                        cudaMemcpyHostToDevice));
+    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_L], chol, P.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_JK] + 2 * P.nint * P.nint * P.n * P.n, P.h_vv.data(),
+                             P.h_vv.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     if (!P.wv.empty())
-      TCI_CUDA(cudaMemcpy(ctx->buf[BUF_WV], P.wv.data(), P.wv.size() * sizeof(double), cudaMemcpyHostToDevice));
+      TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_WV], P.wv.data(), P.wv.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               ctx->stream));
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     std::vector<DHead> dh;
     std::vector<int> dkh;
     for (size_t h = 0; h < P.dheads.size(); ++h) {
@@ -979,6 +1055,10 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
   }
 }
 
+}  // namespace tci
+
+extern "C" {
+
 int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n, void* stream) {
   if (!ctx || !d_c || !d_sigma) return TCI_ERR_ARG;
   try {
@@ -996,6 +1076,7 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     // sigma += S (the caller's sigma accumulates, like htimesc)
     accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(d_sigma, ctx->buf[BUF_S], n);
+    ctx->launch_count++;
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     TCI_CUDA(cudaStreamWaitEvent(user, ctx->ev1, 0));
@@ -1109,37 +1190,71 @@ void jacobi_eigh(std::vector<double> A, int m, std::vector<double>& w, std::vect
 
 extern "C" {
 
+int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                 double* energies, double* vectors, int64_t* iterations) {
+  return tci_davidson_ex(ctx, nroots, tol_residual, tol_energy, maxit, 0, nullptr, energies, vectors, iterations);
+}
+
+int64_t tci_davidson_capacity(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes) {
+  if (n <= 0 || nroots <= 0) return 0;
+  if (maxit <= 0) maxit = 50 * nroots;
+  const double budget = subspace_bytes > 0 ? (double)subspace_bytes : kDefaultSubspaceBytes;
+  // the restart test fires at the first size T with 2 * T * n * 8 >= budget (and T > 4 * nroots);
+  // the expansion that follows a test adds at most nroots vectors
+  const int64_t t = std::max<int64_t>(4 * nroots + 1, (int64_t)std::ceil(budget / (16.0 * (double)n)));
+  return std::min<int64_t>({n, (maxit + 1) * nroots, t - 1 + nroots});
+}
+
+int64_t tci_davidson_bytes(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes) {
+  const int64_t cap = tci_davidson_capacity(n, nroots, maxit, subspace_bytes);
+  // c and H c vectors, the residual, the collapse buffers (2 * 2 * nroots vectors) and the reduction scratch
+  return 8 * (n * (2 * cap + 1 + 4 * nroots) + (cap + 4) * (RBLK + 1) + 16 + 4 * (cap + 4));
+}
+
 // Block Davidson-Liu with HBM-resident expansion and sigma vectors, restating
 // davidson_liu (tiger_fortran/davidson.f90:47-239): per unconverged root one
 // sigma build and subspace expansion; subspace eigensolve; wavefunction,
 // residual, convergence test (is_converged :564-602), diagonal preconditioner
 // (:609-631) and modified Gram-Schmidt with renormalisation after every
 // projection (:702-723).  The initial guess is the unit vectors of the lowest
-// diagonal elements (init_from_diag, initial_davidson_guess.f90:99-137).  When
-// the subspace reaches its capacity it collapses onto the current Ritz vectors.
-int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
-                 double* energies, double* vectors, int64_t* iterations) {
-  if (!ctx || !energies || nroots <= 0) return TCI_ERR_ARG;
+// diagonal elements (init_from_diag, initial_davidson_guess.f90:99-137).
+// The subspace restarts like restart_davidson_subspace
+// (davidson_restart.f90:26-139): when it holds more than 4 vectors per root and
+// its c and H c vectors need at least subspace_bytes (the role of DAVIDSON HARD
+// DRIVE SPACE), it collapses onto the current and the previous Ritz vector of
+// every unconverged root (the current one only for converged roots).  The
+// collapsed set is orthonormalised as a whole, so the subspace basis stays
+// orthonormal.  A non-null cancel flag that becomes non-zero ends the solve
+// with TCI_ERR_CANCELLED at the next iteration boundary.
+int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                    int64_t subspace_bytes, const int32_t* cancel, double* energies, double* vectors,
+                    int64_t* iterations) {
+  if (!ctx || !energies || nroots <= 0 || subspace_bytes < 0) return TCI_ERR_ARG;
   try {
     TCI_CUDA(cudaSetDevice(ctx->device));
     const i64 n = ctx->plan.total_csfs;
     if (nroots > n) throw Error(TCI_ERR_ARG, "more roots than CSFs");
     if (maxit <= 0) maxit = 50 * nroots;
-    const int cap = (int)std::min<i64>(n, std::max<i64>(2 * nroots, (maxit + 1) * nroots));
+    const double budget = subspace_bytes > 0 ? (double)subspace_bytes : kDefaultSubspaceBytes;
+    const int cap = (int)tci_davidson_capacity(n, nroots, maxit, subspace_bytes);
+    const int keep = (int)std::min<i64>(2 * nroots, n);  // vectors kept by a collapse
     ctx->ensure_diag();
     ctx->ensure_scratch(cap + 4);
-    double *Cs = nullptr, *HCs = nullptr, *r = nullptr;
+    double *Cs = nullptr, *HCs = nullptr, *r = nullptr, *tmpC = nullptr, *tmpH = nullptr;
     auto free_all = [&]() {
-      if (Cs) cudaFree(Cs);
-      if (HCs) cudaFree(HCs);
-      if (r) cudaFree(r);
+      for (double* p : {Cs, HCs, r, tmpC, tmpH})
+        if (p) cudaFree(p);
     };
     try {
       cudaError_t e1 = cudaMalloc(&Cs, (size_t)cap * n * sizeof(double));
       cudaError_t e2 = cudaMalloc(&HCs, (size_t)cap * n * sizeof(double));
       cudaError_t e3 = cudaMalloc(&r, (size_t)(n + 8) * sizeof(double));
-      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+      cudaError_t e4 = cudaMalloc(&tmpC, (size_t)keep * n * sizeof(double));
+      cudaError_t e5 = cudaMalloc(&tmpH, (size_t)keep * n * sizeof(double));
+      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess || e5 != cudaSuccess) {
+        cudaGetLastError();
         throw Error(TCI_ERR_MEMORY, "device allocation of the Davidson subspace failed");
+      }
       cudaStream_t st = ctx->stream;
       const unsigned G = 148 * 8, TB = 256;
       // initial guess: unit vectors at the lowest diagonal elements
@@ -1158,9 +1273,19 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
       std::vector<int> root2index(nroots);
       for (int k = 0; k < nroots; ++k) root2index[k] = k;
       std::vector<char> conv(nroots, 0), restarted(maxit + 2, 0);
-      std::vector<double> energy(nroots, 0.0), dE(nroots, 0.0), hsub((size_t)cap * cap, 0.0), w, V, col(cap);
+      std::vector<double> energy(nroots, 0.0), dE(nroots, 0.0), hsub((size_t)cap * cap, 0.0), w, V, Vprev, col(cap);
+      int mprev = 0;  // subspace dimension of Vprev
+      auto lincomb_into = [&](double* dst, const double* src, const std::vector<double>& coef, int m) {
+        TCI_CUDA(cudaMemcpyAsync(ctx->coefs, coef.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
+        lincomb_kernel<<<G, TB, 0, st>>>(dst, 0.0, src, ctx->coefs, nullptr, nullptr, m, n, n);
+        ctx->launch_count++;
+        TCI_CUDA(cudaGetLastError());
+        // the coefficient array is reused by the next call
+        TCI_CUDA(cudaStreamSynchronize(st));
+      };
       i64 it = 0;
       for (it = 1; it <= maxit; ++it) {
+        if (cancel && __atomic_load_n(cancel, __ATOMIC_ACQUIRE) != 0) throw Error(TCI_ERR_CANCELLED, "solve cancelled");
         for (int q = 0; q < nroots; ++q) {
           if (conv[q]) continue;
           const int index = root2index[q];
@@ -1171,38 +1296,82 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
         std::vector<double> h((size_t)num_vec * num_vec);
         for (int a = 0; a < num_vec; ++a)
           for (int b = 0; b < num_vec; ++b) h[(size_t)a * num_vec + b] = hsub[(size_t)a * cap + b];
+        if (!w.empty()) {
+          Vprev = V;
+          mprev = (int)w.size();
+        }
         jacobi_eigh(h, num_vec, w, V);
         for (int q = 0; q < nroots; ++q) {
           dE[q] = std::fabs(w[q] - energy[q]);
           energy[q] = w[q];
         }
-        if (num_vec + nroots > cap) {
-          // collapse onto the current Ritz vectors (and their sigma vectors)
+        const bool over_budget = num_vec > 4 * nroots && 16.0 * (double)n * num_vec >= budget;
+        if (over_budget || num_vec + nroots > cap) {
+          // restart_davidson_subspace: new basis {current, previous} per unconverged root, {current} per
+          // converged root, as coefficient vectors in the present (orthonormal) basis
           restarted[it] = 1;
-          std::vector<double> cvec((size_t)nroots * num_vec);
-          for (int q = 0; q < nroots; ++q)
-            for (int k = 0; k < num_vec; ++k) cvec[(size_t)q * num_vec + k] = V[(size_t)k * num_vec + q];
-          double *tmpC = nullptr, *tmpH = nullptr;
-          TCI_CUDA(cudaMalloc(&tmpC, (size_t)nroots * n * sizeof(double)));
-          TCI_CUDA(cudaMalloc(&tmpH, (size_t)nroots * n * sizeof(double)));
+          // (the current vectors go first so that a full subspace never drops one of them)
+          std::vector<std::vector<double>> B;
           for (int q = 0; q < nroots; ++q) {
-            TCI_CUDA(cudaMemcpyAsync(ctx->coefs, cvec.data() + (size_t)q * num_vec, num_vec * sizeof(double),
-                                     cudaMemcpyHostToDevice, st));
-            lincomb_kernel<<<G, TB, 0, st>>>(tmpC + (size_t)q * n, 0.0, Cs, ctx->coefs, nullptr, nullptr, num_vec, n, n);
-            lincomb_kernel<<<G, TB, 0, st>>>(tmpH + (size_t)q * n, 0.0, HCs, ctx->coefs, nullptr, nullptr, num_vec, n, n);
-            TCI_CUDA(cudaStreamSynchronize(st));
+            std::vector<double> cur(num_vec);
+            for (int k = 0; k < num_vec; ++k) cur[k] = V[(size_t)k * num_vec + q];
+            B.push_back(cur);
           }
-          TCI_CUDA(cudaMemcpyAsync(Cs, tmpC, (size_t)nroots * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-          TCI_CUDA(cudaMemcpyAsync(HCs, tmpH, (size_t)nroots * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          for (int q = 0; q < nroots; ++q) {
+            if (conv[q] || mprev == 0) continue;
+            std::vector<double> prev(num_vec, 0.0);
+            for (int k = 0; k < mprev && k < num_vec; ++k) prev[k] = Vprev[(size_t)k * mprev + q];
+            B.push_back(prev);
+          }
+          const int limit = std::max<int>((int)nroots, std::min<int>(keep, cap - (int)nroots));
+          // modified Gram-Schmidt in coefficient space; nearly dependent vectors are dropped
+          std::vector<std::vector<double>> Q;
+          for (auto& b : B) {
+            for (auto& qv : Q) {
+              double d = 0;
+              for (int k = 0; k < num_vec; ++k) d += qv[k] * b[k];
+              for (int k = 0; k < num_vec; ++k) b[k] -= d * qv[k];
+            }
+            double nr = 0;
+            for (int k = 0; k < num_vec; ++k) nr += b[k] * b[k];
+            nr = std::sqrt(nr);
+            if (nr < 1e-8 || (int)Q.size() >= limit) continue;
+            for (int k = 0; k < num_vec; ++k) b[k] /= nr;
+            Q.push_back(b);
+          }
+          const int m2 = (int)Q.size();
+          for (int j = 0; j < m2; ++j) {
+            lincomb_into(tmpC + (size_t)j * n, Cs, Q[j], num_vec);
+            lincomb_into(tmpH + (size_t)j * n, HCs, Q[j], num_vec);
+          }
+          TCI_CUDA(cudaMemcpyAsync(Cs, tmpC, (size_t)m2 * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          TCI_CUDA(cudaMemcpyAsync(HCs, tmpH, (size_t)m2 * n * sizeof(double), cudaMemcpyDeviceToDevice, st));
           TCI_CUDA(cudaStreamSynchronize(st));
-          cudaFree(tmpC);
-          cudaFree(tmpH);
+          // H in the new basis: Q^T hsub Q
+          std::vector<double> hq((size_t)num_vec * m2, 0.0), hn((size_t)m2 * m2, 0.0);
+          for (int a = 0; a < num_vec; ++a)
+            for (int j = 0; j < m2; ++j) {
+              double t = 0;
+              for (int b = 0; b < num_vec; ++b) t += hsub[(size_t)a * cap + b] * Q[j][b];
+              hq[(size_t)a * m2 + j] = t;
+            }
+          for (int i = 0; i < m2; ++i)
+            for (int j = 0; j < m2; ++j) {
+              double t = 0;
+              for (int a = 0; a < num_vec; ++a) t += Q[i][a] * hq[(size_t)a * m2 + j];
+              hn[(size_t)i * m2 + j] = t;
+            }
+          for (int i = 0; i < m2; ++i)
+            for (int j = 0; j < m2; ++j) hn[(size_t)i * m2 + j] = hn[(size_t)j * m2 + i] =
+                0.5 * (hn[(size_t)i * m2 + j] + hn[(size_t)j * m2 + i]);
           std::fill(hsub.begin(), hsub.end(), 0.0);
-          for (int q = 0; q < nroots; ++q) hsub[(size_t)q * cap + q] = w[q];
-          num_vec = (int)nroots;
-          V.assign((size_t)num_vec * num_vec, 0.0);
-          for (int q = 0; q < nroots; ++q) V[(size_t)q * num_vec + q] = 1.0;
-          w.resize(num_vec);
+          for (int i = 0; i < m2; ++i)
+            for (int j = 0; j < m2; ++j) hsub[(size_t)i * cap + j] = hn[(size_t)i * m2 + j];
+          num_vec = m2;
+          jacobi_eigh(hn, num_vec, w, V);
+          for (int q = 0; q < nroots; ++q) energy[q] = w[q];
+          Vprev.clear();
+          mprev = 0;
         }
         // the Ritz vectors live in the subspace of this iteration (subspace_size in
         // davidson.f90:140); vectors appended below for earlier roots are not part of it
@@ -1218,6 +1387,7 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
           TCI_CUDA(cudaMemcpyAsync(ctx->coefs, ca.data(), subspace_size * sizeof(double), cudaMemcpyHostToDevice, st));
           TCI_CUDA(cudaMemcpyAsync(ctx->coefs + cap, cb.data(), subspace_size * sizeof(double), cudaMemcpyHostToDevice, st));
           lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, HCs, ctx->coefs + cap, subspace_size, n, n);
+          ctx->launch_count++;
           TCI_CUDA(cudaGetLastError());
           double nrm2 = 0.0;
           ctx->multi_dot(r, 0, 1, r, n, &nrm2);
@@ -1234,6 +1404,7 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
             continue;
           }
           precondition_kernel<<<G, TB, 0, st>>>(r, ctx->hd, energy[q], n);
+          ctx->launch_count++;
           TCI_CUDA(cudaGetLastError());
           double* dev_ov = ctx->dots + (size_t)(cap + 4) * RBLK;
           for (int k = 0; k < num_vec; ++k) {
@@ -1241,6 +1412,7 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
             axpy_scale_kernel<<<G, TB, 0, st>>>(r, Cs + (size_t)k * n, dev_ov, n);
             ctx->dot_dev(r, r, n, dev_ov + 1);
             normalize_kernel<<<G, TB, 0, st>>>(r, dev_ov + 1, n);
+            ctx->launch_count += 2;
           }
           TCI_CUDA(cudaGetLastError());
           if (num_vec >= cap) throw Error(TCI_ERR_INTERNAL, "Davidson subspace capacity exceeded");
@@ -1261,8 +1433,7 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
         for (int q = 0; q < nroots; ++q) {
           std::vector<double> cb(m);
           for (int k = 0; k < m; ++k) cb[k] = V[(size_t)k * m + q];
-          TCI_CUDA(cudaMemcpyAsync(ctx->coefs, cb.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
-          lincomb_kernel<<<G, TB, 0, st>>>(r, 0.0, Cs, ctx->coefs, nullptr, nullptr, m, n, n);
+          lincomb_into(r, Cs, cb, m);
           double nrm2 = 0.0;
           ctx->multi_dot(r, 0, 1, r, n, &nrm2);
           std::vector<double> hv(n);
@@ -1284,14 +1455,8 @@ int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_e
 
 int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   if (!ctx || !out || len < 8) return TCI_ERR_ARG;
-  if (len >= 9) {
-    double launches = 1.0;  // final accumulation into the caller's sigma
-    for (const auto& s : ctx->sigma)
-      if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
-          ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && ctx->plan.nD > 0))
-        launches += 1.0;
-    out[8] = launches;
-  }
+  if (len >= 9) out[8] = 1.0 + (double)ctx->sigma_launches();  // + the accumulation into the caller's sigma
+  if (len >= 10) out[9] = (double)ctx->launch_count;
   out[0] = (double)ctx->plan.total_csfs;
   out[1] = ctx->bytes_held;
   out[2] = ctx->init_seconds;
@@ -1329,6 +1494,7 @@ int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const doub
     TCI_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev0, 0));
     multi_dot_partial<<<RBLK, RB, 0, ctx->stream>>>(d_A, lda, (int)m, d_x, n, ctx->dotbuf);
     multi_dot_final<<<(unsigned)((m + 127) / 128), 128, 0, ctx->stream>>>(ctx->dotbuf, (int)m, RBLK, d_out);
+    ctx->launch_count += 2;
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     TCI_CUDA(cudaStreamWaitEvent(user, ctx->ev1, 0));
