@@ -186,6 +186,51 @@ int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps,
 int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len);
 void tci_destroy(tci_ctx* ctx);
 
+/* ---- Serving: continuously batched CI solves on one GPU ----------------
+ * No counterpart in the reference, which runs one solve per process
+ * (tiger_fortran/tiger_ci.f90 -> davidson_liu).  Submitted solves are
+ * planned on host threads, admitted in arrival order when a slot is free and
+ * their device-memory estimate fits the HBM budget, and solved by
+ * tci_davidson_ex on a context of their own (own CUDA stream), so the sigma
+ * builds of the admitted requests overlap on the device.  A request's result
+ * is the one a lone tci_davidson_ex call gives. */
+typedef struct tci_server tci_server;
+typedef struct {
+  int64_t device;
+  int64_t slots;                     /* solves on the GPU at once (1..64)            */
+  int64_t planners;                  /* host threads building plans (1..64)          */
+  int64_t hbm_budget_bytes;          /* device bytes all admitted solves may reserve */
+  int64_t precision;                 /* TCI_PRECISION_*                              */
+  int64_t subspace_vectors_per_root; /* Davidson c / H c vectors per root before a
+                                        restart (0: 12)                              */
+  int64_t schedule_only;             /* 1: no device work; an admitted request holds
+                                        its slot and reservation schedule_only_ms and
+                                        returns NaN energies (scheduling tests)      */
+  double schedule_only_ms;
+  int64_t inject_worker_exit_at;     /* host fault injection: the worker thread that
+                                        makes this admission (1-based) dies; 0 off   */
+} tci_server_config;
+int tci_server_create(const tci_server_config* cfg, tci_server** out);
+/* Copies the deck and operator (the caller may free them on return); rejects
+ * non-finite operator values (TCI_ERR_INPUT).  *id identifies the request. */
+int tci_server_submit(tci_server* s, const tci_deck* deck, const tci_operator* op, int64_t nroots, double tol_residual,
+                      double tol_energy, int64_t maxit, int64_t* id);
+/* Waits up to timeout_s seconds (< 0: no limit; TCI_ERR_TIMEOUT when it runs
+ * out) and returns the request's status.  energies[len]; info[9] = status,
+ * iterations, submit / planned / admitted / done times (s since the server
+ * started), reserved device bytes, total_csfs, core energy. */
+int tci_server_wait(tci_server* s, int64_t id, double timeout_s, double* energies, int64_t len, double* info);
+/* Cancels a queued request at once, a running one at its next iteration
+ * (its status becomes TCI_ERR_CANCELLED). */
+int tci_server_cancel(tci_server* s, int64_t id);
+/* out[13]: submitted, succeeded, failed, cancelled, queued, running, peak
+ * running, peak reserved bytes, p50 and p99 time to solution (s), solves/s
+ * (successes over first submission .. last success), worker restarts,
+ * reserved bytes now. */
+int tci_server_stats(tci_server* s, double* out, int64_t len);
+/* Cancels what is running or queued and joins the server's threads. */
+void tci_server_destroy(tci_server* s);
+
 #ifdef __cplusplus
 }
 #endif

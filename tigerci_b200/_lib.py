@@ -40,6 +40,12 @@ EXPORTS = [
     "tci_davidson_ex",
     "tci_davidson_capacity",
     "tci_davidson_bytes",
+    "tci_server_create",
+    "tci_server_submit",
+    "tci_server_wait",
+    "tci_server_cancel",
+    "tci_server_stats",
+    "tci_server_destroy",
     "tci_dots",
     "tci_dots_noalloc",
     "tci_ctx_stats",

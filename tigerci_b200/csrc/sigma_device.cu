@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "../../include/tigerci_sigma.h"
@@ -451,6 +452,10 @@ constexpr int RB = 256;     // threads per reduction block
 constexpr int RBLK = 592;   // reduction blocks (4 x 148 SMs)
 // default Davidson subspace budget: the reference's DAVIDSON HARD DRIVE SPACE default of 30 GB
 constexpr double kDefaultSubspaceBytes = 30e9;
+// Several contexts may live in one process, driven from different host threads
+// (the request server).  A graph capture on one thread and a cudaFree (which
+// synchronises the device) on another are kept apart by this lock.
+std::mutex g_capture_free_mu;
 
 // partial[k * RBLK + b] = sum over block b's chunk of A[k][i] * x[i]
 __global__ void __launch_bounds__(RB) multi_dot_partial(const double* __restrict__ A, long long lda, int m,
@@ -589,7 +594,6 @@ struct tci_ctx {
   long long launch_count = 0;    // kernels this context has launched (sigma builds, Davidson, projections)
 
   ~tci_ctx() {
-    if (dotbuf) cudaFree(dotbuf);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (graph_exec_prof) cudaGraphExecDestroy(graph_exec_prof);
@@ -597,6 +601,8 @@ struct tci_ctx {
     for (auto e : step_ev) cudaEventDestroy(e);
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    std::lock_guard<std::mutex> lk(g_capture_free_mu);
+    if (dotbuf) cudaFree(dotbuf);
     for (int b = 0; b < NUM_BUFS; ++b)
       if (buf[b]) cudaFree(buf[b]);
     for (void* p : owned) cudaFree(p);
@@ -785,6 +791,7 @@ struct tci_ctx {
       cudaGraph_t& g = profiling ? graph_prof : graph;
       cudaGraphExec_t& ge = profiling ? graph_exec_prof : graph_exec;
       if (!ge) {
+        std::lock_guard<std::mutex> lk(g_capture_free_mu);
         TCI_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         try {
           record_steps(profiling, true);
@@ -851,7 +858,10 @@ struct tci_ctx {
     if (plan.n_trip > 0 && nm > 0 &&
         !tci_tc_host::prepare(tc_trip, w32m, nm, uhi, ulo, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
-    TCI_CUDA(cudaFree(buf[BUF_W]));
+    {
+      std::lock_guard<std::mutex> lk(g_capture_free_mu);
+      TCI_CUDA(cudaFree(buf[BUF_W]));
+    }
     bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
     buf[BUF_W] = nullptr;
   }
@@ -1038,6 +1048,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     // init-only buffers
     for (int b : {BUF_X, BUF_L, BUF_LE, BUF_LI}) {
       if (ctx->buf[b]) {
+        std::lock_guard<std::mutex> lk(g_capture_free_mu);
         TCI_CUDA(cudaFree(ctx->buf[b]));
         ctx->bytes_held -= (double)P.buf_size[b] * sizeof(double);
         ctx->buf[b] = nullptr;
@@ -1242,6 +1253,8 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
     ctx->ensure_scratch(cap + 4);
     double *Cs = nullptr, *HCs = nullptr, *r = nullptr, *tmpC = nullptr, *tmpH = nullptr;
     auto free_all = [&]() {
+      cudaStreamSynchronize(ctx->stream);
+      std::lock_guard<std::mutex> lk(g_capture_free_mu);
       for (double* p : {Cs, HCs, r, tmpC, tmpH})
         if (p) cudaFree(p);
     };
@@ -1483,7 +1496,10 @@ int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const doub
     const int64_t need = m * (RBLK + 1);
     if (need > ctx->dotbuf_cap) {
       TCI_CUDA(cudaStreamSynchronize(ctx->stream));
-      if (ctx->dotbuf) TCI_CUDA(cudaFree(ctx->dotbuf));
+      if (ctx->dotbuf) {
+        std::lock_guard<std::mutex> lk(g_capture_free_mu);
+        TCI_CUDA(cudaFree(ctx->dotbuf));
+      }
       ctx->dotbuf = nullptr;
       ctx->dotbuf_cap = 0;
       if (cudaMalloc(&ctx->dotbuf, need * sizeof(double)) != cudaSuccess)
