@@ -55,6 +55,9 @@ TOL_RESIDUAL, TOL_ENERGY = 1e-6, 1e-8
 # GPU solve's iteration count at 1 root); converts the oracle's sigma time
 # into a solve time for the CPU arm
 SIGMA_BUILDS_PER_SOLVE = 33
+# ncu DRAM bytes (read + write) of one launch over its algorithmic bytes (the W operators), measured at 120
+# virtuals: FP64 split-K all-external 845.1 MB / 829.5 MB; tcgen05 all-external 219.2 MB / 211.0 MB
+TRAFFIC_RATIO = {"fp64": 845.142 / 829.498, "tf32x3": 219.224 / 210.954}
 
 
 def deck_and_operator(molecular=False):
@@ -357,7 +360,9 @@ def main():
              "ms_per_build": 1e3 * m["t_total"] / args.sigma_builds,
              "sigma_tflops": st["flops_per_sigma"] * args.sigma_builds * world / m["t_total"] / 1e12,
              "roofline": {"kernel": kernel, "bound": "hbm", "achieved": bytes_ / t_dom / 1e9, "peak": hbm,
-                          "unit": "GB/s", "frac": bytes_ / t_dom / 1e9 / hbm, "traffic": None,
+                          "unit": "GB/s", "frac": bytes_ / t_dom / 1e9 / hbm,
+                          "traffic": TRAFFIC_RATIO[f] * bytes_, "algorithmic_bytes": bytes_,
+                          "traffic_source": "ncu dram read+write ratio at 120 virtuals x full-size bytes",
                           "peak_kind": peak_kind, "ms": 1e3 * t_dom},
              "launches_per_build": m["launches"] / args.sigma_builds,
              "step_ms": {k: round(v, 4) for k, v in sorted(m["prof"].items(), key=lambda kv: -kv[1])[:12]},

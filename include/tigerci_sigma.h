@@ -181,7 +181,13 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len);
 /* Waits for the context's stream and reports a device-side failure recorded
  * by a bounded wait (TCI_ERR_TIMEOUT), else 0. */
 int tci_check(tci_ctx* ctx);
+/* on: bit 0 times the sigma plan steps (tci_step_times); bit 1 times the
+ * phases of tci_davidson / tci_davidson_ex (synchronising the stream at each
+ * phase boundary), read with tci_davidson_phase_times: ms[8] = set-up, sigma,
+ * projections, subspace eigensolve, residual, preconditioner + Gram-Schmidt,
+ * restart, finish.  Both reset the accumulated times. */
 int tci_profile(tci_ctx* ctx, int64_t on);
+int tci_davidson_phase_times(const tci_ctx* ctx, double* ms, int64_t len);
 int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps, int64_t* nbuilds);
 int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len);
 void tci_destroy(tci_ctx* ctx);

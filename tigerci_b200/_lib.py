@@ -50,6 +50,7 @@ EXPORTS = [
     "tci_dots_noalloc",
     "tci_ctx_stats",
     "tci_profile",
+    "tci_davidson_phase_times",
     "tci_step_times",
     "tci_step_name",
     "tci_destroy",
@@ -123,6 +124,7 @@ def lib():
         L.tci_dots_noalloc.argtypes = [P, i64, i64, P, i64, P, P]
         L.tci_ctx_stats.argtypes = [P, P, i64]
         L.tci_profile.argtypes = [P, i64]
+        L.tci_davidson_phase_times.argtypes = [P, P, i64]
         L.tci_step_times.argtypes = [P, P, i64, P, P]
         L.tci_step_name.argtypes = [P, i64, C.c_char_p, i64]
         L.tci_destroy.argtypes = [P]

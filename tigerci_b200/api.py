@@ -227,9 +227,17 @@ class SigmaBuilder:
                                     ptr(v) if v is not None else None, C.byref(it)))
         return e, v, it.value
 
-    def profile(self, on: bool = True):
-        """Per-step CUDA-event timing of subsequent sigma builds."""
-        check(lib().tci_profile(self._h, 1 if on else 0))
+    def profile(self, on: bool = True, davidson_phases: bool = False):
+        """Per-step CUDA-event timing of subsequent sigma builds; with
+        davidson_phases, wall time per Davidson phase (stream synchronised at
+        each phase boundary)."""
+        check(lib().tci_profile(self._h, (1 if on else 0) | (2 if davidson_phases else 0)))
+
+    def davidson_phase_times(self) -> dict:
+        ms = np.zeros(8)
+        check(lib().tci_davidson_phase_times(self._h, ptr(ms), 8))
+        keys = ["setup", "sigma", "projection", "subspace_eig", "residual", "precondition_mgs", "restart", "finish"]
+        return dict(zip(keys, ms.tolist()))
 
     def step_times(self) -> list:
         """[(step name, accumulated ms)] and the number of profiled builds."""

@@ -592,6 +592,9 @@ struct tci_ctx {
   std::vector<double> step_ms;          // accumulated per sigma step
   long long profiled_builds = 0;
   long long launch_count = 0;    // kernels this context has launched (sigma builds, Davidson, projections)
+  bool dav_phases = false;       // time the Davidson phases (stream synchronised at each boundary)
+  double dav_ms[8] = {};         // setup, sigma, projection, subspace eigensolve, residual,
+                                 // preconditioner + Gram-Schmidt, restart, finish
 
   ~tci_ctx() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -1251,6 +1254,17 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
     const int keep = (int)std::min<i64>(2 * nroots, n);  // vectors kept by a collapse
     ctx->ensure_diag();
     ctx->ensure_scratch(cap + 4);
+    // phase timing (tci_profile bit 1): the stream is synchronised at every boundary
+    auto tp = std::chrono::steady_clock::now();
+    int cur_phase = 0;
+    auto mark = [&](int ph) {
+      if (!ctx->dav_phases) return;
+      TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+      const auto t = std::chrono::steady_clock::now();
+      ctx->dav_ms[cur_phase] += std::chrono::duration<double, std::milli>(t - tp).count();
+      tp = t;
+      cur_phase = ph;
+    };
     double *Cs = nullptr, *HCs = nullptr, *r = nullptr, *tmpC = nullptr, *tmpH = nullptr;
     auto free_all = [&]() {
       cudaStreamSynchronize(ctx->stream);
@@ -1302,7 +1316,9 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
         for (int q = 0; q < nroots; ++q) {
           if (conv[q]) continue;
           const int index = root2index[q];
+          mark(1);
           ctx->sigma_of(Cs + (size_t)index * n, HCs + (size_t)index * n);
+          mark(2);
           ctx->multi_dot(Cs, n, index + 1, HCs + (size_t)index * n, n, col.data());
           for (int k = 0; k <= index; ++k) hsub[(size_t)k * cap + index] = hsub[(size_t)index * cap + k] = col[k];
         }
@@ -1313,6 +1329,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
           Vprev = V;
           mprev = (int)w.size();
         }
+        mark(3);
         jacobi_eigh(h, num_vec, w, V);
         for (int q = 0; q < nroots; ++q) {
           dE[q] = std::fabs(w[q] - energy[q]);
@@ -1322,6 +1339,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
         if (over_budget || num_vec + nroots > cap) {
           // restart_davidson_subspace: new basis {current, previous} per unconverged root, {current} per
           // converged root, as coefficient vectors in the present (orthonormal) basis
+          mark(6);
           restarted[it] = 1;
           // (the current vectors go first so that a full subspace never drops one of them)
           std::vector<std::vector<double>> B;
@@ -1391,6 +1409,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
         const int subspace_size = num_vec;
         for (int q = 0; q < nroots; ++q) {
           if (conv[q]) continue;
+          mark(4);
           // residual r = sum_k a_k (Hc_k - E c_k)
           std::vector<double> ca(subspace_size), cb(subspace_size);
           for (int k = 0; k < subspace_size; ++k) {
@@ -1416,6 +1435,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
             conv[q] = 1;
             continue;
           }
+          mark(5);
           precondition_kernel<<<G, TB, 0, st>>>(r, ctx->hd, energy[q], n);
           ctx->launch_count++;
           TCI_CUDA(cudaGetLastError());
@@ -1438,6 +1458,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
         for (int q = 0; q < nroots; ++q) all = all && conv[q];
         if (all) break;
       }
+      mark(7);
       ctx->check_tc_status();
       for (int q = 0; q < nroots; ++q) energies[q] = energy[q];
       if (iterations) *iterations = std::min<i64>(it, maxit);
@@ -1460,6 +1481,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
       throw;
     }
     free_all();
+    mark(0);
     return TCI_OK;
   } catch (...) {
     return guard_status(std::current_exception());
@@ -1534,9 +1556,17 @@ int tci_check(tci_ctx* ctx) {
 
 int tci_profile(tci_ctx* ctx, int64_t on) {
   if (!ctx) return TCI_ERR_ARG;
-  ctx->profiling = on != 0;
+  ctx->profiling = (on & 1) != 0;
+  ctx->dav_phases = (on & 2) != 0;
   ctx->step_ms.assign(ctx->sigma.size(), 0.0);
   ctx->profiled_builds = 0;
+  for (double& v : ctx->dav_ms) v = 0.0;
+  return TCI_OK;
+}
+
+int tci_davidson_phase_times(const tci_ctx* ctx, double* ms, int64_t len) {
+  if (!ctx || !ms || len < 8) return TCI_ERR_ARG;
+  for (int i = 0; i < 8; ++i) ms[i] = ctx->dav_ms[i];
   return TCI_OK;
 }
 
