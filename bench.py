@@ -409,11 +409,16 @@ def main():
                 energies.append(float(e[0]))
                 iters.append(int(it))
         launches = sb.stats()["launches"] - launches0
+        # one more (untimed) solve with the phases timed (the stream is synchronised at each boundary)
+        sb.profile(False, davidson_phases=True)
+        sb.davidson(1, TOL_RESIDUAL, TOL_ENERGY)
+        phases = {k: round(v, 2) for k, v in sb.davidson_phase_times().items()}
+        sb.profile(False)
         sb.check()
         sb.close()
         t_total = max_over_ranks(sum(times))
         return dict(times=times, t_total=t_total, energy=energies[-1], energies=energies, iterations=iters,
-                    launches=launches, clk=clk, init_s=init_s)
+                    launches=launches, clk=clk, init_s=init_s, phases=phases)
 
     solves = {}
     for f in forms:
@@ -457,7 +462,7 @@ def main():
                 "iterations": m["iterations"][-1], "energy": m["energy"],
                 "energy_minus_fp64": (m["energy"] - e64) if e64 is not None else None,
                 "within_1uEh_of_fp64": meets.get(f), "init_s": m["init_s"],
-                "launches_per_solve": m["launches"] / args.steps}
+                "launches_per_solve": m["launches"] / args.steps, "phase_ms": m["phases"]}
 
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * bm["t_total"] / args.steps, "higher_is_better": True,

@@ -110,10 +110,13 @@ void tci_plan_destroy(tci_plan* plan);
  * (NULL = the legacy default stream). */
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out);
 /* As tci_sigma_init with options: options[0] = precision mode, 0 plain FP64
- * (default), 1 the all-external term on tcgen05 tensor cores with FP32 W
- * operators, 3xTF32 split products and FP64 promotion of the FP32 tensor-core
- * sums every options[1] k elements (multiple of 32, default 128)
- * (TCI_PRECISION_TF32X3); every other term stays FP64. */
+ * (default), 1 mixed (TCI_PRECISION_TF32X3): the integral contractions run on
+ * the tcgen05 tensor cores as 3xTF32 split products with FP32 accumulation
+ * promoted to FP64 every options[1] k elements (multiple of 32, default 128):
+ * the all-external term with FP32 W operators, and the three-, two- and
+ * one-external GEMM steps from their FP64 operands.  options[2] selects those
+ * other GEMM steps: 0 by size (default), 1 all of them, 2 none.  The coupling-
+ * coefficient products, gathers, scatters and reductions stay FP64. */
 #define TCI_PRECISION_FP64 0
 #define TCI_PRECISION_TF32X3 1
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
@@ -215,6 +218,7 @@ typedef struct {
   double schedule_only_ms;
   int64_t inject_worker_exit_at;     /* host fault injection: the worker thread that
                                         makes this admission (1-based) dies; 0 off   */
+  int64_t tc_gemms;                  /* tci_sigma_init_ex options[2] of every request */
 } tci_server_config;
 int tci_server_create(const tci_server_config* cfg, tci_server** out);
 /* Copies the deck and operator (the caller may free them on return); rejects

@@ -47,6 +47,8 @@ def lib():
                                          C.c_void_p]
         L.oracle_allext_sigma.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
+        L.oracle_allext_local_sigma.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
         L.oracle_set_dgemm.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
         _lib = L
@@ -221,4 +223,20 @@ def allext_sigma(space, nint, n, chol, c, nthreads=None, a_range=None):
     a0, a1 = a_range if a_range else (0, n)
     lib().oracle_allext_sigma(nint, n, chol.shape[1], chol.ctypes.data, len(heads), heads.ctypes.data,
                               c.ctypes.data, s.ctypes.data, a0, a1)
+    return s
+
+
+def allext_local_sigma(nint, chol, heads, dom_idx, c, head_range=None):
+    """Reference integral-form all-external sigma over pair domains (detci.c
+    oracle_allext_local_sigma).  heads: int64 rows (off_ab, off_aa, nsf_ab,
+    nsf_aa, nsing, dom_off, dom_len); dom_idx: concatenated sorted domains
+    (external indices); head_range=(h0, h1) restricts the heads (a sample)."""
+    heads = np.ascontiguousarray(np.asarray(heads, dtype=np.int64).reshape(-1, 7))
+    dom_idx = np.ascontiguousarray(np.asarray(dom_idx, dtype=np.int64))
+    chol = np.ascontiguousarray(chol, dtype=np.float64)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    s = np.zeros_like(c)
+    h0, h1 = head_range if head_range else (0, len(heads))
+    lib().oracle_allext_local_sigma(nint, chol.shape[1], chol.ctypes.data, len(heads), heads.ctypes.data,
+                                    dom_idx.ctypes.data, c.ctypes.data, s.ctypes.data, h0, h1)
     return s

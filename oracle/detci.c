@@ -194,6 +194,92 @@ void oracle_allext_sigma(int64_t nint, int64_t n, int64_t nchol, const double* c
 #undef PAIR
 }
 
+/* Local (pair-domain) all-external sigma, integral form.  Same arithmetic as
+ * oracle_allext_sigma, with every external index of head h restricted to its
+ * domain dom[h] (sorted virtual indices; local index = position in the list),
+ * as in ext_3_4_seg_loops_vec_lmo_res_2 (three_and_four_seg_mod_1.f90:3240-3518)
+ * with virtual_truncation (locist_mod.f90:358-451).  heads: 7 int64 per head
+ * (off_ab, off_aa, nsf_ab, nsf_aa, nsing, dom_off, dom_len); blocks of head h
+ * have dom_len-sized external dimensions.  Heads [h_begin, h_end) only (a
+ * sample).  The head loop is parallel: every head owns its sigma blocks. */
+void oracle_allext_local_sigma(int64_t nint, int64_t nchol, const double* chol, int64_t nh, const int64_t* heads,
+                               const int64_t* dom_idx, const double* c, double* sigma, int64_t h_begin,
+                               int64_t h_end) {
+  const double s2 = sqrt(2.0);
+  int64_t nmax = 1;
+  for (int64_t hh = 0; hh < nh; ++hh)
+    if (heads[7 * hh + 6] > nmax) nmax = heads[7 * hh + 6];
+#define PAIR(p, q) ((p) >= (q) ? (p) * ((p) + 1) / 2 + (q) : (q) * ((q) + 1) / 2 + (p))
+#pragma omp parallel
+  {
+    double* Lab = (double*)malloc(sizeof(double) * nmax * nchol);
+    double* Lcd = (double*)malloc(sizeof(double) * nmax * nchol);
+    double* V = (double*)malloc(sizeof(double) * nmax * nmax);
+    double* Vx = (double*)malloc(sizeof(double) * nmax * nmax);
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t hh = h_begin; hh < h_end; ++hh) {
+      const int64_t* H = heads + 7 * hh;
+      const int64_t off_ab = H[0], off_aa = H[1], nsf_ab = H[2], nsf_aa = H[3], nsing = H[4];
+      const int64_t* dom = dom_idx + H[5];
+      const int64_t n = H[6], nab = n * (n - 1) / 2;
+      const int64_t nk = nsf_ab > nsf_aa ? nsf_ab : nsf_aa;
+      for (int64_t a = 0; a < n; ++a) {
+        for (int64_t b = 0; b < n; ++b)
+          memcpy(Lab + b * nchol, chol + PAIR(nint + dom[a], nint + dom[b]) * nchol, sizeof(double) * nchol);
+        for (int64_t cc = 0; cc <= a; ++cc) {
+          for (int64_t d = 0; d < n; ++d)
+            memcpy(Lcd + d * nchol, chol + PAIR(nint + dom[cc], nint + dom[d]) * nchol, sizeof(double) * nchol);
+          if (g_dgemm) {
+            const int nn = (int)n, kk = (int)nchol;
+            const double one = 1.0, zero = 0.0;
+            g_dgemm("T", "N", &nn, &nn, &kk, &one, Lcd, &kk, Lab, &kk, &zero, V, &nn);
+          } else {
+            for (int64_t b = 0; b < n; ++b)
+              for (int64_t d = 0; d < n; ++d) {
+                const double* x = Lab + b * nchol;
+                const double* y = Lcd + d * nchol;
+                double acc = 0.0;
+                for (int64_t J = 0; J < nchol; ++J) acc += x[J] * y[J];
+                V[b * n + d] = acc;
+              }
+          }
+          for (int64_t b = 0; b < n; ++b)
+            for (int64_t d = 0; d < n; ++d) Vx[b * n + d] = V[d * n + b];
+          for (int64_t k = 0; k < nk; ++k) {
+            const int singlet = k < nsing;
+            const double* cab = (k < nsf_ab) ? c + off_ab + k * nab : NULL;
+            const double* caa = (k < nsf_aa) ? c + off_aa + k * n : NULL;
+            double acc = 0.0;
+            if (a != cc) {
+              if (!(k < nsf_ab)) continue;
+              for (int64_t b = 1; b < n; ++b)
+                for (int64_t d = 0; d < b; ++d) {
+                  const double cv = cab[b * (b - 1) / 2 + d];
+                  acc += cv * (singlet ? (V[b * n + d] + Vx[b * n + d]) : (V[b * n + d] - Vx[b * n + d]));
+                }
+              if (singlet && caa)
+                for (int64_t b = 0; b < n; ++b) acc += s2 * caa[b] * V[b * n + b];
+              sigma[off_ab + k * nab + a * (a - 1) / 2 + cc] += acc;
+            } else {
+              if (!singlet || !caa) continue;
+              if (cab)
+                for (int64_t b = 1; b < n; ++b)
+                  for (int64_t d = 0; d < b; ++d) acc += s2 * cab[b * (b - 1) / 2 + d] * V[b * n + d];
+              for (int64_t b = 0; b < n; ++b) acc += caa[b] * V[b * n + b];
+              sigma[off_aa + k * n + a] += acc;
+            }
+          }
+        }
+      }
+    }
+    free(Lab);
+    free(Lcd);
+    free(V);
+    free(Vx);
+  }
+#undef PAIR
+}
+
 int oracle_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -1,5 +1,6 @@
-"""Mixed-precision all-external product on tcgen05 (3xTF32 with FP64 block
-promotion) against the plain-FP64 sigma build."""
+"""Mixed-precision sigma on tcgen05 (3xTF32 with FP64 block promotion: the
+all-external product and the other integral contractions) against the
+plain-FP64 sigma build."""
 import numpy as np
 import pytest
 
@@ -9,25 +10,53 @@ from tigerci_b200.synthetic import random_civec, synthetic_operator
 
 pytestmark = pytest.mark.gpu
 
-# The mixed form only changes the all-external product: FP32 storage of W
-# (2^-24) and split TF32 products (~2^-22) bound its relative error.
+# With only the all-external product on the tensor cores (tc_gemms="none") the
+# error comes from FP32 storage of W (2^-24) and split TF32 products (~2^-22).
 MIXED_RTOL = 2e-6
+# With every contraction on the tensor cores, bounded relative to the
+# two-electron part of sigma (the one-electron part stays FP64).
+MIXED_2E_RTOL = 2e-5
 
 
-def _pair(deck, h, L):
+def _pair(deck, h, L, tc_gemms="by_size"):
     a = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="fp64")
-    b = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="tf32x3")
+    b = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="tf32x3", tc_gemms=tc_gemms)
     return a, b
+
+
+def _two_electron_sigma(deck, h, L, v):
+    """sigma(h, L) - sigma(h, 0): the part of H v the integral contractions produce."""
+    full = T.SigmaBuilder(deck, T.Operator(h, L), device=0)
+    one = T.SigmaBuilder(deck, T.Operator(h, np.zeros_like(L)), device=0)
+    s = full.sigma(v) - one.sigma(v)
+    full.close()
+    one.close()
+    return s
 
 
 @pytest.mark.parametrize("c", [SMALL_CASES[2], SMALL_CASES[3], SMALL_CASES[8]], ids=case_id)
 def test_mixed_small_cases(c, need_gpu):
     h, L = synthetic_operator(c["no"], 10, seed=11, scale=0.3, diag_range=(-3, 1), offdiag_sigma=0.1)
-    a, b = _pair(product_deck(c), h, L)
+    a, b = _pair(product_deck(c), h, L, tc_gemms="none")
     x = random_civec(a.n, 1)
     sa, sb = a.sigma(x), b.sigma(x)
     b.check()
     assert np.abs(sa - sb).max() <= MIXED_RTOL * np.abs(sa).max()
+
+
+@pytest.mark.parametrize("c", [SMALL_CASES[2], SMALL_CASES[3], SMALL_CASES[7], SMALL_CASES[8]], ids=case_id)
+def test_mixed_every_contraction_on_tensor_cores(c, need_gpu):
+    """tc_gemms="all": the three-, two- and one-external GEMM steps (every
+    operand orientation, K-segmented sums, alpha and beta) on tcgen05 too."""
+    h, L = synthetic_operator(c["no"], 10, seed=11, scale=0.3, diag_range=(-3, 1), offdiag_sigma=0.1)
+    deck = product_deck(c)
+    a, b = _pair(deck, h, L, tc_gemms="all")
+    x = random_civec(a.n, 1)
+    sa, sb = a.sigma(x), b.sigma(x)
+    b.check()
+    s2 = _two_electron_sigma(deck, h, L, x)
+    assert np.linalg.norm(sa - sb) <= MIXED_2E_RTOL * np.linalg.norm(s2)
+    assert np.array_equal(sb, b.sigma(x))  # deterministic
 
 
 def test_mixed_medium_case_and_determinism(need_gpu):
@@ -38,7 +67,8 @@ def test_mixed_medium_case_and_determinism(need_gpu):
     x = random_civec(a.n, 3)
     sa, sb = a.sigma(x), b.sigma(x)
     b.check()
-    assert np.abs(sa - sb).max() <= MIXED_RTOL * np.abs(sa).max()
+    s2 = _two_electron_sigma(deck, h, L, x)
+    assert np.linalg.norm(sa - sb) <= MIXED_2E_RTOL * np.linalg.norm(s2)
     assert np.array_equal(sb, b.sigma(x))
 
 
@@ -61,11 +91,11 @@ def _allext_energy(deck, h, L, nint, v):
 
 
 def test_mixed_sigma_error_relative_to_allext_part(need_gpu):
-    """The mixed form differs from FP64 only in the all-external product; its
+    """With only the all-external product on the tensor cores, the mixed form's
     error is bounded relative to that product (FP32 storage + 3xTF32)."""
     deck = T.Deck(16 + 60, 8, 8, 16, 1, ["2" * 8 + "0" * 8])
     h, L = synthetic_operator(76, 200, seed=1234)
-    a, b = _pair(deck, h, L)
+    a, b = _pair(deck, h, L, tc_gemms="none")
     x = random_civec(a.n, 5)
     d = b.sigma(x) - a.sigma(x)
     s4 = _allext_sigma(deck, h, L, 16, x)
@@ -77,7 +107,7 @@ def test_mixed_davidson_within_one_microhartree_physical_scale(need_gpu):
     mixed form's roots agree with plain FP64 within 1 microhartree."""
     deck = T.Deck(16 + 60, 8, 8, 16, 1, ["2" * 8 + "0" * 8])
     h, L = synthetic_operator(76, 200, seed=1234, scale=0.02, diag_range=(-2.0, 1.0), offdiag_sigma=0.02)
-    a, b = _pair(deck, h, L)
+    a, b = _pair(deck, h, L, tc_gemms="all")
     ea, va, _ = a.davidson(2, 1e-7, 1e-11, want_vectors=True)
     eb, _, _ = b.davidson(2, 1e-7, 1e-11)
     b.check()
@@ -88,12 +118,12 @@ def test_mixed_davidson_within_one_microhartree_physical_scale(need_gpu):
 
 def test_mixed_davidson_relative_bound_large_scale(need_gpu):
     """At the benchmark's unit-variance scale the mixed roots agree with FP64
-    within the all-external product's error bound: |dE| <= eps * |H_allext v|."""
+    within the contractions' error bound: |dE| <= eps * |H_2e v|."""
     deck = T.Deck(16 + 60, 8, 8, 16, 1, ["2" * 8 + "0" * 8])
     h, L = synthetic_operator(76, 200, seed=1234)
-    a, b = _pair(deck, h, L)
+    a, b = _pair(deck, h, L, tc_gemms="all")
     ea, va, _ = a.davidson(2, 1e-6, 1e-10, want_vectors=True)
     eb, _, _ = b.davidson(2, 1e-6, 1e-10)
     b.check()
-    s4 = np.linalg.norm(_allext_sigma(deck, h, L, 16, va[0]))
-    assert np.abs(ea - eb).max() < 1e-6 * s4 + 1e-8
+    s2 = np.linalg.norm(_two_electron_sigma(deck, h, L, va[0]))
+    assert np.abs(ea - eb).max() < 1e-6 * s2 + 1e-8

@@ -48,8 +48,9 @@ def _run(cmd):
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
-    headers = glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True) + glob.glob(
-        os.path.join(HERE, "..", "include", "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True) +
+               glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True) +
+               glob.glob(os.path.join(HERE, "..", "include", "*.h")))
     objs = []
     for src in sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp"))):
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")

@@ -7,9 +7,11 @@
 // W tile is split in shared memory into TF32 hi/lo parts; U arrives pre-split.
 // Three kind::tf32 MMAs per k-step (hi*hi + hi*lo + lo*hi) accumulate FP32 in
 // TMEM; every KBLOCK elements of k the partial sums are read back with
-// tcgen05.ld and added into the FP64 output (promotion keeps the FP32
-// accumulation error at the block length).  The product is HBM bound: W is
-// read exactly once.
+// tcgen05.ld and added into FP64 accumulators held in registers (promotion
+// keeps the FP32 accumulation error at the block length), which are written
+// to the output once at the end.  The product is HBM bound: W is read exactly
+// once.  One launch covers both operators (W+ with the singlet blocks, W-
+// with the triplet blocks), so their tiles share the waves.
 //
 // Warp roles (320 threads): warps 0-3 epilogue (TMEM lane quadrants 0-3),
 // warps 4-7 hi/lo split, warp 8 TMA producer, warp 9 TMEM allocator + MMA
@@ -18,6 +20,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -109,11 +112,29 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 // Error codes written to the kernel's status word.
 enum : int { ST_OK = 0, ST_TIMEOUT_FULL = 1, ST_TIMEOUT_CONV = 2, ST_TIMEOUT_EMPTY = 3, ST_TIMEOUT_D = 4, ST_TIMEOUT_DE = 5 };
 
+// One product of the launch: Y (m x np, row pitch ldy) = U W over `tiles`
+// panels of BM W rows.
+struct Product {
+  int np, m, tiles;
+  double* Y;
+  long long ldy;
+};
+
 __global__ void __launch_bounds__(NTHREADS, 1)
-    allext_tf32x3_kernel(const __grid_constant__ CUtensorMap wmap, const __grid_constant__ CUtensorMap uhi_map,
-                         const __grid_constant__ CUtensorMap ulo_map, int np, int m, double* __restrict__ Y,
-                         long long ldy, int* __restrict__ status, int kb_per_block) {
+    allext_tf32x3_kernel(const __grid_constant__ CUtensorMap wmap0, const __grid_constant__ CUtensorMap uhi_map0,
+                         const __grid_constant__ CUtensorMap ulo_map0, const __grid_constant__ CUtensorMap wmap1,
+                         const __grid_constant__ CUtensorMap uhi_map1, const __grid_constant__ CUtensorMap ulo_map1,
+                         Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
   const int KB_PER_BLOCK = kb_per_block;
+  // which product this CTA works on (uniform over the CTA: the early exit precedes all set-up)
+  const bool second = (int)blockIdx.x >= p0.tiles;
+  const Product P = second ? p1 : p0;
+  const CUtensorMap* wmap = second ? &wmap1 : &wmap0;
+  const CUtensorMap* uhi_map = second ? &uhi_map1 : &uhi_map0;
+  const CUtensorMap* ulo_map = second ? &ulo_map1 : &ulo_map0;
+  const int np = P.np, m = P.m;
+  const int ublock = blockIdx.y;       // which group of BN CI blocks
+  if (ublock * BN >= m) return;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
@@ -121,12 +142,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint64_t* empty = conv + STAGES;
   uint64_t* dfull = empty + STAGES;   // 2
   uint64_t* dempty = dfull + 2;       // 2
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(dempty + 2);
+  uint64_t* mma_done = dempty + 2;    // 1: drain of the MMAs in flight after an abort
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row0 = blockIdx.x * BM;
-  const int ublock = blockIdx.y;       // which group of BN CI blocks
+  const int row0 = (second ? (int)blockIdx.x - p0.tiles : (int)blockIdx.x) * BM;
   const int nk = (np + BK - 1) / BK;
   const int nblocks = (nk + KB_PER_BLOCK - 1) / KB_PER_BLOCK;
 
@@ -140,6 +161,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_init(&dfull[b], 1);
       mbar_init(&dempty[b], 4);
     }
+    mbar_init(mma_done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -162,6 +184,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 8) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
+      int last = -1;  // last k-step whose copies were issued
       for (int kb = 0; kb < nk && !aborted(); ++kb) {
         const int s = kb % STAGES;
         if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1)) {
@@ -170,9 +193,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         uint8_t* st = base + s * STAGE_BYTES;
         mbar_expect_tx(&full[s], W_BYTES + 2 * U_BYTES);
-        tma_load_2d(st, &wmap, &full[s], kb * BK, row0);
-        tma_load_2d(st + 2 * W_BYTES, &uhi_map, &full[s], kb * BK, ublock * BN);
-        tma_load_2d(st + 2 * W_BYTES + U_BYTES, &ulo_map, &full[s], kb * BK, ublock * BN);
+        tma_load_2d(st, wmap, &full[s], kb * BK, row0);
+        tma_load_2d(st + 2 * W_BYTES, uhi_map, &full[s], kb * BK, ublock * BN);
+        tma_load_2d(st + 2 * W_BYTES + U_BYTES, ulo_map, &full[s], kb * BK, ublock * BN);
+        last = kb;
+      }
+      if (aborted()) {
+        // the copies of the last STAGES issued k-steps may still be landing: wait (bounded) for them
+        // before the shared memory is released
+        for (int kb = (last - STAGES + 1 > 0 ? last - STAGES + 1 : 0); kb <= last; ++kb)
+          mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
       }
     }
   } else if (warp >= 4 && warp < 8) {
@@ -187,13 +217,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       uint32_t* whi = reinterpret_cast<uint32_t*>(base + s * STAGE_BYTES);
       uint32_t* wlo = reinterpret_cast<uint32_t*>(base + s * STAGE_BYTES + W_BYTES);
       // a warp per 128-byte row: lane l holds element l (conflict free; the
-      // swizzle permutes 16-byte chunks within the row, lo keeps the same layout)
-      for (int r = cw; r < BM; r += 4) {
-        const uint32_t x = whi[r * BK + lane];
-        const uint32_t hi = x & 0xFFFFE000u;
-        const float lo = __uint_as_float(x) - __uint_as_float(hi);
-        whi[r * BK + lane] = hi;
-        wlo[r * BK + lane] = __float_as_uint(lo);
+      // swizzle permutes 16-byte chunks within the row, lo keeps the same layout).
+      // Eight rows per batch: their loads are issued before any store, so the
+      // shared-memory latency is paid once per batch.
+#pragma unroll
+      for (int r0 = cw; r0 < BM; r0 += 4 * 8) {
+        uint32_t x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = whi[(r0 + 4 * i) * BK + lane];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const uint32_t hi = x[i] & 0xFFFFE000u;
+          const float lo = __uint_as_float(x[i]) - __uint_as_float(hi);
+          whi[(r0 + 4 * i) * BK + lane] = hi;
+          wlo[(r0 + 4 * i) * BK + lane] = __float_as_uint(lo);
+        }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -229,10 +267,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         mma_commit(&empty[s]);
         if ((kb % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || kb == nk - 1) mma_commit(&dfull[buf]);
       }
+      if (aborted()) {
+        // MMAs issued before the abort may still be writing TMEM: wait (bounded) for all of them
+        mma_commit(mma_done);
+        mbar_wait(mma_done, 0);
+      }
     }
   } else {
-    // ---------------- epilogue: FP32 block sums -> FP64 output ----------------
+    // ---------------- epilogue: FP32 block sums -> FP64 register accumulators ----------------
     const int r = row0 + warp * 32 + lane;  // W row owned by this thread
+    double acc[BN];
+#pragma unroll
+    for (int t = 0; t < BN; ++t) acc[t] = 0.0;
     for (int blk = 0; blk < nblocks && !aborted(); ++blk) {
       const int buf = blk & 1;
       if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
@@ -250,21 +296,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
               "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (r < np) {
 #pragma unroll
-          for (int t = 0; t < 16; ++t) {
-            const int j = ublock * BN + c * 16 + t;
-            if (j < m) {
-              double* y = Y + (long long)j * ldy + r;
-              const double x = (double)__uint_as_float(v[t]);
-              *y = (blk == 0) ? x : *y + x;
-            }
-          }
-        }
+        for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
       }
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
       if (lane == 0) mbar_arrive(&dempty[buf]);
+    }
+    if (!aborted() && r < np) {
+#pragma unroll
+      for (int t = 0; t < BN; ++t) {
+        const int j = ublock * BN + t;
+        if (j < m) P.Y[(long long)j * P.ldy + r] = acc[t];
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -394,11 +438,26 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
   return true;
 }
 
-cudaError_t launch(const AllextTc& t, cudaStream_t st) {
+cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
+  if (!a && !b) return cudaSuccess;
+  if (!a) std::swap(a, b);
   const int smem = tci_tc::STAGES * tci_tc::STAGE_BYTES + 1024 + 256;
-  dim3 grid((unsigned)((t.np + tci_tc::BM - 1) / tci_tc::BM), (unsigned)(padded_rows(t.m) / tci_tc::BN));
-  tci_tc::allext_tf32x3_kernel<<<grid, tci_tc::NTHREADS, smem, st>>>(t.wmap, t.uhi, t.ulo, (int)t.np, (int)t.m, t.y,
-                                                                     t.np, t.status, (int)(t.kblock / tci_tc::BK));
+  auto product = [](const AllextTc* t) {
+    tci_tc::Product p{};
+    if (!t) return p;
+    p.np = (int)t->np;
+    p.m = (int)t->m;
+    p.tiles = (int)((t->np + tci_tc::BM - 1) / tci_tc::BM);
+    p.Y = t->y;
+    p.ldy = t->np;
+    return p;
+  };
+  const tci_tc::Product p0 = product(a), p1 = product(b);
+  const int64_t ub = std::max(padded_rows(a->m), b ? padded_rows(b->m) : 0) / tci_tc::BN;
+  dim3 grid((unsigned)(p0.tiles + p1.tiles), (unsigned)ub);
+  const AllextTc* c = b ? b : a;  // maps of the second product (unused when there is none)
+  tci_tc::allext_tf32x3_kernel<<<grid, tci_tc::NTHREADS, smem, st>>>(a->wmap, a->uhi, a->ulo, c->wmap, c->uhi, c->ulo,
+                                                                     p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
   return cudaGetLastError();
 }
 

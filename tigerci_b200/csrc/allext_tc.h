@@ -22,6 +22,8 @@ cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st
 cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo, cudaStream_t st);
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
              int* status, int64_t kblock, std::string& err);
-cudaError_t launch(const AllextTc& t, cudaStream_t st);
+// Both products in one launch (either may be null; they must share the status
+// word and promotion block).
+cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);
 
 }  // namespace tci_tc_host

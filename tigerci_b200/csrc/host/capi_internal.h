@@ -15,6 +15,8 @@ void operator_from_c(const tci_operator* op, const CsfSpace& sp, Operator& out);
 // (chol: the host Cholesky vectors the plan was built for).
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
                   tci_ctx** out);
+// Selects the GEMM steps that run on the tensor cores in the mixed form (tci_sigma_init_ex options[2]).
+void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode);
 // Device bytes of such a context: peak during set-up and held afterwards.
 void ctx_device_bytes(const Plan& plan, int64_t precision, double* peak, double* resident);
 }  // namespace tci

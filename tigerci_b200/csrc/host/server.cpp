@@ -220,6 +220,7 @@ struct tci_server {
           tci_ctx* ctx = nullptr;
           status = ctx_from_plan(std::move(*r->sp), std::move(*r->plan), r->chol.data(), cfg.device, cfg.precision,
                                  128, &ctx);
+          if (status == TCI_OK) ctx_set_tc_gemms(ctx, cfg.tc_gemms);
           if (status == TCI_OK)
             status = tci_davidson_ex(ctx, r->nroots, r->tol_r, r->tol_e, r->maxit, r->subspace_bytes, &r->cancel,
                                      e.data(), nullptr, &iters);
@@ -302,7 +303,8 @@ int tci_server_create(const tci_server_config* cfg, tci_server** out) {
   if (!cfg || !out) return TCI_ERR_ARG;
   *out = nullptr;
   if (cfg->slots < 1 || cfg->slots > 64 || cfg->planners < 1 || cfg->planners > 64 || cfg->hbm_budget_bytes <= 0 ||
-      cfg->precision < 0 || cfg->precision > 1 || cfg->device < 0 || cfg->schedule_only_ms < 0) {
+      cfg->precision < 0 || cfg->precision > 1 || cfg->device < 0 || cfg->schedule_only_ms < 0 ||
+      cfg->tc_gemms < 0 || cfg->tc_gemms > 2) {
     set_error("tci_server_create: slots and planners in 1..64, a positive budget, a known precision");
     return TCI_ERR_ARG;
   }

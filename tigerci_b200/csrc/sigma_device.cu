@@ -23,6 +23,8 @@
 
 #include "../../include/tigerci_sigma.h"
 #include "allext_tc.h"
+#include "gemm_tables.h"
+#include "gemm_tc.h"
 #include "host/capi_internal.h"
 #include "host/plan.h"
 
@@ -32,26 +34,16 @@ using namespace tci;
   do {                                                                                       \
     cudaError_t _e = (call);                                                                 \
     if (_e != cudaSuccess)                                                                   \
-      throw Error(TCI_ERR_CUDA, std::string(#call) + " failed: " + cudaGetErrorString(_e)); \
+      throw Error(TCI_ERR_CUDA, std::string(#call) + " (sigma_device.cu:" + std::to_string(__LINE__) + \
+                                    ") failed: " + cudaGetErrorString(_e));                            \
   } while (0)
 
 namespace {
 
 // ----------------------------------------------------------------------------
 // device-side table layouts (plain structs, 8-byte fields)
-struct DGemmProblem {
-  double* C;
-  long long ldc, M, N, tiles_n, tile_begin;
-  double beta;
-  long long seg_begin, seg_end;
-};
-struct DGemmSeg {
-  const double* A;
-  const double* B;
-  long long lda, ldb, K;
-  int tA, tB;
-  double alpha;
-};
+using tci_dev::DGemmProblem;
+using tci_dev::DGemmSeg;
 struct DAxpyTarget {
   double* dst;             // already offset by base
   long long base;          // offset of this chunk inside the target range (applied to sources)
@@ -533,6 +525,11 @@ struct DevStep {
   int nprob = 0;
   long long ntiles = 0;
   int cfg = 0;  // 0: 64x128 tiles, 1: 128x64 tiles
+  // the same problems tiled for the tensor-core kernel (mixed-precision form)
+  DGemmProblem* probs_tc = nullptr;
+  DGemmSeg* segs_tc = nullptr;
+  long long ntiles_tc = 0;
+  bool tc_ok = false;  // worth the tensor cores: enough work and tiles mostly full
   // AXPY / DOT
   DAxpyTarget* at = nullptr;
   DAxpySource* as = nullptr;
@@ -575,10 +572,13 @@ struct tci_ctx {
   bool use_graph = true;                // replay the sigma steps as one CUDA graph
   int64_t precision = 0;                // 0 plain FP64; 1 all-external on tcgen05 (3xTF32, FP64 promotion)
   int64_t tc_kblock = 128;              // k elements per FP64 promotion block of the tensor-core product
+  int64_t tc_mode = 0;                  // precision 1: other GEMM steps on the tensor cores by size (0), all (1), none (2)
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
-  float* uhi = nullptr;                 // split CI blocks for the tensor-core product
+  float* uhi = nullptr;                 // split singlet CI blocks for the tensor-core product
   float* ulo = nullptr;
+  float* uhi_t = nullptr;               // split triplet CI blocks
+  float* ulo_t = nullptr;
   int* tc_status = nullptr;
   tci_tc_host::AllextTc tc_sing, tc_trip;
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
@@ -640,7 +640,7 @@ struct tci_ctx {
         const i64 tm = (g.M + BMh - 1) / BMh, tn = (g.N + BNh - 1) / BNh;
         if (g.M <= 0 || g.N <= 0) continue;
         check_range(g.c, g.offC, (g.M - 1) * g.ldc + g.N);
-        pr.push_back(DGemmProblem{ptr(g.c, g.offC), g.ldc, g.M, g.N, tn, tiles, g.beta, g.seg_begin, g.seg_end});
+        pr.push_back(DGemmProblem{ptr(g.c, g.offC), g.ldc, g.M, g.N, tn, tiles, g.beta, g.seg_begin, g.seg_end, 0});
         tiles += tm * tn;
       }
       for (auto& g : s.gs) sg.push_back(DGemmSeg{ptr(g.a, g.offA), ptr(g.b, g.offB), g.lda, g.ldb, g.K, g.tA, g.tB, g.alpha});
@@ -661,6 +661,45 @@ struct tci_ctx {
       d.segs = upload(sg, owned);
       d.nprob = (int)pr.size();
       d.ntiles = tiles;
+      if (s.name != "all-external" && !pr.empty()) {
+        // tensor-core tables: 128 x 64 tiles; a problem whose M fills the 128-row tiles worse than its N
+        // would is computed transposed (C^T = B^T A^T) with its own copy of the segments
+        const i64 TM = tci_gtc_host::tile_m(), TN = tci_gtc_host::tile_n();
+        std::vector<DGemmProblem> pt = pr;
+        std::vector<DGemmSeg> st;
+        long long tt = 0;
+        double flops = 0, useful = 0, issued = 0;
+        auto fill = [&](i64 M, i64 N) {
+          return (double)M * (double)N /
+                 ((double)((M + TM - 1) / TM * TM) * (double)((N + TN - 1) / TN * TN));
+        };
+        for (auto& g : pt) {
+          const bool tr = fill(g.N, g.M) > fill(g.M, g.N);
+          const long long b = (long long)st.size();
+          for (long long q = g.seg_begin; q < g.seg_end; ++q) {
+            DGemmSeg x = sg[q];
+            if (tr) x = DGemmSeg{x.B, x.A, x.ldb, x.lda, x.K, x.tB ? 0 : 1, x.tA ? 0 : 1, x.alpha};
+            st.push_back(x);
+          }
+          g.seg_begin = b;
+          g.seg_end = (long long)st.size();
+          if (tr) std::swap(g.M, g.N);
+          g.trans_c = tr ? 1 : 0;
+          const i64 tm = (g.M + TM - 1) / TM, tn = (g.N + TN - 1) / TN;
+          g.tiles_n = tn;
+          g.tile_begin = tt;
+          tt += tm * tn;
+          double k = 0;
+          for (long long q = g.seg_begin; q < g.seg_end; ++q) k += (double)st[q].K;
+          flops += 2.0 * (double)g.M * (double)g.N * k;
+          useful += (double)g.M * (double)g.N * k;
+          issued += (double)(tm * TM) * (double)(tn * TN) * k;
+        }
+        d.probs_tc = upload(pt, owned);
+        d.segs_tc = upload(st, owned);
+        d.ntiles_tc = tt;
+        d.tc_ok = flops >= 5e7 && useful >= 0.25 * issued;
+      }
     } else if (s.kind == STEP_AXPY) {
       std::vector<DAxpyTarget> t;
       std::vector<DAxpySource> so;
@@ -756,7 +795,7 @@ struct tci_ctx {
     for (const auto& s : sigma) {
       if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
       if (precision == 1 && s.kind == STEP_GEMM && s.name == "all-external") {
-        k += (plan.n_sing > 0 ? 2 : 0) + (plan.n_trip > 0 && plan.nm > 0 ? 2 : 0);
+        k += (has_sing() ? 1 : 0) + (has_trip() ? 1 : 0) + ((has_sing() || has_trip()) ? 1 : 0);
         continue;
       }
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
@@ -823,15 +862,14 @@ struct tci_ctx {
     }
   }
 
+  bool has_sing() const { return plan.n_sing > 0; }
+  bool has_trip() const { return plan.n_trip > 0 && plan.nm > 0; }
   void run_allext_tc() {
-    if (plan.n_sing > 0) {
+    if (has_sing())
       TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_us, plan.n_sing, plan.np, uhi, ulo, stream));
-      TCI_CUDA(tci_tc_host::launch(tc_sing, stream));
-    }
-    if (plan.n_trip > 0 && plan.nm > 0) {
-      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, uhi, ulo, stream));
-      TCI_CUDA(tci_tc_host::launch(tc_trip, stream));
-    }
+    if (has_trip())
+      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, uhi_t, ulo_t, stream));
+    TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream));
   }
 
   // Moves W+/W- to FP32 for the tensor-core product and releases the FP64 copy.
@@ -846,11 +884,15 @@ struct tci_ctx {
     };
     alloc_f(&w32p, (size_t)np * tci_tc_host::padded_ld(np));
     if (nm > 0) alloc_f(&w32m, (size_t)nm * tci_tc_host::padded_ld(nm));
-    const i64 mrows = tci_tc_host::padded_rows(std::max<i64>(1, std::max(plan.n_sing, plan.n_trip)));
-    alloc_f(&uhi, (size_t)mrows * tci_tc_host::padded_ld(np));
-    alloc_f(&ulo, (size_t)mrows * tci_tc_host::padded_ld(np));
+    alloc_f(&uhi, (size_t)tci_tc_host::padded_rows(std::max<i64>(1, plan.n_sing)) * tci_tc_host::padded_ld(np));
+    alloc_f(&ulo, (size_t)tci_tc_host::padded_rows(std::max<i64>(1, plan.n_sing)) * tci_tc_host::padded_ld(np));
+    if (has_trip()) {
+      alloc_f(&uhi_t, (size_t)tci_tc_host::padded_rows(plan.n_trip) * tci_tc_host::padded_ld(nm));
+      alloc_f(&ulo_t, (size_t)tci_tc_host::padded_rows(plan.n_trip) * tci_tc_host::padded_ld(nm));
+    }
     TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
     owned.push_back(tc_status);
+    TCI_CUDA(tci_gtc_host::prepare());
     TCI_CUDA(cudaMemsetAsync(tc_status, 0, sizeof(int), stream));
     TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
     if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
@@ -859,7 +901,7 @@ struct tci_ctx {
     if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, uhi, ulo, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     if (plan.n_trip > 0 && nm > 0 &&
-        !tci_tc_host::prepare(tc_trip, w32m, nm, uhi, ulo, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
+        !tci_tc_host::prepare(tc_trip, w32m, nm, uhi_t, ulo_t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     {
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
@@ -874,7 +916,7 @@ struct tci_ctx {
     if (!tc_status) return;
     int st = 0;
     TCI_CUDA(cudaMemcpy(&st, tc_status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (st != 0) throw Error(TCI_ERR_TIMEOUT, "tensor-core all-external kernel: a bounded wait gave up (code " + std::to_string(st) + ")");
+    if (st != 0) throw Error(TCI_ERR_TIMEOUT, "tensor-core kernel: a bounded wait gave up (code " + std::to_string(st) + ")");
   }
 
   void check_range(int b, i64 off, i64 len) const {
@@ -883,12 +925,24 @@ struct tci_ctx {
   }
 
   void run(const DevStep& s) {
+    try {
+      run_step(s);
+    } catch (const Error& e) {
+      throw Error(e.code, "plan step '" + s.name + "': " + e.what());
+    }
+  }
+
+  void run_step(const DevStep& s) {
     // the tensor-core form writes the all-external products directly
     if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
     switch (s.kind) {
       case STEP_GEMM:
         if (precision == 1 && s.name == "all-external") {
           run_allext_tc();
+          break;
+        }
+        if (precision == 1 && s.probs_tc && (tc_mode == 1 || (tc_mode == 0 && s.tc_ok))) {
+          TCI_CUDA(tci_gtc_host::launch(s.probs_tc, s.nprob, s.segs_tc, s.ntiles_tc, tc_status, (int)tc_kblock, stream));
           break;
         }
         if (s.ntiles > 0) {
@@ -937,14 +991,17 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
 
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
                       int64_t n_options, tci_ctx** out) {
-  int64_t precision = 0, kblock = 128;
+  int64_t precision = 0, kblock = 128, tc_mode = 0;
   if (options && n_options > 0) precision = options[0];
   if (options && n_options > 1 && options[1] > 0) kblock = options[1];
-  if (precision < 0 || precision > 1) {
-    set_error("unknown precision mode");
+  if (options && n_options > 2) tc_mode = options[2];
+  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2) {
+    set_error("unknown precision mode or tensor-core GEMM selection");
     return TCI_ERR_ARG;
   }
-  return init_impl(deck, op, device, precision, kblock, out);
+  const int rc = init_impl(deck, op, device, precision, kblock, out);
+  if (rc == TCI_OK) tci::ctx_set_tc_gemms(*out, tc_mode);
+  return rc;
 }
 
 static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, int64_t kblock,
@@ -982,15 +1039,22 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
   const double diag = 8.0 * (double)P.total_csfs;
   double pk = all, res = all - init_only + diag;
   if (precision == 1) {
-    const i64 mrows = tci_tc_host::padded_rows(std::max<i64>(1, std::max(P.n_sing, P.n_trip)));
     const double f32 = 4.0 * ((double)P.np * tci_tc_host::padded_ld(P.np) +
                               (P.nm > 0 ? (double)P.nm * tci_tc_host::padded_ld(P.nm) : 0.0) +
-                              2.0 * (double)mrows * tci_tc_host::padded_ld(P.np));
+                              2.0 * (double)tci_tc_host::padded_rows(std::max<i64>(1, P.n_sing)) *
+                                  tci_tc_host::padded_ld(P.np) +
+                              (P.nm > 0 ? 2.0 * (double)tci_tc_host::padded_rows(std::max<i64>(1, P.n_trip)) *
+                                              tci_tc_host::padded_ld(P.nm)
+                                        : 0.0));
     pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
     res += f32 - 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]);
   }
   *peak = std::max(pk, res);
   *resident = res;
+}
+
+void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode) {
+  if (ctx) ctx->tc_mode = mode;
 }
 
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,

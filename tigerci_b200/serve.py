@@ -33,7 +33,7 @@ class TciServerConfig(C.Structure):
     _fields_ = [("device", C.c_int64), ("slots", C.c_int64), ("planners", C.c_int64),
                 ("hbm_budget_bytes", C.c_int64), ("precision", C.c_int64),
                 ("subspace_vectors_per_root", C.c_int64), ("schedule_only", C.c_int64),
-                ("schedule_only_ms", C.c_double), ("inject_worker_exit_at", C.c_int64)]
+                ("schedule_only_ms", C.c_double), ("inject_worker_exit_at", C.c_int64), ("tc_gemms", C.c_int64)]
 
 
 def _bind():
@@ -73,11 +73,11 @@ class Result:
 class Server:
     def __init__(self, device: int = 0, slots: int = 4, hbm_budget: float = 150e9, precision: str = "tf32x3",
                  planners: int = 2, subspace_vectors_per_root: int = 12, schedule_only: bool = False,
-                 schedule_only_ms: float = 0.0, inject_worker_exit_at: int = 0):
+                 schedule_only_ms: float = 0.0, inject_worker_exit_at: int = 0, tc_gemms: str = "by_size"):
         self._L = _bind()
         cfg = TciServerConfig(device, slots, planners, int(hbm_budget), PRECISIONS[precision],
                               subspace_vectors_per_root, 1 if schedule_only else 0, float(schedule_only_ms),
-                              inject_worker_exit_at)
+                              inject_worker_exit_at, {"by_size": 0, "all": 1, "none": 2}[tc_gemms])
         h = C.c_void_p()
         check(self._L.tci_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
