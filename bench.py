@@ -223,6 +223,60 @@ def serve_measure(n_requests, slots, device):
             "stand_in": "synthetic MO operators with the H_n chains' orbital counts (no integral engine)"}
 
 
+def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3):
+    """All-external term over uneven pair domains: n_pairs internal pairs (35
+    doubly occupied internal orbitals), domains of 20..180 of 400 external
+    orbitals (seed 99), Cholesky rank 2400 as in the kernel-scale operator.
+    Times tci_local_apply (one CUDA graph per application) in both forms."""
+    import torch
+
+    from tigerci_b200 import local
+    from tigerci_b200.synthetic import synthetic_operator
+
+    n_int, n_virt, nchol = 35, 400, 2400
+    heads, dom, total = local.pair_domain_problem(n_pairs, n_int, n_virt, 20, 180, seed=99)
+    _, L = synthetic_operator(n_int + n_virt, nchol, seed=1234)
+    rng = np.random.default_rng(7)
+    c_host = rng.standard_normal(total)
+    c = torch.from_numpy(c_host).cuda(device)
+    out = {"workload": f"{len(heads)} internal pairs, domains U{{20..180}} of {n_virt} externals (seed 99), "
+                       f"Cholesky rank {nchol}; CI length {total}",
+           "heads": int(len(heads))}
+    sig = {}
+    for form, n_steps in (("tf32x3", steps), ("fp64", 1)):
+        t0 = time.perf_counter()
+        op = local.LocalAllExternal(n_int, n_virt, L, heads, dom, total, device=device, precision=form)
+        init_s = time.perf_counter() - t0
+        st = op.stats()
+        s = torch.zeros_like(c)
+        for _ in range(warmup if form == "tf32x3" else 1):
+            op.apply_device(c.data_ptr(), s.data_ptr())
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n_steps)]
+        for i in range(n_steps):
+            s.zero_()
+            ev[i][0].record()
+            op.apply_device(c.data_ptr(), s.data_ptr())
+            ev[i][1].record()
+        torch.cuda.synchronize()
+        t = sum(a.elapsed_time(b) for a, b in ev) / 1e3 / n_steps
+        sig[form] = s.cpu().numpy()
+        # 3xTF32 issues three MMAs per product: its FP32-accurate peak is a third of the TF32 peak
+        # (half the measured dense BF16 figure)
+        peak = bf16 / 2 / 3 if form == "tf32x3" else None
+        out[form] = {"ms_per_apply": 1e3 * t, "tflops": st["flops"] / t / 1e12,
+                     "flops_per_apply": st["flops"], "chunk": int(st["chunk"]), "tile_cfg": int(st["tile_cfg"]),
+                     "autotune_candidates": int(st["candidates"]), "device_gb": st["device_bytes"] / 1e9,
+                     "init_s": init_s,
+                     "roofline": {"bound": "tensor", "achieved": st["flops"] / t / 1e12, "peak": peak,
+                                  "unit": "TFLOP/s", "frac": (st["flops"] / t / 1e12 / peak) if peak else None,
+                                  "peak_kind": "3xTF32: measured dense BF16 / 2 / 3" if peak else None}}
+        op.close()
+    a, b = sig["tf32x3"], sig["fp64"]
+    out["mixed_rel_err_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -238,6 +292,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving stream to replay")
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--serve-only", action="store_true", help="only the serving measurement")
+    ap.add_argument("--local-pairs", type=int, default=600, help="pairs of the pair-domain workload (0: skip)")
+    ap.add_argument("--local-only", action="store_true", help="only the pair-domain measurement")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -277,6 +333,10 @@ def main():
     if args.serve_only:
         if rank == 0:
             print(json.dumps({"serving": serve_measure(args.serve_requests, args.serve_slots, local)}), flush=True)
+        return
+    if args.local_only:
+        if rank == 0:
+            print(json.dumps({"local_pairs": local_measure(args.local_pairs, local, hbm, bf16)}), flush=True)
         return
 
     # ---- sigma builds on the operator exactly as the kernel-scale configuration specifies
@@ -489,6 +549,11 @@ def main():
             line["serving"] = serve_measure(args.serve_requests, args.serve_slots, local)
         except Exception as exc:
             line["serving"] = {"error": str(exc)[:300]}
+    if args.local_pairs > 0:
+        try:
+            line["local_pairs"] = local_measure(args.local_pairs, local, hbm, bf16)
+        except Exception as exc:
+            line["local_pairs"] = {"error": str(exc)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_sample()
         t_solve = cb["t_sigma"] * SIGMA_BUILDS_PER_SOLVE

@@ -195,6 +195,37 @@ int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps,
 int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len);
 void tci_destroy(tci_ctx* ctx);
 
+/* ---- Local pair domains: the all-external term over uneven domains -----
+ * Replaces the local all-external loops (ext_3_4_seg_loops_vec_lmo_res_2,
+ * tiger_fortran/three_and_four_seg_mod_1.f90:3240-3518, over the domains of
+ * virtual_truncation, tiger_fortran/locist_mod.f90:358-451) for a set of N-2
+ * heads, each with its own sorted domain of external orbitals.  heads: 7
+ * int64 per head: off_ab, off_aa (CI offsets of the head's ab and aa blocks),
+ * nsf_ab, nsf_aa (spin functions with an ab / aa block), nsing (the first
+ * nsing are singlet-coupled), dom_off, dom_len (its slice of dom_idx: sorted
+ * external indices 0..num_external-1).  A block of a head has its domain's
+ * size: ab n(n-1)/2 per spin function, pair index i(i-1)/2+j (i > j), aa n.
+ * chol is the tci_operator Cholesky array over num_internal + num_external
+ * orbitals.  Applied in the Cholesky form (two grouped GEMMs over all heads
+ * per chunk of Cholesky vectors).  options: [0] precision (TCI_PRECISION_*),
+ * [1] device bytes for the per-chunk buffers (default 16e9), [2] promotion
+ * block, [3] 0 to skip the set-up autotuning of chunk size and tile shape. */
+typedef struct tci_local tci_local;
+int tci_local_create(int64_t num_internal, int64_t num_external, const double* chol, int64_t nchol, int64_t n_heads,
+                     const int64_t* heads, const int64_t* dom_idx, int64_t total_len, int64_t device,
+                     const int64_t* options, int64_t n_options, tci_local** out);
+/* sigma += A c on device arrays of length total_len, ordered on stream (NULL =
+ * legacy default stream). */
+int tci_local_apply(tci_local* loc, const double* d_c, double* d_sigma, int64_t n, void* stream);
+/* The same with host arrays. */
+int tci_local_apply_host(tci_local* loc, const double* c, double* sigma, int64_t n);
+/* out[9]: flops per application (4 nchol sum n^3 over head spin functions),
+ * gathered Cholesky bytes per application, device bytes, chunk size, FP64 tile
+ * shape of the second GEMM, autotuned time (ms), autotuner candidates, last
+ * host application (ms), head spin-function blocks. */
+int tci_local_stats(const tci_local* loc, double* out, int64_t len);
+void tci_local_destroy(tci_local* loc);
+
 /* ---- Serving: continuously batched CI solves on one GPU ----------------
  * No counterpart in the reference, which runs one solve per process
  * (tiger_fortran/tiger_ci.f90 -> davidson_liu).  Submitted solves are

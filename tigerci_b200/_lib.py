@@ -40,6 +40,11 @@ EXPORTS = [
     "tci_davidson_ex",
     "tci_davidson_capacity",
     "tci_davidson_bytes",
+    "tci_local_create",
+    "tci_local_apply",
+    "tci_local_apply_host",
+    "tci_local_stats",
+    "tci_local_destroy",
     "tci_server_create",
     "tci_server_submit",
     "tci_server_wait",

@@ -529,6 +529,11 @@ struct DevStep {
   DGemmProblem* probs_tc = nullptr;
   DGemmSeg* segs_tc = nullptr;
   long long ntiles_tc = 0;
+  int nprob_tc = 0;
+  DGemmProblem* probs_f = nullptr;  // its FP64 part (same-head one-electron-like segments)
+  DGemmSeg* segs_f = nullptr;
+  long long ntiles_f = 0;
+  int nprob_f = 0;
   bool tc_ok = false;  // worth the tensor cores: enough work and tiles mostly full
   // AXPY / DOT
   DAxpyTarget* at = nullptr;
@@ -662,42 +667,43 @@ struct tci_ctx {
       d.nprob = (int)pr.size();
       d.ntiles = tiles;
       if (s.name != "all-external" && !pr.empty()) {
-        // tensor-core tables: 128 x 64 tiles; a problem whose M fills the 128-row tiles worse than its N
-        // would is computed transposed (C^T = B^T A^T) with its own copy of the segments
-        const i64 TM = tci_gtc_host::tile_m(), TN = tci_gtc_host::tile_n();
-        std::vector<DGemmProblem> pt = pr;
-        std::vector<DGemmSeg> st;
-        long long tt = 0;
-        double flops = 0, useful = 0, issued = 0;
-        auto fill = [&](i64 M, i64 N) {
-          return (double)M * (double)N /
-                 ((double)((M + TM - 1) / TM * TM) * (double)((N + TN - 1) / TN * TN));
-        };
-        for (auto& g : pt) {
-          const bool tr = fill(g.N, g.M) > fill(g.M, g.N);
-          const long long b = (long long)st.size();
+        // Mixed form.  Segments whose operand is a same-head one-electron-like operator (BUF_F: h, J_ii,
+        // K_ii combinations, orbital-energy magnitudes) stay on the FP64 kernel; the cross-head integral
+        // segments go to the tensor cores (3xTF32), added after the FP64 part (beta 1 where both exist).
+        std::vector<tci_dev::HostGemm> f64, tcp;
+        for (const auto& g : pr) {
+          tci_dev::HostGemm hf{g.C, g.ldc, g.M, g.N, g.beta, {}}, ht{g.C, g.ldc, g.M, g.N, g.beta, {}};
           for (long long q = g.seg_begin; q < g.seg_end; ++q) {
-            DGemmSeg x = sg[q];
-            if (tr) x = DGemmSeg{x.B, x.A, x.ldb, x.lda, x.K, x.tB ? 0 : 1, x.tA ? 0 : 1, x.alpha};
-            st.push_back(x);
+            const bool f = s.gs[(size_t)q].a == BUF_F || s.gs[(size_t)q].b == BUF_F;
+            (f ? hf : ht).segs.push_back(sg[(size_t)q]);
           }
-          g.seg_begin = b;
-          g.seg_end = (long long)st.size();
-          if (tr) std::swap(g.M, g.N);
-          g.trans_c = tr ? 1 : 0;
-          const i64 tm = (g.M + TM - 1) / TM, tn = (g.N + TN - 1) / TN;
-          g.tiles_n = tn;
-          g.tile_begin = tt;
-          tt += tm * tn;
+          if (!hf.segs.empty()) {
+            f64.push_back(hf);
+            ht.beta = 1.0;
+          }
+          if (!ht.segs.empty() || hf.segs.empty()) tcp.push_back(ht);
+        }
+        std::vector<DGemmProblem> pf, pt;
+        std::vector<DGemmSeg> sf, st;
+        d.ntiles_f = tci_dev::tile_problems(f64, tci_dev::gemm_f64_tile_m(d.cfg), tci_dev::gemm_f64_tile_n(d.cfg), false,
+                                            pf, sf);
+        // 128 x 64 tiles; a problem short in M is computed transposed
+        d.ntiles_tc = tci_dev::tile_problems(tcp, tci_gtc_host::tile_m(), tci_gtc_host::tile_n(), true, pt, st);
+        double flops = 0, useful = 0, issued = 0;
+        const i64 TM = tci_gtc_host::tile_m(), TN = tci_gtc_host::tile_n();
+        for (const auto& g : pt) {
           double k = 0;
-          for (long long q = g.seg_begin; q < g.seg_end; ++q) k += (double)st[q].K;
+          for (long long q = g.seg_begin; q < g.seg_end; ++q) k += (double)st[(size_t)q].K;
           flops += 2.0 * (double)g.M * (double)g.N * k;
           useful += (double)g.M * (double)g.N * k;
-          issued += (double)(tm * TM) * (double)(tn * TN) * k;
+          issued += (double)((g.M + TM - 1) / TM * TM) * (double)((g.N + TN - 1) / TN * TN) * k;
         }
+        d.probs_f = upload(pf, owned);
+        d.segs_f = upload(sf, owned);
+        d.nprob_f = (int)pf.size();
         d.probs_tc = upload(pt, owned);
         d.segs_tc = upload(st, owned);
-        d.ntiles_tc = tt;
+        d.nprob_tc = (int)pt.size();
         d.tc_ok = flops >= 5e7 && useful >= 0.25 * issued;
       }
     } else if (s.kind == STEP_AXPY) {
@@ -789,6 +795,10 @@ struct tci_ctx {
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     sigma_count++;
   }
+  // the mixed form runs this GEMM step on the tensor cores
+  bool uses_tc(const DevStep& s) const {
+    return precision == 1 && s.probs_tc && (tc_mode == 1 || (tc_mode == 0 && s.tc_ok));
+  }
   // kernels one sigma build launches (graph nodes included)
   long long sigma_launches() const {
     long long k = 0;
@@ -796,6 +806,10 @@ struct tci_ctx {
       if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
       if (precision == 1 && s.kind == STEP_GEMM && s.name == "all-external") {
         k += (has_sing() ? 1 : 0) + (has_trip() ? 1 : 0) + ((has_sing() || has_trip()) ? 1 : 0);
+        continue;
+      }
+      if (s.kind == STEP_GEMM && uses_tc(s)) {
+        k += (s.ntiles_f > 0 ? 1 : 0) + (s.ntiles_tc > 0 ? 1 : 0);
         continue;
       }
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
@@ -941,8 +955,9 @@ struct tci_ctx {
           run_allext_tc();
           break;
         }
-        if (precision == 1 && s.probs_tc && (tc_mode == 1 || (tc_mode == 0 && s.tc_ok))) {
-          TCI_CUDA(tci_gtc_host::launch(s.probs_tc, s.nprob, s.segs_tc, s.ntiles_tc, tc_status, (int)tc_kblock, stream));
+        if (uses_tc(s)) {
+          TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
+          TCI_CUDA(tci_gtc_host::launch(s.probs_tc, s.nprob_tc, s.segs_tc, s.ntiles_tc, tc_status, (int)tc_kblock, stream));
           break;
         }
         if (s.ntiles > 0) {
@@ -979,6 +994,16 @@ struct tci_ctx {
     TCI_CUDA(cudaGetLastError());
   }
 };
+
+namespace tci_dev {
+cudaError_t launch_gemm_f64(int cfg, const DGemmProblem* probs, int nprob, const DGemmSeg* segs, long long ntiles,
+                            cudaStream_t st) {
+  if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
+  if (cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)ntiles, 256, 0, st>>>(probs, nprob, segs);
+  else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)ntiles, 256, 0, st>>>(probs, nprob, segs);
+  return cudaGetLastError();
+}
+}  // namespace tci_dev
 
 extern "C" {
 
