@@ -116,7 +116,11 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
  * the all-external term with FP32 W operators, and the three-, two- and
  * one-external GEMM steps from their FP64 operands.  options[2] selects those
  * other GEMM steps: 0 by size (default), 1 all of them, 2 none.  The coupling-
- * coefficient products, gathers, scatters and reductions stay FP64. */
+ * coefficient products, same-head one-electron-like operators, gathers,
+ * scatters and reductions stay FP64.  options[3] = 1 (default) keeps the FP64
+ * W as well and reports every tci_davidson root as the Rayleigh quotient of
+ * its Ritz vector with one plain-FP64 sigma build (error second order in the
+ * eigenvector error of the mixed products); 0 releases the FP64 W. */
 #define TCI_PRECISION_FP64 0
 #define TCI_PRECISION_TF32X3 1
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,

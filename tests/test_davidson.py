@@ -161,3 +161,19 @@ def test_device_solve_can_be_cancelled(need_gpu):
     e, _, _ = sb.davidson(1, 1e-9, 1e-13, cancel=flag)  # the context stays usable
     assert np.isfinite(e).all()
     sb.close()
+
+
+@pytest.mark.gpu
+def test_context_reused_for_more_roots(need_gpu):
+    """A context that solved for one root solves for three (larger subspace and
+    reduction scratch) exactly as a fresh context does."""
+    c = SMALL_CASES[8]
+    h, L = _op(c)
+    a = T.SigmaBuilder(product_deck(c), T.Operator(h, L), device=0)
+    a.davidson(1, 1e-8, 1e-12)
+    e3, _, _ = a.davidson(3, 1e-8, 1e-12)
+    b = T.SigmaBuilder(product_deck(c), T.Operator(h, L), device=0)
+    f3, _, _ = b.davidson(3, 1e-8, 1e-12)
+    assert np.array_equal(e3, f3)
+    a.close()
+    b.close()

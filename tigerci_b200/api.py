@@ -162,14 +162,15 @@ class SigmaBuilder:
     TC_GEMMS = {"by_size": 0, "all": 1, "none": 2}
 
     def __init__(self, deck: Deck, op: Operator, device: int = 0, precision: str = "fp64", promote_every: int = 128,
-                 tc_gemms: str = "by_size"):
+                 tc_gemms: str = "by_size", fp64_finish: bool = True):
         self._d = deck.c_struct()
         self._o = op.c_struct()
         self._op = op
         self.precision = precision
         h = C.c_void_p()
-        opts = np.array([self.PRECISIONS[precision], promote_every, self.TC_GEMMS[tc_gemms]], dtype=np.int64)
-        check(lib().tci_sigma_init_ex(C.byref(self._d), C.byref(self._o), device, ptr(opts), 3, C.byref(h)))
+        opts = np.array([self.PRECISIONS[precision], promote_every, self.TC_GEMMS[tc_gemms], 1 if fp64_finish else 0],
+                        dtype=np.int64)
+        check(lib().tci_sigma_init_ex(C.byref(self._d), C.byref(self._o), device, ptr(opts), 4, C.byref(h)))
         self._h = h
         self.n = int(self.stats()["total_csfs"])
 

@@ -124,10 +124,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     allext_tf32x3_kernel(const __grid_constant__ CUtensorMap wmap0, const __grid_constant__ CUtensorMap uhi_map0,
                          const __grid_constant__ CUtensorMap ulo_map0, const __grid_constant__ CUtensorMap wmap1,
                          const __grid_constant__ CUtensorMap uhi_map1, const __grid_constant__ CUtensorMap ulo_map1,
-                         Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
+                         Product p0, Product p1, int* __restrict__ status, int kb_per_block, int ksplit) {
   const int KB_PER_BLOCK = kb_per_block;
-  // which product this CTA works on (uniform over the CTA: the early exit precedes all set-up)
-  const bool second = (int)blockIdx.x >= p0.tiles;
+  // CTA -> (tile, k split); which product the tile belongs to (uniform over the CTA: the early exit
+  // precedes all set-up)
+  const int tile = (int)blockIdx.x / ksplit, split = (int)blockIdx.x % ksplit;
+  const bool second = tile >= p0.tiles;
   const Product P = second ? p1 : p0;
   const CUtensorMap* wmap = second ? &wmap1 : &wmap0;
   const CUtensorMap* uhi_map = second ? &uhi_map1 : &uhi_map0;
@@ -147,8 +149,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row0 = (second ? (int)blockIdx.x - p0.tiles : (int)blockIdx.x) * BM;
-  const int nk = (np + BK - 1) / BK;
+  const int row0 = (second ? tile - p0.tiles : tile) * BM;
+  // k steps of this split: [kbase, kbase + nk)
+  const int nk_all = (np + BK - 1) / BK, per = (nk_all + ksplit - 1) / ksplit;
+  const int kbase = split * per;
+  const int nk = nk_all - kbase < per ? (nk_all - kbase > 0 ? nk_all - kbase : 0) : per;
   const int nblocks = (nk + KB_PER_BLOCK - 1) / KB_PER_BLOCK;
 
   if (threadIdx.x == 0) {
@@ -193,9 +198,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         uint8_t* st = base + s * STAGE_BYTES;
         mbar_expect_tx(&full[s], W_BYTES + 2 * U_BYTES);
-        tma_load_2d(st, wmap, &full[s], kb * BK, row0);
-        tma_load_2d(st + 2 * W_BYTES, uhi_map, &full[s], kb * BK, ublock * BN);
-        tma_load_2d(st + 2 * W_BYTES + U_BYTES, ulo_map, &full[s], kb * BK, ublock * BN);
+        tma_load_2d(st, wmap, &full[s], (kbase + kb) * BK, row0);
+        tma_load_2d(st + 2 * W_BYTES, uhi_map, &full[s], (kbase + kb) * BK, ublock * BN);
+        tma_load_2d(st + 2 * W_BYTES + U_BYTES, ulo_map, &full[s], (kbase + kb) * BK, ublock * BN);
         last = kb;
       }
       if (aborted()) {
@@ -307,7 +312,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
       for (int t = 0; t < BN; ++t) {
         const int j = ublock * BN + t;
-        if (j < m) P.Y[(long long)j * P.ldy + r] = acc[t];
+        if (j < m) {
+          // two splits add into the zeroed output: x + y rounds the same in either order, so the
+          // result does not depend on which split finishes first
+          if (ksplit == 1) P.Y[(long long)j * P.ldy + r] = acc[t];
+          else atomicAdd(&P.Y[(long long)j * P.ldy + r], acc[t]);
+        }
       }
     }
   }
@@ -438,6 +448,19 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
   return true;
 }
 
+// Two k splits when the tiles fill fewer than four waves of one CTA per SM: the
+// last, partly filled wave then costs less (more than two splits would make
+// the atomic accumulation order-dependent).
+int ksplit(const AllextTc* a, const AllextTc* b) {
+  if (!a) std::swap(a, b);
+  if (!a) return 1;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t ub = std::max(padded_rows(a->m), b ? padded_rows(b->m) : 0) / tci_tc::BN;
+  const int64_t tiles = ((a->np + tci_tc::BM - 1) / tci_tc::BM + (b ? (b->np + tci_tc::BM - 1) / tci_tc::BM : 0)) * ub;
+  return tiles < 4 * (int64_t)sms ? 2 : 1;
+}
+
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   if (!a && !b) return cudaSuccess;
   if (!a) std::swap(a, b);
@@ -454,10 +477,16 @@ cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   };
   const tci_tc::Product p0 = product(a), p1 = product(b);
   const int64_t ub = std::max(padded_rows(a->m), b ? padded_rows(b->m) : 0) / tci_tc::BN;
-  dim3 grid((unsigned)(p0.tiles + p1.tiles), (unsigned)ub);
+  const int ks = ksplit(a, b);
+  if (ks > 1) {  // the two splits accumulate into zeroed outputs
+    cudaError_t e = cudaMemsetAsync(a->y, 0, sizeof(double) * (size_t)(a->m * a->np), st);
+    if (e == cudaSuccess && b) e = cudaMemsetAsync(b->y, 0, sizeof(double) * (size_t)(b->m * b->np), st);
+    if (e != cudaSuccess) return e;
+  }
+  dim3 grid((unsigned)((p0.tiles + p1.tiles) * ks), (unsigned)ub);
   const AllextTc* c = b ? b : a;  // maps of the second product (unused when there is none)
-  tci_tc::allext_tf32x3_kernel<<<grid, tci_tc::NTHREADS, smem, st>>>(a->wmap, a->uhi, a->ulo, c->wmap, c->uhi, c->ulo,
-                                                                     p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
+  tci_tc::allext_tf32x3_kernel<<<grid, tci_tc::NTHREADS, smem, st>>>(
+      a->wmap, a->uhi, a->ulo, c->wmap, c->uhi, c->ulo, p0, p1, a->status, (int)(a->kblock / tci_tc::BK), ks);
   return cudaGetLastError();
 }
 

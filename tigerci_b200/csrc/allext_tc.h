@@ -25,5 +25,6 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
 // Both products in one launch (either may be null; they must share the status
 // word and promotion block).
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);
+int ksplit(const AllextTc* a, const AllextTc* b);  // k splits launch() uses (1 or 2)
 
 }  // namespace tci_tc_host

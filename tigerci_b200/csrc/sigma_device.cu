@@ -578,6 +578,7 @@ struct tci_ctx {
   int64_t precision = 0;                // 0 plain FP64; 1 all-external on tcgen05 (3xTF32, FP64 promotion)
   int64_t tc_kblock = 128;              // k elements per FP64 promotion block of the tensor-core product
   int64_t tc_mode = 0;                  // precision 1: other GEMM steps on the tensor cores by size (0), all (1), none (2)
+  int64_t refine = 1;                   // precision 1: roots finished as FP64 Rayleigh quotients (keeps the FP64 W)
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* uhi = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -591,6 +592,7 @@ struct tci_ctx {
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
   double* dots = nullptr;        // reduction scratch: partial sums and results
   double* coefs = nullptr;       // small device coefficient arrays
+  int scratch_cap = 0;           // vectors dots / coefs are sized for
   double* dotbuf = nullptr;      // tci_dots reduction scratch
   int64_t dotbuf_cap = 0;        // doubles
   std::vector<cudaEvent_t> step_ev;     // 2 per sigma step
@@ -598,6 +600,9 @@ struct tci_ctx {
   long long profiled_builds = 0;
   long long launch_count = 0;    // kernels this context has launched (sigma builds, Davidson, projections)
   bool dav_phases = false;       // time the Davidson phases (stream synchronised at each boundary)
+  // Davidson vectors, kept between solves (reallocated only when a solve needs more)
+  double *dav_c = nullptr, *dav_hc = nullptr, *dav_r = nullptr, *dav_tc = nullptr, *dav_th = nullptr;
+  int64_t dav_cap = 0, dav_keep = 0;
   double dav_ms[8] = {};         // setup, sigma, projection, subspace eigensolve, residual,
                                  // preconditioner + Gram-Schmidt, restart, finish
 
@@ -611,6 +616,8 @@ struct tci_ctx {
     if (stream) cudaStreamSynchronize(stream);
     std::lock_guard<std::mutex> lk(g_capture_free_mu);
     if (dotbuf) cudaFree(dotbuf);
+    for (double* p : {dav_c, dav_hc, dav_r, dav_tc, dav_th})
+      if (p) cudaFree(p);
     for (int b = 0; b < NUM_BUFS; ++b)
       if (buf[b]) cudaFree(buf[b]);
     for (void* p : owned) cudaFree(p);
@@ -762,12 +769,24 @@ struct tci_ctx {
     TCI_CUDA(cudaStreamSynchronize(stream));
   }
 
+  // reduction scratch for projections of up to mmax vectors (grows when a solve needs more)
   void ensure_scratch(int mmax) {
-    if (dots) return;
+    if (dots && mmax <= scratch_cap) return;
+    if (dots) {
+      TCI_CUDA(cudaStreamSynchronize(stream));
+      std::lock_guard<std::mutex> lk(g_capture_free_mu);
+      for (void* p : {(void*)dots, (void*)coefs}) {
+        cudaFree(p);
+        owned.erase(std::find(owned.begin(), owned.end(), p));
+      }
+      dots = coefs = nullptr;
+      scratch_cap = 0;
+    }
     TCI_CUDA(cudaMalloc(&dots, ((size_t)mmax * (RBLK + 1) + 16) * sizeof(double)));
     owned.push_back(dots);
     TCI_CUDA(cudaMalloc(&coefs, (size_t)4 * mmax * sizeof(double)));
     owned.push_back(coefs);
+    scratch_cap = mmax;
   }
 
   // out[0..m) = A[k] . x  (host result), deterministic
@@ -917,12 +936,32 @@ struct tci_ctx {
     if (plan.n_trip > 0 && nm > 0 &&
         !tci_tc_host::prepare(tc_trip, w32m, nm, uhi_t, ulo_t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
-    {
+    if (!refine) {  // the FP64 W is only needed for the FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
       TCI_CUDA(cudaFree(buf[BUF_W]));
+      bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
+      buf[BUF_W] = nullptr;
     }
-    bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
-    buf[BUF_W] = nullptr;
+  }
+
+  // One plain-FP64 sigma build in a mixed-precision context (the steps launched
+  // one by one, outside the context's graph): d_s = H d_c.
+  void sigma_of_fp64(const double* d_c, double* d_s) {
+    const i64 n = plan.total_csfs;
+    if (!buf[BUF_W]) throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
+    TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
+    const int64_t saved = precision;
+    precision = 0;
+    try {
+      record_steps(false, false);
+    } catch (...) {
+      precision = saved;
+      throw;
+    }
+    launch_count += sigma_launches();
+    precision = saved;
+    TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   }
 
   // Status word of the bounded waits inside the tensor-core kernel.
@@ -1008,7 +1047,7 @@ cudaError_t launch_gemm_f64(int cfg, const DGemmProblem* probs, int nprob, const
 extern "C" {
 
 static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, int64_t kblock,
-                     tci_ctx** out);
+                     tci_ctx** out, int64_t refine = 1);
 
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out) {
   return init_impl(deck, op, device, 0, 128, out);
@@ -1016,21 +1055,22 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
 
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
                       int64_t n_options, tci_ctx** out) {
-  int64_t precision = 0, kblock = 128, tc_mode = 0;
+  int64_t precision = 0, kblock = 128, tc_mode = 0, refine = 1;
   if (options && n_options > 0) precision = options[0];
   if (options && n_options > 1 && options[1] > 0) kblock = options[1];
   if (options && n_options > 2) tc_mode = options[2];
-  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2) {
-    set_error("unknown precision mode or tensor-core GEMM selection");
+  if (options && n_options > 3) refine = options[3];
+  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2 || refine < 0 || refine > 1) {
+    set_error("unknown precision mode, tensor-core GEMM selection or finish");
     return TCI_ERR_ARG;
   }
-  const int rc = init_impl(deck, op, device, precision, kblock, out);
+  const int rc = init_impl(deck, op, device, precision, kblock, out, refine);
   if (rc == TCI_OK) tci::ctx_set_tc_gemms(*out, tc_mode);
   return rc;
 }
 
 static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, int64_t kblock,
-                     tci_ctx** out) {
+                     tci_ctx** out, int64_t refine) {
   if (!out) return TCI_ERR_ARG;
   *out = nullptr;
   try {
@@ -1041,7 +1081,7 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
     Operator o;
     operator_from_c(op, sp, o);
     build_plan(sp, o, plan);
-    const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out);
+    const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out, refine);
     if (rc == TCI_OK) (*out)->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rc;
   } catch (...) {
@@ -1053,7 +1093,7 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
 
 namespace tci {
 
-void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* resident) {
+void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* resident, int64_t refine) {
   double all = 0, init_only = 0;
   for (int b = 0; b < NUM_BUFS; ++b) {
     const double bytes = (double)std::max<i64>(0, P.buf_size[b]) * 8.0;
@@ -1072,7 +1112,7 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                                               tci_tc_host::padded_ld(P.nm)
                                         : 0.0));
     pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
-    res += f32 - 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]);
+    res += f32 - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
   *peak = std::max(pk, res);
   *resident = res;
@@ -1083,7 +1123,7 @@ void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode) {
 }
 
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
-                  tci_ctx** out) {
+                  tci_ctx** out, int64_t refine) {
   if (!out || !chol) return TCI_ERR_ARG;
   *out = nullptr;
   if (precision < 0 || precision > 1) {
@@ -1149,6 +1189,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     if (const char* g = std::getenv("TCI_NO_GRAPH")) ctx->use_graph = (g[0] == '0');
     ctx->precision = precision;
     ctx->tc_kblock = kblock;
+    ctx->refine = refine;
     ctx->setup_precision();
     ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = ctx.release();
@@ -1354,23 +1395,37 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
       tp = t;
       cur_phase = ph;
     };
-    double *Cs = nullptr, *HCs = nullptr, *r = nullptr, *tmpC = nullptr, *tmpH = nullptr;
-    auto free_all = [&]() {
-      cudaStreamSynchronize(ctx->stream);
-      std::lock_guard<std::mutex> lk(g_capture_free_mu);
-      for (double* p : {Cs, HCs, r, tmpC, tmpH})
-        if (p) cudaFree(p);
-    };
-    try {
-      cudaError_t e1 = cudaMalloc(&Cs, (size_t)cap * n * sizeof(double));
-      cudaError_t e2 = cudaMalloc(&HCs, (size_t)cap * n * sizeof(double));
-      cudaError_t e3 = cudaMalloc(&r, (size_t)(n + 8) * sizeof(double));
-      cudaError_t e4 = cudaMalloc(&tmpC, (size_t)keep * n * sizeof(double));
-      cudaError_t e5 = cudaMalloc(&tmpH, (size_t)keep * n * sizeof(double));
+    // the subspace vectors stay allocated in the context between solves
+    auto free_all = [&]() { cudaStreamSynchronize(ctx->stream); };
+    if (ctx->dav_cap < cap || ctx->dav_keep < keep) {
+      TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+      {
+        std::lock_guard<std::mutex> lk(g_capture_free_mu);
+        for (double** p : {&ctx->dav_c, &ctx->dav_hc, &ctx->dav_r, &ctx->dav_tc, &ctx->dav_th}) {
+          if (*p) cudaFree(*p);
+          *p = nullptr;
+        }
+      }
+      ctx->dav_cap = ctx->dav_keep = 0;
+      cudaError_t e1 = cudaMalloc(&ctx->dav_c, (size_t)cap * n * sizeof(double));
+      cudaError_t e2 = cudaMalloc(&ctx->dav_hc, (size_t)cap * n * sizeof(double));
+      cudaError_t e3 = cudaMalloc(&ctx->dav_r, (size_t)(n + 8) * sizeof(double));
+      cudaError_t e4 = cudaMalloc(&ctx->dav_tc, (size_t)keep * n * sizeof(double));
+      cudaError_t e5 = cudaMalloc(&ctx->dav_th, (size_t)keep * n * sizeof(double));
       if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess || e5 != cudaSuccess) {
         cudaGetLastError();
+        std::lock_guard<std::mutex> lk(g_capture_free_mu);
+        for (double** p : {&ctx->dav_c, &ctx->dav_hc, &ctx->dav_r, &ctx->dav_tc, &ctx->dav_th}) {
+          if (*p) cudaFree(*p);
+          *p = nullptr;
+        }
         throw Error(TCI_ERR_MEMORY, "device allocation of the Davidson subspace failed");
       }
+      ctx->dav_cap = cap;
+      ctx->dav_keep = keep;
+    }
+    double *Cs = ctx->dav_c, *HCs = ctx->dav_hc, *r = ctx->dav_r, *tmpC = ctx->dav_tc, *tmpH = ctx->dav_th;
+    try {
       cudaStream_t st = ctx->stream;
       const unsigned G = 148 * 8, TB = 256;
       // initial guess: unit vectors at the lowest diagonal elements
@@ -1549,6 +1604,21 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
       }
       mark(7);
       ctx->check_tc_status();
+      if (ctx->precision == 1 && ctx->refine) {
+        // FP64 finish: each root is reported as the Rayleigh quotient of its Ritz vector with the plain-FP64
+        // sigma.  Its error is second order in the eigenvector error the mixed products leave.
+        const int m = (int)w.size();
+        for (int q = 0; q < nroots; ++q) {
+          std::vector<double> cb(m);
+          for (int k = 0; k < m; ++k) cb[k] = V[(size_t)k * m + q];
+          lincomb_into(r, Cs, cb, m);
+          ctx->sigma_of_fp64(r, tmpH);
+          double rr = 0.0, rhr = 0.0;
+          ctx->multi_dot(r, 0, 1, r, n, &rr);
+          ctx->multi_dot(r, 0, 1, tmpH, n, &rhr);
+          energy[q] = rhr / rr;
+        }
+      }
       for (int q = 0; q < nroots; ++q) energies[q] = energy[q];
       if (iterations) *iterations = std::min<i64>(it, maxit);
       if (vectors) {
