@@ -46,7 +46,8 @@ constexpr int B_BYTES = BN * BK * 4;  // 8 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
-static_assert(BM * BK == 32 * 32 * NPROD && BN * BK == 16 * 32 * NPROD, "producer element counts");
+static_assert(BM * BK == 32 * 32 * NPROD && BN * BK == 16 * 32 * NPROD && NPROD == 4 && BK == 32,
+              "producer element maps");
 
 enum : int { ST_TIMEOUT_EMPTY = 11, ST_TIMEOUT_FULL = 12, ST_TIMEOUT_D = 13, ST_TIMEOUT_DE = 14 };
 
@@ -152,10 +153,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const long long gm = m0 + pw + NPROD * i;
             xa[i] = (gm < P.M && gk < S.K) ? S.A[gm * S.lda + gk] : 0.0;
           }
-        } else {  // A[k][m]: a warp reads one k for 32 consecutive rows, lane = row
+        } else {  // A[k][m]: warp pw takes k in [8 pw, 8 pw + 8); an instruction reads 4 k rows x 8
+                  // consecutive m (lane = 8 (k & 3) + (m & 7)), so its shared-memory stores hit 32 banks
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
-            const long long gk = k0 + pw + NPROD * (i >> 2), gm = m0 + (i & 3) * 32 + lane;
+            const long long gk = k0 + 8 * pw + 4 * (i >> 4) + (lane >> 3), gm = m0 + 8 * (i & 15) + (lane & 7);
             xa[i] = (gm < P.M && gk < S.K) ? S.A[gk * S.lda + gm] : 0.0;
           }
         }
@@ -167,10 +169,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const long long gn = n0 + pw + NPROD * i;
             xb[i] = (gn < P.N && gk < S.K) ? S.B[gn * S.ldb + gk] : 0.0;
           }
-        } else {  // B[k][n]: lane = n
+        } else {  // B[k][n]: as the transposed A path, 4 k rows x 8 consecutive n per instruction
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
-            const long long gk = k0 + pw + NPROD * (i >> 1), gn = n0 + (i & 1) * 32 + lane;
+            const long long gk = k0 + 8 * pw + 4 * (i >> 3) + (lane >> 3), gn = n0 + 8 * (i & 7) + (lane & 7);
             xb[i] = (gn < P.N && gk < S.K) ? S.B[gk * S.ldb + gn] : 0.0;
           }
         }
@@ -179,7 +181,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           for (int i = 0; i < 32; ++i) split_store(ahi, alo, pw + NPROD * i, lane, xa[i]);
         } else {
 #pragma unroll
-          for (int i = 0; i < 32; ++i) split_store(ahi, alo, (i & 3) * 32 + lane, pw + NPROD * (i >> 2), xa[i]);
+          for (int i = 0; i < 32; ++i)
+            split_store(ahi, alo, 8 * (i & 15) + (lane & 7), 8 * pw + 4 * (i >> 4) + (lane >> 3), xa[i]);
         }
         // the segment's alpha is folded into B
         if (S.tB) {
@@ -187,7 +190,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           for (int i = 0; i < 16; ++i) split_store(bhi, blo, pw + NPROD * i, lane, S.alpha * xb[i]);
         } else {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) split_store(bhi, blo, (i & 1) * 32 + lane, pw + NPROD * (i >> 1), S.alpha * xb[i]);
+          for (int i = 0; i < 16; ++i)
+            split_store(bhi, blo, 8 * (i & 7) + (lane & 7), 8 * pw + 4 * (i >> 3) + (lane >> 3), S.alpha * xb[i]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();

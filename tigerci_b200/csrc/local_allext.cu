@@ -202,7 +202,8 @@ struct tci_local {
       throw Error(TCI_ERR_MEMORY, "device allocation failed (local all-external tables)");
     }
     owned.push_back(d);
-    LCUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    // stream-ordered before the kernels that read it (see sigma_device.cu upload)
+    LCUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     return d;
   }
   double* alloc(size_t n) {
@@ -384,7 +385,7 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
                     sizeof(double) * (size_t)(a + 1) * nchol);
       }
       double* tmp = L->alloc(lvv.size());
-      LCUDA(cudaMemcpy(tmp, lvv.data(), lvv.size() * sizeof(double), cudaMemcpyHostToDevice));
+      LCUDA(cudaMemcpyAsync(tmp, lvv.data(), lvv.size() * sizeof(double), cudaMemcpyHostToDevice, L->stream));
       L->LT = L->alloc(lvv.size());
       dim3 grid((unsigned)((nchol + 31) / 32), (unsigned)((L->npv + 31) / 32));
       transpose_l<<<grid, dim3(32, 8), 0, L->stream>>>(tmp, L->npv, nchol, L->LT);
@@ -400,13 +401,13 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
     L->R = L->alloc((size_t)dtot);
     L->Cb = L->alloc((size_t)total_len);
     L->Sb = L->alloc((size_t)total_len);
-    LCUDA(cudaMemset(L->Cb, 0, sizeof(double) * (size_t)total_len));
+    LCUDA(cudaMemsetAsync(L->Cb, 0, sizeof(double) * (size_t)total_len, L->stream));
     L->dheads = L->upload(L->heads);
     L->dblocks = L->upload(L->blocks);
     L->ddom = L->upload(dom);
     LCUDA(cudaMalloc(&L->status, sizeof(int)));
     L->owned.push_back(L->status);
-    LCUDA(cudaMemset(L->status, 0, sizeof(int)));
+    LCUDA(cudaMemsetAsync(L->status, 0, sizeof(int), L->stream));
     if (L->precision == 1) LCUDA(tci_gtc_host::prepare());
 
     // autotuner: chunk size (largest, half) x FP64 tile shape of the second GEMM; one timed run each

@@ -262,44 +262,76 @@ __global__ void __launch_bounds__(256, 2) gemm_tiled_f64(const DGemmProblem* __r
   }
 }
 
-__global__ void axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg, const DAxpySource* __restrict__ src) {
-  const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (w >= ntg) return;
-  const DAxpyTarget T = tg[w];
-  if (T.len < 8 && T.src_end - T.src_begin > 8) {
-    // short target, many sources: lanes stride over the sources, fixed-order warp reduction
+// Segmented AXPY: target chunk t (at most AXPY_CHUNK elements) gets
+//   dst[i] += sum_s coef_s * scale_s * src_s[base + i].
+// One block per chunk; warp w takes the sources w, w + 8, ... in table order,
+// and the eight warps' partial sums are added in warp order, so the result is
+// independent of timing.  A short target with many sources spreads the
+// sources over all threads instead.
+constexpr int AXPY_CHUNK = 256;
+__global__ void __launch_bounds__(256) axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg,
+                                                     const DAxpySource* __restrict__ src) {
+  __shared__ double part[8][AXPY_CHUNK];
+  const long long t = blockIdx.x;
+  if (t >= ntg) return;
+  const DAxpyTarget T = tg[t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (T.len < 8 && T.src_end - T.src_begin > 64) {
     for (long long i = 0; i < T.len; ++i) {
       double acc = 0.0;
-      for (long long s = T.src_begin + lane; s < T.src_end; s += 32) {
+      for (long long s = T.src_begin + threadIdx.x; s < T.src_end; s += 256) {
         const DAxpySource S = src[s];
         const double c = S.scale ? S.coef * (*S.scale) : S.coef;
         acc = fma(c, S.src[T.base + i], acc);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) T.dst[i] += acc;
+      if (lane == 0) part[warp][0] = acc;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += part[w][0];
+        T.dst[i] += v;
+      }
+      __syncthreads();
     }
     return;
   }
-  for (long long i = lane; i < T.len; i += 32) {
-    double acc = 0.0;
-    for (long long s = T.src_begin; s < T.src_end; ++s) {
-      const DAxpySource S = src[s];
-      const double c = S.scale ? S.coef * (*S.scale) : S.coef;
-      acc = fma(c, S.src[T.base + i], acc);
+  double acc[AXPY_CHUNK / 32];
+#pragma unroll
+  for (int e = 0; e < AXPY_CHUNK / 32; ++e) acc[e] = 0.0;
+  for (long long s = T.src_begin + warp; s < T.src_end; s += 8) {
+    const DAxpySource S = src[s];
+    const double c = S.scale ? S.coef * (*S.scale) : S.coef;
+    const double* x = S.src + T.base;
+#pragma unroll
+    for (int e = 0; e < AXPY_CHUNK / 32; ++e) {
+      const long long i = lane + 32 * e;
+      if (i < T.len) acc[e] = fma(c, x[i], acc[e]);
     }
-    T.dst[i] += acc;
+  }
+#pragma unroll
+  for (int e = 0; e < AXPY_CHUNK / 32; ++e) part[warp][lane + 32 * e] = acc[e];
+  __syncthreads();
+  if (threadIdx.x < T.len) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) v += part[w][threadIdx.x];
+    T.dst[threadIdx.x] += v;
   }
 }
 
-__global__ void dot_segments(const DDotTarget* __restrict__ tg, long long ntg, const DDotSource* __restrict__ src) {
-  const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (w >= ntg) return;
-  const DDotTarget T = tg[w];
+// Segmented dot products: *dst += sum_s coef_s (a_s . b_s).  One block per
+// target; warp w takes the sources w, w + 8, ...; fixed-order reductions.
+__global__ void __launch_bounds__(256) dot_segments(const DDotTarget* __restrict__ tg, long long ntg,
+                                                    const DDotSource* __restrict__ src) {
+  __shared__ double part[8];
+  const long long t = blockIdx.x;
+  if (t >= ntg) return;
+  const DDotTarget T = tg[t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double total = 0.0;
-  for (long long s = T.src_begin; s < T.src_end; ++s) {
+  for (long long s = T.src_begin + warp; s < T.src_end; s += 8) {
     const DDotSource S = src[s];
     double acc = 0.0;
     for (long long i = lane; i < S.len; i += 32) acc = fma(S.a[i], S.b[i], acc);
@@ -307,10 +339,15 @@ __global__ void dot_segments(const DDotTarget* __restrict__ tg, long long ntg, c
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     total = fma(S.coef, acc, total);
   }
-  if (lane == 0) *T.dst += total;
+  if (lane == 0) part[warp] = total;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < 8; ++w) v += part[w];
+    *T.dst += v;
+  }
 }
 
-// D[dk](j,i) = c_ab[k][i(i-1)/2+j], D(i,j) = p * same (i > j); D(a,a) = sqrt2 c_aa[k][a]
 __global__ void unpack_pairs(const DHead* __restrict__ heads, const int* __restrict__ dk_head, long long nD, long long n,
                              const double* __restrict__ c, double* __restrict__ D) {
   const long long dk = blockIdx.y;
@@ -546,13 +583,16 @@ struct DevStep {
   long long zlen = 0;
 };
 
+// Device copy of a host table, ordered on `st` before the kernels that read it.
+// (A plain cudaMemcpy from pageable memory may return before its DMA lands, and
+// runs on the legacy stream, which a non-blocking stream does not wait for.)
 template <class T>
-T* upload(const std::vector<T>& v, std::vector<void*>& owned) {
+T* upload(const std::vector<T>& v, std::vector<void*>& owned, cudaStream_t st) {
   if (v.empty()) return nullptr;
   T* d = nullptr;
   TCI_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
   owned.push_back(d);
-  TCI_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  TCI_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   return d;
 }
 
@@ -669,8 +709,8 @@ struct tci_ctx {
           check_range(x.b, x.offB, (rb - 1) * x.ldb + cb);
         }
       }
-      d.probs = upload(pr, owned);
-      d.segs = upload(sg, owned);
+      d.probs = upload(pr, owned, stream);
+      d.segs = upload(sg, owned, stream);
       d.nprob = (int)pr.size();
       d.ntiles = tiles;
       if (s.name != "all-external" && !pr.empty()) {
@@ -705,18 +745,18 @@ struct tci_ctx {
           useful += (double)g.M * (double)g.N * k;
           issued += (double)((g.M + TM - 1) / TM * TM) * (double)((g.N + TN - 1) / TN * TN) * k;
         }
-        d.probs_f = upload(pf, owned);
-        d.segs_f = upload(sf, owned);
+        d.probs_f = upload(pf, owned, stream);
+        d.segs_f = upload(sf, owned, stream);
         d.nprob_f = (int)pf.size();
-        d.probs_tc = upload(pt, owned);
-        d.segs_tc = upload(st, owned);
+        d.probs_tc = upload(pt, owned, stream);
+        d.segs_tc = upload(st, owned, stream);
         d.nprob_tc = (int)pt.size();
         d.tc_ok = flops >= 5e7 && useful >= 0.25 * issued;
       }
     } else if (s.kind == STEP_AXPY) {
       std::vector<DAxpyTarget> t;
       std::vector<DAxpySource> so;
-      constexpr i64 kChunk = 1024;  // elements per warp: long rows are spread over many warps
+      constexpr i64 kChunk = AXPY_CHUNK;  // elements per block: long rows are spread over many blocks
       for (auto& x : s.at) {
         check_range(x.dst, x.off, x.len);
         for (i64 b = 0; b < x.len; b += kChunk)
@@ -728,8 +768,8 @@ struct tci_ctx {
       }
       for (auto& x : s.at)
         for (i64 q = x.src_begin; q < x.src_end; ++q) check_range(s.as[q].src, s.as[q].off, x.len);
-      d.at = upload(t, owned);
-      d.as = upload(so, owned);
+      d.at = upload(t, owned, stream);
+      d.as = upload(so, owned, stream);
       d.ntg = (long long)t.size();
     } else if (s.kind == STEP_DOT) {
       std::vector<DDotTarget> t;
@@ -740,8 +780,8 @@ struct tci_ctx {
         check_range(x.b, x.boff, x.len);
         so.push_back(DDotSource{ptr(x.a, x.aoff), ptr(x.b, x.boff), x.len, x.coef});
       }
-      d.dt = upload(t, owned);
-      d.ds = upload(so, owned);
+      d.dt = upload(t, owned, stream);
+      d.ds = upload(so, owned, stream);
       d.ntg = (long long)t.size();
     } else if (s.kind == STEP_ZERO) {
       check_range(s.buf, s.off, s.len);
@@ -761,7 +801,7 @@ struct tci_ctx {
     std::vector<DDiag> e;
     for (auto& d : plan.diag) e.push_back(DDiag{d.off, d.len, d.type, d.beta, d.foff, d.singlet});
     for (auto& d : plan.diag) check_range(BUF_S, d.off, d.len);
-    DDiag* de = upload(e, owned);
+    DDiag* de = upload(e, owned, stream);
     if (!e.empty())
       build_diag_kernel<<<(unsigned)e.size(), 256, 0, stream>>>(de, (long long)e.size(), plan.n, plan.np, plan.nm,
                                                                 buf[BUF_F], buf[BUF_W], hd);
@@ -1005,10 +1045,10 @@ struct tci_ctx {
         }
         break;
       case STEP_AXPY:
-        if (s.ntg > 0) axpy_segments<<<(unsigned)((s.ntg + 7) / 8), 256, 0, stream>>>(s.at, s.ntg, s.as);
+        if (s.ntg > 0) axpy_segments<<<(unsigned)s.ntg, 256, 0, stream>>>(s.at, s.ntg, s.as);
         break;
       case STEP_DOT:
-        if (s.ntg > 0) dot_segments<<<(unsigned)((s.ntg + 7) / 8), 256, 0, stream>>>(s.dt, s.ntg, s.ds);
+        if (s.ntg > 0) dot_segments<<<(unsigned)s.ntg, 256, 0, stream>>>(s.dt, s.ntg, s.ds);
         break;
       case STEP_ZERO:
         if (s.zlen > 0) TCI_CUDA(cudaMemsetAsync(s.zptr, 0, s.zlen * sizeof(double), stream));
@@ -1171,8 +1211,8 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
       dh.push_back(DHead{d.off_ab, d.off_aa, d.nsf_ab, d.nsf_aa, d.nsing, d.nD, d.dk0});
       for (i64 k = 0; k < d.nD; ++k) dkh.push_back((int)h);
     }
-    ctx->dheads = upload(dh, ctx->owned);
-    ctx->dk_head = upload(dkh, ctx->owned);
+    ctx->dheads = upload(dh, ctx->owned, ctx->stream);
+    ctx->dk_head = upload(dkh, ctx->owned, ctx->stream);
     for (auto& s : P.init_steps) ctx->init.push_back(ctx->lower(s));
     for (auto& s : P.sigma_steps) ctx->sigma.push_back(ctx->lower(s));
     for (auto& s : ctx->init) ctx->run(s);
