@@ -25,6 +25,7 @@
 #include "allext_tc.h"
 #include "gemm_tables.h"
 #include "gemm_tc.h"
+#include "gemm_tma.h"
 #include "host/capi_internal.h"
 #include "host/plan.h"
 
@@ -567,6 +568,11 @@ struct DevStep {
   DGemmSeg* segs_tc = nullptr;
   long long ntiles_tc = 0;
   int nprob_tc = 0;
+  // two-external step on the TMA-fed kernel (integrals x pair matrices); tables when the step qualifies
+  TmaProblem* tma_probs = nullptr;
+  TmaSeg* tma_segs = nullptr;
+  int tma_nprob = 0;
+  long long tma_ntiles = 0;
   DGemmProblem* probs_f = nullptr;  // its FP64 part (same-head one-electron-like segments)
   DGemmSeg* segs_f = nullptr;
   long long ntiles_f = 0;
@@ -619,6 +625,9 @@ struct tci_ctx {
   int64_t tc_kblock = 128;              // k elements per FP64 promotion block of the tensor-core product
   int64_t tc_mode = 0;                  // precision 1: other GEMM steps on the tensor cores by size (0), all (1), none (2)
   int64_t refine = 1;                   // precision 1: roots finished as FP64 Rayleigh quotients (keeps the FP64 W)
+  float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;  // split integrals / pair matrices
+  tci_gtma_host::TmaMaps tma_maps;
+  bool tma_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* uhi = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -670,6 +679,49 @@ struct tci_ctx {
     if (b < 0 || b >= NUM_BUFS || !buf[b]) throw Error(TCI_ERR_INTERNAL, "plan references an unallocated buffer");
     if (off < 0 || off > plan.buf_size[b]) throw Error(TCI_ERR_INTERNAL, "plan offset outside its buffer");
     return buf[b] + off;
+  }
+
+  // Tables of the TMA-fed two-external kernel: every tensor-core segment must be an n x n integral matrix
+  // (BUF_JK) times an n x n pair matrix (BUF_D); otherwise the step keeps the producer-fed kernel.
+  void lower_tma(const Step& s, DevStep& d, const std::vector<DGemmProblem>& pr) {
+    const i64 n = plan.n, n2 = n * n;
+    std::vector<double> psign((size_t)std::max<i64>(plan.nD, 1), 1.0);
+    for (const auto& h : plan.dheads)
+      for (i64 k = 0; k < h.nD; ++k) psign[(size_t)(h.dk0 + k)] = k < h.nsing ? 1.0 : -1.0;
+    std::vector<TmaProblem> tp;
+    std::vector<TmaSeg> ts;
+    long long tiles = 0;
+    const long long per = ((n + tci_gtma_host::tile_m() - 1) / tci_gtma_host::tile_m()) *
+                          ((n + tci_gtma_host::tile_n() - 1) / tci_gtma_host::tile_n());
+    size_t gi = 0;
+    for (const auto& g : s.gp) {
+      if (g.M <= 0 || g.N <= 0) continue;
+      const DGemmProblem& dp = pr[gi++];
+      if (g.M != n || g.N != n || g.ldc != n) return;
+      TmaProblem q{dp.C, tiles, g.beta, (long long)ts.size(), 0};
+      bool has_f = false;
+      for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
+        const GemmSeg& x = s.gs[(size_t)k];
+        if (x.a == BUF_F || x.b == BUF_F) {
+          has_f = true;
+          continue;
+        }
+        if (x.a != BUF_JK || x.b != BUF_D || x.K != n || x.lda != n || x.ldb != n || x.tA || x.tB || x.offA % n ||
+            x.offB % n2)
+          return;
+        ts.push_back(TmaSeg{x.offA / n, x.offB / n, x.alpha * psign[(size_t)(x.offB / n2)]});
+      }
+      q.seg_end = (long long)ts.size();
+      if (has_f) q.beta = 1.0;  // the FP64 part of the step runs first
+      if (q.seg_end == q.seg_begin && has_f) continue;
+      tp.push_back(q);
+      tiles += per;
+    }
+    if (tp.empty()) return;
+    d.tma_probs = upload(tp, owned, stream);
+    d.tma_segs = upload(ts, owned, stream);
+    d.tma_nprob = (int)tp.size();
+    d.tma_ntiles = tiles;
   }
 
   DevStep lower(const Step& s) {
@@ -752,6 +804,7 @@ struct tci_ctx {
         d.segs_tc = upload(st, owned, stream);
         d.nprob_tc = (int)pt.size();
         d.tc_ok = flops >= 5e7 && useful >= 0.25 * issued;
+        if (s.name == "dd two-external") lower_tma(s, d, pr);
       }
     } else if (s.kind == STEP_AXPY) {
       std::vector<DAxpyTarget> t;
@@ -868,7 +921,7 @@ struct tci_ctx {
         continue;
       }
       if (s.kind == STEP_GEMM && uses_tc(s)) {
-        k += (s.ntiles_f > 0 ? 1 : 0) + (s.ntiles_tc > 0 ? 1 : 0);
+        k += (s.ntiles_f > 0 ? 1 : 0) + ((s.tma_probs && tma_ready) ? 2 : (s.ntiles_tc > 0 ? 1 : 0));
         continue;
       }
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
@@ -966,6 +1019,21 @@ struct tci_ctx {
     TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
+    bool any_tma = false;
+    for (const auto& st : sigma) any_tma = any_tma || st.tma_probs;
+    if (any_tma && plan.nD > 0) {
+      const i64 n = plan.n, ld = tci_gtma_host::pitch(n);
+      const i64 xrows = plan.buf_size[BUF_JK] / n, drows = plan.nD * n;
+      alloc_f(&jk_hi, (size_t)(xrows * ld));
+      alloc_f(&jk_lo, (size_t)(xrows * ld));
+      alloc_f(&d_hi, (size_t)(drows * ld));
+      alloc_f(&d_lo, (size_t)(drows * ld));
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, jk_hi, jk_lo, stream));
+      std::string err;
+      if (!tci_gtma_host::prepare(tma_maps, jk_hi, jk_lo, xrows, d_hi, d_lo, drows, n, err))
+        throw Error(TCI_ERR_CUDA, err);
+      tma_ready = true;
+    }
     TCI_CUDA(cudaMemsetAsync(tc_status, 0, sizeof(int), stream));
     TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
     if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
@@ -1032,6 +1100,12 @@ struct tci_ctx {
       case STEP_GEMM:
         if (precision == 1 && s.name == "all-external") {
           run_allext_tc();
+          break;
+        }
+        if (uses_tc(s) && s.tma_probs && tma_ready) {
+          TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
+          TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * plan.n, plan.n, d_hi, d_lo, stream));
+          TCI_CUDA(tci_gtma_host::launch(tma_maps, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, tc_status, stream));
           break;
         }
         if (uses_tc(s)) {
@@ -1150,7 +1224,10 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                                   tci_tc_host::padded_ld(P.np) +
                               (P.nm > 0 ? 2.0 * (double)tci_tc_host::padded_rows(std::max<i64>(1, P.n_trip)) *
                                               tci_tc_host::padded_ld(P.nm)
-                                        : 0.0));
+                                        : 0.0) +
+                              // split integrals and pair matrices of the TMA-fed two-external step
+                              2.0 * (double)tci_gtma_host::pitch(P.n) *
+                                  (double)(P.buf_size[BUF_JK] / std::max<i64>(1, P.n) + P.nD * P.n));
     pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
     res += f32 - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
