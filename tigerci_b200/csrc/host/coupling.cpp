@@ -30,8 +30,11 @@ inline bool create(Det& d, int x, double& ph) {
 }  // namespace
 
 const CsfExpansion& CouplingEngine::expand(const Config& c) {
-  auto it = cache_.find(c.occ);
-  if (it != cache_.end()) return *it->second;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = cache_.find(c.occ);
+    if (it != cache_.end()) return *it->second;
+  }
   auto e = std::make_unique<CsfExpansion>();
   const int n = (int)c.occ.size();
   if (2 * n > 128) throw Error(4, "coupling engine supports at most 64 orbitals");
@@ -51,6 +54,9 @@ const CsfExpansion& CouplingEngine::expand(const Config& c) {
     e->dets.push_back(d);
     e->index[d] = (int)r;
   }
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = cache_.find(c.occ);
+  if (it != cache_.end()) return *it->second;  // another thread expanded it meanwhile
   auto& ref = *e;
   cache_[c.occ] = std::move(e);
   return ref;

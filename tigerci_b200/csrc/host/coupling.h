@@ -13,6 +13,7 @@
 #include "tci_host.h"
 
 #include <memory>
+#include <mutex>
 
 namespace tci {
 
@@ -48,6 +49,7 @@ class CouplingEngine {
 
  private:
   const SpinTables& tables_;
+  std::mutex mu_;  // expand() may be called from several threads; cached entries never move
   std::map<std::vector<int8_t>, std::unique_ptr<CsfExpansion>> cache_;
 };
 

@@ -19,7 +19,12 @@
 // (UNPACK -> products -> PACK), so one canonical external pattern fixes it.
 #include "plan.h"
 
+#include <omp.h>
+
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <memory>
 #include <tuple>
@@ -205,6 +210,7 @@ void Builder::internal_blocks() {
   };
   const Pat pats[4] = {{0, -1, -1, 0}, {1, e0, -1, 1}, {2, e0, e0, 2}, {2, e0, e1, 3}};
   const int ni = (int)nint;
+  bool bad_count = false;
   for (const Pat& pt : pats) {
     const auto& heads = sp.paths[pt.kind];
     auto nsf_of = [&](const Head& h) -> i64 {
@@ -218,12 +224,23 @@ void Builder::internal_blocks() {
     auto cfg = [&](const Head& h) {
       return pt.kind == 0 ? cfgV(h) : pt.kind == 1 ? cfgS(h, pt.x) : cfgD(h, pt.x, pt.y);
     };
-    std::map<std::pair<i64, i64>, std::vector<double>> blocks;
-    for (size_t hs = 0; hs < heads.size(); ++hs) {
+    // Heads in parallel: every source head hs owns the blocks keyed (target, hs), so the per-thread maps
+    // merge without collisions and the merged (ordered) map does not depend on the schedule.
+    std::vector<std::map<std::pair<i64, i64>, std::vector<double>>> tblocks((size_t)omp_get_max_threads());
+    std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
+    for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long hsl = 0; hsl < (long long)heads.size(); ++hsl) {
+      const size_t hs = (size_t)hsl;
+      auto& blocks = tblocks[(size_t)omp_get_thread_num()];
+      CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
       const Head& S = heads[hs];
       if (!S.kept || nsf_of(S) == 0) continue;
-      const CsfExpansion& eS = eng->expand(cfg(S));
-      if (eS.nsf != nsf_of(S)) throw Error(4, "spin-function count mismatch in zero-external block");
+      const CsfExpansion& eS = E.expand(cfg(S));
+      if (eS.nsf != nsf_of(S)) {
+        bad_count = true;
+        continue;
+      }
       for (size_t r = 0; r < eS.dets.size(); ++r) {
         const double* thS = eS.basis->coeff.data() + r * eS.nsf;
         const Det d0 = eS.dets[r];
@@ -238,7 +255,7 @@ void Builder::internal_blocks() {
           for (int p = 0; p < ni; ++p) o[p] = (int8_t)(((d >> (2 * p)) & 1) + ((d >> (2 * p + 1)) & 1));
           const Head* Tg = find(pt.kind, o);
           if (!Tg || nsf_of(*Tg) == 0) return;
-          const CsfExpansion& eT = eng->expand(cfg(*Tg));
+          const CsfExpansion& eT = E.expand(cfg(*Tg));
           auto it = eT.index.find(d);
           if (it == eT.index.end()) return;
           const double* thT = eT.basis->coeff.data() + (size_t)it->second * eT.nsf;
@@ -308,6 +325,10 @@ void Builder::internal_blocks() {
               }
       }
     }
+    if (bad_count) throw Error(4, "spin-function count mismatch in zero-external block");
+    std::map<std::pair<i64, i64>, std::vector<double>> blocks;
+    for (auto& tb : tblocks)
+      for (auto& kv : tb) blocks[kv.first] = std::move(kv.second);
     for (auto& kv : blocks)
       if (kv.first.first == kv.first.second) {
         const i64 ns = nsf_of(heads[kv.first.first]);
@@ -864,12 +885,19 @@ void Builder::ss() {
 // SV: sigma_mu[k'] += c_v[k] w ; sigma_v[k] += <w, c_mu[k']>.
 // ops e_{xi,jk} = a+_x a+_j a_k a_i with (xi|jk), and E_xi with h_xi.
 void Builder::sv() {
-  std::map<std::pair<i64, i64>, std::vector<double>> wmap;  // (mu row, v csf) -> w
-  for (size_t hv = 0; hv < sp.paths[0].size(); ++hv) {
-    const Head& V = sp.paths[0][hv];
+  // (mu row, v csf) -> w; valence heads in parallel, each owning the keys of its own CSFs
+  std::vector<std::map<std::pair<i64, i64>, std::vector<double>>> twmap((size_t)omp_get_max_threads());
+  std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
+  for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long hvl = 0; hvl < (long long)sp.paths[0].size(); ++hvl) {
+    auto& wmap = twmap[(size_t)omp_get_thread_num()];
+    CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
+    const Head& V = sp.paths[0][(size_t)hvl];
     if (!has(V)) continue;
     auto add = [&](const Head* Mu, Op o, const double* vec, double hval_scale, i64 hi) {
-      auto m = M(cfgS(*Mu, e0), cfgV(V), o);  // predicted 1
+      std::vector<double> m;
+      E.matrix(cfgS(*Mu, e0), cfgV(V), o, m);  // predicted 1
       for (i64 kt = 0; kt < Mu->nsf; ++kt)
         for (i64 ks = 0; ks < V.nsf; ++ks) {
           const double a = m[kt * V.nsf + ks];
@@ -883,34 +911,44 @@ void Builder::sv() {
           }
         }
     };
+    // one working occupation, changed in place (no allocation per candidate)
+    std::vector<int8_t> o(V.occ.begin(), V.occ.end());
     for (i64 i = 0; i < nint; ++i) {
       if (V.occ[i] == 0) continue;
-      std::vector<int8_t> o1(V.occ.begin(), V.occ.end());
-      o1[i] -= 1;
-      if (const Head* Mu = find(1, o1); Mu && has(*Mu)) add(Mu, Op{e0, (int)i, -1, -1}, nullptr, 1.0, i);
+      o[i] -= 1;
+      if (const Head* Mu = find(1, o); Mu && has(*Mu)) add(Mu, Op{e0, (int)i, -1, -1}, nullptr, 1.0, i);
       for (i64 k = 0; k < nint; ++k) {
-        if (o1[k] == 0) continue;
-        std::vector<int8_t> o2 = o1;
-        o2[k] -= 1;
+        if (o[k] == 0) continue;
+        o[k] -= 1;
         for (i64 j = 0; j < nint; ++j) {
-          if (o2[j] == 2) continue;
-          std::vector<int8_t> o3 = o2;
-          o3[j] += 1;
-          const Head* Mu = find(1, o3);
-          if (!Mu || !has(*Mu)) continue;
-          // (xi|jk) = (ix|jk) = I3[i][j][k][x]
-          add(Mu, Op{e0, (int)i, (int)j, (int)k}, I.i3(i, j, k), 0.0, 0);
+          if (o[j] == 2) continue;
+          o[j] += 1;
+          const Head* Mu = find(1, o);
+          if (Mu && has(*Mu)) add(Mu, Op{e0, (int)i, (int)j, (int)k}, I.i3(i, j, k), 0.0, 0);  // (xi|jk) = I3[i][j][k][x]
+          o[j] -= 1;
         }
+        o[k] += 1;
       }
+      o[i] += 1;
     }
   }
+  std::map<std::pair<i64, i64>, std::vector<double>> wmap;
+  for (auto& tw : twmap)
+    for (auto& kv : tw) wmap[kv.first] = std::move(kv.second);
   if (wmap.empty()) return;
   const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
   std::vector<std::pair<std::pair<i64, i64>, i64>> rows;
+  std::vector<const std::vector<double>*> src;
   for (auto& kv : wmap) {
     rows.push_back({kv.first, wbase + (i64)rows.size()});
-    P.wv.insert(P.wv.end(), kv.second.begin(), kv.second.end());
+    src.push_back(&kv.second);
   }
+  // one allocation, rows copied in parallel (hundreds of MB at the kernel-scale size)
+  const size_t w0 = P.wv.size();
+  P.wv.resize(w0 + src.size() * (size_t)n);
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < (long long)src.size(); ++t)
+    std::copy(src[(size_t)t]->begin(), src[(size_t)t]->end(), P.wv.begin() + (std::ptrdiff_t)(w0 + (size_t)t * n));
   Step& fw = step(P.sigma_steps, STEP_AXPY, "sv forward");
   std::map<i64, std::vector<size_t>> by_mu;
   for (size_t t = 0; t < rows.size(); ++t) by_mu[rows[t].first.first].push_back(t);
@@ -1141,23 +1179,43 @@ void Builder::run() {
   I.N = N;
   I.h = op.h;
   I.L = op.chol;
+  // TCI_PLAN_TIMING=1 prints the wall time of every phase of the plan build to stderr
+  const bool timing = std::getenv("TCI_PLAN_TIMING") != nullptr;
+  auto t_last = std::chrono::steady_clock::now();
+  auto tick = [&](const char* what) {
+    if (!timing) return;
+    const auto t = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "plan %-16s %8.3f s\n", what, std::chrono::duration<double>(t - t_last).count());
+    t_last = t;
+  };
+  tick("spin tables");
   I.build();
+  tick("integrals");
   offJ = 0;
   offK = nint * nint * n2;
   offH = 2 * nint * nint * n2;
   setup_heads();
   init_steps();
+  tick("heads, init");
   zero_step(P.sigma_steps, BUF_R, 0, P.nD * n2, "zero accumulators");
   step(P.sigma_steps, STEP_UNPACK, "unpack");
   allext();
+  tick("all-external");
   dd_x();
+  tick("dd");
   ds();
+  tick("ds");
   dv();
+  tick("dv");
   ss();
+  tick("ss");
   sv();
+  tick("sv");
   internal_blocks();
+  tick("internal");
   step(P.sigma_steps, STEP_PACK, "pack");
   build_diag();
+  tick("diagonal");
   P.h_vv.assign(n2, 0.0);
   for (i64 a = 0; a < n; ++a)
     for (i64 b = 0; b < n; ++b) P.h_vv[a * n + b] = I.h1(nint + a, nint + b);
