@@ -263,6 +263,48 @@ __global__ void __launch_bounds__(256, 2) gemm_tiled_f64(const DGemmProblem* __r
   }
 }
 
+// Skinny grouped GEMM (M <= SKINNY_M, B given as N x K): one warp per output
+// column n of a problem computes C[m][n] for every row m as dot products over
+// the segments (lanes along k, fixed-order warp reductions).  Covers the
+// one-row products that would fill 1/64 of a tile of the tiled kernel.
+constexpr int SKINNY_M = 8;
+__global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __restrict__ probs, int nprob,
+                                                       const DGemmSeg* __restrict__ segs, long long nwarps) {
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nwarps) return;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile_begin <= w) lo = mid;
+    else hi = mid - 1;
+  }
+  const DGemmProblem P = probs[lo];
+  const long long n = w - P.tile_begin;
+  double acc[SKINNY_M];
+#pragma unroll
+  for (int m = 0; m < SKINNY_M; ++m) acc[m] = 0.0;
+  for (long long q = P.seg_begin; q < P.seg_end; ++q) {
+    const DGemmSeg S = segs[q];
+    const double* b = S.B + n * S.ldb;
+#pragma unroll
+    for (int m = 0; m < SKINNY_M; ++m) {
+      if (m >= P.M) break;
+      const double* a = S.A + m * S.lda;
+      double d = 0.0;
+      for (long long k = lane; k < S.K; k += 32) d = fma(a[k], b[k], d);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+      acc[m] = fma(S.alpha, d, acc[m]);
+    }
+  }
+  if (lane == 0)
+    for (int m = 0; m < SKINNY_M && m < P.M; ++m) {
+      double* c = P.C + m * P.ldc + n;
+      *c = (P.beta == 0.0 ? 0.0 : P.beta * *c) + acc[m];
+    }
+}
+
 // Segmented AXPY: target chunk t (at most AXPY_CHUNK elements) gets
 //   dst[i] += sum_s coef_s * scale_s * src_s[base + i].
 // One block per chunk; warp w takes the sources w, w + 8, ... in table order,
@@ -573,6 +615,10 @@ struct DevStep {
   TmaSeg* tma_segs = nullptr;
   int tma_nprob = 0;
   long long tma_ntiles = 0;
+  // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
+  DGemmProblem* skinny_probs = nullptr;
+  int skinny_nprob = 0;
+  long long skinny_nwarps = 0;
   DGemmProblem* probs_f = nullptr;  // its FP64 part (same-head one-electron-like segments)
   DGemmSeg* segs_f = nullptr;
   long long ntiles_f = 0;
@@ -761,10 +807,33 @@ struct tci_ctx {
           check_range(x.b, x.offB, (rb - 1) * x.ldb + cb);
         }
       }
-      d.probs = upload(pr, owned, stream);
       d.segs = upload(sg, owned, stream);
-      d.nprob = (int)pr.size();
-      d.ntiles = tiles;
+      {
+        // FP64 form: skinny problems (one-row products) to the warp-per-column kernel, the rest tiled
+        std::vector<DGemmProblem> reg, sk;
+        long long rt = 0, wk = 0;
+        for (const auto& g : pr) {
+          bool skinny = g.M <= SKINNY_M && s.name != "all-external";
+          for (long long q = g.seg_begin; skinny && q < g.seg_end; ++q) skinny = sg[(size_t)q].tA == 0 && sg[(size_t)q].tB == 1;
+          if (skinny) {
+            DGemmProblem x = g;
+            x.tile_begin = wk;  // first warp (one per output column)
+            wk += g.N;
+            sk.push_back(x);
+          } else {
+            DGemmProblem x = g;
+            x.tile_begin = rt;
+            rt += ((g.M + BMh - 1) / BMh) * x.tiles_n;
+            reg.push_back(x);
+          }
+        }
+        d.probs = upload(reg, owned, stream);
+        d.nprob = (int)reg.size();
+        d.ntiles = rt;
+        d.skinny_probs = upload(sk, owned, stream);
+        d.skinny_nprob = (int)sk.size();
+        d.skinny_nwarps = wk;
+      }
       if (s.name != "all-external" && !pr.empty()) {
         // Mixed form.  Segments whose operand is a same-head one-electron-like operator (BUF_F: h, J_ii,
         // K_ii combinations, orbital-energy magnitudes) stay on the FP64 kernel; the cross-head integral
@@ -924,6 +993,7 @@ struct tci_ctx {
         k += (s.ntiles_f > 0 ? 1 : 0) + ((s.tma_probs && tma_ready) ? 2 : (s.ntiles_tc > 0 ? 1 : 0));
         continue;
       }
+      if (s.kind == STEP_GEMM && s.skinny_nwarps > 0) k += 1;
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
           ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && plan.nD > 0))
         k += 1;
@@ -1113,6 +1183,9 @@ struct tci_ctx {
           TCI_CUDA(tci_gtc_host::launch(s.probs_tc, s.nprob_tc, s.segs_tc, s.ntiles_tc, tc_status, (int)tc_kblock, stream));
           break;
         }
+        if (s.skinny_nwarps > 0)
+          gemm_skinny_f64<<<(unsigned)((s.skinny_nwarps + 7) / 8), 256, 0, stream>>>(s.skinny_probs, s.skinny_nprob,
+                                                                                  s.segs, s.skinny_nwarps);
         if (s.ntiles > 0) {
           if (s.cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
           else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
