@@ -1,23 +1,23 @@
-// Two-external (internal pair) step of the mixed form fed entirely by TMA:
+// Grouped 3xTF32 GEMM on tcgen05 fed entirely by TMA, for plan steps whose
+// operands are rows of two fixed arrays (mixed form):
 //
-//   R_t (n x n) = beta R_t + sum_s alpha_s X_s D_s
+//   C_p = beta C_p + sum_s alpha_s A[a_row_s + m, k0_s + k] B[b_row_s + n, k0_s + k]
 //
-// X_s is a (ij|ab) or (ia|jb) integral matrix (static), D_s the dense pair
-// matrix of a source CI block (rebuilt every sigma).  Both are kept as TF32
-// high / FP32 low parts in HBM (integrals split once at set-up, the pair
-// matrices split by a small kernel right after they are unpacked), so the
-// kernel streams them with TMA into the 128-byte-swizzle K-major layout with
-// no conversion in the loop.  D_s enters as the K-major B operand through its
-// symmetry: a pair matrix of a singlet-coupled function is symmetric and of a
-// triplet-coupled one antisymmetric, so D^T = p D and the sign p folds into
-// alpha.  Each segment (K = n) is one FP32 accumulation block in TMEM; the
-// epilogue adds alpha_s p_s times it into FP64 registers, so the segments'
-// coefficients never touch the operands.
+// Both arrays are kept as TF32 high / FP32 low parts in HBM (static operands
+// split once at set-up, per-sigma operands split by a small kernel right after
+// they are produced), so the kernel streams K-major tiles straight into the
+// 128-byte-swizzle layout with no conversion in the loop.  Users: the
+// two-external step (integral matrices x pair matrices; the pair matrix enters
+// as the K-major B operand through its symmetry, D^T = p D, the sign folded
+// into alpha) and the forward three-external step (V_i rows x pair-matrix rows,
+// computed transposed).  A segment's k steps form FP32 accumulation blocks of
+// at most kblock elements in a double-buffered TMEM accumulator; the epilogue
+// adds alpha_s times each block into FP64 registers, so the coefficients never
+// touch the operands, and writes C (or C^T) once.
 //
 // Warp roles (192 threads): 0-3 epilogue, 4 TMA producer, 5 TMEM allocator +
-// MMA issuer.  Bounded waits as in the other tcgen05 kernels; on an abort the
-// kernel waits (bounded) for its copies and MMAs in flight, frees its TMEM and
-// returns.
+// MMA issuer.  Bounded waits; on an abort the kernel waits (bounded) for its
+// copies and MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -50,9 +50,9 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1)
-    gemm_tma_tf32x3(const __grid_constant__ CUtensorMap xhi, const __grid_constant__ CUtensorMap xlo,
-                    const __grid_constant__ CUtensorMap dhi, const __grid_constant__ CUtensorMap dlo,
-                    const TmaProblem* __restrict__ probs, int nprob, const TmaSeg* __restrict__ segs, int n,
+    gemm_tma_tf32x3(const __grid_constant__ CUtensorMap ahi_map, const __grid_constant__ CUtensorMap alo_map,
+                    const __grid_constant__ CUtensorMap bhi_map, const __grid_constant__ CUtensorMap blo_map,
+                    const TmaProblem* __restrict__ probs, int nprob, const TmaSeg* __restrict__ segs, int kbs,
                     int* __restrict__ status) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -73,11 +73,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   }
   const TmaProblem P = probs[lo];
   const long long t = tile - P.tile_begin;
-  const int tiles_n = (n + BN - 1) / BN;
-  const int m0 = (int)(t / tiles_n) * BM, n0 = (int)(t % tiles_n) * BN;
-  const int ksteps = (n + BK - 1) / BK;       // per segment: one FP32 accumulation block
-  const int nseg = (int)(P.seg_end - P.seg_begin);
-  const int nsteps = nseg * ksteps;
+  const int m0 = (int)(t / P.tiles_n) * BM, n0 = (int)(t % P.tiles_n) * BN;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -112,56 +108,65 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 4) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
-      int last = -1;
-      for (int step = 0; step < nsteps && !aborted(); ++step) {
-        const int s = step % STAGES;
-        if (step >= STAGES && !mbar_wait(&empty[s], ((step / STAGES) - 1) & 1)) {
-          fail(ST_TIMEOUT_EMPTY);
-          break;
+      int step = 0, last = -1;
+      for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
+        const TmaSeg S = segs[q];
+        const int nk = (int)((S.K + BK - 1) / BK);
+        for (int kk = 0; kk < nk && !aborted(); ++kk, ++step) {
+          const int s = step % STAGES;
+          if (step >= STAGES && !mbar_wait(&empty[s], ((step / STAGES) - 1) & 1)) {
+            fail(ST_TIMEOUT_EMPTY);
+            break;
+          }
+          const int x = (int)S.k0 + kk * BK;
+          uint8_t* st = base + s * STAGE_BYTES;
+          mbar_expect_tx(&full[s], 2 * A_BYTES + 2 * B_BYTES);
+          tma_load_2d(st, &ahi_map, &full[s], x, (int)S.a_row + m0);
+          tma_load_2d(st + A_BYTES, &alo_map, &full[s], x, (int)S.a_row + m0);
+          tma_load_2d(st + 2 * A_BYTES, &bhi_map, &full[s], x, (int)S.b_row + n0);
+          tma_load_2d(st + 2 * A_BYTES + B_BYTES, &blo_map, &full[s], x, (int)S.b_row + n0);
+          last = step;
         }
-        const TmaSeg S = segs[P.seg_begin + step / ksteps];
-        const int k0 = (step % ksteps) * BK;
-        uint8_t* st = base + s * STAGE_BYTES;
-        mbar_expect_tx(&full[s], 2 * A_BYTES + 2 * B_BYTES);
-        tma_load_2d(st, &xhi, &full[s], k0, (int)S.x_row + m0);
-        tma_load_2d(st + A_BYTES, &xlo, &full[s], k0, (int)S.x_row + m0);
-        tma_load_2d(st + 2 * A_BYTES, &dhi, &full[s], k0, (int)S.d_row + n0);
-        tma_load_2d(st + 2 * A_BYTES + B_BYTES, &dlo, &full[s], k0, (int)S.d_row + n0);
-        last = step;
       }
       if (aborted())
-        for (int step = (last - STAGES + 1 > 0 ? last - STAGES + 1 : 0); step <= last; ++step)
-          mbar_wait(&full[step % STAGES], (step / STAGES) & 1);
+        for (int st = (last - STAGES + 1 > 0 ? last - STAGES + 1 : 0); st <= last; ++st)
+          mbar_wait(&full[st % STAGES], (st / STAGES) & 1);
     }
   } else if (warp == 5) {
-    // ---------------- MMA issuer: one TMEM block per segment ----------------
+    // ---------------- MMA issuer: blocks of at most kbs k steps, never across segments ----------------
     if (lane == 0) {
-      for (int step = 0; step < nsteps && !aborted(); ++step) {
-        const int s = step % STAGES;
-        const int blk = step / ksteps, buf = blk & 1;
-        const bool first = (step % ksteps) == 0;
-        if (first && blk >= 2 && !mbar_wait(&dempty[buf], ((blk / 2) - 1) & 1)) {
-          fail(ST_TIMEOUT_DE);
-          break;
-        }
-        if (!mbar_wait(&full[s], (step / STAGES) & 1)) {
-          fail(ST_TIMEOUT_FULL);
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        uint8_t* st = base + s * STAGE_BYTES;
-        const uint32_t d = tmem + (uint32_t)(buf * BN);
+      int step = 0, blk = 0;
+      for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
+        const int nk = (int)((segs[q].K + BK - 1) / BK);
+        for (int kk = 0; kk < nk && !aborted(); ++kk, ++step) {
+          const int s = step % STAGES, buf = blk & 1;
+          const bool first = (kk % kbs) == 0;
+          if (first && blk >= 2 && !mbar_wait(&dempty[buf], ((blk / 2) - 1) & 1)) {
+            fail(ST_TIMEOUT_DE);
+            break;
+          }
+          if (!mbar_wait(&full[s], (step / STAGES) & 1)) {
+            fail(ST_TIMEOUT_FULL);
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          uint8_t* st = base + s * STAGE_BYTES;
+          const uint32_t d = tmem + (uint32_t)(buf * BN);
 #pragma unroll
-        for (int kk = 0; kk < BK / 8; ++kk) {
-          const uint64_t ahi = smem_desc_sw128(st + kk * 32), alo = smem_desc_sw128(st + A_BYTES + kk * 32);
-          const uint64_t bhi = smem_desc_sw128(st + 2 * A_BYTES + kk * 32);
-          const uint64_t blo = smem_desc_sw128(st + 2 * A_BYTES + B_BYTES + kk * 32);
-          mma_tf32(d, ahi, bhi, kIdesc, (first && kk == 0) ? 0u : 1u);
-          mma_tf32(d, ahi, blo, kIdesc, 1u);
-          mma_tf32(d, alo, bhi, kIdesc, 1u);
+          for (int k8 = 0; k8 < BK / 8; ++k8) {
+            const uint64_t ahi = smem_desc_sw128(st + k8 * 32), alo = smem_desc_sw128(st + A_BYTES + k8 * 32);
+            const uint64_t bhi = smem_desc_sw128(st + 2 * A_BYTES + k8 * 32);
+            const uint64_t blo = smem_desc_sw128(st + 2 * A_BYTES + B_BYTES + k8 * 32);
+            mma_tf32(d, ahi, bhi, kIdesc, (first && k8 == 0) ? 0u : 1u);
+            mma_tf32(d, ahi, blo, kIdesc, 1u);
+            mma_tf32(d, alo, bhi, kIdesc, 1u);
+          }
+          mma_commit(&empty[s]);
+          if ((kk % kbs) == kbs - 1 || kk == nk - 1) {
+            mma_commit(&dfull[buf]);
+            ++blk;
+          }
         }
-        mma_commit(&empty[s]);
-        if ((step % ksteps) == ksteps - 1) mma_commit(&dfull[buf]);
       }
       if (aborted()) {
         mma_commit(mma_done);
@@ -169,36 +174,52 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
   } else {
-    // ---------------- epilogue: alpha_s * block -> FP64 registers -> R ----------------
-    const int r = m0 + warp * 32 + lane;
+    // ---------------- epilogue: alpha_s * block -> FP64 registers -> C ----------------
+    const long long r = m0 + warp * 32 + lane;
     double acc[BN];
 #pragma unroll
     for (int j = 0; j < BN; ++j) acc[j] = 0.0;
-    for (int blk = 0; blk < nseg && !aborted(); ++blk) {
-      const int buf = blk & 1;
-      const double a = segs[P.seg_begin + blk].alpha;
-      if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
-        fail(ST_TIMEOUT_D);
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;");
+    int blk = 0;
+    for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
+      const double a = segs[q].alpha;
+      const int nk = (int)((segs[q].K + BK - 1) / BK);
+      const int nb = (nk + kbs - 1) / kbs;
+      for (int b = 0; b < nb && !aborted(); ++b, ++blk) {
+        const int buf = blk & 1;
+        if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
+          fail(ST_TIMEOUT_D);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-      for (int c = 0; c < BN / 16; ++c) {
-        uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16), v);
+        for (int c = 0; c < BN / 16; ++c) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16), v);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
+          for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&dempty[buf]);
       }
-      asm volatile("tcgen05.fence::before_thread_sync;");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&dempty[buf]);
     }
-    if (!aborted() && r < n) {
-      double* crow = P.C + (long long)r * n;
+    if (!aborted() && r < P.M) {
+      if (!P.trans_c) {
+        double* crow = P.C + r * P.ldc;
 #pragma unroll
-      for (int j = 0; j < BN; ++j) {
-        const int c = n0 + j;
-        if (c < n) crow[c] = (P.beta == 0.0 ? 0.0 : P.beta * crow[c]) + acc[j];
+        for (int j = 0; j < BN; ++j) {
+          const long long c = n0 + j;
+          if (c < P.N) crow[c] = (P.beta == 0.0 ? 0.0 : P.beta * crow[c]) + acc[j];
+        }
+      } else {  // C^T: element (r, c) goes to C[c][r]; lanes hold consecutive r (coalesced)
+#pragma unroll
+        for (int j = 0; j < BN; ++j) {
+          const long long c = n0 + j;
+          if (c < P.N) {
+            double* y = P.C + c * P.ldc + r;
+            *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + acc[j];
+          }
+        }
       }
     }
   }
@@ -208,16 +229,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
 }
 
-// rows x n FP64 (row pitch n) -> TF32 hi / FP32 lo with row pitch ldp (columns n..ldp zero)
-__global__ void split_rows(const double* __restrict__ src, long long rows, int n, int ldp, float* __restrict__ hi,
-                           float* __restrict__ lo) {
+// rows x cols FP64 (row pitch ld) -> TF32 hi / FP32 lo with row pitch ldp (columns cols..ldp zero)
+__global__ void split_rows(const double* __restrict__ src, long long rows, long long cols, long long ld, long long ldp,
+                           float* __restrict__ hi, float* __restrict__ lo) {
   const long long total = rows * ldp;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const long long r = e / ldp;
-    const int c = (int)(e % ldp);
+    const long long r = e / ldp, c = e % ldp;
     float h = 0.0f, l = 0.0f;
-    if (c < n) {
-      const double x = src[r * n + c];
+    if (c < cols) {
+      const double x = src[r * ld + c];
       h = __uint_as_float(__float_as_uint((float)x) & 0xFFFFE000u);
       l = (float)(x - (double)h);
     }
@@ -279,20 +299,20 @@ namespace tci_gtma_host {
 
 int tile_m() { return tci_gtma::BM; }
 int tile_n() { return tci_gtma::BN; }
-int64_t pitch(int64_t n) { return (n + 31) / 32 * 32; }
+int64_t pitch(int64_t cols) { return (cols + 31) / 32 * 32; }
 
-cudaError_t split(const double* src, int64_t rows, int64_t n, float* hi, float* lo, cudaStream_t st) {
+cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st) {
   if (rows <= 0) return cudaSuccess;
-  tci_gtma::split_rows<<<148 * 8, 256, 0, st>>>(src, rows, (int)n, (int)pitch(n), hi, lo);
+  tci_gtma::split_rows<<<148 * 8, 256, 0, st>>>(src, rows, cols, ld, pitch(cols), hi, lo);
   return cudaGetLastError();
 }
 
-bool prepare(TmaMaps& m, const float* xhi, const float* xlo, int64_t xrows, const float* dhi, const float* dlo,
-             int64_t drows, int64_t n, std::string& err) {
-  m.n = n;
-  const uint64_t ldp = (uint64_t)pitch(n);
-  if (!make_map(&m.xhi, xhi, xrows, n, ldp, tci_gtma::BM, err) || !make_map(&m.xlo, xlo, xrows, n, ldp, tci_gtma::BM, err) ||
-      !make_map(&m.dhi, dhi, drows, n, ldp, tci_gtma::BN, err) || !make_map(&m.dlo, dlo, drows, n, ldp, tci_gtma::BN, err))
+bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int64_t acols, const float* bhi,
+             const float* blo, int64_t brows, int64_t bcols, std::string& err) {
+  if (!make_map(&m.ahi, ahi, arows, acols, pitch(acols), tci_gtma::BM, err) ||
+      !make_map(&m.alo, alo, arows, acols, pitch(acols), tci_gtma::BM, err) ||
+      !make_map(&m.bhi, bhi, brows, bcols, pitch(bcols), tci_gtma::BN, err) ||
+      !make_map(&m.blo, blo, brows, bcols, pitch(bcols), tci_gtma::BN, err))
     return false;
   static bool attr = false;
   if (!attr) {
@@ -307,10 +327,10 @@ bool prepare(TmaMaps& m, const float* xhi, const float* xlo, int64_t xrows, cons
 }
 
 cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const TmaSeg* segs, long long ntiles,
-                   int* status, cudaStream_t st) {
+                   int kblock, int* status, cudaStream_t st) {
   if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
   tci_gtma::gemm_tma_tf32x3<<<(unsigned)ntiles, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
-      m.xhi, m.xlo, m.dhi, m.dlo, probs, nprob, segs, (int)m.n, status);
+      m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, kblock / tci_gtma::BK, status);
   return cudaGetLastError();
 }
 

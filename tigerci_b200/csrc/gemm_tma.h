@@ -1,4 +1,4 @@
-// Host interface of the TMA-fed two-external kernel (gemm_tma.cu).
+// Host interface of the TMA-fed 3xTF32 grouped GEMM (gemm_tma.cu).
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -6,34 +6,37 @@
 #include <cstdint>
 #include <string>
 
-// R_t = beta R_t + sum over segments alpha X D (all n x n), tiles of 128 x 64
+// C (row pitch ldc) = beta C + sum over segments alpha A_rows B_rows^T, tiles of 128 x 64
 struct TmaProblem {
-  double* C;                    // R_t (row pitch n)
-  long long tile_begin;
+  double* C;
+  long long ldc, M, N, tiles_n, tile_begin;
   double beta;
   long long seg_begin, seg_end;
+  long long trans_c;  // the tile computes C^T: element (r, c) is stored at C[c][r]
 };
 struct TmaSeg {
-  long long x_row;              // first row of X in the split integral rows
-  long long d_row;              // first row of D in the split pair-matrix rows
-  double alpha;                 // coefficient times the transposition sign of D
+  long long a_row, b_row;  // first rows of the segment in the A and B arrays
+  long long k0, K;         // columns k0 .. k0+K-1 (k0 a multiple of 32; K ends on a multiple of 32 or the row end)
+  double alpha;
 };
 
 namespace tci_gtma_host {
 
+// TF32-high / FP32-low copies of two FP64 row arrays, and their tensor maps
 struct TmaMaps {
-  CUtensorMap xhi, xlo, dhi, dlo;
-  int64_t n = 0;
+  CUtensorMap ahi, alo, bhi, blo;
 };
 
 int tile_m();
 int tile_n();
-int64_t pitch(int64_t n);  // FP32 row pitch of the split arrays (multiple of 32)
-// rows x n FP64 (pitch n) -> hi / lo FP32 (pitch `pitch(n)`)
-cudaError_t split(const double* src, int64_t rows, int64_t n, float* hi, float* lo, cudaStream_t st);
-bool prepare(TmaMaps& m, const float* xhi, const float* xlo, int64_t xrows, const float* dhi, const float* dlo,
-             int64_t drows, int64_t n, std::string& err);
+int64_t pitch(int64_t cols);  // FP32 row pitch of a split array (multiple of 32)
+// rows x cols FP64 (row pitch ld) -> hi / lo FP32 (row pitch pitch(cols), zero padded)
+cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st);
+// maps over split arrays of arows x acols and brows x bcols
+bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int64_t acols, const float* bhi,
+             const float* blo, int64_t brows, int64_t bcols, std::string& err);
+// kblock: k elements per FP64 promotion block (multiple of 32)
 cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const TmaSeg* segs, long long ntiles,
-                   int* status, cudaStream_t st);
+                   int kblock, int* status, cudaStream_t st);
 
 }  // namespace tci_gtma_host

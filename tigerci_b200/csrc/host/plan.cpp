@@ -574,7 +574,8 @@ void Builder::ds() {
       if (used[i]) outs.push_back({Y + i * P.nD * n, i});
     // split-K over (q,s): the output is only nD x n, the contraction n^2 long
     const i64 S = std::max<i64>(1, std::min<i64>(32, n2 / 2048));
-    const i64 kc = (n2 + S - 1) / S;
+    // chunks start on multiples of 32 columns (the tensor-core form loads 32-column tiles by TMA)
+    const i64 kc = ((n2 + S - 1) / S + 31) / 32 * 32;
     const i64 Pt = T.alloc(S * (i64)outs.size() * P.nD * n);
     Step g = mkstep(STEP_GEMM, "three-external forward");
     for (size_t o = 0; o < outs.size(); ++o)

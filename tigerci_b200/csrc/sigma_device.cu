@@ -615,6 +615,7 @@ struct DevStep {
   TmaSeg* tma_segs = nullptr;
   int tma_nprob = 0;
   long long tma_ntiles = 0;
+  int tma_kind = 0;  // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows)
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
   DGemmProblem* skinny_probs = nullptr;
   int skinny_nprob = 0;
@@ -671,9 +672,11 @@ struct tci_ctx {
   int64_t tc_kblock = 128;              // k elements per FP64 promotion block of the tensor-core product
   int64_t tc_mode = 0;                  // precision 1: other GEMM steps on the tensor cores by size (0), all (1), none (2)
   int64_t refine = 1;                   // precision 1: roots finished as FP64 Rayleigh quotients (keeps the FP64 W)
-  float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;  // split integrals / pair matrices
-  tci_gtma_host::TmaMaps tma_maps;
-  bool tma_ready = false;
+  // split operands of the TMA-fed steps: integrals and V_i once, the pair matrices every build
+  float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;
+  float *v_hi = nullptr, *v_lo = nullptr, *df_hi = nullptr, *df_lo = nullptr;
+  tci_gtma_host::TmaMaps tma_dd, tma_t3;
+  bool tma_dd_ready = false, tma_t3_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* uhi = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -727,43 +730,72 @@ struct tci_ctx {
     return buf[b] + off;
   }
 
-  // Tables of the TMA-fed two-external kernel: every tensor-core segment must be an n x n integral matrix
-  // (BUF_JK) times an n x n pair matrix (BUF_D); otherwise the step keeps the producer-fed kernel.
+  // Tables of the TMA-fed kernel for the two-external step (every tensor-core segment an n x n integral
+  // matrix of BUF_JK times an n x n pair matrix of BUF_D) and the forward three-external step (pair-matrix
+  // rows times V_i rows, computed transposed); a step that does not fit keeps the producer-fed kernel.
   void lower_tma(const Step& s, DevStep& d, const std::vector<DGemmProblem>& pr) {
     const i64 n = plan.n, n2 = n * n;
-    std::vector<double> psign((size_t)std::max<i64>(plan.nD, 1), 1.0);
-    for (const auto& h : plan.dheads)
-      for (i64 k = 0; k < h.nD; ++k) psign[(size_t)(h.dk0 + k)] = k < h.nsing ? 1.0 : -1.0;
+    const i64 TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n();
     std::vector<TmaProblem> tp;
     std::vector<TmaSeg> ts;
     long long tiles = 0;
-    const long long per = ((n + tci_gtma_host::tile_m() - 1) / tci_gtma_host::tile_m()) *
-                          ((n + tci_gtma_host::tile_n() - 1) / tci_gtma_host::tile_n());
-    size_t gi = 0;
-    for (const auto& g : s.gp) {
-      if (g.M <= 0 || g.N <= 0) continue;
-      const DGemmProblem& dp = pr[gi++];
-      if (g.M != n || g.N != n || g.ldc != n) return;
-      TmaProblem q{dp.C, tiles, g.beta, (long long)ts.size(), 0};
-      bool has_f = false;
-      for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
-        const GemmSeg& x = s.gs[(size_t)k];
-        if (x.a == BUF_F || x.b == BUF_F) {
-          has_f = true;
-          continue;
-        }
-        if (x.a != BUF_JK || x.b != BUF_D || x.K != n || x.lda != n || x.ldb != n || x.tA || x.tB || x.offA % n ||
-            x.offB % n2)
-          return;
-        ts.push_back(TmaSeg{x.offA / n, x.offB / n, x.alpha * psign[(size_t)(x.offB / n2)]});
-      }
-      q.seg_end = (long long)ts.size();
-      if (has_f) q.beta = 1.0;  // the FP64 part of the step runs first
-      if (q.seg_end == q.seg_begin && has_f) continue;
+    auto push = [&](TmaProblem q) {
+      q.tiles_n = (q.N + TN - 1) / TN;
+      q.tile_begin = tiles;
+      tiles += ((q.M + TM - 1) / TM) * q.tiles_n;
       tp.push_back(q);
-      tiles += per;
+    };
+    size_t gi = 0;
+    if (s.name == "dd two-external") {
+      std::vector<double> psign((size_t)std::max<i64>(plan.nD, 1), 1.0);
+      for (const auto& h : plan.dheads)
+        for (i64 k = 0; k < h.nD; ++k) psign[(size_t)(h.dk0 + k)] = k < h.nsing ? 1.0 : -1.0;
+      for (const auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        const DGemmProblem& dp = pr[gi++];
+        if (g.M != n || g.N != n || g.ldc != n) return;
+        TmaProblem q{dp.C, n, n, n, 0, 0, g.beta, (long long)ts.size(), 0, 0};
+        bool has_f = false;
+        for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
+          const GemmSeg& x = s.gs[(size_t)k];
+          if (x.a == BUF_F || x.b == BUF_F) {
+            has_f = true;
+            continue;
+          }
+          if (x.a != BUF_JK || x.b != BUF_D || x.K != n || x.lda != n || x.ldb != n || x.tA || x.tB || x.offA % n ||
+              x.offB % n2)
+            return;
+          ts.push_back(TmaSeg{x.offA / n, x.offB / n, 0, n, x.alpha * psign[(size_t)(x.offB / n2)]});
+        }
+        q.seg_end = (long long)ts.size();
+        if (has_f) q.beta = 1.0;  // the FP64 part of the step runs first
+        if (q.seg_end == q.seg_begin && has_f) continue;
+        push(q);
+      }
+      d.tma_kind = 1;
+    } else if (s.name == "three-external forward") {
+      for (const auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        const DGemmProblem& dp = pr[gi++];
+        if (g.N != n || g.ldc != n || g.seg_end - g.seg_begin != 1) return;
+        const GemmSeg& x = s.gs[(size_t)g.seg_begin];
+        if (x.a != BUF_D || x.b != BUF_V || x.tA || !x.tB || x.lda != n2 || x.ldb != n2 || x.offA % 32 ||
+            x.offB % n2 != x.offA || !((x.offA + x.K) % 32 == 0 || x.offA + x.K == n2) || g.M > plan.nD)
+          return;
+        // C^T (n x nD) = V_i rows (n x K) . pair rows (nD x K)^T
+        TmaProblem q{dp.C, n, n, g.M, 0, 0, g.beta, (long long)ts.size(), 0, 1};
+        ts.push_back(TmaSeg{(x.offB - x.offA) / n2 * n, 0, x.offA, x.K, x.alpha});
+        q.seg_end = (long long)ts.size();
+        push(q);
+      }
+      d.tma_kind = 2;
+    } else {
+      return;
     }
-    if (tp.empty()) return;
+    if (tp.empty()) {
+      d.tma_kind = 0;
+      return;
+    }
     d.tma_probs = upload(tp, owned, stream);
     d.tma_segs = upload(ts, owned, stream);
     d.tma_nprob = (int)tp.size();
@@ -838,8 +870,12 @@ struct tci_ctx {
         // Mixed form.  Segments whose operand is a same-head one-electron-like operator (BUF_F: h, J_ii,
         // K_ii combinations, orbital-energy magnitudes) stay on the FP64 kernel; the cross-head integral
         // segments go to the tensor cores (3xTF32), added after the FP64 part (beta 1 where both exist).
+        // Problems of at most SKINNY_M rows stay whole on the skinny FP64 kernel (launched in this form too).
         std::vector<tci_dev::HostGemm> f64, tcp;
         for (const auto& g : pr) {
+          bool skinny = g.M <= SKINNY_M;
+          for (long long q = g.seg_begin; skinny && q < g.seg_end; ++q) skinny = sg[(size_t)q].tA == 0 && sg[(size_t)q].tB == 1;
+          if (skinny) continue;
           tci_dev::HostGemm hf{g.C, g.ldc, g.M, g.N, g.beta, {}}, ht{g.C, g.ldc, g.M, g.N, g.beta, {}};
           for (long long q = g.seg_begin; q < g.seg_end; ++q) {
             const bool f = s.gs[(size_t)q].a == BUF_F || s.gs[(size_t)q].b == BUF_F;
@@ -873,7 +909,7 @@ struct tci_ctx {
         d.segs_tc = upload(st, owned, stream);
         d.nprob_tc = (int)pt.size();
         d.tc_ok = flops >= 5e7 && useful >= 0.25 * issued;
-        if (s.name == "dd two-external") lower_tma(s, d, pr);
+        lower_tma(s, d, pr);
       }
     } else if (s.kind == STEP_AXPY) {
       std::vector<DAxpyTarget> t;
@@ -976,6 +1012,7 @@ struct tci_ctx {
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     sigma_count++;
   }
+  bool tma_ok(const DevStep& s) const { return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready); }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
     return precision == 1 && s.probs_tc && (tc_mode == 1 || (tc_mode == 0 && s.tc_ok));
@@ -990,7 +1027,8 @@ struct tci_ctx {
         continue;
       }
       if (s.kind == STEP_GEMM && uses_tc(s)) {
-        k += (s.ntiles_f > 0 ? 1 : 0) + ((s.tma_probs && tma_ready) ? 2 : (s.ntiles_tc > 0 ? 1 : 0));
+        k += (s.skinny_nwarps > 0 ? 1 : 0) + (s.ntiles_f > 0 ? 1 : 0) +
+             ((s.tma_probs && tma_ok(s)) ? 2 : (s.ntiles_tc > 0 ? 1 : 0));
         continue;
       }
       if (s.kind == STEP_GEMM && s.skinny_nwarps > 0) k += 1;
@@ -1089,26 +1127,38 @@ struct tci_ctx {
     TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
-    bool any_tma = false;
-    for (const auto& st : sigma) any_tma = any_tma || st.tma_probs;
-    if (any_tma && plan.nD > 0) {
-      const i64 n = plan.n, ld = tci_gtma_host::pitch(n);
-      const i64 xrows = plan.buf_size[BUF_JK] / n, drows = plan.nD * n;
+    bool want_dd = false, want_t3 = false;
+    for (const auto& st : sigma) {
+      want_dd = want_dd || (st.tma_probs && st.tma_kind == 1);
+      want_t3 = want_t3 || (st.tma_probs && st.tma_kind == 2);
+    }
+    const i64 n = plan.n, n2 = n * n;
+    std::string err;
+    if (want_dd && plan.nD > 0) {
+      const i64 ld = tci_gtma_host::pitch(n), xrows = plan.buf_size[BUF_JK] / n, drows = plan.nD * n;
       alloc_f(&jk_hi, (size_t)(xrows * ld));
       alloc_f(&jk_lo, (size_t)(xrows * ld));
       alloc_f(&d_hi, (size_t)(drows * ld));
       alloc_f(&d_lo, (size_t)(drows * ld));
-      TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, jk_hi, jk_lo, stream));
-      std::string err;
-      if (!tci_gtma_host::prepare(tma_maps, jk_hi, jk_lo, xrows, d_hi, d_lo, drows, n, err))
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, n, jk_hi, jk_lo, stream));
+      if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows, n, d_hi, d_lo, drows, n, err)) throw Error(TCI_ERR_CUDA, err);
+      tma_dd_ready = true;
+    }
+    if (want_t3 && plan.nD > 0) {
+      const i64 ld = tci_gtma_host::pitch(n2), vrows = plan.nint * n;
+      alloc_f(&v_hi, (size_t)(vrows * ld));
+      alloc_f(&v_lo, (size_t)(vrows * ld));
+      alloc_f(&df_hi, (size_t)(plan.nD * ld));
+      alloc_f(&df_lo, (size_t)(plan.nD * ld));
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_V], vrows, n2, n2, v_hi, v_lo, stream));
+      if (!tci_gtma_host::prepare(tma_t3, v_hi, v_lo, vrows, n2, df_hi, df_lo, plan.nD, n2, err))
         throw Error(TCI_ERR_CUDA, err);
-      tma_ready = true;
+      tma_t3_ready = true;
     }
     TCI_CUDA(cudaMemsetAsync(tc_status, 0, sizeof(int), stream));
     TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
     if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
     TCI_CUDA(cudaStreamSynchronize(stream));
-    std::string err;
     if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, uhi, ulo, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     if (plan.n_trip > 0 && nm > 0 &&
@@ -1172,10 +1222,21 @@ struct tci_ctx {
           run_allext_tc();
           break;
         }
-        if (uses_tc(s) && s.tma_probs && tma_ready) {
-          TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
-          TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * plan.n, plan.n, d_hi, d_lo, stream));
-          TCI_CUDA(tci_gtma_host::launch(tma_maps, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, tc_status, stream));
+        if (uses_tc(s) && s.skinny_nwarps > 0)
+          gemm_skinny_f64<<<(unsigned)((s.skinny_nwarps + 7) / 8), 256, 0, stream>>>(s.skinny_probs, s.skinny_nprob,
+                                                                                  s.segs, s.skinny_nwarps);
+        if (uses_tc(s) && s.tma_probs && tma_ok(s)) {
+          const i64 n = plan.n;
+          if (s.tma_kind == 1) {
+            TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
+            TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * n, n, n, d_hi, d_lo, stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_dd, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          } else {
+            TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_t3, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          }
           break;
         }
         if (uses_tc(s)) {
@@ -1300,7 +1361,8 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                                         : 0.0) +
                               // split integrals and pair matrices of the TMA-fed two-external step
                               2.0 * (double)tci_gtma_host::pitch(P.n) *
-                                  (double)(P.buf_size[BUF_JK] / std::max<i64>(1, P.n) + P.nD * P.n));
+                                  (double)(P.buf_size[BUF_JK] / std::max<i64>(1, P.n) + P.nD * P.n) +
+                              2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * (double)(P.nint * P.n + P.nD));
     pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
     res += f32 - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
