@@ -13,7 +13,8 @@
 // computed transposed).  A segment's k steps form FP32 accumulation blocks of
 // at most kblock elements in a double-buffered TMEM accumulator; the epilogue
 // adds alpha_s times each block into FP64 registers, so the coefficients never
-// touch the operands, and writes C (or C^T) once.
+// touch the operands, and writes C (or C^T) once, or, for a product that feeds
+// the next one, its TF32 high / FP32 low parts.
 //
 // Warp roles (192 threads): 0-3 epilogue, 4 TMA producer, 5 TMEM allocator +
 // MMA issuer.  Bounded waits; on an abort the kernel waits (bounded) for its
@@ -204,7 +205,19 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
     if (!aborted() && r < P.M) {
-      if (!P.trans_c) {
+      if (P.c_hi) {  // split output: the next product's operand, in the layout split_rows writes
+        float* hrow = P.c_hi + r * P.ldcs;
+        float* lrow = P.c_lo + r * P.ldcs;
+#pragma unroll
+        for (int j = 0; j < BN; ++j) {
+          const long long c = n0 + j;
+          if (c < P.N) {
+            const float h = __uint_as_float(__float_as_uint((float)acc[j]) & 0xFFFFE000u);
+            hrow[c] = h;
+            lrow[c] = (float)(acc[j] - (double)h);
+          }
+        }
+      } else if (!P.trans_c) {
         double* crow = P.C + r * P.ldc;
 #pragma unroll
         for (int j = 0; j < BN; ++j) {

@@ -13,6 +13,9 @@ struct TmaProblem {
   double beta;
   long long seg_begin, seg_end;
   long long trans_c;  // the tile computes C^T: element (r, c) is stored at C[c][r]
+  float* c_hi;        // non-null: C is written instead as TF32 high / FP32 low parts (row pitch ldcs, beta 0)
+  float* c_lo;
+  long long ldcs;
 };
 struct TmaSeg {
   long long a_row, b_row;  // first rows of the segment in the A and B arrays

@@ -19,7 +19,10 @@
 //   T_hk (Jc n_h x n_h) = [L^J_h]_J (Jc n_h x n_h) D_hk
 //   R_hk (n_h x n_h)   += 1/2 sum_J T_hkJ L^J_h       (Jc K-segments of n_h)
 //
-// on the FP64 SIMT kernel or, in the mixed form, on the tcgen05 3xTF32 kernel.
+// on the FP64 SIMT kernel or, in the mixed form, on the TMA-fed tcgen05 3xTF32
+// kernel: there L^J_h, D_hk and T_hk live as TF32-high / FP32-low rows (pitch a
+// multiple of 32, zero past each domain), the first GEMM writes T_hk directly
+// in that split form and the second accumulates R_hk in FP64.
 // The chunk size and the FP64 tile shape of the second GEMM come from a small
 // autotuner that times each candidate once at set-up.  One application
 // (unpack, chunks, pack) is captured as one CUDA graph.
@@ -35,7 +38,7 @@
 
 #include "../../include/tigerci_sigma.h"
 #include "gemm_tables.h"
-#include "gemm_tc.h"
+#include "gemm_tma.h"
 #include "host/capi_internal.h"
 
 using namespace tci;
@@ -62,10 +65,12 @@ struct DLocBlock {
   long long d_off;           // offset of D_hk / R_hk (n x n)
   long long head;            // index of the head
   long long t_off;           // offset of T_hk (jmax n x n) in the chunk buffer
+  long long drow, trow;      // mixed form: first row of D_hk / T_hk in the split arrays
 };
 // one head for the gather
 struct DLocHead {
   long long dom_off, n, lc_off;  // domain slice, offset of L^J_h (jmax x n x n) in the chunk buffer
+  long long lrow;                // mixed form: first row of L^J_h (jmax n rows) in the split array
 };
 
 __device__ __forceinline__ long long vpair(long long a, long long b) {
@@ -137,6 +142,47 @@ __global__ void pack_local(const DLocBlock* __restrict__ blk, const double* __re
       sigma[B.off_aa + B.k * n + a] += 1.4142135623730951 * Rk[a * n + a];
 }
 
+// TF32 high part (low 13 mantissa bits cleared) and FP32 remainder, as the TMA-fed kernel reads them
+__device__ __forceinline__ void split_put(float* hi, float* lo, long long i, double x) {
+  const float h = __uint_as_float(__float_as_uint((float)x) & 0xFFFFE000u);
+  hi[i] = h;
+  lo[i] = (float)(x - (double)h);
+}
+
+// Mixed form: the gathered L^J_h as split rows of pitch ldp (row lrow + j n + a, column c)
+__global__ void gather_lc_split(const double* __restrict__ LT, long long npv, long long J0,
+                                const DLocHead* __restrict__ heads, const long long* __restrict__ dom,
+                                float* __restrict__ hi, float* __restrict__ lo, long long ldp) {
+  const DLocHead H = heads[blockIdx.x];
+  const long long j = blockIdx.y;
+  const double* row = LT + (J0 + j) * npv;
+  const long long* d = dom + H.dom_off;
+  const long long r0 = H.lrow + j * H.n;
+  for (long long e = threadIdx.x; e < H.n * H.n; e += blockDim.x) {
+    const long long a = e / H.n, c = e % H.n;
+    split_put(hi, lo, (r0 + a) * ldp + c, row[vpair(d[a], d[c])]);
+  }
+}
+
+// Mixed form: D_hk as split rows of pitch ldp (same matrix as unpack_local)
+__global__ void unpack_local_split(const DLocBlock* __restrict__ blk, const double* __restrict__ c,
+                                   float* __restrict__ hi, float* __restrict__ lo, long long ldp) {
+  const DLocBlock B = blk[blockIdx.x];
+  const long long n = B.n, nab = n * (n - 1) / 2;
+  for (long long e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const long long r = e / n, s = e % n;
+    double v = 0.0;
+    if (r == s) {
+      if (B.aa) v = 1.4142135623730951 * c[B.off_aa + B.k * n + r];
+    } else if (B.ab) {
+      const long long i = r > s ? r : s, j = r > s ? s : r;
+      const double x = c[B.off_ab + B.k * nab + i * (i - 1) / 2 + j];
+      v = (r < s) ? x : B.p * x;
+    }
+    split_put(hi, lo, (B.drow + r) * ldp + s, v);
+  }
+}
+
 __global__ void add_into(double* __restrict__ dst, const double* __restrict__ src, long long n) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] += src[i];
@@ -148,7 +194,12 @@ struct GemmLaunch {
   int nprob = 0;
   long long ntiles = 0;
   int cfg = 0;  // FP64 tile shape
-  bool tc = false;
+};
+struct TmaLaunch {
+  TmaProblem* probs = nullptr;
+  TmaSeg* segs = nullptr;
+  int nprob = 0;
+  long long ntiles = 0;
 };
 
 }  // namespace
@@ -173,6 +224,11 @@ struct tci_local {
   std::vector<DLocHead> heads;
   int* status = nullptr;
   GemmLaunch g1, g2, g1r, g2r;  // full chunks and the shorter last chunk
+  // mixed form: split arrays (row pitch ldp) and the TMA-fed tables
+  long long ldp = 0, rows_l = 0, rows_d = 0, rows_t = 0;
+  float *lc_hi = nullptr, *lc_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr, *t_hi = nullptr, *t_lo = nullptr;
+  tci_gtma_host::TmaMaps map1, map2;  // T = Lc D ; R += 1/2 T Lc
+  TmaLaunch m1, m2, m1r, m2r;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -217,7 +273,7 @@ struct tci_local {
     return p;
   }
 
-  // GEMM tables for chunks of j vectors (the chunk buffers are laid out for jmax)
+  // FP64 form: GEMM tables for chunks of j vectors (the chunk buffers are laid out for jmax)
   void make_gemms(int64_t j, int cfg_second, GemmLaunch& a, GemmLaunch& b) {
     std::vector<HostGemm> v1, v2;
     for (const auto& B : blocks) {
@@ -233,11 +289,8 @@ struct tci_local {
     auto finish = [&](std::vector<HostGemm>& v, int cfg, GemmLaunch& g) {
       std::vector<DGemmProblem> pr;
       std::vector<DGemmSeg> sg;
-      g.tc = precision == 1;
       g.cfg = cfg;
-      if (g.tc) g.ntiles = tci_dev::tile_problems(v, tci_gtc_host::tile_m(), tci_gtc_host::tile_n(), true, pr, sg);
-      else
-        g.ntiles = tci_dev::tile_problems(v, tci_dev::gemm_f64_tile_m(cfg), tci_dev::gemm_f64_tile_n(cfg), false, pr, sg);
+      g.ntiles = tci_dev::tile_problems(v, tci_dev::gemm_f64_tile_m(cfg), tci_dev::gemm_f64_tile_n(cfg), false, pr, sg);
       g.probs = upload(pr);
       g.segs = upload(sg);
       g.nprob = (int)pr.size();
@@ -246,15 +299,66 @@ struct tci_local {
     finish(v2, cfg_second, b);
   }
 
+  // mixed form: TMA-fed tables for chunks of j vectors
+  void make_tma(int64_t j, TmaLaunch& a, TmaLaunch& b) {
+    const long long TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n();
+    std::vector<TmaProblem> p1, p2;
+    std::vector<TmaSeg> s1, s2;
+    long long t1 = 0, t2 = 0;
+    for (const auto& B : blocks) {
+      const DLocHead& H = heads[B.head];
+      const long long n = B.n, tn = (n + TN - 1) / TN;
+      // T_hk (j n x n) = Lc_h D_hk, written split; D_hk enters as the K-major operand through D^T = p D
+      TmaProblem q1{nullptr, 0, j * n, n, tn, t1, 0.0, (long long)s1.size(), 0, 0,
+                    t_hi + B.trow * ldp, t_lo + B.trow * ldp, ldp};
+      s1.push_back(TmaSeg{H.lrow, B.drow, 0, n, B.p});
+      q1.seg_end = (long long)s1.size();
+      t1 += ((j * n + TM - 1) / TM) * tn;
+      p1.push_back(q1);
+      // R_hk += 1/2 sum_J T_hkJ L^J_h (L^J_h symmetric: its rows are the K-major operand)
+      TmaProblem q2{R + B.d_off, n, n, n, tn, t2, 1.0, (long long)s2.size(), 0, 0, nullptr, nullptr, 0};
+      for (int64_t q = 0; q < j; ++q) s2.push_back(TmaSeg{B.trow + q * n, H.lrow + q * n, 0, n, 0.5});
+      q2.seg_end = (long long)s2.size();
+      t2 += ((n + TM - 1) / TM) * tn;
+      p2.push_back(q2);
+    }
+    a.probs = upload(p1);
+    a.segs = upload(s1);
+    a.nprob = (int)p1.size();
+    a.ntiles = t1;
+    b.probs = upload(p2);
+    b.segs = upload(s2);
+    b.nprob = (int)p2.size();
+    b.ntiles = t2;
+  }
+
   void launch_gemm(const GemmLaunch& g) {
     if (g.ntiles <= 0) return;
-    if (g.tc) LCUDA(tci_gtc_host::launch(g.probs, g.nprob, g.segs, g.ntiles, status, (int)kblock, stream));
-    else LCUDA(tci_dev::launch_gemm_f64(g.cfg, g.probs, g.nprob, g.segs, g.ntiles, stream));
+    LCUDA(tci_dev::launch_gemm_f64(g.cfg, g.probs, g.nprob, g.segs, g.ntiles, stream));
   }
 
   // One application on the internal buffers: Sb = A Cb.
   void record_apply() {
     const unsigned nb = (unsigned)blocks.size();
+    if (precision == 1) {
+      unpack_local_split<<<nb, 256, 0, stream>>>(dblocks, Cb, d_hi, d_lo, ldp);
+      LCUDA(cudaGetLastError());
+      LCUDA(cudaMemsetAsync(R, 0, sizeof(double) * (size_t)rlen, stream));
+      LCUDA(cudaMemsetAsync(Sb, 0, sizeof(double) * (size_t)total, stream));
+      for (int64_t J0 = 0; J0 < nchol; J0 += jc) {
+        const int64_t jn = std::min<int64_t>(jc, nchol - J0);
+        gather_lc_split<<<dim3((unsigned)heads.size(), (unsigned)jn), 256, 0, stream>>>(LT, npv, J0, dheads, ddom,
+                                                                                       lc_hi, lc_lo, ldp);
+        LCUDA(cudaGetLastError());
+        const TmaLaunch& a = jn == jc ? m1 : m1r;
+        const TmaLaunch& b = jn == jc ? m2 : m2r;
+        LCUDA(tci_gtma_host::launch(map1, a.probs, a.nprob, a.segs, a.ntiles, (int)kblock, status, stream));
+        LCUDA(tci_gtma_host::launch(map2, b.probs, b.nprob, b.segs, b.ntiles, (int)kblock, status, stream));
+      }
+      pack_local<<<nb, 256, 0, stream>>>(dblocks, R, Sb);
+      LCUDA(cudaGetLastError());
+      return;
+    }
     unpack_local<<<nb, 256, 0, stream>>>(dblocks, Cb, D);
     LCUDA(cudaGetLastError());
     LCUDA(cudaMemsetAsync(R, 0, sizeof(double) * (size_t)rlen, stream));
@@ -275,9 +379,14 @@ struct tci_local {
     release_graph();
     jc = j;
     cfg2 = cfg;
-    make_gemms(jc, cfg2, g1, g2);
     const int64_t rem = nchol % jc;
-    if (rem) make_gemms(rem, cfg2, g1r, g2r);
+    if (precision == 1) {
+      make_tma(jc, m1, m2);
+      if (rem) make_tma(rem, m1r, m2r);
+    } else {
+      make_gemms(jc, cfg2, g1, g2);
+      if (rem) make_gemms(rem, cfg2, g1r, g2r);
+    }
     LCUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
       record_apply();
@@ -326,7 +435,7 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
     const bool tune = !(options && n_options > 3 && options[3] == 0);
     if (L->precision < 0 || L->precision > 1 || L->kblock % 32) throw Error(TCI_ERR_ARG, "bad precision or promotion block");
     // heads and blocks (host checks: every index below is bounds-checked here, not on the device)
-    long long dtot = 0, lc_per_j = 0, t_per_j = 0, dom_total = 0;
+    long long dtot = 0, lc_per_j = 0, t_per_j = 0, dom_total = 0, lrows = 0, drows = 0, nmax = 0;
     for (int64_t h = 0; h < n_heads; ++h) {
       const int64_t* H = heads + 7 * h;
       const int64_t off_ab = H[0], off_aa = H[1], nsf_ab = H[2], nsf_aa = H[3], nsing = H[4], doff = H[5], n = H[6];
@@ -339,16 +448,19 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
         throw Error(TCI_ERR_INPUT, "head block outside the CI vector");
       const long long nk = std::max(nsf_ab, nsf_aa);
       if (nk == 0) continue;
-      L->heads.push_back(DLocHead{doff, n, lc_per_j});  // offsets per Cholesky vector, scaled by jmax below
+      L->heads.push_back(DLocHead{doff, n, lc_per_j, lrows});  // offsets per Cholesky vector, scaled by jmax below
       const long long hi = (long long)L->heads.size() - 1;
       for (long long k = 0; k < nk; ++k) {
         L->blocks.push_back(DLocBlock{off_ab, off_aa, n, k, k < nsf_ab ? 1 : 0, k < nsf_aa ? 1 : 0,
-                                      k < nsing ? 1.0 : -1.0, dtot, hi, t_per_j});
+                                      k < nsing ? 1.0 : -1.0, dtot, hi, t_per_j, drows, drows});
         dtot += n * n;
+        drows += n;
         t_per_j += n * n;
         L->flops += 4.0 * (double)nchol * (double)n * (double)n * (double)n;
       }
       lc_per_j += n * n;
+      lrows += n;
+      nmax = std::max<long long>(nmax, n);
       L->lbytes += 8.0 * (double)nchol * (double)n * (double)n;
     }
     if (L->heads.empty()) throw Error(TCI_ERR_INPUT, "no head has a CI block");
@@ -360,10 +472,22 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
           throw Error(TCI_ERR_INPUT, "domains must be sorted, distinct external indices");
       }
     // chunk size: the gathered L^J_h and the T_hk of one chunk fit the budget
-    const double per_j = 8.0 * (double)(lc_per_j + t_per_j);
+    // (mixed form: TF32-high / FP32-low rows of pitch ldp instead of FP64 squares)
+    L->ldp = tci_gtma_host::pitch(nmax);
+    const double per_j = L->precision == 1 ? 8.0 * (double)L->ldp * (double)(lrows + drows)
+                                           : 8.0 * (double)(lc_per_j + t_per_j);
     L->jmax = std::max<int64_t>(1, std::min<int64_t>(nchol, (int64_t)(budget / per_j)));
-    for (auto& H : L->heads) H.lc_off *= L->jmax;
-    for (auto& B : L->blocks) B.t_off *= L->jmax;
+    for (auto& H : L->heads) {
+      H.lc_off *= L->jmax;
+      H.lrow *= L->jmax;
+    }
+    for (auto& B : L->blocks) {
+      B.t_off *= L->jmax;
+      B.trow *= L->jmax;
+    }
+    L->rows_l = lrows * L->jmax;
+    L->rows_d = drows;
+    L->rows_t = drows * L->jmax;
     L->rlen = dtot;
 
     int ndev = 0;
@@ -395,9 +519,27 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
       L->owned.erase(std::find(L->owned.begin(), L->owned.end(), (void*)tmp));
       L->dev_bytes -= (double)lvv.size() * sizeof(double);
     }
-    L->Lc = L->alloc((size_t)(lc_per_j * L->jmax));
-    L->T = L->alloc((size_t)(t_per_j * L->jmax));
-    L->D = L->alloc((size_t)dtot);
+    if (L->precision == 1) {
+      // split arrays, zeroed once: the columns past each domain's n stay zero (the padding of the K tiles)
+      auto falloc = [&](float** p, long long rows) {
+        *p = reinterpret_cast<float*>(L->alloc((size_t)(rows * L->ldp + 1) / 2));
+        LCUDA(cudaMemsetAsync(*p, 0, sizeof(float) * (size_t)(rows * L->ldp), L->stream));
+      };
+      falloc(&L->lc_hi, L->rows_l);
+      falloc(&L->lc_lo, L->rows_l);
+      falloc(&L->d_hi, L->rows_d);
+      falloc(&L->d_lo, L->rows_d);
+      falloc(&L->t_hi, L->rows_t);
+      falloc(&L->t_lo, L->rows_t);
+      std::string err;
+      if (!tci_gtma_host::prepare(L->map1, L->lc_hi, L->lc_lo, L->rows_l, nmax, L->d_hi, L->d_lo, L->rows_d, nmax, err) ||
+          !tci_gtma_host::prepare(L->map2, L->t_hi, L->t_lo, L->rows_t, nmax, L->lc_hi, L->lc_lo, L->rows_l, nmax, err))
+        throw Error(TCI_ERR_CUDA, err);
+    } else {
+      L->Lc = L->alloc((size_t)(lc_per_j * L->jmax));
+      L->T = L->alloc((size_t)(t_per_j * L->jmax));
+      L->D = L->alloc((size_t)dtot);
+    }
     L->R = L->alloc((size_t)dtot);
     L->Cb = L->alloc((size_t)total_len);
     L->Sb = L->alloc((size_t)total_len);
@@ -408,7 +550,6 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
     LCUDA(cudaMalloc(&L->status, sizeof(int)));
     L->owned.push_back(L->status);
     LCUDA(cudaMemsetAsync(L->status, 0, sizeof(int), L->stream));
-    if (L->precision == 1) LCUDA(tci_gtc_host::prepare());
 
     // autotuner: chunk size (largest, half) x FP64 tile shape of the second GEMM; one timed run each
     std::vector<std::pair<int64_t, int>> cand;

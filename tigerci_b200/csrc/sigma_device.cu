@@ -754,7 +754,7 @@ struct tci_ctx {
         if (g.M <= 0 || g.N <= 0) continue;
         const DGemmProblem& dp = pr[gi++];
         if (g.M != n || g.N != n || g.ldc != n) return;
-        TmaProblem q{dp.C, n, n, n, 0, 0, g.beta, (long long)ts.size(), 0, 0};
+        TmaProblem q{dp.C, n, n, n, 0, 0, g.beta, (long long)ts.size(), 0, 0, nullptr, nullptr, 0};
         bool has_f = false;
         for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
           const GemmSeg& x = s.gs[(size_t)k];
@@ -783,8 +783,8 @@ struct tci_ctx {
             x.offB % n2 != x.offA || !((x.offA + x.K) % 32 == 0 || x.offA + x.K == n2) || g.M > plan.nD)
           return;
         // C^T (n x nD) = V_i rows (n x K) . pair rows (nD x K)^T
-        TmaProblem q{dp.C, n, n, g.M, 0, 0, g.beta, (long long)ts.size(), 0, 1};
-        ts.push_back(TmaSeg{(x.offB - x.offA) / n2 * n, 0, x.offA, x.K, x.alpha});
+        TmaProblem q{dp.C, n, n, g.M, 0, 0, g.beta, (long long)ts.size(), 0, 1, nullptr, nullptr, 0};
+        ts.push_back(TmaSeg{(x.offB - x.offA) / n2, 0, x.offA, x.K, x.alpha});  // first row of V_i: i n
         q.seg_end = (long long)ts.size();
         push(q);
       }
