@@ -8,10 +8,20 @@
 // Three kind::tf32 MMAs per k-step (hi*hi + hi*lo + lo*hi) accumulate FP32 in
 // TMEM; every KBLOCK elements of k the partial sums are read back with
 // tcgen05.ld and added into FP64 accumulators held in registers (promotion
-// keeps the FP32 accumulation error at the block length), which are written
-// to the output once at the end.  The product is HBM bound: W is read exactly
-// once.  One launch covers both operators (W+ with the singlet blocks, W-
-// with the triplet blocks), so their tiles share the waves.
+// keeps the FP32 accumulation error at the block length).  The product is HBM
+// bound: W is read exactly once.
+//
+// Work split (persistent, stream-K): one launch covers both operators (W+
+// with the singlet blocks, W- with the triplet blocks).  Their k-steps form
+// one linear sequence (operator, CI-block group, 128-row panel, k); each CTA
+// (one per SM) takes an equal contiguous range of it, so the pipeline runs
+// without refills from panel to panel and every SM streams the same number of
+// W bytes.  A range is at least one panel long, so a panel is shared by at
+// most two CTAs: both add their FP64 partial sums into the zeroed output, and
+// a + b rounds the same in either order, so the result does not depend on
+// which CTA finishes first.  The MMA's N is the operator's own CI-block count
+// rounded up to 16 (at most 64), not a fixed 64, and the TMA producer keeps
+// the W tiles a few stages beyond its ring already on their way into L2.
 //
 // Warp roles (320 threads): warps 0-3 epilogue (TMEM lane quadrants 0-3),
 // warps 4-7 hi/lo split, warp 8 TMA producer, warp 9 TMEM allocator + MMA
@@ -26,53 +36,24 @@
 #include <string>
 
 #include "allext_tc.h"
+#include "tc_common.cuh"
 
 namespace tci_tc {
 
-constexpr int BM = 128;      // W rows per CTA tile (MMA M)
-constexpr int BN = 64;       // CI blocks per tile (MMA N)
+using namespace tci_tcx;
+
+constexpr int BM = 128;      // W rows per panel (MMA M)
+constexpr int BN = 64;       // largest CI-block group (MMA N)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
 constexpr int STAGES = 4;
+constexpr int PREFETCH = 8;  // W tiles requested into L2 ahead of the ring
 // The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
 // a launch parameter: the tensor core's FP32 accumulation error grows with it.
 constexpr int W_BYTES = BM * BK * 4;   // 16 KB
-constexpr int U_BYTES = BN * BK * 4;   // 8 KB
+constexpr int U_BYTES = BN * BK * 4;   // 8 KB (room for the largest group)
 constexpr int STAGE_BYTES = 2 * W_BYTES + 2 * U_BYTES;
 constexpr int NTHREADS = 320;
-constexpr long long SPIN_LIMIT = 1ll << 22;  // bounded mbarrier waits (~seconds)
-
-struct Smem {
-  // stage buffers start at a 1024-byte aligned base (128B swizzle atoms)
-  uint8_t* base;
-};
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// Bounded wait for the phase with the given parity; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long i = 0; i < SPIN_LIMIT; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
   asm volatile(
@@ -81,62 +62,55 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
-
-// tcgen05 shared-memory matrix descriptor: K-major, 128-byte swizzle,
-// 8-row core matrices 1024 bytes apart (SBO), version 1.
-__device__ __forceinline__ uint64_t smem_desc(const void* p) {
-  const uint64_t addr = smem_u32(p);
-  uint64_t d = 0;
-  d |= (addr & 0x3FFFFull) >> 4;           // start address
-  d |= (uint64_t)(16 >> 4) << 16;          // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
-  d |= (uint64_t)1 << 46;                  // descriptor version
-  d |= (uint64_t)2 << 61;                  // 128-byte swizzle
-  return d;
-}
-
-// Instruction descriptor: D f32, A/B tf32, both K-major, M = 128, N = 64.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
-}
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+// Hint: bring a tile into L2 (no shared memory, no completion to wait for).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y)
                : "memory");
 }
 
 // Error codes written to the kernel's status word.
 enum : int { ST_OK = 0, ST_TIMEOUT_FULL = 1, ST_TIMEOUT_CONV = 2, ST_TIMEOUT_EMPTY = 3, ST_TIMEOUT_D = 4, ST_TIMEOUT_DE = 5 };
 
-// One product of the launch: Y (m x np, row pitch ldy) = U W over `tiles`
-// panels of BM W rows.
+// One operator of the launch: Y (m x np, row pitch ldy) = U W, as groups of
+// bn CI blocks x panels of BM W rows x nk k-steps.
 struct Product {
-  int np, m, tiles;
+  int np, m, bn, groups, panels, nk;
+  long long units;  // groups * panels * nk
   double* Y;
   long long ldy;
 };
+
+// A run of consecutive k-steps of one (operator, group, panel) inside a CTA's range.
+struct Segment {
+  int prod, group, panel, k0, k1;
+};
+
+// The segment starting at linear k-step position pos (pos < end).
+__device__ __forceinline__ Segment segment_at(const Product& p0, const Product& p1, long long pos, long long end) {
+  Segment g;
+  g.prod = pos >= p0.units ? 1 : 0;
+  const Product& P = g.prod ? p1 : p0;
+  const long long u = g.prod ? pos - p0.units : pos;
+  const long long per_group = (long long)P.panels * P.nk;
+  g.group = (int)(u / per_group);
+  const long long v = u - (long long)g.group * per_group;
+  g.panel = (int)(v / P.nk);
+  g.k0 = (int)(v - (long long)g.panel * P.nk);
+  const long long left = end - pos;
+  g.k1 = (long long)(P.nk - g.k0) < left ? P.nk : (int)(g.k0 + left);
+  return g;
+}
 
 __global__ void __launch_bounds__(NTHREADS, 1)
     allext_tf32x3_kernel(const __grid_constant__ CUtensorMap wmap0, const __grid_constant__ CUtensorMap uhi_map0,
                          const __grid_constant__ CUtensorMap ulo_map0, const __grid_constant__ CUtensorMap wmap1,
                          const __grid_constant__ CUtensorMap uhi_map1, const __grid_constant__ CUtensorMap ulo_map1,
-                         Product p0, Product p1, int* __restrict__ status, int kb_per_block, int ksplit) {
+                         Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
   const int KB_PER_BLOCK = kb_per_block;
-  // CTA -> (tile, k split); which product the tile belongs to (uniform over the CTA: the early exit
-  // precedes all set-up)
-  const int tile = (int)blockIdx.x / ksplit, split = (int)blockIdx.x % ksplit;
-  const bool second = tile >= p0.tiles;
-  const Product P = second ? p1 : p0;
-  const CUtensorMap* wmap = second ? &wmap1 : &wmap0;
-  const CUtensorMap* uhi_map = second ? &uhi_map1 : &uhi_map0;
-  const CUtensorMap* ulo_map = second ? &ulo_map1 : &ulo_map0;
-  const int np = P.np, m = P.m;
-  const int ublock = blockIdx.y;       // which group of BN CI blocks
-  if (ublock * BN >= m) return;
+  const long long total = p0.units + p1.units;
+  const long long begin = total * (long long)blockIdx.x / gridDim.x;
+  const long long end = total * (long long)(blockIdx.x + 1) / gridDim.x;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
@@ -149,12 +123,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row0 = (second ? tile - p0.tiles : tile) * BM;
-  // k steps of this split: [kbase, kbase + nk)
-  const int nk_all = (np + BK - 1) / BK, per = (nk_all + ksplit - 1) / ksplit;
-  const int kbase = split * per;
-  const int nk = nk_all - kbase < per ? (nk_all - kbase > 0 ? nk_all - kbase : 0) : per;
-  const int nblocks = (nk + KB_PER_BLOCK - 1) / KB_PER_BLOCK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -189,33 +157,45 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 8) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
-      int last = -1;  // last k-step whose copies were issued
-      for (int kb = 0; kb < nk && !aborted(); ++kb) {
-        const int s = kb % STAGES;
-        if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1)) {
-          fail(ST_TIMEOUT_EMPTY);
-          break;
+      int step = 0, last = -1;  // k-steps issued so far in this CTA; the last one
+      for (long long pos = begin; pos < end && !aborted();) {
+        const Segment g = segment_at(p0, p1, pos, end);
+        const CUtensorMap* wmap = g.prod ? &wmap1 : &wmap0;
+        const CUtensorMap* uhi_map = g.prod ? &uhi_map1 : &uhi_map0;
+        const CUtensorMap* ulo_map = g.prod ? &ulo_map1 : &ulo_map0;
+        const int bn = g.prod ? p1.bn : p0.bn;
+        const uint32_t bytes = (uint32_t)(W_BYTES + 2 * bn * BK * 4);
+        for (int k = g.k0; k < g.k0 + PREFETCH && k < g.k1; ++k) tma_prefetch_2d(wmap, k * BK, g.panel * BM);
+        for (int k = g.k0; k < g.k1 && !aborted(); ++k, ++step) {
+          const int s = step % STAGES;
+          if (step >= STAGES && !mbar_wait(&empty[s], ((step / STAGES) - 1) & 1)) {
+            fail(ST_TIMEOUT_EMPTY);
+            break;
+          }
+          if (k + PREFETCH < g.k1) tma_prefetch_2d(wmap, (k + PREFETCH) * BK, g.panel * BM);
+          uint8_t* st = base + s * STAGE_BYTES;
+          mbar_expect_tx(&full[s], bytes);
+          tma_load_2d(st, wmap, &full[s], k * BK, g.panel * BM);
+          tma_load_2d(st + 2 * W_BYTES, uhi_map, &full[s], k * BK, g.group * bn);
+          tma_load_2d(st + 2 * W_BYTES + U_BYTES, ulo_map, &full[s], k * BK, g.group * bn);
+          last = step;
         }
-        uint8_t* st = base + s * STAGE_BYTES;
-        mbar_expect_tx(&full[s], W_BYTES + 2 * U_BYTES);
-        tma_load_2d(st, wmap, &full[s], (kbase + kb) * BK, row0);
-        tma_load_2d(st + 2 * W_BYTES, uhi_map, &full[s], (kbase + kb) * BK, ublock * BN);
-        tma_load_2d(st + 2 * W_BYTES + U_BYTES, ulo_map, &full[s], (kbase + kb) * BK, ublock * BN);
-        last = kb;
+        pos += g.k1 - g.k0;
       }
       if (aborted()) {
         // the copies of the last STAGES issued k-steps may still be landing: wait (bounded) for them
         // before the shared memory is released
-        for (int kb = (last - STAGES + 1 > 0 ? last - STAGES + 1 : 0); kb <= last; ++kb)
-          mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
+        for (int st = (last - STAGES + 1 > 0 ? last - STAGES + 1 : 0); st <= last; ++st)
+          mbar_wait(&full[st % STAGES], (st / STAGES) & 1);
       }
     }
   } else if (warp >= 4 && warp < 8) {
     // ---------------- TF32 hi/lo split of the W tile (in place + lo copy) ----------------
     const int cw = warp - 4;
-    for (int kb = 0; kb < nk && !aborted(); ++kb) {
-      const int s = kb % STAGES;
-      if (!mbar_wait(&full[s], (kb / STAGES) & 1)) {
+    const long long nsteps = end - begin;
+    for (long long step = 0; step < nsteps && !aborted(); ++step) {
+      const int s = (int)(step % STAGES);
+      if (!mbar_wait(&full[s], (uint32_t)((step / STAGES) & 1))) {
         fail(ST_TIMEOUT_FULL);
         break;
       }
@@ -243,34 +223,44 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (lane == 0) mbar_arrive(&conv[s]);
     }
   } else if (warp == 9) {
-    // ---------------- MMA issuer ----------------
+    // ---------------- MMA issuer: promotion blocks of KB_PER_BLOCK steps, never across segments ----------------
     if (lane == 0) {
-      for (int kb = 0; kb < nk && !aborted(); ++kb) {
-        const int s = kb % STAGES;
-        const int blk = kb / KB_PER_BLOCK, buf = blk & 1;
-        const bool first = (kb % KB_PER_BLOCK) == 0;
-        if (first && blk >= 2 && !mbar_wait(&dempty[buf], ((blk / 2) - 1) & 1)) {
-          fail(ST_TIMEOUT_DE);
-          break;
-        }
-        if (!mbar_wait(&conv[s], (kb / STAGES) & 1)) {
-          fail(ST_TIMEOUT_CONV);
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        uint8_t* st = base + s * STAGE_BYTES;
-        const uint32_t d = tmem + (uint32_t)(buf * BN);
+      int step = 0, blk = 0;
+      for (long long pos = begin; pos < end && !aborted();) {
+        const Segment g = segment_at(p0, p1, pos, end);
+        const uint32_t idesc = idesc_tf32(BM, g.prod ? p1.bn : p0.bn);
+        for (int k = g.k0; k < g.k1 && !aborted(); ++k, ++step) {
+          const int kin = k - g.k0;
+          const bool first = (kin % KB_PER_BLOCK) == 0;
+          const int buf = blk & 1;
+          if (first && blk >= 2 && !mbar_wait(&dempty[buf], ((blk / 2) - 1) & 1)) {
+            fail(ST_TIMEOUT_DE);
+            break;
+          }
+          const int s = step % STAGES;
+          if (!mbar_wait(&conv[s], (step / STAGES) & 1)) {
+            fail(ST_TIMEOUT_CONV);
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          uint8_t* st = base + s * STAGE_BYTES;
+          const uint32_t d = tmem + (uint32_t)(buf * BN);
 #pragma unroll
-        for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 32 bytes per MMA step
-          const uint64_t ahi = smem_desc(st + kk * 32), alo = smem_desc(st + W_BYTES + kk * 32);
-          const uint64_t bhi = smem_desc(st + 2 * W_BYTES + kk * 32);
-          const uint64_t blo = smem_desc(st + 2 * W_BYTES + U_BYTES + kk * 32);
-          mma_tf32(d, ahi, bhi, (first && kk == 0) ? 0u : 1u);
-          mma_tf32(d, ahi, blo, 1u);
-          mma_tf32(d, alo, bhi, 1u);
+          for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 32 bytes per MMA step
+            const uint64_t ahi = smem_desc_sw128(st + kk * 32), alo = smem_desc_sw128(st + W_BYTES + kk * 32);
+            const uint64_t bhi = smem_desc_sw128(st + 2 * W_BYTES + kk * 32);
+            const uint64_t blo = smem_desc_sw128(st + 2 * W_BYTES + U_BYTES + kk * 32);
+            mma_tf32(d, ahi, bhi, idesc, (first && kk == 0) ? 0u : 1u);
+            mma_tf32(d, ahi, blo, idesc, 1u);
+            mma_tf32(d, alo, bhi, idesc, 1u);
+          }
+          mma_commit(&empty[s]);
+          if ((kin % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || k == g.k1 - 1) {
+            mma_commit(&dfull[buf]);
+            ++blk;
+          }
         }
-        mma_commit(&empty[s]);
-        if ((kb % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || kb == nk - 1) mma_commit(&dfull[buf]);
+        pos += g.k1 - g.k0;
       }
       if (aborted()) {
         // MMAs issued before the abort may still be writing TMEM: wait (bounded) for all of them
@@ -279,46 +269,45 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
   } else {
-    // ---------------- epilogue: FP32 block sums -> FP64 register accumulators ----------------
-    const int r = row0 + warp * 32 + lane;  // W row owned by this thread
-    double acc[BN];
+    // ---------------- epilogue: FP32 block sums -> FP64 register accumulators -> Y ----------------
+    int blk = 0;
+    for (long long pos = begin; pos < end && !aborted();) {
+      const Segment g = segment_at(p0, p1, pos, end);
+      const Product& P = g.prod ? p1 : p0;
+      const int nblocks = (g.k1 - g.k0 + KB_PER_BLOCK - 1) / KB_PER_BLOCK;
+      double acc[BN];
 #pragma unroll
-    for (int t = 0; t < BN; ++t) acc[t] = 0.0;
-    for (int blk = 0; blk < nblocks && !aborted(); ++blk) {
-      const int buf = blk & 1;
-      if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
-        fail(ST_TIMEOUT_D);
-        break;
+      for (int t = 0; t < BN; ++t) acc[t] = 0.0;
+      for (int b = 0; b < nblocks && !aborted(); ++b, ++blk) {
+        const int buf = blk & 1;
+        if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
+          fail(ST_TIMEOUT_D);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+        for (int c = 0; c < BN / 16; ++c) {
+          if (c * 16 < P.bn) {
+            uint32_t v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16), v);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&dempty[buf]);
       }
-      asm volatile("tcgen05.fence::after_thread_sync;");
+      const int r = g.panel * BM + warp * 32 + lane;  // W row owned by this thread
+      if (!aborted() && r < P.np) {
 #pragma unroll
-      for (int c = 0; c < BN / 16; ++c) {
-        uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&dempty[buf]);
-    }
-    if (!aborted() && r < np) {
-#pragma unroll
-      for (int t = 0; t < BN; ++t) {
-        const int j = ublock * BN + t;
-        if (j < m) {
-          // two splits add into the zeroed output: x + y rounds the same in either order, so the
-          // result does not depend on which split finishes first
-          if (ksplit == 1) P.Y[(long long)j * P.ldy + r] = acc[t];
-          else atomicAdd(&P.Y[(long long)j * P.ldy + r], acc[t]);
+        for (int t = 0; t < BN; ++t) {
+          const int j = g.group * P.bn + t;
+          // one or two CTAs add into the zeroed output (see the header)
+          if (t < P.bn && j < P.m) atomicAdd(&P.Y[(long long)j * P.ldy + r], acc[t]);
         }
       }
+      pos += g.k1 - g.k0;
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -426,20 +415,25 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
     err = "promotion block must be a positive multiple of 32";
     return false;
   }
+  if (m <= 0 || np <= 0) {
+    err = "empty all-external product";
+    return false;
+  }
   t.kblock = kblock;
   t.np = np;
   t.m = m;
+  // MMA N: the CI blocks of one group, rounded up to 16 (groups of BN when there are more)
+  t.bn = m >= tci_tc::BN ? tci_tc::BN : (m + 15) / 16 * 16;
   t.y = y;
   t.status = status;
   const uint64_t ld = (uint64_t)padded_ld(np);
   if (!make_map(&t.wmap, w32, np, np, ld, tci_tc::BM, err)) return false;
-  if (!make_map(&t.uhi, uhi, padded_rows(m), np, ld, tci_tc::BN, err)) return false;
-  if (!make_map(&t.ulo, ulo, padded_rows(m), np, ld, tci_tc::BN, err)) return false;
+  if (!make_map(&t.uhi, uhi, padded_rows(m), np, ld, (uint32_t)t.bn, err)) return false;
+  if (!make_map(&t.ulo, ulo, padded_rows(m), np, ld, (uint32_t)t.bn, err)) return false;
   static bool attr = false;
   if (!attr) {
-    const int smem = tci_tc::STAGES * tci_tc::STAGE_BYTES + 1024 + 256;
-    if (cudaFuncSetAttribute(tci_tc::allext_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-        cudaSuccess) {
+    if (cudaFuncSetAttribute(tci_tc::allext_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tci_tc::SMEM_BYTES) != cudaSuccess) {
       err = "cannot raise the dynamic shared memory limit";
       return false;
     }
@@ -448,45 +442,36 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
   return true;
 }
 
-// Two k splits when the tiles fill fewer than four waves of one CTA per SM: the
-// last, partly filled wave then costs less (more than two splits would make
-// the atomic accumulation order-dependent).
-int ksplit(const AllextTc* a, const AllextTc* b) {
-  if (!a) std::swap(a, b);
-  if (!a) return 1;
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t ub = std::max(padded_rows(a->m), b ? padded_rows(b->m) : 0) / tci_tc::BN;
-  const int64_t tiles = ((a->np + tci_tc::BM - 1) / tci_tc::BM + (b ? (b->np + tci_tc::BM - 1) / tci_tc::BM : 0)) * ub;
-  return tiles < 4 * (int64_t)sms ? 2 : 1;
-}
-
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   if (!a && !b) return cudaSuccess;
   if (!a) std::swap(a, b);
-  const int smem = tci_tc::STAGES * tci_tc::STAGE_BYTES + 1024 + 256;
   auto product = [](const AllextTc* t) {
     tci_tc::Product p{};
     if (!t) return p;
     p.np = (int)t->np;
     p.m = (int)t->m;
-    p.tiles = (int)((t->np + tci_tc::BM - 1) / tci_tc::BM);
+    p.bn = (int)t->bn;
+    p.groups = (int)((t->m + t->bn - 1) / t->bn);
+    p.panels = (int)((t->np + tci_tc::BM - 1) / tci_tc::BM);
+    p.nk = (int)((t->np + tci_tc::BK - 1) / tci_tc::BK);
+    p.units = (long long)p.groups * p.panels * p.nk;
     p.Y = t->y;
     p.ldy = t->np;
     return p;
   };
   const tci_tc::Product p0 = product(a), p1 = product(b);
-  const int64_t ub = std::max(padded_rows(a->m), b ? padded_rows(b->m) : 0) / tci_tc::BN;
-  const int ks = ksplit(a, b);
-  if (ks > 1) {  // the two splits accumulate into zeroed outputs
-    cudaError_t e = cudaMemsetAsync(a->y, 0, sizeof(double) * (size_t)(a->m * a->np), st);
-    if (e == cudaSuccess && b) e = cudaMemsetAsync(b->y, 0, sizeof(double) * (size_t)(b->m * b->np), st);
-    if (e != cudaSuccess) return e;
-  }
-  dim3 grid((unsigned)((p0.tiles + p1.tiles) * ks), (unsigned)ub);
+  // one CTA per SM, each range at least one panel long (a panel then spans at most two ranges)
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long total = p0.units + p1.units, nk_max = std::max(p0.nk, p1.nk);
+  const long long grid = std::max<long long>(1, std::min<long long>(sms, total / nk_max));
+  // the CTAs add into zeroed outputs
+  cudaError_t e = cudaMemsetAsync(a->y, 0, sizeof(double) * (size_t)(a->m * a->np), st);
+  if (e == cudaSuccess && b) e = cudaMemsetAsync(b->y, 0, sizeof(double) * (size_t)(b->m * b->np), st);
+  if (e != cudaSuccess) return e;
   const AllextTc* c = b ? b : a;  // maps of the second product (unused when there is none)
-  tci_tc::allext_tf32x3_kernel<<<grid, tci_tc::NTHREADS, smem, st>>>(
-      a->wmap, a->uhi, a->ulo, c->wmap, c->uhi, c->ulo, p0, p1, a->status, (int)(a->kblock / tci_tc::BK), ks);
+  tci_tc::allext_tf32x3_kernel<<<(unsigned)grid, tci_tc::NTHREADS, tci_tc::SMEM_BYTES, st>>>(
+      a->wmap, a->uhi, a->ulo, c->wmap, c->uhi, c->ulo, p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
   return cudaGetLastError();
 }
 

@@ -11,6 +11,7 @@ namespace tci_tc_host {
 struct AllextTc {
   CUtensorMap wmap, uhi, ulo;  // W (np x np, fp32), U hi / lo (padded rows x np, fp32)
   int64_t np = 0, m = 0;
+  int64_t bn = 64;             // MMA N: CI blocks per group (m rounded up to 16, at most 64)
   double* y = nullptr;         // m x np FP64 output (overwritten)
   int* status = nullptr;       // device status word (0 ok, else a bounded wait gave up)
   int64_t kblock = 256;        // k elements per FP64 promotion block
@@ -23,8 +24,7 @@ cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
              int* status, int64_t kblock, std::string& err);
 // Both products in one launch (either may be null; they must share the status
-// word and promotion block).
+// word and promotion block).  Persistent: at most one CTA per SM.
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);
-int ksplit(const AllextTc* a, const AllextTc* b);  // k splits launch() uses (1 or 2)
 
 }  // namespace tci_tc_host
