@@ -4,9 +4,13 @@
 //
 // W (the packed all-external operator W+ or W-, see plan.cpp) is stored in HBM
 // as FP32 and streamed once per sigma build by TMA (128-byte swizzle).  Each
-// W tile is split in shared memory into TF32 hi/lo parts; U arrives pre-split.
-// Three kind::tf32 MMAs per k-step (hi*hi + hi*lo + lo*hi) accumulate FP32 in
-// TMEM; every KBLOCK elements of k the partial sums are read back with
+// W tile is split into TF32 hi/lo parts by converter warps that read it from
+// shared memory a row per thread and store both parts into tensor memory,
+// where the MMA takes its A operand: shared memory then carries W once (TMA
+// write, converter read) instead of once per MMA, which is what bounded the
+// shared-memory form at small N.  U arrives pre-split and is the B operand in
+// shared memory.  Three kind::tf32 MMAs per k-step (hi*hi + hi*lo + lo*hi)
+// accumulate FP32 in TMEM; every KBLOCK elements of k the partial sums are read back with
 // tcgen05.ld and added into FP64 accumulators held in registers (promotion
 // keeps the FP32 accumulation error at the block length).  The product is HBM
 // bound: W is read exactly once.
@@ -45,13 +49,17 @@ using namespace tci_tcx;
 constexpr int BM = 128;      // W rows per panel (MMA M)
 constexpr int BN = 64;       // largest CI-block group (MMA N)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
-constexpr int STAGES = 4;
+constexpr int STAGES = 6;
 constexpr int PREFETCH = 8;  // W tiles requested into L2 ahead of the ring
 // The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
 // a launch parameter: the tensor core's FP32 accumulation error grows with it.
 constexpr int W_BYTES = BM * BK * 4;   // 16 KB
 constexpr int U_BYTES = BN * BK * 4;   // 8 KB (room for the largest group)
-constexpr int STAGE_BYTES = 2 * W_BYTES + 2 * U_BYTES;
+constexpr int STAGE_BYTES = W_BYTES + 2 * U_BYTES;
+// TMEM columns: accumulators 2 x BN, then per stage the A operand's hi (BK columns) and lo (BK columns)
+constexpr int A_COL0 = 2 * BN;
+constexpr int TMEM_COLS = 512;
+static_assert(A_COL0 + STAGES * 2 * BK <= TMEM_COLS, "TMEM columns");
 constexpr int NTHREADS = 320;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 
@@ -62,6 +70,26 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
+// D (tmem) += A (tmem: lane = row, one column per k) * B (shared memory descriptor)
+__device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
+}
+// 32 consecutive 32-bit TMEM columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
+      "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
+      "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+      : "memory");
+}
+
 // Hint: bring a tile into L2 (no shared memory, no completion to wait for).
 __device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
   asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
@@ -138,9 +166,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 9) {  // TMEM: 2 accumulator buffers of BN fp32 columns
+  if (warp == 9) {  // TMEM: 2 accumulator buffers of BN fp32 columns + the A operand of every stage
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * BN));
+                 "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -176,8 +204,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           uint8_t* st = base + s * STAGE_BYTES;
           mbar_expect_tx(&full[s], bytes);
           tma_load_2d(st, wmap, &full[s], k * BK, g.panel * BM);
-          tma_load_2d(st + 2 * W_BYTES, uhi_map, &full[s], k * BK, g.group * bn);
-          tma_load_2d(st + 2 * W_BYTES + U_BYTES, ulo_map, &full[s], k * BK, g.group * bn);
+          tma_load_2d(st + W_BYTES, uhi_map, &full[s], k * BK, g.group * bn);
+          tma_load_2d(st + W_BYTES + U_BYTES, ulo_map, &full[s], k * BK, g.group * bn);
           last = step;
         }
         pos += g.k1 - g.k0;
@@ -190,8 +218,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
   } else if (warp >= 4 && warp < 8) {
-    // ---------------- TF32 hi/lo split of the W tile (in place + lo copy) ----------------
-    const int cw = warp - 4;
+    // ---------------- TF32 hi/lo split of the W tile into TMEM (A operand) ----------------
+    // thread = W row 32 cw + lane = TMEM lane; the 128-byte swizzle puts the 16-byte chunks of
+    // eight consecutive rows on distinct banks, so the row-per-thread reads are conflict free
+    const int cw = warp - 4, row = cw * 32 + lane;
     const long long nsteps = end - begin;
     for (long long step = 0; step < nsteps && !aborted(); ++step) {
       const int s = (int)(step % STAGES);
@@ -199,26 +229,28 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fail(ST_TIMEOUT_FULL);
         break;
       }
-      uint32_t* whi = reinterpret_cast<uint32_t*>(base + s * STAGE_BYTES);
-      uint32_t* wlo = reinterpret_cast<uint32_t*>(base + s * STAGE_BYTES + W_BYTES);
-      // a warp per 128-byte row: lane l holds element l (conflict free; the
-      // swizzle permutes 16-byte chunks within the row, lo keeps the same layout).
-      // Eight rows per batch: their loads are issued before any store, so the
-      // shared-memory latency is paid once per batch.
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint8_t* w = base + s * STAGE_BYTES + row * 128;
+      uint32_t hi[BK], lo[BK];
 #pragma unroll
-      for (int r0 = cw; r0 < BM; r0 += 4 * 8) {
-        uint32_t x[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) x[i] = whi[(r0 + 4 * i) * BK + lane];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const uint32_t hi = x[i] & 0xFFFFE000u;
-          const float lo = __uint_as_float(x[i]) - __uint_as_float(hi);
-          whi[(r0 + 4 * i) * BK + lane] = hi;
-          wlo[(r0 + 4 * i) * BK + lane] = __float_as_uint(lo);
-        }
+      for (int j = 0; j < BK / 4; ++j) {
+        const uint4 q = *reinterpret_cast<const uint4*>(w + ((j ^ (row & 7)) << 4));
+        hi[4 * j] = q.x;
+        hi[4 * j + 1] = q.y;
+        hi[4 * j + 2] = q.z;
+        hi[4 * j + 3] = q.w;
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+      for (int k = 0; k < BK; ++k) {
+        const uint32_t h = hi[k] & 0xFFFFE000u;
+        lo[k] = __float_as_uint(__uint_as_float(hi[k]) - __uint_as_float(h));
+        hi[k] = h;
+      }
+      const uint32_t acol = tmem + ((uint32_t)(cw * 32) << 16) + (uint32_t)(A_COL0 + s * 2 * BK);
+      tmem_st32(acol, hi);
+      tmem_st32(acol + BK, lo);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
       if (lane == 0) mbar_arrive(&conv[s]);
     }
@@ -245,14 +277,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           asm volatile("tcgen05.fence::after_thread_sync;");
           uint8_t* st = base + s * STAGE_BYTES;
           const uint32_t d = tmem + (uint32_t)(buf * BN);
+          const uint32_t ahi = tmem + (uint32_t)(A_COL0 + s * 2 * BK), alo = ahi + BK;
 #pragma unroll
-          for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 32 bytes per MMA step
-            const uint64_t ahi = smem_desc_sw128(st + kk * 32), alo = smem_desc_sw128(st + W_BYTES + kk * 32);
-            const uint64_t bhi = smem_desc_sw128(st + 2 * W_BYTES + kk * 32);
-            const uint64_t blo = smem_desc_sw128(st + 2 * W_BYTES + U_BYTES + kk * 32);
-            mma_tf32(d, ahi, bhi, idesc, (first && kk == 0) ? 0u : 1u);
-            mma_tf32(d, ahi, blo, idesc, 1u);
-            mma_tf32(d, alo, bhi, idesc, 1u);
+          for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 8 TMEM columns / 32 bytes of a B row per MMA step
+            const uint64_t bhi = smem_desc_sw128(st + W_BYTES + kk * 32);
+            const uint64_t blo = smem_desc_sw128(st + W_BYTES + U_BYTES + kk * 32);
+            mma_tf32_ta(d, ahi + kk * 8, bhi, idesc, (first && kk == 0) ? 0u : 1u);
+            mma_tf32_ta(d, ahi + kk * 8, blo, idesc, 1u);
+            mma_tf32_ta(d, alo + kk * 8, bhi, idesc, 1u);
           }
           mma_commit(&empty[s]);
           if ((kin % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || k == g.k1 - 1) {
@@ -313,7 +345,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
-  if (warp == 9) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+  if (warp == 9) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
 // FP64 -> FP32 copy with a padded leading dimension (W at init).
