@@ -3,7 +3,11 @@
 //   Y[j][r] = sum_k W[r][k] U[j][k]      (W symmetric np x np, U: m CI blocks)
 //
 // W (the packed all-external operator W+ or W-, see plan.cpp) is stored in HBM
-// as FP32 and streamed once per sigma build by TMA (128-byte swizzle).  Each
+// as FP32 tiles of 128 rows x 32 k, each a contiguous 16 KB block already in
+// the 128-byte swizzle layout and ordered panel-major then k, so that a CTA's
+// range of k-steps is one sequential stream of HBM, fetched by plain bulk
+// copies and requested into L2 a few tiles ahead.  It is read once per sigma
+// build.  Each
 // W tile is split into TF32 hi/lo parts by converter warps that read it from
 // shared memory a row per thread and store both parts into tensor memory,
 // where the MMA takes its A operand: shared memory then carries W once (TMA
@@ -24,8 +28,7 @@
 // most two CTAs: both add their FP64 partial sums into the zeroed output, and
 // a + b rounds the same in either order, so the result does not depend on
 // which CTA finishes first.  The MMA's N is the operator's own CI-block count
-// rounded up to 16 (at most 64), not a fixed 64, and the TMA producer keeps
-// the W tiles a few stages beyond its ring already on their way into L2.
+// rounded up to 16 (at most 64), not a fixed 64.
 //
 // Warp roles (320 threads): warps 0-3 epilogue (TMEM lane quadrants 0-3),
 // warps 4-7 hi/lo split, warp 8 TMA producer, warp 9 TMEM allocator + MMA
@@ -51,6 +54,7 @@ constexpr int BN = 64;       // largest CI-block group (MMA N)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
 constexpr int STAGES = 6;
 constexpr int PREFETCH = 8;  // W tiles requested into L2 ahead of the ring
+constexpr int TILE_FLOATS = BM * BK;  // one W tile
 // The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
 // a launch parameter: the tensor core's FP32 accumulation error grows with it.
 constexpr int W_BYTES = BM * BK * 4;   // 16 KB
@@ -90,10 +94,16 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32
       : "memory");
 }
 
-// Hint: bring a tile into L2 (no shared memory, no completion to wait for).
-__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
-  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
-               "r"(x), "r"(y)
+// Contiguous global -> shared copy completing on an mbarrier (addresses 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Hint: bring a contiguous range into L2 (no shared memory, no completion to wait for).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
                : "memory");
 }
 
@@ -103,6 +113,7 @@ enum : int { ST_OK = 0, ST_TIMEOUT_FULL = 1, ST_TIMEOUT_CONV = 2, ST_TIMEOUT_EMP
 // One operator of the launch: Y (m x np, row pitch ldy) = U W, as groups of
 // bn CI blocks x panels of BM W rows x nk k-steps.
 struct Product {
+  const float* W;   // tiles of TILE_FLOATS: tile (panel, k) at (panel nk + k) TILE_FLOATS
   int np, m, bn, groups, panels, nk;
   long long units;  // groups * panels * nk
   double* Y;
@@ -131,8 +142,7 @@ __device__ __forceinline__ Segment segment_at(const Product& p0, const Product& 
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1)
-    allext_tf32x3_kernel(const __grid_constant__ CUtensorMap wmap0, const __grid_constant__ CUtensorMap uhi_map0,
-                         const __grid_constant__ CUtensorMap ulo_map0, const __grid_constant__ CUtensorMap wmap1,
+    allext_tf32x3_kernel(const __grid_constant__ CUtensorMap uhi_map0, const __grid_constant__ CUtensorMap ulo_map0,
                          const __grid_constant__ CUtensorMap uhi_map1, const __grid_constant__ CUtensorMap ulo_map1,
                          Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
   const int KB_PER_BLOCK = kb_per_block;
@@ -188,22 +198,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int step = 0, last = -1;  // k-steps issued so far in this CTA; the last one
       for (long long pos = begin; pos < end && !aborted();) {
         const Segment g = segment_at(p0, p1, pos, end);
-        const CUtensorMap* wmap = g.prod ? &wmap1 : &wmap0;
+        const float* wt = (g.prod ? p1.W : p0.W) + (long long)g.panel * (g.prod ? p1.nk : p0.nk) * TILE_FLOATS;
         const CUtensorMap* uhi_map = g.prod ? &uhi_map1 : &uhi_map0;
         const CUtensorMap* ulo_map = g.prod ? &ulo_map1 : &ulo_map0;
         const int bn = g.prod ? p1.bn : p0.bn;
         const uint32_t bytes = (uint32_t)(W_BYTES + 2 * bn * BK * 4);
-        for (int k = g.k0; k < g.k0 + PREFETCH && k < g.k1; ++k) tma_prefetch_2d(wmap, k * BK, g.panel * BM);
+        for (int k = g.k0; k < g.k0 + PREFETCH && k < g.k1; ++k) bulk_prefetch_l2(wt + (long long)k * TILE_FLOATS, W_BYTES);
         for (int k = g.k0; k < g.k1 && !aborted(); ++k, ++step) {
           const int s = step % STAGES;
           if (step >= STAGES && !mbar_wait(&empty[s], ((step / STAGES) - 1) & 1)) {
             fail(ST_TIMEOUT_EMPTY);
             break;
           }
-          if (k + PREFETCH < g.k1) tma_prefetch_2d(wmap, (k + PREFETCH) * BK, g.panel * BM);
+          if (k + PREFETCH < g.k1) bulk_prefetch_l2(wt + (long long)(k + PREFETCH) * TILE_FLOATS, W_BYTES);
           uint8_t* st = base + s * STAGE_BYTES;
           mbar_expect_tx(&full[s], bytes);
-          tma_load_2d(st, wmap, &full[s], k * BK, g.panel * BM);
+          bulk_load(st, wt + (long long)k * TILE_FLOATS, W_BYTES, &full[s]);
           tma_load_2d(st + W_BYTES, uhi_map, &full[s], k * BK, g.group * bn);
           tma_load_2d(st + W_BYTES + U_BYTES, ulo_map, &full[s], k * BK, g.group * bn);
           last = step;
@@ -348,13 +358,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 9) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-// FP64 -> FP32 copy with a padded leading dimension (W at init).
-__global__ void to_f32_padded(const double* __restrict__ src, long long rows, long long cols, long long lds,
-                              float* __restrict__ dst, long long ldd) {
-  const long long total = rows * ldd;
+// FP64 W (np x np) -> FP32 tiles (W at init): tile (panel, k) holds rows panel BM .. +BM-1, columns
+// k BK .. +BK-1 in the 128-byte swizzle layout (16-byte chunks of row r permuted by r mod 8), zero past np.
+__global__ void to_f32_tiles(const double* __restrict__ src, long long np, int nk, float* __restrict__ dst,
+                             long long total) {
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const long long r = e / ldd, c = e % ldd;
-    dst[e] = (c < cols) ? (float)src[r * lds + c] : 0.0f;
+    const long long t = e / TILE_FLOATS;
+    const int i = (int)(e % TILE_FLOATS);  // element index within the tile: row i / BK, column i % BK
+    const int r = i / BK, c = i % BK;
+    const long long panel = t / nk, k = t % nk;
+    const long long gr = panel * BM + r, gc = k * BK + c;
+    const float v = (gr < np && gc < np) ? (float)src[gr * np + gc] : 0.0f;
+    dst[t * TILE_FLOATS + (sw128_offset(r, c) >> 2)] = v;
   }
 }
 
@@ -431,8 +446,13 @@ namespace tci_tc_host {
 int64_t padded_ld(int64_t np) { return (np + 31) / 32 * 32; }
 int64_t padded_rows(int64_t m) { return (m + tci_tc::BN - 1) / tci_tc::BN * tci_tc::BN; }
 
+int64_t w32_floats(int64_t np) {
+  return (np + tci_tc::BM - 1) / tci_tc::BM * tci_tc::BM * ((np + tci_tc::BK - 1) / tci_tc::BK * tci_tc::BK);
+}
+
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st) {
-  tci_tc::to_f32_padded<<<148 * 16, 256, 0, st>>>(w64, np, np, np, w32, padded_ld(np));
+  tci_tc::to_f32_tiles<<<148 * 16, 256, 0, st>>>(w64, np, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
+                                                  (long long)w32_floats(np));
   return cudaGetLastError();
 }
 
@@ -458,8 +478,12 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
   t.bn = m >= tci_tc::BN ? tci_tc::BN : (m + 15) / 16 * 16;
   t.y = y;
   t.status = status;
+  if (reinterpret_cast<uintptr_t>(w32) & 15) {
+    err = "W tiles not 16-byte aligned";
+    return false;
+  }
+  t.w = w32;
   const uint64_t ld = (uint64_t)padded_ld(np);
-  if (!make_map(&t.wmap, w32, np, np, ld, tci_tc::BM, err)) return false;
   if (!make_map(&t.uhi, uhi, padded_rows(m), np, ld, (uint32_t)t.bn, err)) return false;
   if (!make_map(&t.ulo, ulo, padded_rows(m), np, ld, (uint32_t)t.bn, err)) return false;
   static bool attr = false;
@@ -480,6 +504,7 @@ cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   auto product = [](const AllextTc* t) {
     tci_tc::Product p{};
     if (!t) return p;
+    p.W = t->w;
     p.np = (int)t->np;
     p.m = (int)t->m;
     p.bn = (int)t->bn;
@@ -503,7 +528,7 @@ cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   const AllextTc* c = b ? b : a;  // maps of the second product (unused when there is none)
   tci_tc::allext_tf32x3_kernel<<<(unsigned)grid, tci_tc::NTHREADS, tci_tc::SMEM_BYTES, st>>>(
-      a->wmap, a->uhi, a->ulo, c->wmap, c->uhi, c->ulo, p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
+      a->uhi, a->ulo, c->uhi, c->ulo, p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
   return cudaGetLastError();
 }
 

@@ -9,7 +9,8 @@
 namespace tci_tc_host {
 
 struct AllextTc {
-  CUtensorMap wmap, uhi, ulo;  // W (np x np, fp32), U hi / lo (padded rows x np, fp32)
+  CUtensorMap uhi, ulo;        // U hi / lo (padded rows x np, fp32)
+  const float* w = nullptr;    // W as FP32 tiles (convert_w)
   int64_t np = 0, m = 0;
   int64_t bn = 64;             // MMA N: CI blocks per group (m rounded up to 16, at most 64)
   double* y = nullptr;         // m x np FP64 output (overwritten)
@@ -19,6 +20,8 @@ struct AllextTc {
 
 int64_t padded_ld(int64_t np);   // fp32 row pitch (multiple of 32 elements)
 int64_t padded_rows(int64_t m);  // rows of the split U (multiple of 64)
+int64_t w32_floats(int64_t np);  // size of W's FP32 tile array
+// FP64 W (np x np) -> the tile array the kernel streams (w32_floats(np) floats)
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st);
 cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo, cudaStream_t st);
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,

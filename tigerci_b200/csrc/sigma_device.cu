@@ -1116,8 +1116,8 @@ struct tci_ctx {
       owned.push_back(*p);
       bytes_held += (double)n * sizeof(float);
     };
-    alloc_f(&w32p, (size_t)np * tci_tc_host::padded_ld(np));
-    if (nm > 0) alloc_f(&w32m, (size_t)nm * tci_tc_host::padded_ld(nm));
+    alloc_f(&w32p, (size_t)tci_tc_host::w32_floats(np));
+    if (nm > 0) alloc_f(&w32m, (size_t)tci_tc_host::w32_floats(nm));
     alloc_f(&uhi, (size_t)tci_tc_host::padded_rows(std::max<i64>(1, plan.n_sing)) * tci_tc_host::padded_ld(np));
     alloc_f(&ulo, (size_t)tci_tc_host::padded_rows(std::max<i64>(1, plan.n_sing)) * tci_tc_host::padded_ld(np));
     if (has_trip()) {
@@ -1352,8 +1352,8 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
   const double diag = 8.0 * (double)P.total_csfs;
   double pk = all, res = all - init_only + diag;
   if (precision == 1) {
-    const double f32 = 4.0 * ((double)P.np * tci_tc_host::padded_ld(P.np) +
-                              (P.nm > 0 ? (double)P.nm * tci_tc_host::padded_ld(P.nm) : 0.0) +
+    const double f32 = 4.0 * ((double)tci_tc_host::w32_floats(P.np) +
+                              (P.nm > 0 ? (double)tci_tc_host::w32_floats(P.nm) : 0.0) +
                               2.0 * (double)tci_tc_host::padded_rows(std::max<i64>(1, P.n_sing)) *
                                   tci_tc_host::padded_ld(P.np) +
                               (P.nm > 0 ? 2.0 * (double)tci_tc_host::padded_rows(std::max<i64>(1, P.n_trip)) *
