@@ -13,8 +13,11 @@
 // where the MMA takes its A operand: shared memory then carries W once (TMA
 // write, converter read) instead of once per MMA, which is what bounded the
 // shared-memory form at small N.  U arrives pre-split and is the B operand in
-// shared memory.  Three kind::tf32 MMAs per k-step (hi*hi + hi*lo + lo*hi)
-// accumulate FP32 in TMEM; every KBLOCK elements of k the partial sums are read back with
+// shared memory, its high rows directly followed by its low rows.  Per 8-wide
+// k slice two kind::tf32 MMAs (W_hi x [U_hi; U_lo] with N = 2 bn, then W_lo x
+// U_hi with N = bn into the first bn columns) form the three 3xTF32 products:
+// small MMAs cost nearly a fixed time each, so two instructions instead of
+// three is what counts.  They accumulate FP32 in TMEM; every KBLOCK elements of k the partial sums are read back with
 // tcgen05.ld and added into FP64 accumulators held in registers (promotion
 // keeps the FP32 accumulation error at the block length).  The product is HBM
 // bound: W is read exactly once.
@@ -52,16 +55,18 @@ using namespace tci_tcx;
 constexpr int BM = 128;      // W rows per panel (MMA M)
 constexpr int BN = 64;       // largest CI-block group (MMA N)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
-constexpr int STAGES = 6;
+constexpr int STAGES = 4;
 constexpr int PREFETCH = 8;  // W tiles requested into L2 ahead of the ring
 constexpr int TILE_FLOATS = BM * BK;  // one W tile
 // The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
 // a launch parameter: the tensor core's FP32 accumulation error grows with it.
 constexpr int W_BYTES = BM * BK * 4;   // 16 KB
-constexpr int U_BYTES = BN * BK * 4;   // 8 KB (room for the largest group)
-constexpr int STAGE_BYTES = W_BYTES + 2 * U_BYTES;
-// TMEM columns: accumulators 2 x BN, then per stage the A operand's hi (BK columns) and lo (BK columns)
-constexpr int A_COL0 = 2 * BN;
+constexpr int U_BYTES = 2 * BN * BK * 4;   // 16 KB: U hi rows then U lo rows (room for the largest group)
+constexpr int STAGE_BYTES = W_BYTES + U_BYTES;
+// TMEM columns: two accumulator buffers of 2 BN (hi x [hi; lo] + lo x hi), then per stage the A
+// operand's hi (BK columns) and lo (BK columns)
+constexpr int ACC_COLS = 2 * BN;
+constexpr int A_COL0 = 2 * ACC_COLS;
 constexpr int TMEM_COLS = 512;
 static_assert(A_COL0 + STAGES * 2 * BK <= TMEM_COLS, "TMEM columns");
 constexpr int NTHREADS = 320;
@@ -215,7 +220,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           mbar_expect_tx(&full[s], bytes);
           bulk_load(st, wt + (long long)k * TILE_FLOATS, W_BYTES, &full[s]);
           tma_load_2d(st + W_BYTES, uhi_map, &full[s], k * BK, g.group * bn);
-          tma_load_2d(st + W_BYTES + U_BYTES, ulo_map, &full[s], k * BK, g.group * bn);
+          tma_load_2d(st + W_BYTES + bn * BK * 4, ulo_map, &full[s], k * BK, g.group * bn);
           last = step;
         }
         pos += g.k1 - g.k0;
@@ -270,7 +275,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int step = 0, blk = 0;
       for (long long pos = begin; pos < end && !aborted();) {
         const Segment g = segment_at(p0, p1, pos, end);
-        const uint32_t idesc = idesc_tf32(BM, g.prod ? p1.bn : p0.bn);
+        const int bn = g.prod ? p1.bn : p0.bn;
+        const uint32_t idesc_both = idesc_tf32(BM, 2 * bn), idesc_hi = idesc_tf32(BM, bn);
         for (int k = g.k0; k < g.k1 && !aborted(); ++k, ++step) {
           const int kin = k - g.k0;
           const bool first = (kin % KB_PER_BLOCK) == 0;
@@ -286,15 +292,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
           uint8_t* st = base + s * STAGE_BYTES;
-          const uint32_t d = tmem + (uint32_t)(buf * BN);
+          const uint32_t d = tmem + (uint32_t)(buf * ACC_COLS);
           const uint32_t ahi = tmem + (uint32_t)(A_COL0 + s * 2 * BK), alo = ahi + BK;
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 8 TMEM columns / 32 bytes of a B row per MMA step
-            const uint64_t bhi = smem_desc_sw128(st + W_BYTES + kk * 32);
-            const uint64_t blo = smem_desc_sw128(st + W_BYTES + U_BYTES + kk * 32);
-            mma_tf32_ta(d, ahi + kk * 8, bhi, idesc, (first && kk == 0) ? 0u : 1u);
-            mma_tf32_ta(d, ahi + kk * 8, blo, idesc, 1u);
-            mma_tf32_ta(d, alo + kk * 8, bhi, idesc, 1u);
+            const uint64_t b = smem_desc_sw128(st + W_BYTES + kk * 32);  // U hi rows, then U lo rows
+            mma_tf32_ta(d, ahi + kk * 8, b, idesc_both, (first && kk == 0) ? 0u : 1u);
+            mma_tf32_ta(d, alo + kk * 8, b, idesc_hi, 1u);
           }
           mma_commit(&empty[s]);
           if ((kin % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || k == g.k1 - 1) {
@@ -327,11 +331,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t dq = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * ACC_COLS);
 #pragma unroll
         for (int c = 0; c < BN / 16; ++c) {
           if (c * 16 < P.bn) {
             uint32_t v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16), v);
+            tmem_ld16(dq + (uint32_t)(c * 16), v);  // hi x hi + lo x hi
+#pragma unroll
+            for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
+            tmem_ld16(dq + (uint32_t)(P.bn + c * 16), v);  // hi x lo
 #pragma unroll
             for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
           }
