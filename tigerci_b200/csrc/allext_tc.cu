@@ -7,20 +7,25 @@
 // the 128-byte swizzle layout and ordered panel-major then k, so that a CTA's
 // range of k-steps is one sequential stream of HBM, fetched by plain bulk
 // copies and requested into L2 a few tiles ahead.  It is read once per sigma
-// build.  Each
-// W tile is split into TF32 hi/lo parts by converter warps that read it from
-// shared memory a row per thread and store both parts into tensor memory,
-// where the MMA takes its A operand: shared memory then carries W once (TMA
-// write, converter read) instead of once per MMA, which is what bounded the
-// shared-memory form at small N.  U arrives pre-split and is the B operand in
-// shared memory, its high rows directly followed by its low rows.  Per 8-wide
-// k slice two kind::tf32 MMAs (W_hi x [U_hi; U_lo] with N = 2 bn, then W_lo x
-// U_hi with N = bn into the first bn columns) form the three 3xTF32 products:
-// small MMAs cost nearly a fixed time each, so two instructions instead of
-// three is what counts.  They accumulate FP32 in TMEM; every KBLOCK elements of k the partial sums are read back with
+// build.  U arrives split into TF32 high and FP32 low rows, interleaved
+// (row 2j = hi U[j], row 2j+1 = lo U[j]).
+//
+// The 3xTF32 products hi*hi + hi*lo + lo*hi come from ONE kind::tf32 MMA per
+// 8-wide k slice: A = the interleaved U rows of a group of bn <= 64 CI blocks
+// (M = 128 TMEM lanes, 2 bn of them used), B = the W panel's 128 rows followed
+// by their low parts (N = 256).  Lane 2j then holds U_hi[j] W_hi + U_hi[j] W_lo
+// in its two column halves and lane 2j+1 holds U_lo[j] W_hi (its second half,
+// lo x lo, is not used); the epilogue joins the lane pair with a shuffle.  On
+// B200 an MMA costs about the same time whatever its N (measured: ~220 cycles
+// per kind::tf32 slice for N = 16..256), so the instruction count is what
+// bounds this product, and this arrangement needs a quarter of the MMAs of
+// W-in-M with three products.  The tensor core reads a kind::tf32 operand's
+// top 19 bits only (raw FP32 and masked operands gave bit-identical results
+// on B200), so the W tile serves as its own high part as it lands; the
+// converter warps write only the low parts.  The MMAs accumulate FP32 in
+// TMEM; every KBLOCK elements of k the partial sums are read back with
 // tcgen05.ld and added into FP64 accumulators held in registers (promotion
-// keeps the FP32 accumulation error at the block length).  The product is HBM
-// bound: W is read exactly once.
+// keeps the FP32 accumulation error at the block length).
 //
 // Work split (persistent, stream-K): one launch covers both operators (W+
 // with the singlet blocks, W- with the triplet blocks).  Their k-steps form
@@ -30,13 +35,12 @@
 // W bytes.  A range is at least one panel long, so a panel is shared by at
 // most two CTAs: both add their FP64 partial sums into the zeroed output, and
 // a + b rounds the same in either order, so the result does not depend on
-// which CTA finishes first.  The MMA's N is the operator's own CI-block count
-// rounded up to 16 (at most 64), not a fixed 64.
+// which CTA finishes first.
 //
-// Warp roles (320 threads): warps 0-3 epilogue (TMEM lane quadrants 0-3),
-// warps 4-7 hi/lo split, warp 8 TMA producer, warp 9 TMEM allocator + MMA
-// issuer.  Every mbarrier wait is bounded; on timeout the kernel records an
-// error code, drains and returns (no trap).
+// Warp roles (448 threads): warps 0-3 and 10-13 epilogue (two per TMEM lane
+// quadrant), warps 4-7 low parts of the W tile, warp 8 producer (bulk copy +
+// TMA), warp 9 TMEM allocator + MMA issuer.  Every mbarrier wait is bounded; on timeout
+// the kernel records an error code, drains and returns (no trap).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -52,24 +56,22 @@ namespace tci_tc {
 
 using namespace tci_tcx;
 
-constexpr int BM = 128;      // W rows per panel (MMA M)
-constexpr int BN = 64;       // largest CI-block group (MMA N)
+constexpr int BM = 128;      // W rows per panel
+constexpr int BN = 64;       // largest CI-block group (2 BN interleaved U rows = the MMA's M)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
 constexpr int STAGES = 4;
 constexpr int PREFETCH = 8;  // W tiles requested into L2 ahead of the ring
 constexpr int TILE_FLOATS = BM * BK;  // one W tile
+constexpr int MMA_N = 2 * BM;         // W rows, then their low parts
 // The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
 // a launch parameter: the tensor core's FP32 accumulation error grows with it.
-constexpr int W_BYTES = BM * BK * 4;   // 16 KB
-constexpr int U_BYTES = 2 * BN * BK * 4;   // 16 KB: U hi rows then U lo rows (room for the largest group)
-constexpr int STAGE_BYTES = W_BYTES + U_BYTES;
-// TMEM columns: two accumulator buffers of 2 BN (hi x [hi; lo] + lo x hi), then per stage the A
-// operand's hi (BK columns) and lo (BK columns)
-constexpr int ACC_COLS = 2 * BN;
-constexpr int A_COL0 = 2 * ACC_COLS;
-constexpr int TMEM_COLS = 512;
-static_assert(A_COL0 + STAGES * 2 * BK <= TMEM_COLS, "TMEM columns");
-constexpr int NTHREADS = 320;
+constexpr int W_BYTES = BM * BK * 4;        // 16 KB
+constexpr int B_BYTES = 2 * W_BYTES;        // W tile (its own high part) + low parts
+constexpr int A_BYTES = 2 * BN * BK * 4;    // 16 KB: interleaved U rows (room for the largest group)
+constexpr int STAGE_BYTES = B_BYTES + A_BYTES;
+constexpr int TMEM_COLS = 2 * MMA_N;        // two accumulator buffers
+constexpr int NTHREADS = 448;
+constexpr int EPI_WARPS = 8;  // warps 0-3 and 10-13: two per TMEM lane quadrant, each half of the panel
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
@@ -79,26 +81,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
-// D (tmem) += A (tmem: lane = row, one column per k) * B (shared memory descriptor)
-__device__ __forceinline__ void mma_tf32_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
-                                            uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
-}
-// 32 consecutive 32-bit TMEM columns of this warp's 32 lanes
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
-      "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
-      "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
-      : "memory");
-}
-
 // Contiguous global -> shared copy completing on an mbarrier (addresses 16-byte aligned, size a multiple of 16).
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -111,6 +93,14 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
                : "memory");
 }
+
+// 8 consecutive 32-bit TMEM columns of this warp's 32 lanes (complete after tmem_wait_ld).
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Error codes written to the kernel's status word.
 enum : int { ST_OK = 0, ST_TIMEOUT_FULL = 1, ST_TIMEOUT_CONV = 2, ST_TIMEOUT_EMPTY = 3, ST_TIMEOUT_D = 4, ST_TIMEOUT_DE = 5 };
@@ -147,8 +137,7 @@ __device__ __forceinline__ Segment segment_at(const Product& p0, const Product& 
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1)
-    allext_tf32x3_kernel(const __grid_constant__ CUtensorMap uhi_map0, const __grid_constant__ CUtensorMap ulo_map0,
-                         const __grid_constant__ CUtensorMap uhi_map1, const __grid_constant__ CUtensorMap ulo_map1,
+    allext_tf32x3_kernel(const __grid_constant__ CUtensorMap u_map0, const __grid_constant__ CUtensorMap u_map1,
                          Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
   const int KB_PER_BLOCK = kb_per_block;
   const long long total = p0.units + p1.units;
@@ -175,13 +164,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&dfull[b], 1);
-      mbar_init(&dempty[b], 4);
+      mbar_init(&dempty[b], EPI_WARPS);
     }
     mbar_init(mma_done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 9) {  // TMEM: 2 accumulator buffers of BN fp32 columns + the A operand of every stage
+  if (warp == 9) {  // TMEM: 2 accumulator buffers of MMA_N fp32 columns
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -198,14 +187,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   auto aborted = [&]() { return *(volatile int*)abort_flag != 0; };
 
   if (warp == 8) {
-    // ---------------- TMA producer ----------------
+    // ---------------- producer: W tile by bulk copy (L2 lead), U rows by TMA ----------------
     if (lane == 0) {
       int step = 0, last = -1;  // k-steps issued so far in this CTA; the last one
       for (long long pos = begin; pos < end && !aborted();) {
         const Segment g = segment_at(p0, p1, pos, end);
         const float* wt = (g.prod ? p1.W : p0.W) + (long long)g.panel * (g.prod ? p1.nk : p0.nk) * TILE_FLOATS;
-        const CUtensorMap* uhi_map = g.prod ? &uhi_map1 : &uhi_map0;
-        const CUtensorMap* ulo_map = g.prod ? &ulo_map1 : &ulo_map0;
+        const CUtensorMap* u_map = g.prod ? &u_map1 : &u_map0;
         const int bn = g.prod ? p1.bn : p0.bn;
         const uint32_t bytes = (uint32_t)(W_BYTES + 2 * bn * BK * 4);
         for (int k = g.k0; k < g.k0 + PREFETCH && k < g.k1; ++k) bulk_prefetch_l2(wt + (long long)k * TILE_FLOATS, W_BYTES);
@@ -219,8 +207,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           uint8_t* st = base + s * STAGE_BYTES;
           mbar_expect_tx(&full[s], bytes);
           bulk_load(st, wt + (long long)k * TILE_FLOATS, W_BYTES, &full[s]);
-          tma_load_2d(st + W_BYTES, uhi_map, &full[s], k * BK, g.group * bn);
-          tma_load_2d(st + W_BYTES + bn * BK * 4, ulo_map, &full[s], k * BK, g.group * bn);
+          tma_load_2d(st + B_BYTES, u_map, &full[s], k * BK, g.group * 2 * bn);
           last = step;
         }
         pos += g.k1 - g.k0;
@@ -233,10 +220,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
   } else if (warp >= 4 && warp < 8) {
-    // ---------------- TF32 hi/lo split of the W tile into TMEM (A operand) ----------------
-    // thread = W row 32 cw + lane = TMEM lane; the 128-byte swizzle puts the 16-byte chunks of
-    // eight consecutive rows on distinct banks, so the row-per-thread reads are conflict free
-    const int cw = warp - 4, row = cw * 32 + lane;
+    // ---------------- low parts of the W tile: rows BM.. of the B operand ----------------
+    const int cw = warp - 4;
     const long long nsteps = end - begin;
     for (long long step = 0; step < nsteps && !aborted(); ++step) {
       const int s = (int)(step % STAGES);
@@ -244,39 +229,31 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fail(ST_TIMEOUT_FULL);
         break;
       }
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint8_t* w = base + s * STAGE_BYTES + row * 128;
-      uint32_t hi[BK], lo[BK];
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(base + s * STAGE_BYTES);
+      float* wlo = reinterpret_cast<float*>(base + s * STAGE_BYTES + W_BYTES);
+      // a warp per 128-byte row, lane l holds element l (conflict free); row r + BM has the same
+      // swizzle permutation as row r, so the low part keeps the tile's layout.  Eight rows per
+      // batch: their loads are issued before any store.
 #pragma unroll
-      for (int j = 0; j < BK / 4; ++j) {
-        const uint4 q = *reinterpret_cast<const uint4*>(w + ((j ^ (row & 7)) << 4));
-        hi[4 * j] = q.x;
-        hi[4 * j + 1] = q.y;
-        hi[4 * j + 2] = q.z;
-        hi[4 * j + 3] = q.w;
-      }
+      for (int r0 = cw; r0 < BM; r0 += 4 * 8) {
+        uint32_t x[8];
 #pragma unroll
-      for (int k = 0; k < BK; ++k) {
-        const uint32_t h = hi[k] & 0xFFFFE000u;
-        lo[k] = __float_as_uint(__uint_as_float(hi[k]) - __uint_as_float(h));
-        hi[k] = h;
+        for (int i = 0; i < 8; ++i) x[i] = w[(r0 + 4 * i) * BK + lane];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          wlo[(r0 + 4 * i) * BK + lane] = __uint_as_float(x[i]) - __uint_as_float(x[i] & 0xFFFFE000u);
       }
-      const uint32_t acol = tmem + ((uint32_t)(cw * 32) << 16) + (uint32_t)(A_COL0 + s * 2 * BK);
-      tmem_st32(acol, hi);
-      tmem_st32(acol + BK, lo);
-      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&conv[s]);
     }
   } else if (warp == 9) {
     // ---------------- MMA issuer: promotion blocks of KB_PER_BLOCK steps, never across segments ----------------
     if (lane == 0) {
+      const uint32_t idesc = idesc_tf32(2 * BN, MMA_N);
       int step = 0, blk = 0;
       for (long long pos = begin; pos < end && !aborted();) {
         const Segment g = segment_at(p0, p1, pos, end);
-        const int bn = g.prod ? p1.bn : p0.bn;
-        const uint32_t idesc_both = idesc_tf32(BM, 2 * bn), idesc_hi = idesc_tf32(BM, bn);
         for (int k = g.k0; k < g.k1 && !aborted(); ++k, ++step) {
           const int kin = k - g.k0;
           const bool first = (kin % KB_PER_BLOCK) == 0;
@@ -292,14 +269,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
           uint8_t* st = base + s * STAGE_BYTES;
-          const uint32_t d = tmem + (uint32_t)(buf * ACC_COLS);
-          const uint32_t ahi = tmem + (uint32_t)(A_COL0 + s * 2 * BK), alo = ahi + BK;
+          const uint32_t d = tmem + (uint32_t)(buf * MMA_N);
 #pragma unroll
-          for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 8 TMEM columns / 32 bytes of a B row per MMA step
-            const uint64_t b = smem_desc_sw128(st + W_BYTES + kk * 32);  // U hi rows, then U lo rows
-            mma_tf32_ta(d, ahi + kk * 8, b, idesc_both, (first && kk == 0) ? 0u : 1u);
-            mma_tf32_ta(d, alo + kk * 8, b, idesc_hi, 1u);
-          }
+          for (int kk = 0; kk < BK / 8; ++kk)  // 8 tf32 = 32 bytes of every row per MMA
+            mma_tf32(d, smem_desc_sw128(st + B_BYTES + kk * 32), smem_desc_sw128(st + kk * 32), idesc,
+                     (first && kk == 0) ? 0u : 1u);
           mma_commit(&empty[s]);
           if ((kin % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || k == g.k1 - 1) {
             mma_commit(&dfull[buf]);
@@ -314,48 +288,68 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         mbar_wait(mma_done, 0);
       }
     }
-  } else {
-    // ---------------- epilogue: FP32 block sums -> FP64 register accumulators -> Y ----------------
+  } else if (warp < 4 || warp >= 10) {
+    // ---------------- epilogue: lane pairs joined, FP32 block sums -> FP64 registers -> Y ----------------
+    // TMEM lane quadrant q = warp mod 4: lane l is U row 32 q + l = CI block 16 q + l / 2, high (even)
+    // or low (odd) part; warps 0-3 take panel columns 0-63, warps 10-13 columns 64-127.  Per 8-column
+    // chunk the even lane keeps columns 0-3 and the odd lane 4-7 after the pair exchange.
+    const int q = warp & 3, half = warp >= 10 ? 1 : 0;
+    const int odd = lane & 1;
+    const int jl = 16 * q + (lane >> 1);  // CI block within the group
+    constexpr int COLS = BM / 2;          // panel columns per warp
     int blk = 0;
     for (long long pos = begin; pos < end && !aborted();) {
       const Segment g = segment_at(p0, p1, pos, end);
       const Product& P = g.prod ? p1 : p0;
+      const bool active = 32 * q < 2 * P.bn;  // warp-uniform: the quadrant holds used U rows
       const int nblocks = (g.k1 - g.k0 + KB_PER_BLOCK - 1) / KB_PER_BLOCK;
-      double acc[BN];
+      double acc[COLS / 2];
 #pragma unroll
-      for (int t = 0; t < BN; ++t) acc[t] = 0.0;
+      for (int t = 0; t < COLS / 2; ++t) acc[t] = 0.0;
       for (int b = 0; b < nblocks && !aborted(); ++b, ++blk) {
         const int buf = blk & 1;
         if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
           fail(ST_TIMEOUT_D);
           break;
         }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t dq = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * ACC_COLS);
+        if (active) {
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t dq = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * MMA_N + half * COLS);
 #pragma unroll
-        for (int c = 0; c < BN / 16; ++c) {
-          if (c * 16 < P.bn) {
-            uint32_t v[16];
-            tmem_ld16(dq + (uint32_t)(c * 16), v);  // hi x hi + lo x hi
+          for (int c0 = 0; c0 < COLS / 8; c0 += 2) {  // two 8-column chunks per wait
+            uint32_t vh[2][8], vl[2][8];
 #pragma unroll
-            for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
-            tmem_ld16(dq + (uint32_t)(P.bn + c * 16), v);  // hi x lo
+            for (int i = 0; i < 2; ++i) {
+              tmem_ld8(dq + (uint32_t)((c0 + i) * 8), vh[i]);       // x W_hi
+              tmem_ld8(dq + (uint32_t)(BM + (c0 + i) * 8), vl[i]);  // x W_lo
+            }
+            tmem_wait_ld();
 #pragma unroll
-            for (int t = 0; t < 16; ++t) acc[c * 16 + t] += (double)__uint_as_float(v[t]);
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int t = 0; t < 4; ++t) {
+                // even lane: U_hi (W_hi + W_lo); odd lane: U_lo W_hi (both FP32 block sums)
+                const float s0 = __uint_as_float(vh[i][t]) + (odd ? 0.0f : __uint_as_float(vl[i][t]));
+                const float s1 = __uint_as_float(vh[i][4 + t]) + (odd ? 0.0f : __uint_as_float(vl[i][4 + t]));
+                const float recv = __shfl_xor_sync(0xffffffffu, odd ? s0 : s1, 1);
+                acc[(c0 + i) * 4 + t] += (double)((odd ? s1 : s0) + recv);
+              }
           }
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncwarp();
         if (lane == 0) mbar_arrive(&dempty[buf]);
       }
-      const int r = g.panel * BM + warp * 32 + lane;  // W row owned by this thread
-      if (!aborted() && r < P.np) {
+      const int j = g.group * P.bn + jl;
+      if (!aborted() && active && jl < P.bn && j < P.m) {
 #pragma unroll
-        for (int t = 0; t < BN; ++t) {
-          const int j = g.group * P.bn + t;
-          // one or two CTAs add into the zeroed output (see the header)
-          if (t < P.bn && j < P.m) atomicAdd(&P.Y[(long long)j * P.ldy + r], acc[t]);
-        }
+        for (int c = 0; c < COLS / 8; ++c)
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const int r = g.panel * BM + half * COLS + c * 8 + (odd ? 4 : 0) + t;
+            // one or two CTAs add into the zeroed output (see the header)
+            if (r < P.np) atomicAdd(&P.Y[(long long)j * P.ldy + r], acc[c * 4 + t]);
+          }
       }
       pos += g.k1 - g.k0;
     }
@@ -381,21 +375,21 @@ __global__ void to_f32_tiles(const double* __restrict__ src, long long np, int n
   }
 }
 
-// U (m x np, FP64) -> TF32 hi (masked) and lo parts, rows padded to a multiple of BN.
-__global__ void split_u(const double* __restrict__ U, int m, int np, long long ldu, float* __restrict__ hi,
-                        float* __restrict__ lo, int mpad, long long ldw) {
-  const long long total = (long long)mpad * ldw;
+// U (m x np, FP64) -> interleaved rows: 2j = TF32 high part of U[j] (masked), 2j+1 = FP32 low
+// part; rows up to 2 mpad, zero past m and np.
+__global__ void split_u(const double* __restrict__ U, int m, int np, long long ldu, float* __restrict__ u2,
+                        int mpad, long long ldw) {
+  const long long total = (long long)mpad * ldw;  // element pairs
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
     const long long j = e / ldw, k = e % ldw;
     float h = 0.0f, l = 0.0f;
     if (j < m && k < np) {
       const double x = U[j * ldu + k];
-      const float xf = (float)x;
-      h = __uint_as_float(__float_as_uint(xf) & 0xFFFFE000u);
+      h = __uint_as_float(__float_as_uint((float)x) & 0xFFFFE000u);
       l = (float)(x - (double)h);
     }
-    hi[e] = h;
-    lo[e] = l;
+    u2[(2 * j) * ldw + k] = h;
+    u2[(2 * j + 1) * ldw + k] = l;
   }
 }
 
@@ -464,13 +458,15 @@ cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st
   return cudaGetLastError();
 }
 
-cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo, cudaStream_t st) {
-  tci_tc::split_u<<<148 * 4, 256, 0, st>>>(u, (int)m, (int)np, np, hi, lo, (int)padded_rows(m), padded_ld(np));
+int64_t u2_floats(int64_t m, int64_t np) { return 2 * padded_rows(m) * padded_ld(np); }
+
+cudaError_t split_u(const double* u, int64_t m, int64_t np, float* u2, cudaStream_t st) {
+  tci_tc::split_u<<<148 * 4, 256, 0, st>>>(u, (int)m, (int)np, np, u2, (int)padded_rows(m), padded_ld(np));
   return cudaGetLastError();
 }
 
-bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
-             int* status, int64_t kblock, std::string& err) {
+bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t m, double* y, int* status,
+             int64_t kblock, std::string& err) {
   if (kblock < tci_tc::BK || kblock % tci_tc::BK) {
     err = "promotion block must be a positive multiple of 32";
     return false;
@@ -482,8 +478,8 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
   t.kblock = kblock;
   t.np = np;
   t.m = m;
-  // MMA N: the CI blocks of one group, rounded up to 16 (groups of BN when there are more)
-  t.bn = m >= tci_tc::BN ? tci_tc::BN : (m + 15) / 16 * 16;
+  // CI blocks per group (their 2 bn interleaved rows fill at most the MMA's 128 rows)
+  t.bn = m >= tci_tc::BN ? tci_tc::BN : m;
   t.y = y;
   t.status = status;
   if (reinterpret_cast<uintptr_t>(w32) & 15) {
@@ -492,8 +488,7 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const 
   }
   t.w = w32;
   const uint64_t ld = (uint64_t)padded_ld(np);
-  if (!make_map(&t.uhi, uhi, padded_rows(m), np, ld, (uint32_t)t.bn, err)) return false;
-  if (!make_map(&t.ulo, ulo, padded_rows(m), np, ld, (uint32_t)t.bn, err)) return false;
+  if (!make_map(&t.u2, u2, 2 * padded_rows(m), np, ld, (uint32_t)(2 * t.bn), err)) return false;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(tci_tc::allext_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -534,9 +529,9 @@ cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(a->y, 0, sizeof(double) * (size_t)(a->m * a->np), st);
   if (e == cudaSuccess && b) e = cudaMemsetAsync(b->y, 0, sizeof(double) * (size_t)(b->m * b->np), st);
   if (e != cudaSuccess) return e;
-  const AllextTc* c = b ? b : a;  // maps of the second product (unused when there is none)
+  const AllextTc* c = b ? b : a;  // map of the second product (unused when there is none)
   tci_tc::allext_tf32x3_kernel<<<(unsigned)grid, tci_tc::NTHREADS, tci_tc::SMEM_BYTES, st>>>(
-      a->uhi, a->ulo, c->uhi, c->ulo, p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
+      a->u2, c->u2, p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
   return cudaGetLastError();
 }
 

@@ -9,23 +9,24 @@
 namespace tci_tc_host {
 
 struct AllextTc {
-  CUtensorMap uhi, ulo;        // U hi / lo (padded rows x np, fp32)
+  CUtensorMap u2;              // U as interleaved TF32-high / FP32-low rows (2 padded_rows x np, fp32)
   const float* w = nullptr;    // W as FP32 tiles (convert_w)
   int64_t np = 0, m = 0;
-  int64_t bn = 64;             // MMA N: CI blocks per group (m rounded up to 16, at most 64)
+  int64_t bn = 64;             // CI blocks per group (m, at most 64)
   double* y = nullptr;         // m x np FP64 output (overwritten)
   int* status = nullptr;       // device status word (0 ok, else a bounded wait gave up)
   int64_t kblock = 256;        // k elements per FP64 promotion block
 };
 
 int64_t padded_ld(int64_t np);   // fp32 row pitch (multiple of 32 elements)
-int64_t padded_rows(int64_t m);  // rows of the split U (multiple of 64)
+int64_t padded_rows(int64_t m);  // CI blocks of the split U (multiple of 64); it has twice as many rows
+int64_t u2_floats(int64_t m, int64_t np);  // size of the split U
 int64_t w32_floats(int64_t np);  // size of W's FP32 tile array
 // FP64 W (np x np) -> the tile array the kernel streams (w32_floats(np) floats)
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st);
-cudaError_t split_u(const double* u, int64_t m, int64_t np, float* hi, float* lo, cudaStream_t st);
-bool prepare(AllextTc& t, const float* w32, int64_t np, const float* uhi, const float* ulo, int64_t m, double* y,
-             int* status, int64_t kblock, std::string& err);
+cudaError_t split_u(const double* u, int64_t m, int64_t np, float* u2, cudaStream_t st);
+bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t m, double* y, int* status,
+             int64_t kblock, std::string& err);
 // Both products in one launch (either may be null; they must share the status
 // word and promotion block).  Persistent: at most one CTA per SM.
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);

@@ -679,10 +679,8 @@ struct tci_ctx {
   bool tma_dd_ready = false, tma_t3_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
-  float* uhi = nullptr;                 // split singlet CI blocks for the tensor-core product
-  float* ulo = nullptr;
-  float* uhi_t = nullptr;               // split triplet CI blocks
-  float* ulo_t = nullptr;
+  float* u2s = nullptr;                 // split singlet CI blocks for the tensor-core product
+  float* u2t = nullptr;                 // split triplet CI blocks
   int* tc_status = nullptr;
   tci_tc_host::AllextTc tc_sing, tc_trip;
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
@@ -1100,9 +1098,9 @@ struct tci_ctx {
   bool has_trip() const { return plan.n_trip > 0 && plan.nm > 0; }
   void run_allext_tc() {
     if (has_sing())
-      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_us, plan.n_sing, plan.np, uhi, ulo, stream));
+      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_us, plan.n_sing, plan.np, u2s, stream));
     if (has_trip())
-      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, uhi_t, ulo_t, stream));
+      TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, u2t, stream));
     TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream));
   }
 
@@ -1118,11 +1116,9 @@ struct tci_ctx {
     };
     alloc_f(&w32p, (size_t)tci_tc_host::w32_floats(np));
     if (nm > 0) alloc_f(&w32m, (size_t)tci_tc_host::w32_floats(nm));
-    alloc_f(&uhi, (size_t)tci_tc_host::padded_rows(std::max<i64>(1, plan.n_sing)) * tci_tc_host::padded_ld(np));
-    alloc_f(&ulo, (size_t)tci_tc_host::padded_rows(std::max<i64>(1, plan.n_sing)) * tci_tc_host::padded_ld(np));
+    alloc_f(&u2s, (size_t)tci_tc_host::u2_floats(std::max<i64>(1, plan.n_sing), np));
     if (has_trip()) {
-      alloc_f(&uhi_t, (size_t)tci_tc_host::padded_rows(plan.n_trip) * tci_tc_host::padded_ld(nm));
-      alloc_f(&ulo_t, (size_t)tci_tc_host::padded_rows(plan.n_trip) * tci_tc_host::padded_ld(nm));
+      alloc_f(&u2t, (size_t)tci_tc_host::u2_floats(plan.n_trip, nm));
     }
     TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
     owned.push_back(tc_status);
@@ -1159,10 +1155,10 @@ struct tci_ctx {
     TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
     if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
     TCI_CUDA(cudaStreamSynchronize(stream));
-    if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, uhi, ulo, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, tc_kblock, err))
+    if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, u2s, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     if (plan.n_trip > 0 && nm > 0 &&
-        !tci_tc_host::prepare(tc_trip, w32m, nm, uhi_t, ulo_t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
+        !tci_tc_host::prepare(tc_trip, w32m, nm, u2t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     if (!refine) {  // the FP64 W is only needed for the FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
