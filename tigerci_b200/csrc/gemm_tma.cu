@@ -259,6 +259,32 @@ __global__ void split_rows(const double* __restrict__ src, long long rows, long 
   }
 }
 
+// nmat matrices of rows x cols FP64 (row-major, consecutive) -> their transposes as TF32 hi / FP32 lo
+// rows of pitch ldp: row mat cols + c holds column c of matrix mat (columns rows..ldp untouched).
+// 32 x 32 tiles through shared memory; grid (ceil(cols/32), ceil(rows/32), nmat), block 32 x 8.
+__global__ void split_transposed(const double* __restrict__ src, long long rows, long long cols, long long ldp,
+                                 float* __restrict__ hi, float* __restrict__ lo) {
+  __shared__ double t[32][33];
+  const long long mat = blockIdx.z;
+  const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+  const double* m = src + mat * rows * cols;
+  for (int y = threadIdx.y; y < 32; y += 8) {
+    const long long r = r0 + y, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) t[y][threadIdx.x] = m[r * cols + c];
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += 8) {
+    const long long c = c0 + y, r = r0 + threadIdx.x;  // output row c, column r
+    if (r < rows && c < cols) {
+      const double x = t[threadIdx.x][y];
+      const float h = __uint_as_float(__float_as_uint((float)x) & 0xFFFFE000u);
+      const long long o = (mat * cols + c) * ldp + r;
+      hi[o] = h;
+      lo[o] = (float)(x - (double)h);
+    }
+  }
+}
+
 }  // namespace tci_gtma
 
 namespace {
@@ -317,6 +343,19 @@ int64_t pitch(int64_t cols) { return (cols + 31) / 32 * 32; }
 cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st) {
   if (rows <= 0) return cudaSuccess;
   tci_gtma::split_rows<<<148 * 8, 256, 0, st>>>(src, rows, cols, ld, pitch(cols), hi, lo);
+  return cudaGetLastError();
+}
+
+cudaError_t split_transposed(const double* src, int64_t nmat, int64_t rows, int64_t cols, float* hi, float* lo,
+                             cudaStream_t st) {
+  if (nmat <= 0 || rows <= 0 || cols <= 0) return cudaSuccess;
+  const int64_t ldp = pitch(rows);
+  // zero the padding columns once (every element below rows is written by the kernel)
+  cudaError_t e = cudaMemsetAsync(hi, 0, sizeof(float) * (size_t)(nmat * cols * ldp), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(lo, 0, sizeof(float) * (size_t)(nmat * cols * ldp), st);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32), (unsigned)nmat);
+  tci_gtma::split_transposed<<<grid, dim3(32, 8), 0, st>>>(src, rows, cols, ldp, hi, lo);
   return cudaGetLastError();
 }
 

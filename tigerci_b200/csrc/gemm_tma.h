@@ -35,6 +35,9 @@ int tile_n();
 int64_t pitch(int64_t cols);  // FP32 row pitch of a split array (multiple of 32)
 // rows x cols FP64 (row pitch ld) -> hi / lo FP32 (row pitch pitch(cols), zero padded)
 cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st);
+// nmat consecutive rows x cols FP64 matrices -> their transposes, split: cols x pitch(rows) each, stacked
+cudaError_t split_transposed(const double* src, int64_t nmat, int64_t rows, int64_t cols, float* hi, float* lo,
+                             cudaStream_t st);
 // maps over split arrays of arows x acols and brows x bcols
 bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int64_t acols, const float* bhi,
              const float* blo, int64_t brows, int64_t bcols, std::string& err);

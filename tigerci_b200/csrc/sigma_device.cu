@@ -615,7 +615,10 @@ struct DevStep {
   TmaSeg* tma_segs = nullptr;
   int tma_nprob = 0;
   long long tma_ntiles = 0;
-  int tma_kind = 0;  // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows)
+  // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows), 3: reverse
+  // three-external (transposed V_i rows x gathered coefficient rows)
+  int tma_kind = 0;
+  long long tma_aux = 0;  // kind 3: offset of the gathered coefficients U in BUF_T0
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
   DGemmProblem* skinny_probs = nullptr;
   int skinny_nprob = 0;
@@ -675,8 +678,9 @@ struct tci_ctx {
   // split operands of the TMA-fed steps: integrals and V_i once, the pair matrices every build
   float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;
   float *v_hi = nullptr, *v_lo = nullptr, *df_hi = nullptr, *df_lo = nullptr;
-  tci_gtma_host::TmaMaps tma_dd, tma_t3;
-  bool tma_dd_ready = false, tma_t3_ready = false;
+  float *vt_hi = nullptr, *vt_lo = nullptr, *u3_hi = nullptr, *u3_lo = nullptr;  // reverse three-external
+  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r;
+  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* u2s = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -787,6 +791,32 @@ struct tci_ctx {
         push(q);
       }
       d.tma_kind = 2;
+    } else if (s.name == "three-external reverse") {
+      // R (nD x n^2) += sum_i U_i (nD x n) V_i (n x n^2), computed as R^T = sum_i V_i^T U_i^T: A = rows of
+      // the transposed V_i (n^2 x n, K-major), B = rows of U_i; the output tile is stored transposed
+      long long ubase = -1;
+      for (const auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        const DGemmProblem& dp = pr[gi++];
+        if (g.M != plan.nD || g.N != n2 || g.ldc != n2) return;
+        TmaProblem q{dp.C, n2, n2, g.M, 0, 0, g.beta, (long long)ts.size(), 0, 1, nullptr, nullptr, 0};
+        for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
+          const GemmSeg& x = s.gs[(size_t)k];
+          if (x.a != BUF_T0 || x.b != BUF_V || x.tA || x.tB || x.lda != n || x.ldb != n2 || x.K != n ||
+              x.offB % (n * n2))
+            return;
+          const i64 i = x.offB / (n * n2);
+          const long long ub = x.offA - i * plan.nD * n;
+          if (ubase < 0) ubase = ub;
+          if (ub != ubase || i >= plan.nint) return;
+          ts.push_back(TmaSeg{i * n2, i * plan.nD, 0, n, x.alpha});
+        }
+        q.seg_end = (long long)ts.size();
+        push(q);
+      }
+      if (ubase < 0 || ubase + plan.nint * plan.nD * n > plan.buf_size[BUF_T0]) return;
+      d.tma_aux = ubase;
+      d.tma_kind = 3;
     } else {
       return;
     }
@@ -1010,7 +1040,9 @@ struct tci_ctx {
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     sigma_count++;
   }
-  bool tma_ok(const DevStep& s) const { return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready); }
+  bool tma_ok(const DevStep& s) const {
+    return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready);
+  }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
     return precision == 1 && s.probs_tc && (tc_mode == 1 || (tc_mode == 0 && s.tc_ok));
@@ -1123,10 +1155,11 @@ struct tci_ctx {
     TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
-    bool want_dd = false, want_t3 = false;
+    bool want_dd = false, want_t3 = false, want_t3r = false;
     for (const auto& st : sigma) {
       want_dd = want_dd || (st.tma_probs && st.tma_kind == 1);
       want_t3 = want_t3 || (st.tma_probs && st.tma_kind == 2);
+      want_t3r = want_t3r || (st.tma_probs && st.tma_kind == 3);
     }
     const i64 n = plan.n, n2 = n * n;
     std::string err;
@@ -1150,6 +1183,18 @@ struct tci_ctx {
       if (!tci_gtma_host::prepare(tma_t3, v_hi, v_lo, vrows, n2, df_hi, df_lo, plan.nD, n2, err))
         throw Error(TCI_ERR_CUDA, err);
       tma_t3_ready = true;
+    }
+    if (want_t3r && plan.nD > 0) {
+      // V_i transposed once (static operator); the gathered coefficients are split every sigma build
+      const i64 ld = tci_gtma_host::pitch(n), vtrows = plan.nint * n2, urows = plan.nint * plan.nD;
+      alloc_f(&vt_hi, (size_t)(vtrows * ld));
+      alloc_f(&vt_lo, (size_t)(vtrows * ld));
+      alloc_f(&u3_hi, (size_t)(urows * ld));
+      alloc_f(&u3_lo, (size_t)(urows * ld));
+      TCI_CUDA(tci_gtma_host::split_transposed(buf[BUF_V], plan.nint, n, n2, vt_hi, vt_lo, stream));
+      if (!tci_gtma_host::prepare(tma_t3r, vt_hi, vt_lo, vtrows, n, u3_hi, u3_lo, urows, n, err))
+        throw Error(TCI_ERR_CUDA, err);
+      tma_t3r_ready = true;
     }
     TCI_CUDA(cudaMemsetAsync(tc_status, 0, sizeof(int), stream));
     TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
@@ -1228,9 +1273,13 @@ struct tci_ctx {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * n, n, n, d_hi, d_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_dd, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
-          } else {
+          } else if (s.tma_kind == 2) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_t3, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          } else {
+            TCI_CUDA(tci_gtma_host::split(buf[BUF_T0] + s.tma_aux, plan.nint * plan.nD, n, n, u3_hi, u3_lo, stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_t3r, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
           }
           break;
@@ -1358,7 +1407,9 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                               // split integrals and pair matrices of the TMA-fed two-external step
                               2.0 * (double)tci_gtma_host::pitch(P.n) *
                                   (double)(P.buf_size[BUF_JK] / std::max<i64>(1, P.n) + P.nD * P.n) +
-                              2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * (double)(P.nint * P.n + P.nD));
+                              2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * (double)(P.nint * P.n + P.nD) +
+                              // transposed V_i and the gathered coefficients of the reverse three-external step
+                              2.0 * (double)tci_gtma_host::pitch(P.n) * (double)(P.nint * P.n * P.n + P.nint * P.nD));
     pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
     res += f32 - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
