@@ -38,7 +38,11 @@ constexpr int NTHREADS = 192;
 constexpr int A_BYTES = BM * BK * 4, B_BYTES = BN * BK * 4;
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
+// B's high rows are followed by its low rows in a stage, so A_hi x [B_hi; B_lo] is one MMA of N = 2 BN
+// and A_lo x B_hi a second one: two instructions per k slice instead of three (an MMA costs about the
+// same time whatever its N)
+constexpr uint32_t kIdescBoth = idesc_tf32(BM, 2 * BN), kIdescHi = idesc_tf32(BM, BN);
+constexpr int ACC_COLS = 2 * BN;  // hi x hi + lo x hi, then hi x lo
 
 enum : int { ST_TIMEOUT_EMPTY = 21, ST_TIMEOUT_FULL = 22, ST_TIMEOUT_D = 23, ST_TIMEOUT_DE = 24 };
 
@@ -92,7 +96,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   }
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * BN));
+                 "r"(2 * ACC_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -152,15 +156,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
           uint8_t* st = base + s * STAGE_BYTES;
-          const uint32_t d = tmem + (uint32_t)(buf * BN);
+          const uint32_t d = tmem + (uint32_t)(buf * ACC_COLS);
 #pragma unroll
           for (int k8 = 0; k8 < BK / 8; ++k8) {
             const uint64_t ahi = smem_desc_sw128(st + k8 * 32), alo = smem_desc_sw128(st + A_BYTES + k8 * 32);
-            const uint64_t bhi = smem_desc_sw128(st + 2 * A_BYTES + k8 * 32);
-            const uint64_t blo = smem_desc_sw128(st + 2 * A_BYTES + B_BYTES + k8 * 32);
-            mma_tf32(d, ahi, bhi, kIdesc, (first && k8 == 0) ? 0u : 1u);
-            mma_tf32(d, ahi, blo, kIdesc, 1u);
-            mma_tf32(d, alo, bhi, kIdesc, 1u);
+            const uint64_t b = smem_desc_sw128(st + 2 * A_BYTES + k8 * 32);  // B hi rows, then B lo rows
+            mma_tf32(d, ahi, b, kIdescBoth, (first && k8 == 0) ? 0u : 1u);
+            mma_tf32(d, alo, b, kIdescHi, 1u);
           }
           mma_commit(&empty[s]);
           if ((kk % kbs) == kbs - 1 || kk == nk - 1) {
@@ -195,7 +197,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
         for (int c = 0; c < BN / 16; ++c) {
           uint32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16), v);
+          const uint32_t tq = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * ACC_COLS + c * 16);
+          tmem_ld16(tq, v);  // hi x hi + lo x hi
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
+          tmem_ld16(tq + BN, v);  // hi x lo
 #pragma unroll
           for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
         }
@@ -239,7 +245,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
-  if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+  if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACC_COLS));
 }
 
 // rows x cols FP64 (row pitch ld) -> TF32 hi / FP32 lo with row pitch ldp (columns cols..ldp zero)
