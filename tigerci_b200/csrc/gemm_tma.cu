@@ -16,8 +16,9 @@
 // touch the operands, and writes C (or C^T) once, or, for a product that feeds
 // the next one, its TF32 high / FP32 low parts.
 //
-// Warp roles (192 threads): 0-3 epilogue, 4 TMA producer, 5 TMEM allocator +
-// MMA issuer.  Bounded waits; on an abort the kernel waits (bounded) for its
+// Tiles are 128 x 128.  Warp roles (320 threads): 0-7 epilogue (two warps per
+// TMEM lane quadrant, one per half of the tile's columns), 8 TMA producer, 9
+// TMEM allocator + MMA issuer.  Bounded waits; on an abort the kernel waits (bounded) for its
 // copies and MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -33,16 +34,23 @@ namespace tci_gtma {
 
 using namespace tci_tcx;
 
-constexpr int BM = 128, BN = 64, BK = 32, STAGES = 4;
-constexpr int NTHREADS = 192;
-constexpr int A_BYTES = BM * BK * 4, B_BYTES = BN * BK * 4;
-constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-// B's high rows are followed by its low rows in a stage, so A_hi x [B_hi; B_lo] is one MMA of N = 2 BN
-// and A_lo x B_hi a second one: two instructions per k slice instead of three (an MMA costs about the
-// same time whatever its N)
-constexpr uint32_t kIdescBoth = idesc_tf32(BM, 2 * BN), kIdescHi = idesc_tf32(BM, BN);
-constexpr int ACC_COLS = 2 * BN;  // hi x hi + lo x hi, then hi x lo
+constexpr int BM = 128, BK = 32;
+constexpr int NTHREADS = 320;
+constexpr int EPI_WARPS = 8;  // warps 0-3: first half of the tile's columns, 4-7: second half (TMEM quadrant = warp mod 4)
+constexpr int A_BYTES = BM * BK * 4;
+constexpr int SMEM_BYTES = 192 * 1024 + 1024 + 256;  // both tile widths use 192 KB of stages
+// Tile width BN = 128 (wide operands) or 64 (B with few rows).  B's high rows are followed by its low
+// rows in a stage, so A_hi x [B_hi; B_lo] is one MMA of N = 2 BN and A_lo x B_hi a second one: two
+// instructions per k slice (an MMA costs about the same time whatever its N, so wide tiles and few
+// instructions are what count).
+template <int BN>
+struct Tile {
+  static constexpr int B_BYTES = BN * BK * 4;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int STAGES = (192 * 1024) / STAGE_BYTES;  // 3 (BN 128) or 4 (BN 64)
+  static constexpr uint32_t kIdescBoth = idesc_tf32(BM, 2 * BN), kIdescHi = idesc_tf32(BM, BN);
+  static constexpr int ACC_COLS = 2 * BN;  // hi x hi + lo x hi, then hi x lo
+};
 
 enum : int { ST_TIMEOUT_EMPTY = 21, ST_TIMEOUT_FULL = 22, ST_TIMEOUT_D = 23, ST_TIMEOUT_DE = 24 };
 
@@ -54,11 +62,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     gemm_tma_tf32x3(const __grid_constant__ CUtensorMap ahi_map, const __grid_constant__ CUtensorMap alo_map,
                     const __grid_constant__ CUtensorMap bhi_map, const __grid_constant__ CUtensorMap blo_map,
                     const TmaProblem* __restrict__ probs, int nprob, const TmaSeg* __restrict__ segs, int kbs,
                     int* __restrict__ status) {
+  using T = Tile<BN>;
+  constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES, B_BYTES = T::B_BYTES, ACC_COLS = T::ACC_COLS;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
@@ -88,13 +99,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&dfull[b], 1);
-      mbar_init(&dempty[b], 4);
+      mbar_init(&dempty[b], EPI_WARPS);
     }
     mbar_init(mma_done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 5) {
+  if (warp == 9) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(2 * ACC_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -110,7 +121,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   };
   auto aborted = [&]() { return *(volatile int*)abort_flag != 0; };
 
-  if (warp == 4) {
+  if (warp == 8) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
       int step = 0, last = -1;
@@ -137,7 +148,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int st = (last - STAGES + 1 > 0 ? last - STAGES + 1 : 0); st <= last; ++st)
           mbar_wait(&full[st % STAGES], (st / STAGES) & 1);
     }
-  } else if (warp == 5) {
+  } else if (warp == 9) {
     // ---------------- MMA issuer: blocks of at most kbs k steps, never across segments ----------------
     if (lane == 0) {
       int step = 0, blk = 0;
@@ -161,8 +172,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           for (int k8 = 0; k8 < BK / 8; ++k8) {
             const uint64_t ahi = smem_desc_sw128(st + k8 * 32), alo = smem_desc_sw128(st + A_BYTES + k8 * 32);
             const uint64_t b = smem_desc_sw128(st + 2 * A_BYTES + k8 * 32);  // B hi rows, then B lo rows
-            mma_tf32(d, ahi, b, kIdescBoth, (first && k8 == 0) ? 0u : 1u);
-            mma_tf32(d, alo, b, kIdescHi, 1u);
+            mma_tf32(d, ahi, b, T::kIdescBoth, (first && k8 == 0) ? 0u : 1u);
+            mma_tf32(d, alo, b, T::kIdescHi, 1u);
           }
           mma_commit(&empty[s]);
           if ((kk % kbs) == kbs - 1 || kk == nk - 1) {
@@ -178,10 +189,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
   } else {
     // ---------------- epilogue: alpha_s * block -> FP64 registers -> C ----------------
-    const long long r = m0 + warp * 32 + lane;
-    double acc[BN];
+    constexpr int COLS = BN / 2;  // tile columns per epilogue warp
+    const int q = warp & 3, half = warp >> 2;
+    const long long r = m0 + q * 32 + lane;
+    const int nc0 = n0 + half * COLS;  // first output column of this warp
+    double acc[COLS];
 #pragma unroll
-    for (int j = 0; j < BN; ++j) acc[j] = 0.0;
+    for (int j = 0; j < COLS; ++j) acc[j] = 0.0;
     int blk = 0;
     for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
       const double a = segs[q].alpha;
@@ -195,9 +209,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-        for (int c = 0; c < BN / 16; ++c) {
+        for (int c = 0; c < COLS / 16; ++c) {
           uint32_t v[16];
-          const uint32_t tq = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * ACC_COLS + c * 16);
+          const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * ACC_COLS + half * COLS + c * 16);
           tmem_ld16(tq, v);  // hi x hi + lo x hi
 #pragma unroll
           for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
@@ -215,8 +229,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         float* hrow = P.c_hi + r * P.ldcs;
         float* lrow = P.c_lo + r * P.ldcs;
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const long long c = n0 + j;
+        for (int j = 0; j < COLS; ++j) {
+          const long long c = nc0 + j;
           if (c < P.N) {
             const float h = __uint_as_float(__float_as_uint((float)acc[j]) & 0xFFFFE000u);
             hrow[c] = h;
@@ -226,14 +240,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       } else if (!P.trans_c) {
         double* crow = P.C + r * P.ldc;
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const long long c = n0 + j;
+        for (int j = 0; j < COLS; ++j) {
+          const long long c = nc0 + j;
           if (c < P.N) crow[c] = (P.beta == 0.0 ? 0.0 : P.beta * crow[c]) + acc[j];
         }
       } else {  // C^T: element (r, c) goes to C[c][r]; lanes hold consecutive r (coalesced)
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const long long c = n0 + j;
+        for (int j = 0; j < COLS; ++j) {
+          const long long c = nc0 + j;
           if (c < P.N) {
             double* y = P.C + c * P.ldc + r;
             *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + acc[j];
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
-  if (warp == 5) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACC_COLS));
+  if (warp == 9) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACC_COLS));
 }
 
 // rows x cols FP64 (row pitch ld) -> TF32 hi / FP32 lo with row pitch ldp (columns cols..ldp zero)
@@ -343,7 +357,7 @@ bool make_map(CUtensorMap* map, const float* p, uint64_t rows, uint64_t n, uint6
 namespace tci_gtma_host {
 
 int tile_m() { return tci_gtma::BM; }
-int tile_n() { return tci_gtma::BN; }
+int tile_n(bool wide) { return wide ? 128 : 64; }
 int64_t pitch(int64_t cols) { return (cols + 31) / 32 * 32; }
 
 cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st) {
@@ -366,15 +380,19 @@ cudaError_t split_transposed(const double* src, int64_t nmat, int64_t rows, int6
 }
 
 bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int64_t acols, const float* bhi,
-             const float* blo, int64_t brows, int64_t bcols, std::string& err) {
+             const float* blo, int64_t brows, int64_t bcols, bool wide, std::string& err) {
+  m.wide = wide;
+  const uint32_t bn = (uint32_t)tile_n(wide);
   if (!make_map(&m.ahi, ahi, arows, acols, pitch(acols), tci_gtma::BM, err) ||
       !make_map(&m.alo, alo, arows, acols, pitch(acols), tci_gtma::BM, err) ||
-      !make_map(&m.bhi, bhi, brows, bcols, pitch(bcols), tci_gtma::BN, err) ||
-      !make_map(&m.blo, blo, brows, bcols, pitch(bcols), tci_gtma::BN, err))
+      !make_map(&m.bhi, bhi, brows, bcols, pitch(bcols), bn, err) ||
+      !make_map(&m.blo, blo, brows, bcols, pitch(bcols), bn, err))
     return false;
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(tci_gtma::gemm_tma_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(tci_gtma::gemm_tma_tf32x3<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tci_gtma::SMEM_BYTES) != cudaSuccess ||
+        cudaFuncSetAttribute(tci_gtma::gemm_tma_tf32x3<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              tci_gtma::SMEM_BYTES) != cudaSuccess) {
       err = "cannot raise the dynamic shared memory limit";
       return false;
@@ -387,8 +405,12 @@ bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int6
 cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const TmaSeg* segs, long long ntiles,
                    int kblock, int* status, cudaStream_t st) {
   if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
-  tci_gtma::gemm_tma_tf32x3<<<(unsigned)ntiles, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
-      m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, kblock / tci_gtma::BK, status);
+  if (m.wide)
+    tci_gtma::gemm_tma_tf32x3<128><<<(unsigned)ntiles, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
+        m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, kblock / tci_gtma::BK, status);
+  else
+    tci_gtma::gemm_tma_tf32x3<64><<<(unsigned)ntiles, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
+        m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, kblock / tci_gtma::BK, status);
   return cudaGetLastError();
 }
 

@@ -6,7 +6,7 @@
 #include <cstdint>
 #include <string>
 
-// C (row pitch ldc) = beta C + sum over segments alpha A_rows B_rows^T, tiles of 128 x 64
+// C (row pitch ldc) = beta C + sum over segments alpha A_rows B_rows^T, tiles of 128 x tile_n(wide)
 struct TmaProblem {
   double* C;
   long long ldc, M, N, tiles_n, tile_begin;
@@ -28,10 +28,11 @@ namespace tci_gtma_host {
 // TF32-high / FP32-low copies of two FP64 row arrays, and their tensor maps
 struct TmaMaps {
   CUtensorMap ahi, alo, bhi, blo;
+  bool wide = true;  // tile width 128 (else 64, for B operands of at most 64 rows per problem)
 };
 
 int tile_m();
-int tile_n();
+int tile_n(bool wide);
 int64_t pitch(int64_t cols);  // FP32 row pitch of a split array (multiple of 32)
 // rows x cols FP64 (row pitch ld) -> hi / lo FP32 (row pitch pitch(cols), zero padded)
 cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st);
@@ -40,7 +41,7 @@ cudaError_t split_transposed(const double* src, int64_t nmat, int64_t rows, int6
                              cudaStream_t st);
 // maps over split arrays of arows x acols and brows x bcols
 bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int64_t acols, const float* bhi,
-             const float* blo, int64_t brows, int64_t bcols, std::string& err);
+             const float* blo, int64_t brows, int64_t bcols, bool wide, std::string& err);
 // kblock: k elements per FP64 promotion block (multiple of 32)
 cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const TmaSeg* segs, long long ntiles,
                    int kblock, int* status, cudaStream_t st);

@@ -301,7 +301,7 @@ struct tci_local {
 
   // mixed form: TMA-fed tables for chunks of j vectors
   void make_tma(int64_t j, TmaLaunch& a, TmaLaunch& b) {
-    const long long TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n();
+    const long long TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n(map1.wide);
     std::vector<TmaProblem> p1, p2;
     std::vector<TmaSeg> s1, s2;
     long long t1 = 0, t2 = 0;
@@ -532,8 +532,11 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
       falloc(&L->t_hi, L->rows_t);
       falloc(&L->t_lo, L->rows_t);
       std::string err;
-      if (!tci_gtma_host::prepare(L->map1, L->lc_hi, L->lc_lo, L->rows_l, nmax, L->d_hi, L->d_lo, L->rows_d, nmax, err) ||
-          !tci_gtma_host::prepare(L->map2, L->t_hi, L->t_lo, L->rows_t, nmax, L->lc_hi, L->lc_lo, L->rows_l, nmax, err))
+      const bool wide = nmax > 64;  // tile width: the B operands have n_h rows per problem
+      if (!tci_gtma_host::prepare(L->map1, L->lc_hi, L->lc_lo, L->rows_l, nmax, L->d_hi, L->d_lo, L->rows_d, nmax, wide,
+                                  err) ||
+          !tci_gtma_host::prepare(L->map2, L->t_hi, L->t_lo, L->rows_t, nmax, L->lc_hi, L->lc_lo, L->rows_l, nmax, wide,
+                                  err))
         throw Error(TCI_ERR_CUDA, err);
     } else {
       L->Lc = L->alloc((size_t)(lc_per_j * L->jmax));

@@ -737,7 +737,8 @@ struct tci_ctx {
   // rows times V_i rows, computed transposed); a step that does not fit keeps the producer-fed kernel.
   void lower_tma(const Step& s, DevStep& d, const std::vector<DGemmProblem>& pr) {
     const i64 n = plan.n, n2 = n * n;
-    const i64 TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n();
+    const i64 TM = tci_gtma_host::tile_m();
+    i64 TN = tci_gtma_host::tile_n(true);
     std::vector<TmaProblem> tp;
     std::vector<TmaSeg> ts;
     long long tiles = 0;
@@ -749,6 +750,7 @@ struct tci_ctx {
     };
     size_t gi = 0;
     if (s.name == "dd two-external") {
+      TN = tci_gtma_host::tile_n(tma_wide(1));
       std::vector<double> psign((size_t)std::max<i64>(plan.nD, 1), 1.0);
       for (const auto& h : plan.dheads)
         for (i64 k = 0; k < h.nD; ++k) psign[(size_t)(h.dk0 + k)] = k < h.nsing ? 1.0 : -1.0;
@@ -776,6 +778,7 @@ struct tci_ctx {
       }
       d.tma_kind = 1;
     } else if (s.name == "three-external forward") {
+      TN = tci_gtma_host::tile_n(tma_wide(2));
       for (const auto& g : s.gp) {
         if (g.M <= 0 || g.N <= 0) continue;
         const DGemmProblem& dp = pr[gi++];
@@ -792,6 +795,7 @@ struct tci_ctx {
       }
       d.tma_kind = 2;
     } else if (s.name == "three-external reverse") {
+      TN = tci_gtma_host::tile_n(tma_wide(3));
       // R (nD x n^2) += sum_i U_i (nD x n) V_i (n x n^2), computed as R^T = sum_i V_i^T U_i^T: A = rows of
       // the transposed V_i (n^2 x n, K-major), B = rows of U_i; the output tile is stored transposed
       long long ubase = -1;
@@ -1040,6 +1044,8 @@ struct tci_ctx {
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     sigma_count++;
   }
+  // TMA-fed kernel's tile width per step kind: 128 unless the B operand has at most 64 rows per problem
+  bool tma_wide(int kind) const { return kind == 1 ? plan.n > 64 : plan.nD > 64; }
   bool tma_ok(const DevStep& s) const {
     return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready);
   }
@@ -1170,7 +1176,7 @@ struct tci_ctx {
       alloc_f(&d_hi, (size_t)(drows * ld));
       alloc_f(&d_lo, (size_t)(drows * ld));
       TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, n, jk_hi, jk_lo, stream));
-      if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows, n, d_hi, d_lo, drows, n, err)) throw Error(TCI_ERR_CUDA, err);
+      if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows, n, d_hi, d_lo, drows, n, tma_wide(1), err)) throw Error(TCI_ERR_CUDA, err);
       tma_dd_ready = true;
     }
     if (want_t3 && plan.nD > 0) {
@@ -1180,7 +1186,7 @@ struct tci_ctx {
       alloc_f(&df_hi, (size_t)(plan.nD * ld));
       alloc_f(&df_lo, (size_t)(plan.nD * ld));
       TCI_CUDA(tci_gtma_host::split(buf[BUF_V], vrows, n2, n2, v_hi, v_lo, stream));
-      if (!tci_gtma_host::prepare(tma_t3, v_hi, v_lo, vrows, n2, df_hi, df_lo, plan.nD, n2, err))
+      if (!tci_gtma_host::prepare(tma_t3, v_hi, v_lo, vrows, n2, df_hi, df_lo, plan.nD, n2, tma_wide(2), err))
         throw Error(TCI_ERR_CUDA, err);
       tma_t3_ready = true;
     }
@@ -1192,7 +1198,7 @@ struct tci_ctx {
       alloc_f(&u3_hi, (size_t)(urows * ld));
       alloc_f(&u3_lo, (size_t)(urows * ld));
       TCI_CUDA(tci_gtma_host::split_transposed(buf[BUF_V], plan.nint, n, n2, vt_hi, vt_lo, stream));
-      if (!tci_gtma_host::prepare(tma_t3r, vt_hi, vt_lo, vtrows, n, u3_hi, u3_lo, urows, n, err))
+      if (!tci_gtma_host::prepare(tma_t3r, vt_hi, vt_lo, vtrows, n, u3_hi, u3_lo, urows, n, tma_wide(3), err))
         throw Error(TCI_ERR_CUDA, err);
       tma_t3r_ready = true;
     }
