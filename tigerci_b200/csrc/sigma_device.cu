@@ -561,6 +561,15 @@ __global__ void multi_dot_final(const double* __restrict__ partial, int m, int n
   out[k] = t;
 }
 
+// out[k] = -(sum of the partials of k): the coefficients of one classical Gram-Schmidt pass
+__global__ void multi_dot_final_neg(const double* __restrict__ partial, int m, int nblk, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  double t = 0.0;
+  for (int b = 0; b < nblk; ++b) t += partial[(long long)k * nblk + b];
+  out[k] = -t;
+}
+
 // out[i] = beta*out[i] + sum_k ca[k] A[k][i] + sum_k cb[k] B[k][i]
 __global__ void lincomb_kernel(double* __restrict__ out, double beta, const double* __restrict__ A,
                                const double* __restrict__ ca, const double* __restrict__ B,
@@ -583,13 +592,7 @@ __global__ void precondition_kernel(double* __restrict__ r, const double* __rest
   }
 }
 
-// r <- (r - ov*c) then scaled by 1/|r| (or zeroed) in a second pass
-__global__ void axpy_scale_kernel(double* __restrict__ r, const double* __restrict__ c, const double* __restrict__ ov,
-                                  long long n) {
-  const double a = *ov;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    r[i] = fma(-a, c[i], r[i]);
-}
+// r scaled by 1/|r| (or zeroed when |r| < 1e-14)
 __global__ void normalize_kernel(double* __restrict__ r, const double* __restrict__ nrm2, long long n) {
   const double nr = sqrt(*nrm2);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -1888,14 +1891,25 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
           precondition_kernel<<<G, TB, 0, st>>>(r, ctx->hd, energy[q], n);
           ctx->launch_count++;
           TCI_CUDA(cudaGetLastError());
+          // Orthogonalise against the basis (the reference's davidson.f90 runs modified Gram-Schmidt,
+          // normalising after each projection).  Here: normalise, then block classical Gram-Schmidt twice
+          // (all projections of one pass from one multi-dot and one linear combination), then normalise
+          // with the same 1e-14 zeroing rule: the same vector up to rounding, as stable as modified
+          // Gram-Schmidt, and four passes over the basis instead of two per basis vector.
           double* dev_ov = ctx->dots + (size_t)(cap + 4) * RBLK;
-          for (int k = 0; k < num_vec; ++k) {
-            ctx->dot_dev(r, Cs + (size_t)k * n, n, dev_ov);
-            axpy_scale_kernel<<<G, TB, 0, st>>>(r, Cs + (size_t)k * n, dev_ov, n);
-            ctx->dot_dev(r, r, n, dev_ov + 1);
-            normalize_kernel<<<G, TB, 0, st>>>(r, dev_ov + 1, n);
-            ctx->launch_count += 2;
+          double* dev_coef = dev_ov + 2;  // num_vec <= cap coefficients fit the buffer's tail
+          ctx->dot_dev(r, r, n, dev_ov + 1);
+          normalize_kernel<<<G, TB, 0, st>>>(r, dev_ov + 1, n);
+          ctx->launch_count++;
+          for (int pass = 0; pass < 2 && num_vec > 0; ++pass) {
+            multi_dot_partial<<<RBLK, RB, 0, st>>>(Cs, n, num_vec, r, n, ctx->dots);
+            multi_dot_final_neg<<<(num_vec + 127) / 128, 128, 0, st>>>(ctx->dots, num_vec, RBLK, dev_coef);
+            lincomb_kernel<<<G, TB, 0, st>>>(r, 1.0, Cs, dev_coef, nullptr, nullptr, num_vec, n, n);
+            ctx->launch_count += 3;
           }
+          ctx->dot_dev(r, r, n, dev_ov + 1);
+          normalize_kernel<<<G, TB, 0, st>>>(r, dev_ov + 1, n);
+          ctx->launch_count++;
           TCI_CUDA(cudaGetLastError());
           if (num_vec >= cap) throw Error(TCI_ERR_INTERNAL, "Davidson subspace capacity exceeded");
           TCI_CUDA(cudaMemcpyAsync(Cs + (size_t)num_vec * n, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
