@@ -16,9 +16,14 @@
 // touch the operands, and writes C (or C^T) once, or, for a product that feeds
 // the next one, its TF32 high / FP32 low parts.
 //
-// Tiles are 128 x 128.  Warp roles (320 threads): 0-7 epilogue (two warps per
-// TMEM lane quadrant, one per half of the tile's columns), 8 TMA producer, 9
-// TMEM allocator + MMA issuer.  Bounded waits; on an abort the kernel waits (bounded) for its
+// Tiles are 128 x 128 (or 128 x 64).  The kernel is persistent: one CTA per
+// SM walks tiles blockIdx.x, blockIdx.x + gridDim.x, ..., with the stage ring
+// and the two TMEM accumulator buffers carrying on from tile to tile, so a
+// tile's epilogue overlaps the next tile's loads and MMAs (the steps with
+// short K, such as the pair-domain products, are made of many small tiles).
+// Warp roles (320 threads): 0-7 epilogue (two warps per TMEM lane quadrant,
+// one per half of the tile's columns), 8 TMA producer, 9 TMEM allocator + MMA
+// issuer.  Bounded waits; on an abort the kernel waits (bounded) for its
 // copies and MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -66,8 +71,8 @@ template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     gemm_tma_tf32x3(const __grid_constant__ CUtensorMap ahi_map, const __grid_constant__ CUtensorMap alo_map,
                     const __grid_constant__ CUtensorMap bhi_map, const __grid_constant__ CUtensorMap blo_map,
-                    const TmaProblem* __restrict__ probs, int nprob, const TmaSeg* __restrict__ segs, int kbs,
-                    int* __restrict__ status) {
+                    const TmaProblem* __restrict__ probs, int nprob, const TmaSeg* __restrict__ segs, long long ntiles,
+                    int kbs, int* __restrict__ status) {
   using T = Tile<BN>;
   constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES, B_BYTES = T::B_BYTES, ACC_COLS = T::ACC_COLS;
   extern __shared__ uint8_t smem_raw[];
@@ -80,16 +85,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
-  const long long tile = blockIdx.x;
-  int lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (probs[mid].tile_begin <= tile) lo = mid;
-    else hi = mid - 1;
-  }
-  const TmaProblem P = probs[lo];
-  const long long t = tile - P.tile_begin;
-  const int m0 = (int)(t / P.tiles_n) * BM, n0 = (int)(t % P.tiles_n) * BN;
+  // persistent: tiles blockIdx.x, blockIdx.x + gridDim.x, ...; every role walks the same tiles in the same
+  // order, the stage ring and the two TMEM accumulator buffers carry on from tile to tile
+  struct TileAt {
+    int prob, m0, n0;
+  };
+  auto tile_at = [&](long long tile) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (probs[mid].tile_begin <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    const long long t = tile - probs[lo].tile_begin;
+    return TileAt{lo, (int)(t / probs[lo].tiles_n) * BM, (int)(t % probs[lo].tiles_n) * BN};
+  };
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -125,23 +135,28 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // ---------------- TMA producer ----------------
     if (lane == 0) {
       int step = 0, last = -1;
-      for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
-        const TmaSeg S = segs[q];
-        const int nk = (int)((S.K + BK - 1) / BK);
-        for (int kk = 0; kk < nk && !aborted(); ++kk, ++step) {
-          const int s = step % STAGES;
-          if (step >= STAGES && !mbar_wait(&empty[s], ((step / STAGES) - 1) & 1)) {
-            fail(ST_TIMEOUT_EMPTY);
-            break;
+      for (long long tile = blockIdx.x; tile < ntiles && !aborted(); tile += gridDim.x) {
+        const TileAt ta = tile_at(tile);
+        const TmaProblem& P = probs[ta.prob];
+        const int m0 = ta.m0, n0 = ta.n0;
+        for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
+          const TmaSeg S = segs[q];
+          const int nk = (int)((S.K + BK - 1) / BK);
+          for (int kk = 0; kk < nk && !aborted(); ++kk, ++step) {
+            const int s = step % STAGES;
+            if (step >= STAGES && !mbar_wait(&empty[s], ((step / STAGES) - 1) & 1)) {
+              fail(ST_TIMEOUT_EMPTY);
+              break;
+            }
+            const int x = (int)S.k0 + kk * BK;
+            uint8_t* st = base + s * STAGE_BYTES;
+            mbar_expect_tx(&full[s], 2 * A_BYTES + 2 * B_BYTES);
+            tma_load_2d(st, &ahi_map, &full[s], x, (int)S.a_row + m0);
+            tma_load_2d(st + A_BYTES, &alo_map, &full[s], x, (int)S.a_row + m0);
+            tma_load_2d(st + 2 * A_BYTES, &bhi_map, &full[s], x, (int)S.b_row + n0);
+            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &blo_map, &full[s], x, (int)S.b_row + n0);
+            last = step;
           }
-          const int x = (int)S.k0 + kk * BK;
-          uint8_t* st = base + s * STAGE_BYTES;
-          mbar_expect_tx(&full[s], 2 * A_BYTES + 2 * B_BYTES);
-          tma_load_2d(st, &ahi_map, &full[s], x, (int)S.a_row + m0);
-          tma_load_2d(st + A_BYTES, &alo_map, &full[s], x, (int)S.a_row + m0);
-          tma_load_2d(st + 2 * A_BYTES, &bhi_map, &full[s], x, (int)S.b_row + n0);
-          tma_load_2d(st + 2 * A_BYTES + B_BYTES, &blo_map, &full[s], x, (int)S.b_row + n0);
-          last = step;
         }
       }
       if (aborted())
@@ -152,33 +167,36 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // ---------------- MMA issuer: blocks of at most kbs k steps, never across segments ----------------
     if (lane == 0) {
       int step = 0, blk = 0;
-      for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
-        const int nk = (int)((segs[q].K + BK - 1) / BK);
-        for (int kk = 0; kk < nk && !aborted(); ++kk, ++step) {
-          const int s = step % STAGES, buf = blk & 1;
-          const bool first = (kk % kbs) == 0;
-          if (first && blk >= 2 && !mbar_wait(&dempty[buf], ((blk / 2) - 1) & 1)) {
-            fail(ST_TIMEOUT_DE);
-            break;
-          }
-          if (!mbar_wait(&full[s], (step / STAGES) & 1)) {
-            fail(ST_TIMEOUT_FULL);
-            break;
-          }
-          asm volatile("tcgen05.fence::after_thread_sync;");
-          uint8_t* st = base + s * STAGE_BYTES;
-          const uint32_t d = tmem + (uint32_t)(buf * ACC_COLS);
+      for (long long tile = blockIdx.x; tile < ntiles && !aborted(); tile += gridDim.x) {
+        const TmaProblem& P = probs[tile_at(tile).prob];
+        for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
+          const int nk = (int)((segs[q].K + BK - 1) / BK);
+          for (int kk = 0; kk < nk && !aborted(); ++kk, ++step) {
+            const int s = step % STAGES, buf = blk & 1;
+            const bool first = (kk % kbs) == 0;
+            if (first && blk >= 2 && !mbar_wait(&dempty[buf], ((blk / 2) - 1) & 1)) {
+              fail(ST_TIMEOUT_DE);
+              break;
+            }
+            if (!mbar_wait(&full[s], (step / STAGES) & 1)) {
+              fail(ST_TIMEOUT_FULL);
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            uint8_t* st = base + s * STAGE_BYTES;
+            const uint32_t d = tmem + (uint32_t)(buf * ACC_COLS);
 #pragma unroll
-          for (int k8 = 0; k8 < BK / 8; ++k8) {
-            const uint64_t ahi = smem_desc_sw128(st + k8 * 32), alo = smem_desc_sw128(st + A_BYTES + k8 * 32);
-            const uint64_t b = smem_desc_sw128(st + 2 * A_BYTES + k8 * 32);  // B hi rows, then B lo rows
-            mma_tf32(d, ahi, b, T::kIdescBoth, (first && k8 == 0) ? 0u : 1u);
-            mma_tf32(d, alo, b, T::kIdescHi, 1u);
-          }
-          mma_commit(&empty[s]);
-          if ((kk % kbs) == kbs - 1 || kk == nk - 1) {
-            mma_commit(&dfull[buf]);
-            ++blk;
+            for (int k8 = 0; k8 < BK / 8; ++k8) {
+              const uint64_t ahi = smem_desc_sw128(st + k8 * 32), alo = smem_desc_sw128(st + A_BYTES + k8 * 32);
+              const uint64_t b = smem_desc_sw128(st + 2 * A_BYTES + k8 * 32);  // B hi rows, then B lo rows
+              mma_tf32(d, ahi, b, T::kIdescBoth, (first && k8 == 0) ? 0u : 1u);
+              mma_tf32(d, alo, b, T::kIdescHi, 1u);
+            }
+            mma_commit(&empty[s]);
+            if ((kk % kbs) == kbs - 1 || kk == nk - 1) {
+              mma_commit(&dfull[buf]);
+              ++blk;
+            }
           }
         }
       }
@@ -190,67 +208,72 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   } else {
     // ---------------- epilogue: alpha_s * block -> FP64 registers -> C ----------------
     constexpr int COLS = BN / 2;  // tile columns per epilogue warp
-    const int q = warp & 3, half = warp >> 2;
-    const long long r = m0 + q * 32 + lane;
-    const int nc0 = n0 + half * COLS;  // first output column of this warp
-    double acc[COLS];
-#pragma unroll
-    for (int j = 0; j < COLS; ++j) acc[j] = 0.0;
+    const int quad = warp & 3, half = warp >> 2;  // TMEM lane quadrant (= warp mod 4), column half
     int blk = 0;
-    for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
-      const double a = segs[q].alpha;
-      const int nk = (int)((segs[q].K + BK - 1) / BK);
-      const int nb = (nk + kbs - 1) / kbs;
-      for (int b = 0; b < nb && !aborted(); ++b, ++blk) {
-        const int buf = blk & 1;
-        if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
-          fail(ST_TIMEOUT_D);
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
+    for (long long tile = blockIdx.x; tile < ntiles && !aborted(); tile += gridDim.x) {
+      const TileAt ta = tile_at(tile);
+      const TmaProblem& P = probs[ta.prob];
+      const long long r = ta.m0 + quad * 32 + lane;
+      const int nc0 = ta.n0 + half * COLS;  // first output column of this warp
+      double acc[COLS];
 #pragma unroll
-        for (int c = 0; c < COLS / 16; ++c) {
-          uint32_t v[16];
-          const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * ACC_COLS + half * COLS + c * 16);
-          tmem_ld16(tq, v);  // hi x hi + lo x hi
-#pragma unroll
-          for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
-          tmem_ld16(tq + BN, v);  // hi x lo
-#pragma unroll
-          for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&dempty[buf]);
-      }
-    }
-    if (!aborted() && r < P.M) {
-      if (P.c_hi) {  // split output: the next product's operand, in the layout split_rows writes
-        float* hrow = P.c_hi + r * P.ldcs;
-        float* lrow = P.c_lo + r * P.ldcs;
-#pragma unroll
-        for (int j = 0; j < COLS; ++j) {
-          const long long c = nc0 + j;
-          if (c < P.N) {
-            const float h = __uint_as_float(__float_as_uint((float)acc[j]) & 0xFFFFE000u);
-            hrow[c] = h;
-            lrow[c] = (float)(acc[j] - (double)h);
+      for (int j = 0; j < COLS; ++j) acc[j] = 0.0;
+      for (long long q = P.seg_begin; q < P.seg_end && !aborted(); ++q) {
+        const double a = segs[q].alpha;
+        const int nk = (int)((segs[q].K + BK - 1) / BK);
+        const int nb = (nk + kbs - 1) / kbs;
+        for (int b = 0; b < nb && !aborted(); ++b, ++blk) {
+          const int buf = blk & 1;
+          if (!mbar_wait(&dfull[buf], (blk / 2) & 1)) {
+            fail(ST_TIMEOUT_D);
+            break;
           }
-        }
-      } else if (!P.trans_c) {
-        double* crow = P.C + r * P.ldc;
+          asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-        for (int j = 0; j < COLS; ++j) {
-          const long long c = nc0 + j;
-          if (c < P.N) crow[c] = (P.beta == 0.0 ? 0.0 : P.beta * crow[c]) + acc[j];
-        }
-      } else {  // C^T: element (r, c) goes to C[c][r]; lanes hold consecutive r (coalesced)
+          for (int c = 0; c < COLS / 16; ++c) {
+            uint32_t v[16];
+            const uint32_t tq =
+                tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * ACC_COLS + half * COLS + c * 16);
+            tmem_ld16(tq, v);  // hi x hi + lo x hi
 #pragma unroll
-        for (int j = 0; j < COLS; ++j) {
-          const long long c = nc0 + j;
-          if (c < P.N) {
-            double* y = P.C + c * P.ldc + r;
-            *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + acc[j];
+            for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
+            tmem_ld16(tq + BN, v);  // hi x lo
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[c * 16 + j] = fma(a, (double)__uint_as_float(v[j]), acc[c * 16 + j]);
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&dempty[buf]);
+        }
+      }
+      if (!aborted() && r < P.M) {
+        if (P.c_hi) {  // split output: the next product's operand, in the layout split_rows writes
+          float* hrow = P.c_hi + r * P.ldcs;
+          float* lrow = P.c_lo + r * P.ldcs;
+#pragma unroll
+          for (int j = 0; j < COLS; ++j) {
+            const long long c = nc0 + j;
+            if (c < P.N) {
+              const float h = __uint_as_float(__float_as_uint((float)acc[j]) & 0xFFFFE000u);
+              hrow[c] = h;
+              lrow[c] = (float)(acc[j] - (double)h);
+            }
+          }
+        } else if (!P.trans_c) {
+          double* crow = P.C + r * P.ldc;
+#pragma unroll
+          for (int j = 0; j < COLS; ++j) {
+            const long long c = nc0 + j;
+            if (c < P.N) crow[c] = (P.beta == 0.0 ? 0.0 : P.beta * crow[c]) + acc[j];
+          }
+        } else {  // C^T: element (r, c) goes to C[c][r]; lanes hold consecutive r (coalesced)
+#pragma unroll
+          for (int j = 0; j < COLS; ++j) {
+            const long long c = nc0 + j;
+            if (c < P.N) {
+              double* y = P.C + c * P.ldc + r;
+              *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + acc[j];
+            }
           }
         }
       }
@@ -403,14 +426,19 @@ bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int6
 }
 
 cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const TmaSeg* segs, long long ntiles,
-                   int kblock, int* status, cudaStream_t st) {
+                   int kblock, int* status, cudaStream_t st, bool persistent) {
   if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
+  // persistent: one CTA per SM (the stages take 192 KB of shared memory); otherwise a CTA per tile, which
+  // the hardware schedules dynamically (better for few tiles of very uneven length)
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)(persistent ? std::min<long long>(ntiles, sms) : ntiles);
   if (m.wide)
-    tci_gtma::gemm_tma_tf32x3<128><<<(unsigned)ntiles, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
-        m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, kblock / tci_gtma::BK, status);
+    tci_gtma::gemm_tma_tf32x3<128><<<grid, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
+        m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, ntiles, kblock / tci_gtma::BK, status);
   else
-    tci_gtma::gemm_tma_tf32x3<64><<<(unsigned)ntiles, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
-        m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, kblock / tci_gtma::BK, status);
+    tci_gtma::gemm_tma_tf32x3<64><<<grid, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(
+        m.ahi, m.alo, m.bhi, m.blo, probs, nprob, segs, ntiles, kblock / tci_gtma::BK, status);
   return cudaGetLastError();
 }
 

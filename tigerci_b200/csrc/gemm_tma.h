@@ -43,7 +43,9 @@ cudaError_t split_transposed(const double* src, int64_t nmat, int64_t rows, int6
 bool prepare(TmaMaps& m, const float* ahi, const float* alo, int64_t arows, int64_t acols, const float* bhi,
              const float* blo, int64_t brows, int64_t bcols, bool wide, std::string& err);
 // kblock: k elements per FP64 promotion block (multiple of 32)
+// persistent: at most one CTA per SM walking the tiles in a fixed order (tiles of similar length);
+// otherwise one CTA per tile
 cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const TmaSeg* segs, long long ntiles,
-                   int kblock, int* status, cudaStream_t st);
+                   int kblock, int* status, cudaStream_t st, bool persistent = true);
 
 }  // namespace tci_gtma_host

@@ -353,7 +353,8 @@ struct tci_local {
         const TmaLaunch& a = jn == jc ? m1 : m1r;
         const TmaLaunch& b = jn == jc ? m2 : m2r;
         LCUDA(tci_gtma_host::launch(map1, a.probs, a.nprob, a.segs, a.ntiles, (int)kblock, status, stream));
-        LCUDA(tci_gtma_host::launch(map2, b.probs, b.nprob, b.segs, b.ntiles, (int)kblock, status, stream));
+        // second GEMM: few tiles with K = j n_h of very different length, left to the hardware scheduler
+        LCUDA(tci_gtma_host::launch(map2, b.probs, b.nprob, b.segs, b.ntiles, (int)kblock, status, stream, false));
       }
       pack_local<<<nb, 256, 0, stream>>>(dblocks, R, Sb);
       LCUDA(cudaGetLastError());

@@ -619,9 +619,11 @@ struct DevStep {
   int tma_nprob = 0;
   long long tma_ntiles = 0;
   // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows), 3: reverse
-  // three-external (transposed V_i rows x gathered coefficient rows)
+  // three-external (transposed V_i rows x gathered coefficient rows), 4: singles-singles two-external
+  // (integral rows x gathered single-vector rows, computed transposed)
   int tma_kind = 0;
-  long long tma_aux = 0;  // kind 3: offset of the gathered coefficients U in BUF_T0
+  long long tma_aux = 0;   // kinds 3, 4: offset of the gathered coefficients in BUF_T0
+  long long tma_rows = 0;  // kind 4: rows of the gathered coefficients
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
   DGemmProblem* skinny_probs = nullptr;
   int skinny_nprob = 0;
@@ -682,8 +684,9 @@ struct tci_ctx {
   float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;
   float *v_hi = nullptr, *v_lo = nullptr, *df_hi = nullptr, *df_lo = nullptr;
   float *vt_hi = nullptr, *vt_lo = nullptr, *u3_hi = nullptr, *u3_lo = nullptr;  // reverse three-external
-  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r;
-  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false;
+  float *cg_hi = nullptr, *cg_lo = nullptr;                                        // singles-singles
+  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss;
+  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false, tma_ss_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* u2s = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -824,6 +827,39 @@ struct tci_ctx {
       if (ubase < 0 || ubase + plan.nint * plan.nD * n > plan.buf_size[BUF_T0]) return;
       d.tma_aux = ubase;
       d.tma_kind = 3;
+    } else if (s.name == "ss two-external") {
+      // Y rows (M x n) = gathered rows (M x n) X^T with X an n x n integral matrix of BUF_JK, computed as
+      // Y^T = X Cg^T: A = rows of X, B = the gathered rows.  Problems of at most SKINNY_M rows (the
+      // one-electron-like operators among them) stay on the skinny FP64 kernel.
+      TN = tci_gtma_host::tile_n(tma_wide(4));
+      long long lo = -1, hi = -1;
+      for (const auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        const DGemmProblem& dp = pr[gi++];
+        bool skinny = g.M <= SKINNY_M;
+        for (i64 k = g.seg_begin; skinny && k < g.seg_end; ++k) skinny = s.gs[(size_t)k].tA == 0 && s.gs[(size_t)k].tB == 1;
+        if (skinny) continue;
+        if (g.N != n || g.ldc != n) return;
+        TmaProblem q{dp.C, n, n, g.M, 0, 0, g.beta, (long long)ts.size(), 0, 1, nullptr, nullptr, 0};
+        for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
+          const GemmSeg& x = s.gs[(size_t)k];
+          if (x.a != BUF_T0 || x.b != BUF_JK || x.tA || !x.tB || x.lda != n || x.ldb != n || x.K != n || x.offB % n)
+            return;
+          lo = lo < 0 ? x.offA : std::min<long long>(lo, x.offA);
+          hi = std::max<long long>(hi, x.offA + g.M * n);
+          ts.push_back(TmaSeg{x.offB / n, x.offA, 0, n, x.alpha});  // b_row: offset for now, a row below
+        }
+        q.seg_end = (long long)ts.size();
+        push(q);
+      }
+      if (lo < 0) return;
+      for (auto& x : ts) {
+        if ((x.b_row - lo) % n) return;  // the gathered rows are consecutive n-vectors from lo
+        x.b_row = (x.b_row - lo) / n;
+      }
+      d.tma_aux = lo;
+      d.tma_rows = (hi - lo) / n;
+      d.tma_kind = 4;
     } else {
       return;
     }
@@ -945,6 +981,7 @@ struct tci_ctx {
         d.nprob_tc = (int)pt.size();
         d.tc_ok = flops >= 5e7 && useful >= 0.25 * issued;
         lower_tma(s, d, pr);
+        if (d.tma_probs) d.tc_ok = flops >= 5e7;  // the TMA-fed tables tile the step well
       }
     } else if (s.kind == STEP_AXPY) {
       std::vector<DAxpyTarget> t;
@@ -1048,9 +1085,10 @@ struct tci_ctx {
     sigma_count++;
   }
   // TMA-fed kernel's tile width per step kind: 128 unless the B operand has at most 64 rows per problem
-  bool tma_wide(int kind) const { return kind == 1 ? plan.n > 64 : plan.nD > 64; }
+  bool tma_wide(int kind) const { return kind == 1 ? plan.n > 64 : kind == 4 ? false : plan.nD > 64; }
   bool tma_ok(const DevStep& s) const {
-    return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready);
+    return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready) ||
+           (s.tma_kind == 4 && tma_ss_ready);
   }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
@@ -1164,23 +1202,40 @@ struct tci_ctx {
     TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
-    bool want_dd = false, want_t3 = false, want_t3r = false;
+    bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false;
+    long long ss_rows = 0;
     for (const auto& st : sigma) {
       want_dd = want_dd || (st.tma_probs && st.tma_kind == 1);
       want_t3 = want_t3 || (st.tma_probs && st.tma_kind == 2);
       want_t3r = want_t3r || (st.tma_probs && st.tma_kind == 3);
+      if (st.tma_probs && st.tma_kind == 4) {
+        want_ss = true;
+        ss_rows = std::max(ss_rows, st.tma_rows);
+      }
     }
     const i64 n = plan.n, n2 = n * n;
     std::string err;
-    if (want_dd && plan.nD > 0) {
-      const i64 ld = tci_gtma_host::pitch(n), xrows = plan.buf_size[BUF_JK] / n, drows = plan.nD * n;
+    const i64 xrows = plan.buf_size[BUF_JK] / std::max<i64>(1, n);
+    if ((want_dd && plan.nD > 0) || (want_ss && xrows > 0)) {  // the integral matrices, split once
+      const i64 ld = tci_gtma_host::pitch(n);
       alloc_f(&jk_hi, (size_t)(xrows * ld));
       alloc_f(&jk_lo, (size_t)(xrows * ld));
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, n, jk_hi, jk_lo, stream));
+    }
+    if (want_dd && plan.nD > 0) {
+      const i64 ld = tci_gtma_host::pitch(n), drows = plan.nD * n;
       alloc_f(&d_hi, (size_t)(drows * ld));
       alloc_f(&d_lo, (size_t)(drows * ld));
-      TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, n, jk_hi, jk_lo, stream));
       if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows, n, d_hi, d_lo, drows, n, tma_wide(1), err)) throw Error(TCI_ERR_CUDA, err);
       tma_dd_ready = true;
+    }
+    if (want_ss && xrows > 0 && ss_rows > 0) {
+      const i64 ld = tci_gtma_host::pitch(n);
+      alloc_f(&cg_hi, (size_t)(ss_rows * ld));
+      alloc_f(&cg_lo, (size_t)(ss_rows * ld));
+      if (!tci_gtma_host::prepare(tma_ss, jk_hi, jk_lo, xrows, n, cg_hi, cg_lo, ss_rows, n, tma_wide(4), err))
+        throw Error(TCI_ERR_CUDA, err);
+      tma_ss_ready = true;
     }
     if (want_t3 && plan.nD > 0) {
       const i64 ld = tci_gtma_host::pitch(n2), vrows = plan.nint * n;
@@ -1285,6 +1340,10 @@ struct tci_ctx {
           } else if (s.tma_kind == 2) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_t3, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          } else if (s.tma_kind == 4) {
+            TCI_CUDA(tci_gtma_host::split(buf[BUF_T0] + s.tma_aux, s.tma_rows, n, n, cg_hi, cg_lo, stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_ss, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
           } else {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_T0] + s.tma_aux, plan.nint * plan.nD, n, n, u3_hi, u3_lo, stream));
@@ -1419,8 +1478,15 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                               2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * (double)(P.nint * P.n + P.nD) +
                               // transposed V_i and the gathered coefficients of the reverse three-external step
                               2.0 * (double)tci_gtma_host::pitch(P.n) * (double)(P.nint * P.n * P.n + P.nint * P.nD));
-    pk = std::max(pk, res + f32);  // FP64 and FP32 operators coexist until the FP64 copy is released
-    res += f32 - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
+    // gathered single-vector rows of the singles-singles step (problems above the skinny size)
+    double ss_rows = 0;
+    for (const auto& st : P.sigma_steps)
+      if (st.name == "ss two-external")
+        for (const auto& g : st.gp)
+          if (g.M > SKINNY_M) ss_rows += (double)g.M;
+    const double f32_all = f32 + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows;
+    pk = std::max(pk, res + f32_all);  // FP64 and FP32 operators coexist until the FP64 copy is released
+    res += f32_all - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
   *peak = std::max(pk, res);
   *resident = res;
