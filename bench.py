@@ -55,9 +55,11 @@ TOL_RESIDUAL, TOL_ENERGY = 1e-6, 1e-8
 # GPU solve's iteration count at 1 root); converts the oracle's sigma time
 # into a solve time for the CPU arm
 SIGMA_BUILDS_PER_SOLVE = 33
-# ncu DRAM bytes (read + write) of one launch over its algorithmic bytes (the W operators), measured at 120
-# virtuals: FP64 split-K all-external 845.1 MB / 829.5 MB; tcgen05 all-external 219.2 MB / 211.0 MB
-TRAFFIC_RATIO = {"fp64": 845.142 / 829.498, "tf32x3": 219.224 / 210.954}
+# ncu DRAM bytes (read + write) of one launch over its algorithmic bytes (the W operators): FP64 split-K
+# all-external at 120 virtuals 845.1 MB / 829.5 MB; tcgen05 all-external at 140 virtuals 809.9 MB / 773.4 MB
+TRAFFIC_RATIO = {"fp64": 845.142 / 829.498, "tf32x3": (800.509 + 9.346) / 773.381}
+TRAFFIC_SOURCE = {"fp64": "ncu dram read+write ratio at 120 virtuals x full-size bytes",
+                  "tf32x3": "ncu dram read+write ratio at 140 virtuals x full-size bytes"}
 
 
 def deck_and_operator(molecular=False):
@@ -422,7 +424,7 @@ def main():
              "roofline": {"kernel": kernel, "bound": "hbm", "achieved": bytes_ / t_dom / 1e9, "peak": hbm,
                           "unit": "GB/s", "frac": bytes_ / t_dom / 1e9 / hbm,
                           "traffic": TRAFFIC_RATIO[f] * bytes_, "algorithmic_bytes": bytes_,
-                          "traffic_source": "ncu dram read+write ratio at 120 virtuals x full-size bytes",
+                          "traffic_source": TRAFFIC_SOURCE[f],
                           "peak_kind": peak_kind, "ms": 1e3 * t_dom},
              "launches_per_build": m["launches"] / args.sigma_builds,
              "step_ms": {k: round(v, 4) for k, v in sorted(m["prof"].items(), key=lambda kv: -kv[1])[:12]},
