@@ -117,10 +117,14 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
  * one-external GEMM steps from their FP64 operands.  options[2] selects those
  * other GEMM steps: 0 by size (default), 1 all of them, 2 none.  The coupling-
  * coefficient products, same-head one-electron-like operators, gathers,
- * scatters and reductions stay FP64.  options[3] = 1 (default) keeps the FP64
- * W as well and reports every tci_davidson root as the Rayleigh quotient of
- * its Ritz vector with one plain-FP64 sigma build (error second order in the
- * eigenvector error of the mixed products); 0 releases the FP64 W. */
+ * scatters and reductions stay FP64.  options[3] picks how tci_davidson
+ * reports the roots of the mixed form: 2 (default) as the Rayleigh quotient of
+ * each Ritz vector with one sigma build in which every term is FP64 but the
+ * all-external one, which stays on its tensor-core kernel (the FP64 W is
+ * released after the diagonal is built); 1 the same with a plain-FP64 sigma
+ * build (the FP64 W stays resident); 0 the mixed Ritz values.  The finished
+ * root's error is second order in the eigenvector error of the mixed products
+ * plus, for 2, the first-order error of the all-external term alone. */
 #define TCI_PRECISION_FP64 0
 #define TCI_PRECISION_TF32X3 1
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,

@@ -129,14 +129,16 @@ def test_mixed_davidson_relative_bound_large_scale(need_gpu):
     assert np.abs(ea - eb).max() < 1e-6 * s2 + 1e-8
 
 
-def test_mixed_roots_with_fp64_finish_match_fp64_closely(need_gpu):
+@pytest.mark.parametrize("finish", ["no_allext", "full"])
+def test_mixed_roots_with_fp64_finish_match_fp64_closely(finish, need_gpu):
     """The mixed form's roots, finished as FP64 Rayleigh quotients of its Ritz
-    vectors, agree with the plain-FP64 roots to the FP64 tolerance (1e-8 Eh);
-    without the finish they carry the mixed products' first-order error."""
+    vectors (every term FP64, or every term but the all-external one), agree
+    with the plain-FP64 roots to the FP64 tolerance (1e-8 Eh); without the
+    finish they carry the mixed products' first-order error."""
     deck = T.Deck(16 + 60, 8, 8, 16, 1, ["2" * 8 + "0" * 8])
     h, L = synthetic_operator(76, 200, seed=1234, scale=0.02, diag_range=(-2.0, 1.0), offdiag_sigma=0.02)
     a = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="fp64")
-    b = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="tf32x3", tc_gemms="all")
+    b = T.SigmaBuilder(deck, T.Operator(h, L), device=0, precision="tf32x3", tc_gemms="all", fp64_finish=finish)
     ea, _, _ = a.davidson(2, 1e-7, 1e-11)
     eb, _, _ = b.davidson(2, 1e-7, 1e-11)
     b.check()

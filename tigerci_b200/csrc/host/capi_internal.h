@@ -13,11 +13,12 @@ void build_space_from_c(const tci_deck* d, CsfSpace& sp);
 void operator_from_c(const tci_operator* op, const CsfSpace& sp, Operator& out);
 // Device half of tci_sigma_init: a context from a host-built space and plan
 // (chol: the host Cholesky vectors the plan was built for).
-// refine: in the mixed form, keep the FP64 W and finish every root as an FP64 Rayleigh quotient.
+// refine (mixed form): finish every root as an FP64 Rayleigh quotient, 1 with a plain-FP64 sigma build
+// (keeps the FP64 W), 2 with every term FP64 but the all-external one (default), 0 not at all.
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
-                  tci_ctx** out, int64_t refine = 1);
+                  tci_ctx** out, int64_t refine = 2);
 // Selects the GEMM steps that run on the tensor cores in the mixed form (tci_sigma_init_ex options[2]).
 void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode);
 // Device bytes of such a context: peak during set-up and held afterwards.
-void ctx_device_bytes(const Plan& plan, int64_t precision, double* peak, double* resident, int64_t refine = 1);
+void ctx_device_bytes(const Plan& plan, int64_t precision, double* peak, double* resident, int64_t refine = 2);
 }  // namespace tci

@@ -679,7 +679,10 @@ struct tci_ctx {
   int64_t precision = 0;                // 0 plain FP64; 1 all-external on tcgen05 (3xTF32, FP64 promotion)
   int64_t tc_kblock = 128;              // k elements per FP64 promotion block of the tensor-core product
   int64_t tc_mode = 0;                  // precision 1: other GEMM steps on the tensor cores by size (0), all (1), none (2)
-  int64_t refine = 1;                   // precision 1: roots finished as FP64 Rayleigh quotients (keeps the FP64 W)
+  // precision 1: roots finished as FP64 Rayleigh quotients: 1 with a plain-FP64 sigma build (keeps the FP64 W),
+  // 2 with every term FP64 but the all-external one, which stays on its tensor-core kernel (no FP64 W kept)
+  int64_t refine = 2;
+  bool allext_tc_in_fp64 = false;       // set during a refine-2 finish build
   // split operands of the TMA-fed steps: integrals and V_i once, the pair matrices every build
   float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;
   float *v_hi = nullptr, *v_lo = nullptr, *df_hi = nullptr, *df_lo = nullptr;
@@ -1098,8 +1101,9 @@ struct tci_ctx {
   long long sigma_launches() const {
     long long k = 0;
     for (const auto& s : sigma) {
-      if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
-      if (precision == 1 && s.kind == STEP_GEMM && s.name == "all-external") {
+      const bool tc_allext = precision == 1 || allext_tc_in_fp64;
+      if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
+      if (tc_allext && s.kind == STEP_GEMM && s.name == "all-external") {
         k += (has_sing() ? 1 : 0) + (has_trip() ? 1 : 0) + ((has_sing() || has_trip()) ? 1 : 0);
         continue;
       }
@@ -1269,7 +1273,7 @@ struct tci_ctx {
     if (plan.n_trip > 0 && nm > 0 &&
         !tci_tc_host::prepare(tc_trip, w32m, nm, u2t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
-    if (!refine) {  // the FP64 W is only needed for the FP64 finish of the roots
+    if (refine != 1) {  // the FP64 W is only needed for the plain-FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
       TCI_CUDA(cudaFree(buf[BUF_W]));
       bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
@@ -1281,19 +1285,23 @@ struct tci_ctx {
   // one by one, outside the context's graph): d_s = H d_c.
   void sigma_of_fp64(const double* d_c, double* d_s) {
     const i64 n = plan.total_csfs;
-    if (!buf[BUF_W]) throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
+    const bool tc_allext = refine == 2 && precision == 1;
+    if (!buf[BUF_W] && !tc_allext) throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
     TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     const int64_t saved = precision;
     precision = 0;
+    allext_tc_in_fp64 = tc_allext;
     try {
       record_steps(false, false);
     } catch (...) {
       precision = saved;
+      allext_tc_in_fp64 = false;
       throw;
     }
     launch_count += sigma_launches();
     precision = saved;
+    allext_tc_in_fp64 = false;
     TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   }
 
@@ -1320,10 +1328,11 @@ struct tci_ctx {
 
   void run_step(const DevStep& s) {
     // the tensor-core form writes the all-external products directly
-    if (precision == 1 && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
+    const bool tc_allext = precision == 1 || allext_tc_in_fp64;
+    if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
     switch (s.kind) {
       case STEP_GEMM:
-        if (precision == 1 && s.name == "all-external") {
+        if (tc_allext && s.name == "all-external") {
           run_allext_tc();
           break;
         }
@@ -1408,7 +1417,7 @@ cudaError_t launch_gemm_f64(int cfg, const DGemmProblem* probs, int nprob, const
 extern "C" {
 
 static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t device, int64_t precision, int64_t kblock,
-                     tci_ctx** out, int64_t refine = 1);
+                     tci_ctx** out, int64_t refine = 2);
 
 int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device, tci_ctx** out) {
   return init_impl(deck, op, device, 0, 128, out);
@@ -1416,12 +1425,12 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
 
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,
                       int64_t n_options, tci_ctx** out) {
-  int64_t precision = 0, kblock = 128, tc_mode = 0, refine = 1;
+  int64_t precision = 0, kblock = 128, tc_mode = 0, refine = 2;
   if (options && n_options > 0) precision = options[0];
   if (options && n_options > 1 && options[1] > 0) kblock = options[1];
   if (options && n_options > 2) tc_mode = options[2];
   if (options && n_options > 3) refine = options[3];
-  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2 || refine < 0 || refine > 1) {
+  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2 || refine < 0 || refine > 2) {
     set_error("unknown precision mode, tensor-core GEMM selection or finish");
     return TCI_ERR_ARG;
   }
@@ -1486,7 +1495,7 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
           if (g.M > SKINNY_M) ss_rows += (double)g.M;
     const double f32_all = f32 + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows;
     pk = std::max(pk, res + f32_all);  // FP64 and FP32 operators coexist until the FP64 copy is released
-    res += f32_all - (refine ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
+    res += f32_all - (refine == 1 ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
   *peak = std::max(pk, res);
   *resident = res;
@@ -1991,7 +2000,8 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
       ctx->check_tc_status();
       if (ctx->precision == 1 && ctx->refine) {
         // FP64 finish: each root is reported as the Rayleigh quotient of its Ritz vector with the plain-FP64
-        // sigma.  Its error is second order in the eigenvector error the mixed products leave.
+        // sigma (refine 2: all terms FP64 but the all-external one).  Its error is second order in the
+        // eigenvector error the mixed products leave.
         const int m = (int)w.size();
         for (int q = 0; q < nroots; ++q) {
           std::vector<double> cb(m);
