@@ -43,7 +43,10 @@ constexpr int BM = 128, BK = 32;
 constexpr int NTHREADS = 320;
 constexpr int EPI_WARPS = 8;  // warps 0-3: first half of the tile's columns, 4-7: second half (TMEM quadrant = warp mod 4)
 constexpr int A_BYTES = BM * BK * 4;
-constexpr int SMEM_BYTES = 192 * 1024 + 1024 + 256;  // both tile widths use 192 KB of stages
+// Output staging: per epilogue warp 32 rows x 33 floats (or 32 x 16 doubles), so that rows leave the
+// epilogue as coalesced 128-byte segments instead of one scattered word per row.
+constexpr int STAGE_OUT_FLOATS = 32 * 33;
+constexpr int SMEM_BYTES = 192 * 1024 + 1024 + 256 + 8 * STAGE_OUT_FLOATS * 4;  // 192 KB of stages
 // Tile width BN = 128 (wide operands) or 64 (B with few rows).  B's high rows are followed by its low
 // rows in a stage, so A_hi x [B_hi; B_lo] is one MMA of N = 2 BN and A_lo x B_hi a second one: two
 // instructions per k slice (an MMA costs about the same time whatever its N, so wide tiles and few
@@ -84,6 +87,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint64_t* mma_done = dempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  float* stage_out = reinterpret_cast<float*>(base + STAGES * STAGE_BYTES + 256);  // EPI_WARPS x STAGE_OUT_FLOATS
 
   // persistent: tiles blockIdx.x, blockIdx.x + gridDim.x, ...; every role walks the same tiles in the same
   // order, the stage ring and the two TMEM accumulator buffers carry on from tile to tile
@@ -246,34 +250,58 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (lane == 0) mbar_arrive(&dempty[buf]);
         }
       }
-      if (!aborted() && r < P.M) {
-        if (P.c_hi) {  // split output: the next product's operand, in the layout split_rows writes
-          float* hrow = P.c_hi + r * P.ldcs;
-          float* lrow = P.c_lo + r * P.ldcs;
+      // warp-uniform abort test: the staged stores below are warp-wide
+      const bool stop = __any_sync(0xffffffffu, aborted());
+      const long long r0w = ta.m0 + quad * 32;  // the warp's first row
+      float* sb = stage_out + warp * STAGE_OUT_FLOATS;
+      if (!stop && P.c_hi) {
+        // split output (the next product's operand, in the layout split_rows writes): 32 x 32 blocks through
+        // shared memory, high parts then low parts, each row written as one 128-byte segment
 #pragma unroll
-          for (int j = 0; j < COLS; ++j) {
-            const long long c = nc0 + j;
-            if (c < P.N) {
-              const float h = __uint_as_float(__float_as_uint((float)acc[j]) & 0xFFFFE000u);
-              hrow[c] = h;
-              lrow[c] = (float)(acc[j] - (double)h);
+        for (int c0 = 0; c0 < COLS; c0 += 32)
+#pragma unroll 1
+          for (int part = 0; part < 2; ++part) {
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj) {
+              const double x = acc[c0 + jj];
+              const float h = __uint_as_float(__float_as_uint((float)x) & 0xFFFFE000u);
+              sb[lane * 33 + jj] = part == 0 ? h : (float)(x - (double)h);
+            }
+            __syncwarp();
+            float* out = part == 0 ? P.c_hi : P.c_lo;
+            const long long col = nc0 + c0 + lane;
+            for (int i = 0; i < 32; ++i) {
+              const long long row = r0w + i;
+              if (row < P.M && col < P.N) out[row * P.ldcs + col] = sb[i * 33 + lane];
+            }
+            __syncwarp();
+          }
+      } else if (!stop && !P.trans_c) {
+        // FP64 rows: 32 x 16 blocks through shared memory (XOR-swizzled columns), two rows per store
+        double* db = reinterpret_cast<double*>(sb);
+#pragma unroll
+        for (int c0 = 0; c0 < COLS; c0 += 16) {
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) db[lane * 16 + (jj ^ (lane & 15))] = acc[c0 + jj];
+          __syncwarp();
+          for (int ii = 0; ii < 16; ++ii) {
+            const int i = 2 * ii + (lane >> 4), j = lane & 15;
+            const double v = db[i * 16 + (j ^ (i & 15))];
+            const long long row = r0w + i, col = nc0 + c0 + j;
+            if (row < P.M && col < P.N) {
+              double* y = P.C + row * P.ldc + col;
+              *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + v;
             }
           }
-        } else if (!P.trans_c) {
-          double* crow = P.C + r * P.ldc;
+          __syncwarp();
+        }
+      } else if (!stop && r < P.M) {  // C^T: element (r, c) goes to C[c][r]; lanes hold consecutive r (coalesced)
 #pragma unroll
-          for (int j = 0; j < COLS; ++j) {
-            const long long c = nc0 + j;
-            if (c < P.N) crow[c] = (P.beta == 0.0 ? 0.0 : P.beta * crow[c]) + acc[j];
-          }
-        } else {  // C^T: element (r, c) goes to C[c][r]; lanes hold consecutive r (coalesced)
-#pragma unroll
-          for (int j = 0; j < COLS; ++j) {
-            const long long c = nc0 + j;
-            if (c < P.N) {
-              double* y = P.C + c * P.ldc + r;
-              *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + acc[j];
-            }
+        for (int j = 0; j < COLS; ++j) {
+          const long long c = nc0 + j;
+          if (c < P.N) {
+            double* y = P.C + c * P.ldc + r;
+            *y = (P.beta == 0.0 ? 0.0 : P.beta * *y) + acc[j];
           }
         }
       }
