@@ -227,7 +227,7 @@ struct tci_local {
   // mixed form: split arrays (row pitch ldp) and the TMA-fed tables
   long long ldp = 0, rows_l = 0, rows_d = 0, rows_t = 0;
   float *lc_hi = nullptr, *lc_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr, *t_hi = nullptr, *t_lo = nullptr;
-  tci_gtma_host::TmaMaps map1, map2;  // T = Lc D ; R += 1/2 T Lc
+  tci_gtma_host::TmaMaps map1, map1n, map2;  // T = Lc D (128- or 64-wide tiles) ; R += 1/2 T Lc
   TmaLaunch m1, m2, m1r, m2r;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -299,21 +299,22 @@ struct tci_local {
     finish(v2, cfg_second, b);
   }
 
-  // mixed form: TMA-fed tables for chunks of j vectors
-  void make_tma(int64_t j, TmaLaunch& a, TmaLaunch& b) {
-    const long long TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n(map1.wide);
+  // mixed form: TMA-fed tables for chunks of j vectors; narrow1: the first GEMM on 64-wide tiles
+  void make_tma(int64_t j, bool narrow1, TmaLaunch& a, TmaLaunch& b) {
+    const long long TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n(map2.wide);
+    const long long TN1 = tci_gtma_host::tile_n(narrow1 ? map1n.wide : map1.wide);
     std::vector<TmaProblem> p1, p2;
     std::vector<TmaSeg> s1, s2;
     long long t1 = 0, t2 = 0;
     for (const auto& B : blocks) {
       const DLocHead& H = heads[B.head];
-      const long long n = B.n, tn = (n + TN - 1) / TN;
+      const long long n = B.n, tn = (n + TN - 1) / TN, tn1 = (n + TN1 - 1) / TN1;
       // T_hk (j n x n) = Lc_h D_hk, written split; D_hk enters as the K-major operand through D^T = p D
-      TmaProblem q1{nullptr, 0, j * n, n, tn, t1, 0.0, (long long)s1.size(), 0, 0,
+      TmaProblem q1{nullptr, 0, j * n, n, tn1, t1, 0.0, (long long)s1.size(), 0, 0,
                     t_hi + B.trow * ldp, t_lo + B.trow * ldp, ldp};
       s1.push_back(TmaSeg{H.lrow, B.drow, 0, n, B.p});
       q1.seg_end = (long long)s1.size();
-      t1 += ((j * n + TM - 1) / TM) * tn;
+      t1 += ((j * n + TM - 1) / TM) * tn1;
       p1.push_back(q1);
       // R_hk += 1/2 sum_J T_hkJ L^J_h (L^J_h symmetric: its rows are the K-major operand)
       TmaProblem q2{R + B.d_off, n, n, n, tn, t2, 1.0, (long long)s2.size(), 0, 0, nullptr, nullptr, 0};
@@ -352,7 +353,8 @@ struct tci_local {
         LCUDA(cudaGetLastError());
         const TmaLaunch& a = jn == jc ? m1 : m1r;
         const TmaLaunch& b = jn == jc ? m2 : m2r;
-        LCUDA(tci_gtma_host::launch(map1, a.probs, a.nprob, a.segs, a.ntiles, (int)kblock, status, stream));
+        LCUDA(tci_gtma_host::launch(cfg2 == 1 ? map1n : map1, a.probs, a.nprob, a.segs, a.ntiles, (int)kblock, status,
+                                    stream));
         // second GEMM: few tiles with K = j n_h of very different length, left to the hardware scheduler
         LCUDA(tci_gtma_host::launch(map2, b.probs, b.nprob, b.segs, b.ntiles, (int)kblock, status, stream, false));
       }
@@ -382,8 +384,8 @@ struct tci_local {
     cfg2 = cfg;
     const int64_t rem = nchol % jc;
     if (precision == 1) {
-      make_tma(jc, m1, m2);
-      if (rem) make_tma(rem, m1r, m2r);
+      make_tma(jc, cfg2 == 1, m1, m2);
+      if (rem) make_tma(rem, cfg2 == 1, m1r, m2r);
     } else {
       make_gemms(jc, cfg2, g1, g2);
       if (rem) make_gemms(rem, cfg2, g1r, g2r);
@@ -536,6 +538,8 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
       const bool wide = nmax > 64;  // tile width: the B operands have n_h rows per problem
       if (!tci_gtma_host::prepare(L->map1, L->lc_hi, L->lc_lo, L->rows_l, nmax, L->d_hi, L->d_lo, L->rows_d, nmax, wide,
                                   err) ||
+          !tci_gtma_host::prepare(L->map1n, L->lc_hi, L->lc_lo, L->rows_l, nmax, L->d_hi, L->d_lo, L->rows_d, nmax,
+                                  false, err) ||
           !tci_gtma_host::prepare(L->map2, L->t_hi, L->t_lo, L->rows_t, nmax, L->lc_hi, L->lc_lo, L->rows_l, nmax, wide,
                                   err))
         throw Error(TCI_ERR_CUDA, err);
@@ -555,11 +559,11 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
     L->owned.push_back(L->status);
     LCUDA(cudaMemsetAsync(L->status, 0, sizeof(int), L->stream));
 
-    // autotuner: chunk size (largest, half) x FP64 tile shape of the second GEMM; one timed run each
+    // autotuner: chunk size (largest, half, quarter) x FP64 tile shape of the second GEMM (mixed form: tile
+    // width of the first GEMM, 128 or 64); one timed run each
     std::vector<std::pair<int64_t, int>> cand;
-    for (int64_t j : {L->jmax, std::max<int64_t>(1, L->jmax / 2)})
+    for (int64_t j : {L->jmax, std::max<int64_t>(1, L->jmax / 2), std::max<int64_t>(1, L->jmax / 4)})
       for (int cfg : {0, 1}) {
-        if (L->precision == 1 && cfg == 1) continue;  // the tensor-core kernel has one tile shape
         if (std::find(cand.begin(), cand.end(), std::make_pair(j, cfg)) == cand.end()) cand.push_back({j, cfg});
       }
     if (!tune) cand.resize(1);
