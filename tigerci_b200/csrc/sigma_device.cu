@@ -1187,6 +1187,46 @@ struct tci_ctx {
     TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream));
   }
 
+  // X (M x M, FP64) = A A^T with A = M rows of K values in BUF_T0, on the TMA-fed 3xTF32 kernel (set-up).
+  void exchange_product_tc(const GemmProblem& g, const GemmSeg& x, int64_t kblock) {
+    const i64 M = g.M, K = x.K, ld = tci_gtma_host::pitch(K);
+    check_range(BUF_T0, x.offA, (M - 1) * x.lda + K);
+    check_range(g.c, g.offC, (M - 1) * g.ldc + M);
+    float *ah = nullptr, *al = nullptr;
+    int* st = nullptr;
+    auto release = [&]() {
+      cudaStreamSynchronize(stream);
+      std::lock_guard<std::mutex> lk(g_capture_free_mu);
+      for (void* p : {(void*)ah, (void*)al, (void*)st})
+        if (p) cudaFree(p);
+    };
+    try {
+      TCI_CUDA(cudaMalloc(&ah, sizeof(float) * (size_t)(M * ld)));
+      TCI_CUDA(cudaMalloc(&al, sizeof(float) * (size_t)(M * ld)));
+      TCI_CUDA(cudaMalloc(&st, sizeof(int)));
+      TCI_CUDA(cudaMemsetAsync(st, 0, sizeof(int), stream));
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_T0] + x.offA, M, K, x.lda, ah, al, stream));
+      tci_gtma_host::TmaMaps m;
+      std::string err;
+      if (!tci_gtma_host::prepare(m, ah, al, M, K, ah, al, M, K, true, err)) throw Error(TCI_ERR_CUDA, err);
+      const i64 TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n(true);
+      std::vector<TmaProblem> q{TmaProblem{ptr(g.c, g.offC), g.ldc, M, M, (M + TN - 1) / TN, 0, 0.0, 0, 1, 0, nullptr,
+                                           nullptr, 0}};
+      std::vector<TmaSeg> sg{TmaSeg{0, 0, 0, K, x.alpha}};
+      TmaProblem* dq = upload(q, owned, stream);
+      TmaSeg* ds = upload(sg, owned, stream);
+      TCI_CUDA(tci_gtma_host::launch(m, dq, 1, ds, ((M + TM - 1) / TM) * q[0].tiles_n, (int)kblock, st, stream));
+      int h = 0;
+      TCI_CUDA(cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      TCI_CUDA(cudaStreamSynchronize(stream));
+      if (h != 0) throw Error(TCI_ERR_TIMEOUT, "tensor-core exchange product: a bounded wait gave up");
+    } catch (...) {
+      release();
+      throw;
+    }
+    release();
+  }
+
   // Moves W+/W- to FP32 for the tensor-core product and releases the FP64 copy.
   void setup_precision() {
     if (precision != 1) return;
@@ -1556,9 +1596,37 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     }
     ctx->dheads = upload(dh, ctx->owned, ctx->stream);
     ctx->dk_head = upload(dkh, ctx->owned, ctx->stream);
-    for (auto& s : P.init_steps) ctx->init.push_back(ctx->lower(s));
+    // Mixed form without the plain-FP64 finish: the exchange product X = Lpk Lpk^T of the all-external
+    // operators (the largest set-up GEMM, 2 npk^2 N flops) runs on the TMA-fed tensor-core kernel; its
+    // 3xTF32 error is of the order of W's own FP32 rounding in that form.  The other banks stay FP64.
+    const bool x_tc = precision == 1 && refine != 1;
+    GemmProblem xg{};
+    GemmSeg xs{};
+    bool have_x = false;
+    size_t banks = (size_t)-1;
+    for (auto& s : P.init_steps) {
+      if (x_tc && s.kind == STEP_GEMM && s.name == "integral banks") {
+        Step s2 = s;
+        for (size_t g = 0; g < s2.gp.size(); ++g)
+          if (s2.gp[g].c == BUF_X && s2.gp[g].seg_end - s2.gp[g].seg_begin == 1) {
+            xg = s2.gp[g];
+            xs = s2.gs[(size_t)xg.seg_begin];
+            s2.gp.erase(s2.gp.begin() + (long)g);
+            have_x = xs.a == BUF_T0 && xs.b == BUF_T0 && xs.offA == xs.offB && !xs.tA && xs.tB && xg.M == xg.N;
+            if (!have_x) s2 = s;  // not the expected shape: leave it on the FP64 kernel
+            break;
+          }
+        banks = ctx->init.size();
+        ctx->init.push_back(ctx->lower(s2));
+        continue;
+      }
+      ctx->init.push_back(ctx->lower(s));
+    }
     for (auto& s : P.sigma_steps) ctx->sigma.push_back(ctx->lower(s));
-    for (auto& s : ctx->init) ctx->run(s);
+    for (size_t i = 0; i < ctx->init.size(); ++i) {
+      ctx->run(ctx->init[i]);
+      if (i == banks && have_x) ctx->exchange_product_tc(xg, xs, kblock);
+    }
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     // init-only buffers
     for (int b : {BUF_X, BUF_L, BUF_LE, BUF_LI}) {
