@@ -266,33 +266,54 @@ __global__ void __launch_bounds__(256, 2) gemm_tiled_f64(const DGemmProblem* __r
 // Skinny grouped GEMM (M <= SKINNY_M, B given as N x K): one warp per output
 // column n of a problem computes C[m][n] for every row m as dot products over
 // the segments (lanes along k, fixed-order warp reductions).  Covers the
-// one-row products that would fill 1/64 of a tile of the tiled kernel.
+// one-row products that would fill 1/64 of a tile of the tiled kernel.  Warp
+// numbers are laid out so that the 8 warps of a block share one problem: the
+// block looks its problem up once, and its warps read the same A rows (L1).
 constexpr int SKINNY_M = 8;
 __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __restrict__ probs, int nprob,
                                                        const DGemmSeg* __restrict__ segs, long long nwarps) {
-  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nwarps) return;
-  int lo = 0, hi = nprob - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (probs[mid].tile_begin <= w) lo = mid;
-    else hi = mid - 1;
+  __shared__ int prob_of_block;
+  const long long w0 = (long long)blockIdx.x * 8;  // first warp of the block
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (probs[mid].tile_begin <= w0) lo = mid;
+      else hi = mid - 1;
+    }
+    prob_of_block = lo;
   }
-  const DGemmProblem P = probs[lo];
+  __syncthreads();
+  const long long w = w0 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const DGemmProblem P = probs[prob_of_block];
   const long long n = w - P.tile_begin;
+  if (w >= nwarps || n >= P.N) return;
   double acc[SKINNY_M];
 #pragma unroll
   for (int m = 0; m < SKINNY_M; ++m) acc[m] = 0.0;
   for (long long q = P.seg_begin; q < P.seg_end; ++q) {
     const DGemmSeg S = segs[q];
     const double* b = S.B + n * S.ldb;
+    // 16-byte loads when both rows start on 16 bytes and K is even
+    const bool vec = ((reinterpret_cast<uintptr_t>(S.A) | reinterpret_cast<uintptr_t>(b)) & 15) == 0 &&
+                     ((S.lda | S.K) & 1) == 0;
 #pragma unroll
     for (int m = 0; m < SKINNY_M; ++m) {
       if (m >= P.M) break;
       const double* a = S.A + m * S.lda;
       double d = 0.0;
-      for (long long k = lane; k < S.K; k += 32) d = fma(a[k], b[k], d);
+      if (vec) {
+        const double2* a2 = reinterpret_cast<const double2*>(a);
+        const double2* b2 = reinterpret_cast<const double2*>(b);
+        for (long long k = lane; k < S.K / 2; k += 32) {
+          const double2 x = __ldg(a2 + k), y = __ldg(b2 + k);
+          d = fma(x.x, y.x, d);
+          d = fma(x.y, y.y, d);
+        }
+      } else {
+        for (long long k = lane; k < S.K; k += 32) d = fma(__ldg(a + k), __ldg(b + k), d);
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
       acc[m] = fma(S.alpha, d, acc[m]);
@@ -923,8 +944,8 @@ struct tci_ctx {
           for (long long q = g.seg_begin; skinny && q < g.seg_end; ++q) skinny = sg[(size_t)q].tA == 0 && sg[(size_t)q].tB == 1;
           if (skinny) {
             DGemmProblem x = g;
-            x.tile_begin = wk;  // first warp (one per output column)
-            wk += g.N;
+            x.tile_begin = wk;  // first warp (one per output column); a block of 8 warps stays in one problem
+            wk += (g.N + 7) / 8 * 8;
             sk.push_back(x);
           } else {
             DGemmProblem x = g;
