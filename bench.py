@@ -232,7 +232,7 @@ def serve_measure(n_requests, slots, device, serial_every=4, planners=4):
             "stand_in": "synthetic MO operators with the H_n chains' orbital counts (no integral engine)"}
 
 
-def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3):
+def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3, nchol=2400, forms=("tf32x3", "fp64")):
     """All-external term over uneven pair domains: n_pairs internal pairs (35
     doubly occupied internal orbitals), domains of 20..180 of 400 external
     orbitals (seed 99), Cholesky rank 2400 as in the kernel-scale operator.
@@ -242,7 +242,7 @@ def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3):
     from tigerci_b200 import local
     from tigerci_b200.synthetic import synthetic_operator
 
-    n_int, n_virt, nchol = 35, 400, 2400
+    n_int, n_virt = 35, 400
     heads, dom, total = local.pair_domain_problem(n_pairs, n_int, n_virt, 20, 180, seed=99)
     _, L = synthetic_operator(n_int + n_virt, nchol, seed=1234)
     rng = np.random.default_rng(7)
@@ -252,7 +252,7 @@ def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3):
                        f"Cholesky rank {nchol}; CI length {total}",
            "heads": int(len(heads))}
     sig = {}
-    for form, n_steps in (("tf32x3", steps), ("fp64", 1)):
+    for form, n_steps in [(f, steps if f == "tf32x3" else 1) for f in forms]:
         t0 = time.perf_counter()
         op = local.LocalAllExternal(n_int, n_virt, L, heads, dom, total, device=device, precision=form)
         init_s = time.perf_counter() - t0
@@ -281,8 +281,9 @@ def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3):
                                   "unit": "TFLOP/s", "frac": (st["flops"] / t / 1e12 / peak) if peak else None,
                                   "peak_kind": "3xTF32: measured dense BF16 / 2 / 3" if peak else None}}
         op.close()
-    a, b = sig["tf32x3"], sig["fp64"]
-    out["mixed_rel_err_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    if "tf32x3" in sig and "fp64" in sig:
+        a, b = sig["tf32x3"], sig["fp64"]
+        out["mixed_rel_err_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     return out
 
 
@@ -301,6 +302,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=96, help="requests of the serving stream to replay")
     ap.add_argument("--serve-slots", type=int, default=6)
     ap.add_argument("--serve-planners", type=int, default=4, help="host threads building plans for the server")
+    ap.add_argument("--local-nchol", type=int, default=2400, help="Cholesky rank of the pair-domain workload")
+    ap.add_argument("--local-forms", default="tf32x3,fp64", help="forms of the pair-domain measurement")
     ap.add_argument("--serve-only", action="store_true", help="only the serving measurement")
     ap.add_argument("--local-pairs", type=int, default=600, help="pairs of the pair-domain workload (0: skip)")
     ap.add_argument("--local-only", action="store_true", help="only the pair-domain measurement")
@@ -346,7 +349,8 @@ def main():
         return
     if args.local_only:
         if rank == 0:
-            print(json.dumps({"local_pairs": local_measure(args.local_pairs, local, hbm, bf16)}), flush=True)
+            print(json.dumps({"local_pairs": local_measure(args.local_pairs, local, hbm, bf16, nchol=args.local_nchol,
+                                                    forms=tuple(f for f in args.local_forms.split(",") if f))}), flush=True)
         return
 
     # ---- sigma builds on the operator exactly as the kernel-scale configuration specifies
@@ -561,7 +565,8 @@ def main():
             line["serving"] = {"error": str(exc)[:300]}
     if args.local_pairs > 0:
         try:
-            line["local_pairs"] = local_measure(args.local_pairs, local, hbm, bf16)
+            line["local_pairs"] = local_measure(args.local_pairs, local, hbm, bf16, nchol=args.local_nchol,
+                                                    forms=tuple(f for f in args.local_forms.split(",") if f))
         except Exception as exc:
             line["local_pairs"] = {"error": str(exc)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
