@@ -106,6 +106,8 @@ struct Builder {
   i64 nint = 0, n = 0, n2 = 0, nab = 0, N = 0;
   int e0 = 0, e1 = 0, e2 = 0;
   std::unordered_map<std::vector<int8_t>, i64, VecHash> idx[3];
+  // the same index keyed by the packed occupation (2 bits per internal orbital; nint <= 32)
+  std::unordered_map<uint64_t, i64> pidx[3];
   std::vector<i64> dk0, nDh;  // per N-2 path
   i64 nF = 0;                 // matrices used in BUF_F
   Scratch T;                  // BUF_T0 regions used per sigma build
@@ -181,7 +183,14 @@ struct Builder {
 void Builder::setup_heads() {
   for (int k = 0; k < 3; ++k)
     for (size_t p = 0; p < sp.paths[k].size(); ++p)
-      if (sp.paths[k][p].kept) idx[k][sp.paths[k][p].occ] = (i64)p;
+      if (sp.paths[k][p].kept) {
+        idx[k][sp.paths[k][p].occ] = (i64)p;
+        if (nint <= 32) {
+          uint64_t key = 0;
+          for (i64 q = 0; q < nint; ++q) key |= (uint64_t)sp.paths[k][p].occ[(size_t)q] << (2 * q);
+          pidx[k][key] = (i64)p;
+        }
+      }
   const auto& D = sp.paths[2];
   dk0.assign(D.size(), -1);
   nDh.assign(D.size(), 0);
@@ -229,11 +238,19 @@ void Builder::internal_blocks() {
     std::vector<std::map<std::pair<i64, i64>, std::vector<double>>> tblocks((size_t)omp_get_max_threads());
     std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
     for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
+    // per thread: the expansion of each head of this pattern, looked up once
+    std::vector<std::vector<const CsfExpansion*>> hexp((size_t)omp_get_max_threads(),
+                                                       std::vector<const CsfExpansion*>(heads.size(), nullptr));
+    const bool packed = nint <= 32;
+    const uint64_t mask2 = packed ? (nint == 32 ? ~0ull : ((1ull << (2 * nint)) - 1)) & 0x5555555555555555ull : 0;
 #pragma omp parallel for schedule(dynamic, 4)
     for (long long hsl = 0; hsl < (long long)heads.size(); ++hsl) {
       const size_t hs = (size_t)hsl;
       auto& blocks = tblocks[(size_t)omp_get_thread_num()];
       CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
+      auto& hx = hexp[(size_t)omp_get_thread_num()];
+      // this source head's blocks by target, moved into the thread's map when the head is done
+      std::unordered_map<i64, std::vector<double>> local;
       const Head& S = heads[hs];
       if (!S.kept || nsf_of(S) == 0) continue;
       const CsfExpansion& eS = E.expand(cfg(S));
@@ -251,15 +268,24 @@ void Builder::internal_blocks() {
         }
         auto emit = [&](Det d, double val) {
           if (val == 0.0) return;
-          std::vector<int8_t> o(ni);
-          for (int p = 0; p < ni; ++p) o[p] = (int8_t)(((d >> (2 * p)) & 1) + ((d >> (2 * p + 1)) & 1));
-          const Head* Tg = find(pt.kind, o);
-          if (!Tg || nsf_of(*Tg) == 0) return;
-          const CsfExpansion& eT = E.expand(cfg(*Tg));
+          const Head* Tg = nullptr;
+          if (packed) {  // per-orbital electron counts of the determinant, 2 bits each
+            const uint64_t lo = (uint64_t)d;
+            auto it = pidx[pt.kind].find((lo & mask2) + ((lo >> 1) & mask2));
+            if (it != pidx[pt.kind].end()) Tg = &heads[(size_t)it->second];
+          } else {
+            std::vector<int8_t> o(ni);
+            for (int p = 0; p < ni; ++p) o[p] = (int8_t)(((d >> (2 * p)) & 1) + ((d >> (2 * p + 1)) & 1));
+            Tg = find(pt.kind, o);
+          }
+          if (!Tg || !Tg->kept || nsf_of(*Tg) == 0) return;
+          const size_t ti = (size_t)(Tg->lex - 1);
+          if (!hx[ti]) hx[ti] = &E.expand(cfg(*Tg));
+          const CsfExpansion& eT = *hx[ti];
           auto it = eT.index.find(d);
           if (it == eT.index.end()) return;
           const double* thT = eT.basis->coeff.data() + (size_t)it->second * eT.nsf;
-          auto& blk = blocks[{Tg->lex - 1, (i64)hs}];
+          auto& blk = local[Tg->lex - 1];
           if (blk.empty()) blk.assign((size_t)eT.nsf * eS.nsf, 0.0);
           const double f = val * eT.sign * eS.sign;
           for (int a = 0; a < eT.nsf; ++a) {
@@ -324,6 +350,7 @@ void Builder::internal_blocks() {
                 emit(d, ph * v);
               }
       }
+      for (auto& kv : local) blocks[{kv.first, (i64)hs}] = std::move(kv.second);
     }
     if (bad_count) throw Error(4, "spin-function count mismatch in zero-external block");
     std::map<std::pair<i64, i64>, std::vector<double>> blocks;
