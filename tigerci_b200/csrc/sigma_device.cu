@@ -1576,6 +1576,16 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
   }
   try {
     auto t0 = std::chrono::steady_clock::now();
+    // TCI_INIT_TIMING=1 prints the device set-up phases (each ends with a stream synchronisation)
+    const bool timing = std::getenv("TCI_INIT_TIMING") != nullptr;
+    auto tp = t0;
+    auto phase = [&](const char* what, cudaStream_t st) {
+      if (!timing) return;
+      cudaStreamSynchronize(st);
+      const auto now = std::chrono::steady_clock::now();
+      std::fprintf(stderr, "init %-28s %.3f s\n", what, std::chrono::duration<double>(now - tp).count());
+      tp = now;
+    };
     std::unique_ptr<tci_ctx> ctx(new tci_ctx());
     int ndev = 0;
     TCI_CUDA(cudaGetDeviceCount(&ndev));
@@ -1617,6 +1627,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     }
     ctx->dheads = upload(dh, ctx->owned, ctx->stream);
     ctx->dk_head = upload(dkh, ctx->owned, ctx->stream);
+    phase("buffers and uploads", ctx->stream);
     // Mixed form without the plain-FP64 finish: the exchange product X = Lpk Lpk^T of the all-external
     // operators (the largest set-up GEMM, 2 npk^2 N flops) runs on the TMA-fed tensor-core kernel; its
     // 3xTF32 error is of the order of W's own FP32 rounding in that form.  The other banks stay FP64.
@@ -1644,9 +1655,14 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
       ctx->init.push_back(ctx->lower(s));
     }
     for (auto& s : P.sigma_steps) ctx->sigma.push_back(ctx->lower(s));
+    phase("lowering (step tables)", ctx->stream);
     for (size_t i = 0; i < ctx->init.size(); ++i) {
       ctx->run(ctx->init[i]);
-      if (i == banks && have_x) ctx->exchange_product_tc(xg, xs, kblock);
+      phase(ctx->init[i].name.c_str(), ctx->stream);
+      if (i == banks && have_x) {
+        ctx->exchange_product_tc(xg, xs, kblock);
+        phase("exchange product (tcgen05)", ctx->stream);
+      }
     }
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     // init-only buffers
@@ -1663,6 +1679,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     ctx->tc_kblock = kblock;
     ctx->refine = refine;
     ctx->setup_precision();
+    phase("precision set-up", ctx->stream);
     ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = ctx.release();
     return TCI_OK;
