@@ -266,8 +266,8 @@ void Builder::internal_blocks() {
           if ((d0 >> x) & 1) occ[no++] = x;
           else vir[nv++] = x;
         }
-        auto emit = [&](Det d, double val) {
-          if (val == 0.0) return;
+        // the kept head of this pattern whose configuration is the determinant's (nullptr if none)
+        auto target_of = [&](Det d) -> const Head* {
           const Head* Tg = nullptr;
           if (packed) {  // per-orbital electron counts of the determinant, 2 bits each
             const uint64_t lo = (uint64_t)d;
@@ -278,7 +278,10 @@ void Builder::internal_blocks() {
             for (int p = 0; p < ni; ++p) o[p] = (int8_t)(((d >> (2 * p)) & 1) + ((d >> (2 * p + 1)) & 1));
             Tg = find(pt.kind, o);
           }
-          if (!Tg || !Tg->kept || nsf_of(*Tg) == 0) return;
+          return (Tg && Tg->kept && nsf_of(*Tg) != 0) ? Tg : nullptr;
+        };
+        auto emit_to = [&](const Head* Tg, Det d, double val) {
+          if (val == 0.0 || !Tg) return;
           const size_t ti = (size_t)(Tg->lex - 1);
           if (!hx[ti]) hx[ti] = &E.expand(cfg(*Tg));
           const CsfExpansion& eT = *hx[ti];
@@ -292,6 +295,9 @@ void Builder::internal_blocks() {
             if (thT[a] == 0.0) continue;
             for (int b = 0; b < eS.nsf; ++b) blk[(size_t)a * eS.nsf + b] += f * thT[a] * thS[b];
           }
+        };
+        auto emit = [&](Det d, double val) {
+          if (val != 0.0) emit_to(target_of(d), d, val);
         };
         auto orb = [](int x) { return x >> 1; };
         auto spn = [](int x) { return x & 1; };
@@ -333,6 +339,10 @@ void Builder::internal_blocks() {
               for (int dd = c + 1; dd < nv; ++dd) {
                 const int xa = occ[a], xb = occ[b], xc = vir[c], xd = vir[dd];
                 if (spn(xa) + spn(xb) != spn(xc) + spn(xd)) continue;
+                // the target configuration first: most candidates leave the CI space
+                const Det dt = d0 ^ ((((Det)1) << xa) | (((Det)1) << xb) | (((Det)1) << xc) | (((Det)1) << xd));
+                const Head* Tg = target_of(dt);
+                if (!Tg) continue;
                 double v = 0;
                 if (spn(xc) == spn(xa) && spn(xd) == spn(xb)) v += I.i4(orb(xc), orb(xa), orb(xd), orb(xb));
                 if (spn(xc) == spn(xb) && spn(xd) == spn(xa)) v -= I.i4(orb(xc), orb(xb), orb(xd), orb(xa));
@@ -347,7 +357,7 @@ void Builder::internal_blocks() {
                 d |= ((Det)1) << xd;
                 if (parity_below(d, xc)) ph = -ph;
                 d |= ((Det)1) << xc;
-                emit(d, ph * v);
+                emit_to(Tg, d, ph * v);
               }
       }
       for (auto& kv : local) blocks[{kv.first, (i64)hs}] = std::move(kv.second);
