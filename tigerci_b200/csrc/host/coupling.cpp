@@ -63,16 +63,21 @@ const CsfExpansion& CouplingEngine::expand(const Config& c) {
 }
 
 void CouplingEngine::matrix(const Config& L, const Config& R, const Op& op, std::vector<double>& out) {
-  const auto& eL = expand(L);
-  const auto& eR = expand(R);
+  matrix(expand(L), expand(R), op, out);
+}
+
+void CouplingEngine::matrix(const CsfExpansion& eL, const CsfExpansion& eR, const Op& op, std::vector<double>& out) {
   out.assign((size_t)eL.nsf * eR.nsf, 0.0);
-  accumulate(L, R, op, 1.0, out);
+  accumulate(eL, eR, op, 1.0, out);
 }
 
 void CouplingEngine::accumulate(const Config& L, const Config& R, const Op& op, double coef,
                                 std::vector<double>& out) {
-  const auto& eL = expand(L);
-  const auto& eR = expand(R);
+  accumulate(expand(L), expand(R), op, coef, out);
+}
+
+void CouplingEngine::accumulate(const CsfExpansion& eL, const CsfExpansion& eR, const Op& op, double coef,
+                                std::vector<double>& out) {
   const int nL = eL.nsf, nR = eR.nsf;
   if (nL == 0 || nR == 0) return;
   const double* TL = eL.basis->coeff.data();

@@ -45,6 +45,9 @@ class CouplingEngine {
   void matrix(const Config& L, const Config& R, const Op& op, std::vector<double>& out);
   // Accumulate coef * <L|op|R> into out (nsf(L) x nsf(R)).
   void accumulate(const Config& L, const Config& R, const Op& op, double coef, std::vector<double>& out);
+  // The same for configurations already expanded (by this or another engine).
+  void matrix(const CsfExpansion& L, const CsfExpansion& R, const Op& op, std::vector<double>& out);
+  void accumulate(const CsfExpansion& L, const CsfExpansion& R, const Op& op, double coef, std::vector<double>& out);
   const SpinTables& tables() const { return tables_; }
 
  private:

@@ -927,15 +927,22 @@ void Builder::sv() {
   std::vector<std::map<std::pair<i64, i64>, std::vector<double>>> twmap((size_t)omp_get_max_threads());
   std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
   for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
+  // per thread: the expansion of each N-1 head (with the external electron), looked up once
+  std::vector<std::vector<const CsfExpansion*>> hexp1((size_t)omp_get_max_threads(),
+                                                      std::vector<const CsfExpansion*>(sp.paths[1].size(), nullptr));
 #pragma omp parallel for schedule(dynamic, 4)
   for (long long hvl = 0; hvl < (long long)sp.paths[0].size(); ++hvl) {
     auto& wmap = twmap[(size_t)omp_get_thread_num()];
     CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
     const Head& V = sp.paths[0][(size_t)hvl];
     if (!has(V)) continue;
+    const CsfExpansion& eV = E.expand(cfgV(V));
+    auto& hx = hexp1[(size_t)omp_get_thread_num()];
+    std::vector<double> m;
     auto add = [&](const Head* Mu, Op o, const double* vec, double hval_scale, i64 hi) {
-      std::vector<double> m;
-      E.matrix(cfgS(*Mu, e0), cfgV(V), o, m);  // predicted 1
+      const size_t mi = (size_t)(Mu->lex - 1);
+      if (!hx[mi]) hx[mi] = &E.expand(cfgS(*Mu, e0));
+      E.matrix(*hx[mi], eV, o, m);  // predicted 1
       for (i64 kt = 0; kt < Mu->nsf; ++kt)
         for (i64 ks = 0; ks < V.nsf; ++ks) {
           const double a = m[kt * V.nsf + ks];
