@@ -331,8 +331,10 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
 // One block per chunk; warp w takes the sources w, w + 8, ... in table order,
 // and the eight warps' partial sums are added in warp order, so the result is
 // independent of timing.  A short target with many sources spreads the
-// sources over all threads instead.
+// sources over all threads instead; a target with few sources (a gather or a
+// scatter) gives each thread one element and all the sources in order.
 constexpr int AXPY_CHUNK = 256;
+constexpr int AXPY_DIRECT = 8;  // targets with at most this many sources: one thread per element
 __global__ void __launch_bounds__(256) axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg,
                                                      const DAxpySource* __restrict__ src) {
   __shared__ double part[8][AXPY_CHUNK];
@@ -340,6 +342,19 @@ __global__ void __launch_bounds__(256) axpy_segments(const DAxpyTarget* __restri
   if (t >= ntg) return;
   const DAxpyTarget T = tg[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (T.src_end - T.src_begin <= AXPY_DIRECT) {
+    // few sources (gathers, scatters): a thread per element sums every source in table order
+    for (long long i = threadIdx.x; i < T.len; i += blockDim.x) {
+      double acc = 0.0;
+      for (long long s = T.src_begin; s < T.src_end; ++s) {
+        const DAxpySource S = src[s];
+        const double c = S.scale ? S.coef * (*S.scale) : S.coef;
+        acc = fma(c, S.src[T.base + i], acc);
+      }
+      T.dst[i] += acc;
+    }
+    return;
+  }
   if (T.len < 8 && T.src_end - T.src_begin > 64) {
     for (long long i = 0; i < T.len; ++i) {
       double acc = 0.0;
@@ -550,6 +565,45 @@ constexpr double kDefaultSubspaceBytes = 30e9;
 // synchronises the device) on another are kept apart by this lock.
 std::mutex g_capture_free_mu;
 
+// Device memory of the sigma contexts comes from one stream-ordered pool per device that keeps the pages
+// it has mapped (release threshold unlimited): a context set up after another one was destroyed (the
+// request server, repeated set-ups in one process) reuses them instead of mapping new memory, which made
+// set-up and tear-down times vary by hundreds of milliseconds.  Allocations and frees are ordered on the
+// context's stream.
+cudaError_t dev_malloc_v(void** p, size_t bytes, cudaStream_t st) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, st);
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pools[dev], &props);
+      if (e != cudaSuccess) {
+        pools[dev] = nullptr;
+        return e;
+      }
+      uint64_t keep = UINT64_MAX;
+      e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+    }
+    pool = pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes, cudaStream_t st) {
+  return dev_malloc_v(reinterpret_cast<void**>(p), bytes, st);
+}
+inline cudaError_t dev_free(void* p, cudaStream_t st) { return p ? cudaFreeAsync(p, st) : cudaSuccess; }
+
 // partial[k * RBLK + b] = sum over block b's chunk of A[k][i] * x[i]
 __global__ void __launch_bounds__(RB) multi_dot_partial(const double* __restrict__ A, long long lda, int m,
                                                         const double* __restrict__ x, long long n,
@@ -672,7 +726,7 @@ template <class T>
 T* upload(const std::vector<T>& v, std::vector<void*>& owned, cudaStream_t st) {
   if (v.empty()) return nullptr;
   T* d = nullptr;
-  TCI_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+  TCI_CUDA(dev_malloc(&d, v.size() * sizeof(T), st));
   owned.push_back(d);
   TCI_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   return d;
@@ -745,12 +799,11 @@ struct tci_ctx {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     std::lock_guard<std::mutex> lk(g_capture_free_mu);
-    if (dotbuf) cudaFree(dotbuf);
-    for (double* p : {dav_c, dav_hc, dav_r, dav_tc, dav_th})
-      if (p) cudaFree(p);
-    for (int b = 0; b < NUM_BUFS; ++b)
-      if (buf[b]) cudaFree(buf[b]);
-    for (void* p : owned) cudaFree(p);
+    dev_free(dotbuf, stream);
+    for (double* p : {dav_c, dav_hc, dav_r, dav_tc, dav_th}) dev_free(p, stream);
+    for (int b = 0; b < NUM_BUFS; ++b) dev_free(buf[b], stream);
+    for (void* p : owned) dev_free(p, stream);
+    if (stream) cudaStreamSynchronize(stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1049,7 +1102,7 @@ struct tci_ctx {
   void ensure_diag() {
     if (hd) return;
     const i64 n = plan.total_csfs;
-    TCI_CUDA(cudaMalloc(&hd, n * sizeof(double)));
+    TCI_CUDA(dev_malloc(&hd, n * sizeof(double), stream));
     owned.push_back(hd);
     TCI_CUDA(cudaMemsetAsync(hd, 0, n * sizeof(double), stream));
     std::vector<DDiag> e;
@@ -1070,15 +1123,15 @@ struct tci_ctx {
       TCI_CUDA(cudaStreamSynchronize(stream));
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
       for (void* p : {(void*)dots, (void*)coefs}) {
-        cudaFree(p);
+        dev_free(p, stream);
         owned.erase(std::find(owned.begin(), owned.end(), p));
       }
       dots = coefs = nullptr;
       scratch_cap = 0;
     }
-    TCI_CUDA(cudaMalloc(&dots, ((size_t)mmax * (RBLK + 1) + 16) * sizeof(double)));
+    TCI_CUDA(dev_malloc(&dots, ((size_t)mmax * (RBLK + 1) + 16) * sizeof(double), stream));
     owned.push_back(dots);
-    TCI_CUDA(cudaMalloc(&coefs, (size_t)4 * mmax * sizeof(double)));
+    TCI_CUDA(dev_malloc(&coefs, (size_t)4 * mmax * sizeof(double), stream));
     owned.push_back(coefs);
     scratch_cap = mmax;
   }
@@ -1218,13 +1271,13 @@ struct tci_ctx {
     auto release = [&]() {
       cudaStreamSynchronize(stream);
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
-      for (void* p : {(void*)ah, (void*)al, (void*)st})
-        if (p) cudaFree(p);
+      for (void* p : {(void*)ah, (void*)al, (void*)st}) dev_free(p, stream);
+      cudaStreamSynchronize(stream);
     };
     try {
-      TCI_CUDA(cudaMalloc(&ah, sizeof(float) * (size_t)(M * ld)));
-      TCI_CUDA(cudaMalloc(&al, sizeof(float) * (size_t)(M * ld)));
-      TCI_CUDA(cudaMalloc(&st, sizeof(int)));
+      TCI_CUDA(dev_malloc(&ah, sizeof(float) * (size_t)(M * ld), stream));
+      TCI_CUDA(dev_malloc(&al, sizeof(float) * (size_t)(M * ld), stream));
+      TCI_CUDA(dev_malloc(&st, sizeof(int), stream));
       TCI_CUDA(cudaMemsetAsync(st, 0, sizeof(int), stream));
       TCI_CUDA(tci_gtma_host::split(buf[BUF_T0] + x.offA, M, K, x.lda, ah, al, stream));
       tci_gtma_host::TmaMaps m;
@@ -1254,7 +1307,10 @@ struct tci_ctx {
     ensure_diag();  // the diagonal reads the FP64 W
     const i64 np = plan.np, nm = plan.nm;
     auto alloc_f = [&](float** p, size_t n) {
-      if (cudaMalloc(p, n * sizeof(float)) != cudaSuccess) throw Error(TCI_ERR_MEMORY, "device allocation failed (fp32 operators)");
+      if (dev_malloc(p, n * sizeof(float), stream) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(TCI_ERR_MEMORY, "device allocation failed (fp32 operators)");
+      }
       owned.push_back(*p);
       bytes_held += (double)n * sizeof(float);
     };
@@ -1264,7 +1320,7 @@ struct tci_ctx {
     if (has_trip()) {
       alloc_f(&u2t, (size_t)tci_tc_host::u2_floats(plan.n_trip, nm));
     }
-    TCI_CUDA(cudaMalloc(&tc_status, sizeof(int)));
+    TCI_CUDA(dev_malloc(&tc_status, sizeof(int), stream));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
     bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false;
@@ -1336,7 +1392,7 @@ struct tci_ctx {
       throw Error(TCI_ERR_CUDA, err);
     if (refine != 1) {  // the FP64 W is only needed for the plain-FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
-      TCI_CUDA(cudaFree(buf[BUF_W]));
+      TCI_CUDA(dev_free(buf[BUF_W], stream));
       bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
       buf[BUF_W] = nullptr;
     }
@@ -1600,7 +1656,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     Plan& P = ctx->plan;
     for (int b = 0; b < NUM_BUFS; ++b) {
       if (P.buf_size[b] <= 0) continue;
-      cudaError_t e = cudaMalloc(&ctx->buf[b], P.buf_size[b] * sizeof(double));
+      cudaError_t e = dev_malloc(&ctx->buf[b], P.buf_size[b] * sizeof(double), ctx->stream);
       if (e != cudaSuccess) {
         cudaGetLastError();
         throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
@@ -1669,7 +1725,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     for (int b : {BUF_X, BUF_L, BUF_LE, BUF_LI}) {
       if (ctx->buf[b]) {
         std::lock_guard<std::mutex> lk(g_capture_free_mu);
-        TCI_CUDA(cudaFree(ctx->buf[b]));
+        TCI_CUDA(dev_free(ctx->buf[b], ctx->stream));
         ctx->bytes_held -= (double)P.buf_size[b] * sizeof(double);
         ctx->buf[b] = nullptr;
       }
@@ -1891,23 +1947,25 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
       {
         std::lock_guard<std::mutex> lk(g_capture_free_mu);
         for (double** p : {&ctx->dav_c, &ctx->dav_hc, &ctx->dav_r, &ctx->dav_tc, &ctx->dav_th}) {
-          if (*p) cudaFree(*p);
+          dev_free(*p, ctx->stream);
           *p = nullptr;
         }
       }
       ctx->dav_cap = ctx->dav_keep = 0;
-      cudaError_t e1 = cudaMalloc(&ctx->dav_c, (size_t)cap * n * sizeof(double));
-      cudaError_t e2 = cudaMalloc(&ctx->dav_hc, (size_t)cap * n * sizeof(double));
-      cudaError_t e3 = cudaMalloc(&ctx->dav_r, (size_t)(n + 8) * sizeof(double));
-      cudaError_t e4 = cudaMalloc(&ctx->dav_tc, (size_t)keep * n * sizeof(double));
-      cudaError_t e5 = cudaMalloc(&ctx->dav_th, (size_t)keep * n * sizeof(double));
+      cudaStream_t ds = ctx->stream;
+      cudaError_t e1 = dev_malloc(&ctx->dav_c, (size_t)cap * n * sizeof(double), ds);
+      cudaError_t e2 = dev_malloc(&ctx->dav_hc, (size_t)cap * n * sizeof(double), ds);
+      cudaError_t e3 = dev_malloc(&ctx->dav_r, (size_t)(n + 8) * sizeof(double), ds);
+      cudaError_t e4 = dev_malloc(&ctx->dav_tc, (size_t)keep * n * sizeof(double), ds);
+      cudaError_t e5 = dev_malloc(&ctx->dav_th, (size_t)keep * n * sizeof(double), ds);
       if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess || e5 != cudaSuccess) {
         cudaGetLastError();
         std::lock_guard<std::mutex> lk(g_capture_free_mu);
         for (double** p : {&ctx->dav_c, &ctx->dav_hc, &ctx->dav_r, &ctx->dav_tc, &ctx->dav_th}) {
-          if (*p) cudaFree(*p);
+          dev_free(*p, ctx->stream);
           *p = nullptr;
         }
+        cudaStreamSynchronize(ctx->stream);
         throw Error(TCI_ERR_MEMORY, "device allocation of the Davidson subspace failed");
       }
       ctx->dav_cap = cap;
@@ -2180,12 +2238,14 @@ int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const doub
       TCI_CUDA(cudaStreamSynchronize(ctx->stream));
       if (ctx->dotbuf) {
         std::lock_guard<std::mutex> lk(g_capture_free_mu);
-        TCI_CUDA(cudaFree(ctx->dotbuf));
+        TCI_CUDA(dev_free(ctx->dotbuf, ctx->stream));
       }
       ctx->dotbuf = nullptr;
       ctx->dotbuf_cap = 0;
-      if (cudaMalloc(&ctx->dotbuf, need * sizeof(double)) != cudaSuccess)
+      if (dev_malloc(&ctx->dotbuf, need * sizeof(double), ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
         throw Error(TCI_ERR_MEMORY, "device allocation of the projection scratch failed");
+      }
       ctx->dotbuf_cap = need;
     }
     TCI_CUDA(cudaEventRecord(ctx->ev0, user));
