@@ -1,14 +1,18 @@
 // Device executor of the sigma plan (host/plan.h) and the device half of the C
-// ABI.  FP64 throughout.  Kernels:
-//   gemm_grouped_f64  C = beta*C + sum_seg alpha*op(A)op(B), one CTA per 64x64
-//                     tile of every problem, segments summed in table order
-//   axpy_segments     one warp per target range, sources summed in table order
-//   dot_segments      one warp per target scalar
+// ABI.  Kernels here (FP64):
+//   gemm_tiled_f64    C = beta*C + sum_seg alpha*op(A)op(B), one CTA per 64x128
+//                     or 128x64 tile of every problem, segments summed in table
+//                     order (split-K for few-tile, long-K steps)
+//   gemm_skinny_f64   problems of at most 8 rows: a warp per output column
+//   axpy_segments     one block per target chunk, sources summed in table order
+//   dot_segments      one block per target scalar
 //   unpack_pairs / pack_pairs   SCEP <-> dense external pair matrices
 //                     (tiger_fortran/scepmaker_mod.f90:121-257, 633-800)
 //   build_allext      W+ / W- from the packed external (ab|cd) block
-// The plan is replayed in a fixed launch order on one stream, so every sigma
-// build is bitwise reproducible.
+//   Davidson kernels  projections, linear combinations, preconditioner
+// The mixed form's tensor-core steps run on allext_tc.cu, gemm_tma.cu and
+// gemm_tc.cu.  The plan is replayed in a fixed launch order on one stream, so
+// every sigma build is bitwise reproducible.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -401,7 +405,8 @@ __global__ void __launch_bounds__(256) axpy_segments(const DAxpyTarget* __restri
 }
 
 // Segmented dot products: *dst += sum_s coef_s (a_s . b_s).  One block per
-// target; warp w takes the sources w, w + 8, ...; fixed-order reductions.
+// target; warp w takes the sources w, w + 8, ... and reduces across its lanes
+// once; fixed-order reductions.
 __global__ void __launch_bounds__(256) dot_segments(const DDotTarget* __restrict__ tg, long long ntg,
                                                     const DDotSource* __restrict__ src) {
   __shared__ double part[8];
@@ -409,15 +414,26 @@ __global__ void __launch_bounds__(256) dot_segments(const DDotTarget* __restrict
   if (t >= ntg) return;
   const DDotTarget T = tg[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // each lane keeps sum_s coef_s sum_{its i} a_s[i] b_s[i] over the warp's sources; one reduction at the end
   double total = 0.0;
   for (long long s = T.src_begin + warp; s < T.src_end; s += 8) {
     const DDotSource S = src[s];
     double acc = 0.0;
-    for (long long i = lane; i < S.len; i += 32) acc = fma(S.a[i], S.b[i], acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (((reinterpret_cast<uintptr_t>(S.a) | reinterpret_cast<uintptr_t>(S.b)) & 15) == 0 && (S.len & 1) == 0) {
+      const double2* a2 = reinterpret_cast<const double2*>(S.a);
+      const double2* b2 = reinterpret_cast<const double2*>(S.b);
+      for (long long i = lane; i < S.len / 2; i += 32) {
+        const double2 x = __ldg(a2 + i), y = __ldg(b2 + i);
+        acc = fma(x.x, y.x, acc);
+        acc = fma(x.y, y.y, acc);
+      }
+    } else {
+      for (long long i = lane; i < S.len; i += 32) acc = fma(__ldg(S.a + i), __ldg(S.b + i), acc);
+    }
     total = fma(S.coef, acc, total);
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
   if (lane == 0) part[warp] = total;
   __syncthreads();
   if (threadIdx.x == 0) {
