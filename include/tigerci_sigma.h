@@ -122,11 +122,12 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
  * each Ritz vector with one sigma build in which every term is FP64 but the
  * all-external one, which stays on its tensor-core kernel (the FP64 W is
  * released after the diagonal is built); 1 the same with a plain-FP64 sigma
- * build (the FP64 W stays resident); 0 the mixed Ritz values.  The finished
+ * build (the FP64 W stays resident); 3 as 2 with the three-external
+ * contractions on the tensor cores too; 0 the mixed Ritz values.  The finished
  * root's error is second order in the eigenvector error of the mixed products
- * plus, for 2, the first-order error of the all-external term alone.  In modes
- * 2 and 0 the set-up exchange product of the all-external operators runs on
- * the tensor cores as well (3xTF32, FP64 promotion). */
+ * plus, for 2 and 3, the first-order error of the terms left on the tensor
+ * cores.  In modes 0, 2 and 3 the set-up exchange product of the all-external
+ * operators runs on the tensor cores as well (3xTF32, FP64 promotion). */
 #define TCI_PRECISION_FP64 0
 #define TCI_PRECISION_TF32X3 1
 int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t device, const int64_t* options,

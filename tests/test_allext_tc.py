@@ -129,7 +129,7 @@ def test_mixed_davidson_relative_bound_large_scale(need_gpu):
     assert np.abs(ea - eb).max() < 1e-6 * s2 + 1e-8
 
 
-@pytest.mark.parametrize("finish", ["no_allext", "full"])
+@pytest.mark.parametrize("finish", ["no_allext", "full", "no_allext_3ext"])
 def test_mixed_roots_with_fp64_finish_match_fp64_closely(finish, need_gpu):
     """The mixed form's roots, finished as FP64 Rayleigh quotients of its Ritz
     vectors (every term FP64, or every term but the all-external one), agree

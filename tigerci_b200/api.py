@@ -166,13 +166,14 @@ class SigmaBuilder:
         """fp64_finish (mixed form): "no_allext" (default) reports each root as the Rayleigh quotient of its
         Ritz vector with a sigma build in which every term is FP64 but the all-external one, which stays on
         its tensor-core kernel (no FP64 W kept); "full" / True does the same with a plain-FP64 sigma build
-        (the FP64 W stays resident); "none" / False reports the mixed Ritz values."""
+        (the FP64 W stays resident); "no_allext_3ext" is "no_allext" with the three-external contractions on
+        the tensor cores too; "none" / False reports the mixed Ritz values."""
         self._d = deck.c_struct()
         self._o = op.c_struct()
         self._op = op
         self.precision = precision
         h = C.c_void_p()
-        finish = {True: 1, False: 0, "full": 1, "none": 0, "no_allext": 2}[fp64_finish]
+        finish = {True: 1, False: 0, "full": 1, "none": 0, "no_allext": 2, "no_allext_3ext": 3}[fp64_finish]
         opts = np.array([self.PRECISIONS[precision], promote_every, self.TC_GEMMS[tc_gemms], finish], dtype=np.int64)
         check(lib().tci_sigma_init_ex(C.byref(self._d), C.byref(self._o), device, ptr(opts), 4, C.byref(h)))
         self._h = h

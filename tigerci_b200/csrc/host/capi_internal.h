@@ -14,7 +14,8 @@ void operator_from_c(const tci_operator* op, const CsfSpace& sp, Operator& out);
 // Device half of tci_sigma_init: a context from a host-built space and plan
 // (chol: the host Cholesky vectors the plan was built for).
 // refine (mixed form): finish every root as an FP64 Rayleigh quotient, 1 with a plain-FP64 sigma build
-// (keeps the FP64 W), 2 with every term FP64 but the all-external one (default), 0 not at all.
+// (keeps the FP64 W), 2 with every term FP64 but the all-external one (default), 3 as 2 with the
+// three-external contractions on the tensor cores too, 0 not at all.
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
                   tci_ctx** out, int64_t refine = 2);
 // Selects the GEMM steps that run on the tensor cores in the mixed form (tci_sigma_init_ex options[2]).

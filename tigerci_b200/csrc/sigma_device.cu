@@ -1418,7 +1418,7 @@ struct tci_ctx {
   // one by one, outside the context's graph): d_s = H d_c.
   void sigma_of_fp64(const double* d_c, double* d_s) {
     const i64 n = plan.total_csfs;
-    const bool tc_allext = refine == 2 && precision == 1;
+    const bool tc_allext = (refine == 2 || refine == 3) && precision == 1;
     if (!buf[BUF_W] && !tc_allext) throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
     TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
@@ -1472,7 +1472,9 @@ struct tci_ctx {
         if (uses_tc(s) && s.skinny_nwarps > 0)
           gemm_skinny_f64<<<(unsigned)((s.skinny_nwarps + 7) / 8), 256, 0, stream>>>(s.skinny_probs, s.skinny_nprob,
                                                                                   s.segs, s.skinny_nwarps);
-        if (uses_tc(s) && s.tma_probs && tma_ok(s)) {
+        // finish mode 3: the three-external contractions stay on the tensor cores too
+        if ((uses_tc(s) || (allext_tc_in_fp64 && refine == 3 && (s.tma_kind == 2 || s.tma_kind == 3))) &&
+            s.tma_probs && tma_ok(s)) {
           const i64 n = plan.n;
           if (s.tma_kind == 1) {
             TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
@@ -1563,7 +1565,7 @@ int tci_sigma_init_ex(const tci_deck* deck, const tci_operator* op, int64_t devi
   if (options && n_options > 1 && options[1] > 0) kblock = options[1];
   if (options && n_options > 2) tc_mode = options[2];
   if (options && n_options > 3) refine = options[3];
-  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2 || refine < 0 || refine > 2) {
+  if (precision < 0 || precision > 1 || tc_mode < 0 || tc_mode > 2 || refine < 0 || refine > 3) {
     set_error("unknown precision mode, tensor-core GEMM selection or finish");
     return TCI_ERR_ARG;
   }
