@@ -12,7 +12,7 @@
 // fold the segment's alpha into B, split every element into a TF32 high part
 // and an FP32 low part (x = hi + lo), and store both into shared memory in the
 // K-major 128-byte-swizzle layout that the MMA descriptors read.  One thread
-// issues three kind::tf32 MMAs per 8-wide k slice (hi*hi + hi*lo + lo*hi) into
+// issues two kind::tf32 MMAs per 8-wide k slice (A_hi x [B_hi; B_lo], A_lo x B_hi) into
 // a double-buffered TMEM accumulator; every KB_PER_BLOCK k-steps the four
 // epilogue warps add the FP32 block sums into FP64 registers, and write
 // C = beta C + acc once at the end.
@@ -45,7 +45,10 @@ constexpr int A_BYTES = BM * BK * 4;  // 16 KB
 constexpr int B_BYTES = BN * BK * 4;  // 8 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
+// B's high rows are followed by its low rows in a stage: A_hi x [B_hi; B_lo] is one MMA of N = 2 BN and
+// A_lo x B_hi a second one (two instructions per k slice instead of three)
+constexpr uint32_t kIdescBoth = idesc_tf32(BM, 2 * BN), kIdescHi = idesc_tf32(BM, BN);
+constexpr int ACC_COLS = 2 * BN;  // hi x hi + lo x hi, then hi x lo
 static_assert(BM * BK == 32 * 32 * NPROD && BN * BK == 16 * 32 * NPROD && NPROD == 4 && BK == 32,
               "producer element maps");
 
@@ -106,9 +109,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {  // TMEM: two accumulator buffers of BN fp32 columns
+  if (warp == 8) {  // TMEM: two accumulator buffers of ACC_COLS fp32 columns
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * BN));
+                 "r"(2 * ACC_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -215,15 +218,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
         uint8_t* st = base + s * STAGE_BYTES;
-        const uint32_t d = tmem + (uint32_t)(buf * BN);
+        const uint32_t d = tmem + (uint32_t)(buf * ACC_COLS);
 #pragma unroll
         for (int kk = 0; kk < BK / 8; ++kk) {  // 8 tf32 = 32 bytes per MMA k slice
           const uint64_t ahi = smem_desc_sw128(st + kk * 32), alo = smem_desc_sw128(st + A_BYTES + kk * 32);
-          const uint64_t bhi = smem_desc_sw128(st + 2 * A_BYTES + kk * 32);
-          const uint64_t blo = smem_desc_sw128(st + 2 * A_BYTES + B_BYTES + kk * 32);
-          mma_tf32(d, ahi, bhi, kIdesc, (first && kk == 0) ? 0u : 1u);
-          mma_tf32(d, ahi, blo, kIdesc, 1u);
-          mma_tf32(d, alo, bhi, kIdesc, 1u);
+          const uint64_t b = smem_desc_sw128(st + 2 * A_BYTES + kk * 32);  // B hi rows, then B lo rows
+          mma_tf32(d, ahi, b, kIdescBoth, (first && kk == 0) ? 0u : 1u);
+          mma_tf32(d, alo, b, kIdescHi, 1u);
         }
         mma_commit(&empty[s]);
         if ((step % KB) == KB - 1 || step == nsteps - 1) mma_commit(&dfull[buf]);
@@ -249,7 +250,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
       for (int c = 0; c < BN / 16; ++c) {
         uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * BN + c * 16), v);
+        const uint32_t tq = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * ACC_COLS + c * 16);
+        tmem_ld16(tq, v);  // hi x hi + lo x hi
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[c * 16 + j] += (double)__uint_as_float(v[j]);
+        tmem_ld16(tq + BN, v);  // hi x lo
 #pragma unroll
         for (int j = 0; j < 16; ++j) acc[c * 16 + j] += (double)__uint_as_float(v[j]);
       }
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
-  if (warp == 8) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+  if (warp == 8) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACC_COLS));
 }
 
 }  // namespace tci_gtc
