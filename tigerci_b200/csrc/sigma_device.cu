@@ -711,7 +711,8 @@ struct DevStep {
   long long tma_ntiles = 0;
   // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows), 3: reverse
   // three-external (transposed V_i rows x gathered coefficient rows), 4: singles-singles two-external
-  // (integral rows x gathered single-vector rows, computed transposed)
+  // (integral rows x gathered single-vector rows, computed transposed), 5: forward one-external
+  // (coupling-vector rows x pair matrices)
   int tma_kind = 0;
   long long tma_aux = 0;   // kinds 3, 4: offset of the gathered coefficients in BUF_T0
   long long tma_rows = 0;  // kind 4: rows of the gathered coefficients
@@ -779,8 +780,9 @@ struct tci_ctx {
   float *v_hi = nullptr, *v_lo = nullptr, *df_hi = nullptr, *df_lo = nullptr;
   float *vt_hi = nullptr, *vt_lo = nullptr, *u3_hi = nullptr, *u3_lo = nullptr;  // reverse three-external
   float *cg_hi = nullptr, *cg_lo = nullptr;                                        // singles-singles
-  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss;
-  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false, tma_ss_ready = false;
+  float *wv_hi = nullptr, *wv_lo = nullptr;                                        // one-external vectors
+  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss, tma_1x;
+  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false, tma_ss_ready = false, tma_1x_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* u2s = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -920,6 +922,27 @@ struct tci_ctx {
       if (ubase < 0 || ubase + plan.nint * plan.nD * n > plan.buf_size[BUF_T0]) return;
       d.tma_aux = ubase;
       d.tma_kind = 3;
+    } else if (s.name == "one-external forward") {
+      // Z rows (M x n) = coupling-vector rows of BUF_WV (M x n) x D_d, D_d entering as the K-major operand
+      // through its symmetry (D^T = p D, the sign folded into alpha)
+      TN = tci_gtma_host::tile_n(tma_wide(5));
+      std::vector<double> psign((size_t)std::max<i64>(plan.nD, 1), 1.0);
+      for (const auto& h : plan.dheads)
+        for (i64 k = 0; k < h.nD; ++k) psign[(size_t)(h.dk0 + k)] = k < h.nsing ? 1.0 : -1.0;
+      for (const auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        const DGemmProblem& dp = pr[gi++];
+        if (g.N != n || g.ldc != n || g.seg_end - g.seg_begin != 1) return;
+        const GemmSeg& x = s.gs[(size_t)g.seg_begin];
+        if (x.a != BUF_WV || x.b != BUF_D || x.tA || x.tB || x.lda != n || x.ldb != n || x.K != n || x.offA % n ||
+            x.offB % n2)
+          return;
+        TmaProblem q{dp.C, n, g.M, n, 0, 0, g.beta, (long long)ts.size(), 0, 0, nullptr, nullptr, 0};
+        ts.push_back(TmaSeg{x.offA / n, x.offB / n, 0, n, x.alpha * psign[(size_t)(x.offB / n2)]});
+        q.seg_end = (long long)ts.size();
+        push(q);
+      }
+      d.tma_kind = 5;
     } else if (s.name == "ss two-external") {
       // Y rows (M x n) = gathered rows (M x n) X^T with X an n x n integral matrix of BUF_JK, computed as
       // Y^T = X Cg^T: A = rows of X, B = the gathered rows.  Problems of at most SKINNY_M rows (the
@@ -1178,10 +1201,12 @@ struct tci_ctx {
     sigma_count++;
   }
   // TMA-fed kernel's tile width per step kind: 128 unless the B operand has at most 64 rows per problem
-  bool tma_wide(int kind) const { return kind == 1 ? plan.n > 64 : kind == 4 ? false : plan.nD > 64; }
+  bool tma_wide(int kind) const {
+    return (kind == 1 || kind == 5) ? plan.n > 64 : kind == 4 ? false : plan.nD > 64;
+  }
   bool tma_ok(const DevStep& s) const {
     return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready) ||
-           (s.tma_kind == 4 && tma_ss_ready);
+           (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready);
   }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
@@ -1339,12 +1364,13 @@ struct tci_ctx {
     TCI_CUDA(dev_malloc(&tc_status, sizeof(int), stream));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
-    bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false;
+    bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false, want_1x = false;
     long long ss_rows = 0;
     for (const auto& st : sigma) {
       want_dd = want_dd || (st.tma_probs && st.tma_kind == 1);
       want_t3 = want_t3 || (st.tma_probs && st.tma_kind == 2);
       want_t3r = want_t3r || (st.tma_probs && st.tma_kind == 3);
+      want_1x = want_1x || (st.tma_probs && st.tma_kind == 5);
       if (st.tma_probs && st.tma_kind == 4) {
         want_ss = true;
         ss_rows = std::max(ss_rows, st.tma_rows);
@@ -1359,12 +1385,25 @@ struct tci_ctx {
       alloc_f(&jk_lo, (size_t)(xrows * ld));
       TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, n, jk_hi, jk_lo, stream));
     }
-    if (want_dd && plan.nD > 0) {
+    if ((want_dd || want_1x) && plan.nD > 0) {  // the pair matrices, split every build
       const i64 ld = tci_gtma_host::pitch(n), drows = plan.nD * n;
       alloc_f(&d_hi, (size_t)(drows * ld));
       alloc_f(&d_lo, (size_t)(drows * ld));
+    }
+    if (want_dd && plan.nD > 0) {
+      const i64 drows = plan.nD * n;
       if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows, n, d_hi, d_lo, drows, n, tma_wide(1), err)) throw Error(TCI_ERR_CUDA, err);
       tma_dd_ready = true;
+    }
+    const i64 wvrows = plan.buf_size[BUF_WV] / std::max<i64>(1, n);
+    if (want_1x && plan.nD > 0 && wvrows > 0) {  // the one-external coupling vectors, split once
+      const i64 ld = tci_gtma_host::pitch(n), drows = plan.nD * n;
+      alloc_f(&wv_hi, (size_t)(wvrows * ld));
+      alloc_f(&wv_lo, (size_t)(wvrows * ld));
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_WV], wvrows, n, n, wv_hi, wv_lo, stream));
+      if (!tci_gtma_host::prepare(tma_1x, wv_hi, wv_lo, wvrows, n, d_hi, d_lo, drows, n, tma_wide(5), err))
+        throw Error(TCI_ERR_CUDA, err);
+      tma_1x_ready = true;
     }
     if (want_ss && xrows > 0 && ss_rows > 0) {
       const i64 ld = tci_gtma_host::pitch(n);
@@ -1484,6 +1523,10 @@ struct tci_ctx {
           } else if (s.tma_kind == 2) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_t3, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          } else if (s.tma_kind == 5) {
+            TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * n, n, n, d_hi, d_lo, stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_1x, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
           } else if (s.tma_kind == 4) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_T0] + s.tma_aux, s.tma_rows, n, n, cg_hi, cg_lo, stream));
@@ -1621,7 +1664,10 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                                   (double)(P.buf_size[BUF_JK] / std::max<i64>(1, P.n) + P.nD * P.n) +
                               2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * (double)(P.nint * P.n + P.nD) +
                               // transposed V_i and the gathered coefficients of the reverse three-external step
-                              2.0 * (double)tci_gtma_host::pitch(P.n) * (double)(P.nint * P.n * P.n + P.nint * P.nD));
+                              2.0 * (double)tci_gtma_host::pitch(P.n) * (double)(P.nint * P.n * P.n + P.nint * P.nD) +
+                              // one-external coupling vectors
+                              2.0 * (double)tci_gtma_host::pitch(P.n) *
+                                  (double)(P.buf_size[BUF_WV] / std::max<i64>(1, P.n)));
     // gathered single-vector rows of the singles-singles step (problems above the skinny size)
     double ss_rows = 0;
     for (const auto& st : P.sigma_steps)
