@@ -764,7 +764,8 @@ void Builder::dv() {
   zero_step(P.sigma_steps, BUF_T0, F2, nk * P.nD, "dv forward zero");
   {  // F2 (nk x nD) = Kbank (nk x n^2) * D^T, split over the n^2 contraction
     const i64 S = std::max<i64>(1, std::min<i64>(64, n2 / 1024));
-    const i64 kc = (n2 + S - 1) / S;
+    // chunks start on multiples of 32 columns (the tensor-core form loads 32-column tiles by TMA)
+    const i64 kc = ((n2 + S - 1) / S + 31) / 32 * 32;
     const i64 Pt = T.alloc(S * nk * P.nD);
     Step& g = step(P.sigma_steps, STEP_GEMM, "dv forward");
     for (i64 sidx = 0; sidx < S; ++sidx) {

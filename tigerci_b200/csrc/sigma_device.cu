@@ -712,7 +712,7 @@ struct DevStep {
   // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows), 3: reverse
   // three-external (transposed V_i rows x gathered coefficient rows), 4: singles-singles two-external
   // (integral rows x gathered single-vector rows, computed transposed), 5: forward one-external
-  // (coupling-vector rows x pair matrices)
+  // (coupling-vector rows x pair matrices), 6: dv forward (exchange-bank rows x pair-matrix rows)
   int tma_kind = 0;
   long long tma_aux = 0;   // kinds 3, 4: offset of the gathered coefficients in BUF_T0
   long long tma_rows = 0;  // kind 4: rows of the gathered coefficients
@@ -781,8 +781,10 @@ struct tci_ctx {
   float *vt_hi = nullptr, *vt_lo = nullptr, *u3_hi = nullptr, *u3_lo = nullptr;  // reverse three-external
   float *cg_hi = nullptr, *cg_lo = nullptr;                                        // singles-singles
   float *wv_hi = nullptr, *wv_lo = nullptr;                                        // one-external vectors
-  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss, tma_1x;
-  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false, tma_ss_ready = false, tma_1x_ready = false;
+  float *kb_hi = nullptr, *kb_lo = nullptr;                                        // dv exchange bank
+  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss, tma_1x, tma_dv;
+  bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false, tma_ss_ready = false, tma_1x_ready = false,
+       tma_dv_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* u2s = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -943,6 +945,33 @@ struct tci_ctx {
         push(q);
       }
       d.tma_kind = 5;
+    } else if (s.name == "dv forward") {
+      // F2 partials (nk x nD, one problem per 32-aligned chunk of the n^2 contraction) = rows of the
+      // exchange bank (nk x n^2, in BUF_JK) x pair-matrix rows (nD x n^2)
+      TN = tci_gtma_host::tile_n(tma_wide(6));
+      long long kbase = -1, nk = -1;
+      for (const auto& g : s.gp) {
+        if (g.M <= 0 || g.N <= 0) continue;
+        const DGemmProblem& dp = pr[gi++];
+        if (g.N != plan.nD || g.ldc != plan.nD || g.seg_end - g.seg_begin != 1) return;
+        const GemmSeg& x = s.gs[(size_t)g.seg_begin];
+        if (x.a != BUF_JK || x.b != BUF_D || x.tA || !x.tB || x.lda != n2 || x.ldb != n2 || x.offB % 32 ||
+            !((x.offB + x.K) % 32 == 0 || x.offB + x.K == n2) || x.offB + x.K > n2)
+          return;
+        if (kbase < 0) {
+          kbase = x.offA - x.offB;
+          nk = g.M;
+        }
+        if (x.offA - x.offB != kbase || g.M != nk) return;
+        TmaProblem q{dp.C, plan.nD, g.M, plan.nD, 0, 0, g.beta, (long long)ts.size(), 0, 0, nullptr, nullptr, 0};
+        ts.push_back(TmaSeg{0, 0, x.offB, x.K, x.alpha});
+        q.seg_end = (long long)ts.size();
+        push(q);
+      }
+      if (kbase < 0 || kbase + nk * n2 > plan.buf_size[BUF_JK]) return;
+      d.tma_aux = kbase;
+      d.tma_rows = nk;
+      d.tma_kind = 6;
     } else if (s.name == "ss two-external") {
       // Y rows (M x n) = gathered rows (M x n) X^T with X an n x n integral matrix of BUF_JK, computed as
       // Y^T = X Cg^T: A = rows of X, B = the gathered rows.  Problems of at most SKINNY_M rows (the
@@ -1202,11 +1231,11 @@ struct tci_ctx {
   }
   // TMA-fed kernel's tile width per step kind: 128 unless the B operand has at most 64 rows per problem
   bool tma_wide(int kind) const {
-    return (kind == 1 || kind == 5) ? plan.n > 64 : kind == 4 ? false : plan.nD > 64;
+    return (kind == 1 || kind == 5) ? plan.n > 64 : kind == 4 ? false : plan.nD > 64;  // 2, 3, 6: B = pair rows
   }
   bool tma_ok(const DevStep& s) const {
     return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready) ||
-           (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready);
+           (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready) || (s.tma_kind == 6 && tma_dv_ready);
   }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
@@ -1364,13 +1393,19 @@ struct tci_ctx {
     TCI_CUDA(dev_malloc(&tc_status, sizeof(int), stream));
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
-    bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false, want_1x = false;
+    bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false, want_1x = false, want_dv = false;
+    long long dv_base = 0, dv_rows = 0;
     long long ss_rows = 0;
     for (const auto& st : sigma) {
       want_dd = want_dd || (st.tma_probs && st.tma_kind == 1);
       want_t3 = want_t3 || (st.tma_probs && st.tma_kind == 2);
       want_t3r = want_t3r || (st.tma_probs && st.tma_kind == 3);
       want_1x = want_1x || (st.tma_probs && st.tma_kind == 5);
+      if (st.tma_probs && st.tma_kind == 6) {
+        want_dv = true;
+        dv_base = st.tma_aux;
+        dv_rows = st.tma_rows;
+      }
       if (st.tma_probs && st.tma_kind == 4) {
         want_ss = true;
         ss_rows = std::max(ss_rows, st.tma_rows);
@@ -1413,12 +1448,24 @@ struct tci_ctx {
         throw Error(TCI_ERR_CUDA, err);
       tma_ss_ready = true;
     }
+    if ((want_t3 || want_dv) && plan.nD > 0) {  // pair matrices as rows of n^2, split every build
+      const i64 ld = tci_gtma_host::pitch(n2);
+      alloc_f(&df_hi, (size_t)(plan.nD * ld));
+      alloc_f(&df_lo, (size_t)(plan.nD * ld));
+    }
+    if (want_dv && plan.nD > 0 && dv_rows > 0) {  // the exchange bank of the dv step, split once
+      const i64 ld = tci_gtma_host::pitch(n2);
+      alloc_f(&kb_hi, (size_t)(dv_rows * ld));
+      alloc_f(&kb_lo, (size_t)(dv_rows * ld));
+      TCI_CUDA(tci_gtma_host::split(buf[BUF_JK] + dv_base, dv_rows, n2, n2, kb_hi, kb_lo, stream));
+      if (!tci_gtma_host::prepare(tma_dv, kb_hi, kb_lo, dv_rows, n2, df_hi, df_lo, plan.nD, n2, tma_wide(6), err))
+        throw Error(TCI_ERR_CUDA, err);
+      tma_dv_ready = true;
+    }
     if (want_t3 && plan.nD > 0) {
       const i64 ld = tci_gtma_host::pitch(n2), vrows = plan.nint * n;
       alloc_f(&v_hi, (size_t)(vrows * ld));
       alloc_f(&v_lo, (size_t)(vrows * ld));
-      alloc_f(&df_hi, (size_t)(plan.nD * ld));
-      alloc_f(&df_lo, (size_t)(plan.nD * ld));
       TCI_CUDA(tci_gtma_host::split(buf[BUF_V], vrows, n2, n2, v_hi, v_lo, stream));
       if (!tci_gtma_host::prepare(tma_t3, v_hi, v_lo, vrows, n2, df_hi, df_lo, plan.nD, n2, tma_wide(2), err))
         throw Error(TCI_ERR_CUDA, err);
@@ -1523,6 +1570,10 @@ struct tci_ctx {
           } else if (s.tma_kind == 2) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_t3, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          } else if (s.tma_kind == 6) {
+            TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_dv, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
           } else if (s.tma_kind == 5) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * n, n, n, d_hi, d_lo, stream));
@@ -1669,12 +1720,15 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                               2.0 * (double)tci_gtma_host::pitch(P.n) *
                                   (double)(P.buf_size[BUF_WV] / std::max<i64>(1, P.n)));
     // gathered single-vector rows of the singles-singles step (problems above the skinny size)
-    double ss_rows = 0;
-    for (const auto& st : P.sigma_steps)
+    double ss_rows = 0, dv_rows = 0;
+    for (const auto& st : P.sigma_steps) {
       if (st.name == "ss two-external")
         for (const auto& g : st.gp)
           if (g.M > SKINNY_M) ss_rows += (double)g.M;
-    const double f32_all = f32 + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows;
+      if (st.name == "dv forward" && !st.gp.empty()) dv_rows = (double)st.gp[0].M;  // the exchange bank's rows
+    }
+    const double f32_all = f32 + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows +
+                           4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * dv_rows;
     pk = std::max(pk, res + f32_all);  // FP64 and FP32 operators coexist until the FP64 copy is released
     res += f32_all - (refine == 1 ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
