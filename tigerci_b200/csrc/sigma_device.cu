@@ -712,10 +712,12 @@ struct DevStep {
   // 1: two-external (integrals x pair matrices), 2: forward three-external (V_i x pair rows), 3: reverse
   // three-external (transposed V_i rows x gathered coefficient rows), 4: singles-singles two-external
   // (integral rows x gathered single-vector rows, computed transposed), 5: forward one-external
-  // (coupling-vector rows x pair matrices), 6: dv forward (exchange-bank rows x pair-matrix rows)
+  // (coupling-vector rows x pair matrices), 6: dv forward (exchange-bank rows x pair-matrix rows), 7: dv
+  // reverse (transposed exchange-bank rows x transposed gathered rows, transposed output)
   int tma_kind = 0;
   long long tma_aux = 0;   // kinds 3, 4: offset of the gathered coefficients in BUF_T0
-  long long tma_rows = 0;  // kind 4: rows of the gathered coefficients
+  long long tma_rows = 0;  // kinds 4, 6, 7: rows of the gathered coefficients / of the exchange bank
+  long long tma_aux2 = 0;  // kind 7: offset of the exchange bank in BUF_JK
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
   DGemmProblem* skinny_probs = nullptr;
   int skinny_nprob = 0;
@@ -782,9 +784,10 @@ struct tci_ctx {
   float *cg_hi = nullptr, *cg_lo = nullptr;                                        // singles-singles
   float *wv_hi = nullptr, *wv_lo = nullptr;                                        // one-external vectors
   float *kb_hi = nullptr, *kb_lo = nullptr;                                        // dv exchange bank
-  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss, tma_1x, tma_dv;
+  float *kbt_hi = nullptr, *kbt_lo = nullptr, *g2t_hi = nullptr, *g2t_lo = nullptr;  // dv reverse
+  tci_gtma_host::TmaMaps tma_dd, tma_t3, tma_t3r, tma_ss, tma_1x, tma_dv, tma_dvr;
   bool tma_dd_ready = false, tma_t3_ready = false, tma_t3r_ready = false, tma_ss_ready = false, tma_1x_ready = false,
-       tma_dv_ready = false;
+       tma_dv_ready = false, tma_dvr_ready = false;
   float* w32p = nullptr;                // FP32 W+ / W- (precision 1)
   float* w32m = nullptr;
   float* u2s = nullptr;                 // split singlet CI blocks for the tensor-core product
@@ -972,6 +975,26 @@ struct tci_ctx {
       d.tma_aux = kbase;
       d.tma_rows = nk;
       d.tma_kind = 6;
+    } else if (s.name == "dv reverse") {
+      // R (nD x n^2) += G2^T (nD x nk) Kbank (nk x n^2), computed as R^T = Kbank^T G2: A = rows of the
+      // transposed exchange bank (split once), B = rows of the transposed gathered G2 (split every build)
+      TN = tci_gtma_host::tile_n(tma_wide(7));
+      if (s.gp.size() != 1) return;
+      const GemmProblem& g = s.gp[0];
+      const DGemmProblem& dp = pr[gi++];
+      if (g.M != plan.nD || g.N != n2 || g.ldc != n2 || g.seg_end - g.seg_begin != 1) return;
+      const GemmSeg& x = s.gs[(size_t)g.seg_begin];
+      if (x.a != BUF_T0 || x.b != BUF_JK || !x.tA || x.tB || x.lda != plan.nD || x.ldb != n2 ||
+          x.offB + x.K * n2 > plan.buf_size[BUF_JK] || x.offA + x.K * plan.nD > plan.buf_size[BUF_T0])
+        return;
+      TmaProblem q{dp.C, n2, n2, plan.nD, 0, 0, g.beta, (long long)ts.size(), 0, 1, nullptr, nullptr, 0};
+      ts.push_back(TmaSeg{0, 0, 0, x.K, x.alpha});
+      q.seg_end = (long long)ts.size();
+      push(q);
+      d.tma_aux = x.offA;    // G2 in BUF_T0 (K x nD)
+      d.tma_rows = x.K;      // nk
+      d.tma_aux2 = x.offB;   // the exchange bank in BUF_JK (K x n^2)
+      d.tma_kind = 7;
     } else if (s.name == "ss two-external") {
       // Y rows (M x n) = gathered rows (M x n) X^T with X an n x n integral matrix of BUF_JK, computed as
       // Y^T = X Cg^T: A = rows of X, B = the gathered rows.  Problems of at most SKINNY_M rows (the
@@ -1231,11 +1254,12 @@ struct tci_ctx {
   }
   // TMA-fed kernel's tile width per step kind: 128 unless the B operand has at most 64 rows per problem
   bool tma_wide(int kind) const {
-    return (kind == 1 || kind == 5) ? plan.n > 64 : kind == 4 ? false : plan.nD > 64;  // 2, 3, 6: B = pair rows
+    return (kind == 1 || kind == 5) ? plan.n > 64 : kind == 4 ? false : plan.nD > 64;  // 2, 3, 6, 7: B has nD rows
   }
   bool tma_ok(const DevStep& s) const {
     return (s.tma_kind == 1 && tma_dd_ready) || (s.tma_kind == 2 && tma_t3_ready) || (s.tma_kind == 3 && tma_t3r_ready) ||
-           (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready) || (s.tma_kind == 6 && tma_dv_ready);
+           (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready) || (s.tma_kind == 6 && tma_dv_ready) ||
+           (s.tma_kind == 7 && tma_dvr_ready);
   }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
@@ -1394,13 +1418,19 @@ struct tci_ctx {
     owned.push_back(tc_status);
     TCI_CUDA(tci_gtc_host::prepare());
     bool want_dd = false, want_t3 = false, want_t3r = false, want_ss = false, want_1x = false, want_dv = false;
-    long long dv_base = 0, dv_rows = 0;
+    bool want_dvr = false;
+    long long dv_base = 0, dv_rows = 0, dvr_base = 0, dvr_rows = 0;
     long long ss_rows = 0;
     for (const auto& st : sigma) {
       want_dd = want_dd || (st.tma_probs && st.tma_kind == 1);
       want_t3 = want_t3 || (st.tma_probs && st.tma_kind == 2);
       want_t3r = want_t3r || (st.tma_probs && st.tma_kind == 3);
       want_1x = want_1x || (st.tma_probs && st.tma_kind == 5);
+      if (st.tma_probs && st.tma_kind == 7) {
+        want_dvr = true;
+        dvr_base = st.tma_aux2;
+        dvr_rows = st.tma_rows;
+      }
       if (st.tma_probs && st.tma_kind == 6) {
         want_dv = true;
         dv_base = st.tma_aux;
@@ -1461,6 +1491,18 @@ struct tci_ctx {
       if (!tci_gtma_host::prepare(tma_dv, kb_hi, kb_lo, dv_rows, n2, df_hi, df_lo, plan.nD, n2, tma_wide(6), err))
         throw Error(TCI_ERR_CUDA, err);
       tma_dv_ready = true;
+    }
+    if (want_dvr && plan.nD > 0 && dvr_rows > 0) {  // transposed exchange bank, once; transposed G2 per build
+      const i64 ld = tci_gtma_host::pitch(dvr_rows);
+      alloc_f(&kbt_hi, (size_t)(n2 * ld));
+      alloc_f(&kbt_lo, (size_t)(n2 * ld));
+      alloc_f(&g2t_hi, (size_t)(plan.nD * ld));
+      alloc_f(&g2t_lo, (size_t)(plan.nD * ld));
+      TCI_CUDA(tci_gtma_host::split_transposed(buf[BUF_JK] + dvr_base, 1, dvr_rows, n2, kbt_hi, kbt_lo, stream));
+      if (!tci_gtma_host::prepare(tma_dvr, kbt_hi, kbt_lo, n2, dvr_rows, g2t_hi, g2t_lo, plan.nD, dvr_rows,
+                                  tma_wide(7), err))
+        throw Error(TCI_ERR_CUDA, err);
+      tma_dvr_ready = true;
     }
     if (want_t3 && plan.nD > 0) {
       const i64 ld = tci_gtma_host::pitch(n2), vrows = plan.nint * n;
@@ -1570,6 +1612,11 @@ struct tci_ctx {
           } else if (s.tma_kind == 2) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_t3, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
+                                           tc_status, stream));
+          } else if (s.tma_kind == 7) {
+            TCI_CUDA(tci_gtma_host::split_transposed(buf[BUF_T0] + s.tma_aux, 1, s.tma_rows, plan.nD, g2t_hi, g2t_lo,
+                                                     stream));
+            TCI_CUDA(tci_gtma_host::launch(tma_dvr, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
           } else if (s.tma_kind == 6) {
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD, n * n, n * n, df_hi, df_lo, stream));
@@ -1728,7 +1775,8 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
       if (st.name == "dv forward" && !st.gp.empty()) dv_rows = (double)st.gp[0].M;  // the exchange bank's rows
     }
     const double f32_all = f32 + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows +
-                           4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * dv_rows;
+                           4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * dv_rows +
+                           4.0 * 2.0 * (double)tci_gtma_host::pitch((i64)dv_rows) * (double)(P.n * P.n + P.nD);
     pk = std::max(pk, res + f32_all);  // FP64 and FP32 operators coexist until the FP64 copy is released
     res += f32_all - (refine == 1 ? 0.0 : 8.0 * (double)std::max<i64>(0, P.buf_size[BUF_W]));
   }
