@@ -797,6 +797,7 @@ struct tci_ctx {
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
   cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
+  std::vector<i64> lowest_diag;  // CSF indices of the lowest diagonal elements, ascending (initial guesses)
   double* dots = nullptr;        // reduction scratch: partial sums and results
   double* coefs = nullptr;       // small device coefficient arrays
   int scratch_cap = 0;           // vectors dots / coefs are sized for
@@ -2141,13 +2142,18 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
     try {
       cudaStream_t st = ctx->stream;
       const unsigned G = 148 * 8, TB = 256;
-      // initial guess: unit vectors at the lowest diagonal elements
-      std::vector<double> hd(n);
-      TCI_CUDA(cudaMemcpy(hd.data(), ctx->hd, n * sizeof(double), cudaMemcpyDeviceToHost));
-      std::vector<i64> idx(n);
-      for (i64 i = 0; i < n; ++i) idx[i] = i;
-      std::partial_sort(idx.begin(), idx.begin() + nroots, idx.end(),
-                        [&](i64 a, i64 b) { return hd[a] < hd[b] || (hd[a] == hd[b] && a < b); });
+      // initial guess: unit vectors at the lowest diagonal elements (the order is a property of the
+      // operator: kept in the context for the next solve)
+      if ((i64)ctx->lowest_diag.size() < nroots) {
+        std::vector<double> hd(n);
+        TCI_CUDA(cudaMemcpy(hd.data(), ctx->hd, n * sizeof(double), cudaMemcpyDeviceToHost));
+        std::vector<i64> all(n);
+        for (i64 i = 0; i < n; ++i) all[i] = i;
+        std::partial_sort(all.begin(), all.begin() + nroots, all.end(),
+                          [&](i64 a, i64 b) { return hd[a] < hd[b] || (hd[a] == hd[b] && a < b); });
+        ctx->lowest_diag.assign(all.begin(), all.begin() + nroots);
+      }
+      const std::vector<i64>& idx = ctx->lowest_diag;
       TCI_CUDA(cudaMemsetAsync(Cs, 0, (size_t)nroots * n * sizeof(double), st));
       const double one = 1.0;
       for (i64 k = 0; k < nroots; ++k)
