@@ -116,7 +116,8 @@ int tci_sigma_init(const tci_deck* deck, const tci_operator* op, int64_t device,
  * the all-external term with FP32 W operators, and the three-, two- and
  * one-external GEMM steps from their FP64 operands.  options[2] selects those
  * other GEMM steps: 0 by size (default), 1 all of them, 2 none.  The coupling-
- * coefficient products, same-head one-electron-like operators, gathers,
+ * coefficient products, same-head one-electron-like operators (on the
+ * tensor cores in the two-external step when options[3] != 0), gathers,
  * scatters and reductions stay FP64.  options[3] picks how tci_davidson
  * reports the roots of the mixed form: 2 (default) as the Rayleigh quotient of
  * each Ritz vector with one sigma build in which every term is FP64 but the

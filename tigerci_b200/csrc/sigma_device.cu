@@ -777,6 +777,9 @@ struct tci_ctx {
   // 2 with every term FP64 but the all-external one, which stays on its tensor-core kernel (no FP64 W kept)
   int64_t refine = 2;
   bool allext_tc_in_fp64 = false;       // set during a refine-2 finish build
+  // mixed form with an FP64 finish: the same-head one-electron-like products of the dd step run on the
+  // tensor cores as well (the finish's FP64 sigma build carries them in FP64 for the reported roots)
+  bool f_on_tc = false;
   // split operands of the TMA-fed steps: integrals and V_i once, the pair matrices every build
   float *jk_hi = nullptr, *jk_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr;
   float *v_hi = nullptr, *v_lo = nullptr, *df_hi = nullptr, *df_lo = nullptr;
@@ -867,9 +870,16 @@ struct tci_ctx {
         if (g.M != n || g.N != n || g.ldc != n) return;
         TmaProblem q{dp.C, n, n, n, 0, 0, g.beta, (long long)ts.size(), 0, 0, nullptr, nullptr, 0};
         bool has_f = false;
+        const i64 xrows = plan.buf_size[BUF_JK] / n;  // F rows follow the integral rows in the split array
         for (i64 k = g.seg_begin; k < g.seg_end; ++k) {
           const GemmSeg& x = s.gs[(size_t)k];
           if (x.a == BUF_F || x.b == BUF_F) {
+            if (f_on_tc && x.a == BUF_F && x.b == BUF_D && x.K == n && x.lda == n && x.ldb == n && !x.tA && !x.tB &&
+                x.offA % n == 0 && x.offB % n2 == 0) {
+              ts.push_back(TmaSeg{xrows + x.offA / n, x.offB / n, 0, n, x.alpha * psign[(size_t)(x.offB / n2)]});
+              continue;
+            }
+            if (f_on_tc) return;  // an F segment of another shape: leave the step on the older path
             has_f = true;
             continue;
           }
@@ -1110,6 +1120,7 @@ struct tci_ctx {
         // Mixed form.  Segments whose operand is a same-head one-electron-like operator (BUF_F: h, J_ii,
         // K_ii combinations, orbital-energy magnitudes) stay on the FP64 kernel; the cross-head integral
         // segments go to the tensor cores (3xTF32), added after the FP64 part (beta 1 where both exist).
+        // With f_on_tc the dd step's TMA lowering takes the F segments onto the tensor cores as well.
         // Problems of at most SKINNY_M rows stay whole on the skinny FP64 kernel (launched in this form too).
         std::vector<tci_dev::HostGemm> f64, tcp;
         for (const auto& g : pr) {
@@ -1277,7 +1288,8 @@ struct tci_ctx {
         continue;
       }
       if (s.kind == STEP_GEMM && uses_tc(s)) {
-        k += (s.skinny_nwarps > 0 ? 1 : 0) + (s.ntiles_f > 0 ? 1 : 0) +
+        const bool f_in_tma = f_on_tc && s.tma_kind == 1 && s.tma_probs && tma_ok(s);
+        k += (s.skinny_nwarps > 0 ? 1 : 0) + ((s.ntiles_f > 0 && !f_in_tma) ? 1 : 0) +
              ((s.tma_probs && tma_ok(s)) ? 2 : (s.ntiles_tc > 0 ? 1 : 0));
         continue;
       }
@@ -1445,11 +1457,15 @@ struct tci_ctx {
     const i64 n = plan.n, n2 = n * n;
     std::string err;
     const i64 xrows = plan.buf_size[BUF_JK] / std::max<i64>(1, n);
+    // with f_on_tc the same-head operators (BUF_F) follow the integral matrices in the same split array
+    const i64 frows = f_on_tc ? plan.buf_size[BUF_F] / std::max<i64>(1, n) : 0;
     if ((want_dd && plan.nD > 0) || (want_ss && xrows > 0)) {  // the integral matrices, split once
       const i64 ld = tci_gtma_host::pitch(n);
-      alloc_f(&jk_hi, (size_t)(xrows * ld));
-      alloc_f(&jk_lo, (size_t)(xrows * ld));
+      alloc_f(&jk_hi, (size_t)((xrows + frows) * ld));
+      alloc_f(&jk_lo, (size_t)((xrows + frows) * ld));
       TCI_CUDA(tci_gtma_host::split(buf[BUF_JK], xrows, n, n, jk_hi, jk_lo, stream));
+      if (frows > 0)
+        TCI_CUDA(tci_gtma_host::split(buf[BUF_F], frows, n, n, jk_hi + xrows * ld, jk_lo + xrows * ld, stream));
     }
     if ((want_dd || want_1x) && plan.nD > 0) {  // the pair matrices, split every build
       const i64 ld = tci_gtma_host::pitch(n), drows = plan.nD * n;
@@ -1458,7 +1474,8 @@ struct tci_ctx {
     }
     if (want_dd && plan.nD > 0) {
       const i64 drows = plan.nD * n;
-      if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows, n, d_hi, d_lo, drows, n, tma_wide(1), err)) throw Error(TCI_ERR_CUDA, err);
+      if (!tci_gtma_host::prepare(tma_dd, jk_hi, jk_lo, xrows + frows, n, d_hi, d_lo, drows, n, tma_wide(1), err))
+        throw Error(TCI_ERR_CUDA, err);
       tma_dd_ready = true;
     }
     const i64 wvrows = plan.buf_size[BUF_WV] / std::max<i64>(1, n);
@@ -1606,7 +1623,7 @@ struct tci_ctx {
             s.tma_probs && tma_ok(s)) {
           const i64 n = plan.n;
           if (s.tma_kind == 1) {
-            TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
+            if (!f_on_tc) TCI_CUDA(tci_dev::launch_gemm_f64(s.cfg, s.probs_f, s.nprob_f, s.segs_f, s.ntiles_f, stream));
             TCI_CUDA(tci_gtma_host::split(buf[BUF_D], plan.nD * n, n, n, d_hi, d_lo, stream));
             TCI_CUDA(tci_gtma_host::launch(tma_dd, s.tma_probs, s.tma_nprob, s.tma_segs, s.tma_ntiles, (int)tc_kblock,
                                            tc_status, stream));
@@ -1767,6 +1784,9 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
                               // one-external coupling vectors
                               2.0 * (double)tci_gtma_host::pitch(P.n) *
                                   (double)(P.buf_size[BUF_WV] / std::max<i64>(1, P.n)));
+    // the same-head operators beside the integrals in the split array (mixed form with a finish)
+    const double f32_f =
+        refine != 0 ? 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * (double)(P.buf_size[BUF_F] / std::max<i64>(1, P.n)) : 0.0;
     // gathered single-vector rows of the singles-singles step (problems above the skinny size)
     double ss_rows = 0, dv_rows = 0;
     for (const auto& st : P.sigma_steps) {
@@ -1775,7 +1795,7 @@ void ctx_device_bytes(const Plan& P, int64_t precision, double* peak, double* re
           if (g.M > SKINNY_M) ss_rows += (double)g.M;
       if (st.name == "dv forward" && !st.gp.empty()) dv_rows = (double)st.gp[0].M;  // the exchange bank's rows
     }
-    const double f32_all = f32 + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows +
+    const double f32_all = f32 + f32_f + 4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n) * ss_rows +
                            4.0 * 2.0 * (double)tci_gtma_host::pitch(P.n * P.n) * dv_rows +
                            4.0 * 2.0 * (double)tci_gtma_host::pitch((i64)dv_rows) * (double)(P.n * P.n + P.nD);
     pk = std::max(pk, res + f32_all);  // FP64 and FP32 operators coexist until the FP64 copy is released
@@ -1859,6 +1879,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     GemmSeg xs{};
     bool have_x = false;
     size_t banks = (size_t)-1;
+    ctx->f_on_tc = precision == 1 && refine != 0;
     for (auto& s : P.init_steps) {
       if (x_tc && s.kind == STEP_GEMM && s.name == "integral banks") {
         Step s2 = s;
