@@ -39,6 +39,37 @@ namespace {
 const double kSqrt2 = std::sqrt(2.0);
 constexpr double kTiny = 1e-14;
 
+// Open-addressing map from a packed occupation key (2 bits per internal orbital) to a head index, for the
+// lookups of the zero-external enumeration (one per candidate excitation): linear probing in a power-of-two
+// table at most half full.
+struct KeyIndex {
+  std::vector<uint64_t> keys;
+  std::vector<i64> vals;
+  uint64_t mask = 0;
+  static constexpr uint64_t kEmpty = ~0ull;
+  static uint64_t slot(uint64_t k) { return (k * 0x9E3779B97F4A7C15ull) >> 20; }
+  void build(const std::vector<std::pair<uint64_t, i64>>& kv) {
+    size_t cap = 16;
+    while (cap < 2 * kv.size()) cap <<= 1;
+    keys.assign(cap, kEmpty);
+    vals.assign(cap, -1);
+    mask = cap - 1;
+    for (const auto& e : kv) {
+      uint64_t h = slot(e.first) & mask;
+      while (keys[h] != kEmpty && keys[h] != e.first) h = (h + 1) & mask;
+      keys[h] = e.first;
+      vals[h] = e.second;
+    }
+  }
+  i64 find(uint64_t k) const {
+    if (keys.empty()) return -1;
+    for (uint64_t h = slot(k) & mask;; h = (h + 1) & mask) {
+      if (keys[h] == k) return vals[h];
+      if (keys[h] == kEmpty) return -1;
+    }
+  }
+};
+
 struct VecHash {
   size_t operator()(const std::vector<int8_t>& v) const {
     size_t h = 1469598103934665603ull;
@@ -78,11 +109,43 @@ struct Ints {
         for (i64 k = 0; k < ni; ++k)
           for (i64 l = 0; l < ni; ++l) I4[((i * ni + j) * ni + k) * ni + l] = eri(i, j, k, l);
     I3.assign(ni * ni * ni * n, 0.0);
-#pragma omp parallel for collapse(2) schedule(dynamic)
+    // (iq|jk) = L[pair(i, q)] . L[pair(j, k)]: the internal pair rows (the first ni(ni+1)/2 rows of L)
+    // transposed once, then 4 rows L[pair(i, q)] x 8 internal pairs per register block, every dot still
+    // summed in J order (the same value as eri())
+    const i64 npr = ni * (ni + 1) / 2, npr8 = (npr + 7) / 8 * 8, nq4 = (n + 3) / 4;
+    std::vector<double> Lt((size_t)(N * npr8), 0.0);
+    std::vector<int> pj((size_t)npr), pk((size_t)npr);
+    for (i64 j = 0; j < ni; ++j)
+      for (i64 k = 0; k <= j; ++k) {
+        pj[(size_t)pair(j, k)] = (int)j;
+        pk[(size_t)pair(j, k)] = (int)k;
+      }
+    for (i64 pr = 0; pr < npr; ++pr)
+      for (i64 J = 0; J < N; ++J) Lt[(size_t)(J * npr8 + pr)] = L[pr * N + J];
+#pragma omp parallel for collapse(3) schedule(dynamic)
     for (i64 i = 0; i < ni; ++i)
-      for (i64 q = 0; q < n; ++q)
-        for (i64 j = 0; j < ni; ++j)
-          for (i64 k = 0; k < ni; ++k) I3[((i * ni + j) * ni + k) * n + q] = eri(i, ni + q, j, k);
+      for (i64 qb = 0; qb < nq4; ++qb)
+        for (i64 pb = 0; pb < npr8; pb += 8) {
+          const double* a[4];
+          for (int r = 0; r < 4; ++r) a[r] = L + pair(i, ni + std::min<i64>(qb * 4 + r, n - 1)) * N;
+          double acc[4][8] = {};
+          for (i64 J = 0; J < N; ++J) {
+            const double* lt = &Lt[(size_t)(J * npr8 + pb)];
+            for (int r = 0; r < 4; ++r) {
+              const double x = a[r][J];
+              for (int c = 0; c < 8; ++c) acc[r][c] += x * lt[c];
+            }
+          }
+          for (int r = 0; r < 4; ++r) {
+            const i64 q = qb * 4 + r;
+            if (q >= n) break;
+            for (int c = 0; c < 8 && pb + c < npr; ++c) {
+              const i64 j = pj[(size_t)(pb + c)], k = pk[(size_t)(pb + c)];
+              I3[(size_t)(((i * ni + j) * ni + k) * n + q)] = acc[r][c];
+              I3[(size_t)(((i * ni + k) * ni + j) * n + q)] = acc[r][c];
+            }
+          }
+        }
   }
 };
 
@@ -107,7 +170,7 @@ struct Builder {
   int e0 = 0, e1 = 0, e2 = 0;
   std::unordered_map<std::vector<int8_t>, i64, VecHash> idx[3];
   // the same index keyed by the packed occupation (2 bits per internal orbital; nint <= 32)
-  std::unordered_map<uint64_t, i64> pidx[3];
+  KeyIndex pidx[3];
   std::vector<i64> dk0, nDh;  // per N-2 path
   i64 nF = 0;                 // matrices used in BUF_F
   Scratch T;                  // BUF_T0 regions used per sigma build
@@ -181,16 +244,19 @@ struct Builder {
 };
 
 void Builder::setup_heads() {
-  for (int k = 0; k < 3; ++k)
+  for (int k = 0; k < 3; ++k) {
+    std::vector<std::pair<uint64_t, i64>> kv;
     for (size_t p = 0; p < sp.paths[k].size(); ++p)
       if (sp.paths[k][p].kept) {
         idx[k][sp.paths[k][p].occ] = (i64)p;
         if (nint <= 32) {
           uint64_t key = 0;
           for (i64 q = 0; q < nint; ++q) key |= (uint64_t)sp.paths[k][p].occ[(size_t)q] << (2 * q);
-          pidx[k][key] = (i64)p;
+          kv.push_back({key, (i64)p});
         }
       }
+    pidx[k].build(kv);
+  }
   const auto& D = sp.paths[2];
   dk0.assign(D.size(), -1);
   nDh.assign(D.size(), 0);
@@ -233,30 +299,71 @@ void Builder::internal_blocks() {
     auto cfg = [&](const Head& h) {
       return pt.kind == 0 ? cfgV(h) : pt.kind == 1 ? cfgS(h, pt.x) : cfgD(h, pt.x, pt.y);
     };
-    // Heads in parallel: every source head hs owns the blocks keyed (target, hs), so the per-thread maps
-    // merge without collisions and the merged (ordered) map does not depend on the schedule.
-    std::vector<std::map<std::pair<i64, i64>, std::vector<double>>> tblocks((size_t)omp_get_max_threads());
-    std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
+    // Heads in parallel: every source head hs owns its blocks (by target, in target order), so the result
+    // does not depend on the schedule.
+    std::vector<std::vector<std::pair<i64, std::vector<double>>>> by_src(heads.size());
+    const int nthr = omp_get_max_threads();
+    std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)nthr);
     for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
     // per thread: the expansion of each head of this pattern, looked up once
     std::vector<std::vector<const CsfExpansion*>> hexp((size_t)omp_get_max_threads(),
                                                        std::vector<const CsfExpansion*>(heads.size(), nullptr));
     const bool packed = nint <= 32;
     const uint64_t mask2 = packed ? (nint == 32 ? ~0ull : ((1ull << (2 * nint)) - 1)) & 0x5555555555555555ull : 0;
+    // per thread: the slot of each target head in the current source head's block list (-1: none yet)
+    std::vector<std::vector<int>> slot((size_t)nthr, std::vector<int>(heads.size(), -1));
+    // per thread: bit (p, q, r, s) set when removing electrons from spatial orbitals p <= q and adding them to
+    // r <= s turns the current source head into a kept head of the pattern (the target of a double
+    // excitation depends only on its spatial orbitals, so one lookup per spatial move serves every
+    // determinant and spin assignment)
+    const size_t nq = packed ? (size_t)ni * ni * ni * ni : 0;
+    std::vector<std::vector<uint64_t>> dbits((size_t)nthr, std::vector<uint64_t>((nq + 63) / 64, 0));
+    // and whether any such move starts with (p, q) or with (p, q, r): whole loop levels skipped
+    std::vector<std::vector<uint8_t>> dany((size_t)nthr, std::vector<uint8_t>(packed ? (size_t)ni * ni * (ni + 1) : 0, 0));
 #pragma omp parallel for schedule(dynamic, 4)
     for (long long hsl = 0; hsl < (long long)heads.size(); ++hsl) {
       const size_t hs = (size_t)hsl;
-      auto& blocks = tblocks[(size_t)omp_get_thread_num()];
-      CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
-      auto& hx = hexp[(size_t)omp_get_thread_num()];
-      // this source head's blocks by target, moved into the thread's map when the head is done
-      std::unordered_map<i64, std::vector<double>> local;
+      const int th = omp_get_thread_num();
+      CouplingEngine& E = *engines[(size_t)th];  // per-thread expansion cache
+      auto& hx = hexp[(size_t)th];
+      auto& sl = slot[(size_t)th];
+      auto& db = dbits[(size_t)th];
+      uint8_t* any3 = dany[(size_t)th].data();             // (p, q, r)
+      uint8_t* any2 = any3 + (packed ? (size_t)ni * ni * ni : 0);  // (p, q)
+      // this source head's blocks by target
+      auto& local = by_src[hs];
       const Head& S = heads[hs];
       if (!S.kept || nsf_of(S) == 0) continue;
       const CsfExpansion& eS = E.expand(cfg(S));
       if (eS.nsf != nsf_of(S)) {
         bad_count = true;
         continue;
+      }
+      auto kept_target = [&](i64 t) { return t >= 0 && heads[(size_t)t].kept && nsf_of(heads[(size_t)t]) != 0; };
+      if (packed) {  // the spatial double moves of this head that stay in the pattern's kept heads
+        std::fill(db.begin(), db.end(), 0ull);
+        std::fill(dany[(size_t)th].begin(), dany[(size_t)th].end(), (uint8_t)0);
+        uint64_t key = 0;
+        for (int p = 0; p < ni; ++p) key |= (uint64_t)S.occ[(size_t)p] << (2 * p);
+        for (int p = 0; p < ni; ++p) {
+          if (S.occ[(size_t)p] == 0) continue;
+          for (int q = p; q < ni; ++q) {
+            if (S.occ[(size_t)q] < (q == p ? 2 : 1)) continue;
+            const uint64_t k2 = key - (1ull << (2 * p)) - (1ull << (2 * q));
+            auto o = [&](int x) { return (int)((k2 >> (2 * x)) & 3); };
+            for (int r = 0; r < ni; ++r) {
+              if (o(r) == 2) continue;
+              for (int t = r; t < ni; ++t) {
+                if (o(t) > (t == r ? 0 : 1)) continue;
+                if (!kept_target(pidx[pt.kind].find(k2 + (1ull << (2 * r)) + (1ull << (2 * t))))) continue;
+                const size_t bit = (((size_t)p * ni + q) * ni + r) * ni + t;
+                db[bit >> 6] |= 1ull << (bit & 63);
+                any3[((size_t)p * ni + q) * ni + r] = 1;
+                any2[(size_t)p * ni + q] = 1;
+              }
+            }
+          }
+        }
       }
       for (size_t r = 0; r < eS.dets.size(); ++r) {
         const double* thS = eS.basis->coeff.data() + r * eS.nsf;
@@ -271,8 +378,8 @@ void Builder::internal_blocks() {
           const Head* Tg = nullptr;
           if (packed) {  // per-orbital electron counts of the determinant, 2 bits each
             const uint64_t lo = (uint64_t)d;
-            auto it = pidx[pt.kind].find((lo & mask2) + ((lo >> 1) & mask2));
-            if (it != pidx[pt.kind].end()) Tg = &heads[(size_t)it->second];
+            const i64 t = pidx[pt.kind].find((lo & mask2) + ((lo >> 1) & mask2));
+            if (t >= 0) Tg = &heads[(size_t)t];
           } else {
             std::vector<int8_t> o(ni);
             for (int p = 0; p < ni; ++p) o[p] = (int8_t)(((d >> (2 * p)) & 1) + ((d >> (2 * p + 1)) & 1));
@@ -285,11 +392,24 @@ void Builder::internal_blocks() {
           const size_t ti = (size_t)(Tg->lex - 1);
           if (!hx[ti]) hx[ti] = &E.expand(cfg(*Tg));
           const CsfExpansion& eT = *hx[ti];
-          auto it = eT.index.find(d);
-          if (it == eT.index.end()) return;
-          const double* thT = eT.basis->coeff.data() + (size_t)it->second * eT.nsf;
-          auto& blk = local[Tg->lex - 1];
-          if (blk.empty()) blk.assign((size_t)eT.nsf * eS.nsf, 0.0);
+          int row = -1;
+          if (eT.dets.size() <= 32) {
+            for (size_t x = 0; x < eT.dets.size(); ++x)
+              if (eT.dets[x] == d) {
+                row = (int)x;
+                break;
+              }
+          } else {
+            auto it = eT.index.find(d);
+            if (it != eT.index.end()) row = it->second;
+          }
+          if (row < 0) return;
+          const double* thT = eT.basis->coeff.data() + (size_t)row * eT.nsf;
+          if (sl[ti] < 0) {
+            sl[ti] = (int)local.size();
+            local.emplace_back((i64)ti, std::vector<double>((size_t)eT.nsf * eS.nsf, 0.0));
+          }
+          auto& blk = local[(size_t)sl[ti]].second;
           const double f = val * eT.sign * eS.sign;
           for (int a = 0; a < eT.nsf; ++a) {
             if (thT[a] == 0.0) continue;
@@ -334,11 +454,17 @@ void Builder::internal_blocks() {
             emit(d, ph * v);
           }
         for (int a = 0; a < no; ++a)  // doubles (xa,xb) -> (xc,xd)
-          for (int b = a + 1; b < no; ++b)
-            for (int c = 0; c < nv; ++c)
+          for (int b = a + 1; b < no; ++b) {
+            if (packed && !any2[(size_t)orb(occ[a]) * ni + orb(occ[b])]) continue;
+            for (int c = 0; c < nv; ++c) {
+              if (packed && !any3[((size_t)orb(occ[a]) * ni + orb(occ[b])) * ni + orb(vir[c])]) continue;
               for (int dd = c + 1; dd < nv; ++dd) {
                 const int xa = occ[a], xb = occ[b], xc = vir[c], xd = vir[dd];
                 if (spn(xa) + spn(xb) != spn(xc) + spn(xd)) continue;
+                if (packed) {
+                  const size_t bit = (((size_t)orb(xa) * ni + orb(xb)) * ni + orb(xc)) * ni + orb(xd);
+                  if (!((db[bit >> 6] >> (bit & 63)) & 1)) continue;
+                }
                 // the target configuration first: most candidates leave the CI space
                 const Det dt = d0 ^ ((((Det)1) << xa) | (((Det)1) << xb) | (((Det)1) << xc) | (((Det)1) << xd));
                 const Head* Tg = target_of(dt);
@@ -359,35 +485,59 @@ void Builder::internal_blocks() {
                 d |= ((Det)1) << xc;
                 emit_to(Tg, d, ph * v);
               }
+            }
+          }
       }
-      for (auto& kv : local) blocks[{kv.first, (i64)hs}] = std::move(kv.second);
+      for (const auto& kv : local) sl[(size_t)kv.first] = -1;
+      std::sort(local.begin(), local.end(),
+                [](const std::pair<i64, std::vector<double>>& x, const std::pair<i64, std::vector<double>>& y) {
+                  return x.first < y.first;
+                });
     }
     if (bad_count) throw Error(4, "spin-function count mismatch in zero-external block");
-    std::map<std::pair<i64, i64>, std::vector<double>> blocks;
-    for (auto& tb : tblocks)
-      for (auto& kv : tb) blocks[kv.first] = std::move(kv.second);
-    for (auto& kv : blocks)
-      if (kv.first.first == kv.first.second) {
-        const i64 ns = nsf_of(heads[kv.first.first]);
-        for (i64 a = 0; a < ns; ++a) beta_diag[{pt.block, kv.first.first, a}] = kv.second[(size_t)a * ns + a];
+    // blocks by target, sources ascending
+    std::vector<std::vector<std::pair<i64, const std::vector<double>*>>> bytgt(heads.size());
+    for (size_t hs = 0; hs < heads.size(); ++hs)
+      for (const auto& tb : by_src[hs]) {
+        bytgt[(size_t)tb.first].push_back({(i64)hs, &tb.second});
+        if (tb.first == (i64)hs) {
+          const i64 ns = nsf_of(heads[hs]);
+          for (i64 a = 0; a < ns; ++a) beta_diag[{pt.block, (i64)hs, a}] = tb.second[(size_t)a * ns + a];
+        }
       }
-    std::map<i64, std::vector<std::pair<i64, const std::vector<double>*>>> bytgt;
-    for (auto& kv : blocks) bytgt[kv.first.first].push_back({kv.first.second, &kv.second});
-    for (auto& tv : bytgt) {
-      const Head& Tg = heads[tv.first];
-      const i64 nsfT = nsf_of(Tg);
-      for (i64 a = 0; a < nsfT; ++a) {
-        AxpyTarget tg{BUF_S, off_of(Tg) + a * len, len, (i64)st.as.size(), 0};
-        for (auto& sv : tv.second) {
-          const Head& S = heads[sv.first];
+    // the sources of every target row, built per target in parallel and appended in target order
+    std::vector<std::vector<AxpySource>> tsrc(heads.size());
+    std::vector<std::vector<i64>> tcount(heads.size());
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long long tl = 0; tl < (long long)heads.size(); ++tl) {
+      const auto& tv = bytgt[(size_t)tl];
+      if (tv.empty()) continue;
+      const i64 nsfT = nsf_of(heads[(size_t)tl]);
+      auto& out = tsrc[(size_t)tl];
+      auto& cnt = tcount[(size_t)tl];
+      cnt.assign((size_t)nsfT, 0);
+      for (i64 a = 0; a < nsfT; ++a)
+        for (const auto& sv : tv) {
+          const Head& S = heads[(size_t)sv.first];
           const i64 nsfS = nsf_of(S);
           for (i64 b = 0; b < nsfS; ++b) {
             const double v = (*sv.second)[(size_t)a * nsfS + b];
             if (std::fabs(v) < kTiny) continue;
-            st.as.push_back(AxpySource{BUF_C, off_of(S) + b * len, v, -1, 0});
-            P.flops_total += 2.0 * len;
+            out.push_back(AxpySource{BUF_C, off_of(S) + b * len, v, -1, 0});
+            ++cnt[(size_t)a];
           }
         }
+    }
+    for (size_t t = 0; t < heads.size(); ++t) {
+      if (bytgt[t].empty()) continue;
+      const Head& Tg = heads[t];
+      size_t next = 0;
+      for (i64 a = 0; a < (i64)tcount[t].size(); ++a) {
+        AxpyTarget tg{BUF_S, off_of(Tg) + a * len, len, (i64)st.as.size(), 0};
+        const i64 c = tcount[t][(size_t)a];
+        st.as.insert(st.as.end(), tsrc[t].begin() + (long)next, tsrc[t].begin() + (long)(next + (size_t)c));
+        next += (size_t)c;
+        P.flops_total += 2.0 * (double)len * (double)c;
         tg.src_end = (i64)st.as.size();
         if (tg.src_end > tg.src_begin) st.at.push_back(tg);
       }
@@ -925,7 +1075,7 @@ void Builder::ss() {
 // ops e_{xi,jk} = a+_x a+_j a_k a_i with (xi|jk), and E_xi with h_xi.
 void Builder::sv() {
   // (mu row, v csf) -> w; valence heads in parallel, each owning the keys of its own CSFs
-  std::vector<std::map<std::pair<i64, i64>, std::vector<double>>> twmap((size_t)omp_get_max_threads());
+  std::vector<std::vector<std::pair<std::pair<i64, i64>, std::vector<double>>>> vout(sp.paths[0].size());
   std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
   for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
   // per thread: the expansion of each N-1 head (with the external electron), looked up once
@@ -933,7 +1083,7 @@ void Builder::sv() {
                                                       std::vector<const CsfExpansion*>(sp.paths[1].size(), nullptr));
 #pragma omp parallel for schedule(dynamic, 4)
   for (long long hvl = 0; hvl < (long long)sp.paths[0].size(); ++hvl) {
-    auto& wmap = twmap[(size_t)omp_get_thread_num()];
+    std::map<std::pair<i64, i64>, std::vector<double>> wmap;
     CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
     const Head& V = sp.paths[0][(size_t)hvl];
     if (!has(V)) continue;
@@ -977,24 +1127,35 @@ void Builder::sv() {
       }
       o[i] += 1;
     }
+    auto& out = vout[(size_t)hvl];
+    out.reserve(wmap.size());
+    for (auto& kv : wmap) out.emplace_back(kv.first, std::move(kv.second));
   }
-  std::map<std::pair<i64, i64>, std::vector<double>> wmap;
-  for (auto& tw : twmap)
-    for (auto& kv : tw) wmap[kv.first] = std::move(kv.second);
-  if (wmap.empty()) return;
+  // every key in (mu row, v csf) order
+  std::vector<std::pair<std::pair<i64, i64>, std::vector<double>*>> keys;
+  for (auto& out : vout)
+    for (auto& kv : out) keys.push_back({kv.first, &kv.second});
+  if (keys.empty()) return;
+  std::sort(keys.begin(), keys.end(),
+            [](const std::pair<std::pair<i64, i64>, std::vector<double>*>& x,
+               const std::pair<std::pair<i64, i64>, std::vector<double>*>& y) { return x.first < y.first; });
   const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
   std::vector<std::pair<std::pair<i64, i64>, i64>> rows;
-  std::vector<const std::vector<double>*> src;
-  for (auto& kv : wmap) {
+  std::vector<std::vector<double>*> src;
+  rows.reserve(keys.size());
+  src.reserve(keys.size());
+  for (auto& kv : keys) {
     rows.push_back({kv.first, wbase + (i64)rows.size()});
-    src.push_back(&kv.second);
+    src.push_back(kv.second);
   }
   // one allocation, rows copied in parallel (hundreds of MB at the kernel-scale size)
   const size_t w0 = P.wv.size();
   P.wv.resize(w0 + src.size() * (size_t)n);
 #pragma omp parallel for schedule(static)
-  for (long long t = 0; t < (long long)src.size(); ++t)
+  for (long long t = 0; t < (long long)src.size(); ++t) {
     std::copy(src[(size_t)t]->begin(), src[(size_t)t]->end(), P.wv.begin() + (std::ptrdiff_t)(w0 + (size_t)t * n));
+    std::vector<double>().swap(*src[(size_t)t]);  // released here, in parallel
+  }
   Step& fw = step(P.sigma_steps, STEP_AXPY, "sv forward");
   std::map<i64, std::vector<size_t>> by_mu;
   for (size_t t = 0; t < rows.size(); ++t) by_mu[rows[t].first.first].push_back(t);

@@ -16,9 +16,36 @@
 // sources of an entry are summed in table order, so a sigma build is
 // deterministic (same result alone or interleaved with other requests).
 #pragma once
+#include <memory>
+#include <new>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
 #include "tci_host.h"
 
 namespace tci {
+
+// Allocator whose value-construction leaves the elements uninitialised: large arrays the plan builder fills
+// in parallel right after sizing them (the first touch of each page then happens on the filling thread).
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new ((void*)p) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+};
 
 enum BufId : int {
   BUF_C = 0,   // input CI vector
@@ -123,7 +150,7 @@ struct Plan {
   std::vector<double> dk_sign;   // +1 singlet-coupled, -1 triplet-coupled per dense matrix
   std::vector<i64> buf_size;     // doubles per buffer
   std::vector<double> h_vv;      // external one-electron block (n x n), uploaded into BUF_JK tail
-  std::vector<double> wv;        // BUF_WV contents
+  std::vector<double, NoInitAlloc<double>> wv;  // BUF_WV contents
   std::vector<Step> init_steps;  // run once after upload of L
   std::vector<Step> sigma_steps; // run per sigma build
   std::vector<DiagEntry> diag;   // diagonal H_ii assembly
