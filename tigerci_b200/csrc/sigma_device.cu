@@ -503,38 +503,52 @@ __device__ __forceinline__ long long pk(long long a, long long b) {
 }
 
 // W+ (np x np, rows [aa (n); ab a>b]) and W- (nm x nm) from X[(ab)][(cd)] = (ab|cd)
+// x = a(a-1)/2 + b with a > b (the reference's pair order idx = a(a-1)/2 + b)
+__device__ __forceinline__ void unpair_idx(long long x, long long& a, long long& b) {
+  long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)x)) * 0.5);
+  while (i * (i - 1) / 2 > x) --i;
+  while ((i + 1) * i / 2 <= x) ++i;
+  a = i;
+  b = x - i * (i - 1) / 2;
+}
+
+// One W row per block iteration (W+ rows, then W- rows), the threads along its columns.  The column pair
+// (b, d), d the fast index, lands in X's column index in both terms (X = Lpk Lpk^T is symmetric, so the
+// exchange term is read as X[(c b)][(a d)]): consecutive columns read consecutive X words for d <= c, a.
 __global__ void build_allext(const double* __restrict__ X, long long n, double* __restrict__ W) {
   const long long nab = n * (n - 1) / 2, np = n + nab, nm = nab, npk = n * (n + 1) / 2;
-  const long long total = np * np + nm * nm;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    long long r, c;
-    bool plus;
-    if (e < np * np) { r = e / np; c = e % np; plus = true; }
-    else { r = (e - np * np) / nm; c = (e - np * np) % nm; plus = false; }
-    auto unpair = [&](long long x, long long& a, long long& b) {
-      long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)x)) * 0.5);
-      while (i * (i - 1) / 2 > x) --i;
-      while ((i + 1) * i / 2 <= x) ++i;
-      a = i;
-      b = x - i * (i - 1) / 2;
-    };
-    double v;
-    if (plus) {
-      const bool rd = r < n, cd = c < n;
-      long long a, cc, b, d;
-      if (rd) { a = r; cc = r; } else unpair(r - n, a, cc);
-      if (cd) { b = c; d = c; } else unpair(c - n, b, d);
-      if (rd && cd) v = X[pk(a, b) * npk + pk(a, b)];
-      else if (rd) v = 1.4142135623730951 * X[pk(a, b) * npk + pk(a, d)];
-      else if (cd) v = 1.4142135623730951 * X[pk(a, b) * npk + pk(cc, b)];
-      else v = X[pk(a, b) * npk + pk(cc, d)] + X[pk(a, d) * npk + pk(cc, b)];
+  for (long long row = blockIdx.x; row < np + nm; row += gridDim.x) {
+    const bool plus = row < np;
+    const long long r = plus ? row : row - np, ncol = plus ? np : nm;
+    double* __restrict__ w = W + (plus ? r * np : np * np + r * nm);
+    long long a, cc;
+    const bool rd = plus && r < n;
+    if (rd) {
+      a = r;
+      cc = r;
     } else {
-      long long a, cc, b, d;
-      unpair(r, a, cc);
-      unpair(c, b, d);
-      v = X[pk(a, b) * npk + pk(cc, d)] - X[pk(a, d) * npk + pk(cc, b)];
+      unpair_idx(plus ? r - n : r, a, cc);
     }
-    W[e] = v;
+    for (long long c = threadIdx.x; c < ncol; c += blockDim.x) {
+      const bool cd = plus && c < n;
+      long long b, d;
+      if (cd) {
+        b = c;
+        d = c;
+      } else {
+        unpair_idx(plus ? c - n : c, b, d);
+      }
+      double v;
+      if (plus) {
+        if (rd && cd) v = X[pk(a, b) * npk + pk(a, b)];
+        else if (rd) v = 1.4142135623730951 * X[pk(a, b) * npk + pk(a, d)];
+        else if (cd) v = 1.4142135623730951 * X[pk(a, b) * npk + pk(cc, b)];
+        else v = X[pk(a, b) * npk + pk(cc, d)] + X[pk(cc, b) * npk + pk(a, d)];
+      } else {
+        v = X[pk(a, b) * npk + pk(cc, d)] - X[pk(cc, b) * npk + pk(a, d)];
+      }
+      w[c] = v;
+    }
   }
 }
 
