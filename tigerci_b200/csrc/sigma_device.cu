@@ -293,6 +293,7 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
   const DGemmProblem P = probs[prob_of_block];
   const long long n = w - P.tile_begin;
   if (w >= nwarps || n >= P.N) return;
+  // each lane keeps sum_q alpha_q (its part of A_m . b_q); one reduction per row at the end
   double acc[SKINNY_M];
 #pragma unroll
   for (int m = 0; m < SKINNY_M; ++m) acc[m] = 0.0;
@@ -302,6 +303,29 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
     // 16-byte loads when both rows start on 16 bytes and K is even
     const bool vec = ((reinterpret_cast<uintptr_t>(S.A) | reinterpret_cast<uintptr_t>(b)) & 15) == 0 &&
                      ((S.lda | S.K) & 1) == 0;
+    if (vec && S.K <= 256) {  // the b row in registers once, every row of A against it
+      const double2* b2 = reinterpret_cast<const double2*>(b);
+      const long long h = S.K / 2;
+      double2 y[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) y[e] = lane + 32 * e < h ? __ldg(b2 + lane + 32 * e) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int m = 0; m < SKINNY_M; ++m) {
+        if (m >= P.M) break;
+        const double2* a2 = reinterpret_cast<const double2*>(S.A + m * S.lda);
+        double2 x[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) x[e] = lane + 32 * e < h ? __ldg(a2 + lane + 32 * e) : make_double2(0.0, 0.0);
+        double d = 0.0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          d = fma(x[e].x, y[e].x, d);
+          d = fma(x[e].y, y[e].y, d);
+        }
+        acc[m] = fma(S.alpha, d, acc[m]);
+      }
+      continue;
+    }
 #pragma unroll
     for (int m = 0; m < SKINNY_M; ++m) {
       if (m >= P.M) break;
@@ -318,11 +342,13 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
       } else {
         for (long long k = lane; k < S.K; k += 32) d = fma(__ldg(a + k), __ldg(b + k), d);
       }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
       acc[m] = fma(S.alpha, d, acc[m]);
     }
   }
+#pragma unroll
+  for (int m = 0; m < SKINNY_M; ++m)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[m] += __shfl_xor_sync(0xffffffffu, acc[m], o);
   if (lane == 0)
     for (int m = 0; m < SKINNY_M && m < P.M; ++m) {
       double* c = P.C + m * P.ldc + n;
@@ -339,7 +365,9 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
 // scatter) gives each thread one element and all the sources in order.
 constexpr int AXPY_CHUNK = 256;
 constexpr int AXPY_DIRECT = 8;  // targets with at most this many sources: one thread per element
-__global__ void __launch_bounds__(256) axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg,
+// PAIRS: two sources per pass in the general path (steps whose targets have many sources; more registers).
+template <bool PAIRS>
+__global__ void __launch_bounds__(256, PAIRS ? 4 : 5) axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg,
                                                      const DAxpySource* __restrict__ src) {
   __shared__ double part[8][AXPY_CHUNK];
   const long long t = blockIdx.x;
@@ -383,7 +411,31 @@ __global__ void __launch_bounds__(256) axpy_segments(const DAxpyTarget* __restri
   double acc[AXPY_CHUNK / 32];
 #pragma unroll
   for (int e = 0; e < AXPY_CHUNK / 32; ++e) acc[e] = 0.0;
-  for (long long s = T.src_begin + warp; s < T.src_end; s += 8) {
+  long long s = T.src_begin + warp;
+  // two sources per pass: both rows' loads are in flight before the first product (same order of fmas)
+  for (; PAIRS && s + 8 < T.src_end; s += 16) {
+    const DAxpySource S0 = src[s], S1 = src[s + 8];
+    const double c0 = S0.scale ? S0.coef * (*S0.scale) : S0.coef;
+    const double c1 = S1.scale ? S1.coef * (*S1.scale) : S1.coef;
+    const double* x0 = S0.src + T.base;
+    const double* x1 = S1.src + T.base;
+    double v0[AXPY_CHUNK / 32], v1[AXPY_CHUNK / 32];
+#pragma unroll
+    for (int e = 0; e < AXPY_CHUNK / 32; ++e) {
+      const long long i = lane + 32 * e;
+      v0[e] = i < T.len ? x0[i] : 0.0;
+      v1[e] = i < T.len ? x1[i] : 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < AXPY_CHUNK / 32; ++e) {
+      const long long i = lane + 32 * e;
+      if (i < T.len) {
+        acc[e] = fma(c0, v0[e], acc[e]);
+        acc[e] = fma(c1, v1[e], acc[e]);
+      }
+    }
+  }
+  for (; s < T.src_end; s += 8) {
     const DAxpySource S = src[s];
     const double c = S.scale ? S.coef * (*S.scale) : S.coef;
     const double* x = S.src + T.base;
@@ -416,7 +468,47 @@ __global__ void __launch_bounds__(256) dot_segments(const DDotTarget* __restrict
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // each lane keeps sum_s coef_s sum_{its i} a_s[i] b_s[i] over the warp's sources; one reduction at the end
   double total = 0.0;
-  for (long long s = T.src_begin + warp; s < T.src_end; s += 8) {
+  long long s = T.src_begin + warp;
+  // short rows (up to 256 elements, 16-byte aligned, even length), two sources per pass: every load of both
+  // is issued before the first product; the fmas keep the order of the general loop below
+  for (; s + 8 < T.src_end; s += 16) {
+    const DDotSource S0 = src[s], S1 = src[s + 8];
+    const bool fast = ((reinterpret_cast<uintptr_t>(S0.a) | reinterpret_cast<uintptr_t>(S0.b) |
+                        reinterpret_cast<uintptr_t>(S1.a) | reinterpret_cast<uintptr_t>(S1.b)) & 15) == 0 &&
+                      ((S0.len | S1.len) & 1) == 0 && S0.len <= 256 && S1.len <= 256;
+    if (!fast) break;
+    const double2* a0 = reinterpret_cast<const double2*>(S0.a);
+    const double2* b0 = reinterpret_cast<const double2*>(S0.b);
+    const double2* a1 = reinterpret_cast<const double2*>(S1.a);
+    const double2* b1 = reinterpret_cast<const double2*>(S1.b);
+    const long long h0 = S0.len / 2, h1 = S1.len / 2;
+    double2 x0[4], y0[4], x1[4], y1[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const long long i = lane + 32 * e;
+      const double2 z = make_double2(0.0, 0.0);
+      x0[e] = i < h0 ? __ldg(a0 + i) : z;
+      y0[e] = i < h0 ? __ldg(b0 + i) : z;
+      x1[e] = i < h1 ? __ldg(a1 + i) : z;
+      y1[e] = i < h1 ? __ldg(b1 + i) : z;
+    }
+    double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (lane + 32 * e < h0) {
+        acc0 = fma(x0[e].x, y0[e].x, acc0);
+        acc0 = fma(x0[e].y, y0[e].y, acc0);
+      }
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (lane + 32 * e < h1) {
+        acc1 = fma(x1[e].x, y1[e].x, acc1);
+        acc1 = fma(x1[e].y, y1[e].y, acc1);
+      }
+    total = fma(S0.coef, acc0, total);
+    total = fma(S1.coef, acc1, total);
+  }
+  for (; s < T.src_end; s += 8) {
     const DDotSource S = src[s];
     double acc = 0.0;
     if (((reinterpret_cast<uintptr_t>(S.a) | reinterpret_cast<uintptr_t>(S.b)) & 15) == 0 && (S.len & 1) == 0) {
@@ -634,25 +726,39 @@ cudaError_t dev_malloc(T** p, size_t bytes, cudaStream_t st) {
 }
 inline cudaError_t dev_free(void* p, cudaStream_t st) { return p ? cudaFreeAsync(p, st) : cudaSuccess; }
 
-// partial[k * RBLK + b] = sum over block b's chunk of A[k][i] * x[i]
+// partial[k * RBLK + b] = sum over block b's chunk of A[k][i] * x[i].  Four rows per pass share the loads
+// of x (each row's products are still summed in the order of the one-row loop).
 __global__ void __launch_bounds__(RB) multi_dot_partial(const double* __restrict__ A, long long lda, int m,
                                                         const double* __restrict__ x, long long n,
                                                         double* __restrict__ partial) {
-  __shared__ double red[RB / 32];
+  __shared__ double red[4][RB / 32];
   const long long chunk = (n + gridDim.x - 1) / gridDim.x;
   const long long i0 = (long long)blockIdx.x * chunk, i1 = min(n, i0 + chunk);
-  for (int k = 0; k < m; ++k) {
-    const double* a = A + (long long)k * lda;
-    double acc = 0.0;
-    for (long long i = i0 + threadIdx.x; i < i1; i += RB) acc = fma(a[i], x[i], acc);
+  for (int k0 = 0; k0 < m; k0 += 4) {
+    const int nk = min(4, m - k0);
+    const double* a0 = A + (long long)k0 * lda;
+    const double* a1 = nk > 1 ? a0 + lda : a0;
+    const double* a2 = nk > 2 ? a0 + 2 * lda : a0;
+    const double* a3 = nk > 3 ? a0 + 3 * lda : a0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long i = i0 + threadIdx.x; i < i1; i += RB) {
+      const double xi = x[i];
+      acc[0] = fma(a0[i], xi, acc[0]);
+      acc[1] = fma(a1[i], xi, acc[1]);
+      acc[2] = fma(a2[i], xi, acc[2]);
+      acc[3] = fma(a3[i], xi, acc[3]);
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = acc[q];
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < nk) {
       double t = 0.0;
-      for (int w = 0; w < RB / 32; ++w) t += red[w];
-      partial[(long long)k * gridDim.x + blockIdx.x] = t;
+      for (int w = 0; w < RB / 32; ++w) t += red[threadIdx.x][w];
+      partial[(long long)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = t;
     }
     __syncthreads();
   }
@@ -747,6 +853,7 @@ struct DevStep {
   DDotTarget* dt = nullptr;
   DDotSource* ds = nullptr;
   long long ntg = 0;
+  bool axpy_pairs = false;  // targets with many sources on average: the two-sources-per-pass kernel
   // ZERO
   double* zptr = nullptr;
   long long zlen = 0;
@@ -1178,23 +1285,43 @@ struct tci_ctx {
         if (d.tma_probs) d.tc_ok = flops >= 5e7;  // the TMA-fed tables tile the step well
       }
     } else if (s.kind == STEP_AXPY) {
-      std::vector<DAxpyTarget> t;
-      std::vector<DAxpySource> so;
       constexpr i64 kChunk = AXPY_CHUNK;  // elements per block: long rows are spread over many blocks
-      for (auto& x : s.at) {
-        check_range(x.dst, x.off, x.len);
+      // chunk counts first, then targets and sources converted (and range-checked) in parallel
+      std::vector<i64> first(s.at.size() + 1, 0);
+      for (size_t i = 0; i < s.at.size(); ++i) first[i + 1] = first[i] + (std::max<i64>(0, s.at[i].len) + kChunk - 1) / kChunk;
+      std::vector<DAxpyTarget> t((size_t)first.back());
+      std::vector<DAxpySource> so(s.as.size());
+      int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+      for (long long i = 0; i < (long long)s.at.size(); ++i) {
+        const AxpyTarget& x = s.at[(size_t)i];
+        if (!range_ok(x.dst, x.off, x.len) || x.src_begin < 0 || x.src_end > (i64)s.as.size()) {
+          bad |= 1;
+          continue;
+        }
         for (i64 b = 0; b < x.len; b += kChunk)
-          t.push_back(DAxpyTarget{ptr(x.dst, x.off) + b, b, std::min(kChunk, x.len - b), x.src_begin, x.src_end});
+          t[(size_t)(first[(size_t)i] + b / kChunk)] =
+              DAxpyTarget{buf[x.dst] + x.off + b, b, std::min(kChunk, x.len - b), x.src_begin, x.src_end};
+        // source length equals its target's length
+        for (i64 q = x.src_begin; q < x.src_end; ++q)
+          if (!range_ok(s.as[(size_t)q].src, s.as[(size_t)q].off, x.len)) bad |= 1;
       }
-      for (auto& x : s.as) {
-        // source length equals its target's length; the offset is checked against the buffer
-        so.push_back(DAxpySource{ptr(x.src, x.off), x.sbuf >= 0 ? ptr(x.sbuf, x.sidx) : nullptr, x.coef});
+#pragma omp parallel for schedule(static) reduction(| : bad)
+      for (long long q = 0; q < (long long)s.as.size(); ++q) {
+        const AxpySource& x = s.as[(size_t)q];
+        if (!range_ok(x.src, x.off, 0) || (x.sbuf >= 0 && !range_ok(x.sbuf, x.sidx, 0))) {
+          bad |= 1;
+          continue;
+        }
+        so[(size_t)q] = DAxpySource{buf[x.src] + x.off, x.sbuf >= 0 ? buf[x.sbuf] + x.sidx : nullptr, x.coef};
       }
-      for (auto& x : s.at)
-        for (i64 q = x.src_begin; q < x.src_end; ++q) check_range(s.as[q].src, s.as[q].off, x.len);
+      if (bad) throw Error(TCI_ERR_INTERNAL, "plan range outside its buffer (or an unallocated buffer)");
       d.at = upload(t, owned, stream);
       d.as = upload(so, owned, stream);
       d.ntg = (long long)t.size();
+      // many sources per target, and no short targets (whose path the occupancy bound of that kernel slows)
+      d.axpy_pairs = !s.at.empty() && s.as.size() >= 32 * s.at.size() &&
+                     std::all_of(s.at.begin(), s.at.end(), [](const AxpyTarget& x) { return x.len >= 8; });
     } else if (s.kind == STEP_DOT) {
       std::vector<DDotTarget> t;
       std::vector<DDotSource> so;
@@ -1606,6 +1733,10 @@ struct tci_ctx {
     if (st != 0) throw Error(TCI_ERR_TIMEOUT, "tensor-core kernel: a bounded wait gave up (code " + std::to_string(st) + ")");
   }
 
+  // the range lies in an allocated buffer (no throw: usable inside parallel loops)
+  bool range_ok(int b, i64 off, i64 len) const {
+    return b >= 0 && b < NUM_BUFS && buf[b] && off >= 0 && len >= 0 && off + len <= plan.buf_size[b];
+  }
   void check_range(int b, i64 off, i64 len) const {
     if (b < 0 || b >= NUM_BUFS || off < 0 || len < 0 || off + len > plan.buf_size[b])
       throw Error(TCI_ERR_INTERNAL, "plan range outside its buffer");
@@ -1683,7 +1814,10 @@ struct tci_ctx {
         }
         break;
       case STEP_AXPY:
-        if (s.ntg > 0) axpy_segments<<<(unsigned)s.ntg, 256, 0, stream>>>(s.at, s.ntg, s.as);
+        if (s.ntg > 0) {
+          if (s.axpy_pairs) axpy_segments<true><<<(unsigned)s.ntg, 256, 0, stream>>>(s.at, s.ntg, s.as);
+          else axpy_segments<false><<<(unsigned)s.ntg, 256, 0, stream>>>(s.at, s.ntg, s.as);
+        }
         break;
       case STEP_DOT:
         if (s.ntg > 0) dot_segments<<<(unsigned)s.ntg, 256, 0, stream>>>(s.dt, s.ntg, s.ds);
@@ -1912,7 +2046,14 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
       }
       ctx->init.push_back(ctx->lower(s));
     }
-    for (auto& s : P.sigma_steps) ctx->sigma.push_back(ctx->lower(s));
+    for (auto& s : P.sigma_steps) {
+      ctx->sigma.push_back(ctx->lower(s));
+      if (timing) {  // the σ steps whose tables take a noticeable time
+        cudaStreamSynchronize(ctx->stream);
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
+        if (dt > 0.002) phase(("  lowering " + s.name).c_str(), ctx->stream);
+      }
+    }
     phase("lowering (step tables)", ctx->stream);
     for (size_t i = 0; i < ctx->init.size(); ++i) {
       ctx->run(ctx->init[i]);
