@@ -110,9 +110,9 @@ struct Ints {
           for (i64 l = 0; l < ni; ++l) I4[((i * ni + j) * ni + k) * ni + l] = eri(i, j, k, l);
     I3.assign(ni * ni * ni * n, 0.0);
     // (iq|jk) = L[pair(i, q)] . L[pair(j, k)]: the internal pair rows (the first ni(ni+1)/2 rows of L)
-    // transposed once, then 4 rows L[pair(i, q)] x 8 internal pairs per register block, every dot still
+    // transposed once, then 4 rows L[pair(i, q)] x 4 internal pairs per register block, every dot still
     // summed in J order (the same value as eri())
-    const i64 npr = ni * (ni + 1) / 2, npr8 = (npr + 7) / 8 * 8, nq4 = (n + 3) / 4;
+    const i64 npr = ni * (ni + 1) / 2, npr8 = (npr + 3) / 4 * 4, nq4 = (n + 3) / 4;
     std::vector<double> Lt((size_t)(N * npr8), 0.0);
     std::vector<int> pj((size_t)npr), pk((size_t)npr);
     for (i64 j = 0; j < ni; ++j)
@@ -125,21 +125,27 @@ struct Ints {
 #pragma omp parallel for collapse(3) schedule(dynamic)
     for (i64 i = 0; i < ni; ++i)
       for (i64 qb = 0; qb < nq4; ++qb)
-        for (i64 pb = 0; pb < npr8; pb += 8) {
-          const double* a[4];
-          for (int r = 0; r < 4; ++r) a[r] = L + pair(i, ni + std::min<i64>(qb * 4 + r, n - 1)) * N;
-          double acc[4][8] = {};
-          for (i64 J = 0; J < N; ++J) {
-            const double* lt = &Lt[(size_t)(J * npr8 + pb)];
-            for (int r = 0; r < 4; ++r) {
-              const double x = a[r][J];
-              for (int c = 0; c < 8; ++c) acc[r][c] += x * lt[c];
-            }
+        for (i64 pb = 0; pb < npr8; pb += 4) {
+          const double* a0 = L + pair(i, ni + std::min<i64>(qb * 4 + 0, n - 1)) * N;
+          const double* a1 = L + pair(i, ni + std::min<i64>(qb * 4 + 1, n - 1)) * N;
+          const double* a2 = L + pair(i, ni + std::min<i64>(qb * 4 + 2, n - 1)) * N;
+          const double* a3 = L + pair(i, ni + std::min<i64>(qb * 4 + 3, n - 1)) * N;
+          double c00 = 0, c01 = 0, c02 = 0, c03 = 0, c10 = 0, c11 = 0, c12 = 0, c13 = 0;
+          double c20 = 0, c21 = 0, c22 = 0, c23 = 0, c30 = 0, c31 = 0, c32 = 0, c33 = 0;
+          const double* lt = &Lt[(size_t)pb];
+          for (i64 J = 0; J < N; ++J, lt += npr8) {
+            const double l0 = lt[0], l1 = lt[1], l2 = lt[2], l3 = lt[3];
+            const double x0 = a0[J], x1 = a1[J], x2 = a2[J], x3 = a3[J];
+            c00 += x0 * l0; c01 += x0 * l1; c02 += x0 * l2; c03 += x0 * l3;
+            c10 += x1 * l0; c11 += x1 * l1; c12 += x1 * l2; c13 += x1 * l3;
+            c20 += x2 * l0; c21 += x2 * l1; c22 += x2 * l2; c23 += x2 * l3;
+            c30 += x3 * l0; c31 += x3 * l1; c32 += x3 * l2; c33 += x3 * l3;
           }
+          const double acc[4][4] = {{c00, c01, c02, c03}, {c10, c11, c12, c13}, {c20, c21, c22, c23}, {c30, c31, c32, c33}};
           for (int r = 0; r < 4; ++r) {
             const i64 q = qb * 4 + r;
             if (q >= n) break;
-            for (int c = 0; c < 8 && pb + c < npr; ++c) {
+            for (int c = 0; c < 4 && pb + c < npr; ++c) {
               const i64 j = pj[(size_t)(pb + c)], k = pk[(size_t)(pb + c)];
               I3[(size_t)(((i * ni + j) * ni + k) * n + q)] = acc[r][c];
               I3[(size_t)(((i * ni + k) * ni + j) * n + q)] = acc[r][c];
