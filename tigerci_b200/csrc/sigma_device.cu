@@ -367,7 +367,7 @@ constexpr int AXPY_CHUNK = 256;
 constexpr int AXPY_DIRECT = 8;  // targets with at most this many sources: one thread per element
 // PAIRS: two sources per pass in the general path (steps whose targets have many sources; more registers).
 template <bool PAIRS>
-__global__ void __launch_bounds__(256, PAIRS ? 4 : 5) axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg,
+__global__ void __launch_bounds__(256, PAIRS ? 4 : 0) axpy_segments(const DAxpyTarget* __restrict__ tg, long long ntg,
                                                      const DAxpySource* __restrict__ src) {
   __shared__ double part[8][AXPY_CHUNK];
   const long long t = blockIdx.x;
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(256, PAIRS ? 4 : 5) axpy_segments(const DAxpyT
   for (int e = 0; e < AXPY_CHUNK / 32; ++e) acc[e] = 0.0;
   long long s = T.src_begin + warp;
   // two sources per pass: both rows' loads are in flight before the first product (same order of fmas)
-  for (; PAIRS && s + 8 < T.src_end; s += 16) {
+  if constexpr (PAIRS) for (; s + 8 < T.src_end; s += 16) {
     const DAxpySource S0 = src[s], S1 = src[s + 8];
     const double c0 = S0.scale ? S0.coef * (*S0.scale) : S0.coef;
     const double c1 = S1.scale ? S1.coef * (*S1.scale) : S1.coef;
@@ -435,8 +435,8 @@ __global__ void __launch_bounds__(256, PAIRS ? 4 : 5) axpy_segments(const DAxpyT
       }
     }
   }
-  for (; s < T.src_end; s += 8) {
-    const DAxpySource S = src[s];
+  for (long long r = s; r < T.src_end; r += 8) {
+    const DAxpySource S = src[r];
     const double c = S.scale ? S.coef * (*S.scale) : S.coef;
     const double* x = S.src + T.base;
 #pragma unroll
