@@ -534,19 +534,32 @@ void Builder::internal_blocks() {
           }
         }
     }
+    // every target's place in the step tables (target order), then the rows copied in parallel
+    std::vector<size_t> soff(heads.size() + 1, 0), toff(heads.size() + 1, 0);
     for (size_t t = 0; t < heads.size(); ++t) {
-      if (bytgt[t].empty()) continue;
+      size_t rows = 0;
+      for (i64 c : tcount[t]) rows += c > 0 ? 1 : 0;
+      soff[t + 1] = soff[t] + tsrc[t].size();
+      toff[t + 1] = toff[t] + rows;
+      // exact: integer-valued terms far below 2^53, so the sum does not depend on the order
+      for (i64 c : tcount[t]) P.flops_total += 2.0 * (double)len * (double)c;
+    }
+    const size_t s0 = st.as.size(), t0 = st.at.size();
+    st.as.resize(s0 + soff.back());
+    st.at.resize(t0 + toff.back());
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long long tl = 0; tl < (long long)heads.size(); ++tl) {
+      const size_t t = (size_t)tl;
+      if (tsrc[t].empty()) continue;
+      std::copy(tsrc[t].begin(), tsrc[t].end(), st.as.begin() + (std::ptrdiff_t)(s0 + soff[t]));
       const Head& Tg = heads[t];
-      size_t next = 0;
+      size_t next = s0 + soff[t], j = t0 + toff[t];
       for (i64 a = 0; a < (i64)tcount[t].size(); ++a) {
-        AxpyTarget tg{BUF_S, off_of(Tg) + a * len, len, (i64)st.as.size(), 0};
         const i64 c = tcount[t][(size_t)a];
-        st.as.insert(st.as.end(), tsrc[t].begin() + (long)next, tsrc[t].begin() + (long)(next + (size_t)c));
+        if (c > 0) st.at[j++] = AxpyTarget{BUF_S, off_of(Tg) + a * len, len, (i64)next, (i64)(next + (size_t)c)};
         next += (size_t)c;
-        P.flops_total += 2.0 * (double)len * (double)c;
-        tg.src_end = (i64)st.as.size();
-        if (tg.src_end > tg.src_begin) st.at.push_back(tg);
       }
+      std::vector<AxpySource>().swap(tsrc[t]);
     }
   }
 }
@@ -1163,20 +1176,30 @@ void Builder::sv() {
     std::vector<double>().swap(*src[(size_t)t]);  // released here, in parallel
   }
   Step& fw = step(P.sigma_steps, STEP_AXPY, "sv forward");
-  std::map<i64, std::vector<size_t>> by_mu;
-  for (size_t t = 0; t < rows.size(); ++t) by_mu[rows[t].first.first].push_back(t);
-  for (auto& kv : by_mu) {
-    AxpyTarget tg{BUF_S, kv.first, n, (i64)fw.as.size(), 0};
-    for (size_t t : kv.second) fw.as.push_back(AxpySource{BUF_WV, rows[t].second * n, 1.0, BUF_C, rows[t].first.second});
+  // rows are in (mu row, v csf) order: one target per run of equal mu rows
+  fw.as.reserve(fw.as.size() + rows.size());
+  for (size_t t = 0; t < rows.size();) {
+    AxpyTarget tg{BUF_S, rows[t].first.first, n, (i64)fw.as.size(), 0};
+    const i64 mu = rows[t].first.first;
+    for (; t < rows.size() && rows[t].first.first == mu; ++t)
+      fw.as.push_back(AxpySource{BUF_WV, rows[t].second * n, 1.0, BUF_C, rows[t].first.second});
     tg.src_end = (i64)fw.as.size();
     fw.at.push_back(tg);
   }
   Step& rv = step(P.sigma_steps, STEP_DOT, "sv reverse");
-  std::map<i64, std::vector<size_t>> by_v;
-  for (size_t t = 0; t < rows.size(); ++t) by_v[rows[t].first.second].push_back(t);
-  for (auto& kv : by_v) {
-    DotTarget tg{BUF_S, kv.first, (i64)rv.ds.size(), 0};
-    for (size_t t : kv.second) rv.ds.push_back(DotSource{BUF_WV, BUF_C, rows[t].second * n, rows[t].first.first, n, 1.0});
+  // by v csf, the rows of one v in (mu row) order
+  std::vector<size_t> byv(rows.size());
+  for (size_t t = 0; t < rows.size(); ++t) byv[t] = t;
+  std::stable_sort(byv.begin(), byv.end(),
+                   [&](size_t x, size_t y) { return rows[x].first.second < rows[y].first.second; });
+  rv.ds.reserve(rv.ds.size() + rows.size());
+  for (size_t k = 0; k < byv.size();) {
+    const i64 v = rows[byv[k]].first.second;
+    DotTarget tg{BUF_S, v, (i64)rv.ds.size(), 0};
+    for (; k < byv.size() && rows[byv[k]].first.second == v; ++k) {
+      const size_t t = byv[k];
+      rv.ds.push_back(DotSource{BUF_WV, BUF_C, rows[t].second * n, rows[t].first.first, n, 1.0});
+    }
     tg.src_end = (i64)rv.ds.size();
     rv.dt.push_back(tg);
   }
