@@ -681,18 +681,37 @@ void Builder::ds() {
     i64 mu_row, dkk;
     std::vector<double> w;
   };
-  std::map<std::pair<i64, i64>, size_t> t1_index;
   std::vector<T1> t1;
-  auto w_of = [&](i64 mu_row, i64 dkk) -> std::vector<double>& {
-    auto key = std::make_pair(mu_row, dkk);
-    auto it = t1_index.find(key);
-    if (it != t1_index.end()) return t1[it->second].w;
-    t1_index[key] = t1.size();
-    t1.push_back(T1{mu_row, dkk, std::vector<double>(n, 0.0)});
-    return t1.back().w;
+  // Source heads in parallel: every key (mu row, dk) of T1 and every T3 entry belongs to one source head (dk
+  // is that head's), so per-head lists concatenated in head order give the serial loop's tables exactly.
+  struct HeadOut {
+    std::vector<T3> t3;
+    std::vector<T1> t1;
   };
-  for (size_t hs = 0; hs < sp.paths[2].size(); ++hs) {
-    const Head& S = sp.paths[2][hs];
+  const auto& heads2 = sp.paths[2];
+  std::vector<HeadOut> hout(heads2.size());
+  std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
+  for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long hsl = 0; hsl < (long long)heads2.size(); ++hsl) {
+    const size_t hs = (size_t)hsl;
+    CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
+    auto M = [&](const Config& L, const Config& R, const Op& o) {
+      std::vector<double> m;
+      E.matrix(L, R, o, m);
+      return m;
+    };
+    auto& out = hout[hs];
+    std::map<std::pair<i64, i64>, size_t> t1_index;  // this head's keys, in first-use order in out.t1
+    auto w_of = [&](i64 mu_row, i64 dkk) -> std::vector<double>& {
+      auto key = std::make_pair(mu_row, dkk);
+      auto it = t1_index.find(key);
+      if (it != t1_index.end()) return out.t1[it->second].w;
+      t1_index[key] = out.t1.size();
+      out.t1.push_back(T1{mu_row, dkk, std::vector<double>(n, 0.0)});
+      return out.t1.back().w;
+    };
+    const Head& S = heads2[hs];
     if (!S.kept || nD(S) == 0) continue;
     const i64 nS = nD(S);
     const bool Sab = S.off >= 0;
@@ -715,7 +734,7 @@ void Builder::ds() {
       }
       for (i64 kt = 0; kt < Mu->nsf; ++kt)
         for (i64 ks = 0; ks < nS; ++ks)
-          if (std::fabs(a[kt * nS + ks]) > kTiny) t3.push_back(T3{Mu->off + kt * n, i, dk(S, ks), a[kt * nS + ks]});
+          if (std::fabs(a[kt * nS + ks]) > kTiny) out.t3.push_back(T3{Mu->off + kt * n, i, dk(S, ks), a[kt * nS + ks]});
     }
     // one-external: ops e_{iq,jk} (a+_i a+_j a_k a_q) and E_iq
     auto add_op = [&](const Head* Mu, int i, int j, int k, bool one_el) {
@@ -768,6 +787,10 @@ void Builder::ds() {
         }
       }
     }
+  }
+  for (auto& ho : hout) {
+    t3.insert(t3.end(), ho.t3.begin(), ho.t3.end());
+    for (auto& x : ho.t1) t1.push_back(std::move(x));
   }
 
   // ---- device steps for the three-external term (V_i stored [b][(q,s)])
