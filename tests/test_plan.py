@@ -75,3 +75,33 @@ def test_plan_diagonal_equals_dense_diagonal(c, tmp_path):
         pytest.skip("dense diagonal too large")
     H = od.hamiltonian(h, L)
     assert np.abs(pi.diagonal() - np.diag(H)).max() <= 1e-12 * np.abs(np.diag(H)).max()
+
+
+_EXPORT = r"""
+import sys
+sys.path.insert(0, {root!r})
+import tigerci_b200 as T
+from tigerci_b200.synthetic import synthetic_operator
+deck = T.Deck(26, 4, 2, 10, 1, ["222220", "222202"])
+h, L = synthetic_operator(26, 40, seed=21, scale=0.25, diag_range=(-6, 1), offdiag_sigma=0.05)
+T.Plan(deck, T.Operator(h, L)).export({path!r})
+"""
+
+
+def test_plan_bytes_do_not_depend_on_thread_count(tmp_path):
+    """The plan builder runs heads in parallel (zero-external blocks, three-/one-external
+    couplings, sv rows, the (iq|jk) table); the exported plan is the same byte for byte
+    with one thread and with four."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = []
+    for threads in ("1", "4"):
+        path = str(tmp_path / f"plan_{threads}.bin")
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        subprocess.run([sys.executable, "-c", _EXPORT.format(root=root, path=path)], env=env, check=True,
+                       timeout=300)
+        out.append(open(path, "rb").read())
+    assert len(out[0]) > 0 and out[0] == out[1]
