@@ -87,14 +87,48 @@ def measured_peaks():
 class ClockSampler:
     FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=100):
         self.index = index
+        self.period_ms = period_ms
         self.rows = []
-        self._stop = threading.Event()
+        self._p = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
+    def _read(self):
+        # one nvidia-smi process sampling every period_ms for the whole region (a new process per sample
+        # took ~0.3 s, too few samples for a region of a second)
+        try:
+            for line in self._p.stdout:
+                line = line.strip()
+                if line:
+                    self.rows.append([x.strip() for x in line.split(",")])
+        except Exception:
+            pass
+
+    def __enter__(self):
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                        "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._p = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+        time.sleep(0.3)  # the first sample is taken before the timed work starts
+        return self
+
+    def __exit__(self, *a):
+        if self._p is None:
+            return
+        self._p.terminate()
+        try:
+            self._p.wait(timeout=5)
+        except Exception:
+            self._p.kill()
+            self._p.wait(timeout=5)
+        self._t.join(timeout=5)
+        if not self.rows:  # nothing came through the pipe: one sample now rather than none
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
@@ -102,16 +136,6 @@ class ClockSampler:
                     self.rows.append([x.strip() for x in line.split(",")])
             except Exception:
                 pass
-            self._stop.wait(0.2)
-
-    def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
-        return self
-
-    def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
 
     def summary(self):
         if not self.rows:
