@@ -1116,21 +1116,33 @@ void Builder::ss() {
 // SV: sigma_mu[k'] += c_v[k] w ; sigma_v[k] += <w, c_mu[k']>.
 // ops e_{xi,jk} = a+_x a+_j a_k a_i with (xi|jk), and E_xi with h_xi.
 void Builder::sv() {
-  // (mu row, v csf) -> w; valence heads in parallel, each owning the keys of its own CSFs
-  std::vector<std::vector<std::pair<std::pair<i64, i64>, std::vector<double>>>> vout(sp.paths[0].size());
+  // (mu row, v csf) -> w.  Two passes over the valence heads (in parallel, each head owning the keys of its
+  // own CSFs): the first records every coupling (key, coefficient, integral vector) in loop order, the keys
+  // are then placed in (mu row, v csf) order, and the second accumulates each head's couplings in the same
+  // order directly into the W-vector array (no per-row buffers to copy).
+  struct SvOp {
+    std::pair<i64, i64> key;
+    double a;
+    const double* vec;  // nullptr: the one-electron column h(nint + x, hi) scaled by hs
+    double hs;
+    i64 hi;
+  };
+  const size_t nV = sp.paths[0].size();
+  std::vector<std::vector<SvOp>> vops(nV);
+  std::vector<std::vector<std::pair<i64, i64>>> vkeys(nV);  // each head's keys, sorted
   std::vector<std::unique_ptr<CouplingEngine>> engines((size_t)omp_get_max_threads());
   for (auto& e : engines) e = std::make_unique<CouplingEngine>(tables);
   // per thread: the expansion of each N-1 head (with the external electron), looked up once
   std::vector<std::vector<const CsfExpansion*>> hexp1((size_t)omp_get_max_threads(),
                                                       std::vector<const CsfExpansion*>(sp.paths[1].size(), nullptr));
 #pragma omp parallel for schedule(dynamic, 4)
-  for (long long hvl = 0; hvl < (long long)sp.paths[0].size(); ++hvl) {
-    std::map<std::pair<i64, i64>, std::vector<double>> wmap;
+  for (long long hvl = 0; hvl < (long long)nV; ++hvl) {
     CouplingEngine& E = *engines[(size_t)omp_get_thread_num()];  // per-thread expansion cache
     const Head& V = sp.paths[0][(size_t)hvl];
     if (!has(V)) continue;
     const CsfExpansion& eV = E.expand(cfgV(V));
     auto& hx = hexp1[(size_t)omp_get_thread_num()];
+    auto& ops = vops[(size_t)hvl];
     std::vector<double> m;
     auto add = [&](const Head* Mu, Op o, const double* vec, double hval_scale, i64 hi) {
       const size_t mi = (size_t)(Mu->lex - 1);
@@ -1140,13 +1152,7 @@ void Builder::sv() {
         for (i64 ks = 0; ks < V.nsf; ++ks) {
           const double a = m[kt * V.nsf + ks];
           if (std::fabs(a) <= kTiny) continue;
-          auto& w = wmap[{Mu->off + kt * n, V.off + ks}];
-          if (w.empty()) w.assign(n, 0.0);
-          if (vec) {
-            for (i64 x = 0; x < n; ++x) w[x] += a * vec[x];
-          } else {
-            for (i64 x = 0; x < n; ++x) w[x] += a * hval_scale * I.h1(nint + x, hi);
-          }
+          ops.push_back(SvOp{{Mu->off + kt * n, V.off + ks}, a, vec, hval_scale, hi});
         }
     };
     // one working occupation, changed in place (no allocation per candidate)
@@ -1169,34 +1175,47 @@ void Builder::sv() {
       }
       o[i] += 1;
     }
-    auto& out = vout[(size_t)hvl];
-    out.reserve(wmap.size());
-    for (auto& kv : wmap) out.emplace_back(kv.first, std::move(kv.second));
+    auto& ks = vkeys[(size_t)hvl];
+    ks.reserve(ops.size());
+    for (const auto& op : ops) ks.push_back(op.key);
+    std::sort(ks.begin(), ks.end());
+    ks.erase(std::unique(ks.begin(), ks.end()), ks.end());
   }
-  // every key in (mu row, v csf) order
-  std::vector<std::pair<std::pair<i64, i64>, std::vector<double>*>> keys;
-  for (auto& out : vout)
-    for (auto& kv : out) keys.push_back({kv.first, &kv.second});
+  // every key in (mu row, v csf) order; a row's place is its rank
+  std::vector<std::pair<std::pair<i64, i64>, i64>> keys;  // (key, owning head)
+  for (size_t v = 0; v < nV; ++v)
+    for (const auto& k : vkeys[v]) keys.push_back({k, (i64)v});
   if (keys.empty()) return;
-  std::sort(keys.begin(), keys.end(),
-            [](const std::pair<std::pair<i64, i64>, std::vector<double>*>& x,
-               const std::pair<std::pair<i64, i64>, std::vector<double>*>& y) { return x.first < y.first; });
+  std::sort(keys.begin(), keys.end());
   const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
   std::vector<std::pair<std::pair<i64, i64>, i64>> rows;
-  std::vector<std::vector<double>*> src;
   rows.reserve(keys.size());
-  src.reserve(keys.size());
-  for (auto& kv : keys) {
+  std::vector<std::vector<i64>> vrow(nV);  // per head: the W rows of its sorted keys
+  for (size_t v = 0; v < nV; ++v) vrow[v].reserve(vkeys[v].size());
+  for (const auto& kv : keys) {
+    vrow[(size_t)kv.second].push_back(wbase + (i64)rows.size());  // keys of one head arrive in its sorted order
     rows.push_back({kv.first, wbase + (i64)rows.size()});
-    src.push_back(kv.second);
   }
-  // one allocation, rows copied in parallel (hundreds of MB at the kernel-scale size)
+  // one allocation (hundreds of MB at the kernel-scale size), each head's rows zeroed and accumulated by
+  // the thread that owns the head
   const size_t w0 = P.wv.size();
-  P.wv.resize(w0 + src.size() * (size_t)n);
-#pragma omp parallel for schedule(static)
-  for (long long t = 0; t < (long long)src.size(); ++t) {
-    std::copy(src[(size_t)t]->begin(), src[(size_t)t]->end(), P.wv.begin() + (std::ptrdiff_t)(w0 + (size_t)t * n));
-    std::vector<double>().swap(*src[(size_t)t]);  // released here, in parallel
+  P.wv.resize(w0 + keys.size() * (size_t)n);
+  double* W = P.wv.data();
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long hvl = 0; hvl < (long long)nV; ++hvl) {
+    const auto& ks = vkeys[(size_t)hvl];
+    const auto& rs = vrow[(size_t)hvl];
+    for (i64 r : rs) std::fill(W + (size_t)r * n, W + (size_t)(r + 1) * n, 0.0);
+    for (const auto& op : vops[(size_t)hvl]) {
+      const size_t at = (size_t)(std::lower_bound(ks.begin(), ks.end(), op.key) - ks.begin());
+      double* w = W + (size_t)rs[at] * n;
+      if (op.vec) {
+        for (i64 x = 0; x < n; ++x) w[x] += op.a * op.vec[x];
+      } else {
+        for (i64 x = 0; x < n; ++x) w[x] += op.a * op.hs * I.h1(nint + x, op.hi);
+      }
+    }
+    std::vector<SvOp>().swap(vops[(size_t)hvl]);
   }
   Step& fw = step(P.sigma_steps, STEP_AXPY, "sv forward");
   // rows are in (mu row, v csf) order: one target per run of equal mu rows
