@@ -86,6 +86,14 @@ int tci_space_path(const tci_space* sp, int64_t kind, int64_t lex, int64_t* occ,
  * entries of block kind (0 valence, 1 N-1, 2 N-2), written as (s, f, c) triples. */
 int tci_space_block_counts(const tci_space* sp, int64_t kind, int64_t* out, int64_t max_triples, int64_t* n_triples);
 void tci_space_destroy(tci_space* sp);
+/* Diagonal metric G of the (MR)ACPF / ACPF-2 / (MR)AQCC functionals, replacing
+ * build_compressed_g (tiger_fortran/gtimesc.f90:37-55): get_gvalues (:316-378)
+ * for flag 1 ACPF, 2 ACPF-2, 3 AQCC, 4 custom (g3 = g4 = custom_g), 9 test
+ * (all ones), and build_g_diagonal (:106-201) for the CSF classes: valence
+ * CSFs of a reference configuration (g1), other valence CSFs with the inactive
+ * orbitals full (g2), valence CSFs with an inactive hole (g3), N-1 (g4), N-2
+ * (g5).  g gets n = total_csfs values; cls (may be NULL) the class 1..5. */
+int tci_acpf_gdiag(const tci_space* sp, int64_t flag, double custom_g, double* g, int64_t* cls, int64_t n);
 
 /* ---- Sigma plan (host only) ------------------------------------------------
  * Replaces the iteration-1 loop enumeration ("dry run") of the sigma build:
@@ -160,6 +168,16 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
                     int64_t subspace_bytes, const int32_t* cancel, double* energies, double* vectors,
                     int64_t* iterations);
 int64_t tci_davidson_capacity(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes);
+/* Generalized eigenproblem of the ACPF-type functionals, replacing
+ * davidson_liu_gen_eig (tiger_fortran/davidson.f90:253-469):
+ * (H - e_shift) c = lambda G c with G = diag(g) (host array of total_csfs
+ * positive values, e.g. from tci_acpf_gdiag) and e_shift the reference energy.
+ * Solved as the standard problem of G^-1/2 (H - e_shift) G^-1/2 (y = G^1/2 c)
+ * by the device Davidson of tci_davidson_ex (same tolerances, budget, mixed
+ * form and finish).  energies get lambda + e_shift; vectors (may be NULL) the
+ * unit-norm c of each root. */
+int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                     const double* g, double e_shift, double* energies, double* vectors, int64_t* iterations);
 int64_t tci_davidson_bytes(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes);
 /* Batched projections for a caller-driven Davidson with device-resident vectors
  * (expand_krylov_subspace / orthonormalize_vector, tiger_fortran/davidson.f90:478,

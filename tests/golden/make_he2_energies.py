@@ -8,6 +8,8 @@ Source runs (reference tree, tests/Tests/):
   (driver.sh input deck); printed reference energy and root-1 total energy.
 - Helium2_SDCI_excited: the same deck with NUM ROOTS 2 (same Molden orbitals);
   printed root-1 and root-2 total energies.
+- Helium2_ACPF: the same deck with ACPF FLAG 1 (same Molden orbitals); printed
+  ACPF total energy.
 
 The reference reads the orbitals from the Molden file and computes AO integrals
 with libint (absent from its tree).  Here the AO integrals come from
@@ -45,12 +47,14 @@ def main(ref_root):
     molden = os.path.join(tdir, "Helium2_SDCI", "Helium2_SDCI.molden")
     out1 = os.path.join(tdir, "Helium2_SDCI", "Helium2_SDCI.output")
     outx = os.path.join(tdir, "Helium2_SDCI_excited", "Helium2_SDCI_excited.output")
+    outa = os.path.join(tdir, "Helium2_ACPF", "Helium2_ACPF.output")
     atoms, shells, C, ene, occ = gto.read_molden(molden)
     h, L, e_nuc, S = gto.mo_operator(atoms, shells, C)
     ortho = float(np.abs(C.T @ S @ C - np.eye(C.shape[1])).max())
     e_ref = grab(out1, r"the reference energy is \(elec \+ nuclear\) =\s*(-?\d+\.\d+)")
     e_sd = grab(out1, r"Root\s+1 total energy \(electronic \+ nuclear\) is :\s*(-?\d+\.\d+)")
     e_x = grab(outx, r"Root\s+\d+ total energy \(electronic \+ nuclear\) is :\s*(-?\d+\.\d+)")
+    e_a = grab(outa, r"Root\s+1 total energy \(electronic \+ nuclear\) is :\s*(-?\d+\.\d+)")
     fixture = {
         "source": "tests/Tests/Helium2_SDCI (+ Helium2_SDCI_excited), reference tree",
         "deck": {"num_orbitals": 10, "num_inactive": 2, "num_active": 0, "num_elec": 4, "spin_mult": 1,
@@ -62,6 +66,7 @@ def main(ref_root):
         "reference_energy": e_ref[0],
         "sdci_root1": e_sd[0],
         "sdci_roots_excited_run": e_x,
+        "acpf_root1": e_a[0],
         "reference_energy_tolerance_of_its_test": 1e-6,
     }
     path = os.path.join(HERE, "he2_631gss_sdci.json")

@@ -38,6 +38,8 @@ EXPORTS = [
     "tci_diag",
     "tci_davidson",
     "tci_davidson_ex",
+    "tci_davidson_gen",
+    "tci_acpf_gdiag",
     "tci_davidson_capacity",
     "tci_davidson_bytes",
     "tci_local_create",
@@ -121,6 +123,8 @@ def lib():
         L.tci_diag.argtypes = [P, P, i64]
         L.tci_davidson.argtypes = [P, i64, dbl, dbl, i64, P, P, P]
         L.tci_davidson_ex.argtypes = [P, i64, dbl, dbl, i64, i64, P, P, P, P]
+        L.tci_davidson_gen.argtypes = [P, i64, dbl, dbl, i64, P, dbl, P, P, P]
+        L.tci_acpf_gdiag.argtypes = [P, i64, dbl, P, P, i64]
         L.tci_davidson_capacity.argtypes = [i64, i64, i64, i64]
         L.tci_davidson_capacity.restype = i64
         L.tci_davidson_bytes.argtypes = [i64, i64, i64, i64]

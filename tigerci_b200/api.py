@@ -74,6 +74,14 @@ class CsfSpace:
         check(lib().tci_space_create(C.byref(self._d), C.byref(h)))
         self._h = h
 
+    def acpf_gdiag(self, flag: int = 1, custom_g: float = 0.0):
+        """Diagonal metric of the ACPF-type functionals (build_compressed_g): (g, class 1..5 per CSF)."""
+        n = self.counts()["total_csfs"]
+        g = np.zeros(n)
+        cls = np.zeros(n, dtype=np.int64)
+        check(lib().tci_acpf_gdiag(self._h, flag, custom_g, ptr(g), ptr(cls), n))
+        return g, cls
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib().tci_space_destroy(self._h)
@@ -171,6 +179,7 @@ class SigmaBuilder:
         self._d = deck.c_struct()
         self._o = op.c_struct()
         self._op = op
+        self.deck = deck
         self.precision = precision
         h = C.c_void_p()
         finish = {True: 1, False: 0, "full": 1, "none": 0, "no_allext": 2, "no_allext_3ext": 3}[fp64_finish]
@@ -235,6 +244,30 @@ class SigmaBuilder:
                                     ptr(cancel) if cancel is not None else None, ptr(e),
                                     ptr(v) if v is not None else None, C.byref(it)))
         return e, v, it.value
+
+    def acpf(self, nroots: int = 1, flag: int = 1, custom_g: float = 0.0, tol_residual: float = 1e-6,
+             tol_energy: float = 1e-6, maxit: int = 0, want_vectors: bool = False, e_ref=None):
+        """(MR)ACPF / ACPF-2 / (MR)AQCC roots (acpf_driver + davidson_liu_gen_eig): (H - E_ref) c = lambda G c
+        with G from CsfSpace.acpf_gdiag(flag).  E_ref defaults to the lowest eigenvalue of H in the space of
+        the reference-configuration CSFs (class 1).  Returns (energies, vectors|None, iterations, E_ref);
+        energies are electronic, like davidson()."""
+        g, cls = CsfSpace(self.deck).acpf_gdiag(flag, custom_g)
+        if e_ref is None:
+            idx = np.nonzero(cls == 1)[0]
+            if idx.size == 0:
+                raise ValueError("no reference CSF in the space")
+            Hr = np.zeros((idx.size, idx.size))
+            for j, i in enumerate(idx):
+                x = np.zeros(self.n)
+                x[i] = 1.0
+                Hr[:, j] = self.sigma(x)[idx]
+            e_ref = float(np.linalg.eigvalsh(0.5 * (Hr + Hr.T))[0])
+        e = np.zeros(nroots)
+        v = np.zeros((nroots, self.n)) if want_vectors else None
+        it = C.c_int64()
+        check(lib().tci_davidson_gen(self._h, nroots, tol_residual, tol_energy, maxit, ptr(g), float(e_ref), ptr(e),
+                                     ptr(v) if v is not None else None, C.byref(it)))
+        return e, v, it.value, e_ref
 
     def profile(self, on: bool = True, davidson_phases: bool = False):
         """Per-step CUDA-event timing of subsequent sigma builds; with

@@ -182,6 +182,65 @@ int tci_space_path(const tci_space* s, int64_t kind, int64_t lex, int64_t* occ, 
   return TCI_OK;
 }
 
+int tci_acpf_gdiag(const tci_space* s, int64_t flag, double custom_g, double* g, int64_t* cls, int64_t n) {
+  if (!s || !g || n != s->sp.total_csfs) return TCI_ERR_ARG;
+  try {
+    const CsfSpace& sp = s->sp;
+    const Deck& d = sp.deck;
+    // get_gvalues (gtimesc.f90:316-378)
+    const double N = (double)(d.num_elec - 2 * d.num_frozen);
+    double v[5];
+    if (flag == 1) {
+      v[0] = v[1] = 1.0;
+      v[2] = v[3] = v[4] = 2.0 / N;
+    } else if (flag == 2) {
+      v[0] = v[1] = 1.0;
+      v[2] = v[3] = (4.0 / N) * (1.0 - 1.0 / (2.0 * (N - 1.0)));
+      v[4] = 2.0 / N;
+    } else if (flag == 3) {
+      v[0] = v[1] = 1.0;
+      v[2] = v[3] = v[4] = (4.0 / N) * (1.0 - 1.0 / (2.0 * (N - 1.0)));
+    } else if (flag == 4) {
+      v[0] = v[1] = 1.0;
+      v[2] = v[3] = custom_g;
+      v[4] = 2.0 / N;
+    } else if (flag == 9) {
+      v[0] = v[1] = v[2] = v[3] = v[4] = 1.0;
+    } else {
+      throw Error(TCI_ERR_ARG, "unknown ACPF flag");
+    }
+    // build_g_diagonal (gtimesc.f90:106-201): N-1 CSFs g4, N-2 CSFs g5, valence CSFs by configuration
+    std::vector<int64_t> c((size_t)n, 0);
+    for (i64 i = sp.num_valence; i < sp.num_valence + sp.num_nm1; ++i) c[(size_t)i] = 4;
+    for (i64 i = sp.num_valence + sp.num_nm1; i < n; ++i) c[(size_t)i] = 5;
+    const i64 ni = d.num_internal();
+    for (const Head& h : sp.paths[0]) {
+      if (!h.kept || h.off < 0 || h.nsf <= 0) continue;
+      i64 inact = 0;
+      for (i64 j = 0; j < d.num_inactive; ++j) inact += h.occ[(size_t)j];
+      int k = 3;  // an inactive hole (g_diag_no_external :262-272)
+      if (inact == 2 * d.num_inactive) {
+        bool ref = false;  // active occupations of a reference (:274-291)
+        for (i64 r = 0; r < d.num_ref && !ref; ++r) {
+          bool same = true;
+          for (i64 j = d.num_inactive; j < ni; ++j) same = same && h.occ[(size_t)j] == d.refs[(size_t)(r * ni + j)];
+          ref = same;
+        }
+        k = ref ? 1 : 2;
+      }
+      for (i64 t = 0; t < h.nsf; ++t) c[(size_t)(h.off + t)] = k;
+    }
+    for (i64 i = 0; i < n; ++i) {
+      if (c[(size_t)i] == 0) throw Error(TCI_ERR_INTERNAL, "a CSF without an ACPF class");
+      g[i] = v[c[(size_t)i] - 1];
+      if (cls) cls[i] = c[(size_t)i];
+    }
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
 int tci_space_block_counts(const tci_space* s, int64_t kind, int64_t* out, int64_t max_triples, int64_t* n_triples) {
   if (!s || kind < 0 || kind > 2 || !n_triples) return TCI_ERR_ARG;
   const auto& m = s->sp.cfg_count[kind];

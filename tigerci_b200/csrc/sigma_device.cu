@@ -803,6 +803,23 @@ __global__ void precondition_kernel(double* __restrict__ r, const double* __rest
   }
 }
 
+// Generalized (ACPF-type) solves run on G^-1/2 (H - shift) G^-1/2: x <- s x with s = G^-1/2 before the sigma
+// build, out = s (H x - shift x) after it, and the diagonal s^2 (H_ii - shift).
+__global__ void scale_by(double* __restrict__ x, const double* __restrict__ s, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] *= s[i];
+}
+__global__ void gen_sigma_out(double* __restrict__ out, const double* __restrict__ hx, const double* __restrict__ x,
+                              const double* __restrict__ s, double shift, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = s[i] * (hx[i] - shift * x[i]);
+}
+__global__ void gen_diag(double* __restrict__ out, const double* __restrict__ hd, const double* __restrict__ s,
+                         double shift, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = s[i] * s[i] * (hd[i] - shift);
+}
+
 // r scaled by 1/|r| (or zeroed when |r| < 1e-14)
 __global__ void normalize_kernel(double* __restrict__ r, const double* __restrict__ nrm2, long long n) {
   const double nr = sqrt(*nrm2);
@@ -921,6 +938,9 @@ struct tci_ctx {
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
   cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
+  // generalized solve (tci_davidson_gen): sigma and the diagonal of G^-1/2 (H - gen_shift) G^-1/2
+  const double* gen_s = nullptr;  // G^-1/2 (device) while such a solve runs, else nullptr
+  double gen_shift = 0.0;
   std::vector<i64> lowest_diag;  // CSF indices of the lowest diagonal elements, ascending (initial guesses)
   double* dots = nullptr;        // reduction scratch: partial sums and results
   double* coefs = nullptr;       // small device coefficient arrays
@@ -1400,10 +1420,21 @@ struct tci_ctx {
   void sigma_of(const double* d_c, double* d_s) {
     const i64 n = plan.total_csfs;
     TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     run_sigma_steps();
-    TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    gen_out(d_s);
     sigma_count++;
+  }
+  // d_s = BUF_S, or in a generalized solve G^-1/2 (BUF_S - shift BUF_C)
+  void gen_out(double* d_s) {
+    const i64 n = plan.total_csfs;
+    if (gen_s) {
+      gen_sigma_out<<<148 * 8, 256, 0, stream>>>(d_s, buf[BUF_S], buf[BUF_C], gen_s, gen_shift, n);
+      TCI_CUDA(cudaGetLastError());
+    } else {
+      TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    }
   }
   // TMA-fed kernel's tile width per step kind: 128 unless the B operand has at most 64 rows per problem
   bool tma_wide(int kind) const {
@@ -1708,6 +1739,7 @@ struct tci_ctx {
     const bool tc_allext = (refine == 2 || refine == 3) && precision == 1;
     if (!buf[BUF_W] && !tc_allext) throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
     TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     const int64_t saved = precision;
     precision = 0;
@@ -1722,7 +1754,7 @@ struct tci_ctx {
     launch_count += sigma_launches();
     precision = saved;
     allext_tc_in_fp64 = false;
-    TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    gen_out(d_s);
   }
 
   // Status word of the bounded waits inside the tensor-core kernel.
@@ -2225,6 +2257,74 @@ extern "C" {
 int tci_davidson(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
                  double* energies, double* vectors, int64_t* iterations) {
   return tci_davidson_ex(ctx, nroots, tol_residual, tol_energy, maxit, 0, nullptr, energies, vectors, iterations);
+}
+
+// davidson_liu_gen_eig (tiger_fortran/davidson.f90:253-469): (H - e_shift) c = lambda G c, G = diag(g), solved
+// as the standard problem of G^-1/2 (H - e_shift) G^-1/2 by the device Davidson above (y = G^1/2 c).
+int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
+                     const double* g, double e_shift, double* energies, double* vectors, int64_t* iterations) {
+  if (!ctx || !g || !energies || nroots <= 0 || !std::isfinite(e_shift)) return TCI_ERR_ARG;
+  if (ctx->gen_s) return TCI_ERR_ARG;  // one generalized solve at a time on a context
+  double* ds = nullptr;
+  double* dd = nullptr;
+  double* saved_hd = nullptr;
+  std::vector<i64> saved_low;
+  auto restore = [&]() {
+    if (saved_hd) {
+      ctx->hd = saved_hd;
+      ctx->lowest_diag = saved_low;
+    }
+    ctx->gen_s = nullptr;
+    ctx->gen_shift = 0.0;
+    cudaStreamSynchronize(ctx->stream);
+    std::lock_guard<std::mutex> lk(g_capture_free_mu);
+    dev_free(ds, ctx->stream);
+    dev_free(dd, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+  };
+  try {
+    TCI_CUDA(cudaSetDevice(ctx->device));
+    const i64 n = ctx->plan.total_csfs;
+    std::vector<double> sh((size_t)n);
+    for (i64 i = 0; i < n; ++i) {
+      if (!(g[i] > 0.0) || !std::isfinite(g[i])) throw Error(TCI_ERR_ARG, "the metric must be positive and finite");
+      sh[(size_t)i] = 1.0 / std::sqrt(g[i]);
+    }
+    ctx->ensure_diag();
+    TCI_CUDA(dev_malloc(&ds, (size_t)n * sizeof(double), ctx->stream));
+    TCI_CUDA(dev_malloc(&dd, (size_t)n * sizeof(double), ctx->stream));
+    TCI_CUDA(cudaMemcpyAsync(ds, sh.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    gen_diag<<<148 * 8, 256, 0, ctx->stream>>>(dd, ctx->hd, ds, e_shift, n);
+    TCI_CUDA(cudaGetLastError());
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+    saved_hd = ctx->hd;
+    saved_low = ctx->lowest_diag;
+    ctx->hd = dd;
+    ctx->lowest_diag.clear();  // the initial guess follows the transformed diagonal
+    ctx->gen_s = ds;
+    ctx->gen_shift = e_shift;
+    const int rc = tci_davidson_ex(ctx, nroots, tol_residual, tol_energy, maxit, 0, nullptr, energies, vectors,
+                                   iterations);
+    restore();
+    if (rc != TCI_OK) return rc;
+    for (i64 k = 0; k < nroots; ++k) energies[k] += e_shift;
+    if (vectors)  // c = G^-1/2 y, unit norm
+      for (i64 k = 0; k < nroots; ++k) {
+        double* v = vectors + k * n;
+        double nrm = 0.0;
+        for (i64 i = 0; i < n; ++i) {
+          v[i] *= sh[(size_t)i];
+          nrm += v[i] * v[i];
+        }
+        nrm = std::sqrt(nrm);
+        if (nrm > 0.0)
+          for (i64 i = 0; i < n; ++i) v[i] /= nrm;
+      }
+    return TCI_OK;
+  } catch (...) {
+    restore();
+    return guard_status(std::current_exception());
+  }
 }
 
 int64_t tci_davidson_capacity(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes) {
