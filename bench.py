@@ -330,6 +330,7 @@ def main():
     ap.add_argument("--local-forms", default="tf32x3,fp64", help="forms of the pair-domain measurement")
     ap.add_argument("--serve-only", action="store_true", help="only the serving measurement")
     ap.add_argument("--local-pairs", type=int, default=600, help="pairs of the pair-domain workload (0: skip)")
+    ap.add_argument("--acpf-solves", type=int, default=3, help="timed ACPF solves on the solve operator (0: skip)")
     ap.add_argument("--local-only", action="store_true", help="only the pair-domain measurement")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -518,6 +519,28 @@ def main():
         return dict(times=times, t_total=t_total, energy=energies[-1], energies=energies, iterations=iters,
                     launches=launches, clk=clk, init_s=init_s, phases=phases)
 
+    def acpf_measure(nsolves, form):
+        """ACPF (flag 1) on the same operator: the FP64 form once for its energy, `form` timed (host wall
+        clock around SigmaBuilder.acpf, the metric build included)."""
+        out = {"flag": 1, "what": "(H - E_ref) c = lambda G c, generalized device Davidson"}
+        for f in dict.fromkeys(("fp64", form)):
+            sb = T.SigmaBuilder(deck_m, op_m, device=local, precision=f)
+            e, _, it, e_ref = sb.acpf(1, flag=1, tol_residual=TOL_RESIDUAL, tol_energy=TOL_ENERGY)
+            ts = []
+            for _ in range(nsolves if f == form else 0):
+                torch.cuda.synchronize()
+                t = time.perf_counter()
+                e, _, it, _ = sb.acpf(1, flag=1, tol_residual=TOL_RESIDUAL, tol_energy=TOL_ENERGY, e_ref=e_ref)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t)
+            sb.close()
+            out[f] = {"energy": float(e[0]), "iterations": int(it), "e_ref": float(e_ref)}
+            if ts:
+                out[f].update({"solves_per_s": len(ts) / sum(ts), "ms_per_solve": 1e3 * sum(ts) / len(ts)})
+        if form != "fp64":
+            out[form]["energy_minus_fp64"] = out[form]["energy"] - out["fp64"]["energy"]
+        return out
+
     solves = {}
     for f in forms:
         try:
@@ -587,6 +610,11 @@ def main():
             line["serving"] = serve_measure(args.serve_requests, args.serve_slots, local, planners=args.serve_planners)
         except Exception as exc:
             line["serving"] = {"error": str(exc)[:300]}
+    if args.acpf_solves > 0:
+        try:
+            line["acpf"] = acpf_measure(args.acpf_solves, best)
+        except Exception as exc:
+            line["acpf"] = {"error": str(exc)[:300]}
     if args.local_pairs > 0:
         try:
             line["local_pairs"] = local_measure(args.local_pairs, local, hbm, bf16, nchol=args.local_nchol,
