@@ -523,8 +523,8 @@ def main():
         """ACPF (flag 1) on the same operator: the FP64 form once for its energy, `form` timed (host wall
         clock around SigmaBuilder.acpf, the metric build included)."""
         out = {"flag": 1, "what": "(H - E_ref) c = lambda G c, generalized device Davidson (maxit 50)",
-               "note": "the synthetic operator's correlation energy (0.74 Eh for 16 electrons, g = 2/16) is far "
-                       "outside ACPF's regime: the solve runs to maxit; the pinned He2 case converges"}
+               "note": "on this synthetic operator (SDCI correlation energy 0.74 Eh for 16 electrons, g = 1/8) "
+                       "the solve runs to maxit; the pinned He2 ACPF case converges"}
         for f in dict.fromkeys(("fp64", form)):
             sb = T.SigmaBuilder(deck_m, op_m, device=local, precision=f)
             e, _, it, e_ref = sb.acpf(1, flag=1, tol_residual=TOL_RESIDUAL, tol_energy=TOL_ENERGY)
