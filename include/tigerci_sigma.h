@@ -175,7 +175,9 @@ int64_t tci_davidson_capacity(int64_t n, int64_t nroots, int64_t maxit, int64_t 
  * Solved as the standard problem of G^-1/2 (H - e_shift) G^-1/2 (y = G^1/2 c)
  * by the device Davidson of tci_davidson_ex (same tolerances, budget, mixed
  * form and finish).  energies get lambda + e_shift; vectors (may be NULL) the
- * unit-norm c of each root. */
+ * unit-norm c of each root.  For the length of the call the context's
+ * diagonal and sigma build stand for the transformed operator, so no other
+ * call may use the same context (from another thread) until it returns. */
 int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double tol_energy, int64_t maxit,
                      const double* g, double e_shift, double* energies, double* vectors, int64_t* iterations);
 int64_t tci_davidson_bytes(int64_t n, int64_t nroots, int64_t maxit, int64_t subspace_bytes);
@@ -198,7 +200,9 @@ int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const doub
  * library holds until exit.  Every call shares it and overwrites what it
  * reads, so calls whose kernels overlap on a GPU race.  The first call on a
  * device looks the array's address up (cudaGetSymbolAddress), so make it
- * before any stream capture. */
+ * before any stream capture.  The address belongs to the CUDA context current
+ * at that call; a call under another context of the device (after a
+ * cudaDeviceReset, or a driver-API context of the caller's) looks it up again. */
 #define TCI_DOTS_NOALLOC_MAX_ROWS 64
 int tci_dots_noalloc(const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
                      void* stream);

@@ -108,7 +108,9 @@ def parse_output(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TIGERCI_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference tree> (or set TIGERCI_REFERENCE)")
     runs = []
     seen = set()
     for p in sorted(glob.glob(os.path.join(ref, "tests", "Tests", "*", "*.output"))):

@@ -76,4 +76,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2 and not os.environ.get("TIGERCI_REFERENCE"):
+        sys.exit("usage: make_he2_energies.py <reference tree> (or set TIGERCI_REFERENCE)")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["TIGERCI_REFERENCE"])

@@ -44,6 +44,37 @@ def test_noalloc_projection_matches_allocating_entry_point(need_gpu):
     sb.close()
 
 
+def test_noalloc_calls_leave_free_device_memory_unchanged(need_gpu):
+    """The calls themselves take no device memory: after one warm-up call (which
+    loads the kernels), free memory as the driver reports it is the same
+    before and after a series of calls on a non-default stream."""
+    import torch
+
+    lib = _lib.lib()
+    m, n = 48, 100_003
+    rng = np.random.default_rng(5)
+    A = torch.from_numpy(rng.standard_normal((m, n))).cuda()
+    x = torch.from_numpy(rng.standard_normal(n)).cuda()
+    out = torch.zeros(m, dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+
+    def call():
+        rc = lib.tci_dots_noalloc(ctypes.c_void_p(A.data_ptr()), n, m, ctypes.c_void_p(x.data_ptr()), n,
+                                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+        assert rc == 0, _lib.last_error()
+
+    call()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        call()
+    s.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    host = A.cpu().numpy() @ x.cpu().numpy()
+    assert np.abs(out.cpu().numpy() - host).max() <= RTOL * np.abs(host).max() + 1e-12
+
+
 def test_noalloc_rejects_sizes_beyond_its_fixed_scratch(need_gpu):
     import torch
 

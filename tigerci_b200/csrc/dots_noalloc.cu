@@ -66,25 +66,59 @@ __global__ void noalloc_final(const double* __restrict__ partial, int m, int nbl
   out[k] = t;
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (in host code the array's name is only a host-side shadow).
+// Device address of the scratch array.  In host code the array's name is only
+// a host-side shadow; the address is looked up with cudaGetSymbolAddress with
+// the device current, and it is valid only in the CUDA context it was looked
+// up in (a cudaDeviceReset, or a driver-API caller that makes another context
+// current on the same device, gives the array a new address).  So each cached
+// address is kept with the context it belongs to and looked up again when the
+// current context differs.
+using CtxGetCurrentFn = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+
 std::mutex g_mu;
 constexpr int kMaxDevices = 64;
-double* g_scratch[kMaxDevices] = {};
+struct ScratchSlot {
+  void* ctx = nullptr;
+  double* ptr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+bool g_ctx_fn_resolved = false;
+
+void* current_context() {  // caller holds g_mu
+  if (!g_ctx_fn_resolved) {
+    g_ctx_fn_resolved = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+  }
+  void* ctx = nullptr;
+  if (!g_ctx_get_current) throw tci::Error(TCI_ERR_CUDA, "tci_dots_noalloc: cuCtxGetCurrent unavailable");
+  if (g_ctx_get_current(&ctx) != 0) ctx = nullptr;
+  return ctx;  // nullptr until the runtime has made a context current
+}
 
 double* scratch_of_current_device() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) throw tci::Error(TCI_ERR_CUDA, std::string("cudaGetDevice failed: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) throw tci::Error(TCI_ERR_CUDA, "tci_dots_noalloc: device index out of range");
   std::lock_guard<std::mutex> lk(g_mu);
-  if (dev >= 0 && dev < kMaxDevices && g_scratch[dev]) return g_scratch[dev];
+  void* ctx = current_context();
+  ScratchSlot& slot = g_scratch[dev];
+  if (ctx && slot.ptr && slot.ctx == ctx) return slot.ptr;
   void* p = nullptr;
-  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // also makes the primary context current if none is
   if (e != cudaSuccess || !p)
     throw tci::Error(TCI_ERR_CUDA, std::string("cudaGetSymbolAddress of the projection scratch failed: ") +
                                        cudaGetErrorString(e));
-  if (dev >= 0 && dev < kMaxDevices) g_scratch[dev] = static_cast<double*>(p);
-  return static_cast<double*>(p);
+  ctx = current_context();
+  if (!ctx) throw tci::Error(TCI_ERR_CUDA, "tci_dots_noalloc: no current CUDA context after the symbol lookup");
+  slot.ctx = ctx;
+  slot.ptr = static_cast<double*>(p);
+  return slot.ptr;
 }
 
 }  // namespace
