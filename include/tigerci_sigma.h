@@ -260,6 +260,58 @@ int tci_local_apply_host(tci_local* loc, const double* c, double* sigma, int64_t
 int tci_local_stats(const tci_local* loc, double* out, int64_t len);
 void tci_local_destroy(tci_local* loc);
 
+/* ---- Molecular front end (host) -------------------------------------------
+ * The set-up that produces the tci_operator of a molecule, replacing
+ * cholesky() (tiger_cpp/main.cpp:270-361): the AO two-electron integral
+ * matrix decomposed by pivoted Cholesky with the CD THRESHOLD as dpstf2's
+ * tolerance (Cho_WholeMat::decompose, tiger_cpp/Cholesky.cpp:268-307), and
+ * the vectors transformed to the MO basis (transfrom_to_MO_basis,
+ * tiger_cpp/Cholesky.cpp:78-165; tiger_fortran/cholesky_transform.f90:379).
+ * The reference takes its AO integrals from libint and its orbitals from a
+ * Molden file; here the integrals are computed by the McMurchie-Davidson
+ * scheme, and tci_rhf gives canonical RHF orbitals where no orbitals are
+ * given.  Shells are s, p or d over normalised primitives (Molden [GTO]
+ * convention); Cartesian components in Molden order (p: x y z; d: xx yy zz xy
+ * xz yz), pure d in Molden [5D] order (d0 d+1 d-1 d+2 d-2). */
+typedef struct tci_molecule {
+  int64_t n_atoms;
+  const double* charges;      /* nuclear charge of each atom                       */
+  const double* coords;       /* n_atoms x 3, bohr                                 */
+  int64_t n_shells;
+  const int64_t* shell_atom;  /* 0-based atom of each shell                        */
+  const int64_t* shell_l;     /* 0 s, 1 p, 2 d                                     */
+  const int64_t* shell_nprim; /* primitives of each shell                          */
+  const double* exponents;    /* concatenated over the shells                      */
+  const double* coefficients; /* contraction coefficients of normalised primitives */
+  int64_t pure_d;             /* 1: five pure d functions per d shell; 0: six Cartesian */
+} tci_molecule;
+typedef struct tci_integrals tci_integrals;
+/* AO integrals and the pivoted Cholesky decomposition of (mu nu|lambda sigma)
+ * down to cd_threshold (largest remaining diagonal). */
+int tci_integrals_create(const tci_molecule* mol, double cd_threshold, tci_integrals** out);
+/* out[0..7]: basis functions, Cholesky vectors, nuclear repulsion, seconds,
+ * largest remaining diagonal, ERI shell quartets computed, pivot shell-pair
+ * blocks, shells. */
+int tci_integrals_info(const tci_integrals* it, double* out, int64_t len);
+/* Overlap S and core Hamiltonian h = T + V (nbf x nbf, row major); either may be NULL. */
+int tci_integrals_one_electron(const tci_integrals* it, double* S, double* h, int64_t nbf);
+/* AO Cholesky vectors chol[pq * nchol + J], pq = mu(mu+1)/2 + nu (mu >= nu). */
+int tci_integrals_ao_cholesky(const tci_integrals* it, double* chol, int64_t npair, int64_t nchol);
+/* Exact AO ERI tensor eri[((mu*n + nu)*n + la)*n + si] (not from the
+ * decomposition), for checking small bases (nbf <= 200). */
+int tci_integrals_ao_eri(const tci_integrals* it, double* eri, int64_t nbf);
+/* Closed-shell RHF on the Cholesky vectors (DIIS), n_occ doubly occupied
+ * orbitals; C (nbf x nbf, row major: C[mu * nbf + p]) gets the canonical
+ * orbitals in ascending order of eps.  info[4] (may be NULL): total energy
+ * (nuclear repulsion included), iterations, converged (1/0), DIIS error.
+ * TCI_ERR_INPUT when it does not converge within maxit (<= 0: 100). */
+int tci_rhf(const tci_integrals* it, int64_t n_occ, int64_t maxit, double conv, double* C, double* eps, double* info);
+/* The tci_operator arrays in the basis of the nmo orbitals C (nbf x nmo, row
+ * major): h = C^T h_AO C (nmo x nmo) and chol[pq * nchol + J] = (C^T L^J C)_pq
+ * with pq = p(p+1)/2 + q (p >= q), the cholesky_data layout. */
+int tci_mo_operator(const tci_integrals* it, const double* C, int64_t nmo, double* h, double* chol, int64_t nchol);
+void tci_integrals_destroy(tci_integrals* it);
+
 /* ---- Serving: continuously batched CI solves on one GPU ----------------
  * No counterpart in the reference, which runs one solve per process
  * (tiger_fortran/tiger_ci.f90 -> davidson_liu).  Submitted solves are

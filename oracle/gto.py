@@ -250,6 +250,11 @@ def nuclear_repulsion(atoms) -> float:
     return e
 
 
+def molden_is_pure(path: str) -> bool:
+    """True when the Molden file declares pure (spherical) d functions ([5D], [5D7F] or [5D10F])."""
+    return any(re.match(r"\s*\[5D(7F|10F)?\]", ln, re.I) for ln in open(path))
+
+
 def read_molden(path: str):
     """Atoms (Z, bohr), shells (centre, L, exponents, coefficients) and MO coefficients (nao x nmo) with
     energies and occupations, from a Molden file with [Atoms], [GTO] and [MO] sections."""
@@ -257,7 +262,7 @@ def read_molden(path: str):
     sec = {}
     cur = None
     for ln in text:
-        m = re.match(r"\s*\[(\w[\w ]*)\]\s*(\w*)", ln)
+        m = re.match(r"\s*\[(\w[\w ]*)\]\s*\(?(\w*)", ln)
         if m:
             cur = m.group(1).strip().lower()
             sec[cur] = {"unit": m.group(2).lower(), "lines": []}
@@ -279,7 +284,7 @@ def read_molden(path: str):
         k += 1
         if not t:
             continue
-        if len(t) == 2 and t[0].isdigit():
+        if len(t) <= 2 and t[0].isdigit() and all(x.isdigit() for x in t):
             centre = atoms[int(t[0]) - 1][1]
             continue
         if t[0].lower() in _L:

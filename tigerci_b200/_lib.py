@@ -61,6 +61,14 @@ EXPORTS = [
     "tci_step_times",
     "tci_step_name",
     "tci_destroy",
+    "tci_integrals_create",
+    "tci_integrals_info",
+    "tci_integrals_one_electron",
+    "tci_integrals_ao_cholesky",
+    "tci_integrals_ao_eri",
+    "tci_rhf",
+    "tci_mo_operator",
+    "tci_integrals_destroy",
 ]
 
 
@@ -83,6 +91,21 @@ class TciDeck(C.Structure):
 
 class TciOperator(C.Structure):
     _fields_ = [("h", P), ("chol", P), ("nchol", i64), ("core_energy", dbl)]
+
+
+class TciMolecule(C.Structure):
+    _fields_ = [
+        ("n_atoms", i64),
+        ("charges", P),
+        ("coords", P),
+        ("n_shells", i64),
+        ("shell_atom", P),
+        ("shell_l", P),
+        ("shell_nprim", P),
+        ("exponents", P),
+        ("coefficients", P),
+        ("pure_d", i64),
+    ]
 
 
 class TciError(RuntimeError):
@@ -138,6 +161,15 @@ def lib():
         L.tci_step_name.argtypes = [P, i64, C.c_char_p, i64]
         L.tci_destroy.argtypes = [P]
         L.tci_destroy.restype = None
+        L.tci_integrals_create.argtypes = [C.POINTER(TciMolecule), dbl, C.POINTER(P)]
+        L.tci_integrals_info.argtypes = [P, P, i64]
+        L.tci_integrals_one_electron.argtypes = [P, P, P, i64]
+        L.tci_integrals_ao_cholesky.argtypes = [P, P, i64, i64]
+        L.tci_integrals_ao_eri.argtypes = [P, P, i64]
+        L.tci_rhf.argtypes = [P, i64, i64, dbl, P, P, P]
+        L.tci_mo_operator.argtypes = [P, P, i64, P, P, i64]
+        L.tci_integrals_destroy.argtypes = [P]
+        L.tci_integrals_destroy.restype = None
         _lib = L
     return _lib
 
