@@ -29,9 +29,9 @@ LIB = os.path.join(BUILD, "liboracle.so")
 
 def build_oracle(force=False):
     os.makedirs(BUILD, exist_ok=True)
-    src = os.path.join(HERE, "detci.c")
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
-        subprocess.check_call(["gcc", "-O3", "-march=native", "-fopenmp", "-fPIC", "-shared", "-o", LIB, src, "-lm"])
+    srcs = [os.path.join(HERE, "detci.c"), os.path.join(HERE, "plancpu.c")]
+    if force or not os.path.exists(LIB) or any(os.path.getmtime(LIB) < os.path.getmtime(s) for s in srcs):
+        subprocess.check_call(["gcc", "-O3", "-march=native", "-fopenmp", "-fPIC", "-shared", "-o", LIB, *srcs, "-lm"])
     return LIB
 
 
@@ -51,6 +51,13 @@ def lib():
                                                 C.c_void_p, C.c_void_p, C.c_int64, C.c_int64]
         L.oracle_set_dgemm.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
+        L.plancpu_load.argtypes = [C.c_char_p, C.c_void_p]
+        L.plancpu_load.restype = C.c_void_p
+        L.plancpu_sigma.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.plancpu_integrals.argtypes = [C.c_void_p]
+        L.plancpu_free.argtypes = [C.c_void_p]
+        L.plancpu_total.argtypes = [C.c_void_p]
+        L.plancpu_total.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -240,3 +247,34 @@ def allext_local_sigma(nint, chol, heads, dom_idx, c, head_range=None):
     lib().oracle_allext_local_sigma(nint, chol.shape[1], chol.ctypes.data, len(heads), heads.ctypes.data,
                                     dom_idx.ctypes.data, c.ctypes.data, s.ctypes.data, h0, h1)
     return s
+
+
+class PlanSigmaCPU:
+    """Integral-direct CPU sigma build (plancpu.c): the integrals formed from the
+    Cholesky vectors at every build, the all-external term in the reference's
+    loop form, every other coupling replayed from the loop records of an
+    exported plan (tci_plan_export).  Test and CPU-baseline use only."""
+
+    def __init__(self, plan_path, chol):
+        self._chol = np.ascontiguousarray(chol, dtype=np.float64)
+        self._h = lib().plancpu_load(plan_path.encode(), self._chol.ctypes.data)
+        if not self._h:
+            raise RuntimeError(f"cannot load plan {plan_path}")
+        self.n = int(lib().plancpu_total(self._h))
+
+    def sigma(self, c, integrals=True):
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        s = np.zeros_like(c)
+        lib().plancpu_sigma(self._h, c.ctypes.data, s.ctypes.data, 1 if integrals else 0)
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().plancpu_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -118,6 +118,7 @@ static dgemm_fn g_dgemm = 0;
 /* Optional BLAS dgemm (Fortran ABI), e.g. scipy's bundled OpenBLAS, used for
  * the (ab|cd) slab like the reference's dgemm at mod_1:556. */
 void oracle_set_dgemm(void* fn) { g_dgemm = (dgemm_fn)fn; }
+dgemm_fn oracle_get_dgemm(void) { return g_dgemm; }
 
 void oracle_allext_sigma(int64_t nint, int64_t n, int64_t nchol, const double* chol, int64_t nh,
                          const int64_t* heads, const double* c, double* sigma, int64_t a_begin, int64_t a_end) {

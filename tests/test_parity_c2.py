@@ -72,3 +72,25 @@ def test_allext_sigma_at_full_kernel_scale_against_oracle(need_gpu):
         assert err <= RTOL, (a0, a1, err)
     # nothing outside the N-2 blocks
     assert np.abs(got[:nv + n1]).max() == 0.0
+
+
+def test_full_sigma_at_full_kernel_scale_against_cpu_arm(need_gpu, tmp_path):
+    """Every term at once: the device FP64 sigma of the kernel-scale operator (exactly as specified,
+    L ~ N(0,1)...) against the integral-direct CPU sigma of the oracle (plancpu.c: integrals formed from
+    the Cholesky vectors, the all-external term in the reference's loop form, the other couplings from
+    the plan's loop records), on the same CI vector.  1e-10 relative."""
+    refs = ["2" * 8 + "0" * 8]
+    deck = T.Deck(NINT + NVIRT, 8, 8, 16, 1, refs)
+    h, L = synthetic_operator(NINT + NVIRT, NCHOL, seed=1234)
+    op = T.Operator(h, L)
+    sb = T.SigmaBuilder(deck, op, device=0, precision="fp64")
+    x = random_civec(sb.n, 31)
+    got = sb.sigma(x)
+    sb.close()
+    p = str(tmp_path / "c2.plan")
+    T.Plan(deck, op).export(p)
+    dense.use_blas()
+    pc = dense.PlanSigmaCPU(p, L)
+    ref = pc.sigma(x)
+    pc.close()
+    assert np.abs(got - ref).max() <= RTOL * np.abs(ref).max()
