@@ -20,13 +20,17 @@ sigma    : 100-build style sigma throughput on the operator exactly as the
            kernel-scale configuration specifies (L ~ N(0,1)...), FP64 and
            tf32x3, with the per-step profile and the all-external roofline.
 latency  : p50 / p99 time-to-solution of the timed solves.
-cpu_baseline / --impl reference: the reference's integral-driven
-           all-external loop restated in C (oracle, OpenMP + OpenBLAS dgemm
-           like the reference) on a bounded sample of external indices,
-           extrapolated to a sigma build and then to a solve by the number of
-           sigma builds the FP64 solve takes.  The reference (Fortran +
-           IO_buffer submodule) cannot be compiled here, so this port is its
-           CPU arm.
+cpu_baseline / --impl reference: whole sigma builds of the same problem on the
+           host cores by the oracle's integral-direct CPU sigma
+           (oracle/plancpu.c: integrals formed from the Cholesky vectors at
+           every build as the reference does, the all-external term in the
+           reference's loop form, every other coupling replayed from the loop
+           records, OpenMP + OpenBLAS dgemm).  A step of the reference arm is
+           one such sigma build (a bounded sample of a solve); solves/s is the
+           measured sigma rate over the sigma builds a solve takes (the FP64
+           solve's iteration count, measured on the GPU).  The reference
+           (Fortran + IO_buffer submodule) cannot be compiled here, so this
+           port is its CPU arm.
 N > 1 runs independent replicas (no collective).
 """
 from __future__ import annotations
@@ -51,10 +55,10 @@ WORKLOAD = f"kernel-scale synthetic MRSDCI sigma build: 16 internal (8 inactive 
 METRIC = "Davidson solves/s at 1 \u00b5Eh vs plain FP64 GPU form; \u03c3-build TFLOP/s; p50/p99 lat"
 SOLVE_WORKLOAD = WORKLOAD.replace("sigma build", "Davidson solve (1 root)") + "; operator scaled to molecular magnitude"
 TOL_RESIDUAL, TOL_ENERGY = 1e-6, 1e-8
-# sigma builds one FP64 solve of the molecular-scale problem takes (the FP64
-# GPU solve's iteration count at 1 root); converts the oracle's sigma time
-# into a solve time for the CPU arm
-SIGMA_BUILDS_PER_SOLVE = 33
+# sigma builds one FP64 solve of the molecular-magnitude problem takes: the iterations of the FP64 GPU solve
+# of this operator (one sigma build per iteration at one root), measured on a B200 (27) and re-measured by
+# every run of this benchmark's own arm (solves.fp64.iterations); the reference arm has no GPU to count them
+SIGMA_BUILDS_PER_SOLVE = 27
 # ncu DRAM bytes (read + write) of one launch over its algorithmic bytes (the W operators): FP64 split-K
 # all-external at 120 virtuals 845.1 MB / 829.5 MB; tcgen05 all-external at 140 virtuals 809.9 MB / 773.4 MB
 TRAFFIC_RATIO = {"fp64": 845.142 / 829.498, "tf32x3": (800.509 + 9.346) / 773.381}
@@ -148,59 +152,66 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_sample(budget_s=12.0):
-    """Time the oracle's reference-form all-external loop on a bounded set of
-    external indices a (each a covers the pairs c <= a) and extrapolate."""
-    from oracle import dense, sgga
-    import tigerci_b200 as T  # noqa: F401  (deck/operator helpers only)
+def cpu_sigma_arm(molecular=True, steps=1, warmup=0, c_host=None):
+    """Times whole sigma builds of the benchmark problem with the oracle's
+    integral-direct CPU sigma (oracle/plancpu.c) on all host cores: the plan's
+    loop records exported once, then warmup + steps builds, each forming its
+    integrals from the Cholesky vectors and running every term.  Returns the
+    per-build times, the last sigma and the thread count."""
+    import tempfile
 
-    deck, op = deck_and_operator()
-    osp = sgga.build_space(sgga.Deck(deck.num_orbitals, deck.num_inactive, deck.num_active, deck.num_elec, 1,
-                                     list(deck.refs)))
+    import tigerci_b200 as T
+    from oracle import dense
+
+    deck, op = deck_and_operator(molecular=molecular)
     blas = dense.use_blas()
-    nint = N_INT_INACTIVE + N_INT_ACTIVE
-    rng = np.random.default_rng(3)
-    c = rng.standard_normal(osp.total_csfs)
-    # grow the sample until it takes ~budget_s
-    a1 = N_VIRT
-    a0 = N_VIRT - 4
-    while True:
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "plan.bin")
+        T.Plan(deck, op).export(path)
+        pc = dense.PlanSigmaCPU(path, op.chol)
+    if c_host is None:
+        c_host = np.random.default_rng(3).standard_normal(pc.n)
+        c_host /= np.linalg.norm(c_host)
+    times, sigma = [], None
+    for i in range(warmup + steps):
         t = time.perf_counter()
-        dense.allext_sigma(osp, nint, N_VIRT, op.chol, c, a_range=(a0, a1))
+        sigma = pc.sigma(c_host, integrals=True)
         dt = time.perf_counter() - t
-        if dt > budget_s / 4 or a0 == 0:
-            break
-        a0 = max(0, a1 - int((a1 - a0) * max(2.0, budget_s / max(dt, 1e-3) / 2)))
-    pairs = sum(a + 1 for a in range(a0, a1))
-    total_pairs = N_VIRT * (N_VIRT + 1) // 2
-    t_sigma = dt * total_pairs / pairs
-    threads = dense.lib().oracle_num_threads()
-    return dict(t_sigma=t_sigma, sample=f"all-external term only (the reference spends ~78% of sigma there), "
-                f"external index a in [{a0},{a1}) = {pairs} of {total_pairs} (a,c) pairs, {dt:.1f} s, "
-                f"extrapolated by pair count; OpenBLAS dgemm={'yes' if blas else 'no'}", cores=threads)
+        if i >= warmup:
+            times.append(dt)
+    pc.close()
+    return dict(times=times, sigma=sigma, cores=int(dense.lib().oracle_num_threads()), blas=blas, n=pc.n)
+
+
+CPU_SAMPLE = ("one whole sigma build per step (integrals formed from the Cholesky vectors, all-external term in "
+              "the reference's loop form, every other coupling from the loop records; OpenMP + OpenBLAS dgemm); "
+              "solves/s = 1 / (sigma time x sigma builds per FP64 solve)")
+
+
+def solve_config(n_csf):
+    return {"workload": SOLVE_WORKLOAD, "total_csfs": n_csf, "roots": 1, "tol_residual": TOL_RESIDUAL,
+            "tol_energy": TOL_ENERGY, "parallelism": "single",
+            "l2": "a solve streams the W operators (13.3 GB FP64 / 6.7 GB FP32) > L2 every sigma; "
+                  "256 MB write between timed solves"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    from oracle import dense
-
-    times = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_sample(budget_s=8.0)
-        if i >= args.warmup:
-            times.append(info["t_sigma"])
-    t_solve = float(np.mean(times)) * SIGMA_BUILDS_PER_SOLVE
-    v = 1.0 / t_solve
-    sample = info["sample"] + f"; x {SIGMA_BUILDS_PER_SOLVE} sigma builds per FP64 solve"
+    r = cpu_sigma_arm(molecular=True, steps=args.steps, warmup=args.warmup)
+    t_sigma = float(np.mean(r["times"]))
+    v = 1.0 / (t_sigma * SIGMA_BUILDS_PER_SOLVE)
+    sample = CPU_SAMPLE + f"; {SIGMA_BUILDS_PER_SOLVE} sigma builds per FP64 solve"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_solve,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_sigma,
+            "step": "one whole CPU sigma build (a bounded sample of a solve)",
+            "sigma_builds_per_solve": SIGMA_BUILDS_PER_SOLVE,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded operator of the benchmark shape)",
-            "config": {"workload": SOLVE_WORKLOAD},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": info["cores"], "kind": "port",
-                             "sample": sample},
+            "data": "synthetic (seeded operators of the benchmark shape)",
+            "config": solve_config(r["n"]),
+            "latency_ms": {"p50": 1e3 * float(np.percentile(r["times"], 50)),
+                           "p99": 1e3 * float(np.percentile(r["times"], 99)), "what": "per CPU sigma build"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["cores"], "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -591,11 +602,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1e3 * bm["t_total"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if best == "fp64" else "f64+tf32x3",
             "data": "synthetic (seeded operators of the benchmark shape)",
-            "config": {"workload": SOLVE_WORKLOAD, "form": best, "total_csfs": n_csf, "roots": 1,
-                       "tol_residual": TOL_RESIDUAL, "tol_energy": TOL_ENERGY,
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "a solve streams the W operators (13.3 GB FP64 / 6.7 GB FP32) > L2 every sigma; "
-                             "256 MB write between timed solves"},
+            "config": dict(solve_config(n_csf), parallelism="replicas" if world > 1 else "single"),
+            "form": best,
             "vs_fp64_form": (ok["fp64"]["t_total"] / bm["t_total"]) if "fp64" in ok else None,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "what": "time to solution of the timed solves"},
@@ -624,10 +632,25 @@ def main():
         except Exception as exc:
             line["local_pairs"] = {"error": str(exc)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_sample()
-        t_solve = cb["t_sigma"] * SIGMA_BUILDS_PER_SOLVE
-        line["cpu_baseline"] = {"value": 1.0 / t_solve, "unit": "solves/s", "cores": cb["cores"], "kind": "port",
-                                "sample": cb["sample"] + f"; x {SIGMA_BUILDS_PER_SOLVE} sigma builds per FP64 solve"}
+        # one whole CPU sigma build of the kernel-scale operator, on the CI vector of the device FP64 sigma
+        # builds above: its time gives the CPU solve rate (x the FP64 solve's measured iteration count), its
+        # result the full-size parity of the device FP64 sigma
+        n_sig = ok["fp64"]["iterations"][-1] if "fp64" in ok else SIGMA_BUILDS_PER_SOLVE
+        have = "fp64" in sig and "sigma" in sig["fp64"]
+        cb = cpu_sigma_arm(molecular=False, steps=1, warmup=0, c_host=sig["fp64"]["c_host"] if have else None)
+        t_sigma = cb["times"][0]
+        line["cpu_baseline"] = {"value": 1.0 / (t_sigma * n_sig), "unit": "solves/s", "cores": cb["cores"],
+                                "kind": "port", "sample": CPU_SAMPLE + f"; {n_sig} sigma builds per FP64 solve "
+                                f"(this run's FP64 GPU solve); one build, {t_sigma:.1f} s"}
+        if have:
+            ref = cb["sigma"]
+            line["parity"] = {"what": "device FP64 sigma vs the oracle's integral-direct CPU sigma, kernel-scale "
+                                      "operator, full size, same CI vector (max abs diff / max abs)",
+                              "rel_err": float(np.abs(sig["fp64"]["sigma"] - ref).max() / np.abs(ref).max()),
+                              "tolerance": 1e-10}
+            if "tf32x3" in sig and "sigma" in sig["tf32x3"]:
+                line["parity"]["mixed_rel_err"] = float(np.abs(sig["tf32x3"]["sigma"] - ref).max() / np.abs(ref).max())
+        line["sigma_builds_per_solve_fp64"] = {"measured": n_sig, "reference_arm_uses": SIGMA_BUILDS_PER_SOLVE}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

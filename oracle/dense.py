@@ -56,6 +56,7 @@ def lib():
         L.plancpu_sigma.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.plancpu_integrals.argtypes = [C.c_void_p]
         L.plancpu_free.argtypes = [C.c_void_p]
+        L.plancpu_diag.argtypes = [C.c_void_p, C.c_void_p]
         L.plancpu_total.argtypes = [C.c_void_p]
         L.plancpu_total.restype = C.c_int64
         _lib = L
@@ -267,6 +268,13 @@ class PlanSigmaCPU:
         s = np.zeros_like(c)
         lib().plancpu_sigma(self._h, c.ctypes.data, s.ctypes.data, 1 if integrals else 0)
         return s
+
+    def diag(self):
+        """H_ii (forms the integral banks first)."""
+        lib().plancpu_integrals(self._h)
+        d = np.zeros(self.n)
+        lib().plancpu_diag(self._h, d.ctypes.data)
+        return d
 
     def close(self):
         if getattr(self, "_h", None):

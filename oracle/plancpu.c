@@ -50,6 +50,7 @@ typedef struct { int64_t src, off; double coef; int64_t sbuf, sidx; } as_t;
 typedef struct { int64_t dst, off, s0, s1; } dt_t;
 typedef struct { int64_t a, b, aoff, boff, len; double coef; } ds_t;
 typedef struct { int64_t off_ab, off_aa, nsf_ab, nsf_aa, nsing, nD, dk0; } dh_t;
+typedef struct { int64_t off, len, type; double beta; int64_t foff, singlet; } dg_t;
 
 typedef struct {
   int64_t kind;
@@ -67,6 +68,7 @@ typedef struct {
   int64_t nint, n, nchol, total, npair, nD, ndh, ninit, nsig, nhvv, nwv, np, nm, ndiag;
   int64_t bufsz[NB];
   dh_t* dh;
+  dg_t* dg;
   double* hvv;
   double* wv;
   step_t* init;
@@ -112,7 +114,7 @@ void plancpu_free(void* hp) {
       step_t* s = &lists[l][i];
       free(s->gp), free(s->gs), free(s->at), free(s->as), free(s->dt), free(s->ds);
     }
-  free(p->init), free(p->sig), free(p->dh), free(p->hvv), free(p->wv), free(p->heads5);
+  free(p->init), free(p->sig), free(p->dh), free(p->dg), free(p->hvv), free(p->wv), free(p->heads5);
   free(p);
 }
 
@@ -136,7 +138,8 @@ void* plancpu_load(const char* path, const double* chol) {
   p->hvv = (double*)malloc(8 * (p->nhvv ? p->nhvv : 1));
   p->wv = (double*)malloc(8 * (p->nwv ? p->nwv : 1));
   if ((p->nhvv && rd(f, p->hvv, 8 * p->nhvv)) || (p->nwv && rd(f, p->wv, 8 * p->nwv))) goto fail;
-  if (fseek(f, 48 * p->ndiag, SEEK_CUR)) goto fail; /* diagonal entries */
+  p->dg = (dg_t*)malloc(sizeof(dg_t) * (p->ndiag ? p->ndiag : 1));
+  if (p->ndiag && rd(f, p->dg, sizeof(dg_t) * p->ndiag)) goto fail;
   p->init = (step_t*)calloc(p->ninit ? p->ninit : 1, sizeof(step_t));
   p->sig = (step_t*)calloc(p->nsig ? p->nsig : 1, sizeof(step_t));
   for (int64_t i = 0; i < p->ninit; ++i)
@@ -344,3 +347,47 @@ void plancpu_sigma(void* hp, const double* c, double* sigma, int integrals) {
 }
 
 int64_t plancpu_total(void* hp) { return ((plan_t*)hp)->total; }
+
+/* Diagonal H_ii (the preconditioner of Davidson, diag_element_mod_2.f90:83) from the plan's diagonal
+ * entries: zero-external part beta plus the same-head operators F (formed by plancpu_integrals) and the
+ * all-external diagonal (aa|aa), (aa|cc) +- (ac|ca) from the Cholesky vectors. */
+void plancpu_diag(void* hp, double* out) {
+  plan_t* p = (plan_t*)hp;
+  const int64_t n = p->n, nint = p->nint, nc = p->nchol;
+  const double* F = p->buf[B_F];
+#define PIDX(x, y) ((x) >= (y) ? (x) * ((x) + 1) / 2 + (y) : (y) * ((y) + 1) / 2 + (x))
+  double* aacc = (double*)malloc(sizeof(double) * n * n); /* (aa|cc) */
+  double* acca = (double*)malloc(sizeof(double) * n * n); /* (ac|ca) */
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t a = 0; a < n; ++a)
+    for (int64_t c = 0; c < n; ++c) {
+      const double* la = p->chol + PIDX(nint + a, nint + a) * nc;
+      const double* lc = p->chol + PIDX(nint + c, nint + c) * nc;
+      const double* lx = p->chol + PIDX(nint + a, nint + c) * nc;
+      double s1 = 0.0, s2 = 0.0;
+      for (int64_t J = 0; J < nc; ++J) s1 += la[J] * lc[J], s2 += lx[J] * lx[J];
+      aacc[a * n + c] = s1;
+      acca[a * n + c] = s2;
+    }
+#undef PIDX
+  for (int64_t k = 0; k < p->ndiag; ++k) {
+    const dg_t* d = &p->dg[k];
+    double* o = out + d->off;
+#define FD(a) (d->foff >= 0 ? F[d->foff + (a) * (n + 1)] : 0.0)
+    if (d->type == 0) {
+      o[0] = d->beta;
+    } else if (d->type == 1) {
+      for (int64_t a = 0; a < n; ++a) o[a] = d->beta + FD(a);
+    } else if (d->type == 2) {
+      for (int64_t a = 0; a < n; ++a) o[a] = d->beta + 2.0 * FD(a) + aacc[a * n + a];
+    } else {
+      int64_t e = 0;
+      for (int64_t i = 1; i < n; ++i)
+        for (int64_t j = 0; j < i; ++j, ++e)
+          o[e] = d->beta + FD(i) + FD(j) + aacc[i * n + j] + (d->singlet ? 1.0 : -1.0) * acca[i * n + j];
+    }
+#undef FD
+  }
+  free(aacc);
+  free(acca);
+}

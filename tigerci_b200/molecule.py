@@ -19,8 +19,10 @@ contraction coefficients refer to normalised primitives.
 from __future__ import annotations
 
 import ctypes as C
+import itertools
 import math
 import re
+import time
 from dataclasses import dataclass, field
 from typing import List, Sequence, Tuple
 
@@ -296,3 +298,60 @@ def n_alkane(n_carbon: int = 8, cc: float = 1.53, ch: float = 1.09) -> Tuple[Lis
 def h_chain(n: int, spacing_bohr: float) -> Tuple[List[str], np.ndarray]:
     """Linear H_n chain along z (bohr)."""
     return ["H"] * n, np.array([[0.0, 0.0, i * spacing_bohr] for i in range(n)])
+
+
+# ---- MRSDCI problems of a molecule ---------------------------------------------------------------------
+
+def cas_references(n_inactive: int, n_act_el: int, n_act_orb: int, spin_mult: int = 1) -> List[str]:
+    """REFERENCE OCCUPATIONS of a complete active space: every occupation (0, 1, 2 per active orbital) with
+    n_act_el electrons that can couple to the spin multiplicity, the inactive orbitals doubly occupied."""
+    refs = []
+    for occ in itertools.product((2, 1, 0), repeat=n_act_orb):
+        if sum(occ) != n_act_el:
+            continue
+        singles = occ.count(1)
+        if singles < spin_mult - 1 or (singles - (spin_mult - 1)) % 2:
+            continue
+        refs.append("2" * n_inactive + "".join(str(x) for x in occ))
+    return refs
+
+
+def mrsdci_problem(symbols, coords_bohr, basis: str = "cc-pVDZ", pure_d: bool = True, n_frozen: int = 0,
+                   cas=(4, 4), spin_mult: int = 1, cd_threshold: float = 1e-6, refs=None):
+    """Deck and MO operator of a CAS-reference MRSDCI on canonical RHF orbitals: AO integrals, pivoted
+    Cholesky at cd_threshold, RHF, AO -> MO transform.  cas = (active electrons, active orbitals) taken
+    from the top of the doubly occupied and the bottom of the virtual orbitals; the remaining doubly
+    occupied orbitals are inactive, the lowest n_frozen of them frozen.  refs overrides the complete
+    active space list.  Returns (Deck, Operator with the nuclear repulsion as core energy, info)."""
+    from .api import Deck, Operator
+
+    t0 = time.perf_counter()
+    mol = Molecule.from_atoms(symbols, coords_bohr, basis, pure_d=pure_d)
+    it = Integrals(mol, cd_threshold)
+    t1 = time.perf_counter()
+    nel = mol.n_electrons
+    if nel % 2:
+        raise ValueError("closed-shell RHF orbitals need an even number of electrons")
+    nocc = nel // 2
+    Cm, eps, e_scf, n_scf = it.rhf(nocc)
+    t2 = time.perf_counter()
+    h, L = it.mo_operator(Cm)
+    t3 = time.perf_counter()
+    n_act_el, n_act = cas
+    n_inactive = nocc - n_act_el // 2
+    if n_act_el % 2 or n_inactive < n_frozen or n_inactive + n_act > it.nbf:
+        raise ValueError("inconsistent active space")
+    refs = list(refs) if refs is not None else cas_references(n_inactive, n_act_el, n_act, spin_mult)
+    deck = Deck(it.nbf, n_inactive, n_act, nel, spin_mult, refs, num_frozen=n_frozen)
+    op = Operator(h, L, it.nuclear_repulsion)
+    info = {"nbf": it.nbf, "nchol": it.nchol, "e_scf": e_scf, "scf_iterations": n_scf, "n_refs": len(refs),
+            "seconds": {"integrals_cholesky": t1 - t0, "scf": t2 - t1, "mo_transform": t3 - t2}}
+    it.close()
+    return deck, op, info
+
+
+def water_c1(cd_threshold: float = 1e-6):
+    """H2O (R(O-H) 0.9572 A, HOH 104.52 deg), cc-pVDZ (24 functions), O 1s frozen, CAS(4,4) on canonical RHF
+    orbitals (19 references), singlet."""
+    sym, xyz = water()
+    return mrsdci_problem(sym, xyz, "cc-pVDZ", pure_d=True, n_frozen=1, cas=(4, 4), cd_threshold=cd_threshold)
