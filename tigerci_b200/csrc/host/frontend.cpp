@@ -565,55 +565,114 @@ void decompose(Integrals& it, double thresh) {
   it.cd_threshold = thresh;
 }
 
-// Eigen-decomposition of a symmetric matrix (row major n x n) by cyclic Jacobi rotations; w ascending,
-// eigenvectors as the columns of V.
-void jacobi_eigh(int n, std::vector<double> A, std::vector<double>& w, std::vector<double>& V) {
-  V.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
-  for (int sweep = 0; sweep < 100; ++sweep) {
-    double off = 0.0, tot = 0.0;
-    for (int i = 0; i < n; ++i)
-      for (int j = 0; j < n; ++j) {
-        const double x = A[(size_t)i * n + j] * A[(size_t)i * n + j];
-        tot += x;
-        if (i != j) off += x;
+// Eigen-decomposition of a symmetric matrix (row major n x n): Householder reduction to tridiagonal form
+// (A = Q T Q^T, one reflector per column) and the implicit QL iteration with Wilkinson shifts on T
+// (the Wilkinson-Reinsch procedures tred2 / tql2, Handbook for Automatic Computation II, 1971), the plane
+// rotations accumulated into Q.  w ascending, eigenvectors as the columns of V.
+void eigh_sym(int n, std::vector<double> A, std::vector<double>& w, std::vector<double>& V) {
+  std::vector<double> Q((size_t)n * n, 0.0), v(n), pv(n), u(n);
+  for (int i = 0; i < n; ++i) Q[(size_t)i * n + i] = 1.0;
+  for (int k = 0; k + 2 < n; ++k) {
+    double nrm = 0.0;
+    for (int i = k + 1; i < n; ++i) nrm += A[(size_t)i * n + k] * A[(size_t)i * n + k];
+    nrm = std::sqrt(nrm);
+    if (nrm < 1e-300) continue;
+    const double x0 = A[(size_t)(k + 1) * n + k];
+    const double alpha = x0 > 0 ? -nrm : nrm;
+    std::fill(v.begin(), v.end(), 0.0);
+    for (int i = k + 1; i < n; ++i) v[i] = A[(size_t)i * n + k];
+    v[k + 1] -= alpha;
+    double vn = 0.0;
+    for (int i = k + 1; i < n; ++i) vn += v[i] * v[i];
+    vn = std::sqrt(vn);
+    if (vn < 1e-300) continue;
+    for (int i = k + 1; i < n; ++i) v[i] /= vn;
+    // H A H = A - 2 (v q^T + q v^T), p = A v, q = p - (v.p) v
+    double K = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      const double* a = &A[(size_t)i * n];
+      for (int j = k + 1; j < n; ++j) s += a[j] * v[j];
+      pv[i] = s;
+      K += v[i] * s;
+    }
+    for (int i = 0; i < n; ++i) pv[i] -= K * v[i];
+    for (int i = 0; i < n; ++i) {
+      double* a = &A[(size_t)i * n];
+      const double vi = v[i], qi = pv[i];
+      for (int j = 0; j < n; ++j) a[j] -= 2.0 * (vi * pv[j] + qi * v[j]);
+    }
+    // Q <- Q H
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      const double* q = &Q[(size_t)i * n];
+      for (int j = k + 1; j < n; ++j) s += q[j] * v[j];
+      u[i] = s;
+    }
+    for (int i = 0; i < n; ++i) {
+      double* q = &Q[(size_t)i * n];
+      const double ui = 2.0 * u[i];
+      for (int j = k + 1; j < n; ++j) q[j] -= ui * v[j];
+    }
+  }
+  std::vector<double> d(n), e(n, 0.0);
+  for (int i = 0; i < n; ++i) d[i] = A[(size_t)i * n + i];
+  for (int i = 0; i + 1 < n; ++i) e[i] = A[(size_t)(i + 1) * n + i];  // e[i] couples i and i + 1
+  const double eps = 2.220446049250313e-16;
+  for (int l = 0; l < n; ++l) {
+    for (int iter = 0; iter < 200; ++iter) {
+      int m = l;
+      for (; m + 1 < n; ++m) {
+        const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= eps * dd) break;
       }
-    if (off <= 1e-30 * std::max(tot, 1e-300)) break;
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = A[(size_t)p * n + q];
-        if (std::fabs(apq) < 1e-300) continue;
-        const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-        for (int k = 0; k < n; ++k) {  // columns p, q
-          const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
-          A[(size_t)k * n + p] = c * akp - s * akq;
-          A[(size_t)k * n + q] = s * akp + c * akq;
+      if (m == l) break;
+      // Wilkinson shift from the leading 2 x 2 block of the unreduced part
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool deflated = false;
+      for (; i >= l; --i) {
+        const double f = s * e[i], b = c * e[i];
+        r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {  // underflow: split here
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          deflated = true;
+          break;
         }
-        for (int k = 0; k < n; ++k) {  // rows p, q
-          const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
-          A[(size_t)p * n + k] = c * apk - s * aqk;
-          A[(size_t)q * n + k] = s * apk + c * aqk;
-        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
         for (int k = 0; k < n; ++k) {
-          const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
-          V[(size_t)k * n + p] = c * vkp - s * vkq;
-          V[(size_t)k * n + q] = s * vkp + c * vkq;
+          double* q = &Q[(size_t)k * n];
+          const double t = q[i + 1];
+          q[i + 1] = s * q[i] + c * t;
+          q[i] = c * q[i] - s * t;
         }
       }
+      if (deflated) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
   }
   std::vector<int> ord(n);
   for (int i = 0; i < n; ++i) ord[i] = i;
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return A[(size_t)a * n + a] < A[(size_t)b * n + b]; });
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return d[a] < d[b]; });
   w.resize(n);
-  std::vector<double> V2((size_t)n * n);
+  V.assign((size_t)n * n, 0.0);
   for (int j = 0; j < n; ++j) {
-    w[j] = A[(size_t)ord[j] * n + ord[j]];
-    for (int i = 0; i < n; ++i) V2[(size_t)i * n + j] = V[(size_t)i * n + ord[j]];
+    w[j] = d[ord[j]];
+    for (int i = 0; i < n; ++i) V[(size_t)i * n + j] = Q[(size_t)i * n + ord[j]];
   }
-  V.swap(V2);
 }
 
 // C = A (m x k) * B (k x n), row major, plain blocked loops (small matrices).
@@ -816,7 +875,7 @@ extern "C" int tci_rhf(const tci_integrals* it, int64_t n_occ, int64_t maxit, do
     for (size_t i = 0; i < h.size(); ++i) h[i] = T[i] + V[i];
     // symmetric orthogonaliser X = S^-1/2
     std::vector<double> sw, sv;
-    tci::jacobi_eigh(n, S, sw, sv);
+    tci::eigh_sym(n, S, sw, sv);
     if (sw[0] < 1e-9) throw Error(TCI_ERR_INPUT, "tci_rhf: near-linearly-dependent basis (overlap eigenvalue < 1e-9)");
     std::vector<double> X((size_t)n * n, 0.0);
     for (int i = 0; i < n; ++i)
@@ -829,7 +888,7 @@ extern "C" int tci_rhf(const tci_integrals* it, int64_t n_occ, int64_t maxit, do
       std::vector<double> t1((size_t)n * n), Fp((size_t)n * n), Cp;
       tci::matmul(n, n, n, X.data(), F.data(), t1.data(), true);  // X^T F (X symmetric)
       tci::matmul(n, n, n, t1.data(), X.data(), Fp.data());
-      tci::jacobi_eigh(n, Fp, e, Cp);
+      tci::eigh_sym(n, Fp, e, Cp);
       Cout.resize((size_t)n * n);
       tci::matmul(n, n, n, X.data(), Cp.data(), Cout.data());
     };

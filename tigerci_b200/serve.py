@@ -9,9 +9,10 @@ requests in flight overlap on the GPU.
 
 `hn_chain_stream` generates the serving workload: a seeded Poisson stream of
 linear H_n chain solves (n even in 8..24, H-H spacing in [1.4, 3.0] bohr,
-cc-pVDZ sizes: 5 n orbitals, singlet, 1-4 roots).  No integral engine is
-part of this package, so `request_problem` stands in a seeded synthetic MO
-operator with the chain's orbital counts; see its docstring.
+cc-pVDZ: 5 n orbitals, singlet, 1-4 roots).  `chain_problem` builds a
+request's deck and MO operator through the molecular front end (RHF/cc-pVDZ
+orbitals, Cholesky vectors); `request_problem` is a fast synthetic stand-in
+with the same sizes for scheduling tests.
 """
 from __future__ import annotations
 
@@ -175,3 +176,18 @@ def request_problem(spec: RequestSpec, seed: int = 7):
     h, L = synthetic_operator(nbf, 4 * nbf, seed=seed * 100003 + spec.index, scale=scale, diag_range=(-2.0, 1.0),
                               offdiag_sigma=0.02)
     return deck, Operator(h, L)
+
+
+def chain_problem(spec: RequestSpec, cd_threshold: float = 1e-6, n_active: int = 2):
+    """Deck and MO operator of an H_n chain request through the molecular front end: cc-pVDZ (5 n functions),
+    canonical RHF orbitals, Cholesky vectors of the AO integrals at cd_threshold transformed to them,
+    nuclear repulsion as the core energy.  The references are the complete active space of the n_active
+    orbitals around the Fermi level (n_active electrons: HOMO/LUMO, occupations 20, 11, 02 for the default
+    2), the other occupied orbitals inactive.  A full CAS(n/2, n/2) reference list (tens of thousands of
+    occupations for n = 24) makes the MRCI space of the longer chains intractable for any solver."""
+    from .molecule import h_chain, mrsdci_problem
+
+    sym, xyz = h_chain(spec.n_atoms, spec.spacing)
+    deck, op, _ = mrsdci_problem(sym, xyz, "cc-pVDZ", pure_d=True, n_frozen=0, cas=(n_active, n_active),
+                                 cd_threshold=cd_threshold)
+    return deck, op
