@@ -356,6 +356,120 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
     }
 }
 
+// Row-panel FP64 GEMM for problems with few rows and long rows of B (the all-external product Y = U W: a
+// few dozen gathered CI rows against the np x np operator): C (M x N) = beta C + sum over the segments of
+// alpha A B, A M x K and B K x N row major, M <= MT.  A block of 256 threads owns 128 columns of one problem
+// (tile_begin counts these column blocks).  B streams through shared memory in PANEL_KS-deep k slices by
+// 16-byte cp.async copies, PANEL_STG slices in flight (B is read from HBM exactly once, and enough bytes
+// are in flight to cover its latency); A's slices come the same way from L2.  Warp w computes rows
+// (w / 2) * MT/4 ... of the columns (w % 2) * 64 + 2 lane, +1: per pair of k a thread reads two 16-byte
+// B pairs and MT/4 16-byte A pairs (the same address across the warp) for MT FMAs.  Operands must start
+// on 16 bytes with even leading dimensions and every segment's alpha must be 1 (checked when the step is
+// lowered).  Sums: segments in table order, k ascending.
+constexpr int PANEL_T = 256;
+constexpr int PANEL_COLS = 128;
+constexpr int PANEL_KS = 16;
+constexpr int PANEL_STG = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int MT>
+__global__ void __launch_bounds__(PANEL_T, 2) gemm_panel_f64(const DGemmProblem* __restrict__ probs, int nprob,
+                                                             const DGemmSeg* __restrict__ segs) {
+  constexpr int R = MT / 4;  // rows per warp
+  static_assert(MT % 8 == 0, "MT multiple of 8");
+  extern __shared__ __align__(16) double panel_smem[];
+  double* Ws = panel_smem;                                   // [PANEL_STG][PANEL_KS][PANEL_COLS]
+  double* As = panel_smem + PANEL_STG * PANEL_KS * PANEL_COLS;  // [PANEL_STG][MT][PANEL_KS]
+  const long long tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const DGemmProblem P = probs[lo];
+  const long long n0 = (tile - P.tile_begin) * PANEL_COLS;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = (warp >> 1) * R;
+  const int col = (warp & 1) * 64 + 2 * lane;  // this thread's two columns n0 + col, + 1
+  double acc[R][2];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = 0.0;
+  for (long long sgi = P.seg_begin; sgi < P.seg_end; ++sgi) {
+    const DGemmSeg S = segs[sgi];
+    const long long K = S.K;
+    const long long nsl = (K + PANEL_KS - 1) / PANEL_KS;
+    // one k slice of B (PANEL_KS x 128) and A (MT x PANEL_KS) into stage st, zero past the edges
+    auto issue = [&](long long sl, int st) {
+      const long long k0 = sl * PANEL_KS;
+      double* w = Ws + (size_t)st * PANEL_KS * PANEL_COLS;
+#pragma unroll
+      for (int u = 0; u < (PANEL_KS * PANEL_COLS / 2) / PANEL_T; ++u) {
+        const int e = tid + u * PANEL_T;               // 16-byte chunk
+        const int kk = e / (PANEL_COLS / 2), cc = 2 * (e % (PANEL_COLS / 2));
+        const long long gk = k0 + kk, gn = n0 + cc;
+        const int bytes = (gk < K && gn < P.N) ? (gn + 1 < P.N ? 16 : 8) : 0;
+        cp_async16(w + kk * PANEL_COLS + cc, bytes ? (const void*)(S.B + gk * S.ldb + gn) : (const void*)S.B, bytes);
+      }
+      double* a = As + (size_t)st * MT * PANEL_KS;
+      for (int e = tid; e < MT * PANEL_KS / 2; e += PANEL_T) {
+        const int m = e / (PANEL_KS / 2), kk = 2 * (e % (PANEL_KS / 2));
+        const long long gk = k0 + kk;
+        const int bytes = (m < P.M && gk < K) ? (gk + 1 < K ? 16 : 8) : 0;
+        cp_async16(a + m * PANEL_KS + kk, bytes ? (const void*)(S.A + m * S.lda + gk) : (const void*)S.A, bytes);
+      }
+    };
+    __syncthreads();  // the previous segment's stages have been read
+#pragma unroll
+    for (int st = 0; st < PANEL_STG - 1; ++st) {
+      if (st < nsl) issue(st, st);
+      cp_async_commit();
+    }
+    for (long long sl = 0; sl < nsl; ++sl) {
+      cp_async_wait<PANEL_STG - 2>();  // this thread's copies of slice sl have landed
+      __syncthreads();                 // everyone's have, and slice sl - 1 has been read
+      if (sl + PANEL_STG - 1 < nsl) issue(sl + PANEL_STG - 1, (int)((sl + PANEL_STG - 1) % PANEL_STG));
+      cp_async_commit();
+      const int st = (int)(sl % PANEL_STG);
+      const double* w = Ws + (size_t)st * PANEL_KS * PANEL_COLS + col;
+      const double* a = As + (size_t)st * MT * PANEL_KS + r0 * PANEL_KS;
+#pragma unroll
+      for (int kp = 0; kp < PANEL_KS / 2; ++kp) {
+        const double2 w0 = *reinterpret_cast<const double2*>(w + (2 * kp) * PANEL_COLS);
+        const double2 w1 = *reinterpret_cast<const double2*>(w + (2 * kp + 1) * PANEL_COLS);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double2 x = *reinterpret_cast<const double2*>(a + r * PANEL_KS + 2 * kp);
+          acc[r][0] = fma(x.y, w1.x, fma(x.x, w0.x, acc[r][0]));
+          acc[r][1] = fma(x.y, w1.y, fma(x.x, w0.y, acc[r][1]));
+        }
+      }
+    }
+    cp_async_wait<0>();
+  }
+  const long long n = n0 + col;
+  if (n >= P.N) return;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const long long m = r0 + r;
+    if (m >= P.M) break;
+    double* c = P.C + m * P.ldc + n;
+    c[0] = (P.beta == 0.0) ? acc[r][0] : fma(P.beta, c[0], acc[r][0]);
+    if (n + 1 < P.N) c[1] = (P.beta == 0.0) ? acc[r][1] : fma(P.beta, c[1], acc[r][1]);
+  }
+}
+template <int MT>
+constexpr size_t panel_smem_bytes() {
+  return sizeof(double) * (size_t)PANEL_STG * PANEL_KS * (PANEL_COLS + MT);
+}
+
 // Segmented AXPY: target chunk t (at most AXPY_CHUNK elements) gets
 //   dst[i] += sum_s coef_s * scale_s * src_s[base + i].
 // One block per chunk; warp w takes the sources w, w + 8, ... in table order,
@@ -856,6 +970,10 @@ struct DevStep {
   long long tma_rows = 0;  // kinds 4, 6, 7: rows of the gathered coefficients / of the exchange bank
   long long tma_aux2 = 0;  // kind 7: offset of the exchange bank in BUF_JK
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
+  // FP64 all-external problems on the row-panel kernel, by row class (M <= 16, 24, 32, 40, 48)
+  DGemmProblem* panel_probs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int panel_nprob[5] = {0, 0, 0, 0, 0};
+  long long panel_ntiles[5] = {0, 0, 0, 0, 0};
   DGemmProblem* skinny_probs = nullptr;
   int skinny_nprob = 0;
   long long skinny_nwarps = 0;
@@ -1233,12 +1351,26 @@ struct tci_ctx {
       d.segs = upload(sg, owned, stream);
       {
         // FP64 form: skinny problems (one-row products) to the warp-per-column kernel, the rest tiled
-        std::vector<DGemmProblem> reg, sk;
-        long long rt = 0, wk = 0;
+        std::vector<DGemmProblem> reg, sk, pan[5];
+        long long rt = 0, wk = 0, pt[5] = {0, 0, 0, 0, 0};
         for (const auto& g : pr) {
           bool skinny = g.M <= SKINNY_M && s.name != "all-external";
           for (long long q = g.seg_begin; skinny && q < g.seg_end; ++q) skinny = sg[(size_t)q].tA == 0 && sg[(size_t)q].tB == 1;
-          if (skinny) {
+          // the all-external product (a few dozen CI rows x the operator) on the row-panel kernel
+          bool panel = s.name == "all-external" && g.M <= 48;
+          for (long long q = g.seg_begin; panel && q < g.seg_end; ++q) {
+            const DGemmSeg& x = sg[(size_t)q];
+            panel = x.tA == 0 && x.tB == 0 && x.alpha == 1.0 && ((x.lda | x.ldb) & 1) == 0 &&
+                    ((reinterpret_cast<uintptr_t>(x.A) | reinterpret_cast<uintptr_t>(x.B)) & 15) == 0;
+          }
+          if (panel) {
+            const int c = (int)((g.M + 7) / 8) - 1;  // MT = 8 (c + 1), classes 16 ... 48
+            const int cls = std::max(1, c) - 1;       // 0: MT 16, 1: 24, 2: 32, 3: 40, 4: 48
+            DGemmProblem x = g;
+            x.tile_begin = pt[cls];
+            pt[cls] += (g.N + PANEL_COLS - 1) / PANEL_COLS;
+            pan[cls].push_back(x);
+          } else if (skinny) {
             DGemmProblem x = g;
             x.tile_begin = wk;  // first warp (one per output column); a block of 8 warps stays in one problem
             wk += (g.N + 7) / 8 * 8;
@@ -1256,6 +1388,11 @@ struct tci_ctx {
         d.skinny_probs = upload(sk, owned, stream);
         d.skinny_nprob = (int)sk.size();
         d.skinny_nwarps = wk;
+        for (int c = 0; c < 5; ++c) {
+          d.panel_probs[c] = upload(pan[c], owned, stream);
+          d.panel_nprob[c] = (int)pan[c].size();
+          d.panel_ntiles[c] = pt[c];
+        }
       }
       if (s.name != "all-external" && !pr.empty()) {
         // Mixed form.  Segments whose operand is a same-head one-electron-like operator (BUF_F: h, J_ii,
@@ -1445,6 +1582,20 @@ struct tci_ctx {
            (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready) || (s.tma_kind == 6 && tma_dv_ready) ||
            (s.tma_kind == 7 && tma_dvr_ready);
   }
+  template <int MT>
+  void launch_panel(const DevStep& s, int c) {
+    if (s.panel_ntiles[c] <= 0) return;
+    constexpr size_t smem = panel_smem_bytes<MT>();
+    static bool attr_set[64] = {};  // per device
+    int dev = 0;
+    TCI_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+      TCI_CUDA(cudaFuncSetAttribute(gemm_panel_f64<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_set[dev] = true;
+    }
+    gemm_panel_f64<MT><<<(unsigned)s.panel_ntiles[c], PANEL_T, smem, stream>>>(s.panel_probs[c], s.panel_nprob[c],
+                                                                               s.segs);
+  }
   // the mixed form runs this GEMM step on the tensor cores
   bool uses_tc(const DevStep& s) const {
     return precision == 1 && s.probs_tc && (tc_mode == 1 || (tc_mode == 0 && s.tc_ok));
@@ -1466,6 +1617,8 @@ struct tci_ctx {
         continue;
       }
       if (s.kind == STEP_GEMM && s.skinny_nwarps > 0) k += 1;
+      if (s.kind == STEP_GEMM)
+        for (int c = 0; c < 5; ++c) k += s.panel_ntiles[c] > 0 ? 1 : 0;
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
           ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && plan.nD > 0))
         k += 1;
@@ -1840,6 +1993,11 @@ struct tci_ctx {
         if (s.skinny_nwarps > 0)
           gemm_skinny_f64<<<(unsigned)((s.skinny_nwarps + 7) / 8), 256, 0, stream>>>(s.skinny_probs, s.skinny_nprob,
                                                                                   s.segs, s.skinny_nwarps);
+        launch_panel<16>(s, 0);
+        launch_panel<24>(s, 1);
+        launch_panel<32>(s, 2);
+        launch_panel<40>(s, 3);
+        launch_panel<48>(s, 4);
         if (s.ntiles > 0) {
           if (s.cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
           else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
