@@ -337,6 +337,86 @@ def molecular_measure(device, steps=3, warmup=1):
     return out
 
 
+def local_solve_measure(device, nchol=2400):
+    """The batching configuration as a Davidson solve: 35 doubly occupied internal orbitals (630 internal
+    pairs), 400 externals, every pair and single-hole path with a random domain of 20..180 externals (seed
+    99), Cholesky rank 2400, operator at molecular magnitude; 1 root, residual 1e-6.  The all-external term
+    runs in the pair-domain Cholesky form (grouped GEMMs over uneven domains), every other term on the
+    non-local plan with the blocks padded to all externals; FP64 and mixed forms."""
+    import torch
+
+    import tigerci_b200 as T
+    from tigerci_b200 import local
+    from tigerci_b200.synthetic import synthetic_operator
+
+    deck = local.pair_domain_deck()
+    h, L = synthetic_operator(deck.num_orbitals, nchol, seed=1234, scale=0.02, diag_range=(-2.0, 1.0),
+                              offdiag_sigma=0.02)
+    op = T.Operator(h, L)
+    out = {"workload": "local MRSDCI: 35 doubly occupied internal orbitals (630 pair paths), 400 externals, "
+                       "domains U{20..180} per pair and single-hole path (seed 99), Cholesky rank 2400, molecular "
+                       "magnitude; 1 root, residual 1e-6, energy tolerance 1e-8"}
+    for form in ("tf32x3", "fp64"):
+        t = time.perf_counter()
+        sb = T.SigmaBuilder(deck, op, device=device, precision=form)
+        init_s = time.perf_counter() - t
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        e, _, it = sb.davidson(1, TOL_RESIDUAL, TOL_ENERGY)
+        b.record()
+        torch.cuda.synchronize()
+        st = sb.stats()
+        out["total_csfs"] = sb.n
+        sb.profile(False, davidson_phases=True)
+        sb.davidson(1, TOL_RESIDUAL, TOL_ENERGY)
+        phases = {k: round(v, 1) for k, v in sb.davidson_phase_times().items()}
+        sb.close()
+        out[form] = {"energy": float(e[0]), "iterations": int(it), "ms_per_solve": a.elapsed_time(b),
+                     "solves_per_s": 1e3 / a.elapsed_time(b), "init_s": init_s, "phase_ms": phases,
+                     "device_gb": st["device_bytes"] / 1e9}
+    out["mixed_minus_fp64"] = out["tf32x3"]["energy"] - out["fp64"]["energy"]
+    out["within_1uEh"] = abs(out["mixed_minus_fp64"]) <= 1e-6
+    out["vs_fp64_form"] = out["fp64"]["ms_per_solve"] / out["tf32x3"]["ms_per_solve"]
+    return out
+
+
+def octane_measure(device, nroots=3):
+    """The precision configuration: all-trans n-octane / cc-pVDZ (202 functions), 8 C 1s frozen, CAS(8,8)
+    active space on RHF orbitals with the references of tigerci_b200.molecule.OCTANE_REFS, 3 roots; the mixed
+    form (3xTF32 contractions, FP64 Davidson, FP64 finish) against the plain FP64 GPU form."""
+    import torch
+
+    import tigerci_b200 as T
+    from tigerci_b200 import molecule as M
+
+    t0 = time.perf_counter()
+    deck, op, info = M.octane_c3()
+    out = {"workload": "n-octane (all-trans, staggered), cc-pVDZ (202 functions), 8 C 1s frozen, CAS(8,8) active "
+                       f"space, references {list(M.OCTANE_REFS)} over it, singlet, {nroots} roots, CD 1e-6, residual "
+                       "1e-6 (energy tolerance 1e-10)",
+           "front_end_s": time.perf_counter() - t0, "nchol": info["nchol"], "e_scf": info["e_scf"]}
+    for form in ("fp64", "tf32x3"):
+        t = time.perf_counter()
+        sb = T.SigmaBuilder(deck, op, device=device, precision=form)
+        init_s = time.perf_counter() - t
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        e, _, it = sb.davidson(nroots, 1e-6, 1e-10)
+        b.record()
+        torch.cuda.synchronize()
+        out["total_csfs"] = sb.n
+        st = sb.stats()
+        sb.close()
+        out[form] = {"energies": [float(x) + op.core_energy for x in e], "iterations": int(it),
+                     "ms_per_solve": a.elapsed_time(b), "init_s": init_s, "sigma_flops": st["flops_per_sigma"]}
+    out["mixed_minus_fp64"] = [x - y for x, y in zip(out["tf32x3"]["energies"], out["fp64"]["energies"])]
+    out["max_abs_diff_uEh"] = 1e6 * max(abs(x) for x in out["mixed_minus_fp64"])
+    out["vs_fp64_form"] = out["fp64"]["ms_per_solve"] / out["tf32x3"]["ms_per_solve"]
+    return out
+
+
 def molecular_cpu(mol):
     """The oracle on the same water problem: its Davidson over the integral-direct CPU sigma (integrals formed
     at every build), timed, and the device FP64 root's distance from it."""
@@ -440,6 +520,8 @@ def main():
     ap.add_argument("--acpf-solves", type=int, default=3, help="timed ACPF solves on the solve operator (0: skip)")
     ap.add_argument("--local-only", action="store_true", help="only the pair-domain measurement")
     ap.add_argument("--no-molecular", action="store_true", help="skip the water (front end) measurement")
+    ap.add_argument("--octane-only", action="store_true", help="only the n-octane precision measurement")
+    ap.add_argument("--local-solve-only", action="store_true", help="only the pair-domain Davidson solve")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -479,6 +561,14 @@ def main():
     if args.serve_only:
         if rank == 0:
             print(json.dumps({"serving": serve_measure(args.serve_requests, args.serve_slots, local, planners=args.serve_planners)}), flush=True)
+        return
+    if args.local_solve_only:
+        if rank == 0:
+            print(json.dumps({"local_solve": local_solve_measure(local)}), flush=True)
+        return
+    if args.octane_only:
+        if rank == 0:
+            print(json.dumps({"octane_c3": octane_measure(local)}), flush=True)
         return
     if args.local_only:
         if rank == 0:

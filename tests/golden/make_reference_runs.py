@@ -11,7 +11,9 @@ For each run (tests/Tests/<run>/ in the reference tree) the fixture holds:
 - what the run printed: "Number of cholesky vectors", "the reference energy
   is (elec + nuclear)", every "Root k total energy", and the final
   "Best guess wavefunction summary" of each root (coefficient, spin function,
-  arc weight, internal occupation, virtuals).
+  arc weight, internal occupation, virtuals) with the residual norm |Hc - Ec|
+  of the last iteration (the run stops on the energy change, so its printed
+  coefficients carry an error of that order).
 
 Run once in an environment that has the reference tree:
     python tests/golden/make_reference_runs.py <reference tree>
@@ -75,6 +77,16 @@ def listings(lines):
     return [res[r] for r in sorted(res)]
 
 
+def final_residuals(lines):
+    """|Hc - Ec| of the last Davidson iteration of every root (the iteration tables' rows)."""
+    res = {}
+    for ln in lines:
+        m = re.match(r"\s+(\d+)\s+(\d+)\s+(-?\d\.\d+D[+-]\d+)\s+(\d\.\d+D[+-]\d+)\s+(\d\.\d+D[+-]\d+)\s+[\d.]+\s*$", ln)
+        if m:
+            res[int(m.group(2))] = float(m.group(4).replace("D", "E"))
+    return [res[r] for r in sorted(res)]
+
+
 def grab(lines, pattern):
     return [float(m.group(1)) for ln in lines for m in [re.search(pattern, ln)] if m]
 
@@ -117,6 +129,7 @@ def main(ref_root):
                 "reference_energy": grab(out, r"the reference energy is \(elec \+ nuclear\) =\s*(-?\d+\.\d+)")[0],
                 "roots": grab(out, r"Root\s+\d+ total energy \(electronic \+ nuclear\) is :\s*(-?\d+\.\d+)"),
                 "listings": listings(out),
+                "final_residual_norms": final_residuals(out),
             },
         })
     path = os.path.join(HERE, "reference_runs.json")

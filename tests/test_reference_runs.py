@@ -16,7 +16,9 @@ reference printed: the number of Cholesky vectors (exactly), the closed-shell
 reference energy, every root's total energy (within the 1e-6 Eh tolerance
 of the reference's own test scripts, tests/Tests/*/driver.sh), and the final
 wavefunction listing of each root (the ten largest |c| with their spin
-function, arc weight, internal occupation and virtual orbitals)."""
+function, arc weight, internal occupation and virtual orbitals; |c| within
+the residual norm the reference's last iteration printed, since it stops on
+the energy change with |Hc - Ec| of a few 1e-4 left)."""
 import json
 import os
 
@@ -137,8 +139,11 @@ def test_sdci_roots_and_wavefunction_listing_match_reference(r, need_gpu):
         # may swap entries of equal magnitude, so compare the entries both lists hold
         common = set(got) & set(want)
         assert len(common) >= len(want) - 1, (sorted(got.items()), sorted(want.items()))
+        # the reference stops on the energy change, with |Hc - Ec| of a few 1e-4 left: its printed
+        # coefficients are that far from the converged ones (plus the print's 6 digits)
+        tol = r["printed"]["final_residual_norms"][root] + 5e-6
         for key in common:
-            assert abs(got[key] - want[key]) <= 5e-6 * max(1.0, want[key]) + 1e-6, (key, got[key], want[key])
+            assert abs(got[key] - want[key]) <= tol, (key, got[key], want[key], tol)
 
 
 @pytest.mark.gpu

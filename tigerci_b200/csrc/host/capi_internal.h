@@ -16,8 +16,18 @@ void operator_from_c(const tci_operator* op, const CsfSpace& sp, Operator& out);
 // refine (mixed form): finish every root as an FP64 Rayleigh quotient, 1 with a plain-FP64 sigma build
 // (keeps the FP64 W), 2 with every term FP64 but the all-external one (default), 3 as 2 with the
 // three-external contractions on the tensor cores too, 0 not at all.
+// Local pair domains: the local space, its CSFs' indices in the non-local space of the same deck (the
+// plan's layout), the heads of the pair-domain all-external term (7 int64 each, as tci_local_create takes
+// them) with their domains, and the (aa|cc), (ac|ca) arrays of the all-external diagonal.
+struct LocalSetup {
+  CsfSpace loc;
+  std::vector<long long> map;
+  std::vector<int64_t> heads7, dom_idx;
+  std::vector<double> xdiag;
+};
+void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls);
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
-                  tci_ctx** out, int64_t refine = 2);
+                  tci_ctx** out, int64_t refine = 2, LocalSetup* ls = nullptr);
 // Selects the GEMM steps that run on the tensor cores in the mixed form (tci_sigma_init_ex options[2]).
 void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode);
 // Device bytes of such a context: peak during set-up and held afterwards.

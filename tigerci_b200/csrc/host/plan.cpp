@@ -187,6 +187,8 @@ struct Builder {
   std::map<std::tuple<int, i64, i64>, i64> fdiag;
   void build_diag();
 
+  bool with_allext = true;     // false: no all-external term (no X, W, WBUILD or all-external steps)
+
   Builder(const CsfSpace& s, const Operator& o, Plan& p) : sp(s), op(o), P(p) {}
 
   i64 Jof(i64 i, i64 j) const { return offJ + (i * nint + j) * n2; }
@@ -1397,8 +1399,9 @@ void Builder::init_steps() {
   // packed external pairs (a>=b): rows a(a+1)/2 + b, contiguous in L for each a
   const i64 npk = n * (n + 1) / 2;
   Scratch Ti;
-  const i64 Lpk_off = Ti.alloc(npk * N);
-  for (i64 a = 0; a < n; ++a) g1(BUF_T0, Lpk_off + (a * (a + 1) / 2) * N, (a + 1) * N, Ints::pair(nint + a, nint));
+  const i64 Lpk_off = with_allext ? Ti.alloc(npk * N) : 0;
+  if (with_allext)
+    for (i64 a = 0; a < n; ++a) g1(BUF_T0, Lpk_off + (a * (a + 1) / 2) * N, (a + 1) * N, Ints::pair(nint + a, nint));
   init_scratch = Ti.top;
   Step& gb = step(P.init_steps, STEP_GEMM, "integral banks");
   {  // J[(ij)][(ab)] = LI (nint^2 x N) * LV^T
@@ -1421,6 +1424,7 @@ void Builder::init_steps() {
       gp.seg_end = (i64)gb.gs.size();
       gb.gp.push_back(gp);
     }
+  if (!with_allext) return;
   {  // X = Lpk Lpk^T
     GemmProblem gp{BUF_X, 0, npk, npk, npk, 0.0, (i64)gb.gs.size(), 0};
     gb.gs.push_back(GemmSeg{BUF_T0, BUF_T0, Lpk_off, N, Lpk_off, N, N, 0, 1, 1.0});
@@ -1438,7 +1442,8 @@ void Builder::run() {
   nab = n * (n - 1) / 2;
   N = op.nchol;
   for (const auto& dm : sp.domains)
-    if ((i64)dm.size() != n) throw Error(3, "local pair domains are not supported by the dense-operator plan");
+    if ((i64)dm.size() != n)
+      throw Error(3, "the dense-operator plan is built on the non-local space (domains are mapped onto it)");
   if (nint + 3 > 64) throw Error(3, "at most 61 internal orbitals are supported");
   P.nint = nint;
   P.n = n;
@@ -1477,7 +1482,7 @@ void Builder::run() {
   tick("heads, init");
   zero_step(P.sigma_steps, BUF_R, 0, P.nD * n2, "zero accumulators");
   step(P.sigma_steps, STEP_UNPACK, "unpack");
-  allext();
+  if (with_allext) allext();
   tick("all-external");
   dd_x();
   tick("dd");
@@ -1514,9 +1519,10 @@ void Builder::run() {
 
 }  // namespace
 
-void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan) {
+void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext) {
   plan = Plan();
   Builder b(sp, op, plan);
+  b.with_allext = with_allext;
   b.run();
 }
 

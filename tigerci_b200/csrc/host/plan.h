@@ -168,6 +168,9 @@ struct Operator {
   double core_energy = 0.0;
 };
 
-void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan);
+// with_allext = false leaves the all-external term out (no X / W buffers, no WBUILD, no all-external steps;
+// the diagonal entries of types 2 and 3 then need the all-external diagonal from elsewhere): the form used
+// under local pair domains, whose all-external term runs in the pair-domain Cholesky form.
+void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext = true);
 
 }  // namespace tci

@@ -364,8 +364,8 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
 // are in flight to cover its latency); A's slices come the same way from L2.  Warp w computes rows
 // (w / 2) * MT/4 ... of the columns (w % 2) * 64 + 2 lane, +1: per pair of k a thread reads two 16-byte
 // B pairs and MT/4 16-byte A pairs (the same address across the warp) for MT FMAs.  Operands must start
-// on 16 bytes with even leading dimensions and every segment's alpha must be 1 (checked when the step is
-// lowered).  Sums: segments in table order, k ascending.
+// on 16 bytes with even leading dimensions (checked when the step is lowered).  A segment's alpha scales
+// its B values as they are read.  Sums: segments in table order, k ascending.
 constexpr int PANEL_T = 256;
 constexpr int PANEL_COLS = 128;
 constexpr int PANEL_KS = 16;
@@ -406,6 +406,7 @@ __global__ void __launch_bounds__(PANEL_T, 2) gemm_panel_f64(const DGemmProblem*
     const DGemmSeg S = segs[sgi];
     const long long K = S.K;
     const long long nsl = (K + PANEL_KS - 1) / PANEL_KS;
+    const bool scaled = S.alpha != 1.0;
     // one k slice of B (PANEL_KS x 128) and A (MT x PANEL_KS) into stage st, zero past the edges
     auto issue = [&](long long sl, int st) {
       const long long k0 = sl * PANEL_KS;
@@ -442,8 +443,11 @@ __global__ void __launch_bounds__(PANEL_T, 2) gemm_panel_f64(const DGemmProblem*
       const double* a = As + (size_t)st * MT * PANEL_KS + r0 * PANEL_KS;
 #pragma unroll
       for (int kp = 0; kp < PANEL_KS / 2; ++kp) {
-        const double2 w0 = *reinterpret_cast<const double2*>(w + (2 * kp) * PANEL_COLS);
-        const double2 w1 = *reinterpret_cast<const double2*>(w + (2 * kp + 1) * PANEL_COLS);
+        double2 w0 = *reinterpret_cast<const double2*>(w + (2 * kp) * PANEL_COLS);
+        double2 w1 = *reinterpret_cast<const double2*>(w + (2 * kp + 1) * PANEL_COLS);
+        if (scaled) {  // the segment's alpha on B, as gemm_tiled_f64 applies it
+          w0.x *= S.alpha, w0.y *= S.alpha, w1.x *= S.alpha, w1.y *= S.alpha;
+        }
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const double2 x = *reinterpret_cast<const double2*>(a + r * PANEL_KS + 2 * kp);
@@ -767,8 +771,12 @@ struct DDiag {
   long long foff, singlet;
 };
 
+// All-external part of the diagonal from W (its diagonal elements), or, when the plan has no W (local pair
+// domains), from XD = [(aa|cc); (ac|ca)] (two n x n arrays): W+((ac),(ac)) = (aa|cc) + (ac|ca),
+// W-((ac),(ac)) = (aa|cc) - (ac|ca), W+((aa),(aa)) = (aa|aa).
 __global__ void build_diag_kernel(const DDiag* __restrict__ ent, long long nent, long long n, long long np, long long nm,
-                                  const double* __restrict__ F, const double* __restrict__ W, double* __restrict__ hd) {
+                                  const double* __restrict__ F, const double* __restrict__ W,
+                                  const double* __restrict__ XD, double* __restrict__ hd) {
   const long long e = blockIdx.x;
   if (e >= nent) return;
   const DDiag D = ent[e];
@@ -778,17 +786,31 @@ __global__ void build_diag_kernel(const DDiag* __restrict__ ent, long long nent,
       if (D.foff >= 0) v += F[D.foff + t * (n + 1)];
     } else if (D.type == 2) {
       if (D.foff >= 0) v += 2.0 * F[D.foff + t * (n + 1)];
-      v += W[t * np + t];
+      v += W ? W[t * np + t] : XD[t * n + t];
     } else if (D.type == 3) {
       long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)t)) * 0.5);
       while (i * (i - 1) / 2 > t) --i;
       while ((i + 1) * i / 2 <= t) ++i;
       const long long j = t - i * (i - 1) / 2;
       if (D.foff >= 0) v += F[D.foff + i * (n + 1)] + F[D.foff + j * (n + 1)];
-      v += D.singlet ? W[(n + t) * np + (n + t)] : W[np * np + t * nm + t];
+      if (W) v += D.singlet ? W[(n + t) * np + (n + t)] : W[np * np + t * nm + t];
+      else v += XD[i * n + j] + (D.singlet ? 1.0 : -1.0) * XD[n * n + i * n + j];
     }
     hd[D.off + t] = v;
   }
+}
+
+// Local pair domains: the CI vector in the local layout (n_loc CSFs) and the plan's vectors in the non-local
+// layout; map[i] is the non-local index of local CSF i (an injection: every block padded to all externals).
+__global__ void scatter_local(const double* __restrict__ c_loc, const long long* __restrict__ map, long long n_loc,
+                              double* __restrict__ c_nl) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_loc; i += (long long)gridDim.x * blockDim.x)
+    c_nl[map[i]] = c_loc[i];
+}
+__global__ void gather_local(const double* __restrict__ s_nl, const long long* __restrict__ map, long long n_loc,
+                             double* __restrict__ s_loc) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_loc; i += (long long)gridDim.x * blockDim.x)
+    s_loc[i] = s_nl[map[i]];
 }
 
 // Davidson vector kernels (FP64, deterministic two-pass reductions)
@@ -970,10 +992,10 @@ struct DevStep {
   long long tma_rows = 0;  // kinds 4, 6, 7: rows of the gathered coefficients / of the exchange bank
   long long tma_aux2 = 0;  // kind 7: offset of the exchange bank in BUF_JK
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
-  // FP64 all-external problems on the row-panel kernel, by row class (M <= 16, 24, 32, 40, 48)
-  DGemmProblem* panel_probs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  int panel_nprob[5] = {0, 0, 0, 0, 0};
-  long long panel_ntiles[5] = {0, 0, 0, 0, 0};
+  // FP64 problems of few rows on the row-panel kernel, by row class (M <= 16, 24, ..., 64)
+  DGemmProblem* panel_probs[7] = {};
+  int panel_nprob[7] = {};
+  long long panel_ntiles[7] = {};
   DGemmProblem* skinny_probs = nullptr;
   int skinny_nprob = 0;
   long long skinny_nwarps = 0;
@@ -1056,6 +1078,18 @@ struct tci_ctx {
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
   cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
+  // Local pair domains (a deck with allowed-virtual lists): the CI vectors of the calls have the local layout
+  // (n_loc CSFs); the plan runs on the non-local space of the same deck with every block padded to all
+  // externals (zeros outside the domains): sigma = P^T H P c with P the padding, exact for every term, since
+  // H restricted to the local space is P^T H P.  The all-external term runs on the local layout directly,
+  // in the pair-domain Cholesky form (tci_local); the plan leaves it out.
+  bool local = false;
+  i64 n_loc = 0;
+  long long* d_map = nullptr;    // local CSF -> non-local CSF (device)
+  tci_local* loc_allext = nullptr;
+  double* xdiag = nullptr;       // (aa|cc) and (ac|ca), n x n each: the all-external diagonal without W
+  double *loc_c = nullptr, *loc_s = nullptr;  // local-layout scratch vectors of the sigma entry points
+  i64 nvec() const { return local ? n_loc : plan.total_csfs; }
   // generalized solve (tci_davidson_gen): sigma and the diagonal of G^-1/2 (H - gen_shift) G^-1/2
   const double* gen_s = nullptr;  // G^-1/2 (device) while such a solve runs, else nullptr
   double gen_shift = 0.0;
@@ -1077,6 +1111,7 @@ struct tci_ctx {
                                  // preconditioner + Gram-Schmidt, restart, finish
 
   ~tci_ctx() {
+    if (loc_allext) tci_local_destroy(loc_allext);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (graph_exec_prof) cudaGraphExecDestroy(graph_exec_prof);
@@ -1351,21 +1386,23 @@ struct tci_ctx {
       d.segs = upload(sg, owned, stream);
       {
         // FP64 form: skinny problems (one-row products) to the warp-per-column kernel, the rest tiled
-        std::vector<DGemmProblem> reg, sk, pan[5];
-        long long rt = 0, wk = 0, pt[5] = {0, 0, 0, 0, 0};
+        std::vector<DGemmProblem> reg, sk, pan[7];
+        long long rt = 0, wk = 0, pt[7] = {0, 0, 0, 0, 0, 0, 0};
         for (const auto& g : pr) {
           bool skinny = g.M <= SKINNY_M && s.name != "all-external";
           for (long long q = g.seg_begin; skinny && q < g.seg_end; ++q) skinny = sg[(size_t)q].tA == 0 && sg[(size_t)q].tB == 1;
-          // the all-external product (a few dozen CI rows x the operator) on the row-panel kernel
-          bool panel = s.name == "all-external" && g.M <= 48;
+          // few rows against long rows of B (the all-external product: a few dozen CI rows x the operator;
+          // the reverse three-external product: the pair-matrix rows x the (iq|bs) banks) on the row-panel
+          // kernel when the operands allow 16-byte copies
+          bool panel = g.M <= 64 && g.N >= 1024 && !skinny;
           for (long long q = g.seg_begin; panel && q < g.seg_end; ++q) {
             const DGemmSeg& x = sg[(size_t)q];
-            panel = x.tA == 0 && x.tB == 0 && x.alpha == 1.0 && ((x.lda | x.ldb) & 1) == 0 &&
+            panel = x.tA == 0 && x.tB == 0 && ((x.lda | x.ldb) & 1) == 0 &&
                     ((reinterpret_cast<uintptr_t>(x.A) | reinterpret_cast<uintptr_t>(x.B)) & 15) == 0;
           }
           if (panel) {
-            const int c = (int)((g.M + 7) / 8) - 1;  // MT = 8 (c + 1), classes 16 ... 48
-            const int cls = std::max(1, c) - 1;       // 0: MT 16, 1: 24, 2: 32, 3: 40, 4: 48
+            const int c = (int)((g.M + 7) / 8) - 1;  // MT = 8 (c + 1), classes 16 ... 64
+            const int cls = std::max(1, c) - 1;       // 0: MT 16, 1: 24, ..., 6: 64
             DGemmProblem x = g;
             x.tile_begin = pt[cls];
             pt[cls] += (g.N + PANEL_COLS - 1) / PANEL_COLS;
@@ -1388,7 +1425,7 @@ struct tci_ctx {
         d.skinny_probs = upload(sk, owned, stream);
         d.skinny_nprob = (int)sk.size();
         d.skinny_nwarps = wk;
-        for (int c = 0; c < 5; ++c) {
+        for (int c = 0; c < 7; ++c) {
           d.panel_probs[c] = upload(pan[c], owned, stream);
           d.panel_nprob[c] = (int)pan[c].size();
           d.panel_ntiles[c] = pt[c];
@@ -1503,17 +1540,30 @@ struct tci_ctx {
   void ensure_diag() {
     if (hd) return;
     const i64 n = plan.total_csfs;
-    TCI_CUDA(dev_malloc(&hd, n * sizeof(double), stream));
-    owned.push_back(hd);
-    TCI_CUDA(cudaMemsetAsync(hd, 0, n * sizeof(double), stream));
+    double* full = nullptr;  // the non-local diagonal (local pair domains: gathered into hd afterwards)
+    TCI_CUDA(dev_malloc(&full, n * sizeof(double), stream));
+    TCI_CUDA(cudaMemsetAsync(full, 0, n * sizeof(double), stream));
     std::vector<DDiag> e;
     for (auto& d : plan.diag) e.push_back(DDiag{d.off, d.len, d.type, d.beta, d.foff, d.singlet});
     for (auto& d : plan.diag) check_range(BUF_S, d.off, d.len);
     DDiag* de = upload(e, owned, stream);
+    if (!buf[BUF_W] && !xdiag && std::any_of(e.begin(), e.end(), [](const DDiag& x) { return x.type >= 2; }))
+      throw Error(TCI_ERR_INTERNAL, "no all-external diagonal for the N-2 blocks");
     if (!e.empty())
       build_diag_kernel<<<(unsigned)e.size(), 256, 0, stream>>>(de, (long long)e.size(), plan.n, plan.np, plan.nm,
-                                                                buf[BUF_F], buf[BUF_W], hd);
+                                                                buf[BUF_F], buf[BUF_W], xdiag, full);
     TCI_CUDA(cudaGetLastError());
+    if (local) {
+      TCI_CUDA(dev_malloc(&hd, n_loc * sizeof(double), stream));
+      gather_local<<<148 * 8, 256, 0, stream>>>(full, d_map, n_loc, hd);
+      TCI_CUDA(cudaGetLastError());
+      TCI_CUDA(cudaStreamSynchronize(stream));
+      std::lock_guard<std::mutex> lk(g_capture_free_mu);
+      TCI_CUDA(dev_free(full, stream));
+    } else {
+      hd = full;
+    }
+    owned.push_back(hd);
     TCI_CUDA(cudaStreamSynchronize(stream));
   }
 
@@ -1556,12 +1606,39 @@ struct tci_ctx {
 
   void sigma_of(const double* d_c, double* d_s) {
     const i64 n = plan.total_csfs;
+    if (local) {
+      local_in(d_c);
+      run_sigma_steps();
+      local_out(d_c, d_s);
+      sigma_count++;
+      return;
+    }
     TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     run_sigma_steps();
     gen_out(d_s);
     sigma_count++;
+  }
+  // local layout: the padded input of the plan (zeros outside the domains) and an empty output
+  void local_in(const double* d_c) {
+    if (gen_s) throw Error(TCI_ERR_INPUT, "the generalized (ACPF-type) solve is not available under pair domains");
+    const i64 n = plan.total_csfs;
+    TCI_CUDA(cudaMemsetAsync(buf[BUF_C], 0, n * sizeof(double), stream));
+    scatter_local<<<148 * 8, 256, 0, stream>>>(d_c, d_map, n_loc, buf[BUF_C]);
+    TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
+    launch_count += 1;
+    TCI_CUDA(cudaGetLastError());
+  }
+  // local layout: d_s = P^T (plan's sigma) + the all-external term of the local blocks
+  void local_out(const double* d_c, double* d_s) {
+    gather_local<<<148 * 8, 256, 0, stream>>>(buf[BUF_S], d_map, n_loc, d_s);
+    launch_count += 1;
+    TCI_CUDA(cudaGetLastError());
+    if (loc_allext) {
+      const int rc = tci_local_apply(loc_allext, d_c, d_s, n_loc, stream);
+      if (rc != TCI_OK) throw Error(rc, "pair-domain all-external term failed");
+    }
   }
   // d_s = BUF_S, or in a generalized solve G^-1/2 (BUF_S - shift BUF_C)
   void gen_out(double* d_s) {
@@ -1618,7 +1695,7 @@ struct tci_ctx {
       }
       if (s.kind == STEP_GEMM && s.skinny_nwarps > 0) k += 1;
       if (s.kind == STEP_GEMM)
-        for (int c = 0; c < 5; ++c) k += s.panel_ntiles[c] > 0 ? 1 : 0;
+        for (int c = 0; c < 7; ++c) k += s.panel_ntiles[c] > 0 ? 1 : 0;
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
           ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && plan.nD > 0))
         k += 1;
@@ -1746,11 +1823,14 @@ struct tci_ctx {
       owned.push_back(*p);
       bytes_held += (double)n * sizeof(float);
     };
-    alloc_f(&w32p, (size_t)tci_tc_host::w32_floats(np));
-    if (nm > 0) alloc_f(&w32m, (size_t)tci_tc_host::w32_floats(nm));
-    alloc_f(&u2s, (size_t)tci_tc_host::u2_floats(std::max<i64>(1, plan.n_sing), np));
-    if (has_trip()) {
-      alloc_f(&u2t, (size_t)tci_tc_host::u2_floats(plan.n_trip, nm));
+    const bool allext = np > 0;  // the plan carries the all-external term (not under pair domains)
+    if (allext) {
+      alloc_f(&w32p, (size_t)tci_tc_host::w32_floats(np));
+      if (nm > 0) alloc_f(&w32m, (size_t)tci_tc_host::w32_floats(nm));
+      alloc_f(&u2s, (size_t)tci_tc_host::u2_floats(std::max<i64>(1, plan.n_sing), np));
+      if (has_trip()) {
+        alloc_f(&u2t, (size_t)tci_tc_host::u2_floats(plan.n_trip, nm));
+      }
     }
     TCI_CUDA(dev_malloc(&tc_status, sizeof(int), stream));
     owned.push_back(tc_status);
@@ -1869,15 +1949,17 @@ struct tci_ctx {
       tma_t3r_ready = true;
     }
     TCI_CUDA(cudaMemsetAsync(tc_status, 0, sizeof(int), stream));
-    TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
-    if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
+    if (allext) {
+      TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W], np, w32p, stream));
+      if (nm > 0) TCI_CUDA(tci_tc_host::convert_w(buf[BUF_W] + np * np, nm, w32m, stream));
+    }
     TCI_CUDA(cudaStreamSynchronize(stream));
     if (plan.n_sing > 0 && !tci_tc_host::prepare(tc_sing, w32p, np, u2s, plan.n_sing, buf[BUF_T0] + plan.allext_ys, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
     if (plan.n_trip > 0 && nm > 0 &&
         !tci_tc_host::prepare(tc_trip, w32m, nm, u2t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
-    if (refine != 1) {  // the FP64 W is only needed for the plain-FP64 finish of the roots
+    if (refine != 1 && buf[BUF_W]) {  // the FP64 W is only needed for the plain-FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
       TCI_CUDA(dev_free(buf[BUF_W], stream));
       bytes_held -= (double)plan.buf_size[BUF_W] * sizeof(double);
@@ -1890,10 +1972,15 @@ struct tci_ctx {
   void sigma_of_fp64(const double* d_c, double* d_s) {
     const i64 n = plan.total_csfs;
     const bool tc_allext = (refine == 2 || refine == 3) && precision == 1;
-    if (!buf[BUF_W] && !tc_allext) throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
-    TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
-    TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
+    if (!buf[BUF_W] && !tc_allext && !local)
+      throw Error(TCI_ERR_INTERNAL, "the FP64 operators of this context were released");
+    if (local) {
+      local_in(d_c);
+    } else {
+      TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+      if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
+      TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
+    }
     const int64_t saved = precision;
     precision = 0;
     allext_tc_in_fp64 = tc_allext;
@@ -1907,7 +1994,8 @@ struct tci_ctx {
     launch_count += sigma_launches();
     precision = saved;
     allext_tc_in_fp64 = false;
-    gen_out(d_s);
+    if (local) local_out(d_c, d_s);
+    else gen_out(d_s);
   }
 
   // Status word of the bounded waits inside the tensor-core kernel.
@@ -1998,6 +2086,8 @@ struct tci_ctx {
         launch_panel<32>(s, 2);
         launch_panel<40>(s, 3);
         launch_panel<48>(s, 4);
+        launch_panel<56>(s, 5);
+        launch_panel<64>(s, 6);
         if (s.ntiles > 0) {
           if (s.cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
           else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
@@ -2079,6 +2169,22 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
     auto t0 = std::chrono::steady_clock::now();
     CsfSpace sp;
     Plan plan;
+    if (deck && (deck->nm1_domain_ptr || deck->nm2_domain_ptr)) {
+      // local pair domains: the plan on the non-local space of the same deck, the local layout mapped onto it
+      tci::LocalSetup ls;
+      build_space_from_c(deck, ls.loc);
+      tci_deck nl = *deck;
+      nl.nm1_domain_ptr = nl.nm1_domain_idx = nl.nm2_domain_ptr = nl.nm2_domain_idx = nullptr;
+      build_space_from_c(&nl, sp);
+      Operator o;
+      operator_from_c(op, sp, o);
+      tci::build_local_setup(ls.loc, sp, o, ls);
+      build_plan(sp, o, plan, false);
+      const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out, refine,
+                                        &ls);
+      if (rc == TCI_OK) (*out)->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      return rc;
+    }
     build_space_from_c(deck, sp);
     Operator o;
     operator_from_c(op, sp, o);
@@ -2147,8 +2253,74 @@ void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode) {
   if (ctx) ctx->tc_mode = mode;
 }
 
+void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls) {
+  const i64 n = nl.n_ext, nab = n * (n - 1) / 2, nint = nl.n_int, N = op.nchol;
+  if (loc.n_ext != n || loc.n_int != nint) throw Error(TCI_ERR_INTERNAL, "local and non-local spaces differ in shape");
+  ls.map.assign((size_t)loc.total_csfs, -1);
+  for (int k = 0; k < 3; ++k) {
+    if (loc.paths[k].size() != nl.paths[k].size()) throw Error(TCI_ERR_INTERNAL, "local and non-local heads differ");
+    for (size_t p = 0; p < loc.paths[k].size(); ++p) {
+      const Head &h = loc.paths[k][p], &g = nl.paths[k][p];
+      if (h.occ != g.occ) throw Error(TCI_ERR_INTERNAL, "local and non-local heads differ");
+      if (k == 0) {
+        if (h.off >= 0)
+          for (i64 f = 0; f < h.nsf; ++f) ls.map[(size_t)(h.off + f)] = g.off + f;
+        continue;
+      }
+      if (h.domain < 0) continue;
+      const std::vector<int>& D = loc.domains[(size_t)h.domain];
+      const i64 m = (i64)D.size(), mab = m * (m - 1) / 2;
+      if (k == 1) {
+        if (h.off < 0 || m == 0) continue;
+        if (g.off < 0 || g.nsf != h.nsf) throw Error(TCI_ERR_INTERNAL, "N-1 block missing in the non-local space");
+        for (i64 f = 0; f < h.nsf; ++f)
+          for (i64 a = 0; a < m; ++a) ls.map[(size_t)(h.off + f * m + a)] = g.off + f * n + D[(size_t)a];
+        continue;
+      }
+      if (h.off >= 0 && mab > 0) {
+        if (g.off < 0 || g.nsf != h.nsf) throw Error(TCI_ERR_INTERNAL, "N-2 block missing in the non-local space");
+        for (i64 f = 0; f < h.nsf; ++f)
+          for (i64 i = 1; i < m; ++i)
+            for (i64 j = 0; j < i; ++j) {
+              const i64 I = D[(size_t)i], J = D[(size_t)j];  // sorted: I > J
+              ls.map[(size_t)(h.off + f * mab + i * (i - 1) / 2 + j)] = g.off + f * nab + I * (I - 1) / 2 + J;
+            }
+      }
+      if (h.off_aa >= 0 && m > 0) {
+        if (g.off_aa < 0 || g.nsf_aa != h.nsf_aa) throw Error(TCI_ERR_INTERNAL, "N-2 aa block missing");
+        for (i64 f = 0; f < h.nsf_aa; ++f)
+          for (i64 a = 0; a < m; ++a) ls.map[(size_t)(h.off_aa + f * m + a)] = g.off_aa + f * n + D[(size_t)a];
+      }
+      // the pair-domain all-external term of this head (tci_local heads: off_ab, off_aa, nsf_ab, nsf_aa,
+      // nsing, dom_off, dom_len)
+      const i64 nsf_ab = (h.off >= 0 && mab > 0) ? h.nsf : 0, nsf_aa = (h.off_aa >= 0 && m > 0) ? h.nsf_aa : 0;
+      if (nsf_ab == 0 && nsf_aa == 0) continue;
+      ls.heads7.insert(ls.heads7.end(), {nsf_ab ? h.off : 0, nsf_aa ? h.off_aa : 0, nsf_ab, nsf_aa,
+                                         nsf_aa > 0 ? (i64)loc.fsn[(size_t)h.singles] : 0, (i64)ls.dom_idx.size(), m});
+      for (int a : D) ls.dom_idx.push_back(a);
+    }
+  }
+  for (i64 x : ls.map)
+    if (x < 0) throw Error(TCI_ERR_INTERNAL, "a local CSF has no non-local counterpart");
+  // (aa|cc) and (ac|ca) over the externals, for the all-external part of the diagonal
+  ls.xdiag.assign((size_t)(2 * n * n), 0.0);
+  auto row = [&](i64 p, i64 q) {
+    const i64 P = nint + std::max(p, q), Q = nint + std::min(p, q);
+    return op.chol + (P * (P + 1) / 2 + Q) * N;
+  };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (i64 a = 0; a < n; ++a)
+    for (i64 c = 0; c < n; ++c) {
+      const double *la = row(a, a), *lc = row(c, c), *lx = row(a, c);
+      double s1 = 0.0, s2 = 0.0;
+      for (i64 J = 0; J < N; ++J) s1 += la[J] * lc[J], s2 += lx[J] * lx[J];
+      ls.xdiag[(size_t)(a * n + c)] = s1;
+      ls.xdiag[(size_t)(n * n + a * n + c)] = s2;
+    }
+}
+
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
-                  tci_ctx** out, int64_t refine) {
+                  tci_ctx** out, int64_t refine, LocalSetup* ls) {
   if (!out || !chol) return TCI_ERR_ARG;
   *out = nullptr;
   if (precision < 0 || precision > 1) {
@@ -2208,6 +2380,23 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     }
     ctx->dheads = upload(dh, ctx->owned, ctx->stream);
     ctx->dk_head = upload(dkh, ctx->owned, ctx->stream);
+    if (ls) {
+      ctx->local = true;
+      ctx->n_loc = ls->loc.total_csfs;
+      ctx->d_map = upload(ls->map, ctx->owned, ctx->stream);
+      ctx->xdiag = upload(ls->xdiag, ctx->owned, ctx->stream);
+      for (double** p : {&ctx->loc_c, &ctx->loc_s}) {
+        TCI_CUDA(dev_malloc(p, (size_t)std::max<i64>(1, ctx->n_loc) * sizeof(double), ctx->stream));
+        ctx->owned.push_back(*p);
+      }
+      if (!ls->heads7.empty()) {
+        const int64_t opts[4] = {precision, (int64_t)16e9, kblock, 1};
+        const int rc = tci_local_create(P.nint, P.n, chol, P.nchol, (int64_t)(ls->heads7.size() / 7), ls->heads7.data(),
+                                        ls->dom_idx.data(), ctx->n_loc, device, opts, 4, &ctx->loc_allext);
+        if (rc != TCI_OK) throw Error(rc, "pair-domain all-external set-up failed");
+      }
+      TCI_CUDA(cudaSetDevice(ctx->device));
+    }
     phase("buffers and uploads", ctx->stream);
     // Mixed form without the plain-FP64 finish: the exchange product X = Lpk Lpk^T of the all-external
     // operators (the largest set-up GEMM, 2 npk^2 N flops) runs on the TMA-fed tensor-core kernel; its
@@ -2284,20 +2473,30 @@ extern "C" {
 int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n, void* stream) {
   if (!ctx || !d_c || !d_sigma) return TCI_ERR_ARG;
   try {
-    if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
+    if (n != ctx->nvec()) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
     TCI_CUDA(cudaSetDevice(ctx->device));
     // NULL means the legacy default stream (what an unqualified caller and torch's default stream use)
     cudaStream_t user = stream ? (cudaStream_t)stream : cudaStreamLegacy;
     TCI_CUDA(cudaEventRecord(ctx->ev0, user));
     TCI_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev0, 0));
-    // the plan addresses BUF_C / BUF_S: copy in and accumulate out
-    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
-    TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    ctx->run_sigma_steps();
-    TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    const double* s_out = ctx->buf[BUF_S];
+    if (ctx->local) {  // padded into the plan's layout, the result back in the local layout
+      ctx->local_in(d_c);
+      TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      ctx->run_sigma_steps();
+      ctx->local_out(d_c, ctx->loc_s);
+      TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+      s_out = ctx->loc_s;
+    } else {
+      // the plan addresses BUF_C / BUF_S: copy in and accumulate out
+      TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
+      TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      ctx->run_sigma_steps();
+      TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    }
     // sigma += S (the caller's sigma accumulates, like htimesc)
-    accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(d_sigma, ctx->buf[BUF_S], n);
+    accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(d_sigma, s_out, n);
     ctx->launch_count++;
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -2312,15 +2511,26 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
 int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n) {
   if (!ctx || !c || !sigma) return TCI_ERR_ARG;
   try {
-    if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
+    if (n != ctx->nvec()) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
     TCI_CUDA(cudaSetDevice(ctx->device));
-    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], c, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
-    TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    ctx->run_sigma_steps();
-    TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    const double* s_out = ctx->buf[BUF_S];
+    if (ctx->local) {
+      TCI_CUDA(cudaMemcpyAsync(ctx->loc_c, c, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      ctx->local_in(ctx->loc_c);
+      TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      ctx->run_sigma_steps();
+      ctx->local_out(ctx->loc_c, ctx->loc_s);
+      TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+      s_out = ctx->loc_s;
+    } else {
+      TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_C], c, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      TCI_CUDA(cudaMemsetAsync(ctx->buf[BUF_S], 0, n * sizeof(double), ctx->stream));
+      TCI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+      ctx->run_sigma_steps();
+      TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    }
     std::vector<double> tmp(n);
-    TCI_CUDA(cudaMemcpyAsync(tmp.data(), ctx->buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    TCI_CUDA(cudaMemcpyAsync(tmp.data(), s_out, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     float ms = 0;
     TCI_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -2337,7 +2547,7 @@ int tci_sigma(tci_ctx* ctx, const double* c, double* sigma, int64_t n) {
 int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n) {
   if (!ctx || !hdiag) return TCI_ERR_ARG;
   try {
-    if (n != ctx->plan.total_csfs) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
+    if (n != ctx->nvec()) throw Error(TCI_ERR_ARG, "vector length differs from total_csfs");
     TCI_CUDA(cudaSetDevice(ctx->device));
     ctx->ensure_diag();
     TCI_CUDA(cudaMemcpy(hdiag, ctx->hd, n * sizeof(double), cudaMemcpyDeviceToHost));
@@ -2442,7 +2652,7 @@ int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double t
   };
   try {
     TCI_CUDA(cudaSetDevice(ctx->device));
-    const i64 n = ctx->plan.total_csfs;
+    const i64 n = ctx->nvec();
     std::vector<double> sh((size_t)n);
     for (i64 i = 0; i < n; ++i) {
       if (!(g[i] > 0.0) || !std::isfinite(g[i])) throw Error(TCI_ERR_ARG, "the metric must be positive and finite");
@@ -2522,7 +2732,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
   if (!ctx || !energies || nroots <= 0 || subspace_bytes < 0) return TCI_ERR_ARG;
   try {
     TCI_CUDA(cudaSetDevice(ctx->device));
-    const i64 n = ctx->plan.total_csfs;
+    const i64 n = ctx->nvec();
     if (nroots > n) throw Error(TCI_ERR_ARG, "more roots than CSFs");
     if (maxit <= 0) maxit = 50 * nroots;
     const double budget = subspace_bytes > 0 ? (double)subspace_bytes : kDefaultSubspaceBytes;
@@ -2816,7 +3026,7 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   if (!ctx || !out || len < 8) return TCI_ERR_ARG;
   if (len >= 9) out[8] = 1.0 + (double)ctx->sigma_launches();  // + the accumulation into the caller's sigma
   if (len >= 10) out[9] = (double)ctx->launch_count;
-  out[0] = (double)ctx->plan.total_csfs;
+  out[0] = (double)ctx->nvec();
   out[1] = ctx->bytes_held;
   out[2] = ctx->init_seconds;
   out[3] = ctx->last_sigma_ms;

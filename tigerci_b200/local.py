@@ -104,3 +104,26 @@ def pair_domain_problem(n_pairs=600, n_int=35, n_virt=400, dmin=20, dmax=180, se
         dom.extend(d.tolist())
         doff += n
     return np.array(heads, dtype=np.int64), np.array(dom, dtype=np.int64), off
+
+
+def pair_domain_deck(n_int=35, n_virt=400, dmin=20, dmax=180, seed=99):
+    """Deck of the local MRSDCI with pair domains: n_int doubly occupied internal orbitals (one closed-shell
+    reference), n_virt externals, every N-2 path (the n_int (n_int + 1) / 2 internal pairs, lexical order)
+    and every N-1 path with a seeded random domain: size uniform in [dmin, dmax], a sorted random subset of
+    the externals."""
+    from .api import CsfSpace, Deck
+
+    base = Deck(n_int + n_virt, n_int, 0, 2 * n_int, 1, ["2" * n_int])
+    cnt = CsfSpace(base).counts()
+    rng = np.random.default_rng(seed)
+
+    def doms(k):
+        out = []
+        for _ in range(k):
+            m = int(rng.integers(dmin, dmax + 1))
+            out.append(np.sort(rng.choice(n_virt, size=m, replace=False)).tolist())
+        return out
+
+    nm2 = doms(cnt["paths_nm2"])
+    nm1 = doms(cnt["paths_nm1"])
+    return Deck(n_int + n_virt, n_int, 0, 2 * n_int, 1, ["2" * n_int], nm1_domains=nm1, nm2_domains=nm2)

@@ -355,3 +355,18 @@ def water_c1(cd_threshold: float = 1e-6):
     orbitals (19 references), singlet."""
     sym, xyz = water()
     return mrsdci_problem(sym, xyz, "cc-pVDZ", pure_d=True, n_frozen=1, cas=(4, 4), cd_threshold=cd_threshold)
+
+
+# Reference selection of the octane problem: the CAS(8,8) over the four highest doubly occupied and four lowest
+# virtual RHF orbitals has 1107 singlet occupations, whose MRSDCI space no device holds; the references are the
+# RHF occupation and the HOMO^2 -> LUMO^2 pair excitation within that active space (17,840,355 CSFs).
+OCTANE_REFS = ("22220000", "22202000")
+
+
+def octane_c3(cd_threshold: float = 1e-6):
+    """All-trans n-octane (C-C 1.53 A, C-H 1.09 A, tetrahedral, staggered), cc-pVDZ (202 functions), the 8 C 1s
+    frozen, CAS(8,8) active orbitals on canonical RHF orbitals with the references OCTANE_REFS, singlet."""
+    sym, xyz = n_alkane(8)
+    n_inactive = 33 - 4
+    return mrsdci_problem(sym, xyz, "cc-pVDZ", pure_d=True, n_frozen=8, cas=(8, 8), cd_threshold=cd_threshold,
+                          refs=["2" * n_inactive + r for r in OCTANE_REFS])
