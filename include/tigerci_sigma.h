@@ -173,8 +173,12 @@ int64_t tci_davidson_capacity(int64_t n, int64_t nroots, int64_t maxit, int64_t 
  * (H - e_shift) c = lambda G c with G = diag(g) (host array of total_csfs
  * positive values, e.g. from tci_acpf_gdiag) and e_shift the reference energy.
  * Solved as the standard problem of G^-1/2 (H - e_shift) G^-1/2 (y = G^1/2 c)
- * by the device Davidson of tci_davidson_ex (same tolerances, budget, mixed
- * form and finish).  energies get lambda + e_shift; vectors (may be NULL) the
+ * by the device Davidson of tci_davidson_ex (same budget, mixed form and
+ * finish); the residual norm tested against tol_residual is the reference's,
+ * |(H - e_shift) c - lambda G c| with c of unit G-norm (build_residual_gen_eig,
+ * tiger_fortran/davidson.f90:535-553), and roots are followed by their
+ * overlap with their initial guess (root_following, davidson.f90:732, on by
+ * default in the reference: NO ACPF ROOT FOLLOW unset).  energies get lambda + e_shift; vectors (may be NULL) the
  * unit-norm c of each root.  For the length of the call the context's
  * diagonal and sigma build stand for the transformed operator, so no other
  * call may use the same context (from another thread) until it returns. */
@@ -206,10 +210,12 @@ int tci_dots(tci_ctx* ctx, const double* d_A, int64_t lda, int64_t m, const doub
 #define TCI_DOTS_NOALLOC_MAX_ROWS 64
 int tci_dots_noalloc(const double* d_A, int64_t lda, int64_t m, const double* d_x, int64_t n, double* d_out,
                      void* stream);
-/* out[0..9]: total_csfs, device bytes held, init seconds, last sigma ms,
+/* out[0..10]: total_csfs, device bytes held, init seconds, last sigma ms,
  * flops per sigma, all-external flops, all-external bytes, sigma builds,
  * kernel launches per sigma build (out[8], when len >= 9), kernels launched
- * by this context so far (out[9], when len >= 10) */
+ * by this context so far (out[9], when len >= 10), 1 if the last Davidson
+ * solve met its residual or energy tolerance for every root before maxit,
+ * else 0 (out[10], when len >= 11) */
 int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len);
 /* Per-step CUDA-event timing of the sigma plan (off by default).  When on,
  * every sigma build records an event pair around each plan step on the

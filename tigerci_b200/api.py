@@ -295,8 +295,8 @@ class SigmaBuilder:
         return list(zip(names, ms.tolist())), nb.value
 
     def stats(self) -> dict:
-        out = np.zeros(10, dtype=np.float64)
-        check(lib().tci_ctx_stats(self._h, ptr(out), 10))
+        out = np.zeros(11, dtype=np.float64)
+        check(lib().tci_ctx_stats(self._h, ptr(out), 11))
         keys = ["total_csfs", "device_bytes", "init_seconds", "last_sigma_ms", "flops_per_sigma",
-                "flops_allext", "bytes_allext", "sigma_count", "launches_per_sigma", "launches"]
+                "flops_allext", "bytes_allext", "sigma_count", "launches_per_sigma", "launches", "converged"]
         return dict(zip(keys, out.tolist()))

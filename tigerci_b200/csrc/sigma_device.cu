@@ -1092,7 +1092,11 @@ struct tci_ctx {
   i64 nvec() const { return local ? n_loc : plan.total_csfs; }
   // generalized solve (tci_davidson_gen): sigma and the diagonal of G^-1/2 (H - gen_shift) G^-1/2
   const double* gen_s = nullptr;  // G^-1/2 (device) while such a solve runs, else nullptr
+  const double* gen_g = nullptr;  // G (device) in such a solve: the residual norm is taken in the metric of c
   double gen_shift = 0.0;
+  bool gen_follow = false;        // root following in such a solve (root_following, davidson.f90:732)
+  bool acpf_root_follow = true;   // the reference's default (its keyword NO ACPF ROOT FOLLOW clears it)
+  bool last_converged = false;    // the last Davidson solve met its tolerances for every root
   std::vector<i64> lowest_diag;  // CSF indices of the lowest diagonal elements, ascending (initial guesses)
   double* dots = nullptr;        // reduction scratch: partial sums and results
   double* coefs = nullptr;       // small device coefficient arrays
@@ -2561,6 +2565,27 @@ int tci_diag(tci_ctx* ctx, double* hdiag, int64_t n) {
 
 namespace {
 
+// Root following (root_following, tiger_fortran/davidson.f90:732-812): state q keeps the subspace
+// eigenvector with the largest overlap with the q-th basis vector (its initial guess, or its Ritz vector
+// after a restart), measured in the metric the basis is orthonormal in; the first nroots eigenpairs are
+// replaced by the chosen ones, in state order (a vector chosen twice is used twice, as in the reference).
+void follow_roots(std::vector<double>& w, std::vector<double>& V, int m, int nroots) {
+  std::vector<double> w2(w);
+  std::vector<double> V2(V);
+  for (int q = 0; q < nroots && q < m; ++q) {
+    int best = 0;
+    double bo = -1.0;
+    for (int j = 0; j < m; ++j) {
+      const double o = std::fabs(V[(size_t)q * m + j]);
+      if (o > bo) bo = o, best = j;
+    }
+    w2[(size_t)q] = w[(size_t)best];
+    for (int k = 0; k < m; ++k) V2[(size_t)k * m + q] = V[(size_t)k * m + best];
+  }
+  w.swap(w2);
+  V.swap(V2);
+}
+
 // Cyclic Jacobi eigensolver for the small symmetric subspace matrix (the role of
 // dsyev in dsyev_wrapper, tiger_fortran/math_utils.f90:417-479).  A is m x m row
 // major; on exit w holds ascending eigenvalues and V (m x m, columns) the vectors.
@@ -2635,6 +2660,7 @@ int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double t
   if (ctx->gen_s) return TCI_ERR_ARG;  // one generalized solve at a time on a context
   double* ds = nullptr;
   double* dd = nullptr;
+  double* dg = nullptr;
   double* saved_hd = nullptr;
   std::vector<i64> saved_low;
   auto restore = [&]() {
@@ -2643,11 +2669,14 @@ int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double t
       ctx->lowest_diag = saved_low;
     }
     ctx->gen_s = nullptr;
+    ctx->gen_g = nullptr;
+    ctx->gen_follow = false;
     ctx->gen_shift = 0.0;
     cudaStreamSynchronize(ctx->stream);
     std::lock_guard<std::mutex> lk(g_capture_free_mu);
     dev_free(ds, ctx->stream);
     dev_free(dd, ctx->stream);
+    dev_free(dg, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
   };
   try {
@@ -2661,7 +2690,9 @@ int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double t
     ctx->ensure_diag();
     TCI_CUDA(dev_malloc(&ds, (size_t)n * sizeof(double), ctx->stream));
     TCI_CUDA(dev_malloc(&dd, (size_t)n * sizeof(double), ctx->stream));
+    TCI_CUDA(dev_malloc(&dg, (size_t)n * sizeof(double), ctx->stream));
     TCI_CUDA(cudaMemcpyAsync(ds, sh.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    TCI_CUDA(cudaMemcpyAsync(dg, g, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     gen_diag<<<148 * 8, 256, 0, ctx->stream>>>(dd, ctx->hd, ds, e_shift, n);
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -2670,6 +2701,8 @@ int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double t
     ctx->hd = dd;
     ctx->lowest_diag.clear();  // the initial guess follows the transformed diagonal
     ctx->gen_s = ds;
+    ctx->gen_g = dg;
+    ctx->gen_follow = ctx->acpf_root_follow;
     ctx->gen_shift = e_shift;
     const int rc = tci_davidson_ex(ctx, nroots, tol_residual, tol_energy, maxit, 0, nullptr, energies, vectors,
                                    iterations);
@@ -2783,6 +2816,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
       ctx->dav_keep = keep;
     }
     double *Cs = ctx->dav_c, *HCs = ctx->dav_hc, *r = ctx->dav_r, *tmpC = ctx->dav_tc, *tmpH = ctx->dav_th;
+    bool ran_out = false;  // a root stopped at maxit without meeting either tolerance
     try {
       cudaStream_t st = ctx->stream;
       const unsigned G = 148 * 8, TB = 256;
@@ -2838,6 +2872,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
         }
         mark(3);
         jacobi_eigh(h, num_vec, w, V);
+        if (ctx->gen_follow) follow_roots(w, V, num_vec, (int)nroots);
         for (int q = 0; q < nroots; ++q) {
           dE[q] = std::fabs(w[q] - energy[q]);
           energy[q] = w[q];
@@ -2907,6 +2942,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
             for (int j = 0; j < m2; ++j) hsub[(size_t)i * cap + j] = hn[(size_t)i * m2 + j];
           num_vec = m2;
           jacobi_eigh(hn, num_vec, w, V);
+          if (ctx->gen_follow) follow_roots(w, V, num_vec, (int)nroots);
           for (int q = 0; q < nroots; ++q) energy[q] = w[q];
           Vprev.clear();
           mprev = 0;
@@ -2929,14 +2965,24 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
           ctx->launch_count++;
           TCI_CUDA(cudaGetLastError());
           double nrm2 = 0.0;
-          ctx->multi_dot(r, 0, 1, r, n, &nrm2);
+          if (ctx->gen_g) {
+            // generalized solve: the residual of the reference, (H - E_ref) c - lambda G c = G^1/2 r_y
+            // (build_residual_gen_eig, davidson.f90:535-553), c = G^-1/2 y of unit G-norm as dsygv gives
+            // it: |G^1/2 r_y|^2 = sum_i g_i r_y,i^2
+            TCI_CUDA(cudaMemcpyAsync(tmpC, r, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            scale_by<<<G, TB, 0, st>>>(tmpC, ctx->gen_g, n);
+            ctx->launch_count++;
+            ctx->multi_dot(r, 0, 1, tmpC, n, &nrm2);
+          } else {
+            ctx->multi_dot(r, 0, 1, r, n, &nrm2);
+          }
           const double norm = std::sqrt(nrm2);
           // is_converged: never right after a restart; residual norm, then energy change (i > 1), then maxit
           bool halt = false;
           if (!(restarted[it] || (it > 1 && restarted[it - 1]))) {
             if (norm < tol_residual) halt = true;
             else if (std::fabs(dE[q]) < tol_energy) halt = it > 1;
-            else if (it == maxit) halt = true;
+            else if (it == maxit) halt = true, ran_out = true;
           }
           if (halt) {
             conv[q] = 1;
@@ -2976,6 +3022,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
         for (int q = 0; q < nroots; ++q) all = all && conv[q];
         if (all) break;
       }
+      ctx->last_converged = !ran_out && std::all_of(conv.begin(), conv.end(), [](int x) { return x != 0; });
       mark(7);
       ctx->check_tc_status();
       if (ctx->precision == 1 && ctx->refine) {
@@ -3026,6 +3073,7 @@ int tci_ctx_stats(const tci_ctx* ctx, double* out, int64_t len) {
   if (!ctx || !out || len < 8) return TCI_ERR_ARG;
   if (len >= 9) out[8] = 1.0 + (double)ctx->sigma_launches();  // + the accumulation into the caller's sigma
   if (len >= 10) out[9] = (double)ctx->launch_count;
+  if (len >= 11) out[10] = ctx->last_converged ? 1.0 : 0.0;
   out[0] = (double)ctx->nvec();
   out[1] = ctx->bytes_held;
   out[2] = ctx->init_seconds;
