@@ -1291,13 +1291,16 @@ void Builder::allext() {
     if (nab > 0) gather(Ut + r * nm, nab, d.off_ab + k * nab);
   }
   // FP64 form: Y = U W with the contraction split in S slices (the product has
-  // few output tiles and a very long k); the slices are summed in order.
+  // few output rows and a very long k); the slices are summed in order.  S gives
+  // the row-panel kernel (128 columns per block) about eight blocks per SM; the
+  // slices start on multiples of 32 columns of U (16-byte aligned operands).
   const i64 offWm = np * np;
-  const i64 S = std::max<i64>(1, std::min<i64>(8, np / 2048));
+  const i64 col_blocks = std::max<i64>(1, (np + 127) / 128);
+  const i64 S = std::max<i64>(1, std::min<i64>({16, np / 512, (148 * 8 + col_blocks - 1) / col_blocks}));
   const i64 Ps = T.alloc(S * std::max<i64>(1, P.n_sing) * np), Pt = T.alloc(S * std::max<i64>(1, P.n_trip) * nm);
   Step& g = step(P.sigma_steps, STEP_GEMM, "all-external");
   auto add_split = [&](i64 m, i64 dim, i64 U, i64 woff, i64 part) {
-    const i64 kc = (dim + S - 1) / S;
+    const i64 kc = ((dim + S - 1) / S + 31) / 32 * 32;
     for (i64 sidx = 0; sidx < S; ++sidx) {
       const i64 k0 = sidx * kc, kl = std::min(kc, dim - k0);
       if (kl <= 0) continue;
@@ -1311,7 +1314,7 @@ void Builder::allext() {
   if (P.n_trip > 0 && nm > 0) add_split(P.n_trip, nm, Ut, offWm, Pt);
   Step red = mkstep(STEP_AXPY, "all-external split-k sum");
   auto add_sum = [&](i64 m, i64 dim, i64 Y, i64 part) {
-    const i64 kc = (dim + S - 1) / S;
+    const i64 kc = ((dim + S - 1) / S + 31) / 32 * 32;
     AxpyTarget tg{BUF_T0, Y, m * dim, (i64)red.as.size(), 0};
     for (i64 sidx = 0; sidx < S; ++sidx)
       if (sidx * kc < dim) red.as.push_back(AxpySource{BUF_T0, part + sidx * m * dim, 1.0, -1, 0});

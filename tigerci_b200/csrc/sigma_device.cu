@@ -474,6 +474,128 @@ constexpr size_t panel_smem_bytes() {
   return sizeof(double) * (size_t)PANEL_STG * PANEL_KS * (PANEL_COLS + MT);
 }
 
+// Tiled FP64 GEMM with the operands staged by cp.async (the problem / segment tables and tile numbering
+// of gemm_tiled_f64<64, 128>): 64 x 128 tiles, 16-deep k slices, CP_STG slices in flight, 256 threads with
+// 4 x 8 outputs each (rows ty + 16 i, columns tx + 16 j).  A is M x K row major (tA = 0); B is K x N
+// (TB = 0, staged [k][n]) or N x K (TB = 1, staged [n][k] with its 16-byte chunks XOR-swizzled by the row
+// so that the column reads of a warp spread over the banks).  A segment's alpha scales its B values as
+// they are read, as in gemm_tiled_f64; segments in table order, k ascending.  Operands must start on
+// 16 bytes with even leading dimensions (checked when the step is lowered).
+constexpr int CP_BM = 64, CP_BN = 128, CP_BK = 16, CP_STG = 4;
+template <int TB>
+constexpr size_t cp_smem_bytes() {
+  return sizeof(double) * (size_t)CP_STG * (CP_BM * CP_BK + CP_BK * CP_BN);
+}
+template <int TB>
+__global__ void __launch_bounds__(256, 2) gemm_cp_f64(const DGemmProblem* __restrict__ probs, int nprob,
+                                                      const DGemmSeg* __restrict__ segs) {
+  extern __shared__ __align__(16) double cp_smem[];
+  double* As = cp_smem;                                  // [CP_STG][CP_BM][CP_BK]
+  double* Bs = cp_smem + CP_STG * CP_BM * CP_BK;         // [CP_STG][CP_BK][CP_BN] or [CP_STG][CP_BN][CP_BK]
+  const long long tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const DGemmProblem P = probs[lo];
+  const long long t = tile - P.tile_begin;
+  const long long m0 = (t / P.tiles_n) * CP_BM, n0 = (t % P.tiles_n) * CP_BN;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  for (long long sgi = P.seg_begin; sgi < P.seg_end; ++sgi) {
+    const DGemmSeg S = segs[sgi];
+    const long long K = S.K;
+    const long long nsl = (K + CP_BK - 1) / CP_BK;
+    const double al = S.alpha;
+    auto issue = [&](long long sl, int st) {
+      const long long k0 = sl * CP_BK;
+      double* a = As + (size_t)st * CP_BM * CP_BK;
+      double* b = Bs + (size_t)st * CP_BK * CP_BN;
+      // A: 64 rows x 8 chunks = 512 chunks, 2 per thread
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int e = tid + u * 256;
+        const int m = e >> 3, kc = 2 * (e & 7);
+        const long long gm = m0 + m, gk = k0 + kc;
+        const int bytes = (gm < P.M && gk < K) ? (gk + 1 < K ? 16 : 8) : 0;
+        cp_async16(a + m * CP_BK + kc, bytes ? (const void*)(S.A + gm * S.lda + gk) : (const void*)S.A, bytes);
+      }
+      // B: 16 x 128 doubles = 1024 chunks, 4 per thread
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = tid + u * 256;
+        if (TB == 0) {
+          const int kk = e >> 6, nc = 2 * (e & 63);
+          const long long gk = k0 + kk, gn = n0 + nc;
+          const int bytes = (gk < K && gn < P.N) ? (gn + 1 < P.N ? 16 : 8) : 0;
+          cp_async16(b + kk * CP_BN + nc, bytes ? (const void*)(S.B + gk * S.ldb + gn) : (const void*)S.B, bytes);
+        } else {
+          const int nn = e >> 3, c = e & 7;  // row nn of B (a column of op(B)), chunk c of its 16 k
+          const long long gn = n0 + nn, gk = k0 + 2 * c;
+          const int bytes = (gn < P.N && gk < K) ? (gk + 1 < K ? 16 : 8) : 0;
+          cp_async16(b + nn * CP_BK + 2 * (c ^ (nn & 7)), bytes ? (const void*)(S.B + gn * S.ldb + gk) : (const void*)S.B,
+                     bytes);
+        }
+      }
+    };
+    __syncthreads();  // the previous segment's stages have been read
+#pragma unroll
+    for (int st = 0; st < CP_STG - 1; ++st) {
+      if (st < nsl) issue(st, st);
+      cp_async_commit();
+    }
+    for (long long sl = 0; sl < nsl; ++sl) {
+      cp_async_wait<CP_STG - 2>();
+      __syncthreads();
+      if (sl + CP_STG - 1 < nsl) issue(sl + CP_STG - 1, (int)((sl + CP_STG - 1) % CP_STG));
+      cp_async_commit();
+      const int st = (int)(sl % CP_STG);
+      const double* a = As + (size_t)st * CP_BM * CP_BK;
+      const double* b = Bs + (size_t)st * CP_BK * CP_BN;
+#pragma unroll
+      for (int kp = 0; kp < CP_BK / 2; ++kp) {
+        double2 x[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = *reinterpret_cast<const double2*>(a + (ty + 16 * i) * CP_BK + 2 * kp);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          double b0, b1;
+          if (TB == 0) {
+            b0 = al * b[(2 * kp) * CP_BN + tx + 16 * j];
+            b1 = al * b[(2 * kp + 1) * CP_BN + tx + 16 * j];
+          } else {
+            const int nn = tx + 16 * j;
+            const double2 v = *reinterpret_cast<const double2*>(b + nn * CP_BK + 2 * (kp ^ (nn & 7)));
+            b0 = al * v.x;
+            b1 = al * v.y;
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[i][j] = fma(x[i].y, b1, fma(x[i].x, b0, acc[i][j]));
+        }
+      }
+    }
+    cp_async_wait<0>();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long gm = m0 + ty + 16 * i;
+    if (gm >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const long long gn = n0 + tx + 16 * j;
+      if (gn >= P.N) continue;
+      double* c = P.C + gm * P.ldc + gn;
+      *c = (P.beta == 0.0) ? acc[i][j] : fma(P.beta, *c, acc[i][j]);
+    }
+  }
+}
+
 // Segmented AXPY: target chunk t (at most AXPY_CHUNK elements) gets
 //   dst[i] += sum_s coef_s * scale_s * src_s[base + i].
 // One block per chunk; warp w takes the sources w, w + 8, ... in table order,
@@ -992,6 +1114,10 @@ struct DevStep {
   long long tma_rows = 0;  // kinds 4, 6, 7: rows of the gathered coefficients / of the exchange bank
   long long tma_aux2 = 0;  // kind 7: offset of the exchange bank in BUF_JK
   // FP64 form: problems with at most SKINNY_M rows and B given as N x K run on the skinny kernel
+  // FP64 problems on the cp.async-staged tiled kernel, by orientation of B
+  DGemmProblem* cp_probs[2] = {};
+  int cp_nprob[2] = {};
+  long long cp_ntiles[2] = {};
   // FP64 problems of few rows on the row-panel kernel, by row class (M <= 16, 24, ..., 64)
   DGemmProblem* panel_probs[7] = {};
   int panel_nprob[7] = {};
@@ -1390,8 +1516,8 @@ struct tci_ctx {
       d.segs = upload(sg, owned, stream);
       {
         // FP64 form: skinny problems (one-row products) to the warp-per-column kernel, the rest tiled
-        std::vector<DGemmProblem> reg, sk, pan[7];
-        long long rt = 0, wk = 0, pt[7] = {0, 0, 0, 0, 0, 0, 0};
+        std::vector<DGemmProblem> reg, sk, pan[7], cpp[2];
+        long long rt = 0, wk = 0, pt[7] = {0, 0, 0, 0, 0, 0, 0}, ct[2] = {0, 0};
         for (const auto& g : pr) {
           bool skinny = g.M <= SKINNY_M && s.name != "all-external";
           for (long long q = g.seg_begin; skinny && q < g.seg_end; ++q) skinny = sg[(size_t)q].tA == 0 && sg[(size_t)q].tB == 1;
@@ -1417,15 +1543,37 @@ struct tci_ctx {
             wk += (g.N + 7) / 8 * 8;
             sk.push_back(x);
           } else {
+            // the cp.async-staged tiled kernel where the operands allow 16-byte copies (A not transposed,
+            // one orientation of B per problem), else the register-staged one
+            bool cpk = true;
+            int tb = -1;
+            for (long long q = g.seg_begin; cpk && q < g.seg_end; ++q) {
+              const DGemmSeg& x = sg[(size_t)q];
+              cpk = x.tA == 0 && (tb < 0 || tb == x.tB) && ((x.lda | x.ldb) & 1) == 0 &&
+                    ((reinterpret_cast<uintptr_t>(x.A) | reinterpret_cast<uintptr_t>(x.B)) & 15) == 0;
+              tb = x.tB;
+            }
             DGemmProblem x = g;
-            x.tile_begin = rt;
-            rt += ((g.M + BMh - 1) / BMh) * x.tiles_n;
-            reg.push_back(x);
+            if (cpk && tb >= 0) {
+              x.tiles_n = (g.N + CP_BN - 1) / CP_BN;
+              x.tile_begin = ct[tb];
+              ct[tb] += ((g.M + CP_BM - 1) / CP_BM) * x.tiles_n;
+              cpp[tb].push_back(x);
+            } else {
+              x.tile_begin = rt;
+              rt += ((g.M + BMh - 1) / BMh) * x.tiles_n;
+              reg.push_back(x);
+            }
           }
         }
         d.probs = upload(reg, owned, stream);
         d.nprob = (int)reg.size();
         d.ntiles = rt;
+        for (int b = 0; b < 2; ++b) {
+          d.cp_probs[b] = upload(cpp[b], owned, stream);
+          d.cp_nprob[b] = (int)cpp[b].size();
+          d.cp_ntiles[b] = ct[b];
+        }
         d.skinny_probs = upload(sk, owned, stream);
         d.skinny_nprob = (int)sk.size();
         d.skinny_nwarps = wk;
@@ -1663,6 +1811,19 @@ struct tci_ctx {
            (s.tma_kind == 4 && tma_ss_ready) || (s.tma_kind == 5 && tma_1x_ready) || (s.tma_kind == 6 && tma_dv_ready) ||
            (s.tma_kind == 7 && tma_dvr_ready);
   }
+  template <int TB>
+  void launch_cp(const DevStep& s) {
+    if (s.cp_ntiles[TB] <= 0) return;
+    constexpr size_t smem = cp_smem_bytes<TB>();
+    static bool attr_set[64] = {};  // per device
+    int dev = 0;
+    TCI_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+      TCI_CUDA(cudaFuncSetAttribute(gemm_cp_f64<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      attr_set[dev] = true;
+    }
+    gemm_cp_f64<TB><<<(unsigned)s.cp_ntiles[TB], 256, smem, stream>>>(s.cp_probs[TB], s.cp_nprob[TB], s.segs);
+  }
   template <int MT>
   void launch_panel(const DevStep& s, int c) {
     if (s.panel_ntiles[c] <= 0) return;
@@ -1698,8 +1859,10 @@ struct tci_ctx {
         continue;
       }
       if (s.kind == STEP_GEMM && s.skinny_nwarps > 0) k += 1;
-      if (s.kind == STEP_GEMM)
+      if (s.kind == STEP_GEMM) {
         for (int c = 0; c < 7; ++c) k += s.panel_ntiles[c] > 0 ? 1 : 0;
+        for (int b = 0; b < 2; ++b) k += s.cp_ntiles[b] > 0 ? 1 : 0;
+      }
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
           ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && plan.nD > 0))
         k += 1;
@@ -2092,6 +2255,8 @@ struct tci_ctx {
         launch_panel<48>(s, 4);
         launch_panel<56>(s, 5);
         launch_panel<64>(s, 6);
+        launch_cp<0>(s);
+        launch_cp<1>(s);
         if (s.ntiles > 0) {
           if (s.cfg == 0) gemm_tiled_f64<64, 128, 4, 8><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
           else gemm_tiled_f64<128, 64, 8, 4><<<(unsigned)s.ntiles, 256, 0, stream>>>(s.probs, s.nprob, s.segs);
