@@ -45,6 +45,20 @@ using namespace tci;
 
 namespace {
 
+// Streaming multiprocessors of the current device (cached per device): grid-stride kernels launch a small
+// multiple of it.
+unsigned sm_count() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cached[dev] = v;
+  }
+  return (unsigned)cached[dev];
+}
+
 // ----------------------------------------------------------------------------
 // device-side table layouts (plain structs, 8-byte fields)
 using tci_dev::DGemmProblem;
@@ -1707,7 +1721,7 @@ struct tci_ctx {
     TCI_CUDA(cudaGetLastError());
     if (local) {
       TCI_CUDA(dev_malloc(&hd, n_loc * sizeof(double), stream));
-      gather_local<<<148 * 8, 256, 0, stream>>>(full, d_map, n_loc, hd);
+      gather_local<<<sm_count() * 8, 256, 0, stream>>>(full, d_map, n_loc, hd);
       TCI_CUDA(cudaGetLastError());
       TCI_CUDA(cudaStreamSynchronize(stream));
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
@@ -1766,7 +1780,7 @@ struct tci_ctx {
       return;
     }
     TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
+    if (gen_s) scale_by<<<sm_count() * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     run_sigma_steps();
     gen_out(d_s);
@@ -1777,14 +1791,14 @@ struct tci_ctx {
     if (gen_s) throw Error(TCI_ERR_INPUT, "the generalized (ACPF-type) solve is not available under pair domains");
     const i64 n = plan.total_csfs;
     TCI_CUDA(cudaMemsetAsync(buf[BUF_C], 0, n * sizeof(double), stream));
-    scatter_local<<<148 * 8, 256, 0, stream>>>(d_c, d_map, n_loc, buf[BUF_C]);
+    scatter_local<<<sm_count() * 8, 256, 0, stream>>>(d_c, d_map, n_loc, buf[BUF_C]);
     TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     launch_count += 1;
     TCI_CUDA(cudaGetLastError());
   }
   // local layout: d_s = P^T (plan's sigma) + the all-external term of the local blocks
   void local_out(const double* d_c, double* d_s) {
-    gather_local<<<148 * 8, 256, 0, stream>>>(buf[BUF_S], d_map, n_loc, d_s);
+    gather_local<<<sm_count() * 8, 256, 0, stream>>>(buf[BUF_S], d_map, n_loc, d_s);
     launch_count += 1;
     TCI_CUDA(cudaGetLastError());
     if (loc_allext) {
@@ -1796,7 +1810,7 @@ struct tci_ctx {
   void gen_out(double* d_s) {
     const i64 n = plan.total_csfs;
     if (gen_s) {
-      gen_sigma_out<<<148 * 8, 256, 0, stream>>>(d_s, buf[BUF_S], buf[BUF_C], gen_s, gen_shift, n);
+      gen_sigma_out<<<sm_count() * 8, 256, 0, stream>>>(d_s, buf[BUF_S], buf[BUF_C], gen_s, gen_shift, n);
       TCI_CUDA(cudaGetLastError());
     } else {
       TCI_CUDA(cudaMemcpyAsync(d_s, buf[BUF_S], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
@@ -2145,7 +2159,7 @@ struct tci_ctx {
       local_in(d_c);
     } else {
       TCI_CUDA(cudaMemcpyAsync(buf[BUF_C], d_c, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-      if (gen_s) scale_by<<<148 * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
+      if (gen_s) scale_by<<<sm_count() * 8, 256, 0, stream>>>(buf[BUF_C], gen_s, n);
       TCI_CUDA(cudaMemsetAsync(buf[BUF_S], 0, n * sizeof(double), stream));
     }
     const int64_t saved = precision;
@@ -2288,7 +2302,7 @@ struct tci_ctx {
         }
         break;
       case STEP_WBUILD:
-        build_allext<<<148 * 16, 256, 0, stream>>>(buf[BUF_X], plan.n, buf[BUF_W]);
+        build_allext<<<sm_count() * 16, 256, 0, stream>>>(buf[BUF_X], plan.n, buf[BUF_W]);
         break;
     }
     TCI_CUDA(cudaGetLastError());
@@ -2665,7 +2679,7 @@ int tci_sigma_device(tci_ctx* ctx, const double* d_c, double* d_sigma, int64_t n
       TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     }
     // sigma += S (the caller's sigma accumulates, like htimesc)
-    accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, ctx->stream>>>(d_sigma, s_out, n);
+    accumulate_f64<<<(unsigned)std::min<int64_t>((n + 255) / 256, sm_count() * 8), 256, 0, ctx->stream>>>(d_sigma, s_out, n);
     ctx->launch_count++;
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -2858,7 +2872,7 @@ int tci_davidson_gen(tci_ctx* ctx, int64_t nroots, double tol_residual, double t
     TCI_CUDA(dev_malloc(&dg, (size_t)n * sizeof(double), ctx->stream));
     TCI_CUDA(cudaMemcpyAsync(ds, sh.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     TCI_CUDA(cudaMemcpyAsync(dg, g, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    gen_diag<<<148 * 8, 256, 0, ctx->stream>>>(dd, ctx->hd, ds, e_shift, n);
+    gen_diag<<<sm_count() * 8, 256, 0, ctx->stream>>>(dd, ctx->hd, ds, e_shift, n);
     TCI_CUDA(cudaGetLastError());
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     saved_hd = ctx->hd;
@@ -2984,7 +2998,7 @@ int tci_davidson_ex(tci_ctx* ctx, int64_t nroots, double tol_residual, double to
     bool ran_out = false;  // a root stopped at maxit without meeting either tolerance
     try {
       cudaStream_t st = ctx->stream;
-      const unsigned G = 148 * 8, TB = 256;
+      const unsigned G = sm_count() * 8, TB = 256;
       // initial guess: unit vectors at the lowest diagonal elements (the order is a property of the
       // operator: kept in the context for the next solve)
       if ((i64)ctx->lowest_diag.size() < nroots) {
