@@ -495,13 +495,25 @@ def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3, nchol=2400, for
         # 3xTF32 issues three MMAs per product: its FP32-accurate peak is a third of the TF32 peak
         # (half the measured dense BF16 figure)
         peak = bf16 / 2 / 3 if form == "tf32x3" else None
-        out[form] = {"ms_per_apply": 1e3 * t, "tflops": st["flops"] / t / 1e12,
-                     "flops_per_apply": st["flops"], "chunk": int(st["chunk"]), "tile_cfg": int(st["tile_cfg"]),
+        # the form applied: the Cholesky form's flops are the useful work; the dense form does its own
+        # (padded) flops on the all-external kernel, and those set its tensor roofline
+        fl = st["dense_flops"] if st["form"] == "dense" else st["flops"]
+        kern = ("allext_tf32x3_kernel (dense padded W+/W- over all external pairs, tcgen05 kind::tf32, 3xTF32)"
+                if st["form"] == "dense" else
+                "tma_gemm (grouped 3xTF32, pair-domain Cholesky form)" if form == "tf32x3" else
+                "gemm_f64 grouped (pair-domain Cholesky form, FP64)")
+        out[form] = {"ms_per_apply": 1e3 * t, "form": st["form"], "useful_tflops": st["flops"] / t / 1e12,
+                     "flops_per_apply": fl, "cholesky_form_flops": st["flops"],
+                     "cholesky_form_setup_ms": st["tuned_ms"], "dense_form_setup_ms": st["dense_ms"] or None,
+                     "chunk": int(st["chunk"]), "tile_cfg": int(st["tile_cfg"]),
                      "autotune_candidates": int(st["candidates"]), "device_gb": st["device_bytes"] / 1e9,
                      "init_s": init_s,
-                     "roofline": {"bound": "tensor", "achieved": st["flops"] / t / 1e12, "peak": peak,
-                                  "unit": "TFLOP/s", "frac": (st["flops"] / t / 1e12 / peak) if peak else None,
+                     "roofline": {"kernel": kern, "bound": "tensor", "achieved": fl / t / 1e12, "peak": peak,
+                                  "unit": "TFLOP/s", "frac": (fl / t / 1e12 / peak) if peak else None,
                                   "peak_kind": "3xTF32: measured dense BF16 / 2 / 3" if peak else None}}
+        if st["form"] == "dense":
+            # the W tiles are streamed once per group of 64 CI blocks of each operator
+            out[form]["w_gb"] = st["dense_w_bytes"] / 1e9
         op.close()
     if "tf32x3" in sig and "fp64" in sig:
         a, b = sig["tf32x3"], sig["fp64"]

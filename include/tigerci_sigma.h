@@ -247,9 +247,16 @@ void tci_destroy(tci_ctx* ctx);
  * size: ab n(n-1)/2 per spin function, pair index i(i-1)/2+j (i > j), aa n.
  * chol is the tci_operator Cholesky array over num_internal + num_external
  * orbitals.  Applied in the Cholesky form (two grouped GEMMs over all heads
- * per chunk of Cholesky vectors).  options: [0] precision (TCI_PRECISION_*),
- * [1] device bytes for the per-chunk buffers (default 16e9), [2] promotion
- * block, [3] 0 to skip the set-up autotuning of chunk size and tile shape. */
+ * per chunk of Cholesky vectors) or, in the mixed precision, in the dense
+ * padded integral form (the blocks placed among all externals against FP32
+ * W+ / W- tiles over all external pairs, on the tcgen05 all-external kernel),
+ * whichever a timed run at set-up finds faster.  options: [0] precision
+ * (TCI_PRECISION_*), [1] device bytes for the per-chunk buffers (default
+ * 16e9), [2] promotion block, [3] 0 to skip the set-up autotuning of chunk
+ * size and tile shape, [4] form: 0 the faster (default; the dense form only
+ * where the device has room for X = Lpk Lpk^T and the W tiles), 1 Cholesky,
+ * 2 dense (TCI_ERR_INPUT in FP64 or with a triplet-coupled aa block,
+ * TCI_ERR_MEMORY without the room). */
 typedef struct tci_local tci_local;
 int tci_local_create(int64_t num_internal, int64_t num_external, const double* chol, int64_t nchol, int64_t n_heads,
                      const int64_t* heads, const int64_t* dom_idx, int64_t total_len, int64_t device,
@@ -259,10 +266,13 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
 int tci_local_apply(tci_local* loc, const double* d_c, double* d_sigma, int64_t n, void* stream);
 /* The same with host arrays. */
 int tci_local_apply_host(tci_local* loc, const double* c, double* sigma, int64_t n);
-/* out[9]: flops per application (4 nchol sum n^3 over head spin functions),
- * gathered Cholesky bytes per application, device bytes, chunk size, FP64 tile
- * shape of the second GEMM, autotuned time (ms), autotuner candidates, last
- * host application (ms), head spin-function blocks. */
+/* out[len], len >= 9, up to 13: flops per application (4 nchol sum n^3 over
+ * head spin functions), gathered Cholesky bytes per application, device
+ * bytes, chunk size, FP64 tile shape of the second GEMM, autotuned time (ms),
+ * autotuner candidates, last host application (ms), head spin-function
+ * blocks, form applied (0 Cholesky, 1 dense), the dense form's set-up time
+ * (ms, 0 if not timed), its flops (2 np^2 per singlet-coupled and 2 nm^2 per
+ * triplet-coupled block), its W tile bytes. */
 int tci_local_stats(const tci_local* loc, double* out, int64_t len);
 void tci_local_destroy(tci_local* loc);
 

@@ -375,6 +375,52 @@ __global__ void to_f32_tiles(const double* __restrict__ src, long long np, int n
   }
 }
 
+// The same tiles built directly from the packed external (ab|cd) matrix X (npk x npk, npk = n(n+1)/2,
+// row (ab) = a(a+1)/2 + b, a >= b) without an FP64 W: W+ (plus, np = n + n(n-1)/2 rows: the n pairs (aa),
+// then (ac) a > c at n + a(a-1)/2 + c) or W- (nm = n(n-1)/2 rows (ac)), by the element formulas of the FP64
+// build (sqrt2 on the (aa) rows / columns of W+; (ab|cd) +- (ad|cb) elsewhere).
+__device__ __forceinline__ long long xpk(long long a, long long b) {
+  return a >= b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a;
+}
+__device__ __forceinline__ void xunpair(long long x, long long& a, long long& b) {
+  long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)x)) * 0.5);
+  while (i * (i - 1) / 2 > x) --i;
+  while ((i + 1) * i / 2 <= x) ++i;
+  a = i;
+  b = x - i * (i - 1) / 2;
+}
+__global__ void x_to_f32_tiles(const double* __restrict__ X, long long n, int plus, int nk, float* __restrict__ dst,
+                               long long total) {
+  const long long nab = n * (n - 1) / 2, np = plus ? n + nab : nab, npk = n * (n + 1) / 2;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long t = e / TILE_FLOATS;
+    const int i = (int)(e % TILE_FLOATS);
+    const int r = i / BK, c = i % BK;
+    const long long panel = t / nk, k = t % nk;
+    const long long gr = panel * BM + r, gc = k * BK + c;
+    float v = 0.0f;
+    if (gr < np && gc < np) {
+      long long a, cc, b, d;
+      const bool rd = plus && gr < n, cd = plus && gc < n;
+      if (rd) a = cc = gr;
+      else xunpair(plus ? gr - n : gr, a, cc);
+      if (cd) b = d = gc;
+      else xunpair(plus ? gc - n : gc, b, d);
+      double w;
+      if (plus) {
+        if (rd && cd) w = X[xpk(a, b) * npk + xpk(a, b)];
+        else if (rd) w = 1.4142135623730951 * X[xpk(a, b) * npk + xpk(a, d)];
+        else if (cd) w = 1.4142135623730951 * X[xpk(a, b) * npk + xpk(cc, b)];
+        else w = X[xpk(a, b) * npk + xpk(cc, d)] + X[xpk(cc, b) * npk + xpk(a, d)];
+      } else {
+        w = X[xpk(a, b) * npk + xpk(cc, d)] - X[xpk(cc, b) * npk + xpk(a, d)];
+      }
+      v = (float)w;
+    }
+    dst[t * TILE_FLOATS + (sw128_offset(r, c) >> 2)] = v;
+  }
+}
+
 // U (m x np, FP64) -> interleaved rows: 2j = TF32 high part of U[j] (masked), 2j+1 = FP32 low
 // part; rows up to 2 mpad, zero past m and np.
 __global__ void split_u(const double* __restrict__ U, int m, int np, long long ldu, float* __restrict__ u2,
@@ -455,6 +501,14 @@ int64_t w32_floats(int64_t np) {
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st) {
   tci_tc::to_f32_tiles<<<148 * 16, 256, 0, st>>>(w64, np, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
                                                   (long long)w32_floats(np));
+  return cudaGetLastError();
+}
+
+cudaError_t convert_w_from_x(const double* x, int64_t n, bool plus, float* w32, cudaStream_t st) {
+  const int64_t np = plus ? n + n * (n - 1) / 2 : n * (n - 1) / 2;
+  if (np <= 0) return cudaSuccess;
+  tci_tc::x_to_f32_tiles<<<148 * 16, 256, 0, st>>>(x, n, plus ? 1 : 0, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
+                                                    (long long)w32_floats(np));
   return cudaGetLastError();
 }
 

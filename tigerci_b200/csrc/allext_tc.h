@@ -24,6 +24,9 @@ int64_t u2_floats(int64_t m, int64_t np);  // size of the split U
 int64_t w32_floats(int64_t np);  // size of W's FP32 tile array
 // FP64 W (np x np) -> the tile array the kernel streams (w32_floats(np) floats)
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st);
+// The tiles of W+ (plus) or W- over n externals straight from the packed (ab|cd) matrix X (n(n+1)/2 squared,
+// FP64), without an FP64 W: w32_floats(n + n(n-1)/2) or w32_floats(n(n-1)/2) floats.
+cudaError_t convert_w_from_x(const double* x, int64_t n, bool plus, float* w32, cudaStream_t st);
 cudaError_t split_u(const double* u, int64_t m, int64_t np, float* u2, cudaStream_t st);
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t m, double* y, int* status,
              int64_t kblock, std::string& err);

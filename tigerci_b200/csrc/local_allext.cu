@@ -26,6 +26,22 @@
 // The chunk size and the FP64 tile shape of the second GEMM come from a small
 // autotuner that times each candidate once at set-up.  One application
 // (unpack, chunks, pack) is captured as one CUDA graph.
+//
+// In the mixed form a second, dense form competes with it: the packed
+// integral form of the non-local all-external term (W+ over the pairs (aa)
+// and (ac), W- over (ac), a > c, of ALL externals, as FP32 tiles built once
+// from X = Lpk Lpk^T) applied to the local blocks placed at their pairs among
+// all externals (zero elsewhere, rows of U+ for singlet-coupled and U- for
+// triplet-coupled spin functions) on the tcgen05 all-external kernel
+// (allext_tc.cu), the result read back at the domain's pairs.  Exact: the
+// blocks are zero outside their domains, so (W U)_h restricted to domain(h)
+// is the domain-restricted integral form.  It spends its flops on the zero
+// columns of U (2 np^2 per block against 4 nchol n_h^3 in the Cholesky form)
+// but runs them as one long stream of W tiles at the all-external kernel's
+// rate, which beats the short uneven GEMMs of the Cholesky form when the
+// domains are a sizeable part of the externals.  Both are timed at set-up
+// (device memory permitting: X and the W tiles need 8 npv^2 + 4 np^2 + 4 nm^2
+// bytes) and the faster one is kept.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,10 +50,12 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/tigerci_sigma.h"
 #include "gemm_tables.h"
+#include "allext_tc.h"
 #include "gemm_tma.h"
 #include "host/capi_internal.h"
 
@@ -66,6 +84,7 @@ struct DLocBlock {
   long long head;            // index of the head
   long long t_off;           // offset of T_hk (jmax n x n) in the chunk buffer
   long long drow, trow;      // mixed form: first row of D_hk / T_hk in the split arrays
+  long long urow;            // dense form: row of the block in U+ (p = +1) or U- (p = -1)
 };
 // one head for the gather
 struct DLocHead {
@@ -183,6 +202,56 @@ __global__ void unpack_local_split(const DLocBlock* __restrict__ blk, const doub
   }
 }
 
+// Dense form: the block's entries at their places among all externals, as the interleaved TF32-high /
+// FP32-low rows of U+ (singlet-coupled blocks: the n_ext pairs (aa), then the pairs (ac), a > c, at
+// n_ext + a(a-1)/2 + c) or U- (triplet-coupled blocks: the pairs (ac) at a(a-1)/2 + c).  The rows are zero
+// outside the domain (set before the launch).
+__global__ void gather_dense(const DLocBlock* __restrict__ blk, const DLocHead* __restrict__ heads,
+                             const long long* __restrict__ dom, const double* __restrict__ c, long long n_ext,
+                             float* __restrict__ u2p, long long ldp_p, float* __restrict__ u2m, long long ldp_m) {
+  const DLocBlock B = blk[blockIdx.x];
+  const long long* d = dom + heads[B.head].dom_off;
+  const long long n = B.n, nab = n * (n - 1) / 2;
+  const bool plus = B.p > 0.0;
+  const long long ld = plus ? ldp_p : ldp_m, base = plus ? n_ext : 0;
+  float* hi = (plus ? u2p : u2m) + 2 * B.urow * ld;
+  float* lo = hi + ld;
+  if (B.ab)
+    for (long long e = threadIdx.x; e < nab; e += blockDim.x) {
+      long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
+      while (i * (i - 1) / 2 > e) --i;
+      while ((i + 1) * i / 2 <= e) ++i;
+      const long long I = d[i], J = d[e - i * (i - 1) / 2];  // sorted domain: I > J
+      split_put(hi, lo, base + I * (I - 1) / 2 + J, c[B.off_ab + B.k * nab + e]);
+    }
+  if (B.aa)
+    for (long long a = threadIdx.x; a < n; a += blockDim.x) split_put(hi, lo, d[a], c[B.off_aa + B.k * n + a]);
+}
+
+// Dense form: the block's entries of Y+ (row pitch ldy_p) / Y- (ldy_m) into sigma (every entry of a block is
+// written: sigma holds nothing else there)
+__global__ void scatter_dense(const DLocBlock* __restrict__ blk, const DLocHead* __restrict__ heads,
+                              const long long* __restrict__ dom, const double* __restrict__ yp, long long ldy_p,
+                              const double* __restrict__ ym, long long ldy_m, long long n_ext,
+                              double* __restrict__ sigma) {
+  const DLocBlock B = blk[blockIdx.x];
+  const long long* d = dom + heads[B.head].dom_off;
+  const long long n = B.n, nab = n * (n - 1) / 2;
+  const bool plus = B.p > 0.0;
+  const double* y = plus ? yp + B.urow * ldy_p : ym + B.urow * ldy_m;
+  const long long base = plus ? n_ext : 0;
+  if (B.ab)
+    for (long long e = threadIdx.x; e < nab; e += blockDim.x) {
+      long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
+      while (i * (i - 1) / 2 > e) --i;
+      while ((i + 1) * i / 2 <= e) ++i;
+      const long long I = d[i], J = d[e - i * (i - 1) / 2];
+      sigma[B.off_ab + B.k * nab + e] = y[base + I * (I - 1) / 2 + J];
+    }
+  if (B.aa)
+    for (long long a = threadIdx.x; a < n; a += blockDim.x) sigma[B.off_aa + B.k * n + a] = y[d[a]];
+}
+
 __global__ void add_into(double* __restrict__ dst, const double* __restrict__ src, long long n) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] += src[i];
@@ -215,6 +284,7 @@ struct tci_local {
   double flops = 0, lbytes = 0, dev_bytes = 0, last_ms = 0, tuned_ms = 0;
   int64_t candidates = 0;
   std::vector<void*> owned;
+  std::unordered_map<void*, double> sizes;  // bytes of each alloc() buffer
   double *LT = nullptr, *Lc = nullptr, *T = nullptr, *D = nullptr, *R = nullptr, *Cb = nullptr, *Sb = nullptr;
   long long rlen = 0;
   DLocHead* dheads = nullptr;
@@ -229,6 +299,14 @@ struct tci_local {
   float *lc_hi = nullptr, *lc_lo = nullptr, *d_hi = nullptr, *d_lo = nullptr, *t_hi = nullptr, *t_lo = nullptr;
   tci_gtma_host::TmaMaps map1, map1n, map2;  // T = Lc D (128- or 64-wide tiles) ; R += 1/2 T Lc
   TmaLaunch m1, m2, m1r, m2r;
+  // dense padded integral form (mixed precision): W+ / W- over all externals as FP32 tiles
+  int form = 0;              // form in use: 0 Cholesky, 1 dense
+  bool dense_ready = false;  // the dense operators are built
+  int64_t np_d = 0, nm_d = 0, nsing_d = 0, ntrip_d = 0;
+  float *w32p = nullptr, *w32m = nullptr, *u2p = nullptr, *u2m = nullptr;
+  double *yp = nullptr, *ym = nullptr;
+  tci_tc_host::AllextTc tcp, tcm;
+  double dense_flops = 0, dense_ms = 0, dense_bytes = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -262,6 +340,22 @@ struct tci_local {
     LCUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     return d;
   }
+  // frees an allocation made by alloc()
+  template <class T>
+  void release(T*& p) {
+    if (!p) return;
+    LCUDA(cudaStreamSynchronize(stream));
+    auto it = std::find(owned.begin(), owned.end(), (void*)p);
+    if (it != owned.end()) owned.erase(it);
+    auto sz = sizes.find((void*)p);
+    if (sz != sizes.end()) {
+      dev_bytes -= sz->second;
+      sizes.erase(sz);
+    }
+    LCUDA(cudaFree(p));
+    p = nullptr;
+  }
+  float* alloc_f(size_t n) { return reinterpret_cast<float*>(alloc((n + 1) / 2)); }
   double* alloc(size_t n) {
     double* p = nullptr;
     if (cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(double)) != cudaSuccess) {
@@ -270,6 +364,7 @@ struct tci_local {
     }
     owned.push_back(p);
     dev_bytes += (double)n * sizeof(double);
+    sizes[(void*)p] = (double)n * sizeof(double);
     return p;
   }
 
@@ -338,9 +433,78 @@ struct tci_local {
     LCUDA(tci_dev::launch_gemm_f64(g.cfg, g.probs, g.nprob, g.segs, g.ntiles, stream));
   }
 
+  // Dense form set-up from the virtual-virtual Cholesky rows lpk (npv x nchol, row-major, on the device):
+  // the exchange product X = Lpk Lpk^T (npv x npv) on the TMA-fed 3xTF32 kernel, the W+ / W- tiles read
+  // from it, X released.  Assigns each block its row of U+ / U-.
+  void build_dense(const double* lpk) {
+    const int64_t n = nvirt, nab = n * (n - 1) / 2;
+    np_d = n + nab;
+    nm_d = nab;
+    nsing_d = ntrip_d = 0;
+    for (auto& B : blocks) B.urow = B.p > 0.0 ? nsing_d++ : ntrip_d++;
+    const int64_t ldk = tci_gtma_host::pitch(nchol);
+    float* ah = alloc_f((size_t)(npv * ldk));
+    float* al = alloc_f((size_t)(npv * ldk));
+    double* X = alloc((size_t)(npv * npv));
+    LCUDA(tci_gtma_host::split(lpk, npv, nchol, nchol, ah, al, stream));
+    tci_gtma_host::TmaMaps m;
+    std::string err;
+    if (!tci_gtma_host::prepare(m, ah, al, npv, nchol, ah, al, npv, nchol, true, err)) throw Error(TCI_ERR_CUDA, err);
+    const long long TM = tci_gtma_host::tile_m(), TN = tci_gtma_host::tile_n(true), tn = (npv + TN - 1) / TN;
+    std::vector<TmaProblem> q{TmaProblem{X, npv, npv, npv, tn, 0, 0.0, 0, 1, 0, nullptr, nullptr, 0}};
+    std::vector<TmaSeg> sg{TmaSeg{0, 0, 0, nchol, 1.0}};
+    TmaProblem* dq = upload(q);
+    TmaSeg* ds = upload(sg);
+    LCUDA(tci_gtma_host::launch(m, dq, 1, ds, ((npv + TM - 1) / TM) * tn, (int)kblock, status, stream));
+    LCUDA(cudaStreamSynchronize(stream));
+    check_status();
+    release(ah);
+    release(al);
+    w32p = alloc_f((size_t)tci_tc_host::w32_floats(np_d));
+    LCUDA(tci_tc_host::convert_w_from_x(X, n, true, w32p, stream));
+    if (nm_d > 0) {
+      w32m = alloc_f((size_t)tci_tc_host::w32_floats(nm_d));
+      LCUDA(tci_tc_host::convert_w_from_x(X, n, false, w32m, stream));
+    }
+    release(X);
+    if (nsing_d > 0) {
+      u2p = alloc_f((size_t)tci_tc_host::u2_floats(nsing_d, np_d));
+      yp = alloc((size_t)(nsing_d * np_d));
+      if (!tci_tc_host::prepare(tcp, w32p, np_d, u2p, nsing_d, yp, status, kblock, err)) throw Error(TCI_ERR_CUDA, err);
+    }
+    if (ntrip_d > 0) {
+      u2m = alloc_f((size_t)tci_tc_host::u2_floats(ntrip_d, nm_d));
+      ym = alloc((size_t)(ntrip_d * nm_d));
+      if (!tci_tc_host::prepare(tcm, w32m, nm_d, u2m, ntrip_d, ym, status, kblock, err)) throw Error(TCI_ERR_CUDA, err);
+    }
+    dense_flops = 2.0 * (double)np_d * (double)np_d * (double)nsing_d + 2.0 * (double)nm_d * (double)nm_d * (double)ntrip_d;
+    dense_bytes = 4.0 * ((double)tci_tc_host::w32_floats(np_d) + (nm_d > 0 ? (double)tci_tc_host::w32_floats(nm_d) : 0.0));
+    dense_ready = true;
+  }
+
+  // Dense form, one application: Sb = [U+ W+ ; U- W-] gathered from and scattered to the local blocks.
+  void record_dense() {
+    const unsigned nb = (unsigned)blocks.size();
+    LCUDA(cudaMemsetAsync(Sb, 0, sizeof(double) * (size_t)total, stream));
+    if (nsing_d > 0)
+      LCUDA(cudaMemsetAsync(u2p, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(nsing_d, np_d), stream));
+    if (ntrip_d > 0)
+      LCUDA(cudaMemsetAsync(u2m, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(ntrip_d, nm_d), stream));
+    gather_dense<<<nb, 256, 0, stream>>>(dblocks, dheads, ddom, Cb, nvirt, u2p, tci_tc_host::padded_ld(np_d), u2m,
+                                         tci_tc_host::padded_ld(std::max<int64_t>(1, nm_d)));
+    LCUDA(cudaGetLastError());
+    LCUDA(tci_tc_host::launch(nsing_d > 0 ? &tcp : nullptr, ntrip_d > 0 ? &tcm : nullptr, stream));
+    scatter_dense<<<nb, 256, 0, stream>>>(dblocks, dheads, ddom, yp, np_d, ym, nm_d, nvirt, Sb);
+    LCUDA(cudaGetLastError());
+  }
+
   // One application on the internal buffers: Sb = A Cb.
   void record_apply() {
     const unsigned nb = (unsigned)blocks.size();
+    if (form == 1) {
+      record_dense();
+      return;
+    }
     if (precision == 1) {
       unpack_local_split<<<nb, 256, 0, stream>>>(dblocks, Cb, d_hi, d_lo, ldp);
       LCUDA(cudaGetLastError());
@@ -377,9 +541,10 @@ struct tci_local {
     LCUDA(cudaGetLastError());
   }
 
-  // Tables and graph for chunk size j and second-GEMM tile shape cfg.
+  // Tables and graph for chunk size j and second-GEMM tile shape cfg (Cholesky form).
   void configure(int64_t j, int cfg) {
     release_graph();
+    form = 0;
     jc = j;
     cfg2 = cfg;
     const int64_t rem = nchol % jc;
@@ -390,6 +555,16 @@ struct tci_local {
       make_gemms(jc, cfg2, g1, g2);
       if (rem) make_gemms(rem, cfg2, g1r, g2r);
     }
+    capture();
+  }
+  // Graph of the dense form.
+  void configure_dense() {
+    release_graph();
+    form = 1;
+    capture();
+  }
+  // one application captured as the graph in use
+  void capture() {
     LCUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
       record_apply();
@@ -407,6 +582,25 @@ struct tci_local {
     LCUDA(cudaEventRecord(e0, stream));
     LCUDA(cudaGraphLaunch(exec, stream));
     LCUDA(cudaEventRecord(e1, stream));
+  }
+  // one timed application of the graph in use (ms)
+  float time_once() {
+    run();
+    LCUDA(cudaStreamSynchronize(stream));
+    float ms = 0;
+    LCUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return ms;
+  }
+  // buffers of the Cholesky form (after the dense form was chosen)
+  void release_cholesky() {
+    for (double** p : {&LT, &Lc, &T, &D, &R}) release(*p);
+    for (float** p : {&lc_hi, &lc_lo, &d_hi, &d_lo, &t_hi, &t_lo}) release(*p);
+  }
+  // buffers of the dense form (after the Cholesky form was chosen)
+  void release_dense() {
+    for (float** p : {&w32p, &w32m, &u2p, &u2m}) release(*p);
+    for (double** p : {&yp, &ym}) release(*p);
+    dense_ready = false;
   }
 
   void check_status() {
@@ -436,6 +630,8 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
     const double budget = (options && n_options > 1 && options[1] > 0) ? (double)options[1] : 16e9;
     if (options && n_options > 2 && options[2] > 0) L->kblock = options[2];
     const bool tune = !(options && n_options > 3 && options[3] == 0);
+    const int64_t want_form = (options && n_options > 4) ? options[4] : 0;  // 0 faster, 1 Cholesky, 2 dense
+    if (want_form < 0 || want_form > 2) throw Error(TCI_ERR_ARG, "unknown all-external form");
     if (L->precision < 0 || L->precision > 1 || L->kblock % 32) throw Error(TCI_ERR_ARG, "bad precision or promotion block");
     // heads and blocks (host checks: every index below is bounds-checked here, not on the device)
     long long dtot = 0, lc_per_j = 0, t_per_j = 0, dom_total = 0, lrows = 0, drows = 0, nmax = 0;
@@ -501,8 +697,38 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
     LCUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
     LCUDA(cudaEventCreate(&L->e0));
     LCUDA(cudaEventCreate(&L->e1));
-    // virtual-virtual Cholesky rows, then J-major on the device
+    LCUDA(cudaMalloc(&L->status, sizeof(int)));
+    L->owned.push_back(L->status);
+    LCUDA(cudaMemsetAsync(L->status, 0, sizeof(int), L->stream));
     L->npv = num_external * (num_external + 1) / 2;
+    // form: the dense padded integral form needs the mixed precision and every aa block singlet-coupled
+    bool dense = L->precision == 1 && want_form != 1;
+    for (const auto& B : L->blocks)
+      if (B.aa && B.p < 0.0) dense = false;
+    if (want_form == 2 && !dense)
+      throw Error(TCI_ERR_INPUT, "the dense all-external form needs the mixed precision and singlet-coupled aa blocks");
+    const bool chol_form = want_form != 2;
+    if (dense) {
+      // device bytes it needs at set-up (X, the split Cholesky rows, the W tiles, U and Y), with the
+      // Cholesky form's buffers when both are timed, against what the device has free
+      const int64_t n = num_external, nab = n * (n - 1) / 2, np = n + nab;
+      int64_t ns = 0, nt = 0;
+      for (const auto& B : L->blocks) (B.p > 0.0 ? ns : nt)++;
+      double need = 8.0 * (double)L->npv * (double)L->npv + 8.0 * (double)L->npv * (double)tci_gtma_host::pitch(nchol) +
+                    4.0 * ((double)tci_tc_host::w32_floats(np) + (nab > 0 ? (double)tci_tc_host::w32_floats(nab) : 0.0)) +
+                    (ns > 0 ? 4.0 * (double)tci_tc_host::u2_floats(ns, np) + 8.0 * (double)(ns * np) : 0.0) +
+                    (nt > 0 ? 4.0 * (double)tci_tc_host::u2_floats(nt, nab) + 8.0 * (double)(nt * nab) : 0.0) +
+                    8.0 * (double)L->npv * (double)nchol + 2e9;
+      if (chol_form) need += 8.0 * (double)L->npv * (double)nchol + per_j * (double)L->jmax + 8.0 * (double)dtot;
+      size_t free_b = 0, total_b = 0;
+      LCUDA(cudaMemGetInfo(&free_b, &total_b));
+      if ((double)free_b < need) {
+        if (want_form == 2) throw Error(TCI_ERR_MEMORY, "not enough device memory for the dense all-external form");
+        dense = false;
+      }
+    }
+    // virtual-virtual Cholesky rows (row-major on the device for the dense form's exchange product, J-major
+    // for the Cholesky form)
     {
       std::vector<double> lvv((size_t)(L->npv * nchol));
       for (int64_t a = 0; a < num_external; ++a) {
@@ -513,19 +739,19 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
       }
       double* tmp = L->alloc(lvv.size());
       LCUDA(cudaMemcpyAsync(tmp, lvv.data(), lvv.size() * sizeof(double), cudaMemcpyHostToDevice, L->stream));
-      L->LT = L->alloc(lvv.size());
-      dim3 grid((unsigned)((nchol + 31) / 32), (unsigned)((L->npv + 31) / 32));
-      transpose_l<<<grid, dim3(32, 8), 0, L->stream>>>(tmp, L->npv, nchol, L->LT);
-      LCUDA(cudaGetLastError());
-      LCUDA(cudaStreamSynchronize(L->stream));
-      LCUDA(cudaFree(tmp));
-      L->owned.erase(std::find(L->owned.begin(), L->owned.end(), (void*)tmp));
-      L->dev_bytes -= (double)lvv.size() * sizeof(double);
+      if (dense) L->build_dense(tmp);
+      if (chol_form) {
+        L->LT = L->alloc(lvv.size());
+        dim3 grid((unsigned)((nchol + 31) / 32), (unsigned)((L->npv + 31) / 32));
+        transpose_l<<<grid, dim3(32, 8), 0, L->stream>>>(tmp, L->npv, nchol, L->LT);
+        LCUDA(cudaGetLastError());
+      }
+      L->release(tmp);
     }
-    if (L->precision == 1) {
+    if (chol_form && L->precision == 1) {
       // split arrays, zeroed once: the columns past each domain's n stay zero (the padding of the K tiles)
       auto falloc = [&](float** p, long long rows) {
-        *p = reinterpret_cast<float*>(L->alloc((size_t)(rows * L->ldp + 1) / 2));
+        *p = L->alloc_f((size_t)(rows * L->ldp));
         LCUDA(cudaMemsetAsync(*p, 0, sizeof(float) * (size_t)(rows * L->ldp), L->stream));
       };
       falloc(&L->lc_hi, L->rows_l);
@@ -543,46 +769,56 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
           !tci_gtma_host::prepare(L->map2, L->t_hi, L->t_lo, L->rows_t, nmax, L->lc_hi, L->lc_lo, L->rows_l, nmax, wide,
                                   err))
         throw Error(TCI_ERR_CUDA, err);
-    } else {
+    } else if (chol_form) {
       L->Lc = L->alloc((size_t)(lc_per_j * L->jmax));
       L->T = L->alloc((size_t)(t_per_j * L->jmax));
       L->D = L->alloc((size_t)dtot);
     }
-    L->R = L->alloc((size_t)dtot);
+    if (chol_form) L->R = L->alloc((size_t)dtot);
     L->Cb = L->alloc((size_t)total_len);
     L->Sb = L->alloc((size_t)total_len);
     LCUDA(cudaMemsetAsync(L->Cb, 0, sizeof(double) * (size_t)total_len, L->stream));
+    LCUDA(cudaMemsetAsync(L->Sb, 0, sizeof(double) * (size_t)total_len, L->stream));
     L->dheads = L->upload(L->heads);
     L->dblocks = L->upload(L->blocks);
     L->ddom = L->upload(dom);
-    LCUDA(cudaMalloc(&L->status, sizeof(int)));
-    L->owned.push_back(L->status);
-    LCUDA(cudaMemsetAsync(L->status, 0, sizeof(int), L->stream));
 
     // autotuner: chunk size (largest, half, quarter) x FP64 tile shape of the second GEMM (mixed form: tile
-    // width of the first GEMM, 128 or 64); one timed run each
-    std::vector<std::pair<int64_t, int>> cand;
-    for (int64_t j : {L->jmax, std::max<int64_t>(1, L->jmax / 2), std::max<int64_t>(1, L->jmax / 4)})
-      for (int cfg : {0, 1}) {
-        if (std::find(cand.begin(), cand.end(), std::make_pair(j, cfg)) == cand.end()) cand.push_back({j, cfg});
-      }
-    if (!tune) cand.resize(1);
+    // width of the first GEMM, 128 or 64); one timed run each.  Then the dense form, timed on its second
+    // run; the faster form stays and the other's buffers are released.
     double best = 1e300;
-    std::pair<int64_t, int> pick = cand[0];
-    for (const auto& c : cand) {
-      L->configure(c.first, c.second);
-      L->run();
-      LCUDA(cudaStreamSynchronize(L->stream));
-      float ms = 0;
-      LCUDA(cudaEventElapsedTime(&ms, L->e0, L->e1));
-      if (ms < best) {
-        best = ms;
-        pick = c;
+    if (chol_form) {
+      std::vector<std::pair<int64_t, int>> cand;
+      for (int64_t j : {L->jmax, std::max<int64_t>(1, L->jmax / 2), std::max<int64_t>(1, L->jmax / 4)})
+        for (int cfg : {0, 1}) {
+          if (std::find(cand.begin(), cand.end(), std::make_pair(j, cfg)) == cand.end()) cand.push_back({j, cfg});
+        }
+      if (!tune) cand.resize(1);
+      std::pair<int64_t, int> pick = cand[0];
+      for (const auto& c : cand) {
+        L->configure(c.first, c.second);
+        const float ms = L->time_once();
+        if (ms < best) {
+          best = ms;
+          pick = c;
+        }
+      }
+      L->candidates = (int64_t)cand.size();
+      L->tuned_ms = best;
+      if (pick != std::make_pair(L->jc, L->cfg2)) L->configure(pick.first, pick.second);
+    }
+    if (L->dense_ready) {
+      L->configure_dense();
+      L->time_once();
+      L->dense_ms = L->time_once();
+      L->check_status();
+      if (!chol_form || L->dense_ms < best) {
+        L->release_cholesky();
+      } else {
+        L->release_dense();
+        L->configure(L->jc, L->cfg2);
       }
     }
-    L->candidates = (int64_t)cand.size();
-    L->tuned_ms = best;
-    if (pick != std::make_pair(L->jc, L->cfg2)) L->configure(pick.first, pick.second);
     L->check_status();
     *out = L.release();
     return TCI_OK;
@@ -634,9 +870,10 @@ int tci_local_apply_host(tci_local* L, const double* c, double* sigma, int64_t n
 
 int tci_local_stats(const tci_local* L, double* out, int64_t len) {
   if (!L || !out || len < 9) return TCI_ERR_ARG;
-  const double v[9] = {L->flops,       L->lbytes,        L->dev_bytes, (double)L->jc, (double)L->cfg2,
-                       L->tuned_ms,    (double)L->candidates, L->last_ms, (double)L->blocks.size()};
-  std::memcpy(out, v, sizeof(v));
+  const double v[13] = {L->flops,       L->lbytes,           L->dev_bytes,   (double)L->jc,    (double)L->cfg2,
+                        L->tuned_ms,    (double)L->candidates, L->last_ms,   (double)L->blocks.size(),
+                        (double)L->form, L->dense_ms,        L->dense_flops, L->dense_bytes};
+  std::memcpy(out, v, sizeof(double) * (size_t)std::min<int64_t>(len, 13));
   return TCI_OK;
 }
 

@@ -20,6 +20,9 @@ import numpy as np
 from ._lib import check, lib, ptr
 
 PRECISIONS = {"fp64": 0, "tf32x3": 1}
+# all-external form: the faster of the two (timed at set-up), the pair-domain Cholesky form, or the dense
+# padded integral form (mixed precision only)
+FORMS = {"auto": 0, "cholesky": 1, "dense": 2}
 
 
 def _bind():
@@ -42,16 +45,17 @@ class LocalAllExternal:
     num_internal + num_external orbitals, rows pair = p(p+1)/2 + q (p >= q)."""
 
     def __init__(self, num_internal, num_external, chol, heads, dom_idx, total_len, device=0, precision="fp64",
-                 chunk_bytes=16e9, promote_every=128, autotune=True):
+                 chunk_bytes=16e9, promote_every=128, autotune=True, form="auto"):
         self._L = _bind()
         self.heads = np.ascontiguousarray(np.asarray(heads, dtype=np.int64).reshape(-1, 7))
         self.dom = np.ascontiguousarray(np.asarray(dom_idx, dtype=np.int64))
         chol = np.ascontiguousarray(chol, dtype=np.float64)
         self.n = int(total_len)
-        opts = np.array([PRECISIONS[precision], int(chunk_bytes), promote_every, 1 if autotune else 0], dtype=np.int64)
+        opts = np.array([PRECISIONS[precision], int(chunk_bytes), promote_every, 1 if autotune else 0, FORMS[form]],
+                        dtype=np.int64)
         h = C.c_void_p()
         check(self._L.tci_local_create(num_internal, num_external, ptr(chol), chol.shape[1], len(self.heads),
-                                       ptr(self.heads), ptr(self.dom), self.n, device, ptr(opts), 4, C.byref(h)))
+                                       ptr(self.heads), ptr(self.dom), self.n, device, ptr(opts), 5, C.byref(h)))
         self._h = h
 
     def apply(self, c: np.ndarray) -> np.ndarray:
@@ -65,11 +69,16 @@ class LocalAllExternal:
         check(self._L.tci_local_apply(self._h, C.c_void_p(c_ptr), C.c_void_p(s_ptr), self.n, C.c_void_p(stream or None)))
 
     def stats(self) -> dict:
-        out = np.zeros(9)
-        check(self._L.tci_local_stats(self._h, ptr(out), 9))
+        """form: "cholesky" or "dense" (the one applied); tuned_ms / dense_ms: the set-up timings of the two forms
+        (0 where a form was not timed); flops: the Cholesky form's 4 nchol sum n^3, dense_flops: the dense form's
+        2 np^2 per singlet-coupled and 2 nm^2 per triplet-coupled block; dense_w_bytes: its FP32 W tiles."""
+        out = np.zeros(13)
+        check(self._L.tci_local_stats(self._h, ptr(out), 13))
         keys = ["flops", "cholesky_bytes", "device_bytes", "chunk", "tile_cfg", "tuned_ms", "candidates", "last_ms",
-                "blocks"]
-        return dict(zip(keys, out.tolist()))
+                "blocks", "form", "dense_ms", "dense_flops", "dense_w_bytes"]
+        d = dict(zip(keys, out.tolist()))
+        d["form"] = "dense" if d["form"] == 1 else "cholesky"
+        return d
 
     def close(self):
         if getattr(self, "_h", None):
