@@ -88,6 +88,30 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def fp64_gemm_peak(device):
+    """cuBLAS FP64 GEMM throughput on this GPU (torch.matmul, 8192^3 float64, best of 5 after 2 warm-ups,
+    CUDA events): the compute roof of the FP64 form, which the measured peaks file does not carry."""
+    import torch
+
+    n = 8192
+    g = torch.Generator(device=device).manual_seed(0)
+    a = torch.randn(n, n, dtype=torch.float64, device=device, generator=g)
+    b = torch.randn(n, n, dtype=torch.float64, device=device, generator=g)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
 class ClockSampler:
     FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
 
@@ -382,10 +406,21 @@ def local_solve_measure(device, nchol=2400):
         sb.profile(False, davidson_phases=True)
         sb.davidson(1, TOL_RESIDUAL, TOL_ENERGY)
         phases = {k: round(v, 1) for k, v in sb.davidson_phase_times().items()}
+        # one sigma build with the plan's steps timed (the padded non-local plan; the pair-domain
+        # all-external term runs after it and is timed by the local leg)
+        sb.profile(True)
+        x = np.random.default_rng(3).standard_normal(sb.n)
+        t1 = time.perf_counter()
+        sb.sigma(x)
+        sigma_ms = 1e3 * (time.perf_counter() - t1)
+        steps, nb = sb.step_times()
+        sb.profile(False)
         sb.close()
+        top = sorted(steps, key=lambda kv: -kv[1])[:10]
         out[form] = {"energy": float(e[0]), "iterations": int(it), "ms_per_solve": a.elapsed_time(b),
                      "solves_per_s": 1e3 / a.elapsed_time(b), "init_s": init_s, "phase_ms": phases,
-                     "device_gb": st["device_bytes"] / 1e9}
+                     "device_gb": st["device_bytes"] / 1e9, "sigma_host_ms": round(sigma_ms, 1),
+                     "plan_step_ms": {k: round(v / max(nb, 1), 2) for k, v in top}}
     out["mixed_minus_fp64"] = out["tf32x3"]["energy"] - out["fp64"]["energy"]
     out["within_1uEh"] = abs(out["mixed_minus_fp64"]) <= 1e-6
     out["vs_fp64_form"] = out["fp64"]["ms_per_solve"] / out["tf32x3"]["ms_per_solve"]
@@ -665,13 +700,18 @@ def main():
         if "sb" in sig[f]:
             sig[f].pop("sb").close()
 
+    try:
+        fp64_peak = fp64_gemm_peak(dev) if "fp64" in forms else None
+    except Exception:  # the FP64 roof is a side figure
+        fp64_peak = None
+
     def sigma_summary(f, m):
         if "error" in m:
             return m
         st = m["stats"]
         if f == "fp64":
             t_dom = (m["prof"]["all-external"] + m["prof"].get("all-external split-k sum", 0.0)) / 1e3
-            kernel, bytes_ = "gemm_tiled_f64 split-k (all-external W+/W- product, FP64)", st["bytes_allext"]
+            kernel, bytes_ = "gemm_panel_f64 split-k (all-external W+/W- product, FP64 FMA)", st["bytes_allext"]
         else:
             t_dom = m["prof"]["all-external"] / 1e3
             kernel = "allext_tf32x3_kernel (tcgen05 kind::tf32, TMA, 3xTF32, FP64 promotion)"
@@ -688,6 +728,14 @@ def main():
              "step_ms": {k: round(v, 4) for k, v in sorted(m["prof"].items(), key=lambda kv: -kv[1])[:12]},
              "profiled_ms_per_build": 1e3 * m["t_prof"] / args.sigma_builds, "init_s": m["init_s"],
              "clocks": m["clk"].summary()}
+        if f == "fp64" and fp64_peak:
+            # a few dozen CI rows against W: 2 m flops per 8-byte W element, above the FP64 ridge (peak / HBM
+            # bandwidth) for m >= 32, so the FP64 compute rate bounds it
+            d["roofline_fp64"] = {"kernel": kernel, "bound": "fp64", "achieved": st["flops_allext"] / t_dom / 1e12,
+                                  "peak": fp64_peak, "unit": "TFLOP/s",
+                                  "frac": st["flops_allext"] / t_dom / 1e12 / fp64_peak,
+                                  "peak_kind": "cuBLAS FP64 GEMM measured in this run (8192^3)",
+                                  "flops": st["flops_allext"], "ms": 1e3 * t_dom}
         if "sigma_rel_err_vs_fp64" in m:
             d["sigma_rel_err_vs_fp64"] = m["sigma_rel_err_vs_fp64"]
         return d

@@ -68,6 +68,19 @@ typedef struct tci_operator {
 /* Thread-local message of the last failure (empty string if none). */
 int tci_last_error(char* buf, int64_t len);
 
+/* The tci_operator chol array from Cholesky records addressed through
+ * TigerCI's cholesky_data%mo_ind_inv (tiger_fortran/cholesky_structs.f90;
+ * read as cho_vectors(:, mo_ind_inv(pq)) with 0 meaning a zero vector, e.g.
+ * three_and_four_seg_mod_1.f90:504-512, and restored from CD_restart by
+ * cholesky_transform.f90:234-244): mo_ind_inv[pq] (pq = p(p+1)/2 + q,
+ * 0-based, num_orbitals(num_orbitals+1)/2 entries) is the 1-based record of
+ * pair pq in records (n_records x nchol, row major) or 0.  chol_out gets
+ * npair x nchol.  TCI_ERR_INPUT for an entry outside 0..n_records.  Where
+ * mo_ind_inv is the identity (the reference's transforms write it so) the
+ * records are the chol array as they are. */
+int tci_operator_from_records(int64_t num_orbitals, int64_t nchol, const int64_t* mo_ind_inv, const double* records,
+                              int64_t n_records, double* chol_out);
+
 /* ---- CSF space (host only; no GPU needed) --------------------------------
  * Replaces graph_driver (tiger_fortran/graph_mod.f90:48-99): distinct-row
  * table, tree search and CI-vector index vectors. */
@@ -234,6 +247,14 @@ int tci_davidson_phase_times(const tci_ctx* ctx, double* ms, int64_t len);
 int tci_step_times(const tci_ctx* ctx, double* ms, int64_t len, int64_t* nsteps, int64_t* nbuilds);
 int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len);
 void tci_destroy(tci_ctx* ctx);
+
+/* Self-test of the tensor-core kernels' abort path: a one-CTA kernel waits,
+ * with the kernels' own bounded mbarrier wait, on a barrier that nothing
+ * arrives at; after `polls` polls (0: the kernels' own limit) it records the
+ * stalled-operand code in its status word and returns, and the host reports
+ * TCI_ERR_TIMEOUT with *status_out the code and *ms_out (may be NULL) the
+ * kernel's duration.  The context stays usable. */
+int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out, double* ms_out);
 
 /* ---- Local pair domains: the all-external term over uneven domains -----
  * Replaces the local all-external loops (ext_3_4_seg_loops_vec_lmo_res_2,

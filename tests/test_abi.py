@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 import tigerci_b200 as T
 from tigerci_b200 import _lib
@@ -53,3 +54,29 @@ def test_plan_stats_on_cpu():
     st = T.Plan(deck, T.Operator(h, L)).stats()
     assert st["total_csfs"] == T.CsfSpace(deck).counts()["total_csfs"]
     assert st["flops_allext"] > 0 and st["n_steps"] > 5
+
+
+def test_operator_from_records_follows_mo_ind_inv():
+    """Records addressed through the reference's mo_ind_inv: a permutation with zero (skipped) pairs, the
+    identity, and an entry out of range."""
+    import tigerci_b200 as T
+
+    rng = np.random.default_rng(4)
+    n, nchol = 5, 7
+    npair = n * (n + 1) // 2
+    full = rng.standard_normal((npair, nchol))
+    keep = np.sort(rng.choice(npair, size=11, replace=False))
+    full[np.setdiff1d(np.arange(npair), keep)] = 0.0
+    order = rng.permutation(len(keep))
+    records = full[keep[order]]
+    inv = np.zeros(npair, dtype=np.int64)
+    inv[keep[order]] = np.arange(1, len(keep) + 1)
+    h = np.eye(n)
+    op = T.Operator.from_records(h, records, inv)
+    assert np.array_equal(op.chol, full)
+    ident = T.Operator.from_records(h, full, np.arange(1, npair + 1))
+    assert np.array_equal(ident.chol, full)
+    bad = inv.copy()
+    bad[3] = len(keep) + 1
+    with pytest.raises(Exception):
+        T.Operator.from_records(h, records, bad)

@@ -143,3 +143,34 @@ def test_mixed_roots_with_fp64_finish_match_fp64_closely(finish, need_gpu):
     eb, _, _ = b.davidson(2, 1e-7, 1e-11)
     b.check()
     assert np.abs(ea - eb).max() < 1e-8
+
+
+def test_bounded_wait_gives_up_and_the_context_stays_usable(need_gpu):
+    """The tensor-core kernels' abort path: a wait on an mbarrier that nothing arrives at gives up after its
+    polls, the kernel records the stalled-operand code and returns, the host reports TCI_ERR_TIMEOUT, and a
+    mixed sigma build on the same device afterwards is still correct.  Also reports how long the kernels'
+    own limit lets a stalled wait last."""
+    import ctypes as C
+
+    from tigerci_b200._lib import lib
+
+    L = lib()
+    st, ms = C.c_int64(0), C.c_double(0.0)
+    polls = 1 << 14
+    rc = L.tci_selftest_bounded_wait(0, polls, C.byref(st), C.byref(ms))
+    assert rc == 6 and st.value == 1  # TCI_ERR_TIMEOUT, ST_TIMEOUT_FULL
+    per_poll_ms = ms.value / polls
+    limit_s = per_poll_ms * (1 << 22) / 1e3  # the kernels' SPIN_LIMIT
+    print(f"bounded wait: {1e6 * per_poll_ms:.1f} ns per poll, kernels' limit ~{limit_s:.2f} s")
+    assert limit_s < 60.0
+    if limit_s < 5.0:
+        rc = L.tci_selftest_bounded_wait(0, 0, C.byref(st), C.byref(ms))
+        assert rc == 6 and st.value == 1
+    deck = product_deck(SMALL_CASES[0])
+    h, Lc = synthetic_operator(deck.num_orbitals, 10, seed=3)
+    a, b = _pair(deck, h, Lc)
+    v = random_civec(a.n, 5)
+    ref, got = a.sigma(v), b.sigma(v)
+    a.close()
+    b.close()
+    assert np.abs(got - ref).max() <= MIXED_2E_RTOL * np.abs(ref).max()

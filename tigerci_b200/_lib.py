@@ -61,6 +61,8 @@ EXPORTS = [
     "tci_step_times",
     "tci_step_name",
     "tci_destroy",
+    "tci_selftest_bounded_wait",
+    "tci_operator_from_records",
     "tci_integrals_create",
     "tci_integrals_info",
     "tci_integrals_one_electron",
@@ -161,6 +163,8 @@ def lib():
         L.tci_step_name.argtypes = [P, i64, C.c_char_p, i64]
         L.tci_destroy.argtypes = [P]
         L.tci_destroy.restype = None
+        L.tci_selftest_bounded_wait.argtypes = [i64, i64, P, P]
+        L.tci_operator_from_records.argtypes = [i64, i64, P, P, i64, P]
         L.tci_integrals_create.argtypes = [C.POINTER(TciMolecule), dbl, C.POINTER(P)]
         L.tci_integrals_info.argtypes = [P, P, i64]
         L.tci_integrals_one_electron.argtypes = [P, P, P, i64]

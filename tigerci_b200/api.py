@@ -131,6 +131,23 @@ class Operator:
     def nchol(self):
         return self.chol.shape[1]
 
+    @classmethod
+    def from_records(cls, h: np.ndarray, records: np.ndarray, mo_ind_inv, core_energy: float = 0.0) -> "Operator":
+        """The operator from Cholesky records addressed through the reference's mo_ind_inv (1-based record of
+        each pair, 0 for a zero vector), by tci_operator_from_records."""
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        n = h.shape[0]
+        rec = np.ascontiguousarray(records, dtype=np.float64)
+        if rec.ndim != 2:
+            raise ValueError("records must be n_records x nchol")
+        inv = np.ascontiguousarray(mo_ind_inv, dtype=np.int64)
+        if inv.shape != (n * (n + 1) // 2,):
+            raise ValueError("mo_ind_inv must have n(n+1)/2 entries")
+        chol = np.empty((n * (n + 1) // 2, rec.shape[1]))
+        check(lib().tci_operator_from_records(n, rec.shape[1], ptr(inv), ptr(rec) if rec.size else None,
+                                              rec.shape[0], ptr(chol)))
+        return cls(h, chol, core_energy)
+
     def c_struct(self) -> TciOperator:
         return TciOperator(ptr(self.h), ptr(self.chol), self.nchol, self.core_energy)
 

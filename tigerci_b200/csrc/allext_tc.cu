@@ -439,6 +439,27 @@ __global__ void split_u(const double* __restrict__ U, int m, int np, long long l
   }
 }
 
+// Self-test of the abort path: one CTA waits, with the kernels' own bounded wait, on an mbarrier that
+// nothing arrives at, records the code the kernels record for a stalled operand (ST_TIMEOUT_FULL) and
+// returns; the other warps wait for the abort flag as the kernels' consumers do.  polls: the wait's limit.
+__global__ void bounded_wait_selftest(int* __restrict__ status, long long polls) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (!mbar_wait(&bar, 0, polls)) {
+      atomicCAS(status, 0, ST_TIMEOUT_FULL);
+      *(volatile int*)&abort_flag = 1;
+    }
+  }
+  __syncthreads();
+}
+
 }  // namespace tci_tc
 
 // ---------------------------------------------------------------------------
@@ -511,6 +532,12 @@ cudaError_t convert_w_from_x(const double* x, int64_t n, bool plus, float* w32, 
                                                     (long long)w32_floats(np));
   return cudaGetLastError();
 }
+
+cudaError_t bounded_wait_selftest(int64_t polls, int* status, cudaStream_t st) {
+  tci_tc::bounded_wait_selftest<<<1, 128, 0, st>>>(status, (long long)polls);
+  return cudaGetLastError();
+}
+int64_t spin_limit() { return tci_tcx::SPIN_LIMIT; }
 
 int64_t u2_floats(int64_t m, int64_t np) { return 2 * padded_rows(m) * padded_ld(np); }
 

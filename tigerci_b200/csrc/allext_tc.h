@@ -30,6 +30,10 @@ cudaError_t convert_w_from_x(const double* x, int64_t n, bool plus, float* w32, 
 cudaError_t split_u(const double* u, int64_t m, int64_t np, float* u2, cudaStream_t st);
 bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t m, double* y, int* status,
              int64_t kblock, std::string& err);
+// Self-test of the bounded-wait abort path: a kernel whose wait (polls polls, the kernels' own helper)
+// can never complete records its timeout code in *status and returns.
+cudaError_t bounded_wait_selftest(int64_t polls, int* status, cudaStream_t st);
+int64_t spin_limit();  // the polls of the kernels' bounded waits
 // Both products in one launch (either may be null; they must share the status
 // word and promotion block).  Persistent: at most one CTA per SM.
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);

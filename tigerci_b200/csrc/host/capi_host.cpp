@@ -116,6 +116,29 @@ int tci_last_error(char* buf, int64_t len) {
   return TCI_OK;
 }
 
+int tci_operator_from_records(int64_t num_orbitals, int64_t nchol, const int64_t* mo_ind_inv, const double* records,
+                              int64_t n_records, double* chol_out) {
+  if (num_orbitals <= 0 || nchol <= 0 || n_records < 0 || !mo_ind_inv || !chol_out || (n_records > 0 && !records)) {
+    set_error("tci_operator_from_records: bad argument");
+    return TCI_ERR_ARG;
+  }
+  const int64_t npair = num_orbitals * (num_orbitals + 1) / 2;
+  for (int64_t pq = 0; pq < npair; ++pq)
+    if (mo_ind_inv[pq] < 0 || mo_ind_inv[pq] > n_records) {
+      set_error("mo_ind_inv entry " + std::to_string(pq) + " is outside 0.." + std::to_string(n_records));
+      return TCI_ERR_INPUT;
+    }
+  for (int64_t pq = 0; pq < npair; ++pq) {
+    double* dst = chol_out + pq * nchol;
+    const int64_t r = mo_ind_inv[pq];
+    if (r == 0)
+      std::memset(dst, 0, sizeof(double) * (size_t)nchol);
+    else
+      std::memcpy(dst, records + (r - 1) * nchol, sizeof(double) * (size_t)nchol);
+  }
+  return TCI_OK;
+}
+
 int tci_space_create(const tci_deck* deck, tci_space** out) {
   if (!out) return TCI_ERR_ARG;
   *out = nullptr;

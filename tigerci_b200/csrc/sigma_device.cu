@@ -3349,4 +3349,48 @@ int tci_step_name(const tci_ctx* ctx, int64_t i, char* buf, int64_t len) {
 
 void tci_destroy(tci_ctx* ctx) { delete ctx; }
 
+int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out, double* ms_out) {
+  if (!status_out || polls < 0) return TCI_ERR_ARG;
+  int* st = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&]() {
+    if (s) cudaStreamSynchronize(s);
+    if (st) cudaFree(st);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+  };
+  try {
+    int ndev = 0;
+    TCI_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) throw Error(TCI_ERR_CUDA, "requested device is not available");
+    TCI_CUDA(cudaSetDevice((int)device));
+    TCI_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    TCI_CUDA(cudaEventCreate(&e0));
+    TCI_CUDA(cudaEventCreate(&e1));
+    TCI_CUDA(cudaMalloc(&st, sizeof(int)));
+    TCI_CUDA(cudaMemsetAsync(st, 0, sizeof(int), s));
+    TCI_CUDA(cudaEventRecord(e0, s));
+    TCI_CUDA(tci_tc_host::bounded_wait_selftest(polls ? polls : tci_tc_host::spin_limit(), st, s));
+    TCI_CUDA(cudaEventRecord(e1, s));
+    int h = 0;
+    TCI_CUDA(cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TCI_CUDA(cudaStreamSynchronize(s));
+    float ms = 0;
+    TCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *status_out = h;
+    if (ms_out) *ms_out = ms;
+    cleanup();
+    if (h != 0) {
+      set_error("self-test: the bounded wait gave up (code " + std::to_string(h) + ")");
+      return TCI_ERR_TIMEOUT;
+    }
+    return TCI_OK;
+  } catch (...) {
+    cleanup();
+    return guard_status(std::current_exception());
+  }
+}
+
 }  // extern "C"

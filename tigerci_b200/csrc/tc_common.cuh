@@ -24,10 +24,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// Wait for the phase with the given parity; false when the wait gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Wait for the phase with the given parity; false when the wait gave up after
+// `limit` polls (the kernels use SPIN_LIMIT).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = SPIN_LIMIT) {
   const uint32_t a = smem_u32(bar);
-  for (long long i = 0; i < SPIN_LIMIT; ++i) {
+  for (long long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
