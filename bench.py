@@ -80,6 +80,19 @@ def deck_and_operator(molecular=False):
     return deck, T.Operator(h, L)
 
 
+def _np_default(o):
+    if isinstance(o, np.generic):
+        return o.item()
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError(f"{type(o).__name__} is not JSON serializable")
+
+
+def dumps(obj) -> str:
+    """json.dumps that takes numpy scalars and arrays."""
+    return json.dumps(obj, default=_np_default)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -237,7 +250,7 @@ def run_reference(args, rank, world):
                            "p99": 1e3 * float(np.percentile(r["times"], 99)), "what": "per CPU sigma build"},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["cores"], "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(dumps(line), flush=True)
 
 
 def serve_measure(n_requests, slots, device, serial_per_n=2, planners=4):
@@ -618,19 +631,19 @@ def main():
 
     if args.serve_only:
         if rank == 0:
-            print(json.dumps({"serving": serve_measure(args.serve_requests, args.serve_slots, local, planners=args.serve_planners)}), flush=True)
+            print(dumps({"serving": serve_measure(args.serve_requests, args.serve_slots, local, planners=args.serve_planners)}), flush=True)
         return
     if args.local_solve_only:
         if rank == 0:
-            print(json.dumps({"local_solve": local_solve_measure(local)}), flush=True)
+            print(dumps({"local_solve": local_solve_measure(local)}), flush=True)
         return
     if args.octane_only:
         if rank == 0:
-            print(json.dumps({"octane_c3": octane_measure(local)}), flush=True)
+            print(dumps({"octane_c3": octane_measure(local)}), flush=True)
         return
     if args.local_only:
         if rank == 0:
-            print(json.dumps({"local_pairs": local_measure(args.local_pairs, local, hbm, bf16, nchol=args.local_nchol,
+            print(dumps({"local_pairs": local_measure(args.local_pairs, local, hbm, bf16, nchol=args.local_nchol,
                                                     forms=tuple(f for f in args.local_forms.split(",") if f))}), flush=True)
         return
 
@@ -744,7 +757,7 @@ def main():
     n_csf = next((m["n"] for m in sig.values() if "n" in m), None)
     if args.sigma_only:
         if rank == 0:
-            print(json.dumps({"sigma_only": True, "config": {"workload": WORKLOAD, "total_csfs": n_csf},
+            print(dumps({"sigma_only": True, "config": {"workload": WORKLOAD, "total_csfs": n_csf},
                               "sigma": sigma_lines}), flush=True)
         if dist:
             dist.barrier()
@@ -925,7 +938,7 @@ def main():
             except Exception as exc:
                 line["molecular_c1"]["oracle"] = {"error": str(exc)[:300]}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -255,6 +255,12 @@ void tci_destroy(tci_ctx* ctx);
  * TCI_ERR_TIMEOUT with *status_out the code and *ms_out (may be NULL) the
  * kernel's duration.  The context stays usable. */
 int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out, double* ms_out);
+/* Instruction rate of tcgen05.mma kind::tf32 (M = 128, N = n: 16..256 in
+ * steps of 16, K = 8) on this device: one thread per SM issues iters x nacc
+ * MMAs back to back into nacc independent TMEM accumulators (nacc x n <=
+ * 512 columns) and commits once; *cycles_per_mma = the slowest SM's clock64
+ * span / (iters x nacc), from the second of two launches. */
+int tci_selftest_mma_rate(int64_t device, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma);
 
 /* ---- Local pair domains: the all-external term over uneven domains -----
  * Replaces the local all-external loops (ext_3_4_seg_loops_vec_lmo_res_2,

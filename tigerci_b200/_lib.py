@@ -62,6 +62,7 @@ EXPORTS = [
     "tci_step_name",
     "tci_destroy",
     "tci_selftest_bounded_wait",
+    "tci_selftest_mma_rate",
     "tci_operator_from_records",
     "tci_integrals_create",
     "tci_integrals_info",
@@ -164,6 +165,7 @@ def lib():
         L.tci_destroy.argtypes = [P]
         L.tci_destroy.restype = None
         L.tci_selftest_bounded_wait.argtypes = [i64, i64, P, P]
+        L.tci_selftest_mma_rate.argtypes = [i64, i64, i64, i64, P]
         L.tci_operator_from_records.argtypes = [i64, i64, P, P, i64, P]
         L.tci_integrals_create.argtypes = [C.POINTER(TciMolecule), dbl, C.POINTER(P)]
         L.tci_integrals_info.argtypes = [P, P, i64]

@@ -30,12 +30,16 @@
 // Work split (persistent, stream-K): one launch covers both operators (W+
 // with the singlet blocks, W- with the triplet blocks).  Their k-steps form
 // one linear sequence (operator, CI-block group, 128-row panel, k); each CTA
-// (one per SM) takes an equal contiguous range of it, so the pipeline runs
-// without refills from panel to panel and every SM streams the same number of
-// W bytes.  A range is at least one panel long, so a panel is shared by at
-// most two CTAs: both add their FP64 partial sums into the zeroed output, and
-// a + b rounds the same in either order, so the result does not depend on
-// which CTA finishes first.
+// (one per SM) takes a contiguous range of it, so the pipeline runs without
+// refills from panel to panel.  The CTAs are shared between the operators in
+// proportion to their k-steps; with several CI-block groups the CTAs of an
+// operator are dealt round the groups and the t-th CTA of every group takes
+// the same share of its group's (panel, k) sequence, so the groups stream
+// the same W tiles side by side and a tile leaves HBM once (cta_range).  A
+// range is at least one panel long, so a panel is shared by at most two
+// CTAs: both add their FP64 partial sums into the zeroed output, and a + b
+// rounds the same in either order, so the result does not depend on which
+// CTA finishes first.
 //
 // Warp roles (448 threads): warps 0-3 and 10-13 epilogue (two per TMEM lane
 // quadrant), warps 4-7 low parts of the W tile, warp 8 producer (bulk copy +
@@ -136,13 +140,55 @@ __device__ __forceinline__ Segment segment_at(const Product& p0, const Product& 
   return g;
 }
 
+// The CTA's range of the linear k-step sequence.  The CTAs are shared between the two operators in
+// proportion to their k-steps; within an operator CTA i works on CI-block group i mod G (G groups), and the
+// n_g CTAs of group g split that group's (panel, k) sequence into n_g equal shares, the t-th CTA of every
+// group taking the t-th share.  CTAs with the same t stream the same W tiles at about the same time, so a
+// tile comes from HBM once and from L2 for the other groups.  A share is at least one panel long (n_g is
+// capped at the panel count; CTAs past it stay idle), so a panel is still shared by at most two CTAs.  With
+// fewer CTAs than groups the operator's sequence is split into equal contiguous ranges.
+__device__ __forceinline__ void cta_range(const Product& p0, const Product& p1, long long& begin, long long& end) {
+  const int C = (int)gridDim.x, b = (int)blockIdx.x;
+  const long long total = p0.units + p1.units;
+  if (C == 1) {
+    begin = 0;
+    end = total;
+    return;
+  }
+  int c0 = C;  // CTAs of operator 0
+  if (p0.units == 0) {
+    c0 = 0;
+  } else if (p1.units > 0) {
+    c0 = (int)llround((double)C * (double)p0.units / (double)total);
+    c0 = c0 < 1 ? 1 : (c0 > C - 1 ? C - 1 : c0);
+  }
+  const bool second = b >= c0;
+  const Product& P = second ? p1 : p0;
+  const long long base = second ? p0.units : 0;
+  const int i = second ? b - c0 : b, nc = second ? C - c0 : c0;
+  if (nc < P.groups) {
+    begin = base + P.units * i / nc;
+    end = base + P.units * (i + 1) / nc;
+    return;
+  }
+  const int g = i % P.groups, t = i / P.groups;
+  int ng = nc / P.groups + (g < nc % P.groups ? 1 : 0);
+  if (ng > P.panels) ng = P.panels;
+  const long long per = (long long)P.panels * P.nk, gb = base + (long long)g * per;
+  if (t >= ng) {
+    begin = end = gb;
+    return;
+  }
+  begin = gb + per * t / ng;
+  end = gb + per * (t + 1) / ng;
+}
+
 __global__ void __launch_bounds__(NTHREADS, 1)
     allext_tf32x3_kernel(const __grid_constant__ CUtensorMap u_map0, const __grid_constant__ CUtensorMap u_map1,
                          Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
   const int KB_PER_BLOCK = kb_per_block;
-  const long long total = p0.units + p1.units;
-  const long long begin = total * (long long)blockIdx.x / gridDim.x;
-  const long long end = total * (long long)(blockIdx.x + 1) / gridDim.x;
+  long long begin, end;
+  cta_range(p0, p1, begin, end);
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
@@ -460,6 +506,51 @@ __global__ void bounded_wait_selftest(int* __restrict__ status, long long polls)
   __syncthreads();
 }
 
+// Self-test of the MMA instruction rate: one thread per CTA issues iters x nacc kind::tf32 MMAs (M = 128,
+// N = n, K = 8, operands zero in shared memory) back to back into nacc independent TMEM accumulators of n
+// columns, commits once and waits (bounded); cycles[cta] = clock64 span.  One CTA per SM (the shared memory
+// request keeps a second one off the SM, so the 512-column TMEM allocation never waits on another CTA).
+constexpr int RATE_SMEM = 120 * 1024;
+__global__ void __launch_bounds__(128, 1) mma_rate_selftest(int n, int nacc, int iters, long long* __restrict__ cycles,
+                                                           int* __restrict__ status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* A = base;          // 128 rows x 128 bytes
+  uint8_t* B = base + 16384;  // 256 rows x 128 bytes
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + 16384 + 32768);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
+  for (int i = threadIdx.x; i < (16384 + 32768) / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(base)[i] = 0u;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *slot;
+  if (threadIdx.x == 0) {
+    const uint64_t a = smem_desc_sw128(A), b = smem_desc_sw128(B);
+    const uint32_t id = idesc_tf32(128, n);
+    const long long t0 = clock64();
+    for (int i = 0; i < iters; ++i)
+      for (int q = 0; q < nacc; ++q) mma_tf32(tmem + (uint32_t)(q * n), a, b, id, i > 0 ? 1u : 0u);
+    mma_commit(bar);
+    bool ok = mbar_wait(bar, 0);
+    if (!ok) ok = mbar_wait(bar, 0);
+    cycles[blockIdx.x] = clock64() - t0;
+    if (!ok) atomicCAS(status, 0, ST_TIMEOUT_D);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
 }  // namespace tci_tc
 
 // ---------------------------------------------------------------------------
@@ -538,6 +629,19 @@ cudaError_t bounded_wait_selftest(int64_t polls, int* status, cudaStream_t st) {
   return cudaGetLastError();
 }
 int64_t spin_limit() { return tci_tcx::SPIN_LIMIT; }
+
+cudaError_t mma_rate_selftest(int64_t n, int64_t nacc, int64_t iters, int grid, long long* cycles, int* status,
+                              cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tci_tc::mma_rate_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tci_tc::RATE_SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  tci_tc::mma_rate_selftest<<<grid, 128, tci_tc::RATE_SMEM, st>>>((int)n, (int)nacc, (int)iters, cycles, status);
+  return cudaGetLastError();
+}
 
 int64_t u2_floats(int64_t m, int64_t np) { return 2 * padded_rows(m) * padded_ld(np); }
 

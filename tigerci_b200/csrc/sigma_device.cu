@@ -3393,4 +3393,46 @@ int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out
   }
 }
 
+int tci_selftest_mma_rate(int64_t device, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma) {
+  if (!cycles_per_mma || n < 16 || n > 256 || n % 16 || nacc < 1 || nacc * n > 512 || iters < 1 || iters > (1 << 20))
+    return TCI_ERR_ARG;
+  int* st = nullptr;
+  long long* cyc = nullptr;
+  cudaStream_t s = nullptr;
+  auto cleanup = [&]() {
+    if (s) cudaStreamSynchronize(s);
+    if (st) cudaFree(st);
+    if (cyc) cudaFree(cyc);
+    if (s) cudaStreamDestroy(s);
+  };
+  try {
+    int ndev = 0;
+    TCI_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) throw Error(TCI_ERR_CUDA, "requested device is not available");
+    TCI_CUDA(cudaSetDevice((int)device));
+    const int grid = sm_count();
+    TCI_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    TCI_CUDA(cudaMalloc(&st, sizeof(int)));
+    TCI_CUDA(cudaMalloc(&cyc, sizeof(long long) * (size_t)grid));
+    TCI_CUDA(cudaMemsetAsync(st, 0, sizeof(int), s));
+    std::vector<long long> h((size_t)grid);
+    for (int rep = 0; rep < 2; ++rep)  // the first launch warms up; the second is read
+      TCI_CUDA(tci_tc_host::mma_rate_selftest(n, nacc, iters, grid, cyc, st, s));
+    int hs = 0;
+    TCI_CUDA(cudaMemcpyAsync(h.data(), cyc, sizeof(long long) * (size_t)grid, cudaMemcpyDeviceToHost, s));
+    TCI_CUDA(cudaMemcpyAsync(&hs, st, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TCI_CUDA(cudaStreamSynchronize(s));
+    cleanup();
+    if (hs != 0) {
+      set_error("MMA rate self-test: the commit's bounded wait gave up");
+      return TCI_ERR_TIMEOUT;
+    }
+    *cycles_per_mma = (double)*std::max_element(h.begin(), h.end()) / (double)(iters * nacc);
+    return TCI_OK;
+  } catch (...) {
+    cleanup();
+    return guard_status(std::current_exception());
+  }
+}
+
 }  // extern "C"
