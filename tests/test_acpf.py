@@ -92,3 +92,24 @@ def test_device_acpf_matches_the_printed_energy(need_gpu, precision, tol):
     assert abs(e_ref + en - fx["reference_energy"]) < 1e-8
     assert abs(e[0] + en - fx["acpf_root1"]) < tol
     assert abs(np.linalg.norm(v[0]) - 1.0) < 1e-12
+
+
+@pytest.mark.gpu
+def test_water_mr_acpf_converges_in_both_forms(need_gpu):
+    """MR-ACPF on H2O / cc-pVDZ with CAS(4,4) references through the molecular front end: the generalized
+    solve converges on the reference's residual in both forms, the mixed root is within 1 uEh of the FP64
+    one, and the ACPF energy lies below the MRCI energy of the same space (its size-extensivity shift)."""
+    from tigerci_b200 import molecule as M
+
+    deck, op, _ = M.water_c1()
+    out = {}
+    for f in ("fp64", "tf32x3"):
+        sb = T.SigmaBuilder(deck, op, device=0, precision=f)
+        e, _, it, e_ref = sb.acpf(1, flag=1, tol_residual=1e-6, tol_energy=1e-10)
+        assert sb.stats()["converged"] == 1.0, (f, it)
+        out[f] = float(e[0])
+        if f == "fp64":
+            ci, _, _ = sb.davidson(1, 1e-6, 1e-10)
+            assert out[f] < float(ci[0]) < float(e_ref)
+        sb.close()
+    assert abs(out["tf32x3"] - out["fp64"]) <= 1e-6

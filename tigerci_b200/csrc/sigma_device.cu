@@ -1215,6 +1215,7 @@ struct tci_ctx {
   float* u2t = nullptr;                 // split triplet CI blocks
   int* tc_status = nullptr;
   tci_tc_host::AllextTc tc_sing, tc_trip;
+  int tc_prefetch = 8;  // L2 lead of the all-external launch (timed at set-up)
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
   cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
@@ -1948,7 +1949,8 @@ struct tci_ctx {
       TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_us, plan.n_sing, plan.np, u2s, stream));
     if (has_trip())
       TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, u2t, stream));
-    TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream));
+    TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream,
+                                 tc_prefetch));
   }
 
   // X (M x M, FP64) = A A^T with A = M rows of K values in BUF_T0, on the TMA-fed 3xTF32 kernel (set-up).
@@ -2140,6 +2142,18 @@ struct tci_ctx {
     if (plan.n_trip > 0 && nm > 0 &&
         !tci_tc_host::prepare(tc_trip, w32m, nm, u2t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
+    if (allext && (has_sing() || has_trip())) {
+      // the L2 lead of the all-external launch, timed on zeroed U rows (the outputs are scratch until the
+      // first sigma build)
+      if (u2s) TCI_CUDA(cudaMemsetAsync(u2s, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(std::max<i64>(1, plan.n_sing), np), stream));
+      if (u2t) TCI_CUDA(cudaMemsetAsync(u2t, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(plan.n_trip, nm), stream));
+      tc_prefetch = tci_tc_host::tune_prefetch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream,
+                                               nullptr);
+      TCI_CUDA(cudaStreamSynchronize(stream));
+      int h = 0;
+      TCI_CUDA(cudaMemcpy(&h, tc_status, sizeof(int), cudaMemcpyDeviceToHost));
+      if (h != 0) throw Error(TCI_ERR_TIMEOUT, "all-external kernel: a bounded wait gave up during set-up");
+    }
     if (refine != 1 && buf[BUF_W]) {  // the FP64 W is only needed for the plain-FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
       TCI_CUDA(dev_free(buf[BUF_W], stream));
