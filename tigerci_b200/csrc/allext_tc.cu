@@ -63,21 +63,20 @@ using namespace tci_tcx;
 constexpr int BM = 128;      // W rows per panel
 constexpr int BN = 64;       // largest CI-block group (2 BN interleaved U rows = the MMA's M)
 constexpr int BK = 32;       // fp32 k elements per stage (one 128-byte swizzle row)
-constexpr int MAX_STAGES = 8;  // the stage count is a launch parameter: as many stages as shared memory holds
+constexpr int STAGES = 4;
+constexpr int PREFETCH = 8;  // W tiles requested into L2 ahead of the ring
 constexpr int TILE_FLOATS = BM * BK;  // one W tile
 constexpr int MMA_N = 2 * BM;         // W rows, then their low parts
 // The FP64 promotion block (k elements summed in TMEM before the FP64 add) is
 // a launch parameter: the tensor core's FP32 accumulation error grows with it.
 constexpr int W_BYTES = BM * BK * 4;        // 16 KB
 constexpr int B_BYTES = 2 * W_BYTES;        // W tile (its own high part) + low parts
-// A stage is [U rows: ubytes][W tile][W low parts].  ubytes = 2 bn 128 bytes for the largest group of the
-// launch (bn a multiple of 4, so 1024-byte aligned); the MMA reads M = 128 rows of A whatever bn is, and the
-// rows past 2 bn fall into the stage's own W tile (valid shared memory; their TMEM lanes are not read).
-constexpr int SMEM_LIMIT = 227 * 1024;
+constexpr int A_BYTES = 2 * BN * BK * 4;    // 16 KB: interleaved U rows (room for the largest group)
+constexpr int STAGE_BYTES = B_BYTES + A_BYTES;
 constexpr int TMEM_COLS = 2 * MMA_N;        // two accumulator buffers
 constexpr int NTHREADS = 448;
 constexpr int EPI_WARPS = 8;  // warps 0-3 and 10-13: two per TMEM lane quadrant, each half of the panel
-constexpr int SMEM_TAIL = 1024 + 256;  // alignment slack + barriers, TMEM slot and abort flag
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
   asm volatile(
@@ -186,19 +185,16 @@ __device__ __forceinline__ void cta_range(const Product& p0, const Product& p1, 
 
 __global__ void __launch_bounds__(NTHREADS, 1)
     allext_tf32x3_kernel(const __grid_constant__ CUtensorMap u_map0, const __grid_constant__ CUtensorMap u_map1,
-                         Product p0, Product p1, int* __restrict__ status, int kb_per_block, int STAGES,
-                         int ubytes, int PREFETCH) {
-  // STAGES (<= MAX_STAGES) stages of ubytes + B_BYTES; PREFETCH W tiles requested into L2 ahead of the ring
+                         Product p0, Product p1, int* __restrict__ status, int kb_per_block) {
   const int KB_PER_BLOCK = kb_per_block;
-  const int STAGE_BYTES = ubytes + B_BYTES;
   long long begin, end;
   cta_range(p0, p1, begin, end);
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
-  uint64_t* conv = full + MAX_STAGES;
-  uint64_t* empty = conv + MAX_STAGES;
-  uint64_t* dfull = empty + MAX_STAGES;  // 2
+  uint64_t* conv = full + STAGES;
+  uint64_t* empty = conv + STAGES;
+  uint64_t* dfull = empty + STAGES;   // 2
   uint64_t* dempty = dfull + 2;       // 2
   uint64_t* mma_done = dempty + 2;    // 1: drain of the MMAs in flight after an abort
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
@@ -256,8 +252,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (k + PREFETCH < g.k1) bulk_prefetch_l2(wt + (long long)(k + PREFETCH) * TILE_FLOATS, W_BYTES);
           uint8_t* st = base + s * STAGE_BYTES;
           mbar_expect_tx(&full[s], bytes);
-          bulk_load(st + ubytes, wt + (long long)k * TILE_FLOATS, W_BYTES, &full[s]);
-          tma_load_2d(st, u_map, &full[s], k * BK, g.group * 2 * bn);
+          bulk_load(st, wt + (long long)k * TILE_FLOATS, W_BYTES, &full[s]);
+          tma_load_2d(st + B_BYTES, u_map, &full[s], k * BK, g.group * 2 * bn);
           last = step;
         }
         pos += g.k1 - g.k0;
@@ -279,8 +275,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fail(ST_TIMEOUT_FULL);
         break;
       }
-      const uint32_t* w = reinterpret_cast<const uint32_t*>(base + s * STAGE_BYTES + ubytes);
-      float* wlo = reinterpret_cast<float*>(base + s * STAGE_BYTES + ubytes + W_BYTES);
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(base + s * STAGE_BYTES);
+      float* wlo = reinterpret_cast<float*>(base + s * STAGE_BYTES + W_BYTES);
       // a warp per 128-byte row, lane l holds element l (conflict free); row r + BM has the same
       // swizzle permutation as row r, so the low part keeps the tile's layout.  Eight rows per
       // batch: their loads are issued before any store.
@@ -322,7 +318,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           const uint32_t d = tmem + (uint32_t)(buf * MMA_N);
 #pragma unroll
           for (int kk = 0; kk < BK / 8; ++kk)  // 8 tf32 = 32 bytes of every row per MMA
-            mma_tf32(d, smem_desc_sw128(st + kk * 32), smem_desc_sw128(st + ubytes + kk * 32), idesc,
+            mma_tf32(d, smem_desc_sw128(st + B_BYTES + kk * 32), smem_desc_sw128(st + kk * 32), idesc,
                      (first && kk == 0) ? 0u : 1u);
           mma_commit(&empty[s]);
           if ((kin % KB_PER_BLOCK) == KB_PER_BLOCK - 1 || k == g.k1 - 1) {
@@ -681,7 +677,7 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(tci_tc::allext_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tci_tc::SMEM_LIMIT) != cudaSuccess) {
+                             tci_tc::SMEM_BYTES) != cudaSuccess) {
       err = "cannot raise the dynamic shared memory limit";
       return false;
     }
@@ -690,15 +686,7 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t
   return true;
 }
 
-int stages_for(const AllextTc* a, const AllextTc* b) {
-  int bn = 0;
-  for (const AllextTc* t : {a, b})
-    if (t) bn = std::max<int>(bn, (int)t->bn);
-  const int ubytes = (bn + 3) / 4 * 4 * 2 * tci_tc::BK * 4;
-  return std::min(tci_tc::MAX_STAGES, (tci_tc::SMEM_LIMIT - tci_tc::SMEM_TAIL) / (ubytes + tci_tc::B_BYTES));
-}
-
-cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st, int prefetch, int stages) {
+cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   if (!a && !b) return cudaSuccess;
   if (!a) std::swap(a, b);
   auto product = [](const AllextTc* t) {
@@ -727,47 +715,9 @@ cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st, int pr
   if (e == cudaSuccess && b) e = cudaMemsetAsync(b->y, 0, sizeof(double) * (size_t)(b->m * b->np), st);
   if (e != cudaSuccess) return e;
   const AllextTc* c = b ? b : a;  // map of the second product (unused when there is none)
-  // stage ring: the U rows of the largest group (bn rounded up to a multiple of 4) + the W tile and its low
-  // parts, as many stages as fit (or `stages`, at least 2)
-  const int bn = std::max(p0.bn, p1.bn);
-  const int ubytes = (bn + 3) / 4 * 4 * 2 * tci_tc::BK * 4;
-  const int most = stages_for(a, b);
-  const int ns = stages > 0 ? std::max(2, std::min(stages, most)) : most;
-  const int smem = ns * (ubytes + tci_tc::B_BYTES) + tci_tc::SMEM_TAIL;
-  tci_tc::allext_tf32x3_kernel<<<(unsigned)grid, tci_tc::NTHREADS, smem, st>>>(
-      a->u2, c->u2, p0, p1, a->status, (int)(a->kblock / tci_tc::BK), ns, ubytes, std::max(1, prefetch));
+  tci_tc::allext_tf32x3_kernel<<<(unsigned)grid, tci_tc::NTHREADS, tci_tc::SMEM_BYTES, st>>>(
+      a->u2, c->u2, p0, p1, a->status, (int)(a->kblock / tci_tc::BK));
   return cudaGetLastError();
-}
-
-// Times the launch of a and b for each L2 lead in {8, 16, 32} tiles on the deepest ring (one warm-up and one
-// timed launch each, on st) and returns the fastest lead; *ms (may be null) gets its time.  The launches
-// overwrite the products' outputs.
-int tune_prefetch(const AllextTc* a, const AllextTc* b, cudaStream_t st, float* ms) {
-  int best = 8;
-  float best_ms = 3.4e38f;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
-    if (e0) cudaEventDestroy(e0);
-    cudaGetLastError();
-    return best;
-  }
-  for (int pf : {8, 16, 32}) {
-    if (launch(a, b, st, pf) != cudaSuccess) break;
-    cudaEventRecord(e0, st);
-    if (launch(a, b, st, pf) != cudaSuccess) break;
-    cudaEventRecord(e1, st);
-    if (cudaEventSynchronize(e1) != cudaSuccess) break;
-    float t = 0.0f;
-    cudaEventElapsedTime(&t, e0, e1);
-    if (t < best_ms) {
-      best_ms = t;
-      best = pf;
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (ms) *ms = best_ms;
-  return best;
 }
 
 }  // namespace tci_tc_host

@@ -39,14 +39,7 @@ int64_t spin_limit();  // the polls of the kernels' bounded waits
 cudaError_t mma_rate_selftest(int64_t n, int64_t nacc, int64_t iters, int grid, long long* cycles, int* status,
                               cudaStream_t st);
 // Both products in one launch (either may be null; they must share the status
-// word and promotion block).  Persistent: at most one CTA per SM.  prefetch: W
-// tiles requested into L2 ahead of the stage ring; stages: the ring's depth
-// (0: as many as shared memory holds for the launch's largest CI-block group).
-cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st, int prefetch = 8, int stages = 0);
-// The deepest stage ring of a launch of a and b (either may be null).
-int stages_for(const AllextTc* a, const AllextTc* b);
-// The fastest L2 lead of {8, 16, 32} for a launch of a and b, timed on st (the outputs are overwritten);
-// *ms (may be null) gets its launch time.
-int tune_prefetch(const AllextTc* a, const AllextTc* b, cudaStream_t st, float* ms);
+// word and promotion block).  Persistent: at most one CTA per SM.
+cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);
 
 }  // namespace tci_tc_host

@@ -24,6 +24,10 @@ struct LocalSetup {
   std::vector<long long> map;
   std::vector<int64_t> heads7, dom_idx;
   std::vector<double> xdiag;
+  // per N-2 head of the non-local plan (its dheads order): the slice of dh_dom holding the head's local
+  // domain (sorted externals); length 0 for a head without local CSFs
+  std::vector<int64_t> dh_off, dh_len;
+  std::vector<int> dh_dom;
 };
 void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls);
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,

@@ -307,7 +307,6 @@ struct tci_local {
   double *yp = nullptr, *ym = nullptr;
   tci_tc_host::AllextTc tcp, tcm;
   double dense_flops = 0, dense_ms = 0, dense_bytes = 0;
-  int dense_prefetch = 8;  // L2 lead of the all-external launch (timed at set-up)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -478,12 +477,6 @@ struct tci_local {
       ym = alloc((size_t)(ntrip_d * nm_d));
       if (!tci_tc_host::prepare(tcm, w32m, nm_d, u2m, ntrip_d, ym, status, kblock, err)) throw Error(TCI_ERR_CUDA, err);
     }
-    // the L2 lead, timed on zeroed U rows
-    if (u2p) LCUDA(cudaMemsetAsync(u2p, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(nsing_d, np_d), stream));
-    if (u2m) LCUDA(cudaMemsetAsync(u2m, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(ntrip_d, nm_d), stream));
-    dense_prefetch = tci_tc_host::tune_prefetch(nsing_d > 0 ? &tcp : nullptr, ntrip_d > 0 ? &tcm : nullptr, stream, nullptr);
-    LCUDA(cudaStreamSynchronize(stream));
-    check_status();
     dense_flops = 2.0 * (double)np_d * (double)np_d * (double)nsing_d + 2.0 * (double)nm_d * (double)nm_d * (double)ntrip_d;
     dense_bytes = 4.0 * ((double)tci_tc_host::w32_floats(np_d) + (nm_d > 0 ? (double)tci_tc_host::w32_floats(nm_d) : 0.0));
     dense_ready = true;
@@ -500,7 +493,7 @@ struct tci_local {
     gather_dense<<<nb, 256, 0, stream>>>(dblocks, dheads, ddom, Cb, nvirt, u2p, tci_tc_host::padded_ld(np_d), u2m,
                                          tci_tc_host::padded_ld(std::max<int64_t>(1, nm_d)));
     LCUDA(cudaGetLastError());
-    LCUDA(tci_tc_host::launch(nsing_d > 0 ? &tcp : nullptr, ntrip_d > 0 ? &tcm : nullptr, stream, dense_prefetch));
+    LCUDA(tci_tc_host::launch(nsing_d > 0 ? &tcp : nullptr, ntrip_d > 0 ? &tcm : nullptr, stream));
     scatter_dense<<<nb, 256, 0, stream>>>(dblocks, dheads, ddom, yp, np_d, ym, nm_d, nvirt, Sb);
     LCUDA(cudaGetLastError());
   }

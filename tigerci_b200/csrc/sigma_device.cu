@@ -370,6 +370,108 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
     }
 }
 
+// Domain-restricted two-external products of a local deck (pair domains), on the padded pair matrices:
+//   C[dom[i]][dom[j]] += sum_s alpha_s sum_k A_s[dom[i]][dom_s[k]] B_s[dom_s[k]][dom[j]]   (i, j < m; k < m_s)
+// A_s an n x n integral matrix, B_s the source head's padded pair matrix (zero outside its domain's rows
+// and columns, so only its domain's rows carry terms, and only the columns in both domains are nonzero),
+// C the target head's padded accumulator; all of pitch ld = n.  This is the reference's local two-external
+// product on the common virtuals (two_int_seg_com_lmo_res, three_and_four_seg_mod_2.f90:7137-8005), here
+// over the target's whole domain with the source's zeros in place of the column selection, so that every
+// term of a target block adds into the same tile and the sum stays in a fixed order.  64 x 64 tiles of
+// the m x m domain block, 16-deep k chunks gathered through shared memory; each thread loads the next
+// chunk's eight elements into registers while the current chunk is multiplied.  Segments in table order,
+// k ascending; alpha scales B as it is stored.
+struct DDomProblem {
+  double* C;
+  const int* dom;
+  int m, tiles_n;
+  long long tile_begin, seg_begin, seg_end;
+};
+struct DDomSeg {
+  const double* A;
+  const double* B;
+  const int* dom;
+  int m;
+  double alpha;
+};
+constexpr int DOM_T = 64, DOM_K = 16;
+__global__ void __launch_bounds__(256) gemm_dom_f64(const DDomProblem* __restrict__ probs, int nprob,
+                                                   const DDomSeg* __restrict__ segs, long long ld) {
+  __shared__ double As[DOM_K][DOM_T];
+  __shared__ double Bs[DOM_K][DOM_T];
+  const long long tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile_begin <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const DDomProblem P = probs[lo];
+  const long long t = tile - P.tile_begin;
+  const int r0 = (int)(t / P.tiles_n) * DOM_T, c0 = (int)(t % P.tiles_n) * DOM_T;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int ka = tid & 15, ia = tid >> 4, kb = tid >> 6, jb = tid & 63;
+  // this thread's load slots: A rows ia + 16 q at k = ka; B rows kb + 4 q at column jb
+  long long arow[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) arow[q] = (r0 + ia + 16 * q < P.m) ? (long long)P.dom[r0 + ia + 16 * q] * ld : -1;
+  const long long bcol = (c0 + jb < P.m) ? (long long)P.dom[c0 + jb] : -1;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+  for (long long sgi = P.seg_begin; sgi < P.seg_end; ++sgi) {
+    const DDomSeg S = segs[sgi];
+    const int nch = (S.m + DOM_K - 1) / DOM_K;
+    double ra[4], rb[4];
+    auto fetch = [&](int k0) {
+      const int k = k0 + ka;
+      const long long col = k < S.m ? (long long)S.dom[k] : -1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ra[q] = (arow[q] >= 0 && col >= 0) ? S.A[arow[q] + col] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int kk = k0 + kb + 4 * q;
+        rb[q] = (kk < S.m && bcol >= 0) ? S.B[(long long)S.dom[kk] * ld + bcol] : 0.0;
+      }
+    };
+    fetch(0);
+    for (int ch = 0; ch < nch; ++ch) {
+      __syncthreads();  // the previous chunk's reads of As / Bs are done
+#pragma unroll
+      for (int q = 0; q < 4; ++q) As[ka][ia + 16 * q] = ra[q];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Bs[kb + 4 * q][jb] = S.alpha * rb[q];
+      __syncthreads();
+      if (ch + 1 < nch) fetch((ch + 1) * DOM_K);
+#pragma unroll
+      for (int k = 0; k < DOM_K; ++k) {
+        double a[4], b[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) a[r] = As[k][ty + 16 * r];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) b[c] = Bs[k][tx + 16 * c];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = r0 + ty + 16 * r;
+    if (i >= P.m) continue;
+    double* row = P.C + (long long)P.dom[i] * ld;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int j = c0 + tx + 16 * c;
+      if (j < P.m) row[P.dom[j]] += acc[r][c];
+    }
+  }
+}
+
 // Row-panel FP64 GEMM for problems with few rows and long rows of B (the all-external product Y = U W: a
 // few dozen gathered CI rows against the np x np operator): C (M x N) = beta C + sum over the segments of
 // alpha A B, A M x K and B K x N row major, M <= MT.  A block of 256 threads owns 128 columns of one problem
@@ -1144,6 +1246,11 @@ struct DevStep {
   long long ntiles_f = 0;
   int nprob_f = 0;
   bool tc_ok = false;  // worth the tensor cores: enough work and tiles mostly full
+  // local decks: the two-external step restricted to the heads' domains (gemm_dom_f64)
+  DDomProblem* dom_probs = nullptr;
+  DDomSeg* dom_segs = nullptr;
+  int dom_nprob = 0;
+  long long dom_ntiles = 0;
   // AXPY / DOT
   DAxpyTarget* at = nullptr;
   DAxpySource* as = nullptr;
@@ -1215,7 +1322,6 @@ struct tci_ctx {
   float* u2t = nullptr;                 // split triplet CI blocks
   int* tc_status = nullptr;
   tci_tc_host::AllextTc tc_sing, tc_trip;
-  int tc_prefetch = 8;  // L2 lead of the all-external launch (timed at set-up)
   cudaGraph_t graph = nullptr, graph_prof = nullptr;
   cudaGraphExec_t graph_exec = nullptr, graph_exec_prof = nullptr;  // plain / with per-step event nodes
   double* hd = nullptr;          // diagonal H_ii (device), built on first use
@@ -1491,6 +1597,71 @@ struct tci_ctx {
     d.tma_ntiles = tiles;
   }
 
+  // The two-external step of a local deck's plan on the heads' domains: the same problems and segments
+  // (target pair matrix, integral matrix x source pair matrix, alpha), each restricted to the target's and
+  // the source's domain rows / columns; heads without local CSFs drop out.
+  DevStep lower_dom(const Step& s, const tci::LocalSetup& ls) {
+    DevStep d;
+    d.kind = s.kind;
+    d.name = s.name;
+    const i64 n = plan.n, n2 = n * n;
+    if (ls.dh_len.size() != plan.dheads.size() || ls.dh_off.size() != plan.dheads.size())
+      throw Error(TCI_ERR_INTERNAL, "local domains do not match the plan's heads");
+    for (int x : ls.dh_dom)
+      if (x < 0 || x >= n) throw Error(TCI_ERR_INTERNAL, "local domain entry outside the externals");
+    for (size_t h = 0; h < ls.dh_len.size(); ++h)
+      if (ls.dh_len[h] < 0 || ls.dh_len[h] > n || ls.dh_off[h] + ls.dh_len[h] > (i64)ls.dh_dom.size())
+        throw Error(TCI_ERR_INTERNAL, "local domain slice out of range");
+    std::vector<i64> dk2h((size_t)plan.nD, -1);
+    for (size_t h = 0; h < plan.dheads.size(); ++h)
+      for (i64 k = 0; k < plan.dheads[h].nD; ++k) dk2h[(size_t)(plan.dheads[h].dk0 + k)] = (i64)h;
+    auto head_of = [&](i64 off) {
+      const i64 dk = off / n2;
+      if (off % n2 || dk < 0 || dk >= plan.nD || dk2h[(size_t)dk] < 0)
+        throw Error(TCI_ERR_INTERNAL, "two-external operand is not a pair matrix");
+      return dk2h[(size_t)dk];
+    };
+    const int* ddom = upload(ls.dh_dom, owned, stream);
+    std::vector<DDomProblem> pr;
+    std::vector<DDomSeg> sg;
+    long long tiles = 0;
+    for (const auto& g : s.gp) {
+      if (g.c != BUF_R || g.M != n || g.N != n || g.ldc != n)
+        throw Error(TCI_ERR_INTERNAL, "unexpected two-external problem shape");
+      const i64 h = head_of(g.offC), m = ls.dh_len[(size_t)h];
+      if (m == 0) continue;
+      check_range(BUF_R, g.offC, n2);
+      DDomProblem P{ptr(BUF_R, g.offC), ddom + ls.dh_off[(size_t)h], (int)m, (int)((m + DOM_T - 1) / DOM_T), tiles,
+                    (long long)sg.size(), 0};
+      for (i64 q = g.seg_begin; q < g.seg_end; ++q) {
+        const GemmSeg& x = s.gs[(size_t)q];
+        if (x.b != BUF_D || x.lda != n || x.ldb != n || x.K != n || x.tA || x.tB)
+          throw Error(TCI_ERR_INTERNAL, "unexpected two-external segment shape");
+        const i64 hs = head_of(x.offB), ms = ls.dh_len[(size_t)hs];
+        if (ms == 0) continue;
+        check_range(x.a, x.offA, n2);
+        check_range(BUF_D, x.offB, n2);
+        sg.push_back(DDomSeg{ptr(x.a, x.offA), ptr(BUF_D, x.offB), ddom + ls.dh_off[(size_t)hs], (int)ms, x.alpha});
+      }
+      P.seg_end = (long long)sg.size();
+      if (P.seg_end == P.seg_begin) continue;
+      pr.push_back(P);
+      tiles += (long long)P.tiles_n * P.tiles_n;
+    }
+    d.dom_probs = upload(pr, owned, stream);
+    d.dom_segs = upload(sg, owned, stream);
+    d.dom_nprob = (int)pr.size();
+    d.dom_ntiles = tiles;
+    return d;
+  }
+
+  // local decks: the padded positions of the local CSFs, sorted (empty otherwise)
+  std::vector<long long> loc_pos;
+  bool any_local(i64 off, i64 len) const {
+    auto it = std::lower_bound(loc_pos.begin(), loc_pos.end(), (long long)off);
+    return it != loc_pos.end() && *it < off + len;
+  }
+
   DevStep lower(const Step& s) {
     DevStep d;
     d.kind = s.kind;
@@ -1660,9 +1831,13 @@ struct tci_ctx {
           bad |= 1;
           continue;
         }
-        for (i64 b = 0; b < x.len; b += kChunk)
+        for (i64 b = 0; b < x.len; b += kChunk) {
+          // local decks: a chunk of sigma without local CSFs is never read back (gather_local): dropped
+          const i64 len = std::min(kChunk, x.len - b);
+          const bool keep = x.dst != BUF_S || loc_pos.empty() || any_local(x.off + b, len);
           t[(size_t)(first[(size_t)i] + b / kChunk)] =
-              DAxpyTarget{buf[x.dst] + x.off + b, b, std::min(kChunk, x.len - b), x.src_begin, x.src_end};
+              DAxpyTarget{buf[x.dst] + x.off + b, b, keep ? len : 0, x.src_begin, x.src_end};
+        }
         // source length equals its target's length
         for (i64 q = x.src_begin; q < x.src_end; ++q)
           if (!range_ok(s.as[(size_t)q].src, s.as[(size_t)q].off, x.len)) bad |= 1;
@@ -1677,6 +1852,8 @@ struct tci_ctx {
         so[(size_t)q] = DAxpySource{buf[x.src] + x.off, x.sbuf >= 0 ? buf[x.sbuf] + x.sidx : nullptr, x.coef};
       }
       if (bad) throw Error(TCI_ERR_INTERNAL, "plan range outside its buffer (or an unallocated buffer)");
+      if (!loc_pos.empty())
+        t.erase(std::remove_if(t.begin(), t.end(), [](const DAxpyTarget& x) { return x.len == 0; }), t.end());
       d.at = upload(t, owned, stream);
       d.as = upload(so, owned, stream);
       d.ntg = (long long)t.size();
@@ -1861,6 +2038,10 @@ struct tci_ctx {
   long long sigma_launches() const {
     long long k = 0;
     for (const auto& s : sigma) {
+      if (s.dom_probs) {
+        k += s.dom_ntiles > 0 ? 1 : 0;
+        continue;
+      }
       const bool tc_allext = precision == 1 || allext_tc_in_fp64;
       if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
       if (tc_allext && s.kind == STEP_GEMM && s.name == "all-external") {
@@ -1949,8 +2130,7 @@ struct tci_ctx {
       TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_us, plan.n_sing, plan.np, u2s, stream));
     if (has_trip())
       TCI_CUDA(tci_tc_host::split_u(buf[BUF_T0] + plan.allext_ut, plan.n_trip, plan.nm, u2t, stream));
-    TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream,
-                                 tc_prefetch));
+    TCI_CUDA(tci_tc_host::launch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream));
   }
 
   // X (M x M, FP64) = A A^T with A = M rows of K values in BUF_T0, on the TMA-fed 3xTF32 kernel (set-up).
@@ -2142,18 +2322,6 @@ struct tci_ctx {
     if (plan.n_trip > 0 && nm > 0 &&
         !tci_tc_host::prepare(tc_trip, w32m, nm, u2t, plan.n_trip, buf[BUF_T0] + plan.allext_yt, tc_status, tc_kblock, err))
       throw Error(TCI_ERR_CUDA, err);
-    if (allext && (has_sing() || has_trip())) {
-      // the L2 lead of the all-external launch, timed on zeroed U rows (the outputs are scratch until the
-      // first sigma build)
-      if (u2s) TCI_CUDA(cudaMemsetAsync(u2s, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(std::max<i64>(1, plan.n_sing), np), stream));
-      if (u2t) TCI_CUDA(cudaMemsetAsync(u2t, 0, sizeof(float) * (size_t)tci_tc_host::u2_floats(plan.n_trip, nm), stream));
-      tc_prefetch = tci_tc_host::tune_prefetch(has_sing() ? &tc_sing : nullptr, has_trip() ? &tc_trip : nullptr, stream,
-                                               nullptr);
-      TCI_CUDA(cudaStreamSynchronize(stream));
-      int h = 0;
-      TCI_CUDA(cudaMemcpy(&h, tc_status, sizeof(int), cudaMemcpyDeviceToHost));
-      if (h != 0) throw Error(TCI_ERR_TIMEOUT, "all-external kernel: a bounded wait gave up during set-up");
-    }
     if (refine != 1 && buf[BUF_W]) {  // the FP64 W is only needed for the plain-FP64 finish of the roots
       std::lock_guard<std::mutex> lk(g_capture_free_mu);
       TCI_CUDA(dev_free(buf[BUF_W], stream));
@@ -2224,6 +2392,11 @@ struct tci_ctx {
     if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
     switch (s.kind) {
       case STEP_GEMM:
+        if (s.dom_probs) {  // local deck: the two-external step on the domains
+          if (s.dom_ntiles > 0)
+            gemm_dom_f64<<<(unsigned)s.dom_ntiles, 256, 0, stream>>>(s.dom_probs, s.dom_nprob, s.dom_segs, plan.n);
+          break;
+        }
         if (tc_allext && s.name == "all-external") {
           run_allext_tc();
           break;
@@ -2499,6 +2672,20 @@ void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& 
   }
   for (i64 x : ls.map)
     if (x < 0) throw Error(TCI_ERR_INTERNAL, "a local CSF has no non-local counterpart");
+  // domains of the plan's N-2 heads, in the plan's head order (Builder::setup_heads: kept heads with a
+  // pair matrix)
+  for (size_t p = 0; p < nl.paths[2].size(); ++p) {
+    const Head& g = nl.paths[2][p];
+    if (!g.kept) continue;
+    const i64 nab_f = g.off >= 0 ? g.nsf : 0, naa_f = g.off_aa >= 0 ? g.nsf_aa : 0;
+    if (std::max(nab_f, naa_f) == 0) continue;
+    const Head& h = loc.paths[2][p];
+    ls.dh_off.push_back((int64_t)ls.dh_dom.size());
+    if (h.domain >= 0 && (h.off >= 0 || h.off_aa >= 0)) {
+      for (int a : loc.domains[(size_t)h.domain]) ls.dh_dom.push_back(a);
+    }
+    ls.dh_len.push_back((int64_t)ls.dh_dom.size() - ls.dh_off.back());
+  }
   // (aa|cc) and (ac|ca) over the externals, for the all-external part of the diagonal
   ls.xdiag.assign((size_t)(2 * n * n), 0.0);
   auto row = [&](i64 p, i64 q) {
@@ -2580,6 +2767,8 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     if (ls) {
       ctx->local = true;
       ctx->n_loc = ls->loc.total_csfs;
+      ctx->loc_pos.assign(ls->map.begin(), ls->map.end());
+      std::sort(ctx->loc_pos.begin(), ctx->loc_pos.end());
       ctx->d_map = upload(ls->map, ctx->owned, ctx->stream);
       ctx->xdiag = upload(ls->xdiag, ctx->owned, ctx->stream);
       for (double** p : {&ctx->loc_c, &ctx->loc_s}) {
@@ -2623,7 +2812,10 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
       ctx->init.push_back(ctx->lower(s));
     }
     for (auto& s : P.sigma_steps) {
-      ctx->sigma.push_back(ctx->lower(s));
+      if (ls && s.kind == STEP_GEMM && s.name == "dd two-external")
+        ctx->sigma.push_back(ctx->lower_dom(s, *ls));
+      else
+        ctx->sigma.push_back(ctx->lower(s));
       if (timing) {  // the σ steps whose tables take a noticeable time
         cudaStreamSynchronize(ctx->stream);
         const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
