@@ -385,25 +385,26 @@ def molecular_measure(device, steps=3, warmup=1):
     return out
 
 
-def local_solve_measure(device, nchol=2400):
+def local_solve_measure(device, nchol=2400, n_int=35, n_virt=400, dmax=180):
     """The batching configuration as a Davidson solve: 35 doubly occupied internal orbitals (630 internal
     pairs), 400 externals, every pair and single-hole path with a random domain of 20..180 externals (seed
     99), Cholesky rank 2400, operator at molecular magnitude; 1 root, residual 1e-6.  The all-external term
-    runs in the pair-domain Cholesky form (grouped GEMMs over uneven domains), every other term on the
-    non-local plan with the blocks padded to all externals; FP64 and mixed forms."""
+    runs on the pair-domain operator (the faster of its Cholesky and dense forms), the two-external N-2 step
+    on the domains, every other term on the non-local plan with the blocks padded to all externals; FP64 and
+    mixed forms.  n_int / n_virt / dmax shrink it (profiler captures)."""
     import torch
 
     import tigerci_b200 as T
     from tigerci_b200 import local
     from tigerci_b200.synthetic import synthetic_operator
 
-    deck = local.pair_domain_deck()
+    deck = local.pair_domain_deck(n_int=n_int, n_virt=n_virt, dmax=dmax)
     h, L = synthetic_operator(deck.num_orbitals, nchol, seed=1234, scale=0.02, diag_range=(-2.0, 1.0),
                               offdiag_sigma=0.02)
     op = T.Operator(h, L)
-    out = {"workload": "local MRSDCI: 35 doubly occupied internal orbitals (630 pair paths), 400 externals, "
-                       "domains U{20..180} per pair and single-hole path (seed 99), Cholesky rank 2400, molecular "
-                       "magnitude; 1 root, residual 1e-6, energy tolerance 1e-8"}
+    out = {"workload": f"local MRSDCI: {n_int} doubly occupied internal orbitals ({n_int * (n_int + 1) // 2} pair "
+                       f"paths), {n_virt} externals, domains U{{20..{dmax}}} per pair and single-hole path (seed 99), "
+                       f"Cholesky rank {nchol}, molecular magnitude; 1 root, residual 1e-6, energy tolerance 1e-8"}
     for form in ("tf32x3", "fp64"):
         t = time.perf_counter()
         sb = T.SigmaBuilder(deck, op, device=device, precision=form)
@@ -502,7 +503,7 @@ def molecular_cpu(mol):
             "what": "oracle Davidson (davidson.f90 restated) over the integral-direct CPU sigma"}
 
 
-def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3, nchol=2400, forms=("tf32x3", "fp64")):
+def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3, nchol=2400, forms=("tf32x3", "fp64"), n_virt=400):
     """All-external term over uneven pair domains: n_pairs internal pairs (35
     doubly occupied internal orbitals), domains of 20..180 of 400 external
     orbitals (seed 99), Cholesky rank 2400 as in the kernel-scale operator.
@@ -512,13 +513,13 @@ def local_measure(n_pairs, device, hbm, bf16, steps=3, warmup=3, nchol=2400, for
     from tigerci_b200 import local
     from tigerci_b200.synthetic import synthetic_operator
 
-    n_int, n_virt = 35, 400
-    heads, dom, total = local.pair_domain_problem(n_pairs, n_int, n_virt, 20, 180, seed=99)
+    n_int = 35
+    heads, dom, total = local.pair_domain_problem(n_pairs, n_int, n_virt, 20, min(180, n_virt), seed=99)
     _, L = synthetic_operator(n_int + n_virt, nchol, seed=1234)
     rng = np.random.default_rng(7)
     c_host = rng.standard_normal(total)
     c = torch.from_numpy(c_host).cuda(device)
-    out = {"workload": f"{len(heads)} internal pairs, domains U{{20..180}} of {n_virt} externals (seed 99), "
+    out = {"workload": f"{len(heads)} internal pairs, domains U{{20..{min(180, n_virt)}}} of {n_virt} externals (seed 99), "
                        f"Cholesky rank {nchol}; CI length {total}",
            "heads": int(len(heads))}
     sig = {}
@@ -593,6 +594,8 @@ def main():
     ap.add_argument("--no-molecular", action="store_true", help="skip the water (front end) measurement")
     ap.add_argument("--octane-only", action="store_true", help="only the n-octane precision measurement")
     ap.add_argument("--local-solve-only", action="store_true", help="only the pair-domain Davidson solve")
+    ap.add_argument("--local-virt", type=int, default=400, help="externals of the pair-domain workloads")
+    ap.add_argument("--local-int", type=int, default=35, help="internal orbitals of the pair-domain solve")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -635,7 +638,8 @@ def main():
         return
     if args.local_solve_only:
         if rank == 0:
-            print(dumps({"local_solve": local_solve_measure(local)}), flush=True)
+            print(dumps({"local_solve": local_solve_measure(local, n_int=args.local_int, n_virt=args.local_virt,
+                                                            dmax=min(180, args.local_virt))}), flush=True)
         return
     if args.octane_only:
         if rank == 0:
@@ -644,7 +648,8 @@ def main():
     if args.local_only:
         if rank == 0:
             print(dumps({"local_pairs": local_measure(args.local_pairs, local, hbm, bf16, nchol=args.local_nchol,
-                                                    forms=tuple(f for f in args.local_forms.split(",") if f))}), flush=True)
+                                                    forms=tuple(f for f in args.local_forms.split(",") if f),
+                                                    n_virt=args.local_virt)}), flush=True)
         return
 
     # ---- sigma builds on the operator exactly as the kernel-scale configuration specifies
