@@ -262,6 +262,18 @@ int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out
  * span / (iters x nacc), from the second of two launches. */
 int tci_selftest_mma_rate(int64_t device, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma);
 
+/* ---- A posteriori corrections (calculate_a_posteriori_corrections,
+ * tiger_fortran/aposteriori.f90:28-221, called after a one-root SDCI solve,
+ * driver_sdci.f90:73).  tci_reference_weight: c0^2 = sum of c_i^2 over the
+ * CSFs of the reference configurations (no external electron) of a
+ * space-length vector.  tci_aposteriori: out[5] = the Davidson, renormalised
+ * Davidson, Davidson-Silver, Meissner and Pople corrections for correlation
+ * energy e_corr (total - reference energy), c0^2 and n_corr_elec correlated
+ * electrons (num_elec - 2 num_frozen); TCI_ERR_INPUT below 4 electrons (the
+ * reference prints none there) or outside 1/2 < c0^2 <= 1. */
+int tci_reference_weight(const tci_space* s, const double* c, int64_t n, double* c0sq);
+int tci_aposteriori(int64_t n_corr_elec, double c0sq, double e_corr, double* out, int64_t len);
+
 /* ---- Local pair domains: the all-external term over uneven domains -----
  * Replaces the local all-external loops (ext_3_4_seg_loops_vec_lmo_res_2,
  * tiger_fortran/three_and_four_seg_mod_1.f90:3240-3518, over the domains of

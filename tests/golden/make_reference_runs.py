@@ -87,6 +87,24 @@ def final_residuals(lines):
     return [res[r] for r in sorted(res)]
 
 
+def aposteriori(lines):
+    """The 'A Posteriori Corrections' block (one-root runs): [{"c0sq": x, name: value, ...}] for the two
+    definitions of c0^2 it prints (sum of reference c^2, then <ref|ci>^2)."""
+    out, cur = [], None
+    names = {"Davidson": "davidson", "Renormalized Davidson": "renormalized_davidson",
+             "Davidson-Silver": "davidson_silver", "Meissner": "meissner", "Pople": "pople"}
+    for ln in lines:
+        m = re.match(r"\s*Define c_0\^2 = .*=\s*(-?\d\.\d+E[+-]\d+)", ln)
+        if m:
+            cur = {"c0sq": float(m.group(1))}
+            out.append(cur)
+            continue
+        m = re.match(r"\s*(Davidson|Renormalized Davidson|Davidson-Silver|Meissner|Pople)\s+(-?\d\.\d+E[+-]\d+)\s*$", ln)
+        if m and cur is not None:
+            cur[names[m.group(1)]] = float(m.group(2))
+    return out
+
+
 def grab(lines, pattern):
     return [float(m.group(1)) for ln in lines for m in [re.search(pattern, ln)] if m]
 
@@ -130,6 +148,7 @@ def main(ref_root):
                 "roots": grab(out, r"Root\s+\d+ total energy \(electronic \+ nuclear\) is :\s*(-?\d+\.\d+)"),
                 "listings": listings(out),
                 "final_residual_norms": final_residuals(out),
+                "aposteriori": aposteriori(out),
             },
         })
     path = os.path.join(HERE, "reference_runs.json")

@@ -18,7 +18,8 @@ of the reference's own test scripts, tests/Tests/*/driver.sh), and the final
 wavefunction listing of each root (the ten largest |c| with their spin
 function, arc weight, internal occupation and virtual orbitals; |c| within
 the residual norm the reference's last iteration printed, since it stops on
-the energy change with |Hc - Ec| of a few 1e-4 left)."""
+the energy change with |Hc - Ec| of a few 1e-4 left), and for the one-root runs
+the a posteriori block: c0^2 of the converged vector and the five corrections."""
 import json
 import os
 
@@ -144,6 +145,18 @@ def test_sdci_roots_and_wavefunction_listing_match_reference(r, need_gpu):
         tol = r["printed"]["final_residual_norms"][root] + 5e-6
         for key in common:
             assert abs(got[key] - want[key]) <= tol, (key, got[key], want[key], tol)
+    # a posteriori corrections of the one-root runs: c0^2 of the converged vector against the printed one
+    # (the reference's vector is a residual norm away from converged, so c0^2 is about twice that away)
+    blocks = r["printed"].get("aposteriori")
+    if nroots == 1 and blocks:
+        c0sq = sp.reference_weight(vecs[0])
+        tol = 2.0 * r["printed"]["final_residual_norms"][0] + 1e-7
+        assert abs(c0sq - blocks[0]["c0sq"]) <= tol, (c0sq, blocks[0]["c0sq"], tol)
+        n_corr = deck.num_elec - 2 * deck.num_frozen
+        got = T.aposteriori(c0sq, float(total[0]) - r["printed"]["reference_energy"], n_corr)
+        e_corr = abs(r["printed"]["roots"][-1] - r["printed"]["reference_energy"])
+        for name, v in got.items():
+            assert abs(v - blocks[0][name]) <= e_corr * tol + ENERGY_TOL, (name, v, blocks[0][name])
 
 
 @pytest.mark.gpu

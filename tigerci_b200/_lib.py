@@ -64,6 +64,8 @@ EXPORTS = [
     "tci_selftest_bounded_wait",
     "tci_selftest_mma_rate",
     "tci_operator_from_records",
+    "tci_reference_weight",
+    "tci_aposteriori",
     "tci_integrals_create",
     "tci_integrals_info",
     "tci_integrals_one_electron",
@@ -167,6 +169,8 @@ def lib():
         L.tci_selftest_bounded_wait.argtypes = [i64, i64, P, P]
         L.tci_selftest_mma_rate.argtypes = [i64, i64, i64, i64, P]
         L.tci_operator_from_records.argtypes = [i64, i64, P, P, i64, P]
+        L.tci_reference_weight.argtypes = [P, P, i64, P]
+        L.tci_aposteriori.argtypes = [i64, dbl, dbl, P, i64]
         L.tci_integrals_create.argtypes = [C.POINTER(TciMolecule), dbl, C.POINTER(P)]
         L.tci_integrals_info.argtypes = [P, P, i64]
         L.tci_integrals_one_electron.argtypes = [P, P, P, i64]

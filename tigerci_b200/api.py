@@ -82,6 +82,13 @@ class CsfSpace:
         check(lib().tci_acpf_gdiag(self._h, flag, custom_g, ptr(g), ptr(cls), n))
         return g, cls
 
+    def reference_weight(self, c: np.ndarray) -> float:
+        """c0^2: the squared coefficients of the reference configurations' CSFs summed (tci_reference_weight)."""
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        out = C.c_double()
+        check(lib().tci_reference_weight(self._h, ptr(c), c.size, C.byref(out)))
+        return out.value
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib().tci_space_destroy(self._h)
@@ -112,6 +119,16 @@ class CsfSpace:
         nt = C.c_int64()
         check(lib().tci_space_block_counts(self._h, kind, ptr(out), 64, C.byref(nt)))
         return {int(out[3 * t]): (int(out[3 * t + 1]), int(out[3 * t + 2])) for t in range(nt.value)}
+
+
+APOSTERIORI = ("davidson", "renormalized_davidson", "davidson_silver", "meissner", "pople")
+
+
+def aposteriori(c0sq: float, e_corr: float, n_corr_elec: int) -> dict:
+    """The reference's a posteriori corrections (tci_aposteriori): {name: correction (Eh)}."""
+    out = np.zeros(5)
+    check(lib().tci_aposteriori(int(n_corr_elec), float(c0sq), float(e_corr), ptr(out), 5))
+    return dict(zip(APOSTERIORI, out.tolist()))
 
 
 class Operator:

@@ -1,6 +1,7 @@
 // Host-only part of the C ABI (include/tigerci_sigma.h): error reporting, CSF
 // space queries and plan construction / export.  No CUDA dependency.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -262,6 +263,39 @@ int tci_acpf_gdiag(const tci_space* s, int64_t flag, double custom_g, double* g,
   } catch (...) {
     return guard_status(std::current_exception());
   }
+}
+
+int tci_reference_weight(const tci_space* s, const double* c, int64_t n, double* c0sq) {
+  if (!s || !c || !c0sq || n != s->sp.total_csfs) return TCI_ERR_ARG;
+  // calculate_ref_coeff_squared (aposteriori.f90:133-160): c^2 summed over the CSFs of the reference
+  // configurations with no external electron, i.e. the metric's class 1
+  std::vector<double> g((size_t)n);
+  std::vector<int64_t> cls((size_t)n);
+  const int rc = tci_acpf_gdiag(s, 9, 0.0, g.data(), cls.data(), n);
+  if (rc != TCI_OK) return rc;
+  double t = 0.0;
+  for (int64_t i = 0; i < n; ++i)
+    if (cls[(size_t)i] == 1) t += c[i] * c[i];
+  *c0sq = t;
+  return TCI_OK;
+}
+
+int tci_aposteriori(int64_t n_corr_elec, double c0sq, double e_corr, double* out, int64_t len) {
+  if (!out || len < 5 || !std::isfinite(c0sq) || !std::isfinite(e_corr)) return TCI_ERR_ARG;
+  if (n_corr_elec < 4 || c0sq <= 0.5 || c0sq > 1.0) {
+    set_error("a posteriori corrections need at least 4 correlated electrons and 1/2 < c0^2 <= 1");
+    return TCI_ERR_INPUT;
+  }
+  // the size-extensivity corrections of aposteriori.f90:162-221 (Davidson; renormalised Davidson;
+  // Davidson-Silver; Meissner; Pople in the closed form of Duch and Diercksen, J. Chem. Phys. 101, 3018 (1994))
+  const double q = 1.0 - c0sq, N = (double)n_corr_elec;
+  out[0] = e_corr * q;
+  out[1] = e_corr * q / c0sq;
+  out[2] = e_corr * q / (2.0 * c0sq - 1.0);
+  out[3] = e_corr * (q / c0sq) * ((N - 2.0) * (N - 3.0) / (N * (N - 1.0)));
+  const double d = 2.0 * c0sq - 1.0;
+  out[4] = e_corr * (2.0 * c0sq / (d * (1.0 + std::sqrt(1.0 + 8.0 * c0sq * q / (N * d * d)))) - 1.0);
+  return TCI_OK;
 }
 
 int tci_space_block_counts(const tci_space* s, int64_t kind, int64_t* out, int64_t max_triples, int64_t* n_triples) {
