@@ -378,9 +378,8 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
 // product on the common virtuals (two_int_seg_com_lmo_res, three_and_four_seg_mod_2.f90:7137-8005), here
 // over the target's whole domain with the source's zeros in place of the column selection, so that every
 // term of a target block adds into the same tile and the sum stays in a fixed order.  64 x 64 tiles of
-// the m x m domain block, 16-deep k chunks gathered through shared memory; each thread loads the next
-// chunk's eight elements into registers while the current chunk is multiplied.  Segments in table order,
-// k ascending; alpha scales B as it is stored.
+// the m x m domain block, 16-deep k chunks gathered through shared memory.  Segments in table order, k
+// ascending; alpha scales B as it is stored.
 struct DDomProblem {
   double* C;
   const int* dom;
@@ -394,11 +393,16 @@ struct DDomSeg {
   int m;
   double alpha;
 };
-constexpr int DOM_T = 64, DOM_K = 16;
-__global__ void __launch_bounds__(256) gemm_dom_f64(const DDomProblem* __restrict__ probs, int nprob,
-                                                   const DDomSeg* __restrict__ segs, long long ld) {
-  __shared__ double As[DOM_K][DOM_T];
-  __shared__ double Bs[DOM_K][DOM_T];
+constexpr int DOM_T = 64, DOM_K = 16, DOM_THREADS = 128;
+// 128 threads, 8 x 4 outputs each (rows 8 ty .. 8 ty + 7, columns tx + 16 c): per k, two 16-byte shared loads
+// of A (the same address across the 16 threads of a row group) and four 8-byte loads of B (16 consecutive
+// doubles across the row group) for 32 FMAs.  The (segment, chunk) sequence of a tile runs through two shared
+// buffers: the next chunk's elements are loaded into registers while the current one is multiplied, then
+// stored into the other buffer, one barrier per chunk.
+__global__ void __launch_bounds__(DOM_THREADS) gemm_dom_f64(const DDomProblem* __restrict__ probs, int nprob,
+                                                           const DDomSeg* __restrict__ segs, long long ld) {
+  __shared__ __align__(16) double As[2][DOM_K][DOM_T];
+  __shared__ __align__(16) double Bs[2][DOM_K][DOM_T];
   const long long tile = blockIdx.x;
   int lo = 0, hi = nprob - 1;
   while (lo < hi) {
@@ -410,58 +414,83 @@ __global__ void __launch_bounds__(256) gemm_dom_f64(const DDomProblem* __restric
   const long long t = tile - P.tile_begin;
   const int r0 = (int)(t / P.tiles_n) * DOM_T, c0 = (int)(t % P.tiles_n) * DOM_T;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // load slots: A rows ia + 8 q at k = ka; B rows kb + 2 q at column jb
   const int ka = tid & 15, ia = tid >> 4, kb = tid >> 6, jb = tid & 63;
-  // this thread's load slots: A rows ia + 16 q at k = ka; B rows kb + 4 q at column jb
-  long long arow[4];
+  long long arow[8];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) arow[q] = (r0 + ia + 16 * q < P.m) ? (long long)P.dom[r0 + ia + 16 * q] * ld : -1;
+  for (int q = 0; q < 8; ++q) arow[q] = (r0 + ia + 8 * q < P.m) ? (long long)P.dom[r0 + ia + 8 * q] * ld : -1;
   const long long bcol = (c0 + jb < P.m) ? (long long)P.dom[c0 + jb] : -1;
-  double acc[4][4];
+  double acc[8][4];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+  for (int r = 0; r < 8; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-  for (long long sgi = P.seg_begin; sgi < P.seg_end; ++sgi) {
-    const DDomSeg S = segs[sgi];
-    const int nch = (S.m + DOM_K - 1) / DOM_K;
-    double ra[4], rb[4];
-    auto fetch = [&](int k0) {
-      const int k = k0 + ka;
-      const long long col = k < S.m ? (long long)S.dom[k] : -1;
+  double ra[8], rb[8];
+  auto fetch = [&](const DDomSeg& S, int k0) {
+    const int k = k0 + ka;
+    const long long col = k < S.m ? (long long)S.dom[k] : -1;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) ra[q] = (arow[q] >= 0 && col >= 0) ? S.A[arow[q] + col] : 0.0;
+    for (int q = 0; q < 8; ++q) ra[q] = (arow[q] >= 0 && col >= 0) ? S.A[arow[q] + col] : 0.0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int kk = k0 + kb + 4 * q;
-        rb[q] = (kk < S.m && bcol >= 0) ? S.B[(long long)S.dom[kk] * ld + bcol] : 0.0;
+    for (int q = 0; q < 8; ++q) {
+      const int kk = k0 + kb + 2 * q;
+      rb[q] = (kk < S.m && bcol >= 0) ? S.B[(long long)S.dom[kk] * ld + bcol] : 0.0;
+    }
+  };
+  auto store = [&](int buf, double alpha) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) As[buf][ka][ia + 8 * q] = ra[q];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) Bs[buf][kb + 2 * q][jb] = alpha * rb[q];
+  };
+  long long sc = P.seg_begin;
+  int kc = 0, buf = 0;
+  if (sc < P.seg_end) {
+    DDomSeg S = segs[sc];
+    fetch(S, 0);
+    store(0, S.alpha);
+    __syncthreads();
+    while (true) {
+      // the next (segment, chunk) of the sequence
+      long long sn = sc;
+      int kn = kc + DOM_K;
+      DDomSeg Sn = S;
+      if (kn >= S.m) {
+        ++sn;
+        kn = 0;
+        if (sn < P.seg_end) Sn = segs[sn];
       }
-    };
-    fetch(0);
-    for (int ch = 0; ch < nch; ++ch) {
-      __syncthreads();  // the previous chunk's reads of As / Bs are done
-#pragma unroll
-      for (int q = 0; q < 4; ++q) As[ka][ia + 16 * q] = ra[q];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) Bs[kb + 4 * q][jb] = S.alpha * rb[q];
-      __syncthreads();
-      if (ch + 1 < nch) fetch((ch + 1) * DOM_K);
+      const bool more = sn < P.seg_end;
+      if (more) fetch(Sn, kn);
 #pragma unroll
       for (int k = 0; k < DOM_K; ++k) {
-        double a[4], b[4];
+        const double2* ap = reinterpret_cast<const double2*>(&As[buf][k][8 * ty]);
+        double a[8], bv[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) a[r] = As[k][ty + 16 * r];
+        for (int h = 0; h < 4; ++h) {
+          const double2 v = ap[h];
+          a[2 * h] = v.x;
+          a[2 * h + 1] = v.y;
+        }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) b[c] = Bs[k][tx + 16 * c];
+        for (int c = 0; c < 4; ++c) bv[c] = Bs[buf][k][tx + 16 * c];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < 8; ++r)
 #pragma unroll
-          for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+          for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], bv[c], acc[r][c]);
       }
+      if (more) store(buf ^ 1, Sn.alpha);
+      __syncthreads();
+      if (!more) break;
+      buf ^= 1;
+      sc = sn;
+      kc = kn;
+      S = Sn;
     }
   }
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int i = r0 + ty + 16 * r;
+  for (int r = 0; r < 8; ++r) {
+    const int i = r0 + 8 * ty + r;
     if (i >= P.m) continue;
     double* row = P.C + (long long)P.dom[i] * ld;
 #pragma unroll
@@ -2394,7 +2423,7 @@ struct tci_ctx {
       case STEP_GEMM:
         if (s.dom_probs) {  // local deck: the two-external step on the domains
           if (s.dom_ntiles > 0)
-            gemm_dom_f64<<<(unsigned)s.dom_ntiles, 256, 0, stream>>>(s.dom_probs, s.dom_nprob, s.dom_segs, plan.n);
+            gemm_dom_f64<<<(unsigned)s.dom_ntiles, DOM_THREADS, 0, stream>>>(s.dom_probs, s.dom_nprob, s.dom_segs, plan.n);
           break;
         }
         if (tc_allext && s.name == "all-external") {
