@@ -62,6 +62,12 @@ inline long long tile_problems(const std::vector<HostGemm>& in, long long tm, lo
 // FP64 SIMT grouped GEMM (sigma_device.cu); cfg 0: 64 x 128 tiles, 1: 128 x 64.
 cudaError_t launch_gemm_f64(int cfg, const DGemmProblem* probs, int nprob, const DGemmSeg* segs, long long ntiles,
                             cudaStream_t st);
+// The cp.async-staged FP64 kernel (64 x 128 tiles): A not transposed, B K x N, operands 16-byte aligned
+// with even leading dimensions.
+cudaError_t launch_gemm_cp_f64(const DGemmProblem* probs, int nprob, const DGemmSeg* segs, long long ntiles,
+                               cudaStream_t st);
+inline long long gemm_cp_tile_m() { return 64; }
+inline long long gemm_cp_tile_n() { return 128; }
 inline long long gemm_f64_tile_m(int cfg) { return cfg == 0 ? 64 : 128; }
 inline long long gemm_f64_tile_n(int cfg) { return cfg == 0 ? 128 : 64; }
 

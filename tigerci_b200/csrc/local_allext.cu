@@ -80,16 +80,18 @@ struct DLocBlock {
   long long n, k;            // domain size, spin function
   long long ab, aa;          // spin function k has an ab block / an aa block
   double p;                  // +1 singlet-coupled, -1 triplet-coupled
-  long long d_off;           // offset of D_hk / R_hk (n x n)
+  long long d_off;           // offset of D_hk / R_hk (n rows of pitch ld)
   long long head;            // index of the head
   long long t_off;           // offset of T_hk (jmax n x n) in the chunk buffer
   long long drow, trow;      // mixed form: first row of D_hk / T_hk in the split arrays
   long long urow;            // dense form: row of the block in U+ (p = +1) or U- (p = -1)
+  long long ld;              // row pitch of the FP64 squares: n rounded up to even (16-byte aligned rows)
 };
 // one head for the gather
 struct DLocHead {
   long long dom_off, n, lc_off;  // domain slice, offset of L^J_h (jmax x n x n) in the chunk buffer
   long long lrow;                // mixed form: first row of L^J_h (jmax n rows) in the split array
+  long long ld;                  // row pitch of L^J_h (n rounded up to even)
 };
 
 __device__ __forceinline__ long long vpair(long long a, long long b) {
@@ -111,7 +113,7 @@ __global__ void transpose_l(const double* __restrict__ L, long long npv, long lo
   }
 }
 
-// Lc[lc_off + j n^2 + a n + c] = LT[J0 + j][vpair(dom[a], dom[c])]; blocks run
+// Lc[lc_off + j n ld + a ld + c] = LT[J0 + j][vpair(dom[a], dom[c])]; blocks run
 // head-fastest so that one row LT[J] serves every head from L2.
 __global__ void gather_lc(const double* __restrict__ LT, long long npv, long long J0, const DLocHead* __restrict__ heads,
                           const long long* __restrict__ dom, double* __restrict__ Lc) {
@@ -119,10 +121,10 @@ __global__ void gather_lc(const double* __restrict__ LT, long long npv, long lon
   const long long j = blockIdx.y;
   const double* row = LT + (J0 + j) * npv;
   const long long* d = dom + H.dom_off;
-  double* out = Lc + H.lc_off + j * H.n * H.n;
+  double* out = Lc + H.lc_off + j * H.n * H.ld;
   for (long long e = threadIdx.x; e < H.n * H.n; e += blockDim.x) {
     const long long a = e / H.n, c = e % H.n;
-    out[e] = row[vpair(d[a], d[c])];
+    out[a * H.ld + c] = row[vpair(d[a], d[c])];
   }
 }
 
@@ -140,7 +142,7 @@ __global__ void unpack_local(const DLocBlock* __restrict__ blk, const double* __
       const double x = c[B.off_ab + B.k * nab + i * (i - 1) / 2 + j];
       v = (r < s) ? x : B.p * x;
     }
-    Dk[e] = v;
+    Dk[r * B.ld + s] = v;
   }
 }
 
@@ -154,11 +156,11 @@ __global__ void pack_local(const DLocBlock* __restrict__ blk, const double* __re
       while (i * (i - 1) / 2 > e) --i;
       while ((i + 1) * i / 2 <= e) ++i;
       const long long j = e - i * (i - 1) / 2;
-      sigma[B.off_ab + B.k * nab + e] += Rk[j * n + i] + B.p * Rk[i * n + j];
+      sigma[B.off_ab + B.k * nab + e] += Rk[j * B.ld + i] + B.p * Rk[i * B.ld + j];
     }
   if (B.aa)
     for (long long a = threadIdx.x; a < n; a += blockDim.x)
-      sigma[B.off_aa + B.k * n + a] += 1.4142135623730951 * Rk[a * n + a];
+      sigma[B.off_aa + B.k * n + a] += 1.4142135623730951 * Rk[a * B.ld + a];
 }
 
 // TF32 high part (low 13 mantissa bits cleared) and FP32 remainder, as the TMA-fed kernel reads them
@@ -373,25 +375,29 @@ struct tci_local {
     std::vector<HostGemm> v1, v2;
     for (const auto& B : blocks) {
       const DLocHead& H = heads[B.head];
-      const long long n = B.n;
+      const long long n = B.n, ld = B.ld;
       double* Tk = T + B.t_off;
-      v1.push_back(HostGemm{Tk, n, j * n, n, 0.0, {DGemmSeg{Lc + H.lc_off, D + B.d_off, n, n, n, 0, 0, 1.0}}});
-      HostGemm y{R + B.d_off, n, n, n, 1.0, {}};
+      v1.push_back(HostGemm{Tk, ld, j * n, n, 0.0, {DGemmSeg{Lc + H.lc_off, D + B.d_off, ld, ld, n, 0, 0, 1.0}}});
+      HostGemm y{R + B.d_off, ld, n, n, 1.0, {}};
       for (int64_t q = 0; q < j; ++q)
-        y.segs.push_back(DGemmSeg{Tk + q * n * n, Lc + H.lc_off + q * n * n, n, n, n, 0, 0, 0.5});
+        y.segs.push_back(DGemmSeg{Tk + q * n * ld, Lc + H.lc_off + q * n * ld, ld, ld, n, 0, 0, 0.5});
       v2.push_back(std::move(y));
     }
     auto finish = [&](std::vector<HostGemm>& v, int cfg, GemmLaunch& g) {
       std::vector<DGemmProblem> pr;
       std::vector<DGemmSeg> sg;
       g.cfg = cfg;
-      g.ntiles = tci_dev::tile_problems(v, tci_dev::gemm_f64_tile_m(cfg), tci_dev::gemm_f64_tile_n(cfg), false, pr, sg);
+      const long long tm = cfg == 2 ? tci_dev::gemm_cp_tile_m() : tci_dev::gemm_f64_tile_m(cfg);
+      const long long tn = cfg == 2 ? tci_dev::gemm_cp_tile_n() : tci_dev::gemm_f64_tile_n(cfg);
+      g.ntiles = tci_dev::tile_problems(v, tm, tn, false, pr, sg);
       g.probs = upload(pr);
       g.segs = upload(sg);
       g.nprob = (int)pr.size();
     };
-    finish(v1, 1, a);  // tall problems: 128 x 64 tiles
-    finish(v2, cfg_second, b);
+    // cfg_second 0: both GEMMs on the cp.async-staged kernel (64 x 128 tiles; the even row pitches keep every
+    // operand row 16-byte aligned); 1: the register-staged kernel, 128 x 64 tiles
+    finish(v1, cfg_second == 0 ? 2 : 1, a);
+    finish(v2, cfg_second == 0 ? 2 : 1, b);
   }
 
   // mixed form: TMA-fed tables for chunks of j vectors; narrow1: the first GEMM on 64-wide tiles
@@ -412,7 +418,7 @@ struct tci_local {
       t1 += ((j * n + TM - 1) / TM) * tn1;
       p1.push_back(q1);
       // R_hk += 1/2 sum_J T_hkJ L^J_h (L^J_h symmetric: its rows are the K-major operand)
-      TmaProblem q2{R + B.d_off, n, n, n, tn, t2, 1.0, (long long)s2.size(), 0, 0, nullptr, nullptr, 0};
+      TmaProblem q2{R + B.d_off, B.ld, n, n, tn, t2, 1.0, (long long)s2.size(), 0, 0, nullptr, nullptr, 0};
       for (int64_t q = 0; q < j; ++q) s2.push_back(TmaSeg{B.trow + q * n, H.lrow + q * n, 0, n, 0.5});
       q2.seg_end = (long long)s2.size();
       t2 += ((n + TM - 1) / TM) * tn;
@@ -430,7 +436,8 @@ struct tci_local {
 
   void launch_gemm(const GemmLaunch& g) {
     if (g.ntiles <= 0) return;
-    LCUDA(tci_dev::launch_gemm_f64(g.cfg, g.probs, g.nprob, g.segs, g.ntiles, stream));
+    if (g.cfg == 2) LCUDA(tci_dev::launch_gemm_cp_f64(g.probs, g.nprob, g.segs, g.ntiles, stream));
+    else LCUDA(tci_dev::launch_gemm_f64(g.cfg, g.probs, g.nprob, g.segs, g.ntiles, stream));
   }
 
   // Dense form set-up from the virtual-virtual Cholesky rows lpk (npv x nchol, row-major, on the device):
@@ -647,17 +654,20 @@ int tci_local_create(int64_t num_internal, int64_t num_external, const double* c
         throw Error(TCI_ERR_INPUT, "head block outside the CI vector");
       const long long nk = std::max(nsf_ab, nsf_aa);
       if (nk == 0) continue;
-      L->heads.push_back(DLocHead{doff, n, lc_per_j, lrows});  // offsets per Cholesky vector, scaled by jmax below
+      const long long ld = n + (n & 1);
+      // offsets per Cholesky vector, scaled by jmax below
+      L->heads.push_back(DLocHead{doff, n, lc_per_j, lrows, ld});
       const long long hi = (long long)L->heads.size() - 1;
       for (long long k = 0; k < nk; ++k) {
-        L->blocks.push_back(DLocBlock{off_ab, off_aa, n, k, k < nsf_ab ? 1 : 0, k < nsf_aa ? 1 : 0,
-                                      k < nsing ? 1.0 : -1.0, dtot, hi, t_per_j, drows, drows});
-        dtot += n * n;
+        DLocBlock blk{off_ab, off_aa, n, k, k < nsf_ab ? 1 : 0, k < nsf_aa ? 1 : 0,
+                      k < nsing ? 1.0 : -1.0, dtot, hi, t_per_j, drows, drows, 0, ld};
+        L->blocks.push_back(blk);
+        dtot += n * ld;
         drows += n;
-        t_per_j += n * n;
+        t_per_j += n * ld;
         L->flops += 4.0 * (double)nchol * (double)n * (double)n * (double)n;
       }
-      lc_per_j += n * n;
+      lc_per_j += n * ld;
       lrows += n;
       nmax = std::max<long long>(nmax, n);
       L->lbytes += 8.0 * (double)nchol * (double)n * (double)n;

@@ -2526,6 +2526,23 @@ struct tci_ctx {
 };
 
 namespace tci_dev {
+cudaError_t launch_gemm_cp_f64(const DGemmProblem* probs, int nprob, const DGemmSeg* segs, long long ntiles,
+                               cudaStream_t st) {
+  if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
+  constexpr size_t smem = cp_smem_bytes<0>();
+  static bool attr_set[64] = {};  // per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    e = cudaFuncSetAttribute(gemm_cp_f64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  gemm_cp_f64<0><<<(unsigned)ntiles, 256, smem, st>>>(probs, nprob, segs);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gemm_f64(int cfg, const DGemmProblem* probs, int nprob, const DGemmSeg* segs, long long ntiles,
                             cudaStream_t st) {
   if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
