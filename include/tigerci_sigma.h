@@ -255,12 +255,14 @@ void tci_destroy(tci_ctx* ctx);
  * TCI_ERR_TIMEOUT with *status_out the code and *ms_out (may be NULL) the
  * kernel's duration.  The context stays usable. */
 int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out, double* ms_out);
-/* Instruction rate of tcgen05.mma kind::tf32 (M = 128, N = n: 16..256 in
- * steps of 16, K = 8) on this device: one thread per SM issues iters x nacc
- * MMAs back to back into nacc independent TMEM accumulators (nacc x n <=
- * 512 columns) and commits once; *cycles_per_mma = the slowest SM's clock64
- * span / (iters x nacc), from the second of two launches. */
-int tci_selftest_mma_rate(int64_t device, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma);
+/* Instruction rate of tcgen05.mma kind::tf32 (M = m: 64 or 128; N = n:
+ * 16..256 in steps of 16, or 8..256 in steps of 8 for M = 64; K = 8) on this
+ * device: one thread per SM issues iters x nacc MMAs back to back into nacc
+ * independent TMEM accumulators (nacc x n <= 512 columns, nacc x 2 n for
+ * M = 64) and commits once;
+ * *cycles_per_mma = the slowest SM's clock64 span / (iters x nacc), from the
+ * second of two launches. */
+int tci_selftest_mma_rate(int64_t device, int64_t m, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma);
 
 /* ---- A posteriori corrections (calculate_a_posteriori_corrections,
  * tiger_fortran/aposteriori.f90:28-221, called after a one-root SDCI solve,

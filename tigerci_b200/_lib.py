@@ -167,7 +167,7 @@ def lib():
         L.tci_destroy.argtypes = [P]
         L.tci_destroy.restype = None
         L.tci_selftest_bounded_wait.argtypes = [i64, i64, P, P]
-        L.tci_selftest_mma_rate.argtypes = [i64, i64, i64, i64, P]
+        L.tci_selftest_mma_rate.argtypes = [i64, i64, i64, i64, i64, P]
         L.tci_operator_from_records.argtypes = [i64, i64, P, P, i64, P]
         L.tci_reference_weight.argtypes = [P, P, i64, P]
         L.tci_aposteriori.argtypes = [i64, dbl, dbl, P, i64]

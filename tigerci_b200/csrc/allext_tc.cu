@@ -506,13 +506,13 @@ __global__ void bounded_wait_selftest(int* __restrict__ status, long long polls)
   __syncthreads();
 }
 
-// Self-test of the MMA instruction rate: one thread per CTA issues iters x nacc kind::tf32 MMAs (M = 128,
-// N = n, K = 8, operands zero in shared memory) back to back into nacc independent TMEM accumulators of n
+// Self-test of the MMA instruction rate: one thread per CTA issues iters x nacc kind::tf32 MMAs (M = m, 64 or
+// 128, N = n, K = 8, operands zero in shared memory) back to back into nacc independent TMEM accumulators of n
 // columns, commits once and waits (bounded); cycles[cta] = clock64 span.  One CTA per SM (the shared memory
 // request keeps a second one off the SM, so the 512-column TMEM allocation never waits on another CTA).
 constexpr int RATE_SMEM = 120 * 1024;
-__global__ void __launch_bounds__(128, 1) mma_rate_selftest(int n, int nacc, int iters, long long* __restrict__ cycles,
-                                                           int* __restrict__ status) {
+__global__ void __launch_bounds__(128, 1) mma_rate_selftest(int m, int n, int nacc, int iters,
+                                                           long long* __restrict__ cycles, int* __restrict__ status) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* A = base;          // 128 rows x 128 bytes
@@ -535,10 +535,10 @@ __global__ void __launch_bounds__(128, 1) mma_rate_selftest(int n, int nacc, int
   const uint32_t tmem = *slot;
   if (threadIdx.x == 0) {
     const uint64_t a = smem_desc_sw128(A), b = smem_desc_sw128(B);
-    const uint32_t id = idesc_tf32(128, n);
+    const uint32_t id = idesc_tf32(m, n);
     const long long t0 = clock64();
     for (int i = 0; i < iters; ++i)
-      for (int q = 0; q < nacc; ++q) mma_tf32(tmem + (uint32_t)(q * n), a, b, id, i > 0 ? 1u : 0u);
+      for (int q = 0; q < nacc; ++q) mma_tf32(tmem + (uint32_t)(q * n * (m == 64 ? 2 : 1)), a, b, id, i > 0 ? 1u : 0u);
     mma_commit(bar);
     bool ok = mbar_wait(bar, 0);
     if (!ok) ok = mbar_wait(bar, 0);
@@ -630,8 +630,8 @@ cudaError_t bounded_wait_selftest(int64_t polls, int* status, cudaStream_t st) {
 }
 int64_t spin_limit() { return tci_tcx::SPIN_LIMIT; }
 
-cudaError_t mma_rate_selftest(int64_t n, int64_t nacc, int64_t iters, int grid, long long* cycles, int* status,
-                              cudaStream_t st) {
+cudaError_t mma_rate_selftest(int64_t m, int64_t n, int64_t nacc, int64_t iters, int grid, long long* cycles,
+                              int* status, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(tci_tc::mma_rate_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -639,7 +639,8 @@ cudaError_t mma_rate_selftest(int64_t n, int64_t nacc, int64_t iters, int grid, 
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  tci_tc::mma_rate_selftest<<<grid, 128, tci_tc::RATE_SMEM, st>>>((int)n, (int)nacc, (int)iters, cycles, status);
+  tci_tc::mma_rate_selftest<<<grid, 128, tci_tc::RATE_SMEM, st>>>((int)m, (int)n, (int)nacc, (int)iters, cycles,
+                                                                  status);
   return cudaGetLastError();
 }
 

@@ -34,10 +34,11 @@ bool prepare(AllextTc& t, const float* w32, int64_t np, const float* u2, int64_t
 // can never complete records its timeout code in *status and returns.
 cudaError_t bounded_wait_selftest(int64_t polls, int* status, cudaStream_t st);
 int64_t spin_limit();  // the polls of the kernels' bounded waits
-// Self-test of the kind::tf32 MMA instruction rate (M = 128, N = n in 16..256 step 16, nacc independent
-// accumulators, nacc * n <= 512): cycles[cta] for iters * nacc back-to-back MMAs, one CTA per SM, grid CTAs.
-cudaError_t mma_rate_selftest(int64_t n, int64_t nacc, int64_t iters, int grid, long long* cycles, int* status,
-                              cudaStream_t st);
+// Self-test of the kind::tf32 MMA instruction rate (M = m, 64 or 128; N = n in 16..256 step 16 (8..256 step 8
+// for M = 64); nacc independent accumulators, nacc * n <= 512): cycles[cta] for iters * nacc back-to-back
+// MMAs, one CTA per SM, grid CTAs.
+cudaError_t mma_rate_selftest(int64_t m, int64_t n, int64_t nacc, int64_t iters, int grid, long long* cycles,
+                              int* status, cudaStream_t st);
 // Both products in one launch (either may be null; they must share the status
 // word and promotion block).  Persistent: at most one CTA per SM.
 cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st);

@@ -3645,8 +3645,10 @@ int tci_selftest_bounded_wait(int64_t device, int64_t polls, int64_t* status_out
   }
 }
 
-int tci_selftest_mma_rate(int64_t device, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma) {
-  if (!cycles_per_mma || n < 16 || n > 256 || n % 16 || nacc < 1 || nacc * n > 512 || iters < 1 || iters > (1 << 20))
+int tci_selftest_mma_rate(int64_t device, int64_t m, int64_t n, int64_t nacc, int64_t iters, double* cycles_per_mma) {
+  // M = 64 accumulators are given twice the TMEM columns of their N (the half-lane layouts use up to 2 N)
+  if (!cycles_per_mma || (m != 64 && m != 128) || n > 256 || n < (m == 64 ? 8 : 16) || n % (m == 64 ? 8 : 16) ||
+      nacc < 1 || nacc * n * (m == 64 ? 2 : 1) > 512 || iters < 1 || iters > (1 << 20))
     return TCI_ERR_ARG;
   int* st = nullptr;
   long long* cyc = nullptr;
@@ -3669,7 +3671,7 @@ int tci_selftest_mma_rate(int64_t device, int64_t n, int64_t nacc, int64_t iters
     TCI_CUDA(cudaMemsetAsync(st, 0, sizeof(int), s));
     std::vector<long long> h((size_t)grid);
     for (int rep = 0; rep < 2; ++rep)  // the first launch warms up; the second is read
-      TCI_CUDA(tci_tc_host::mma_rate_selftest(n, nacc, iters, grid, cyc, st, s));
+      TCI_CUDA(tci_tc_host::mma_rate_selftest(m, n, nacc, iters, grid, cyc, st, s));
     int hs = 0;
     TCI_CUDA(cudaMemcpyAsync(h.data(), cyc, sizeof(long long) * (size_t)grid, cudaMemcpyDeviceToHost, s));
     TCI_CUDA(cudaMemcpyAsync(&hs, st, sizeof(int), cudaMemcpyDeviceToHost, s));
