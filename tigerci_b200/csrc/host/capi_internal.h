@@ -31,7 +31,13 @@ struct LocalSetup {
 };
 void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls);
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
-                  tci_ctx** out, int64_t refine = 2, LocalSetup* ls = nullptr);
+                  tci_ctx** out, int64_t refine = 2, LocalSetup* ls = nullptr, tci_ctx* started = nullptr);
+// A context started from the operator part of a plan (build_plan_operator_part): buffers of the integral banks
+// allocated, the Cholesky vectors uploaded and the leading set-up steps run, so that the device builds the
+// banks while the host builds the sigma tables; ctx_from_plan(..., started) completes it with the whole plan
+// (and takes ownership of it, also on failure).
+int ctx_begin_operator(const Plan& early, const double* chol, int64_t device, int64_t precision, int64_t kblock,
+                       int64_t refine, tci_ctx** out);
 // Selects the GEMM steps that run on the tensor cores in the mixed form (tci_sigma_init_ex options[2]).
 void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode);
 // Device bytes of such a context: peak during set-up and held afterwards.

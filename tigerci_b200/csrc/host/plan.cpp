@@ -221,6 +221,7 @@ struct Builder {
   static bool has(const Head& h) { return h.kept && h.nsf > 0 && h.off >= 0; }
 
   void run();
+  void run_operator_part();
   void setup_heads();
   void init_steps();
   void allext();
@@ -1520,7 +1521,50 @@ void Builder::run() {
   P.buf_size[BUF_LI] = nint * nint * N;
 }
 
+// The operator part of the plan alone: the set-up steps that depend on the orbital counts and the Cholesky
+// rank only (gather cholesky rows, integral banks, all-external operators), with the sizes of the buffers they
+// use, exactly as run() makes them (run() emits them first).  The device can build the integral banks from
+// these while the host builds the sigma tables.
+void Builder::run_operator_part() {
+  const Deck& d = sp.deck;
+  nint = sp.n_int;
+  n = sp.n_ext;
+  n2 = n * n;
+  nab = n * (n - 1) / 2;
+  N = op.nchol;
+  P.nint = nint;
+  P.n = n;
+  P.nchol = N;
+  P.total_csfs = sp.total_csfs;
+  P.npair_all = d.num_orbitals * (d.num_orbitals + 1) / 2;
+  P.buf_size.assign(NUM_BUFS, 0);
+  offJ = 0;
+  offK = nint * nint * n2;
+  offH = 2 * nint * nint * n2;
+  init_steps();
+  if (with_allext) {
+    P.np = n + nab;
+    P.nm = nab;
+    P.buf_size[BUF_W] = P.np * P.np + P.nm * P.nm;
+    P.buf_size[BUF_X] = (n * (n + 1) / 2) * (n * (n + 1) / 2);
+  }
+  P.buf_size[BUF_T0] = init_scratch;
+  P.buf_size[BUF_JK] = (2 * nint * nint + 1) * n2;
+  P.buf_size[BUF_V] = nint * n * n2;
+  P.buf_size[BUF_L] = P.npair_all * N;
+  P.buf_size[BUF_LE] = nint * n * N;
+  P.buf_size[BUF_LV] = n2 * N;
+  P.buf_size[BUF_LI] = nint * nint * N;
+}
+
 }  // namespace
+
+void build_plan_operator_part(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext) {
+  plan = Plan();
+  Builder b(sp, op, plan);
+  b.with_allext = with_allext;
+  b.run_operator_part();
+}
 
 void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext) {
   plan = Plan();

@@ -172,5 +172,8 @@ struct Operator {
 // the diagonal entries of types 2 and 3 then need the all-external diagonal from elsewhere): the form used
 // under local pair domains, whose all-external term runs in the pair-domain Cholesky form.
 void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext = true);
+// The leading set-up steps of build_plan's plan that need the orbital counts and the Cholesky rank only
+// (gather cholesky rows, integral banks, all-external operators) and the sizes of their buffers.
+void build_plan_operator_part(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext = true);
 
 }  // namespace tci

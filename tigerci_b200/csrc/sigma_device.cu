@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
+#include <array>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -1319,6 +1321,12 @@ struct tci_ctx {
   int* dk_head = nullptr;
   double bytes_held = 0;
   double init_seconds = 0;
+  // set-up started from the operator part of the plan before the whole plan existed (ctx_begin_operator):
+  // the leading set-up steps already run, and their names and table sizes for the check against the plan
+  size_t early_init = 0;
+  std::vector<std::string> early_names;
+  std::vector<std::array<size_t, 4>> early_shapes;
+  std::vector<i64> early_sizes;
   double last_sigma_ms = 0;
   long long sigma_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -2604,8 +2612,28 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
     build_space_from_c(deck, sp);
     Operator o;
     operator_from_c(op, sp, o);
-    build_plan(sp, o, plan);
-    const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out, refine);
+    // The host builds the sigma tables on a second thread while the device builds the integral banks from the
+    // operator part of the plan (the same leading set-up steps the whole plan starts with).
+    Plan early;
+    tci::build_plan_operator_part(sp, o, early);
+    std::exception_ptr plan_error;
+    std::thread planner([&]() {
+      try {
+        build_plan(sp, o, plan);
+      } catch (...) {
+        plan_error = std::current_exception();
+      }
+    });
+    tci_ctx* started = nullptr;
+    const int rc0 = tci::ctx_begin_operator(early, o.chol, device, precision, kblock, refine, &started);
+    planner.join();
+    if (plan_error || rc0 != TCI_OK) {
+      if (started) tci_destroy(started);
+      if (plan_error) std::rethrow_exception(plan_error);
+      return rc0;
+    }
+    const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out, refine,
+                                      nullptr, started);
     if (rc == TCI_OK) (*out)->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return rc;
   } catch (...) {
@@ -2749,8 +2777,123 @@ void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& 
     }
 }
 
+namespace setup {
+// TCI_INIT_TIMING=1 prints the device set-up phases (each ends with a stream synchronisation)
+struct InitTimer {
+  bool on = std::getenv("TCI_INIT_TIMING") != nullptr;
+  std::chrono::steady_clock::time_point tp = std::chrono::steady_clock::now();
+  void operator()(const char* what, cudaStream_t st) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "init %-28s %.3f s\n", what, std::chrono::duration<double>(now - tp).count());
+    tp = now;
+  }
+};
+
+// A context with its device and stream, nothing allocated.
+std::unique_ptr<tci_ctx> new_ctx(int64_t device) {
+  std::unique_ptr<tci_ctx> ctx(new tci_ctx());
+  int ndev = 0;
+  TCI_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) throw Error(TCI_ERR_CUDA, "requested device is not available");
+  ctx->device = (int)device;
+  TCI_CUDA(cudaSetDevice(ctx->device));
+  TCI_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  TCI_CUDA(cudaEventCreate(&ctx->ev0));
+  TCI_CUDA(cudaEventCreate(&ctx->ev1));
+  return ctx;
+}
+
+// Allocates (zeroed) every buffer of the context's plan that is not allocated yet.
+void alloc_plan_buffers(tci_ctx* ctx) {
+  const Plan& P = ctx->plan;
+  for (int b = 0; b < NUM_BUFS; ++b) {
+    if (P.buf_size[b] <= 0 || ctx->buf[b]) continue;
+    cudaError_t e = dev_malloc(&ctx->buf[b], P.buf_size[b] * sizeof(double), ctx->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+    }
+    // plan steps accumulate into their targets: every buffer starts at zero
+    TCI_CUDA(cudaMemsetAsync(ctx->buf[b], 0, P.buf_size[b] * sizeof(double), ctx->stream));
+    ctx->bytes_held += (double)P.buf_size[b] * sizeof(double);
+  }
+}
+
+// Lowers and runs the plan's set-up steps from index `first` on.  In the mixed form without the plain-FP64
+// finish the exchange product X = Lpk Lpk^T of the all-external operators (the largest set-up GEMM,
+// 2 npk^2 N flops) runs on the TMA-fed tensor-core kernel; its 3xTF32 error is of the order of W's own FP32
+// rounding in that form.  The other banks stay FP64.
+void run_init_steps(tci_ctx* ctx, size_t first, bool x_tc, int64_t kblock, InitTimer& phase) {
+  const Plan& P = ctx->plan;
+  GemmProblem xg{};
+  GemmSeg xs{};
+  bool have_x = false;
+  size_t banks = (size_t)-1;
+  const size_t lowered0 = ctx->init.size();
+  for (size_t i = first; i < P.init_steps.size(); ++i) {
+    const Step& s = P.init_steps[i];
+    if (x_tc && s.kind == STEP_GEMM && s.name == "integral banks") {
+      Step s2 = s;
+      for (size_t g = 0; g < s2.gp.size(); ++g)
+        if (s2.gp[g].c == BUF_X && s2.gp[g].seg_end - s2.gp[g].seg_begin == 1) {
+          xg = s2.gp[g];
+          xs = s2.gs[(size_t)xg.seg_begin];
+          s2.gp.erase(s2.gp.begin() + (long)g);
+          have_x = xs.a == BUF_T0 && xs.b == BUF_T0 && xs.offA == xs.offB && !xs.tA && xs.tB && xg.M == xg.N;
+          if (!have_x) s2 = s;  // not the expected shape: leave it on the FP64 kernel
+          break;
+        }
+      banks = ctx->init.size();
+      ctx->init.push_back(ctx->lower(s2));
+      continue;
+    }
+    ctx->init.push_back(ctx->lower(s));
+  }
+  phase("lowering (set-up steps)", ctx->stream);
+  for (size_t i = lowered0; i < ctx->init.size(); ++i) {
+    ctx->run(ctx->init[i]);
+    phase(ctx->init[i].name.c_str(), ctx->stream);
+    if (i == banks && have_x) {
+      ctx->exchange_product_tc(xg, xs, kblock);
+      phase("exchange product (tcgen05)", ctx->stream);
+    }
+  }
+}
+}  // namespace setup
+using setup::InitTimer;
+
+int ctx_begin_operator(const Plan& early, const double* chol, int64_t device, int64_t precision, int64_t kblock,
+                       int64_t refine, tci_ctx** out) {
+  if (!out || !chol) return TCI_ERR_ARG;
+  *out = nullptr;
+  try {
+    InitTimer phase;
+    std::unique_ptr<tci_ctx> ctx = setup::new_ctx(device);
+    ctx->plan = early;
+    setup::alloc_plan_buffers(ctx.get());
+    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_L], chol, early.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    phase("operator buffers and upload", ctx->stream);
+    setup::run_init_steps(ctx.get(), 0, precision == 1 && refine != 1, kblock, phase);
+    TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->early_init = early.init_steps.size();
+    for (const auto& st : early.init_steps) {
+      ctx->early_names.push_back(st.name);
+      ctx->early_shapes.push_back({st.gp.size(), st.gs.size(), st.at.size(), st.as.size()});
+    }
+    ctx->early_sizes = early.buf_size;
+    *out = ctx.release();
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
-                  tci_ctx** out, int64_t refine, LocalSetup* ls) {
+                  tci_ctx** out, int64_t refine, LocalSetup* ls, tci_ctx* started) {
+  std::unique_ptr<tci_ctx> ctx(started);
   if (!out || !chol) return TCI_ERR_ARG;
   *out = nullptr;
   if (precision < 0 || precision > 1) {
@@ -2759,42 +2902,50 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
   }
   try {
     auto t0 = std::chrono::steady_clock::now();
-    // TCI_INIT_TIMING=1 prints the device set-up phases (each ends with a stream synchronisation)
-    const bool timing = std::getenv("TCI_INIT_TIMING") != nullptr;
-    auto tp = t0;
-    auto phase = [&](const char* what, cudaStream_t st) {
-      if (!timing) return;
-      cudaStreamSynchronize(st);
-      const auto now = std::chrono::steady_clock::now();
-      std::fprintf(stderr, "init %-28s %.3f s\n", what, std::chrono::duration<double>(now - tp).count());
-      tp = now;
-    };
-    std::unique_ptr<tci_ctx> ctx(new tci_ctx());
-    int ndev = 0;
-    TCI_CUDA(cudaGetDeviceCount(&ndev));
-    if (device < 0 || device >= ndev) throw Error(TCI_ERR_CUDA, "requested device is not available");
-    ctx->device = (int)device;
-    TCI_CUDA(cudaSetDevice(ctx->device));
-    TCI_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    TCI_CUDA(cudaEventCreate(&ctx->ev0));
-    TCI_CUDA(cudaEventCreate(&ctx->ev1));
-    ctx->sp = std::move(sp);
-    ctx->plan = std::move(plan);
-    Plan& P = ctx->plan;
-    for (int b = 0; b < NUM_BUFS; ++b) {
-      if (P.buf_size[b] <= 0) continue;
-      cudaError_t e = dev_malloc(&ctx->buf[b], P.buf_size[b] * sizeof(double), ctx->stream);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+    InitTimer phase;
+    const bool timing = phase.on;
+    if (ctx) {
+      // set-up started from the operator part: its steps must be the plan's leading ones, its buffers the
+      // plan's (the scratch buffer grows when the sigma steps need more)
+      if (ls || ctx->device != (int)device) throw Error(TCI_ERR_INTERNAL, "started context does not fit the plan");
+      TCI_CUDA(cudaSetDevice(ctx->device));
+      if (plan.init_steps.size() < ctx->early_init) throw Error(TCI_ERR_INTERNAL, "plan lacks the started steps");
+      for (size_t i = 0; i < ctx->early_init; ++i) {
+        const Step& st = plan.init_steps[i];
+        const std::array<size_t, 4> sh{st.gp.size(), st.gs.size(), st.at.size(), st.as.size()};
+        if (st.name != ctx->early_names[i] || sh != ctx->early_shapes[i])
+          throw Error(TCI_ERR_INTERNAL, "started set-up steps differ from the plan's");
       }
-      // plan steps accumulate into their targets: every buffer starts at zero
-      TCI_CUDA(cudaMemsetAsync(ctx->buf[b], 0, P.buf_size[b] * sizeof(double), ctx->stream));
-      ctx->bytes_held += (double)P.buf_size[b] * sizeof(double);
+      for (int b = 0; b < NUM_BUFS; ++b) {
+        if (!ctx->buf[b]) continue;
+        if (b == BUF_T0 && plan.buf_size[b] > ctx->early_sizes[b]) {
+          std::lock_guard<std::mutex> lk(g_capture_free_mu);
+          TCI_CUDA(dev_free(ctx->buf[b], ctx->stream));
+          ctx->bytes_held -= (double)ctx->early_sizes[b] * sizeof(double);
+          ctx->buf[b] = nullptr;
+        } else if (plan.buf_size[b] != ctx->early_sizes[b] && b != BUF_T0) {
+          throw Error(TCI_ERR_INTERNAL, "started buffer sizes differ from the plan's");
+        }
+      }
+    } else {
+      ctx = setup::new_ctx(device);
     }
+    ctx->sp = std::move(sp);
+    const size_t started_steps = ctx->early_init;
+    if (started_steps) {
+      // the plan's scratch size may be larger; every other size equals the started one
+      const i64 t0size = std::max(plan.buf_size[BUF_T0], ctx->early_sizes[BUF_T0]);
+      ctx->plan = std::move(plan);
+      if (ctx->buf[BUF_T0]) ctx->plan.buf_size[BUF_T0] = t0size;
+    } else {
+      ctx->plan = std::move(plan);
+    }
+    Plan& P = ctx->plan;
+    setup::alloc_plan_buffers(ctx.get());
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
-    TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_L], chol, P.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice,
-                             ctx->stream));
+    if (!started_steps)
+      TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_L], chol, P.buf_size[BUF_L] * sizeof(double), cudaMemcpyHostToDevice,
+                               ctx->stream));
     TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_JK] + 2 * P.nint * P.nint * P.n * P.n, P.h_vv.data(),
                              P.h_vv.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     if (!P.wv.empty())
@@ -2830,33 +2981,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
       TCI_CUDA(cudaSetDevice(ctx->device));
     }
     phase("buffers and uploads", ctx->stream);
-    // Mixed form without the plain-FP64 finish: the exchange product X = Lpk Lpk^T of the all-external
-    // operators (the largest set-up GEMM, 2 npk^2 N flops) runs on the TMA-fed tensor-core kernel; its
-    // 3xTF32 error is of the order of W's own FP32 rounding in that form.  The other banks stay FP64.
-    const bool x_tc = precision == 1 && refine != 1;
-    GemmProblem xg{};
-    GemmSeg xs{};
-    bool have_x = false;
-    size_t banks = (size_t)-1;
     ctx->f_on_tc = precision == 1 && refine != 0;
-    for (auto& s : P.init_steps) {
-      if (x_tc && s.kind == STEP_GEMM && s.name == "integral banks") {
-        Step s2 = s;
-        for (size_t g = 0; g < s2.gp.size(); ++g)
-          if (s2.gp[g].c == BUF_X && s2.gp[g].seg_end - s2.gp[g].seg_begin == 1) {
-            xg = s2.gp[g];
-            xs = s2.gs[(size_t)xg.seg_begin];
-            s2.gp.erase(s2.gp.begin() + (long)g);
-            have_x = xs.a == BUF_T0 && xs.b == BUF_T0 && xs.offA == xs.offB && !xs.tA && xs.tB && xg.M == xg.N;
-            if (!have_x) s2 = s;  // not the expected shape: leave it on the FP64 kernel
-            break;
-          }
-        banks = ctx->init.size();
-        ctx->init.push_back(ctx->lower(s2));
-        continue;
-      }
-      ctx->init.push_back(ctx->lower(s));
-    }
     for (auto& s : P.sigma_steps) {
       if (ls && s.kind == STEP_GEMM && s.name == "dd two-external")
         ctx->sigma.push_back(ctx->lower_dom(s, *ls));
@@ -2864,19 +2989,12 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
         ctx->sigma.push_back(ctx->lower(s));
       if (timing) {  // the σ steps whose tables take a noticeable time
         cudaStreamSynchronize(ctx->stream);
-        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - phase.tp).count();
         if (dt > 0.002) phase(("  lowering " + s.name).c_str(), ctx->stream);
       }
     }
     phase("lowering (step tables)", ctx->stream);
-    for (size_t i = 0; i < ctx->init.size(); ++i) {
-      ctx->run(ctx->init[i]);
-      phase(ctx->init[i].name.c_str(), ctx->stream);
-      if (i == banks && have_x) {
-        ctx->exchange_product_tc(xg, xs, kblock);
-        phase("exchange product (tcgen05)", ctx->stream);
-      }
-    }
+    setup::run_init_steps(ctx.get(), started_steps, precision == 1 && refine != 1, kblock, phase);
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
     // init-only buffers
     for (int b : {BUF_X, BUF_L, BUF_LE, BUF_LI}) {
