@@ -28,6 +28,10 @@ struct LocalSetup {
   // domain (sorted externals); length 0 for a head without local CSFs
   std::vector<int64_t> dh_off, dh_len;
   std::vector<int> dh_dom;
+  // the N-1 heads of the non-local plan: CSF rows [s1_begin, s1_end) of each head (one row of n externals
+  // per spin function) and the slice of s1_dom holding its local domain (length 0: no local CSFs)
+  std::vector<int64_t> s1_begin, s1_end, s1_off, s1_len;
+  std::vector<int> s1_dom;
 };
 void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls);
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,

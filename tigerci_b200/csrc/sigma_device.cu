@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -501,6 +502,113 @@ __global__ void __launch_bounds__(DOM_THREADS) gemm_dom_f64(const DDomProblem* _
       if (j < P.m) row[P.dom[j]] += acc[r][c];
     }
   }
+}
+
+// Domain-restricted three-external products of a local deck (pair domains), on the padded pair matrices and
+// the (iq|bs) banks V_i[b][q n + s] (the reference's local three-external gathers, iabc_sig_cho_big_res,
+// three_and_four_seg_mod_1.f90:1099-1376). The pair matrices of an N-2 head lambda are zero outside
+// D_lambda x D_lambda and only the rows b in D_mu of the N-1 head mu = lambda + e_i reach the local sigma, so
+//   forward  Y_(i,dk)[b] = sum_{q,s in D_lambda} V_i[b][q n + s] D_dk[q][s]          (b in D_mu)
+//   reverse  R_dk[q][s] += sum_i sum_{b in D_mu(i)} U_(i,dk)[b] V_i[b][q n + s]       (q, s in D_lambda)
+// with Y_(i,dk) the row (i nD + dk) n of Y and U_(i,dk) that of U. The pair matrices of one head share its
+// domain: a unit takes up to D3_K of them, so each V_i element it reads serves all. Sums in a fixed order.
+constexpr int D3_K = 4;   // pair matrices (dk) of one head per unit
+constexpr int D3_QC = 8;  // rows q of the D_dk staged in shared memory per pass (forward)
+struct D3Fwd {
+  long long i, dk0;
+  const int* dl;  // D_lambda (sorted externals)
+  const int* dm;  // D_mu
+  int ml, mm, nk;
+};
+struct D3Rev {
+  long long dk0, tile_begin;
+  const int* dl;
+  int ml, nk;
+  long long e_begin, e_end;  // its (i, D_mu) entries
+};
+struct D3RevEntry {
+  long long i;
+  const int* dm;
+  int mm;
+};
+constexpr int D3R_T = 256;  // outputs (q, s) per reverse tile
+__global__ void __launch_bounds__(256) dom3_forward(const D3Fwd* __restrict__ units, const double* __restrict__ V,
+                                                    const double* __restrict__ D, double* __restrict__ Y, long long n,
+                                                    long long nD) {
+  extern __shared__ double d3_smem[];
+  const D3Fwd u = units[blockIdx.x];
+  double* ds = d3_smem;                        // [D3_K][D3_QC][ml]
+  double* yacc = d3_smem + D3_K * D3_QC * u.ml;  // [D3_K][mm]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  const long long n2 = n * n;
+  const double* Vi = V + u.i * n * n2;
+  for (int e = threadIdx.x; e < D3_K * u.mm; e += blockDim.x) yacc[e] = 0.0;
+  for (int q0 = 0; q0 < u.ml; q0 += D3_QC) {
+    const int nq = min(D3_QC, u.ml - q0);
+    __syncthreads();  // the previous pass's reads of ds are done
+    for (int e = threadIdx.x; e < u.nk * nq * u.ml; e += blockDim.x) {
+      const int k = e / (nq * u.ml), r = e - k * (nq * u.ml);
+      const int qq = r / u.ml, sidx = r - qq * u.ml;
+      ds[(k * D3_QC + qq) * u.ml + sidx] = D[(u.dk0 + k) * n2 + (long long)u.dl[q0 + qq] * n + u.dl[sidx]];
+    }
+    __syncthreads();
+    for (int b = warp; b < u.mm; b += nwarp) {
+      const double* vrow = Vi + (long long)u.dm[b] * n2;
+      double part[D3_K] = {0.0, 0.0, 0.0, 0.0};
+      for (int qq = 0; qq < nq; ++qq) {
+        const double* vq = vrow + (long long)u.dl[q0 + qq] * n;
+        for (int sidx = lane; sidx < u.ml; sidx += 32) {
+          const double v = vq[u.dl[sidx]];
+#pragma unroll
+          for (int k = 0; k < D3_K; ++k)
+            if (k < u.nk) part[k] = fma(v, ds[(k * D3_QC + qq) * u.ml + sidx], part[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < D3_K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part[k] += __shfl_xor_sync(0xffffffffu, part[k], o);
+      }
+      if (lane == 0)
+        for (int k = 0; k < u.nk; ++k) yacc[k * u.mm + b] += part[k];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < u.nk * u.mm; e += blockDim.x) {
+    const int k = e / u.mm, b = e - k * u.mm;
+    Y[(u.i * nD + u.dk0 + k) * n + u.dm[b]] = yacc[k * u.mm + b];
+  }
+}
+__global__ void __launch_bounds__(D3R_T) dom3_reverse(const D3Rev* __restrict__ units, int nunit,
+                                                      const D3RevEntry* __restrict__ ent,
+                                                      const double* __restrict__ V, const double* __restrict__ U,
+                                                      double* __restrict__ R, long long n, long long nD) {
+  int lo = 0, hi = nunit - 1;  // the unit of this tile: the last with tile_begin <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (units[mid].tile_begin <= (long long)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const D3Rev u = units[lo];
+  const int e = (int)(((long long)blockIdx.x - u.tile_begin) * D3R_T) + threadIdx.x;
+  if (e >= u.ml * u.ml) return;
+  const long long n2 = n * n;
+  const int q = e / u.ml, sidx = e - q * u.ml;
+  const long long col = (long long)u.dl[q] * n + u.dl[sidx];
+  double acc[D3_K] = {0.0, 0.0, 0.0, 0.0};
+  for (long long p = u.e_begin; p < u.e_end; ++p) {
+    const D3RevEntry E = ent[p];
+    const double* vcol = V + E.i * n * n2 + col;
+    const double* urow = U + (E.i * nD + u.dk0) * n;
+    for (int b = 0; b < E.mm; ++b) {
+      const int bb = E.dm[b];
+      const double v = vcol[(long long)bb * n2];
+#pragma unroll
+      for (int k = 0; k < D3_K; ++k)
+        if (k < u.nk) acc[k] = fma(urow[k * n + bb], v, acc[k]);
+    }
+  }
+  for (int k = 0; k < u.nk; ++k) R[(u.dk0 + k) * n2 + col] += acc[k];
 }
 
 // Row-panel FP64 GEMM for problems with few rows and long rows of B (the all-external product Y = U W: a
@@ -1282,6 +1390,18 @@ struct DevStep {
   DDomSeg* dom_segs = nullptr;
   int dom_nprob = 0;
   long long dom_ntiles = 0;
+  // local decks: the three-external term on the domains (dom3_forward in place of the split-k sum,
+  // dom3_reverse in place of the reverse GEMM); d3_skip marks the padded forward GEMM they replace
+  bool d3_skip = false;
+  int d3 = 0;  // 1: dom3_forward, 2: dom3_reverse
+  D3Fwd* d3f = nullptr;
+  long long d3f_n = 0;
+  size_t d3f_smem = 0;
+  D3Rev* d3r = nullptr;
+  D3RevEntry* d3e = nullptr;
+  int d3r_n = 0;
+  long long d3r_tiles = 0;
+  double* d3_rows = nullptr;  // forward: Y (output); reverse: U (input)
   // AXPY / DOT
   DAxpyTarget* at = nullptr;
   DAxpySource* as = nullptr;
@@ -1692,6 +1812,108 @@ struct tci_ctx {
     return d;
   }
 
+  // The three-external term of a local deck on the domains. Units come from the reverse gather step: each of
+  // its targets is the row U_(i,dk) (one (i, dk) with a nonzero coupling), its sources the CSF rows of the N-1
+  // head mu = lambda + e_i. The zero, scatter and gather steps stay as they are. Returns false (the padded
+  // steps stay) when the plan has no three-external term or a domain is too wide for the staging.
+  bool lower_dom3(const std::vector<Step>& steps, const tci::LocalSetup& ls, DevStep& fwd, DevStep& rev) {
+    const i64 n = plan.n, n2 = n * n, nD = plan.nD, nint = plan.nint;
+    const Step *zy = nullptr, *zu = nullptr, *ga = nullptr;
+    for (const auto& s : steps) {
+      if (s.name == "three-external zero") zy = &s;
+      if (s.name == "three-external reverse zero") zu = &s;
+      if (s.name == "three-external reverse gather") ga = &s;
+    }
+    if (!zy || !zu || !ga || nD == 0) return false;
+    if (zy->buf != BUF_T0 || zu->buf != BUF_T0 || zy->len != nint * nD * n || zu->len != nint * nD * n)
+      throw Error(TCI_ERR_INTERNAL, "unexpected three-external row buffers");
+    const size_t nh1 = ls.s1_begin.size();
+    if (ls.s1_end.size() != nh1 || ls.s1_off.size() != nh1 || ls.s1_len.size() != nh1 ||
+        ls.dh_len.size() != plan.dheads.size())
+      throw Error(TCI_ERR_INTERNAL, "local domains do not match the plan's heads");
+    for (int x : ls.s1_dom)
+      if (x < 0 || x >= n) throw Error(TCI_ERR_INTERNAL, "local domain entry outside the externals");
+    for (size_t h = 0; h < nh1; ++h)
+      if (ls.s1_len[h] < 0 || ls.s1_len[h] > n || ls.s1_off[h] + ls.s1_len[h] > (i64)ls.s1_dom.size())
+        throw Error(TCI_ERR_INTERNAL, "local domain slice out of range");
+    std::vector<std::pair<i64, size_t>> by_begin;  // N-1 heads by their first CSF row
+    for (size_t h = 0; h < nh1; ++h) by_begin.push_back({ls.s1_begin[h], h});
+    std::sort(by_begin.begin(), by_begin.end());
+    auto mu_of = [&](i64 row) -> size_t {
+      auto it = std::upper_bound(by_begin.begin(), by_begin.end(), std::make_pair(row, (size_t)-1));
+      if (it == by_begin.begin()) throw Error(TCI_ERR_INTERNAL, "three-external row outside the N-1 heads");
+      const size_t h = std::prev(it)->second;
+      if (row >= ls.s1_end[h] || (row - ls.s1_begin[h]) % n) throw Error(TCI_ERR_INTERNAL, "three-external row outside the N-1 heads");
+      return h;
+    };
+    std::vector<i64> dk2h((size_t)nD, -1);
+    for (size_t h = 0; h < plan.dheads.size(); ++h)
+      for (i64 k = 0; k < plan.dheads[h].nD; ++k) dk2h[(size_t)(plan.dheads[h].dk0 + k)] = (i64)h;
+    std::map<std::pair<i64, i64>, size_t> mu;  // (lambda head, i) -> mu head
+    for (const auto& t : ga->at) {
+      const i64 rel = t.off - zu->off;
+      if (t.dst != BUF_T0 || t.len != n || rel < 0 || rel % n || rel / n >= nint * nD)
+        throw Error(TCI_ERR_INTERNAL, "unexpected three-external gather target");
+      const i64 i = (rel / n) / nD, dk = (rel / n) % nD, h = dk2h[(size_t)dk];
+      if (h < 0) throw Error(TCI_ERR_INTERNAL, "three-external row of no pair matrix");
+      for (i64 q = t.src_begin; q < t.src_end; ++q) {
+        const AxpySource& x = ga->as[(size_t)q];
+        if (x.src != BUF_C || x.sbuf >= 0) throw Error(TCI_ERR_INTERNAL, "unexpected three-external gather source");
+        const size_t m = mu_of(x.off);
+        auto ins = mu.insert({{h, i}, m});
+        if (ins.first->second != m) throw Error(TCI_ERR_INTERNAL, "three-external coupling of two N-1 heads");
+      }
+    }
+    check_range(BUF_V, 0, nint * n * n2);
+    check_range(BUF_D, 0, nD * n2);
+    check_range(BUF_R, 0, nD * n2);
+    const int* ddl = upload(ls.dh_dom, owned, stream);
+    const int* ddm = upload(ls.s1_dom, owned, stream);
+    std::vector<D3Fwd> fu;
+    std::vector<D3Rev> ru;
+    std::vector<D3RevEntry> re;
+    i64 max_ml = 0, max_mm = 0, tiles = 0;
+    for (auto it = mu.begin(); it != mu.end();) {
+      const i64 h = it->first.first;
+      const i64 ml = ls.dh_len[(size_t)h], dk0 = plan.dheads[(size_t)h].dk0, nh = plan.dheads[(size_t)h].nD;
+      const long long e0 = (long long)re.size();
+      for (; it != mu.end() && it->first.first == h; ++it) {
+        const i64 i = it->first.second, mm = ls.s1_len[it->second];
+        if (ml == 0 || mm == 0) continue;
+        re.push_back(D3RevEntry{i, ddm + ls.s1_off[it->second], (int)mm});
+        max_mm = std::max(max_mm, mm);
+        for (i64 c = 0; c < nh; c += D3_K)
+          fu.push_back(D3Fwd{i, dk0 + c, ddl + ls.dh_off[(size_t)h], ddm + ls.s1_off[it->second], (int)ml, (int)mm,
+                             (int)std::min<i64>(D3_K, nh - c)});
+      }
+      if ((long long)re.size() == e0) continue;
+      max_ml = std::max(max_ml, ml);
+      for (i64 c = 0; c < nh; c += D3_K) {
+        ru.push_back(D3Rev{dk0 + c, tiles, ddl + ls.dh_off[(size_t)h], (int)ml, (int)std::min<i64>(D3_K, nh - c), e0,
+                           (long long)re.size()});
+        tiles += (ml * ml + D3R_T - 1) / D3R_T;
+      }
+    }
+    const size_t smem = (size_t)(D3_K * D3_QC * max_ml + D3_K * max_mm) * sizeof(double);
+    if (smem > 200 * 1024) return false;
+    fwd.d3 = 1;
+    fwd.kind = STEP_AXPY;
+    fwd.name = "three-external split-k sum";
+    fwd.d3f = upload(fu, owned, stream);
+    fwd.d3f_n = (long long)fu.size();
+    fwd.d3f_smem = smem;
+    fwd.d3_rows = ptr(BUF_T0, zy->off);
+    rev.d3 = 2;
+    rev.kind = STEP_GEMM;
+    rev.name = "three-external reverse";
+    rev.d3r = upload(ru, owned, stream);
+    rev.d3e = upload(re, owned, stream);
+    rev.d3r_n = (int)ru.size();
+    rev.d3r_tiles = tiles;
+    rev.d3_rows = ptr(BUF_T0, zu->off);
+    return true;
+  }
+
   // local decks: the padded positions of the local CSFs, sorted (empty otherwise)
   std::vector<long long> loc_pos;
   bool any_local(i64 off, i64 len) const {
@@ -2079,6 +2301,11 @@ struct tci_ctx {
         k += s.dom_ntiles > 0 ? 1 : 0;
         continue;
       }
+      if (s.d3_skip) continue;
+      if (s.d3) {
+        k += (s.d3f_n > 0 || s.d3r_tiles > 0) ? 1 : 0;
+        continue;
+      }
       const bool tc_allext = precision == 1 || allext_tc_in_fp64;
       if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) continue;
       if (tc_allext && s.kind == STEP_GEMM && s.name == "all-external") {
@@ -2427,6 +2654,27 @@ struct tci_ctx {
     // the tensor-core form writes the all-external products directly
     const bool tc_allext = precision == 1 || allext_tc_in_fp64;
     if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
+    if (s.d3_skip) return;
+    if (s.d3 == 1) {  // local deck: the forward three-external term on the domains
+      if (s.d3f_n > 0) {
+        static bool attr_set[64] = {};
+        int dev = 0;
+        TCI_CUDA(cudaGetDevice(&dev));
+        if (s.d3f_smem > 48 * 1024 && dev < 64 && !attr_set[dev]) {
+          TCI_CUDA(cudaFuncSetAttribute(dom3_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+          attr_set[dev] = true;
+        }
+        dom3_forward<<<(unsigned)s.d3f_n, 256, s.d3f_smem, stream>>>(s.d3f, buf[BUF_V], buf[BUF_D], s.d3_rows, plan.n,
+                                                                    plan.nD);
+      }
+      return;
+    }
+    if (s.d3 == 2) {  // local deck: the reverse three-external term on the domains
+      if (s.d3r_tiles > 0)
+        dom3_reverse<<<(unsigned)s.d3r_tiles, D3R_T, 0, stream>>>(s.d3r, s.d3r_n, s.d3e, buf[BUF_V], s.d3_rows,
+                                                                  buf[BUF_R], plan.n, plan.nD);
+      return;
+    }
     switch (s.kind) {
       case STEP_GEMM:
         if (s.dom_probs) {  // local deck: the two-external step on the domains
@@ -2746,6 +2994,18 @@ void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& 
   }
   for (i64 x : ls.map)
     if (x < 0) throw Error(TCI_ERR_INTERNAL, "a local CSF has no non-local counterpart");
+  // domains of the N-1 heads by their CSF rows in the non-local space
+  for (size_t p = 0; p < nl.paths[1].size(); ++p) {
+    const Head& g = nl.paths[1][p];
+    if (!g.kept || g.off < 0 || g.nsf <= 0) continue;
+    const Head& h = loc.paths[1][p];
+    ls.s1_begin.push_back(g.off);
+    ls.s1_end.push_back(g.off + (i64)g.nsf * n);
+    ls.s1_off.push_back((int64_t)ls.s1_dom.size());
+    if (h.domain >= 0 && h.off >= 0)
+      for (int a : loc.domains[(size_t)h.domain]) ls.s1_dom.push_back(a);
+    ls.s1_len.push_back((int64_t)ls.s1_dom.size() - ls.s1_off.back());
+  }
   // domains of the plan's N-2 heads, in the plan's head order (Builder::setup_heads: kept heads with a
   // pair matrix)
   for (size_t p = 0; p < nl.paths[2].size(); ++p) {
@@ -2982,9 +3242,21 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     }
     phase("buffers and uploads", ctx->stream);
     ctx->f_on_tc = precision == 1 && refine != 0;
+    DevStep d3f, d3r;
+    const bool dom3 = ls && ctx->lower_dom3(P.sigma_steps, *ls, d3f, d3r);
     for (auto& s : P.sigma_steps) {
       if (ls && s.kind == STEP_GEMM && s.name == "dd two-external")
         ctx->sigma.push_back(ctx->lower_dom(s, *ls));
+      else if (dom3 && s.name == "three-external forward") {
+        DevStep d;
+        d.kind = s.kind;
+        d.name = s.name;
+        d.d3_skip = true;
+        ctx->sigma.push_back(d);
+      } else if (dom3 && s.name == "three-external split-k sum")
+        ctx->sigma.push_back(d3f);
+      else if (dom3 && s.name == "three-external reverse")
+        ctx->sigma.push_back(d3r);
       else
         ctx->sigma.push_back(ctx->lower(s));
       if (timing) {  // the σ steps whose tables take a noticeable time
