@@ -611,6 +611,65 @@ __global__ void __launch_bounds__(D3R_T) dom3_reverse(const D3Rev* __restrict__ 
   for (int k = 0; k < u.nk; ++k) R[(u.dk0 + k) * n2 + col] += acc[k];
 }
 
+// The N-2 <-> valence exchange term of a local deck on the domains (the reference's local dv loops,
+// three_and_four_seg_mod_2.f90:8007-8165): only the entries (pq, dk) that the plan's couplings use, each over
+// D_lambda x D_lambda of the head lambda of dk, with K_pq the row pq of the exchange bank (n^2 long)
+//   forward  F[pq nD + dk] = sum_{q,s in D_lambda} K_pq[q n + s] D_dk[q][s]
+//   reverse  R_dk[q][s] += sum_pq G[pq nD + dk] K_pq[q n + s]                 (q, s in D_lambda)
+struct DvEntry {
+  long long pq, dk;
+  const int* dl;
+  int ml;
+};
+struct DvTarget {
+  long long dk, tile_begin;
+  const int* dl;
+  int ml;
+  long long e_begin, e_end;  // its entries (pq) in the entry table
+};
+__global__ void __launch_bounds__(256) dom_dv_forward(const DvEntry* __restrict__ ent, long long nent,
+                                                      const double* __restrict__ K, const double* __restrict__ D,
+                                                      double* __restrict__ F, long long n, long long nD) {
+  const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= nent) return;
+  const DvEntry E = ent[w];
+  const long long n2 = n * n;
+  const double* kp = K + E.pq * n2;
+  const double* dp = D + E.dk * n2;
+  double acc = 0.0;
+  for (int q = 0; q < E.ml; ++q) {
+    const long long r = (long long)E.dl[q] * n;
+    for (int sidx = lane; sidx < E.ml; sidx += 32) {
+      const int c = E.dl[sidx];
+      acc = fma(kp[r + c], dp[r + c], acc);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) F[E.pq * nD + E.dk] = acc;
+}
+__global__ void __launch_bounds__(256) dom_dv_reverse(const DvTarget* __restrict__ tg, int ntg,
+                                                      const long long* __restrict__ pqs,
+                                                      const double* __restrict__ K, const double* __restrict__ G,
+                                                      double* __restrict__ R, long long n, long long nD) {
+  int lo = 0, hi = ntg - 1;  // the target of this tile: the last with tile_begin <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tg[mid].tile_begin <= (long long)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const DvTarget T = tg[lo];
+  const int e = (int)(((long long)blockIdx.x - T.tile_begin) * blockDim.x) + threadIdx.x;
+  if (e >= T.ml * T.ml) return;
+  const long long n2 = n * n;
+  const int q = e / T.ml, sidx = e - q * T.ml;
+  const long long col = (long long)T.dl[q] * n + T.dl[sidx];
+  double acc = 0.0;
+  for (long long p = T.e_begin; p < T.e_end; ++p) acc = fma(G[pqs[p] * nD + T.dk], K[pqs[p] * n2 + col], acc);
+  R[T.dk * n2 + col] += acc;
+}
+
 // Row-panel FP64 GEMM for problems with few rows and long rows of B (the all-external product Y = U W: a
 // few dozen gathered CI rows against the np x np operator): C (M x N) = beta C + sum over the segments of
 // alpha A B, A M x K and B K x N row major, M <= MT.  A block of 256 threads owns 128 columns of one problem
@@ -1391,7 +1450,8 @@ struct DevStep {
   int dom_nprob = 0;
   long long dom_ntiles = 0;
   // local decks: the three-external term on the domains (dom3_forward in place of the split-k sum,
-  // dom3_reverse in place of the reverse GEMM); d3_skip marks the padded forward GEMM they replace
+  // dom3_reverse in place of the reverse GEMM); d3_skip marks a padded forward GEMM that a domain kernel
+  // replaces (three-external or N-2 <-> valence)
   bool d3_skip = false;
   int d3 = 0;  // 1: dom3_forward, 2: dom3_reverse
   D3Fwd* d3f = nullptr;
@@ -1402,6 +1462,17 @@ struct DevStep {
   int d3r_n = 0;
   long long d3r_tiles = 0;
   double* d3_rows = nullptr;  // forward: Y (output); reverse: U (input)
+  // local decks: the N-2 <-> valence term on the domains (dom_dv_forward in place of the split-k sum,
+  // dom_dv_reverse in place of the reverse GEMM; the padded forward GEMM marked d3_skip)
+  int dv = 0;  // 1: forward, 2: reverse
+  DvEntry* dv_ent = nullptr;
+  long long dv_nent = 0;
+  DvTarget* dv_tg = nullptr;
+  long long* dv_pq = nullptr;
+  int dv_ntg = 0;
+  long long dv_tiles = 0;
+  double* dv_vals = nullptr;  // forward: F (output); reverse: G (input)
+  double* dv_k = nullptr;     // the exchange bank
   // AXPY / DOT
   DAxpyTarget* at = nullptr;
   DAxpySource* as = nullptr;
@@ -1914,6 +1985,88 @@ struct tci_ctx {
     return true;
   }
 
+  // The N-2 <-> valence term of a local deck on the domains. Forward entries (pq, dk) come from the scatter
+  // step's sources (F + pq nD + dk), reverse ones from the gather step's targets (G + pq nD + dk); the zero,
+  // scatter and gather steps stay. Returns false (the padded steps stay) when the plan has no such term.
+  bool lower_dom_dv(const std::vector<Step>& steps, const tci::LocalSetup& ls, DevStep& fwd, DevStep& rev) {
+    const i64 n = plan.n, n2 = n * n, nD = plan.nD, nk = plan.nint * plan.nint;
+    const Step *zf = nullptr, *zg = nullptr, *sc = nullptr, *ga = nullptr, *gr = nullptr;
+    for (const auto& s : steps) {
+      if (s.name == "dv forward zero") zf = &s;
+      if (s.name == "dv reverse zero") zg = &s;
+      if (s.name == "dv scatter") sc = &s;
+      if (s.name == "dv reverse gather") ga = &s;
+      if (s.name == "dv reverse") gr = &s;
+    }
+    if (!zf || !zg || !sc || !ga || !gr || nD == 0) return false;
+    if (zf->buf != BUF_T0 || zg->buf != BUF_T0 || zf->len != nk * nD || zg->len != nk * nD || gr->gs.size() != 1 ||
+        gr->gs[0].b != BUF_JK || gr->gs[0].a != BUF_T0 || gr->gs[0].offA != zg->off || gr->gs[0].K != nk)
+      throw Error(TCI_ERR_INTERNAL, "unexpected N-2 <-> valence steps");
+    const i64 offK = gr->gs[0].offB;
+    check_range(BUF_JK, offK, nk * n2);
+    check_range(BUF_D, 0, nD * n2);
+    check_range(BUF_R, 0, nD * n2);
+    std::vector<i64> dk2h((size_t)nD, -1);
+    for (size_t h = 0; h < plan.dheads.size(); ++h)
+      for (i64 k = 0; k < plan.dheads[h].nD; ++k) dk2h[(size_t)(plan.dheads[h].dk0 + k)] = (i64)h;
+    if (ls.dh_len.size() != plan.dheads.size()) throw Error(TCI_ERR_INTERNAL, "local domains do not match the plan's heads");
+    auto entry = [&](i64 rel) {
+      if (rel < 0 || rel >= nk * nD) throw Error(TCI_ERR_INTERNAL, "N-2 <-> valence entry out of range");
+      const i64 pq = rel / nD, dk = rel % nD;
+      if (dk2h[(size_t)dk] < 0) throw Error(TCI_ERR_INTERNAL, "N-2 <-> valence entry of no pair matrix");
+      return std::make_pair(pq, dk);
+    };
+    const int* ddl = upload(ls.dh_dom, owned, stream);
+    std::vector<std::pair<i64, i64>> fe;  // forward entries (pq, dk), sorted and unique
+    for (const auto& x : sc->as) {
+      if (x.src != BUF_T0 || x.sbuf >= 0) throw Error(TCI_ERR_INTERNAL, "unexpected N-2 <-> valence scatter source");
+      fe.push_back(entry(x.off - zf->off));
+    }
+    std::sort(fe.begin(), fe.end());
+    fe.erase(std::unique(fe.begin(), fe.end()), fe.end());
+    std::vector<DvEntry> fwe;
+    for (const auto& e : fe) {
+      const i64 h = dk2h[(size_t)e.second], ml = ls.dh_len[(size_t)h];
+      if (ml > 0) fwe.push_back(DvEntry{e.first, e.second, ddl + ls.dh_off[(size_t)h], (int)ml});
+    }
+    std::map<i64, std::vector<i64>> by_dk;  // reverse: dk -> its pq, ascending
+    for (const auto& t : ga->at) {
+      if (t.dst != BUF_T0 || t.len != 1) throw Error(TCI_ERR_INTERNAL, "unexpected N-2 <-> valence gather target");
+      const auto e = entry(t.off - zg->off);
+      by_dk[e.second].push_back(e.first);
+    }
+    std::vector<DvTarget> rt;
+    std::vector<long long> pqs;
+    long long tiles = 0;
+    for (auto& kv : by_dk) {
+      const i64 h = dk2h[(size_t)kv.first], ml = ls.dh_len[(size_t)h];
+      if (ml == 0) continue;
+      std::sort(kv.second.begin(), kv.second.end());
+      kv.second.erase(std::unique(kv.second.begin(), kv.second.end()), kv.second.end());
+      const long long e0 = (long long)pqs.size();
+      pqs.insert(pqs.end(), kv.second.begin(), kv.second.end());
+      rt.push_back(DvTarget{kv.first, tiles, ddl + ls.dh_off[(size_t)h], (int)ml, e0, (long long)pqs.size()});
+      tiles += (ml * ml + 255) / 256;
+    }
+    fwd.dv = 1;
+    fwd.kind = STEP_AXPY;
+    fwd.name = "dv split-k sum";
+    fwd.dv_ent = upload(fwe, owned, stream);
+    fwd.dv_nent = (long long)fwe.size();
+    fwd.dv_vals = ptr(BUF_T0, zf->off);
+    fwd.dv_k = ptr(BUF_JK, offK);
+    rev.dv = 2;
+    rev.kind = STEP_GEMM;
+    rev.name = "dv reverse";
+    rev.dv_tg = upload(rt, owned, stream);
+    rev.dv_pq = upload(pqs, owned, stream);
+    rev.dv_ntg = (int)rt.size();
+    rev.dv_tiles = tiles;
+    rev.dv_vals = ptr(BUF_T0, zg->off);
+    rev.dv_k = ptr(BUF_JK, offK);
+    return true;
+  }
+
   // local decks: the padded positions of the local CSFs, sorted (empty otherwise)
   std::vector<long long> loc_pos;
   bool any_local(i64 off, i64 len) const {
@@ -2302,6 +2455,10 @@ struct tci_ctx {
         continue;
       }
       if (s.d3_skip) continue;
+      if (s.dv) {
+        k += (s.dv_nent > 0 || s.dv_tiles > 0) ? 1 : 0;
+        continue;
+      }
       if (s.d3) {
         k += (s.d3f_n > 0 || s.d3r_tiles > 0) ? 1 : 0;
         continue;
@@ -2655,6 +2812,18 @@ struct tci_ctx {
     const bool tc_allext = precision == 1 || allext_tc_in_fp64;
     if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
     if (s.d3_skip) return;
+    if (s.dv == 1) {  // local deck: the forward N-2 <-> valence term on the domains
+      if (s.dv_nent > 0)
+        dom_dv_forward<<<(unsigned)((s.dv_nent + 7) / 8), 256, 0, stream>>>(s.dv_ent, s.dv_nent, s.dv_k, buf[BUF_D],
+                                                                            s.dv_vals, plan.n, plan.nD);
+      return;
+    }
+    if (s.dv == 2) {  // local deck: the reverse N-2 <-> valence term on the domains
+      if (s.dv_tiles > 0)
+        dom_dv_reverse<<<(unsigned)s.dv_tiles, 256, 0, stream>>>(s.dv_tg, s.dv_ntg, s.dv_pq, s.dv_k, s.dv_vals,
+                                                                  buf[BUF_R], plan.n, plan.nD);
+      return;
+    }
     if (s.d3 == 1) {  // local deck: the forward three-external term on the domains
       if (s.d3f_n > 0) {
         static bool attr_set[64] = {};
@@ -3244,6 +3413,8 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     ctx->f_on_tc = precision == 1 && refine != 0;
     DevStep d3f, d3r;
     const bool dom3 = ls && ctx->lower_dom3(P.sigma_steps, *ls, d3f, d3r);
+    DevStep dvf, dvr;
+    const bool domdv = ls && ctx->lower_dom_dv(P.sigma_steps, *ls, dvf, dvr);
     for (auto& s : P.sigma_steps) {
       if (ls && s.kind == STEP_GEMM && s.name == "dd two-external")
         ctx->sigma.push_back(ctx->lower_dom(s, *ls));
@@ -3257,6 +3428,16 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
         ctx->sigma.push_back(d3f);
       else if (dom3 && s.name == "three-external reverse")
         ctx->sigma.push_back(d3r);
+      else if (domdv && s.name == "dv forward") {
+        DevStep d;
+        d.kind = s.kind;
+        d.name = s.name;
+        d.d3_skip = true;
+        ctx->sigma.push_back(d);
+      } else if (domdv && s.name == "dv split-k sum")
+        ctx->sigma.push_back(dvf);
+      else if (domdv && s.name == "dv reverse")
+        ctx->sigma.push_back(dvr);
       else
         ctx->sigma.push_back(ctx->lower(s));
       if (timing) {  // the σ steps whose tables take a noticeable time
