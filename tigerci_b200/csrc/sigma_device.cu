@@ -373,39 +373,38 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
     }
 }
 
-// Domain-restricted two-external products of a local deck (pair domains), on the padded pair matrices:
-//   C[dom[i]][dom[j]] += sum_s alpha_s sum_k A_s[dom[i]][dom_s[k]] B_s[dom_s[k]][dom[j]]   (i, j < m; k < m_s)
-// A_s an n x n integral matrix, B_s the source head's padded pair matrix (zero outside its domain's rows
-// and columns, so only its domain's rows carry terms, and only the columns in both domains are nonzero),
-// C the target head's padded accumulator; all of pitch ld = n.  This is the reference's local two-external
-// product on the common virtuals (two_int_seg_com_lmo_res, three_and_four_seg_mod_2.f90:7137-8005), here
-// over the target's whole domain with the source's zeros in place of the column selection, so that every
-// term of a target block adds into the same tile and the sum stays in a fixed order.  64 x 64 tiles of
-// the m x m domain block, 16-deep k chunks gathered through shared memory.  Segments in table order, k
-// ascending; alpha scales B as it is stored.
-struct DDomProblem {
+// Domain-restricted two-external products of a local deck (pair domains), on the padded pair matrices, over
+// the common virtuals as the reference takes them (two_int_seg_com_lmo_res, three_and_four_seg_mod_2.f90:
+// 7137-8005, GEMMs at :7718-7751). B_s, the source head's padded pair matrix, is zero outside its domain's
+// rows and columns, and the target needs only its own domain's rows and columns, so a term of source head s
+// reaches only the columns in both domains; segment s carries that list (cols, ncol) and computes
+//   C[dom[i]][cols[j]] += alpha_s sum_k A_s[dom[i]][dom_s[k]] B_s[dom_s[k]][cols[j]]   (i < m, j < ncol, k < m_s)
+// with A_s an n x n integral matrix and C the target head's padded accumulator, all of pitch ld = n:
+// m_target x ncol x m_s per term instead of m_target x m_target x m_s. A block owns 64 rows of the target's
+// domain and walks every (segment, 32-column chunk, 16-deep k chunk) of its target in table order through two
+// shared buffers (one barrier per chunk); at the end of each column chunk it adds its 64 x 32 sums into C.
+// Every element of C is written by one block, its terms in segment order, and the barrier between two column
+// chunks orders the read-modify-writes of different threads of the block: the sum stays in a fixed order.
+// alpha scales B as it is stored.
+struct DComProblem {
   double* C;
   const int* dom;
-  int m, tiles_n;
+  int m;
   long long tile_begin, seg_begin, seg_end;
 };
-struct DDomSeg {
+struct DComSeg {
   const double* A;
   const double* B;
-  const int* dom;
-  int m;
+  const int* dom;   // the source head's domain (the k range)
+  const int* cols;  // the common columns
+  int m, ncol;
   double alpha;
 };
-constexpr int DOM_T = 64, DOM_K = 16, DOM_THREADS = 128;
-// 128 threads, 8 x 4 outputs each (rows 8 ty .. 8 ty + 7, columns tx + 16 c): per k, two 16-byte shared loads
-// of A (the same address across the 16 threads of a row group) and four 8-byte loads of B (16 consecutive
-// doubles across the row group) for 32 FMAs.  The (segment, chunk) sequence of a tile runs through two shared
-// buffers: the next chunk's elements are loaded into registers while the current one is multiplied, then
-// stored into the other buffer, one barrier per chunk.
-__global__ void __launch_bounds__(DOM_THREADS) gemm_dom_f64(const DDomProblem* __restrict__ probs, int nprob,
-                                                           const DDomSeg* __restrict__ segs, long long ld) {
-  __shared__ __align__(16) double As[2][DOM_K][DOM_T];
-  __shared__ __align__(16) double Bs[2][DOM_K][DOM_T];
+constexpr int COM_R = 64, COM_C = 32, COM_K = 16, COM_THREADS = 128;
+__global__ void __launch_bounds__(COM_THREADS) gemm_com_f64(const DComProblem* __restrict__ probs, int nprob,
+                                                           const DComSeg* __restrict__ segs, long long ld) {
+  __shared__ __align__(16) double As[2][COM_K][COM_R];
+  __shared__ __align__(16) double Bs[2][COM_K][COM_C];
   const long long tile = blockIdx.x;
   int lo = 0, hi = nprob - 1;
   while (lo < hi) {
@@ -413,30 +412,26 @@ __global__ void __launch_bounds__(DOM_THREADS) gemm_dom_f64(const DDomProblem* _
     if (probs[mid].tile_begin <= tile) lo = mid;
     else hi = mid - 1;
   }
-  const DDomProblem P = probs[lo];
-  const long long t = tile - P.tile_begin;
-  const int r0 = (int)(t / P.tiles_n) * DOM_T, c0 = (int)(t % P.tiles_n) * DOM_T;
+  const DComProblem P = probs[lo];
+  const int r0 = (int)(tile - P.tile_begin) * COM_R;
+  // outputs: rows 8 ty .. 8 ty + 7, columns tx and tx + 16 of the chunk
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  // load slots: A rows ia + 8 q at k = ka; B rows kb + 2 q at column jb
-  const int ka = tid & 15, ia = tid >> 4, kb = tid >> 6, jb = tid & 63;
+  // load slots: A rows ia + 8 q at k = ka; B rows kb + 4 q at column jb
+  const int ka = tid & 15, ia = tid >> 4, kb = tid >> 5, jb = tid & 31;
   long long arow[8];
 #pragma unroll
   for (int q = 0; q < 8; ++q) arow[q] = (r0 + ia + 8 * q < P.m) ? (long long)P.dom[r0 + ia + 8 * q] * ld : -1;
-  const long long bcol = (c0 + jb < P.m) ? (long long)P.dom[c0 + jb] : -1;
-  double acc[8][4];
-#pragma unroll
-  for (int r = 0; r < 8; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-  double ra[8], rb[8];
-  auto fetch = [&](const DDomSeg& S, int k0) {
+  double acc[8][2];
+  double ra[8], rb[4];
+  auto fetch = [&](const DComSeg& S, int c0, int k0) {
     const int k = k0 + ka;
     const long long col = k < S.m ? (long long)S.dom[k] : -1;
 #pragma unroll
     for (int q = 0; q < 8; ++q) ra[q] = (arow[q] >= 0 && col >= 0) ? S.A[arow[q] + col] : 0.0;
+    const long long bcol = c0 + jb < S.ncol ? (long long)S.cols[c0 + jb] : -1;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int kk = k0 + kb + 2 * q;
+    for (int q = 0; q < 4; ++q) {
+      const int kk = k0 + kb + 4 * q;
       rb[q] = (kk < S.m && bcol >= 0) ? S.B[(long long)S.dom[kk] * ld + bcol] : 0.0;
     }
   };
@@ -444,63 +439,75 @@ __global__ void __launch_bounds__(DOM_THREADS) gemm_dom_f64(const DDomProblem* _
 #pragma unroll
     for (int q = 0; q < 8; ++q) As[buf][ka][ia + 8 * q] = ra[q];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) Bs[buf][kb + 2 * q][jb] = alpha * rb[q];
+    for (int q = 0; q < 4; ++q) Bs[buf][kb + 4 * q][jb] = alpha * rb[q];
+  };
+  auto zero = [&]() {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
   };
   long long sc = P.seg_begin;
-  int kc = 0, buf = 0;
-  if (sc < P.seg_end) {
-    DDomSeg S = segs[sc];
-    fetch(S, 0);
-    store(0, S.alpha);
-    __syncthreads();
-    while (true) {
-      // the next (segment, chunk) of the sequence
-      long long sn = sc;
-      int kn = kc + DOM_K;
-      DDomSeg Sn = S;
-      if (kn >= S.m) {
+  if (sc >= P.seg_end) return;
+  int cc = 0, kc = 0, buf = 0;
+  DComSeg S = segs[sc];
+  zero();
+  fetch(S, 0, 0);
+  store(0, S.alpha);
+  __syncthreads();
+  while (true) {
+    // the next (segment, column chunk, k chunk) of the sequence
+    long long sn = sc;
+    int cn = cc, kn = kc + COM_K;
+    DComSeg Sn = S;
+    if (kn >= S.m) {
+      kn = 0;
+      cn = cc + COM_C;
+      if (cn >= S.ncol) {
+        cn = 0;
         ++sn;
-        kn = 0;
         if (sn < P.seg_end) Sn = segs[sn];
       }
-      const bool more = sn < P.seg_end;
-      if (more) fetch(Sn, kn);
+    }
+    const bool more = sn < P.seg_end;
+    if (more) fetch(Sn, cn, kn);
 #pragma unroll
-      for (int k = 0; k < DOM_K; ++k) {
-        const double2* ap = reinterpret_cast<const double2*>(&As[buf][k][8 * ty]);
-        double a[8], bv[4];
+    for (int k = 0; k < COM_K; ++k) {
+      const double2* ap = reinterpret_cast<const double2*>(&As[buf][k][8 * ty]);
+      double a[8];
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const double2 v = ap[h];
-          a[2 * h] = v.x;
-          a[2 * h + 1] = v.y;
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) bv[c] = Bs[buf][k][tx + 16 * c];
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], bv[c], acc[r][c]);
+      for (int h = 0; h < 4; ++h) {
+        const double2 v = ap[h];
+        a[2 * h] = v.x;
+        a[2 * h + 1] = v.y;
       }
-      if (more) store(buf ^ 1, Sn.alpha);
-      __syncthreads();
-      if (!more) break;
-      buf ^= 1;
-      sc = sn;
-      kc = kn;
-      S = Sn;
-    }
-  }
+      const double b0 = Bs[buf][k][tx], b1 = Bs[buf][k][tx + 16];
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int i = r0 + 8 * ty + r;
-    if (i >= P.m) continue;
-    double* row = P.C + (long long)P.dom[i] * ld;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int j = c0 + tx + 16 * c;
-      if (j < P.m) row[P.dom[j]] += acc[r][c];
+      for (int r = 0; r < 8; ++r) {
+        acc[r][0] = fma(a[r], b0, acc[r][0]);
+        acc[r][1] = fma(a[r], b1, acc[r][1]);
+      }
     }
+    if (sn != sc || cn != cc) {  // this column chunk is complete: add it into C
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = r0 + 8 * ty + r;
+        if (i >= P.m) continue;
+        double* row = P.C + (long long)P.dom[i] * ld;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int j = cc + tx + 16 * c;
+          if (j < S.ncol) row[S.cols[j]] += acc[r][c];
+        }
+      }
+      zero();
+    }
+    if (more) store(buf ^ 1, Sn.alpha);
+    __syncthreads();
+    if (!more) break;
+    buf ^= 1;
+    sc = sn;
+    cc = cn;
+    kc = kn;
+    S = Sn;
   }
 }
 
@@ -569,8 +576,11 @@ __global__ void __launch_bounds__(256) dom3_forward(const D3Fwd* __restrict__ un
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) part[k] += __shfl_xor_sync(0xffffffffu, part[k], o);
       }
-      if (lane == 0)
-        for (int k = 0; k < u.nk; ++k) yacc[k * u.mm + b] += part[k];
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < D3_K; ++k)
+          if (k < u.nk) yacc[k * u.mm + b] += part[k];
+      }
     }
   }
   __syncthreads();
@@ -608,7 +618,9 @@ __global__ void __launch_bounds__(D3R_T) dom3_reverse(const D3Rev* __restrict__ 
         if (k < u.nk) acc[k] = fma(urow[k * n + bb], v, acc[k]);
     }
   }
-  for (int k = 0; k < u.nk; ++k) R[(u.dk0 + k) * n2 + col] += acc[k];
+#pragma unroll
+  for (int k = 0; k < D3_K; ++k)
+    if (k < u.nk) R[(u.dk0 + k) * n2 + col] += acc[k];
 }
 
 // The N-2 <-> valence exchange term of a local deck on the domains (the reference's local dv loops,
@@ -1444,11 +1456,11 @@ struct DevStep {
   long long ntiles_f = 0;
   int nprob_f = 0;
   bool tc_ok = false;  // worth the tensor cores: enough work and tiles mostly full
-  // local decks: the two-external step restricted to the heads' domains (gemm_dom_f64)
-  DDomProblem* dom_probs = nullptr;
-  DDomSeg* dom_segs = nullptr;
-  int dom_nprob = 0;
-  long long dom_ntiles = 0;
+  // local decks: the two-external step on the heads' domains and common columns (gemm_com_f64)
+  DComProblem* com_probs = nullptr;
+  DComSeg* com_segs = nullptr;
+  int com_nprob = 0;
+  long long com_ntiles = 0;
   // local decks: the three-external term on the domains (dom3_forward in place of the split-k sum,
   // dom3_reverse in place of the reverse GEMM); d3_skip marks a padded forward GEMM that a domain kernel
   // replaces (three-external or N-2 <-> valence)
@@ -1826,8 +1838,9 @@ struct tci_ctx {
   }
 
   // The two-external step of a local deck's plan on the heads' domains: the same problems and segments
-  // (target pair matrix, integral matrix x source pair matrix, alpha), each restricted to the target's and
-  // the source's domain rows / columns; heads without local CSFs drop out.
+  // (target pair matrix, integral matrix x source pair matrix, alpha), each restricted to the target's domain
+  // rows, the source's domain as k range and the columns common to both; heads without local CSFs, and
+  // terms without common columns, drop out.
   DevStep lower_dom(const Step& s, const tci::LocalSetup& ls) {
     DevStep d;
     d.kind = s.kind;
@@ -1837,9 +1850,12 @@ struct tci_ctx {
       throw Error(TCI_ERR_INTERNAL, "local domains do not match the plan's heads");
     for (int x : ls.dh_dom)
       if (x < 0 || x >= n) throw Error(TCI_ERR_INTERNAL, "local domain entry outside the externals");
-    for (size_t h = 0; h < ls.dh_len.size(); ++h)
+    for (size_t h = 0; h < ls.dh_len.size(); ++h) {
       if (ls.dh_len[h] < 0 || ls.dh_len[h] > n || ls.dh_off[h] + ls.dh_len[h] > (i64)ls.dh_dom.size())
         throw Error(TCI_ERR_INTERNAL, "local domain slice out of range");
+      if (!std::is_sorted(ls.dh_dom.begin() + ls.dh_off[h], ls.dh_dom.begin() + ls.dh_off[h] + ls.dh_len[h]))
+        throw Error(TCI_ERR_INTERNAL, "local domain not sorted");
+    }
     std::vector<i64> dk2h((size_t)plan.nD, -1);
     for (size_t h = 0; h < plan.dheads.size(); ++h)
       for (i64 k = 0; k < plan.dheads[h].nD; ++k) dk2h[(size_t)(plan.dheads[h].dk0 + k)] = (i64)h;
@@ -1849,37 +1865,70 @@ struct tci_ctx {
         throw Error(TCI_ERR_INTERNAL, "two-external operand is not a pair matrix");
       return dk2h[(size_t)dk];
     };
-    const int* ddom = upload(ls.dh_dom, owned, stream);
-    std::vector<DDomProblem> pr;
-    std::vector<DDomSeg> sg;
-    long long tiles = 0;
+    // common columns of two heads, computed once per head pair
+    std::map<std::pair<i64, i64>, std::pair<i64, i64>> common;  // (target head, source head) -> (offset, count)
+    std::vector<int> cols;
+    auto common_of = [&](i64 ht, i64 hs) {
+      auto it = common.find({ht, hs});
+      if (it != common.end()) return it->second;
+      const int *a = ls.dh_dom.data() + ls.dh_off[(size_t)ht], *b = ls.dh_dom.data() + ls.dh_off[(size_t)hs];
+      const i64 o = (i64)cols.size();
+      std::set_intersection(a, a + ls.dh_len[(size_t)ht], b, b + ls.dh_len[(size_t)hs], std::back_inserter(cols));
+      return common[{ht, hs}] = {o, (i64)cols.size() - o};
+    };
+    struct HostSeg {
+      const double *A, *B;
+      i64 hs, col_off, ncol;
+      double alpha;
+    };
+    struct HostProb {
+      double* C;
+      i64 head, m;
+      std::vector<HostSeg> segs;
+    };
+    std::vector<HostProb> probs;
+    std::vector<char> seen((size_t)plan.nD, 0);
     for (const auto& g : s.gp) {
       if (g.c != BUF_R || g.M != n || g.N != n || g.ldc != n)
         throw Error(TCI_ERR_INTERNAL, "unexpected two-external problem shape");
       const i64 h = head_of(g.offC), m = ls.dh_len[(size_t)h];
+      if (seen[(size_t)(g.offC / n2)]++) throw Error(TCI_ERR_INTERNAL, "two-external target listed twice");
       if (m == 0) continue;
       check_range(BUF_R, g.offC, n2);
-      DDomProblem P{ptr(BUF_R, g.offC), ddom + ls.dh_off[(size_t)h], (int)m, (int)((m + DOM_T - 1) / DOM_T), tiles,
-                    (long long)sg.size(), 0};
+      std::vector<HostSeg> hsg;
       for (i64 q = g.seg_begin; q < g.seg_end; ++q) {
         const GemmSeg& x = s.gs[(size_t)q];
         if (x.b != BUF_D || x.lda != n || x.ldb != n || x.K != n || x.tA || x.tB)
           throw Error(TCI_ERR_INTERNAL, "unexpected two-external segment shape");
-        const i64 hs = head_of(x.offB), ms = ls.dh_len[(size_t)hs];
-        if (ms == 0) continue;
+        const i64 hs = head_of(x.offB);
+        if (ls.dh_len[(size_t)hs] == 0) continue;
+        const auto cm = common_of(h, hs);
+        if (cm.second == 0) continue;
         check_range(x.a, x.offA, n2);
         check_range(BUF_D, x.offB, n2);
-        sg.push_back(DDomSeg{ptr(x.a, x.offA), ptr(BUF_D, x.offB), ddom + ls.dh_off[(size_t)hs], (int)ms, x.alpha});
+        hsg.push_back(HostSeg{ptr(x.a, x.offA), ptr(BUF_D, x.offB), hs, cm.first, cm.second, x.alpha});
       }
-      P.seg_end = (long long)sg.size();
-      if (P.seg_end == P.seg_begin) continue;
-      pr.push_back(P);
-      tiles += (long long)P.tiles_n * P.tiles_n;
+      if (hsg.empty()) continue;
+      probs.push_back(HostProb{ptr(BUF_R, g.offC), h, m, std::move(hsg)});
     }
-    d.dom_probs = upload(pr, owned, stream);
-    d.dom_segs = upload(sg, owned, stream);
-    d.dom_nprob = (int)pr.size();
-    d.dom_ntiles = tiles;
+    const int* ddom = upload(ls.dh_dom, owned, stream);
+    const int* dcols = upload(cols, owned, stream);
+    std::vector<DComProblem> pr;
+    std::vector<DComSeg> sg;
+    long long tiles = 0;
+    for (const auto& p : probs) {
+      DComProblem P{p.C, ddom + ls.dh_off[(size_t)p.head], (int)p.m, tiles, (long long)sg.size(), 0};
+      for (const auto& x : p.segs)
+        sg.push_back(DComSeg{x.A, x.B, ddom + ls.dh_off[(size_t)x.hs], dcols + x.col_off,
+                             (int)ls.dh_len[(size_t)x.hs], (int)x.ncol, x.alpha});
+      P.seg_end = (long long)sg.size();
+      tiles += (p.m + COM_R - 1) / COM_R;
+      pr.push_back(P);
+    }
+    d.com_probs = upload(pr, owned, stream);
+    d.com_segs = upload(sg, owned, stream);
+    d.com_nprob = (int)pr.size();
+    d.com_ntiles = tiles;
     return d;
   }
 
@@ -2450,8 +2499,8 @@ struct tci_ctx {
   long long sigma_launches() const {
     long long k = 0;
     for (const auto& s : sigma) {
-      if (s.dom_probs) {
-        k += s.dom_ntiles > 0 ? 1 : 0;
+      if (s.com_probs) {
+        k += s.com_ntiles > 0 ? 1 : 0;
         continue;
       }
       if (s.d3_skip) continue;
@@ -2846,9 +2895,10 @@ struct tci_ctx {
     }
     switch (s.kind) {
       case STEP_GEMM:
-        if (s.dom_probs) {  // local deck: the two-external step on the domains
-          if (s.dom_ntiles > 0)
-            gemm_dom_f64<<<(unsigned)s.dom_ntiles, DOM_THREADS, 0, stream>>>(s.dom_probs, s.dom_nprob, s.dom_segs, plan.n);
+        if (s.com_probs) {  // local deck: the two-external step on the domains
+          if (s.com_ntiles > 0)
+            gemm_com_f64<<<(unsigned)s.com_ntiles, COM_THREADS, 0, stream>>>(s.com_probs, s.com_nprob, s.com_segs,
+                                                                           plan.n);
           break;
         }
         if (tc_allext && s.name == "all-external") {
