@@ -16,10 +16,11 @@
 // by their low parts (N = 256).  Lane 2j then holds U_hi[j] W_hi + U_hi[j] W_lo
 // in its two column halves and lane 2j+1 holds U_lo[j] W_hi (its second half,
 // lo x lo, is not used); the epilogue joins the lane pair with a shuffle.  On
-// B200 an MMA costs about the same time whatever its N (measured: ~220 cycles
-// per kind::tf32 slice for N = 16..256), so the instruction count is what
-// bounds this product, and this arrangement needs a quarter of the MMAs of
-// W-in-M with three products.  The tensor core reads a kind::tf32 operand's
+// B200 an MMA into one accumulator costs about the same time whatever its M
+// (64, 128) and N (64..256) (measured by mma_rate_selftest below: 188 cycles
+// per kind::tf32 instruction; 150 on two alternating accumulators), so the
+// instruction count is what bounds this product, and this arrangement needs a
+// quarter of the MMAs of W-in-M with three products.  The tensor core reads a kind::tf32 operand's
 // top 19 bits only (raw FP32 and masked operands gave bit-identical results
 // on B200), so the W tile serves as its own high part as it lands; the
 // converter warps write only the low parts.  The MMAs accumulate FP32 in

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <thread>
+#include <tuple>
 #include <array>
 #include <chrono>
 #include <cstdio>
@@ -373,38 +374,97 @@ __global__ void __launch_bounds__(256) gemm_skinny_f64(const DGemmProblem* __res
     }
 }
 
-// Domain-restricted two-external products of a local deck (pair domains), on the padded pair matrices, over
-// the common virtuals as the reference takes them (two_int_seg_com_lmo_res, three_and_four_seg_mod_2.f90:
-// 7137-8005, GEMMs at :7718-7751). B_s, the source head's padded pair matrix, is zero outside its domain's
-// rows and columns, and the target needs only its own domain's rows and columns, so a term of source head s
-// reaches only the columns in both domains; segment s carries that list (cols, ncol) and computes
-//   C[dom[i]][cols[j]] += alpha_s sum_k A_s[dom[i]][dom_s[k]] B_s[dom_s[k]][cols[j]]   (i < m, j < ncol, k < m_s)
-// with A_s an n x n integral matrix and C the target head's padded accumulator, all of pitch ld = n:
-// m_target x ncol x m_s per term instead of m_target x m_target x m_s. A block owns 64 rows of the target's
-// domain and walks every (segment, 32-column chunk, 16-deep k chunk) of its target in table order through two
-// shared buffers (one barrier per chunk); at the end of each column chunk it adds its 64 x 32 sums into C.
-// Every element of C is written by one block, its terms in segment order, and the barrier between two column
-// chunks orders the read-modify-writes of different threads of the block: the sum stays in a fixed order.
-// alpha scales B as it is stored.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// 8-byte form (gathers of single elements); src_bytes 0 fills the destination with zeros
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+
+// Domain-restricted two-external products of a local deck (pair domains) over the common virtuals, as the
+// reference takes them (two_int_seg_com_lmo_res, three_and_four_seg_mod_2.f90:7137-8005, GEMMs at :7718-7751).
+// Source head mu's pair matrix is zero outside D_mu x D_mu and the target head lambda needs only
+// D_lambda x D_lambda, so a term reaches only the columns in both domains:
+//   R_lambda[a][b] += alpha sum_{c in D_mu} X[a][c] D_mu[c][b]      (a in D_lambda, b in D_lambda and D_mu)
+// m_lambda x |common| x m_mu per term instead of m_lambda x m_lambda x m_mu. The step works on compact squares:
+// per sigma build the pair matrices of the local heads are gathered into m x m squares (com_gather_sq), the
+// products accumulate into compact m x m accumulators (zeroed first) that are then added into the padded ones
+// (com_scatter_sq); the integral operands X[D_lambda][D_mu] are constant and compacted once at set-up when the
+// device has room (com_pack_a), else gathered from the n x n matrices. Each term carries its common columns as
+// positions in the source's and in the target's domain. A block owns 64 rows of one target and walks all its
+// (term, 32-column chunk, 16-deep k chunk) in table order, the operands copied by 8-byte cp.async
+// COM_STG - 1 chunks ahead of the FMAs (one barrier per chunk); at the end of each column chunk it adds alpha
+// times its 64 x 32 sums into the target's square. Every element is written by one block, its terms in table
+// order, and the barrier between two column chunks orders the read-modify-writes of different threads: the sum
+// stays in a fixed order.
 struct DComProblem {
-  double* C;
-  const int* dom;
-  int m;
+  double* C;         // the target's compact accumulator (m x m, row pitch `pitch`)
+  const int* dom;    // the target's domain (rows of the gathered integral operand)
+  int m, pitch;
   long long tile_begin, seg_begin, seg_end;
 };
 struct DComSeg {
-  const double* A;
-  const double* B;
-  const int* dom;   // the source head's domain (the k range)
-  const int* cols;  // the common columns
-  int m, ncol;
+  const double* A;   // the n x n integral operand (gathered when Ac is nullptr)
+  const double* Ac;  // A[D_target][D_source], row pitch pitch_a, or nullptr
+  const double* B;   // the source's compact pair matrix, row pitch pitch_b
+  const int* dom;    // the source's domain (the k range)
+  const int* cs;     // the common columns: positions in the source's domain ...
+  const int* ct;     // ... and in the target's
+  int m, ncol, pitch_a, pitch_b;
   double alpha;
 };
-constexpr int COM_R = 64, COM_C = 32, COM_K = 16, COM_THREADS = 128;
-__global__ void __launch_bounds__(COM_THREADS) gemm_com_f64(const DComProblem* __restrict__ probs, int nprob,
-                                                           const DComSeg* __restrict__ segs, long long ld) {
-  __shared__ __align__(16) double As[2][COM_K][COM_R];
-  __shared__ __align__(16) double Bs[2][COM_K][COM_C];
+// one compaction job: Ac[r][c] = A[rows[r]][cols[c]] (r < m, c < ms), row pitch `pitch`
+struct DComPack {
+  const double* A;
+  double* Ac;
+  const int* rows;
+  const int* cols;
+  int m, ms, pitch;
+};
+__global__ void __launch_bounds__(256) com_pack_a(const DComPack* __restrict__ jobs, long long ld) {
+  const DComPack J = jobs[blockIdx.x];
+  for (int e = threadIdx.x; e < J.m * J.ms; e += blockDim.x) {
+    const int r = e / J.ms, c = e - r * J.ms;
+    J.Ac[(long long)r * J.pitch + c] = J.A[(long long)J.rows[r] * ld + J.cols[c]];
+  }
+}
+// a padded n x n matrix and its compact m x m square over a domain
+struct DComSq {
+  double* pad;
+  double* sq;
+  const int* dom;
+  int m, pitch;
+};
+__global__ void __launch_bounds__(256) com_gather_sq(const DComSq* __restrict__ sq, long long ld) {
+  const DComSq Q = sq[blockIdx.x];
+  for (int e = threadIdx.x; e < Q.m * Q.m; e += blockDim.x) {
+    const int r = e / Q.m, c = e - r * Q.m;
+    Q.sq[(long long)r * Q.pitch + c] = Q.pad[(long long)Q.dom[r] * ld + Q.dom[c]];
+  }
+}
+__global__ void __launch_bounds__(256) com_scatter_sq(const DComSq* __restrict__ sq, long long ld) {
+  const DComSq Q = sq[blockIdx.x];
+  for (int e = threadIdx.x; e < Q.m * Q.m; e += blockDim.x) {
+    const int r = e / Q.m, c = e - r * Q.m;
+    Q.pad[(long long)Q.dom[r] * ld + Q.dom[c]] += Q.sq[(long long)r * Q.pitch + c];
+  }
+}
+constexpr int COM_R = 64, COM_C = 32, COM_K = 16, COM_THREADS = 128, COM_STG = 3;
+// position in a block's (segment, column chunk, k chunk) sequence
+struct ComCursor {
+  long long s;
+  int c, k;
+};
+__global__ void __launch_bounds__(COM_THREADS, 4) gemm_com_f64(const DComProblem* __restrict__ probs, int nprob,
+                                                              const DComSeg* __restrict__ segs, long long ld) {
+  __shared__ __align__(16) double As[COM_STG][COM_K][COM_R];
+  __shared__ __align__(16) double Bs[COM_STG][COM_K][COM_C];
   const long long tile = blockIdx.x;
   int lo = 0, hi = nprob - 1;
   while (lo < hi) {
@@ -413,65 +473,74 @@ __global__ void __launch_bounds__(COM_THREADS) gemm_com_f64(const DComProblem* _
     else hi = mid - 1;
   }
   const DComProblem P = probs[lo];
+  if (P.seg_begin >= P.seg_end) return;
   const int r0 = (int)(tile - P.tile_begin) * COM_R;
   // outputs: rows 8 ty .. 8 ty + 7, columns tx and tx + 16 of the chunk
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  // load slots: A rows ia + 8 q at k = ka; B rows kb + 4 q at column jb
+  // copy slots: A rows ia + 8 q at k = ka; B rows kb + 4 q at column jb
   const int ka = tid & 15, ia = tid >> 4, kb = tid >> 5, jb = tid & 31;
-  long long arow[8];
-#pragma unroll
-  for (int q = 0; q < 8; ++q) arow[q] = (r0 + ia + 8 * q < P.m) ? (long long)P.dom[r0 + ia + 8 * q] * ld : -1;
-  double acc[8][2];
-  double ra[8], rb[4];
-  auto fetch = [&](const DComSeg& S, int c0, int k0) {
-    const int k = k0 + ka;
-    const long long col = k < S.m ? (long long)S.dom[k] : -1;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) ra[q] = (arow[q] >= 0 && col >= 0) ? S.A[arow[q] + col] : 0.0;
-    const long long bcol = c0 + jb < S.ncol ? (long long)S.cols[c0 + jb] : -1;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int kk = k0 + kb + 4 * q;
-      rb[q] = (kk < S.m && bcol >= 0) ? S.B[(long long)S.dom[kk] * ld + bcol] : 0.0;
-    }
+  auto advance = [&](ComCursor& x, const DComSeg& S) {
+    x.k += COM_K;
+    if (x.k < S.m) return;
+    x.k = 0;
+    x.c += COM_C;
+    if (x.c < S.ncol) return;
+    x.c = 0;
+    ++x.s;
   };
-  auto store = [&](int buf, double alpha) {
+  // the copies of one chunk into stage st (zeros past the domains, the rows or the common columns)
+  auto issue = [&](const ComCursor& x, const DComSeg& S, int st) {
+    const int k = x.k + ka;
+    if (S.Ac) {  // compacted: 16 consecutive k of a row across the 16 threads of a row group
 #pragma unroll
-    for (int q = 0; q < 8; ++q) As[buf][ka][ia + 8 * q] = ra[q];
+      for (int q = 0; q < 8; ++q) {
+        const int r = r0 + ia + 8 * q;
+        const bool ok = r < P.m && k < S.m;
+        cp_async8(&As[st][ka][ia + 8 * q], ok ? (const void*)(S.Ac + (long long)r * S.pitch_a + k) : (const void*)S.Ac,
+                  ok ? 8 : 0);
+      }
+    } else {
+      const long long col = k < S.m ? (long long)S.dom[k] : -1;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) Bs[buf][kb + 4 * q][jb] = alpha * rb[q];
-  };
-  auto zero = [&]() {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
-  };
-  long long sc = P.seg_begin;
-  if (sc >= P.seg_end) return;
-  int cc = 0, kc = 0, buf = 0;
-  DComSeg S = segs[sc];
-  zero();
-  fetch(S, 0, 0);
-  store(0, S.alpha);
-  __syncthreads();
-  while (true) {
-    // the next (segment, column chunk, k chunk) of the sequence
-    long long sn = sc;
-    int cn = cc, kn = kc + COM_K;
-    DComSeg Sn = S;
-    if (kn >= S.m) {
-      kn = 0;
-      cn = cc + COM_C;
-      if (cn >= S.ncol) {
-        cn = 0;
-        ++sn;
-        if (sn < P.seg_end) Sn = segs[sn];
+      for (int q = 0; q < 8; ++q) {
+        const int r = r0 + ia + 8 * q;
+        const bool ok = r < P.m && col >= 0;
+        cp_async8(&As[st][ka][ia + 8 * q], ok ? (const void*)(S.A + (long long)P.dom[r] * ld + col) : (const void*)S.A,
+                  ok ? 8 : 0);
       }
     }
-    const bool more = sn < P.seg_end;
-    if (more) fetch(Sn, cn, kn);
+    const int bc = x.c + jb < S.ncol ? S.cs[x.c + jb] : -1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int kk = x.k + kb + 4 * q;
+      const bool ok = kk < S.m && bc >= 0;
+      cp_async8(&Bs[st][kb + 4 * q][jb], ok ? (const void*)(S.B + (long long)kk * S.pitch_b + bc) : (const void*)S.B,
+                ok ? 8 : 0);
+    }
+  };
+  // producer cursor: COM_STG - 1 chunks ahead of the consumer
+  ComCursor pc{P.seg_begin, 0, 0};
+  DComSeg PS = segs[pc.s];
+  for (int st = 0; st < COM_STG - 1; ++st) {
+    if (pc.s < P.seg_end) {
+      issue(pc, PS, st);
+      advance(pc, PS);
+      if (pc.s < P.seg_end && pc.c == 0 && pc.k == 0) PS = segs[pc.s];
+    }
+    cp_async_commit();
+  }
+  ComCursor cc{P.seg_begin, 0, 0};
+  DComSeg S = segs[cc.s];
+  double acc[8][2];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
+  for (int it = 0;; ++it) {
+    const int st = it % COM_STG;
+    cp_async_wait<COM_STG - 2>();  // this thread's copies of the chunk have landed
+    __syncthreads();               // everyone's have, and the stage refilled below is no longer read
 #pragma unroll
     for (int k = 0; k < COM_K; ++k) {
-      const double2* ap = reinterpret_cast<const double2*>(&As[buf][k][8 * ty]);
+      const double2* ap = reinterpret_cast<const double2*>(&As[st][k][8 * ty]);
       double a[8];
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
@@ -479,36 +548,45 @@ __global__ void __launch_bounds__(COM_THREADS) gemm_com_f64(const DComProblem* _
         a[2 * h] = v.x;
         a[2 * h + 1] = v.y;
       }
-      const double b0 = Bs[buf][k][tx], b1 = Bs[buf][k][tx + 16];
+      const double b0 = Bs[st][k][tx], b1 = Bs[st][k][tx + 16];
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         acc[r][0] = fma(a[r], b0, acc[r][0]);
         acc[r][1] = fma(a[r], b1, acc[r][1]);
       }
     }
-    if (sn != sc || cn != cc) {  // this column chunk is complete: add it into C
+    // the copies COM_STG - 1 chunks ahead, after the FMAs so that their index loads overlap them
+    if (pc.s < P.seg_end) {
+      issue(pc, PS, (it + COM_STG - 1) % COM_STG);
+      advance(pc, PS);
+      if (pc.s < P.seg_end && pc.c == 0 && pc.k == 0) PS = segs[pc.s];
+    }
+    cp_async_commit();
+    const ComCursor prev = cc;
+    advance(cc, S);
+    if (cc.s != prev.s || cc.c != prev.c) {  // this column chunk is complete: add it into the target's square
+      int ct[2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int j = prev.c + tx + 16 * c;
+        ct[c] = j < S.ncol ? S.ct[j] : -1;
+      }
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         const int i = r0 + 8 * ty + r;
         if (i >= P.m) continue;
-        double* row = P.C + (long long)P.dom[i] * ld;
+        double* row = P.C + (long long)i * P.pitch;
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const int j = cc + tx + 16 * c;
-          if (j < S.ncol) row[S.cols[j]] += acc[r][c];
-        }
+        for (int c = 0; c < 2; ++c)
+          if (ct[c] >= 0) row[ct[c]] += S.alpha * acc[r][c];
       }
-      zero();
+#pragma unroll
+      for (int r = 0; r < 8; ++r) acc[r][0] = acc[r][1] = 0.0;
+      if (cc.s >= P.seg_end) break;
+      if (cc.s != prev.s) S = segs[cc.s];
     }
-    if (more) store(buf ^ 1, Sn.alpha);
-    __syncthreads();
-    if (!more) break;
-    buf ^= 1;
-    sc = sn;
-    cc = cn;
-    kc = kn;
-    S = Sn;
   }
+  cp_async_wait<0>();
 }
 
 // Domain-restricted three-external products of a local deck (pair domains), on the padded pair matrices and
@@ -697,13 +775,6 @@ constexpr int PANEL_COLS = 128;
 constexpr int PANEL_KS = 16;
 constexpr int PANEL_STG = 4;
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <int MT>
 __global__ void __launch_bounds__(PANEL_T, 2) gemm_panel_f64(const DGemmProblem* __restrict__ probs, int nprob,
@@ -1461,6 +1532,15 @@ struct DevStep {
   DComSeg* com_segs = nullptr;
   int com_nprob = 0;
   long long com_ntiles = 0;
+  DComPack* com_pack = nullptr;  // compaction of its constant operands, run once after the set-up steps
+  long long com_njobs = 0;
+  DComSq* com_gather = nullptr;   // pair matrices -> compact squares
+  long long com_ngather = 0;
+  DComSq* com_scatter = nullptr;  // compact accumulators -> padded ones
+  long long com_nscatter = 0;
+  double* com_rsq = nullptr;      // the compact accumulators (zeroed per build)
+  long long com_rsq_len = 0;
+  bool com_step = false;
   // local decks: the three-external term on the domains (dom3_forward in place of the split-k sum,
   // dom3_reverse in place of the reverse GEMM); d3_skip marks a padded forward GEMM that a domain kernel
   // replaces (three-external or N-2 <-> valence)
@@ -1839,8 +1919,8 @@ struct tci_ctx {
 
   // The two-external step of a local deck's plan on the heads' domains: the same problems and segments
   // (target pair matrix, integral matrix x source pair matrix, alpha), each restricted to the target's domain
-  // rows, the source's domain as k range and the columns common to both; heads without local CSFs, and
-  // terms without common columns, drop out.
+  // rows, the source's domain as k range and the columns common to both, on compact squares of the local
+  // heads' pair matrices and accumulators; heads without local CSFs, and terms without common columns, drop out.
   DevStep lower_dom(const Step& s, const tci::LocalSetup& ls) {
     DevStep d;
     d.kind = s.kind;
@@ -1859,68 +1939,141 @@ struct tci_ctx {
     std::vector<i64> dk2h((size_t)plan.nD, -1);
     for (size_t h = 0; h < plan.dheads.size(); ++h)
       for (i64 k = 0; k < plan.dheads[h].nD; ++k) dk2h[(size_t)(plan.dheads[h].dk0 + k)] = (i64)h;
-    auto head_of = [&](i64 off) {
+    auto dk_of = [&](i64 off) {
       const i64 dk = off / n2;
       if (off % n2 || dk < 0 || dk >= plan.nD || dk2h[(size_t)dk] < 0)
         throw Error(TCI_ERR_INTERNAL, "two-external operand is not a pair matrix");
-      return dk2h[(size_t)dk];
+      return dk;
     };
-    // common columns of two heads, computed once per head pair
+    auto mh = [&](i64 h) { return ls.dh_len[(size_t)h]; };
+    auto pitch_of = [](i64 m) { return m + (m & 1); };
+    // compact squares: one per pair matrix of a head with local CSFs, for the sources and for the targets
+    std::vector<i64> sq_off((size_t)plan.nD, -1);
+    i64 sq_len = 0;
+    for (i64 dk = 0; dk < plan.nD; ++dk) {
+      const i64 m = mh(dk2h[(size_t)dk]);
+      if (m == 0) continue;
+      sq_off[(size_t)dk] = sq_len;
+      sq_len += m * pitch_of(m);
+    }
+    // common columns of two heads as positions in each domain, computed once per head pair
     std::map<std::pair<i64, i64>, std::pair<i64, i64>> common;  // (target head, source head) -> (offset, count)
-    std::vector<int> cols;
+    std::vector<int> cpos_s, cpos_t;
     auto common_of = [&](i64 ht, i64 hs) {
       auto it = common.find({ht, hs});
       if (it != common.end()) return it->second;
       const int *a = ls.dh_dom.data() + ls.dh_off[(size_t)ht], *b = ls.dh_dom.data() + ls.dh_off[(size_t)hs];
-      const i64 o = (i64)cols.size();
-      std::set_intersection(a, a + ls.dh_len[(size_t)ht], b, b + ls.dh_len[(size_t)hs], std::back_inserter(cols));
-      return common[{ht, hs}] = {o, (i64)cols.size() - o};
+      const i64 o = (i64)cpos_s.size();
+      for (i64 x = 0, y = 0; x < mh(ht) && y < mh(hs);) {
+        if (a[x] < b[y]) ++x;
+        else if (b[y] < a[x]) ++y;
+        else {
+          cpos_t.push_back((int)x++);
+          cpos_s.push_back((int)y++);
+        }
+      }
+      return common[{ht, hs}] = {o, (i64)cpos_s.size() - o};
     };
     struct HostSeg {
-      const double *A, *B;
-      i64 hs, col_off, ncol;
+      const double* A;
+      i64 dks, hs, col_off, ncol;
       double alpha;
     };
     struct HostProb {
-      double* C;
-      i64 head, m;
+      i64 dk, head, m;
       std::vector<HostSeg> segs;
     };
     std::vector<HostProb> probs;
     std::vector<char> seen((size_t)plan.nD, 0);
+    std::vector<char> src_used((size_t)plan.nD, 0);
     for (const auto& g : s.gp) {
       if (g.c != BUF_R || g.M != n || g.N != n || g.ldc != n)
         throw Error(TCI_ERR_INTERNAL, "unexpected two-external problem shape");
-      const i64 h = head_of(g.offC), m = ls.dh_len[(size_t)h];
-      if (seen[(size_t)(g.offC / n2)]++) throw Error(TCI_ERR_INTERNAL, "two-external target listed twice");
+      const i64 dk = dk_of(g.offC), h = dk2h[(size_t)dk], m = mh(h);
+      if (seen[(size_t)dk]++) throw Error(TCI_ERR_INTERNAL, "two-external target listed twice");
       if (m == 0) continue;
-      check_range(BUF_R, g.offC, n2);
       std::vector<HostSeg> hsg;
       for (i64 q = g.seg_begin; q < g.seg_end; ++q) {
         const GemmSeg& x = s.gs[(size_t)q];
         if (x.b != BUF_D || x.lda != n || x.ldb != n || x.K != n || x.tA || x.tB)
           throw Error(TCI_ERR_INTERNAL, "unexpected two-external segment shape");
-        const i64 hs = head_of(x.offB);
-        if (ls.dh_len[(size_t)hs] == 0) continue;
+        const i64 dks = dk_of(x.offB), hs = dk2h[(size_t)dks];
+        if (mh(hs) == 0) continue;
         const auto cm = common_of(h, hs);
         if (cm.second == 0) continue;
         check_range(x.a, x.offA, n2);
-        check_range(BUF_D, x.offB, n2);
-        hsg.push_back(HostSeg{ptr(x.a, x.offA), ptr(BUF_D, x.offB), hs, cm.first, cm.second, x.alpha});
+        hsg.push_back(HostSeg{ptr(x.a, x.offA), dks, hs, cm.first, cm.second, x.alpha});
+        src_used[(size_t)dks] = 1;
       }
       if (hsg.empty()) continue;
-      probs.push_back(HostProb{ptr(BUF_R, g.offC), h, m, std::move(hsg)});
+      probs.push_back(HostProb{dk, h, m, std::move(hsg)});
     }
+    check_range(BUF_D, 0, plan.nD * n2);
+    check_range(BUF_R, 0, plan.nD * n2);
+    auto dev_alloc = [&](double** p, i64 len) {
+      TCI_CUDA(dev_malloc(p, (size_t)std::max<i64>(1, len) * sizeof(double), stream));
+      owned.push_back(*p);
+      bytes_held += (double)std::max<i64>(1, len) * sizeof(double);
+    };
+    double *dsq = nullptr, *rsq = nullptr;
+    dev_alloc(&dsq, sq_len);
+    dev_alloc(&rsq, sq_len);
     const int* ddom = upload(ls.dh_dom, owned, stream);
-    const int* dcols = upload(cols, owned, stream);
+    const int* dcs = upload(cpos_s, owned, stream);
+    const int* dct = upload(cpos_t, owned, stream);
+    // the integral operands are constant: each distinct (operand, target head, source head) block compacted
+    // once at set-up (row pitch even), when the device has room for them beside a margin
+    std::map<std::tuple<const double*, i64, i64>, i64> apos;
+    i64 abytes = 0;
+    for (const auto& p : probs)
+      for (const auto& x : p.segs) {
+        auto key = std::make_tuple(x.A, p.head, x.hs);
+        if (apos.count(key)) continue;
+        apos[key] = abytes / 8;
+        abytes += 8 * p.m * pitch_of(mh(x.hs));
+      }
+    double* abuf = nullptr;
+    {
+      size_t fr = 0, tot = 0;
+      if (abytes > 0 && cudaMemGetInfo(&fr, &tot) == cudaSuccess && (double)abytes + 8e9 < (double)fr &&
+          dev_malloc(&abuf, (size_t)abytes, stream) == cudaSuccess) {
+        owned.push_back(abuf);
+        bytes_held += (double)abytes;
+      } else {
+        cudaGetLastError();
+        abuf = nullptr;
+      }
+    }
+    std::vector<DComPack> jobs;
+    if (abuf)
+      for (const auto& kv : apos) {
+        const i64 ht = std::get<1>(kv.first), hs = std::get<2>(kv.first);
+        jobs.push_back(DComPack{std::get<0>(kv.first), abuf + kv.second, ddom + ls.dh_off[(size_t)ht],
+                                ddom + ls.dh_off[(size_t)hs], (int)mh(ht), (int)mh(hs), (int)pitch_of(mh(hs))});
+      }
+    // the squares: gathered sources (those some term reads), zeroed and scattered targets
+    std::vector<DComSq> gsq, ssq;
+    for (i64 dk = 0; dk < plan.nD; ++dk) {
+      if (sq_off[(size_t)dk] < 0) continue;
+      const i64 h = dk2h[(size_t)dk];
+      DComSq q{buf[BUF_D] + dk * n2, dsq + sq_off[(size_t)dk], ddom + ls.dh_off[(size_t)h], (int)mh(h),
+               (int)pitch_of(mh(h))};
+      if (src_used[(size_t)dk]) gsq.push_back(q);
+    }
     std::vector<DComProblem> pr;
     std::vector<DComSeg> sg;
     long long tiles = 0;
     for (const auto& p : probs) {
-      DComProblem P{p.C, ddom + ls.dh_off[(size_t)p.head], (int)p.m, tiles, (long long)sg.size(), 0};
-      for (const auto& x : p.segs)
-        sg.push_back(DComSeg{x.A, x.B, ddom + ls.dh_off[(size_t)x.hs], dcols + x.col_off,
-                             (int)ls.dh_len[(size_t)x.hs], (int)x.ncol, x.alpha});
+      ssq.push_back(DComSq{buf[BUF_R] + p.dk * n2, rsq + sq_off[(size_t)p.dk], ddom + ls.dh_off[(size_t)p.head],
+                           (int)p.m, (int)pitch_of(p.m)});
+      DComProblem P{rsq + sq_off[(size_t)p.dk], ddom + ls.dh_off[(size_t)p.head], (int)p.m, (int)pitch_of(p.m),
+                    tiles, (long long)sg.size(), 0};
+      for (const auto& x : p.segs) {
+        const i64 ms = mh(x.hs);
+        const double* ac = abuf ? abuf + apos.at(std::make_tuple(x.A, p.head, x.hs)) : nullptr;
+        sg.push_back(DComSeg{x.A, ac, dsq + sq_off[(size_t)x.dks], ddom + ls.dh_off[(size_t)x.hs], dcs + x.col_off,
+                             dct + x.col_off, (int)ms, (int)x.ncol, (int)pitch_of(ms), (int)pitch_of(ms), x.alpha});
+      }
       P.seg_end = (long long)sg.size();
       tiles += (p.m + COM_R - 1) / COM_R;
       pr.push_back(P);
@@ -1929,6 +2082,15 @@ struct tci_ctx {
     d.com_segs = upload(sg, owned, stream);
     d.com_nprob = (int)pr.size();
     d.com_ntiles = tiles;
+    d.com_pack = upload(jobs, owned, stream);
+    d.com_njobs = (long long)jobs.size();
+    d.com_gather = upload(gsq, owned, stream);
+    d.com_ngather = (long long)gsq.size();
+    d.com_scatter = upload(ssq, owned, stream);
+    d.com_nscatter = (long long)ssq.size();
+    d.com_rsq = rsq;
+    d.com_rsq_len = sq_len;
+    d.com_step = true;
     return d;
   }
 
@@ -2499,8 +2661,8 @@ struct tci_ctx {
   long long sigma_launches() const {
     long long k = 0;
     for (const auto& s : sigma) {
-      if (s.com_probs) {
-        k += s.com_ntiles > 0 ? 1 : 0;
+      if (s.com_step) {
+        k += (s.com_ngather > 0 ? 1 : 0) + (s.com_ntiles > 0 ? 1 : 0) + (s.com_nscatter > 0 ? 1 : 0);
         continue;
       }
       if (s.d3_skip) continue;
@@ -2644,6 +2806,13 @@ struct tci_ctx {
   }
 
   // Moves W+/W- to FP32 for the tensor-core product and releases the FP64 copy.
+  // local decks: the constant operands of the domain steps compacted, once the set-up steps have built them
+  void prepare_local() {
+    for (const auto& st : sigma)
+      if (st.com_njobs > 0) com_pack_a<<<(unsigned)st.com_njobs, 256, 0, stream>>>(st.com_pack, plan.n);
+    TCI_CUDA(cudaGetLastError());
+  }
+
   void setup_precision() {
     if (precision != 1) return;
     ensure_diag();  // the diagonal reads the FP64 W
@@ -2895,10 +3064,16 @@ struct tci_ctx {
     }
     switch (s.kind) {
       case STEP_GEMM:
-        if (s.com_probs) {  // local deck: the two-external step on the domains
-          if (s.com_ntiles > 0)
+        if (s.com_step) {  // local deck: the two-external step on the domains
+          if (s.com_ngather > 0)
+            com_gather_sq<<<(unsigned)s.com_ngather, 256, 0, stream>>>(s.com_gather, plan.n);
+          if (s.com_ntiles > 0) {
+            TCI_CUDA(cudaMemsetAsync(s.com_rsq, 0, (size_t)s.com_rsq_len * sizeof(double), stream));
             gemm_com_f64<<<(unsigned)s.com_ntiles, COM_THREADS, 0, stream>>>(s.com_probs, s.com_nprob, s.com_segs,
                                                                            plan.n);
+          }
+          if (s.com_nscatter > 0)
+            com_scatter_sq<<<(unsigned)s.com_nscatter, 256, 0, stream>>>(s.com_scatter, plan.n);
           break;
         }
         if (tc_allext && s.name == "all-external") {
@@ -3513,6 +3688,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     ctx->tc_kblock = kblock;
     ctx->refine = refine;
     ctx->setup_precision();
+    ctx->prepare_local();
     phase("precision set-up", ctx->stream);
     ctx->init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = ctx.release();
