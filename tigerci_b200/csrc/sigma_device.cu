@@ -760,6 +760,34 @@ __global__ void __launch_bounds__(256) dom_dv_reverse(const DvTarget* __restrict
   R[T.dk * n2 + col] += acc;
 }
 
+// The zero-external step of a local deck on the common positions: a target row of an N-2 or N-1 head
+// (padded: one row of pairs or of externals per spin function) receives coef x the source row of another head
+// of its kind, and only the positions in both heads' domains carry terms (the source row is zero outside its
+// domain, the target's are never read back outside its own): dst[rel[e]] += coef src[rel[e]] over the list of
+// relative positions of the head pair. One block per target row, its sources in table order with a barrier
+// between two (the same position may fall to different threads in two lists): a fixed order of sums.
+struct ZcTarget {
+  double* dst;
+  long long src_begin, src_end;
+};
+struct ZcSource {
+  const double* src;
+  const int* rel;
+  int nrel;
+  double coef;
+};
+__global__ void __launch_bounds__(256) axpy_common(const ZcTarget* __restrict__ tg, const ZcSource* __restrict__ so) {
+  const ZcTarget T = tg[blockIdx.x];
+  for (long long q = T.src_begin; q < T.src_end; ++q) {
+    const ZcSource S = so[q];
+    for (int e = threadIdx.x; e < S.nrel; e += blockDim.x) {
+      const int r = S.rel[e];
+      T.dst[r] = fma(S.coef, S.src[r], T.dst[r]);
+    }
+    __syncthreads();
+  }
+}
+
 // Row-panel FP64 GEMM for problems with few rows and long rows of B (the all-external product Y = U W: a
 // few dozen gathered CI rows against the np x np operator): C (M x N) = beta C + sum over the segments of
 // alpha A B, A M x K and B K x N row major, M <= MT.  A block of 256 threads owns 128 columns of one problem
@@ -1541,6 +1569,10 @@ struct DevStep {
   double* com_rsq = nullptr;      // the compact accumulators (zeroed per build)
   long long com_rsq_len = 0;
   bool com_step = false;
+  // local decks: the zero-external rows of N-2 and N-1 heads on the common positions (axpy_common)
+  ZcTarget* zc_tg = nullptr;
+  ZcSource* zc_src = nullptr;
+  long long zc_ntg = 0;
   // local decks: the three-external term on the domains (dom3_forward in place of the split-k sum,
   // dom3_reverse in place of the reverse GEMM); d3_skip marks a padded forward GEMM that a domain kernel
   // replaces (three-external or N-2 <-> valence)
@@ -2196,6 +2228,123 @@ struct tci_ctx {
     return true;
   }
 
+  // The zero-external step of a local deck: the target rows of N-2 heads (ab and aa blocks) and of N-1 heads
+  // whose sources are all rows of the same kind move to axpy_common over the positions common to the two
+  // heads' domains; the rest (valence rows) stay on the padded AXPY.
+  DevStep lower_zero_local(const Step& s, const tci::LocalSetup& ls) {
+    const i64 n = plan.n, nab = n * (n - 1) / 2;
+    // rows: (begin, end, kind 0 ab / 1 aa / 2 N-1, head slot into the local domain tables)
+    struct Range {
+      i64 begin, end;
+      int kind;
+      size_t h;
+    };
+    std::vector<Range> rg;
+    if (ls.dh_len.size() != plan.dheads.size() || ls.s1_begin.size() != ls.s1_len.size())
+      throw Error(TCI_ERR_INTERNAL, "local domains do not match the plan's heads");
+    for (size_t h = 0; h < plan.dheads.size(); ++h) {
+      const auto& d = plan.dheads[h];
+      if (d.off_ab >= 0 && d.nsf_ab > 0) rg.push_back(Range{d.off_ab, d.off_ab + d.nsf_ab * nab, 0, h});
+      if (d.off_aa >= 0 && d.nsf_aa > 0) rg.push_back(Range{d.off_aa, d.off_aa + d.nsf_aa * n, 1, h});
+    }
+    for (size_t h = 0; h < ls.s1_begin.size(); ++h) rg.push_back(Range{ls.s1_begin[h], ls.s1_end[h], 2, h});
+    std::sort(rg.begin(), rg.end(), [](const Range& a, const Range& b) { return a.begin < b.begin; });
+    auto row_of = [&](i64 off, i64 len) -> const Range* {
+      auto it = std::upper_bound(rg.begin(), rg.end(), off, [](i64 v, const Range& r) { return v < r.begin; });
+      if (it == rg.begin()) return nullptr;
+      const Range& r = *std::prev(it);
+      const i64 rl = r.kind == 0 ? nab : n;
+      if (off >= r.end || len != rl || (off - r.begin) % rl) return nullptr;
+      return &r;
+    };
+    auto dom_of = [&](const Range& r, const int*& p, i64& m) {
+      if (r.kind == 2) {
+        p = ls.s1_dom.data() + ls.s1_off[r.h];
+        m = ls.s1_len[r.h];
+      } else {
+        p = ls.dh_dom.data() + ls.dh_off[r.h];
+        m = ls.dh_len[r.h];
+      }
+    };
+    // relative positions common to two heads of one kind, computed once per pair
+    std::map<std::tuple<int, size_t, size_t>, std::pair<i64, i64>> lists;
+    std::vector<int> rel;
+    auto list_of = [&](const Range& t, const Range& u) {
+      auto key = std::make_tuple(t.kind, t.h, u.h);
+      auto it = lists.find(key);
+      if (it != lists.end()) return it->second;
+      const int *a, *b;
+      i64 ma, mb;
+      dom_of(t, a, ma);
+      dom_of(u, b, mb);
+      std::vector<int> c;
+      std::set_intersection(a, a + ma, b, b + mb, std::back_inserter(c));
+      const i64 o = (i64)rel.size();
+      if (t.kind == 0) {
+        for (size_t i = 1; i < c.size(); ++i)
+          for (size_t j = 0; j < i; ++j) rel.push_back(c[i] * (c[i] - 1) / 2 + c[j]);  // c sorted: c[i] > c[j]
+      } else {
+        rel.insert(rel.end(), c.begin(), c.end());
+      }
+      return lists[key] = {o, (i64)rel.size() - o};
+    };
+    Step rest = s;
+    rest.at.clear();
+    rest.as.clear();
+    struct HT {
+      i64 off, len;
+      std::vector<std::tuple<i64, i64, i64, double>> src;  // (source offset, list offset, list length, coef)
+    };
+    std::vector<HT> loc;
+    for (const auto& t : s.at) {
+      const Range* rt = t.dst == BUF_S ? row_of(t.off, t.len) : nullptr;
+      bool ok = rt != nullptr;
+      for (i64 q = t.src_begin; ok && q < t.src_end; ++q) {
+        const AxpySource& x = s.as[(size_t)q];
+        const Range* rs = x.src == BUF_C && x.sbuf < 0 ? row_of(x.off, t.len) : nullptr;
+        ok = rs && rs->kind == rt->kind;
+      }
+      if (!ok) {  // stays on the padded AXPY
+        AxpyTarget nt = t;
+        nt.src_begin = (i64)rest.as.size();
+        for (i64 q = t.src_begin; q < t.src_end; ++q) rest.as.push_back(s.as[(size_t)q]);
+        nt.src_end = (i64)rest.as.size();
+        rest.at.push_back(nt);
+        continue;
+      }
+      const int* dp;
+      i64 mt;
+      dom_of(*rt, dp, mt);
+      if (mt == 0) continue;  // a head without local CSFs: its sigma is never read back
+      HT h{t.off, t.len, {}};
+      for (i64 q = t.src_begin; q < t.src_end; ++q) {
+        const AxpySource& x = s.as[(size_t)q];
+        const auto l = list_of(*rt, *row_of(x.off, t.len));
+        if (l.second > 0) h.src.emplace_back(x.off, l.first, l.second, x.coef);
+      }
+      if (!h.src.empty()) loc.push_back(std::move(h));
+    }
+    DevStep d = lower(rest);
+    d.name = s.name;
+    const int* drel = upload(rel, owned, stream);
+    std::vector<ZcTarget> zt;
+    std::vector<ZcSource> zs;
+    for (const auto& h : loc) {
+      check_range(BUF_S, h.off, h.len);
+      ZcTarget T{ptr(BUF_S, h.off), (long long)zs.size(), 0};
+      for (const auto& x : h.src) {
+        check_range(BUF_C, std::get<0>(x), h.len);
+        zs.push_back(ZcSource{ptr(BUF_C, std::get<0>(x)), drel + std::get<1>(x), (int)std::get<2>(x), std::get<3>(x)});
+      }
+      T.src_end = (long long)zs.size();
+      zt.push_back(T);
+    }
+    d.zc_tg = upload(zt, owned, stream);
+    d.zc_src = upload(zs, owned, stream);
+    d.zc_ntg = (long long)zt.size();
+    return d;
+  }
+
   // The N-2 <-> valence term of a local deck on the domains. Forward entries (pq, dk) come from the scatter
   // step's sources (F + pq nD + dk), reverse ones from the gather step's targets (G + pq nD + dk); the zero,
   // scatter and gather steps stay. Returns false (the padded steps stay) when the plan has no such term.
@@ -2691,6 +2840,7 @@ struct tci_ctx {
         for (int c = 0; c < 7; ++c) k += s.panel_ntiles[c] > 0 ? 1 : 0;
         for (int b = 0; b < 2; ++b) k += s.cp_ntiles[b] > 0 ? 1 : 0;
       }
+      if (s.zc_ntg > 0) k += 1;
       if ((s.kind == STEP_GEMM && s.ntiles > 0) || ((s.kind == STEP_AXPY || s.kind == STEP_DOT) && s.ntg > 0) ||
           ((s.kind == STEP_UNPACK || s.kind == STEP_PACK) && plan.nD > 0))
         k += 1;
@@ -3147,6 +3297,7 @@ struct tci_ctx {
           if (s.axpy_pairs) axpy_segments<true><<<(unsigned)s.ntg, 256, 0, stream>>>(s.at, s.ntg, s.as);
           else axpy_segments<false><<<(unsigned)s.ntg, 256, 0, stream>>>(s.at, s.ntg, s.as);
         }
+        if (s.zc_ntg > 0) axpy_common<<<(unsigned)s.zc_ntg, 256, 0, stream>>>(s.zc_tg, s.zc_src);
         break;
       case STEP_DOT:
         if (s.ntg > 0) dot_segments<<<(unsigned)s.ntg, 256, 0, stream>>>(s.dt, s.ntg, s.ds);
@@ -3653,6 +3804,8 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
         ctx->sigma.push_back(d3f);
       else if (dom3 && s.name == "three-external reverse")
         ctx->sigma.push_back(d3r);
+      else if (ls && s.kind == STEP_AXPY && s.name == "zero-external")
+        ctx->sigma.push_back(ctx->lower_zero_local(s, *ls));
       else if (domdv && s.name == "dv forward") {
         DevStep d;
         d.kind = s.kind;
