@@ -276,6 +276,23 @@ int tci_selftest_mma_rate(int64_t device, int64_t m, int64_t n, int64_t nacc, in
 int tci_reference_weight(const tci_space* s, const double* c, int64_t n, double* c0sq);
 int tci_aposteriori(int64_t n_corr_elec, double c0sq, double e_corr, double* out, int64_t len);
 
+/* ---- The loop records of the local all-external term (host only) ---------
+ * The reference enumerates the local all-external loops in a dry run before
+ * the first iteration (all_external_3_4_loops_cho_2's first pass,
+ * tiger_fortran/three_and_four_seg_mod_1.f90:414-436, records written by
+ * build_ext_34seg_dryrun, :3142-3238): for each external pair a >= c
+ * (absolute orbital numbers from 1) and each N-2 internal path whose domain
+ * holds both, one record.  tci_local_allext_records writes the records of
+ * the heads and domains this library's pair-domain term applies (the heads
+ * tci_sigma_init builds for a deck with domains), 8 int64 each:
+ * icount = a (a - 1) / 2 + c, head weight (lexical index - 1), ab address and
+ * aa address (1-based CI offsets of the head's blocks, 0 for an absent
+ * block), aa and ab spin functions, and the positions of a and c in the
+ * domain (from 1), heads in the library's order, pairs a >= c within each.
+ * *count = the number of records; out (NULL: count only) takes 8 x *count
+ * entries, TCI_ERR_ARG when cap is smaller or the deck has no domains. */
+int tci_local_allext_records(const tci_deck* deck, int64_t* out, int64_t cap, int64_t* count);
+
 /* ---- Local pair domains: the all-external term over uneven domains -----
  * Replaces the local all-external loops (ext_3_4_seg_loops_vec_lmo_res_2,
  * tiger_fortran/three_and_four_seg_mod_1.f90:3240-3518, over the domains of

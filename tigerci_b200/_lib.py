@@ -66,6 +66,7 @@ EXPORTS = [
     "tci_operator_from_records",
     "tci_reference_weight",
     "tci_aposteriori",
+    "tci_local_allext_records",
     "tci_integrals_create",
     "tci_integrals_info",
     "tci_integrals_one_electron",
@@ -171,6 +172,7 @@ def lib():
         L.tci_operator_from_records.argtypes = [i64, i64, P, P, i64, P]
         L.tci_reference_weight.argtypes = [P, P, i64, P]
         L.tci_aposteriori.argtypes = [i64, dbl, dbl, P, i64]
+        L.tci_local_allext_records.argtypes = [C.POINTER(TciDeck), P, i64, P]
         L.tci_integrals_create.argtypes = [C.POINTER(TciMolecule), dbl, C.POINTER(P)]
         L.tci_integrals_info.argtypes = [P, P, i64]
         L.tci_integrals_one_electron.argtypes = [P, P, P, i64]

@@ -265,6 +265,49 @@ int tci_acpf_gdiag(const tci_space* s, int64_t flag, double custom_g, double* g,
   }
 }
 
+int tci_local_allext_records(const tci_deck* deck, int64_t* out, int64_t cap, int64_t* count) {
+  try {
+    if (!deck || !count || !(deck->nm1_domain_ptr || deck->nm2_domain_ptr)) return TCI_ERR_ARG;
+    tci::LocalSetup ls;
+    build_space_from_c(deck, ls.loc);
+    tci_deck nl = *deck;
+    nl.nm1_domain_ptr = nl.nm1_domain_idx = nl.nm2_domain_ptr = nl.nm2_domain_idx = nullptr;
+    CsfSpace sp;
+    build_space_from_c(&nl, sp);
+    tci::build_local_structure(ls.loc, sp, ls);
+    const i64 nint = ls.loc.n_int, nh = (i64)ls.heads7.size() / 7;
+    i64 nrec = 0;
+    for (i64 j = 0; j < nh; ++j) {
+      const i64 m = ls.heads7[(size_t)(7 * j + 6)];
+      nrec += m * (m + 1) / 2;
+    }
+    *count = nrec;
+    if (!out) return TCI_OK;
+    if (cap < 8 * nrec) return TCI_ERR_ARG;
+    int64_t* r = out;
+    for (i64 j = 0; j < nh; ++j) {
+      const int64_t* h = ls.heads7.data() + 7 * j;
+      const int64_t* dom = ls.dom_idx.data() + h[5];
+      for (i64 ia = 0; ia < h[6]; ++ia)
+        for (i64 ic = 0; ic <= ia; ++ic) {
+          const i64 a = nint + 1 + dom[ia], c = nint + 1 + dom[ic];  // sorted domain: a >= c
+          r[0] = a * (a - 1) / 2 + c;
+          r[1] = ls.heads_lex[(size_t)j] - 1;
+          r[2] = h[2] > 0 ? h[0] + 1 : 0;
+          r[3] = h[3] > 0 ? h[1] + 1 : 0;
+          r[4] = h[3];
+          r[5] = h[2];
+          r[6] = ia + 1;
+          r[7] = ic + 1;
+          r += 8;
+        }
+    }
+    return TCI_OK;
+  } catch (...) {
+    return guard_status(std::current_exception());
+  }
+}
+
 int tci_reference_weight(const tci_space* s, const double* c, int64_t n, double* c0sq) {
   if (!s || !c || !c0sq || n != s->sp.total_csfs) return TCI_ERR_ARG;
   // calculate_ref_coeff_squared (aposteriori.f90:133-160): c^2 summed over the CSFs of the reference

@@ -23,6 +23,7 @@ struct LocalSetup {
   CsfSpace loc;
   std::vector<long long> map;
   std::vector<int64_t> heads7, dom_idx;
+  std::vector<int64_t> heads_lex;  // the lexical index of each heads7 entry's N-2 path
   std::vector<double> xdiag;
   // per N-2 head of the non-local plan (its dheads order): the slice of dh_dom holding the head's local
   // domain (sorted externals); length 0 for a head without local CSFs
@@ -34,6 +35,8 @@ struct LocalSetup {
   std::vector<int> s1_dom;
 };
 void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls);
+// everything of build_local_setup but the all-external diagonal arrays (no operator needed)
+void build_local_structure(const CsfSpace& loc, const CsfSpace& nl, LocalSetup& ls);
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
                   tci_ctx** out, int64_t refine = 2, LocalSetup* ls = nullptr, tci_ctx* started = nullptr);
 // A context started from the operator part of a plan (build_plan_operator_part): buffers of the integral banks

@@ -3491,7 +3491,27 @@ void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode) {
 }
 
 void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& op, LocalSetup& ls) {
-  const i64 n = nl.n_ext, nab = n * (n - 1) / 2, nint = nl.n_int, N = op.nchol;
+  build_local_structure(loc, nl, ls);
+  const i64 n = nl.n_ext, nint = nl.n_int, N = op.nchol;
+  // (aa|cc) and (ac|ca) over the externals, for the all-external part of the diagonal
+  ls.xdiag.assign((size_t)(2 * n * n), 0.0);
+  auto row = [&](i64 p, i64 q) {
+    const i64 P = nint + std::max(p, q), Q = nint + std::min(p, q);
+    return op.chol + (P * (P + 1) / 2 + Q) * N;
+  };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (i64 a = 0; a < n; ++a)
+    for (i64 c = 0; c < n; ++c) {
+      const double *la = row(a, a), *lc = row(c, c), *lx = row(a, c);
+      double s1 = 0.0, s2 = 0.0;
+      for (i64 J = 0; J < N; ++J) s1 += la[J] * lc[J], s2 += lx[J] * lx[J];
+      ls.xdiag[(size_t)(a * n + c)] = s1;
+      ls.xdiag[(size_t)(n * n + a * n + c)] = s2;
+    }
+}
+
+void build_local_structure(const CsfSpace& loc, const CsfSpace& nl, LocalSetup& ls) {
+  const i64 n = nl.n_ext, nab = n * (n - 1) / 2, nint = nl.n_int;
   if (loc.n_ext != n || loc.n_int != nint) throw Error(TCI_ERR_INTERNAL, "local and non-local spaces differ in shape");
   ls.map.assign((size_t)loc.total_csfs, -1);
   for (int k = 0; k < 3; ++k) {
@@ -3534,6 +3554,7 @@ void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& 
       if (nsf_ab == 0 && nsf_aa == 0) continue;
       ls.heads7.insert(ls.heads7.end(), {nsf_ab ? h.off : 0, nsf_aa ? h.off_aa : 0, nsf_ab, nsf_aa,
                                          nsf_aa > 0 ? (i64)loc.fsn[(size_t)h.singles] : 0, (i64)ls.dom_idx.size(), m});
+      ls.heads_lex.push_back(h.lex);
       for (int a : D) ls.dom_idx.push_back(a);
     }
   }
@@ -3565,21 +3586,6 @@ void build_local_setup(const CsfSpace& loc, const CsfSpace& nl, const Operator& 
     }
     ls.dh_len.push_back((int64_t)ls.dh_dom.size() - ls.dh_off.back());
   }
-  // (aa|cc) and (ac|ca) over the externals, for the all-external part of the diagonal
-  ls.xdiag.assign((size_t)(2 * n * n), 0.0);
-  auto row = [&](i64 p, i64 q) {
-    const i64 P = nint + std::max(p, q), Q = nint + std::min(p, q);
-    return op.chol + (P * (P + 1) / 2 + Q) * N;
-  };
-#pragma omp parallel for schedule(dynamic, 4)
-  for (i64 a = 0; a < n; ++a)
-    for (i64 c = 0; c < n; ++c) {
-      const double *la = row(a, a), *lc = row(c, c), *lx = row(a, c);
-      double s1 = 0.0, s2 = 0.0;
-      for (i64 J = 0; J < N; ++J) s1 += la[J] * lc[J], s2 += lx[J] * lx[J];
-      ls.xdiag[(size_t)(a * n + c)] = s1;
-      ls.xdiag[(size_t)(n * n + a * n + c)] = s2;
-    }
 }
 
 namespace setup {

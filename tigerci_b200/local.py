@@ -89,6 +89,22 @@ class LocalAllExternal:
         self.close()
 
 
+RECORD_FIELDS = ("icount", "head_weight", "ab_address", "aa_address", "nsf_aa", "nsf_ab", "a_pos", "c_pos")
+
+
+def allext_records(deck) -> np.ndarray:
+    """The loop records of the pair-domain all-external term for a deck with domains
+    (tci_local_allext_records): one row per (head, external pair a >= c in its domain), columns RECORD_FIELDS,
+    as the reference's dry run of the local all-external loops writes them
+    (build_ext_34seg_dryrun, three_and_four_seg_mod_1.f90:3142-3238)."""
+    d = deck.c_struct()
+    n = C.c_int64()
+    check(lib().tci_local_allext_records(C.byref(d), None, 0, C.byref(n)))
+    out = np.zeros((max(n.value, 1), 8), dtype=np.int64)
+    check(lib().tci_local_allext_records(C.byref(d), ptr(out), out.size, C.byref(n)))
+    return out[:n.value]
+
+
 def pair_domain_problem(n_pairs=600, n_int=35, n_virt=400, dmin=20, dmax=180, seed=99):
     """Heads, domains and CI length of the pair-domain batching workload.
 
