@@ -20,13 +20,13 @@
 // (64, 128) and N (64..256) (measured by mma_rate_selftest below: 188 cycles
 // per kind::tf32 instruction; 150 on two alternating accumulators), so the
 // instruction count is what bounds this product, and this arrangement needs a
-// quarter of the MMAs of W-in-M with three products.  The tensor core reads a kind::tf32 operand's
-// top 19 bits only (raw FP32 and masked operands gave bit-identical results
-// on B200), so the W tile serves as its own high part as it lands; the
-// converter warps write only the low parts.  The MMAs accumulate FP32 in
-// TMEM; every KBLOCK elements of k the partial sums are read back with
-// tcgen05.ld and added into FP64 accumulators held in registers (promotion
-// keeps the FP32 accumulation error at the block length).
+// quarter of the MMAs of W-in-M with three products.  The tensor core reads a
+// kind::tf32 operand's top 19 bits only (raw FP32 and masked operands gave
+// bit-identical results on B200), so the W tile serves as its own high part as
+// it lands; the converter warps write only the low parts.  The MMAs
+// accumulate FP32 in TMEM; every KBLOCK elements of k the partial sums are
+// read back with tcgen05.ld and added into FP64 accumulators held in registers
+// (promotion keeps the FP32 accumulation error at the block length).
 //
 // Work split (persistent, stream-K): one launch covers both operators (W+
 // with the singlet blocks, W- with the triplet blocks).  Their k-steps form
@@ -55,6 +55,7 @@
 #include <string>
 
 #include "allext_tc.h"
+#include "device_info.h"
 #include "tc_common.cuh"
 
 namespace tci_tc {
@@ -612,7 +613,7 @@ int64_t w32_floats(int64_t np) {
 }
 
 cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st) {
-  tci_tc::to_f32_tiles<<<148 * 16, 256, 0, st>>>(w64, np, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
+  tci_tc::to_f32_tiles<<<tci_dev::device_sms() * 16, 256, 0, st>>>(w64, np, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
                                                   (long long)w32_floats(np));
   return cudaGetLastError();
 }
@@ -620,7 +621,7 @@ cudaError_t convert_w(const double* w64, int64_t np, float* w32, cudaStream_t st
 cudaError_t convert_w_from_x(const double* x, int64_t n, bool plus, float* w32, cudaStream_t st) {
   const int64_t np = plus ? n + n * (n - 1) / 2 : n * (n - 1) / 2;
   if (np <= 0) return cudaSuccess;
-  tci_tc::x_to_f32_tiles<<<148 * 16, 256, 0, st>>>(x, n, plus ? 1 : 0, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
+  tci_tc::x_to_f32_tiles<<<tci_dev::device_sms() * 16, 256, 0, st>>>(x, n, plus ? 1 : 0, (int)((np + tci_tc::BK - 1) / tci_tc::BK), w32,
                                                     (long long)w32_floats(np));
   return cudaGetLastError();
 }
@@ -648,7 +649,7 @@ cudaError_t mma_rate_selftest(int64_t m, int64_t n, int64_t nacc, int64_t iters,
 int64_t u2_floats(int64_t m, int64_t np) { return 2 * padded_rows(m) * padded_ld(np); }
 
 cudaError_t split_u(const double* u, int64_t m, int64_t np, float* u2, cudaStream_t st) {
-  tci_tc::split_u<<<148 * 4, 256, 0, st>>>(u, (int)m, (int)np, np, u2, (int)padded_rows(m), padded_ld(np));
+  tci_tc::split_u<<<tci_dev::device_sms() * 4, 256, 0, st>>>(u, (int)m, (int)np, np, u2, (int)padded_rows(m), padded_ld(np));
   return cudaGetLastError();
 }
 
@@ -708,8 +709,7 @@ cudaError_t launch(const AllextTc* a, const AllextTc* b, cudaStream_t st) {
   };
   const tci_tc::Product p0 = product(a), p1 = product(b);
   // one CTA per SM, each range at least one panel long (a panel then spans at most two ranges)
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long sms = tci_dev::device_sms();
   const long long total = p0.units + p1.units, nk_max = std::max(p0.nk, p1.nk);
   const long long grid = std::max<long long>(1, std::min<long long>(sms, total / nk_max));
   // the CTAs add into zeroed outputs

@@ -32,6 +32,7 @@
 #include <cstdint>
 #include <string>
 
+#include "device_info.h"
 #include "gemm_tma.h"
 #include "tc_common.cuh"
 
@@ -413,7 +414,7 @@ int64_t pitch(int64_t cols) { return (cols + 31) / 32 * 32; }
 
 cudaError_t split(const double* src, int64_t rows, int64_t cols, int64_t ld, float* hi, float* lo, cudaStream_t st) {
   if (rows <= 0) return cudaSuccess;
-  tci_gtma::split_rows<<<148 * 8, 256, 0, st>>>(src, rows, cols, ld, pitch(cols), hi, lo);
+  tci_gtma::split_rows<<<tci_dev::device_sms() * 8, 256, 0, st>>>(src, rows, cols, ld, pitch(cols), hi, lo);
   return cudaGetLastError();
 }
 
@@ -458,8 +459,7 @@ cudaError_t launch(const TmaMaps& m, const TmaProblem* probs, int nprob, const T
   if (ntiles <= 0 || nprob <= 0) return cudaSuccess;
   // persistent: one CTA per SM (the stages take 192 KB of shared memory); otherwise a CTA per tile, which
   // the hardware schedules dynamically (better for few tiles of very uneven length)
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long sms = tci_dev::device_sms();
   const unsigned grid = (unsigned)(persistent ? std::min<long long>(ntiles, sms) : ntiles);
   if (m.wide)
     tci_gtma::gemm_tma_tf32x3<128><<<grid, tci_gtma::NTHREADS, tci_gtma::SMEM_BYTES, st>>>(

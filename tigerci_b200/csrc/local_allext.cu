@@ -54,8 +54,9 @@
 #include <vector>
 
 #include "../../include/tigerci_sigma.h"
-#include "gemm_tables.h"
 #include "allext_tc.h"
+#include "device_info.h"
+#include "gemm_tables.h"
 #include "gemm_tma.h"
 #include "host/capi_internal.h"
 
@@ -847,7 +848,7 @@ int tci_local_apply(tci_local* L, const double* d_c, double* d_sigma, int64_t n,
     LCUDA(cudaStreamWaitEvent(L->stream, L->e0, 0));
     LCUDA(cudaMemcpyAsync(L->Cb, d_c, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, L->stream));
     L->run();
-    add_into<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, L->stream>>>(d_sigma, L->Sb, n);
+    add_into<<<(unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)tci_dev::device_sms() * 8), 256, 0, L->stream>>>(d_sigma, L->Sb, n);
     LCUDA(cudaGetLastError());
     LCUDA(cudaEventRecord(L->e1, L->stream));  // after the accumulation into the caller's sigma
     LCUDA(cudaStreamWaitEvent(user, L->e1, 0));

@@ -31,6 +31,7 @@
 
 #include "../../include/tigerci_sigma.h"
 #include "allext_tc.h"
+#include "device_info.h"
 #include "gemm_tables.h"
 #include "gemm_tc.h"
 #include "gemm_tma.h"
@@ -49,19 +50,7 @@ using namespace tci;
 
 namespace {
 
-// Streaming multiprocessors of the current device (cached per device): grid-stride kernels launch a small
-// multiple of it.
-unsigned sm_count() {
-  static int cached[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!cached[dev]) {
-    int v = 0;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    cached[dev] = v;
-  }
-  return (unsigned)cached[dev];
-}
+unsigned sm_count() { return tci_dev::device_sms(); }
 
 // ----------------------------------------------------------------------------
 // device-side table layouts (plain structs, 8-byte fields)
