@@ -593,7 +593,9 @@ struct D3Fwd {
   const int* dl;  // D_lambda (sorted externals)
   const int* dm;  // D_mu
   int ml, mm, nk;
+  int b0, b1;     // the rows [b0, b1) of D_mu this block takes
 };
+constexpr int D3_BCHUNK = 32;  // rows of D_mu per forward block
 struct D3Rev {
   long long dk0, tile_begin;
   const int* dl;
@@ -611,31 +613,40 @@ __global__ void __launch_bounds__(256) dom3_forward(const D3Fwd* __restrict__ un
                                                     long long nD) {
   extern __shared__ double d3_smem[];
   const D3Fwd u = units[blockIdx.x];
-  double* ds = d3_smem;                        // [D3_K][D3_QC][ml]
-  double* yacc = d3_smem + D3_K * D3_QC * u.ml;  // [D3_K][mm]
+  const int nb = u.b1 - u.b0;
+  double* ds = d3_smem;                             // [D3_K][D3_QC][ml]
+  double* yacc = d3_smem + D3_K * D3_QC * u.ml;     // [D3_K][nb]
+  int* sdl = reinterpret_cast<int*>(yacc + D3_K * nb);  // [ml]: D_lambda
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
   const long long n2 = n * n;
   const double* Vi = V + u.i * n * n2;
-  for (int e = threadIdx.x; e < D3_K * u.mm; e += blockDim.x) yacc[e] = 0.0;
+  for (int e = threadIdx.x; e < D3_K * nb; e += blockDim.x) yacc[e] = 0.0;
+  for (int e = threadIdx.x; e < u.ml; e += blockDim.x) sdl[e] = u.dl[e];
   for (int q0 = 0; q0 < u.ml; q0 += D3_QC) {
     const int nq = min(D3_QC, u.ml - q0);
-    __syncthreads();  // the previous pass's reads of ds are done
+    __syncthreads();  // sdl is written / the previous pass's reads of ds are done
     for (int e = threadIdx.x; e < u.nk * nq * u.ml; e += blockDim.x) {
       const int k = e / (nq * u.ml), r = e - k * (nq * u.ml);
       const int qq = r / u.ml, sidx = r - qq * u.ml;
-      ds[(k * D3_QC + qq) * u.ml + sidx] = D[(u.dk0 + k) * n2 + (long long)u.dl[q0 + qq] * n + u.dl[sidx]];
+      ds[(k * D3_QC + qq) * u.ml + sidx] = D[(u.dk0 + k) * n2 + (long long)sdl[q0 + qq] * n + sdl[sidx]];
     }
     __syncthreads();
-    for (int b = warp; b < u.mm; b += nwarp) {
-      const double* vrow = Vi + (long long)u.dm[b] * n2;
+    long long qoff[D3_QC];
+#pragma unroll
+    for (int qq = 0; qq < D3_QC; ++qq) qoff[qq] = qq < nq ? (long long)sdl[q0 + qq] * n : 0;
+    for (int bl = warp; bl < nb; bl += nwarp) {
+      const double* vrow = Vi + (long long)u.dm[u.b0 + bl] * n2;
       double part[D3_K] = {0.0, 0.0, 0.0, 0.0};
-      for (int qq = 0; qq < nq; ++qq) {
-        const double* vq = vrow + (long long)u.dl[q0 + qq] * n;
-        for (int sidx = lane; sidx < u.ml; sidx += 32) {
-          const double v = vq[u.dl[sidx]];
+      for (int sidx = lane; sidx < u.ml; sidx += 32) {
+        const int c = sdl[sidx];
+        double v[D3_QC];
+#pragma unroll
+        for (int qq = 0; qq < D3_QC; ++qq) v[qq] = qq < nq ? vrow[qoff[qq] + c] : 0.0;  // D3_QC loads in flight
+#pragma unroll
+        for (int qq = 0; qq < D3_QC; ++qq) {
 #pragma unroll
           for (int k = 0; k < D3_K; ++k)
-            if (k < u.nk) part[k] = fma(v, ds[(k * D3_QC + qq) * u.ml + sidx], part[k]);
+            if (k < u.nk && qq < nq) part[k] = fma(v[qq], ds[(k * D3_QC + qq) * u.ml + sidx], part[k]);
         }
       }
 #pragma unroll
@@ -646,14 +657,14 @@ __global__ void __launch_bounds__(256) dom3_forward(const D3Fwd* __restrict__ un
       if (lane == 0) {
 #pragma unroll
         for (int k = 0; k < D3_K; ++k)
-          if (k < u.nk) yacc[k * u.mm + b] += part[k];
+          if (k < u.nk) yacc[k * nb + bl] += part[k];
       }
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < u.nk * u.mm; e += blockDim.x) {
-    const int k = e / u.mm, b = e - k * u.mm;
-    Y[(u.i * nD + u.dk0 + k) * n + u.dm[b]] = yacc[k * u.mm + b];
+  for (int e = threadIdx.x; e < u.nk * nb; e += blockDim.x) {
+    const int k = e / nb, bl = e - k * nb;
+    Y[(u.i * nD + u.dk0 + k) * n + u.dm[u.b0 + bl]] = yacc[k * nb + bl];
   }
 }
 __global__ void __launch_bounds__(D3R_T) dom3_reverse(const D3Rev* __restrict__ units, int nunit,
@@ -677,6 +688,7 @@ __global__ void __launch_bounds__(D3R_T) dom3_reverse(const D3Rev* __restrict__ 
     const D3RevEntry E = ent[p];
     const double* vcol = V + E.i * n * n2 + col;
     const double* urow = U + (E.i * nD + u.dk0) * n;
+#pragma unroll 4
     for (int b = 0; b < E.mm; ++b) {
       const int bb = E.dm[b];
       const double v = vcol[(long long)bb * n2];
@@ -2186,8 +2198,9 @@ struct tci_ctx {
         re.push_back(D3RevEntry{i, ddm + ls.s1_off[it->second], (int)mm});
         max_mm = std::max(max_mm, mm);
         for (i64 c = 0; c < nh; c += D3_K)
-          fu.push_back(D3Fwd{i, dk0 + c, ddl + ls.dh_off[(size_t)h], ddm + ls.s1_off[it->second], (int)ml, (int)mm,
-                             (int)std::min<i64>(D3_K, nh - c)});
+          for (i64 b0 = 0; b0 < mm; b0 += D3_BCHUNK)
+            fu.push_back(D3Fwd{i, dk0 + c, ddl + ls.dh_off[(size_t)h], ddm + ls.s1_off[it->second], (int)ml, (int)mm,
+                               (int)std::min<i64>(D3_K, nh - c), (int)b0, (int)std::min<i64>(mm, b0 + D3_BCHUNK)});
       }
       if ((long long)re.size() == e0) continue;
       max_ml = std::max(max_ml, ml);
@@ -2197,7 +2210,8 @@ struct tci_ctx {
         tiles += (ml * ml + D3R_T - 1) / D3R_T;
       }
     }
-    const size_t smem = (size_t)(D3_K * D3_QC * max_ml + D3_K * max_mm) * sizeof(double);
+    const size_t smem = (size_t)(D3_K * D3_QC * max_ml + D3_K * std::min<i64>(max_mm, D3_BCHUNK)) * sizeof(double) +
+                        (size_t)max_ml * sizeof(int);
     if (smem > 200 * 1024) return false;
     fwd.d3 = 1;
     fwd.kind = STEP_AXPY;
