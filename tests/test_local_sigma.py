@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 import tigerci_b200 as T
+from local_helpers import injection
 from oracle import dense, sgga
 from tigerci_b200.synthetic import random_civec, synthetic_operator
 
@@ -49,55 +50,12 @@ def _decks(c, seed):
     return base, loc, nm1, nm2
 
 
-def _injection(loc_deck, nm1, nm2, osp, n):
-    """Local CSF index -> non-local CSF index, from the product's local index vectors and the oracle's
-    non-local layout."""
-    sp = T.CsfSpace(loc_deck)
-    c = sp.counts()
-    P = np.full(c["total_csfs"], -1, dtype=np.int64)
-    nab = n * (n - 1) // 2
-    for kind, npaths in ((0, c["paths_v"]), (1, c["paths_nm1"]), (2, c["paths_nm2"])):
-        off = sp.index_vector(kind)
-        off_aa = sp.index_vector(3) if kind == 2 else None
-        for lex in range(1, npaths + 1):
-            _, info = sp.path(kind, lex)
-            g = osp.paths[kind][lex - 1]
-            if kind == 0:
-                if off[lex - 1] > 0:
-                    for k in range(info["nsf"]):
-                        P[off[lex - 1] - 1 + k] = g["off"] + k
-                continue
-            d = (nm1 if kind == 1 else nm2)[lex - 1]
-            if d == [-1]:
-                continue
-            m = len(d)
-            if kind == 1:
-                if off[lex - 1] > 0:
-                    for k in range(info["nsf"]):
-                        for a in range(m):
-                            P[off[lex - 1] - 1 + k * m + a] = g["off"] + k * n + d[a]
-                continue
-            mab = m * (m - 1) // 2
-            if off[lex - 1] > 0 and mab > 0:
-                for k in range(info["nsf"]):
-                    for i in range(1, m):
-                        for j in range(i):
-                            P[off[lex - 1] - 1 + k * mab + i * (i - 1) // 2 + j] = \
-                                g["off"] + k * nab + d[i] * (d[i] - 1) // 2 + d[j]
-            if off_aa[lex - 1] > 0:
-                for k in range(info["nsf_aa"]):
-                    for a in range(m):
-                        P[off_aa[lex - 1] - 1 + k * m + a] = g["off_aa"] + k * n + d[a]
-    assert (P >= 0).all()
-    return P
-
-
 @pytest.mark.parametrize("c", CASES, ids=lambda c: f"no{c['no']}-m{c['sm']}-r{len(c['refs'])}")
 def test_local_sigma_and_root_against_projected_oracle(c, need_gpu):
     base, loc, nm1, nm2 = _decks(c, seed=c["no"] * 7 + c["sm"])
     h, L = synthetic_operator(c["no"], 12, seed=5, scale=0.3, diag_range=(-3, 1), offdiag_sigma=0.1)
     od = dense.DenseSigma(sgga.Deck(c["no"], c["ni"], c["na"], c["ne"], c["sm"], c["refs"], c.get("nf", 0)))
-    P = _injection(loc, nm1, nm2, od.space, base.num_external)
+    P = injection(loc, nm1, nm2, od.space, base.num_external)
     H = od.hamiltonian(h, L)
     Hl = H[np.ix_(P, P)]
     sb = T.SigmaBuilder(loc, T.Operator(h, L), device=0, precision="fp64")
