@@ -45,6 +45,9 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
 // (and takes ownership of it, also on failure).
 int ctx_begin_operator(const Plan& early, const double* chol, int64_t device, int64_t precision, int64_t kblock,
                        int64_t refine, tci_ctx** out);
+// Uploads the plan's coupling-vector rows (plan.wv, n doubles) into a started context ahead of ctx_from_plan,
+// which then skips them; throws on failure.
+void ctx_upload_wv(tci_ctx* ctx, const double* wv, size_t n);
 // Selects the GEMM steps that run on the tensor cores in the mixed form (tci_sigma_init_ex options[2]).
 void ctx_set_tc_gemms(tci_ctx* ctx, int64_t mode);
 // Device bytes of such a context: peak during set-up and held afterwards.

@@ -188,6 +188,7 @@ struct Builder {
   void build_diag();
 
   bool with_allext = true;     // false: no all-external term (no X, W, WBUILD or all-external steps)
+  std::function<void(const Plan&)> wv_done;  // called once plan.wv is complete (after sv)
 
   Builder(const CsfSpace& s, const Operator& o, Plan& p) : sp(s), op(o), P(p) {}
 
@@ -1498,6 +1499,7 @@ void Builder::run() {
   tick("ss");
   sv();
   tick("sv");
+  if (wv_done) wv_done(P);
   internal_blocks();
   tick("internal");
   step(P.sigma_steps, STEP_PACK, "pack");
@@ -1567,9 +1569,15 @@ void build_plan_operator_part(const CsfSpace& sp, const Operator& op, Plan& plan
 }
 
 void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext) {
+  build_plan(sp, op, plan, with_allext, nullptr);
+}
+
+void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext,
+                const std::function<void(const Plan&)>& wv_done) {
   plan = Plan();
   Builder b(sp, op, plan);
   b.with_allext = with_allext;
+  b.wv_done = wv_done;
   b.run();
 }
 

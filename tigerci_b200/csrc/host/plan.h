@@ -16,6 +16,7 @@
 // sources of an entry are summed in table order, so a sigma build is
 // deterministic (same result alone or interleaved with other requests).
 #pragma once
+#include <functional>
 #include <memory>
 #include <new>
 #include <type_traits>
@@ -172,6 +173,10 @@ struct Operator {
 // the diagonal entries of types 2 and 3 then need the all-external diagonal from elsewhere): the form used
 // under local pair domains, whose all-external term runs in the pair-domain Cholesky form.
 void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext = true);
+// The same, calling wv_done(plan) once the coupling-vector rows (plan.wv) are complete: the later phases
+// (the zero-external blocks, the diagonal) leave plan.wv alone, so another thread may read it from then on.
+void build_plan(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext,
+                const std::function<void(const Plan&)>& wv_done);
 // The leading set-up steps of build_plan's plan that need the orbital counts and the Cholesky rank only
 // (gather cholesky rows, integral banks, all-external operators) and the sizes of their buffers.
 void build_plan_operator_part(const CsfSpace& sp, const Operator& op, Plan& plan, bool with_allext = true);

@@ -24,6 +24,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -1643,6 +1644,7 @@ struct tci_ctx {
   std::vector<std::string> early_names;
   std::vector<std::array<size_t, 4>> early_shapes;
   std::vector<i64> early_sizes;
+  bool wv_uploaded = false;  // the coupling-vector rows went up while the host built the rest of the plan
   double last_sigma_ms = 0;
   long long sigma_count = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -3410,22 +3412,39 @@ static int init_impl(const tci_deck* deck, const tci_operator* op, int64_t devic
     operator_from_c(op, sp, o);
     // The host builds the sigma tables on a second thread while the device builds the integral banks from the
     // operator part of the plan (the same leading set-up steps the whole plan starts with).
+    // The coupling-vector rows are complete before the zero-external blocks (the last long phase): they go up
+    // while the host builds those.
     Plan early;
     tci::build_plan_operator_part(sp, o, early);
-    std::exception_ptr plan_error;
+    std::exception_ptr plan_error, wv_error;
+    std::promise<std::pair<const double*, size_t>> wv_ready;
+    std::future<std::pair<const double*, size_t>> wv_rows = wv_ready.get_future();
     std::thread planner([&]() {
       try {
-        build_plan(sp, o, plan);
+        build_plan(sp, o, plan, true, [&](const Plan& P) { wv_ready.set_value({P.wv.data(), P.wv.size()}); });
       } catch (...) {
         plan_error = std::current_exception();
+      }
+      try {
+        wv_ready.set_value({nullptr, 0});  // the plan failed before its rows were complete
+      } catch (const std::future_error&) {
       }
     });
     tci_ctx* started = nullptr;
     const int rc0 = tci::ctx_begin_operator(early, o.chol, device, precision, kblock, refine, &started);
+    const auto wv = wv_rows.get();
+    if (rc0 == TCI_OK && started && wv.first && wv.second > 0) {
+      try {
+        tci::ctx_upload_wv(started, wv.first, wv.second);
+      } catch (...) {
+        wv_error = std::current_exception();
+      }
+    }
     planner.join();
-    if (plan_error || rc0 != TCI_OK) {
+    if (plan_error || wv_error || rc0 != TCI_OK) {
       if (started) tci_destroy(started);
       if (plan_error) std::rethrow_exception(plan_error);
+      if (wv_error) std::rethrow_exception(wv_error);
       return rc0;
     }
     const int rc = tci::ctx_from_plan(std::move(sp), std::move(plan), o.chol, device, precision, kblock, out, refine,
@@ -3705,6 +3724,23 @@ int ctx_begin_operator(const Plan& early, const double* chol, int64_t device, in
   }
 }
 
+// The coupling-vector rows (plan.wv) of a started context, uploaded as soon as the host has them.
+void ctx_upload_wv(tci_ctx* ctx, const double* wv, size_t n) {
+  TCI_CUDA(cudaSetDevice(ctx->device));
+  double* p = nullptr;
+  cudaError_t e = dev_malloc(&p, n * sizeof(double), ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(TCI_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+  }
+  ctx->buf[BUF_WV] = p;
+  ctx->bytes_held += (double)n * sizeof(double);
+  ctx->early_sizes[BUF_WV] = (i64)n;
+  TCI_CUDA(cudaMemcpyAsync(p, wv, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  TCI_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->wv_uploaded = true;
+}
+
 int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device, int64_t precision, int64_t kblock,
                   tci_ctx** out, int64_t refine, LocalSetup* ls, tci_ctx* started) {
   std::unique_ptr<tci_ctx> ctx(started);
@@ -3762,7 +3798,7 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
                                ctx->stream));
     TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_JK] + 2 * P.nint * P.nint * P.n * P.n, P.h_vv.data(),
                              P.h_vv.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if (!P.wv.empty())
+    if (!P.wv.empty() && !ctx->wv_uploaded)
       TCI_CUDA(cudaMemcpyAsync(ctx->buf[BUF_WV], P.wv.data(), P.wv.size() * sizeof(double), cudaMemcpyHostToDevice,
                                ctx->stream));
     TCI_CUDA(cudaStreamSynchronize(ctx->stream));
