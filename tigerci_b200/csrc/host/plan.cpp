@@ -290,6 +290,11 @@ void Builder::setup_heads() {
 // kind with spectator externals, by Slater rules on the CSF determinants.
 void Builder::internal_blocks() {
   Step& st = step(P.sigma_steps, STEP_AXPY, "zero-external");
+  struct TargetRows {
+    std::vector<AxpySource> src;
+    std::vector<AxpyTarget> rows;  // src_begin / src_end relative to src
+  };
+  std::vector<std::vector<TargetRows>> pattern_rows;  // per pattern, per head
   struct Pat {
     int kind, x, y, block;  // block: 0 valence, 1 N-1 row, 2 N-2 aa, 3 N-2 ab
   };
@@ -330,6 +335,23 @@ void Builder::internal_blocks() {
     std::vector<std::vector<uint64_t>> dbits((size_t)nthr, std::vector<uint64_t>((nq + 63) / 64, 0));
     // and whether any such move starts with (p, q) or with (p, q, r): whole loop levels skipped
     std::vector<std::vector<uint8_t>> dany((size_t)nthr, std::vector<uint8_t>(packed ? (size_t)ni * ni * (ni + 1) : 0, 0));
+    // Pair form, for patterns of up to 8192 heads: every target head within two electron moves of the source
+    // (by internal occupation) and every determinant pair of the two heads that differs in at most four
+    // internal spin orbitals (and not at all in the spectator externals) gives one Slater-rule element, the
+    // same elements the excitation enumeration below reaches from the source determinants; no per-candidate
+    // lookups. The expansions of the pattern's kept heads are made once up front.
+    const bool pair_form = packed && heads.size() <= 8192;
+    std::vector<const CsfExpansion*> pexp(pair_form ? heads.size() : 0, nullptr);
+    if (pair_form) {
+#pragma omp parallel for schedule(dynamic, 16)
+      for (long long tl = 0; tl < (long long)heads.size(); ++tl) {
+        const Head& Tg = heads[(size_t)tl];
+        if (!Tg.kept || nsf_of(Tg) == 0) continue;
+        const CsfExpansion& e = engines[(size_t)omp_get_thread_num()]->expand(cfg(Tg));
+        if (e.nsf == nsf_of(Tg)) pexp[(size_t)tl] = &e;
+      }
+    }
+    const uint64_t int_mask = packed ? (ni == 32 ? ~0ull : ((1ull << (2 * ni)) - 1)) : 0;
 #pragma omp parallel for schedule(dynamic, 4)
     for (long long hsl = 0; hsl < (long long)heads.size(); ++hsl) {
       const size_t hs = (size_t)hsl;
@@ -350,6 +372,95 @@ void Builder::internal_blocks() {
         continue;
       }
       auto kept_target = [&](i64 t) { return t >= 0 && heads[(size_t)t].kept && nsf_of(heads[(size_t)t]) != 0; };
+      if (pair_form) {
+        // target-major: this loop's head is the target T (eS / S name it here), the candidates the sources;
+        // local collects T's blocks in source order
+        auto orb = [](int x) { return x >> 1; };
+        auto spn = [](int x) { return x & 1; };
+        auto low_bit = [](uint64_t v) { return __builtin_ctzll(v); };
+        const CsfExpansion& eT = eS;
+        const Head& Tg = S;
+        for (size_t t = 0; t < heads.size(); ++t) {
+          const CsfExpansion* eSp = pexp[t];
+          if (!eSp) continue;
+          const CsfExpansion& eSrc = *eSp;
+          int dist = 0;
+          for (int p = 0; p < ni && dist <= 4; ++p)
+            dist += std::abs((int)heads[t].occ[(size_t)p] - (int)Tg.occ[(size_t)p]);
+          if (dist > 4) continue;
+          std::vector<double>* blk = nullptr;
+          for (size_t r = 0; r < eSrc.dets.size(); ++r) {
+            const Det d0 = eSrc.dets[r];
+            const double* thS = eSrc.basis->coeff.data() + r * eSrc.nsf;
+            for (size_t q = 0; q < eT.dets.size(); ++q) {
+              const Det dt = eT.dets[q];
+              const Det x = d0 ^ dt;
+              if ((uint64_t)(x >> 64) != 0 || ((uint64_t)x & ~int_mask) != 0) continue;  // externals must agree
+              const uint64_t xl = (uint64_t)x;
+              const int nb = __builtin_popcountll(xl);
+              if (nb > 4) continue;
+              const uint64_t dl = (uint64_t)d0 & int_mask;
+              double val = 0.0;
+              if (nb == 0) {  // diagonal
+                for (uint64_t a = dl; a; a &= a - 1) {
+                  const int xa = low_bit(a), pp = orb(xa);
+                  val += I.h1(pp, pp);
+                  for (uint64_t b = dl; b; b &= b - 1) {
+                    const int xb = low_bit(b), qq = orb(xb);
+                    val += 0.5 * I.i4(pp, pp, qq, qq);
+                    if (spn(xa) == spn(xb)) val -= 0.5 * I.i4(pp, qq, qq, pp);
+                  }
+                }
+              } else if (nb == 2) {  // single xa -> xb
+                const int xa = low_bit(xl & dl), xb = low_bit(xl & ~dl);
+                const int pp = orb(xb), qq = orb(xa);
+                double v = I.h1(pp, qq);
+                for (uint64_t c = dl & ~(1ull << xa); c; c &= c - 1) {
+                  const int xc = low_bit(c), rr = orb(xc);
+                  v += I.i4(pp, qq, rr, rr);
+                  if (spn(xc) == spn(xa)) v -= I.i4(pp, rr, rr, qq);
+                }
+                Det d = d0;
+                double ph = parity_below(d, xa) ? -1.0 : 1.0;
+                d &= ~(((Det)1) << xa);
+                if (parity_below(d, xb)) ph = -ph;
+                val = ph * v;
+              } else {  // double (xa, xb) -> (xc, xd), xa < xb, xc < xd
+                const uint64_t hole = xl & dl, part = xl & ~dl;
+                const int xa = low_bit(hole), xb = low_bit(hole & (hole - 1));
+                const int xc = low_bit(part), xd = low_bit(part & (part - 1));
+                double v = 0.0;
+                if (spn(xc) == spn(xa) && spn(xd) == spn(xb)) v += I.i4(orb(xc), orb(xa), orb(xd), orb(xb));
+                if (spn(xc) == spn(xb) && spn(xd) == spn(xa)) v -= I.i4(orb(xc), orb(xb), orb(xd), orb(xa));
+                if (v != 0.0) {
+                  Det d = d0;  // a+_c a+_d a_b a_a
+                  double ph = 1.0;
+                  if (parity_below(d, xa)) ph = -ph;
+                  d &= ~(((Det)1) << xa);
+                  if (parity_below(d, xb)) ph = -ph;
+                  d &= ~(((Det)1) << xb);
+                  if (parity_below(d, xd)) ph = -ph;
+                  d |= ((Det)1) << xd;
+                  if (parity_below(d, xc)) ph = -ph;
+                  val = ph * v;
+                }
+              }
+              if (val == 0.0) continue;
+              if (!blk) {
+                local.emplace_back((i64)t, std::vector<double>((size_t)eT.nsf * eSrc.nsf, 0.0));
+                blk = &local.back().second;
+              }
+              const double* thT = eT.basis->coeff.data() + q * eT.nsf;
+              const double f = val * eT.sign * eSrc.sign;
+              for (int a = 0; a < eT.nsf; ++a) {
+                if (thT[a] == 0.0) continue;
+                for (int b = 0; b < eSrc.nsf; ++b) (*blk)[(size_t)a * eSrc.nsf + b] += f * thT[a] * thS[b];
+              }
+            }
+          }
+        }
+        continue;  // local is in source order
+      }
       if (packed) {  // the spatial double moves of this head that stay in the pattern's kept heads
         std::fill(db.begin(), db.end(), 0ull);
         std::fill(dany[(size_t)th].begin(), dany[(size_t)th].end(), (uint8_t)0);
@@ -505,9 +616,20 @@ void Builder::internal_blocks() {
                 });
     }
     if (bad_count) throw Error(4, "spin-function count mismatch in zero-external block");
-    // blocks by target, sources ascending
+    // blocks by target, sources ascending (the pair form made them by target already)
     std::vector<std::vector<std::pair<i64, const std::vector<double>*>>> bytgt(heads.size());
-    for (size_t hs = 0; hs < heads.size(); ++hs)
+    if (pair_form) {
+#pragma omp parallel for schedule(dynamic, 16)
+      for (long long tl = 0; tl < (long long)heads.size(); ++tl)
+        for (const auto& sb : by_src[(size_t)tl]) bytgt[(size_t)tl].push_back({sb.first, &sb.second});
+      for (size_t t = 0; t < heads.size(); ++t)
+        for (const auto& sb : by_src[t])
+          if (sb.first == (i64)t) {
+            const i64 ns = nsf_of(heads[t]);
+            for (i64 a = 0; a < ns; ++a) beta_diag[{pt.block, (i64)t, a}] = sb.second[(size_t)a * ns + a];
+          }
+    }
+    for (size_t hs = 0; !pair_form && hs < heads.size(); ++hs)
       for (const auto& tb : by_src[hs]) {
         bytgt[(size_t)tb.first].push_back({(i64)hs, &tb.second});
         if (tb.first == (i64)hs) {
@@ -515,56 +637,59 @@ void Builder::internal_blocks() {
           for (i64 a = 0; a < ns; ++a) beta_diag[{pt.block, (i64)hs, a}] = tb.second[(size_t)a * ns + a];
         }
       }
-    // the sources of every target row, built per target in parallel and appended in target order
-    std::vector<std::vector<AxpySource>> tsrc(heads.size());
-    std::vector<std::vector<i64>> tcount(heads.size());
+    // the rows of every target (sources and row records), built per target in parallel; all patterns' rows
+    // go into the step tables at the end, in pattern and target order
+    auto& po = pattern_rows.emplace_back(heads.size());
 #pragma omp parallel for schedule(dynamic, 16)
     for (long long tl = 0; tl < (long long)heads.size(); ++tl) {
       const auto& tv = bytgt[(size_t)tl];
       if (tv.empty()) continue;
-      const i64 nsfT = nsf_of(heads[(size_t)tl]);
-      auto& out = tsrc[(size_t)tl];
-      auto& cnt = tcount[(size_t)tl];
-      cnt.assign((size_t)nsfT, 0);
-      for (i64 a = 0; a < nsfT; ++a)
+      const Head& Tg = heads[(size_t)tl];
+      const i64 nsfT = nsf_of(Tg);
+      auto& out = po[(size_t)tl];
+      for (i64 a = 0; a < nsfT; ++a) {
+        const i64 begin = (i64)out.src.size();
         for (const auto& sv : tv) {
           const Head& S = heads[(size_t)sv.first];
           const i64 nsfS = nsf_of(S);
           for (i64 b = 0; b < nsfS; ++b) {
             const double v = (*sv.second)[(size_t)a * nsfS + b];
             if (std::fabs(v) < kTiny) continue;
-            out.push_back(AxpySource{BUF_C, off_of(S) + b * len, v, -1, 0});
-            ++cnt[(size_t)a];
+            out.src.push_back(AxpySource{BUF_C, off_of(S) + b * len, v, -1, 0});
           }
         }
-    }
-    // every target's place in the step tables (target order), then the rows copied in parallel
-    std::vector<size_t> soff(heads.size() + 1, 0), toff(heads.size() + 1, 0);
-    for (size_t t = 0; t < heads.size(); ++t) {
-      size_t rows = 0;
-      for (i64 c : tcount[t]) rows += c > 0 ? 1 : 0;
-      soff[t + 1] = soff[t] + tsrc[t].size();
-      toff[t + 1] = toff[t] + rows;
-      // exact: integer-valued terms far below 2^53, so the sum does not depend on the order
-      for (i64 c : tcount[t]) P.flops_total += 2.0 * (double)len * (double)c;
-    }
-    const size_t s0 = st.as.size(), t0 = st.at.size();
-    st.as.resize(s0 + soff.back());
-    st.at.resize(t0 + toff.back());
-#pragma omp parallel for schedule(dynamic, 16)
-    for (long long tl = 0; tl < (long long)heads.size(); ++tl) {
-      const size_t t = (size_t)tl;
-      if (tsrc[t].empty()) continue;
-      std::copy(tsrc[t].begin(), tsrc[t].end(), st.as.begin() + (std::ptrdiff_t)(s0 + soff[t]));
-      const Head& Tg = heads[t];
-      size_t next = s0 + soff[t], j = t0 + toff[t];
-      for (i64 a = 0; a < (i64)tcount[t].size(); ++a) {
-        const i64 c = tcount[t][(size_t)a];
-        if (c > 0) st.at[j++] = AxpyTarget{BUF_S, off_of(Tg) + a * len, len, (i64)next, (i64)(next + (size_t)c)};
-        next += (size_t)c;
+        const i64 end = (i64)out.src.size();
+        if (end > begin) out.rows.push_back(AxpyTarget{BUF_S, off_of(Tg) + a * len, len, begin, end});
       }
-      std::vector<AxpySource>().swap(tsrc[t]);
     }
+    // exact: integer-valued terms far below 2^53, so the sum does not depend on the order
+    for (const auto& tr : po)
+      for (const auto& r : tr.rows) P.flops_total += 2.0 * (double)len * (double)(r.src_end - r.src_begin);
+  }
+  // every target's place in the step tables, then the rows copied in parallel
+  std::vector<std::pair<size_t, size_t>> order;  // (pattern, head) with rows
+  std::vector<size_t> soff(1, 0), toff(1, 0);
+  for (size_t q = 0; q < pattern_rows.size(); ++q)
+    for (size_t t = 0; t < pattern_rows[q].size(); ++t) {
+      const auto& tr = pattern_rows[q][t];
+      if (tr.rows.empty()) continue;
+      order.push_back({q, t});
+      soff.push_back(soff.back() + tr.src.size());
+      toff.push_back(toff.back() + tr.rows.size());
+    }
+  st.as.resize(soff.back());
+  st.at.resize(toff.back());
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long long ol = 0; ol < (long long)order.size(); ++ol) {
+    auto& tr = pattern_rows[order[(size_t)ol].first][order[(size_t)ol].second];
+    std::copy(tr.src.begin(), tr.src.end(), st.as.begin() + (std::ptrdiff_t)soff[(size_t)ol]);
+    for (size_t j = 0; j < tr.rows.size(); ++j) {
+      AxpyTarget x = tr.rows[j];
+      x.src_begin += (i64)soff[(size_t)ol];
+      x.src_end += (i64)soff[(size_t)ol];
+      st.at[toff[(size_t)ol] + j] = x;
+    }
+    std::vector<AxpySource>().swap(tr.src);
   }
 }
 
