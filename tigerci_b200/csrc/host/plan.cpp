@@ -1310,12 +1310,35 @@ void Builder::sv() {
     std::sort(ks.begin(), ks.end());
     ks.erase(std::unique(ks.begin(), ks.end()), ks.end());
   }
-  // every key in (mu row, v csf) order; a row's place is its rank
-  std::vector<std::pair<std::pair<i64, i64>, i64>> keys;  // (key, owning head)
+  // every key in (mu row, v csf) order; a row's place is its rank. The N-1 heads' rows are disjoint ranges
+  // in lexical order, so the keys go into one bucket per N-1 head, each sorted on its own.
+  const size_t nM = sp.paths[1].size();
+  std::vector<i64> m_begin(nM, -1);
+  for (size_t mi = 0; mi < nM; ++mi)
+    if (has(sp.paths[1][mi])) m_begin[mi] = sp.paths[1][mi].off;
+  std::vector<std::pair<i64, size_t>> starts;  // (first row, head) of the N-1 heads with CSFs, by row
+  for (size_t mi = 0; mi < nM; ++mi)
+    if (m_begin[mi] >= 0) starts.push_back({m_begin[mi], mi});
+  std::sort(starts.begin(), starts.end());
+  std::vector<std::vector<std::pair<std::pair<i64, i64>, i64>>> bucket(starts.size());
   for (size_t v = 0; v < nV; ++v)
-    for (const auto& k : vkeys[v]) keys.push_back({k, (i64)v});
+    for (const auto& k : vkeys[v]) {
+      const auto it = std::upper_bound(starts.begin(), starts.end(), std::make_pair(k.first, (size_t)-1));
+      bucket[(size_t)(it - starts.begin()) - 1].push_back({k, (i64)v});
+    }
+#pragma omp parallel for schedule(dynamic, 8)
+  for (long long b = 0; b < (long long)bucket.size(); ++b) std::sort(bucket[(size_t)b].begin(), bucket[(size_t)b].end());
+  std::vector<std::pair<std::pair<i64, i64>, i64>> keys;  // (key, owning head)
+  {
+    size_t total = 0;
+    for (const auto& b : bucket) total += b.size();
+    keys.reserve(total);
+    for (auto& b : bucket) {
+      keys.insert(keys.end(), b.begin(), b.end());
+      std::vector<std::pair<std::pair<i64, i64>, i64>>().swap(b);
+    }
+  }
   if (keys.empty()) return;
-  std::sort(keys.begin(), keys.end());
   const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
   std::vector<std::pair<std::pair<i64, i64>, i64>> rows;
   rows.reserve(keys.size());

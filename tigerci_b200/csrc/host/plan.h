@@ -16,6 +16,9 @@
 // sources of an entry are summed in table order, so a sigma build is
 // deterministic (same result alone or interleaved with other requests).
 #pragma once
+#include <sys/mman.h>
+
+#include <cstdlib>
 #include <functional>
 #include <memory>
 #include <new>
@@ -45,6 +48,24 @@ struct NoInitAlloc : std::allocator<T> {
   template <class U, class... A>
   void construct(U* p, A&&... a) {
     ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+  // large arrays (the coupling-vector rows: hundreds of MB) on 2 MB pages where the kernel allows it: the
+  // threads that fill them fault in 2 MB at a time
+  static constexpr std::size_t kLarge = std::size_t(64) << 20;
+  T* allocate(std::size_t n) {
+    const std::size_t bytes = n * sizeof(T);
+    if (bytes < kLarge) return std::allocator<T>::allocate(n);
+    void* p = nullptr;
+    if (posix_memalign(&p, std::size_t(2) << 20, bytes) != 0) throw std::bad_alloc();
+    madvise(p, bytes, MADV_HUGEPAGE);  // advice only: without it the pages stay 4 KB
+    return static_cast<T*>(p);
+  }
+  void deallocate(T* p, std::size_t n) {
+    if (n * sizeof(T) < kLarge) {
+      std::allocator<T>::deallocate(p, n);
+      return;
+    }
+    std::free(p);
   }
 };
 
