@@ -994,7 +994,13 @@ void Builder::ds() {
     for (size_t t = 0; t < t1.size(); ++t) order[t] = t;
     std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return t1[x].dkk < t1[y].dkk; });
     const i64 wbase = (i64)P.wv.size() / std::max<i64>(n, 1);
-    for (size_t r = 0; r < order.size(); ++r) P.wv.insert(P.wv.end(), t1[order[r]].w.begin(), t1[order[r]].w.end());
+    {
+      const size_t w0 = P.wv.size();
+      P.wv.resize(w0 + order.size() * (size_t)n);
+#pragma omp parallel for schedule(static)
+      for (long long r = 0; r < (long long)order.size(); ++r)
+        std::copy(t1[order[(size_t)r]].w.begin(), t1[order[(size_t)r]].w.end(), P.wv.begin() + (std::ptrdiff_t)(w0 + (size_t)r * n));
+    }
     const i64 m = (i64)order.size();
     const i64 Z = T.alloc(m * n), Cg = T.alloc(m * n);
     zero_step(P.sigma_steps, BUF_T0, Cg, m * n, "one-external gather zero");
