@@ -790,6 +790,58 @@ __global__ void __launch_bounds__(256) axpy_common(const ZcTarget* __restrict__ 
   }
 }
 
+// The one-external term of a local deck on the pair domains: a coupling row w_t (over the externals) meets
+// the pair matrix D_dk of the N-2 head lambda, zero outside D_lambda x D_lambda, so
+//   forward  Z_t[b] = sum_{q in D_lambda} w_t[q] D_dk[q][b]      (b in D_lambda; the rest of the row zero)
+//   reverse  R_dk[q][b] += sum_t w_t[q] Cg_t[b]                   (q, b in D_lambda; t over the rows of dk)
+// with Cg_t the gathered CI row of the row's N-1 CSF (the reference's local one-external loops restrict the
+// same sums to the allowed virtuals, three_and_four_seg_mod_1.f90:1099-1376). One block per row (forward) or
+// per 256 outputs of one pair matrix (reverse); sums in a fixed order.
+struct D1Row {
+  const double* w;
+  const double* D;
+  double* z;
+  const int* dl;
+  int ml;
+};
+struct D1Target {
+  double* R;
+  const double* w;   // the first coupling row of the pair matrix's group
+  const double* cg;  // its first gathered CI row
+  const int* dl;
+  int ml, rows;
+  long long tile_begin;
+};
+__global__ void __launch_bounds__(128) dom1_forward(const D1Row* __restrict__ rows, long long n) {
+  const D1Row U = rows[blockIdx.x];
+  for (long long b = threadIdx.x; b < n; b += blockDim.x) U.z[b] = 0.0;
+  __syncthreads();
+  for (int j = threadIdx.x; j < U.ml; j += blockDim.x) {
+    const int b = U.dl[j];
+    double acc = 0.0;
+    for (int q = 0; q < U.ml; ++q) {
+      const int qq = U.dl[q];
+      acc = fma(U.w[qq], U.D[(long long)qq * n + b], acc);
+    }
+    U.z[b] = acc;
+  }
+}
+__global__ void __launch_bounds__(256) dom1_reverse(const D1Target* __restrict__ tg, int ntg, long long n) {
+  int lo = 0, hi = ntg - 1;  // the target of this tile: the last with tile_begin <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tg[mid].tile_begin <= (long long)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const D1Target T = tg[lo];
+  const int e = (int)(((long long)blockIdx.x - T.tile_begin) * blockDim.x) + threadIdx.x;
+  if (e >= T.ml * T.ml) return;
+  const int q = T.dl[e / T.ml], b = T.dl[e % T.ml];
+  double acc = 0.0;
+  for (int t = 0; t < T.rows; ++t) acc = fma(T.w[(long long)t * n + q], T.cg[(long long)t * n + b], acc);
+  T.R[(long long)q * n + b] += acc;
+}
+
 // Row-panel FP64 GEMM for problems with few rows and long rows of B (the all-external product Y = U W: a
 // few dozen gathered CI rows against the np x np operator): C (M x N) = beta C + sum over the segments of
 // alpha A B, A M x K and B K x N row major, M <= MT.  A block of 256 threads owns 128 columns of one problem
@@ -1590,6 +1642,12 @@ struct DevStep {
   double* d3_rows = nullptr;  // forward: Y (output); reverse: U (input)
   // local decks: the N-2 <-> valence term on the domains (dom_dv_forward in place of the split-k sum,
   // dom_dv_reverse in place of the reverse GEMM; the padded forward GEMM marked d3_skip)
+  int d1 = 0;  // local decks, one-external term on the domains: 1 dom1_forward, 2 dom1_reverse
+  D1Row* d1_rows = nullptr;
+  long long d1_nrows = 0;
+  D1Target* d1_tg = nullptr;
+  int d1_ntg = 0;
+  long long d1_tiles = 0;
   int dv = 0;  // 1: forward, 2: reverse
   DvEntry* dv_ent = nullptr;
   long long dv_nent = 0;
@@ -2350,6 +2408,77 @@ struct tci_ctx {
     return d;
   }
 
+  // The one-external term of a local deck on the pair domains: the forward and reverse GEMMs of the plan
+  // (one problem per pair matrix: its coupling rows against D_dk, and their transposes against the gathered CI
+  // rows) become dom1_forward / dom1_reverse over D_lambda; the gather and scatter steps stay. Returns false
+  // (the padded GEMMs stay) when the plan has no one-external term.
+  bool lower_dom1(const std::vector<Step>& steps, const tci::LocalSetup& ls, DevStep& fwd, DevStep& rev) {
+    const i64 n = plan.n, n2 = n * n;
+    const Step *gf = nullptr, *gr = nullptr;
+    for (const auto& s : steps) {
+      if (s.name == "one-external forward") gf = &s;
+      if (s.name == "one-external reverse") gr = &s;
+    }
+    if (!gf || !gr || plan.nD == 0) return false;
+    if (ls.dh_len.size() != plan.dheads.size()) throw Error(TCI_ERR_INTERNAL, "local domains do not match the plan's heads");
+    std::vector<i64> dk2h((size_t)plan.nD, -1);
+    for (size_t h = 0; h < plan.dheads.size(); ++h)
+      for (i64 k = 0; k < plan.dheads[h].nD; ++k) dk2h[(size_t)(plan.dheads[h].dk0 + k)] = (i64)h;
+    const int* ddl = upload(ls.dh_dom, owned, stream);
+    auto dk_of = [&](i64 off) {
+      const i64 dk = off / n2;
+      if (off % n2 || dk < 0 || dk >= plan.nD || dk2h[(size_t)dk] < 0)
+        throw Error(TCI_ERR_INTERNAL, "one-external operand is not a pair matrix");
+      return dk;
+    };
+    std::vector<D1Row> rows;
+    for (const auto& g : gf->gp) {
+      if (g.seg_end - g.seg_begin != 1 || g.c != BUF_T0 || g.N != n || g.ldc != n)
+        throw Error(TCI_ERR_INTERNAL, "unexpected one-external problem");
+      const GemmSeg& x = gf->gs[(size_t)g.seg_begin];
+      if (x.a != BUF_WV || x.b != BUF_D || x.tA || x.tB || x.lda != n || x.ldb != n || x.K != n || x.alpha != 1.0 ||
+          g.beta != 0.0)
+        throw Error(TCI_ERR_INTERNAL, "unexpected one-external segment");
+      const i64 h = dk2h[(size_t)dk_of(x.offB)], ml = ls.dh_len[(size_t)h];
+      check_range(BUF_WV, x.offA, g.M * n);
+      check_range(BUF_T0, g.offC, g.M * n);
+      check_range(BUF_D, x.offB, n2);
+      for (i64 t = 0; t < g.M; ++t)
+        rows.push_back(D1Row{ptr(BUF_WV, x.offA + t * n), ptr(BUF_D, x.offB), ptr(BUF_T0, g.offC + t * n),
+                             ddl + ls.dh_off[(size_t)h], (int)ml});
+    }
+    std::vector<D1Target> tg;
+    long long tiles = 0;
+    for (const auto& g : gr->gp) {
+      if (g.seg_end - g.seg_begin != 1 || g.c != BUF_R || g.M != n || g.N != n || g.ldc != n)
+        throw Error(TCI_ERR_INTERNAL, "unexpected one-external reverse problem");
+      const GemmSeg& x = gr->gs[(size_t)g.seg_begin];
+      if (x.a != BUF_WV || x.b != BUF_T0 || !x.tA || x.tB || x.lda != n || x.ldb != n || x.alpha != 1.0 ||
+          g.beta != 1.0)
+        throw Error(TCI_ERR_INTERNAL, "unexpected one-external reverse segment");
+      const i64 h = dk2h[(size_t)dk_of(g.offC)], ml = ls.dh_len[(size_t)h];
+      if (ml == 0) continue;
+      check_range(BUF_WV, x.offA, x.K * n);
+      check_range(BUF_T0, x.offB, x.K * n);
+      check_range(BUF_R, g.offC, n2);
+      tg.push_back(D1Target{ptr(BUF_R, g.offC), ptr(BUF_WV, x.offA), ptr(BUF_T0, x.offB), ddl + ls.dh_off[(size_t)h],
+                            (int)ml, (int)x.K, tiles});
+      tiles += (ml * ml + 255) / 256;
+    }
+    fwd.d1 = 1;
+    fwd.kind = STEP_GEMM;
+    fwd.name = gf->name;
+    fwd.d1_rows = upload(rows, owned, stream);
+    fwd.d1_nrows = (long long)rows.size();
+    rev.d1 = 2;
+    rev.kind = STEP_GEMM;
+    rev.name = gr->name;
+    rev.d1_tg = upload(tg, owned, stream);
+    rev.d1_ntg = (int)tg.size();
+    rev.d1_tiles = tiles;
+    return true;
+  }
+
   // The N-2 <-> valence term of a local deck on the domains. Forward entries (pq, dk) come from the scatter
   // step's sources (F + pq nD + dk), reverse ones from the gather step's targets (G + pq nD + dk); the zero,
   // scatter and gather steps stay. Returns false (the padded steps stay) when the plan has no such term.
@@ -2820,6 +2949,10 @@ struct tci_ctx {
         continue;
       }
       if (s.d3_skip) continue;
+      if (s.d1) {
+        k += (s.d1_nrows > 0 || s.d1_tiles > 0) ? 1 : 0;
+        continue;
+      }
       if (s.dv) {
         k += (s.dv_nent > 0 || s.dv_tiles > 0) ? 1 : 0;
         continue;
@@ -3185,6 +3318,14 @@ struct tci_ctx {
     const bool tc_allext = precision == 1 || allext_tc_in_fp64;
     if (tc_allext && (s.name == "all-external zero" || s.name == "all-external split-k sum")) return;
     if (s.d3_skip) return;
+    if (s.d1 == 1) {  // local deck: the forward one-external term on the domains
+      if (s.d1_nrows > 0) dom1_forward<<<(unsigned)s.d1_nrows, 128, 0, stream>>>(s.d1_rows, plan.n);
+      return;
+    }
+    if (s.d1 == 2) {  // local deck: the reverse one-external term on the domains
+      if (s.d1_tiles > 0) dom1_reverse<<<(unsigned)s.d1_tiles, 256, 0, stream>>>(s.d1_tg, s.d1_ntg, plan.n);
+      return;
+    }
     if (s.dv == 1) {  // local deck: the forward N-2 <-> valence term on the domains
       if (s.dv_nent > 0)
         dom_dv_forward<<<(unsigned)((s.dv_nent + 7) / 8), 256, 0, stream>>>(s.dv_ent, s.dv_nent, s.dv_k, buf[BUF_D],
@@ -3836,6 +3977,8 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
     const bool dom3 = ls && ctx->lower_dom3(P.sigma_steps, *ls, d3f, d3r);
     DevStep dvf, dvr;
     const bool domdv = ls && ctx->lower_dom_dv(P.sigma_steps, *ls, dvf, dvr);
+    DevStep d1f, d1r;
+    const bool dom1 = ls && ctx->lower_dom1(P.sigma_steps, *ls, d1f, d1r);
     for (auto& s : P.sigma_steps) {
       if (ls && s.kind == STEP_GEMM && s.name == "dd two-external")
         ctx->sigma.push_back(ctx->lower_dom(s, *ls));
@@ -3849,6 +3992,10 @@ int ctx_from_plan(CsfSpace&& sp, Plan&& plan, const double* chol, int64_t device
         ctx->sigma.push_back(d3f);
       else if (dom3 && s.name == "three-external reverse")
         ctx->sigma.push_back(d3r);
+      else if (dom1 && s.name == "one-external forward")
+        ctx->sigma.push_back(d1f);
+      else if (dom1 && s.name == "one-external reverse")
+        ctx->sigma.push_back(d1r);
       else if (ls && s.kind == STEP_AXPY && s.name == "zero-external")
         ctx->sigma.push_back(ctx->lower_zero_local(s, *ls));
       else if (domdv && s.name == "dv forward") {
