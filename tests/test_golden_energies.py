@@ -10,7 +10,7 @@ Tolerance: the printed energies carry 15 digits; the Molden orbitals are
 orthonormal in this AO metric to 2e-8 and the reference screened its integrals
 at 1e-9, so agreement is expected at the 1e-9 level (observed: 1e-11 for the
 reference energy, 1e-9 and 2e-9 for the two roots).  The tests use 1e-8 Eh, the
-north star's FP64 energy bar, and 1 uEh for the mixed form.
+FP64 energy bar of this library, and 1 uEh for the mixed form.
 """
 import json
 import os
